@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark: IF-RK4 steps/s of the forced-turbulence workload on B200.
+
+Workload (default): FFF 256^3, Carati constant energy supply on shell 3
+(band 2 < |K| <= 3, epsilon = 0.1), nu = 1e-3, dt = 5e-4, initial E(k) ~
+k^4 exp(-2 (k/4)^2) random phase (seed 0), total energy 0.5, two-thirds
+dealiasing, rotational (u x omega) form, FP32 transforms with FP64 sums and
+integrating factor.  One step = one full IF-RK4 step (4 right-hand sides).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tarang_b200|reference]
+
+Multi-GPU (torchrun, one rank per GPU): the field does not shard (no pencil
+decomposition), so ranks run independent replicas; value = steps of all ranks
+/ max-over-ranks time ("scaling": "weak").  `--impl reference` times the FP64
+CPU restatement of the reference algorithm (oracle/tarang_ref.py) on the host
+cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 steps/s, FFF forced turbulence 256^3 (FP32 transforms, FP64 sums)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tarang_b200", choices=["tarang_b200", "reference"])
+    ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--form", default="rotational", choices=["rotational", "conservative"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
+    return ap.parse_args()
+
+
+def workload(N):
+    return {"workload": f"FFF {N}^3 forced isotropic turbulence (Carati energy supply shell 3, eps=0.1), "
+                        f"nu=1e-3, dt=5e-4, IC k^4 exp(-2(k/4)^2) E=0.5 seed 0",
+            "N": N, "nu": 1e-3, "dt": 5e-4, "k0": 4.0, "forcing_shell": 3, "epsilon": 0.1,
+            "dealias": "two_thirds"}
+
+
+def energy_supply(nsh):
+    es = np.zeros(nsh)
+    es[3] = 0.1
+    return es
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling (nvidia-smi) during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kclass: str, N: int, prec: str):
+    """DRAM bytes per launch of a kernel class from the committed ncu summary, scaled to N^3."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                p = line.split()
+                if len(p) >= 5 and p[0] == "traffic" and p[1] == kclass and p[2] == prec:
+                    n0, b = int(p[3]), float(p[4])
+                    return b * (N / n0) ** 3
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline_oracle(N, steps_cap_s=20.0, max_steps=50):
+    """Time the FP64 oracle (restatement of the reference algorithm) on this host."""
+    from oracle import tarang_ref as R
+    g = R.Grid((N, N, N))
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    cfg = R.FluidConfig(g, nu=1e-3, dt=5e-4, dealias_mode=R.DEALIAS_TWO_THIRDS,
+                        forcing=R.CaratiForcing(2.0, 3.0, energy_supply(g.n_shells())))
+    mis = g.modes_in_shell()
+    R.rk4_step(cfg, V, mis)  # warm-up (plans, page-in)
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        V = R.rk4_step(cfg, V, mis)
+        n += 1
+        if time.perf_counter() - t0 > steps_cap_s:
+            break
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    N = args.N
+    from oracle import tarang_ref as R
+    g = R.Grid((N, N, N))
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    cfg = R.FluidConfig(g, nu=1e-3, dt=5e-4, dealias_mode=R.DEALIAS_TWO_THIRDS,
+                        forcing=R.CaratiForcing(2.0, 3.0, energy_supply(g.n_shells())))
+    mis = g.modes_in_shell()
+    for _ in range(args.warmup):
+        V = R.rk4_step(cfg, V, mis)
+    budget = 150.0
+    n, t0 = 0, time.perf_counter()
+    while n < args.steps:
+        V = R.rk4_step(cfg, V, mis)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    v = n / el
+    cores = os.cpu_count()
+    sample = f"{n} of {args.steps} requested RK4 steps at {N}^3 (FP64, scipy.fft workers={R.WORKERS}), {el:.1f} s"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload(N),
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import tarang_b200 as tb
+    from tarang_b200 import _lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    N = args.N
+    nsh = int(math.ceil(math.sqrt(3) * (N // 2))) + 1
+    forcing = tb.Forcing(2.0, 3.0, energy_supply(nsh))
+    plan = tb.Plan(N, precision=args.precision, nlin_form=args.form, dealias="two_thirds", nu=1e-3, dt=5e-4,
+                   forcing=forcing)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    plan.set_stream(stream)
+    u = plan.field(3)
+    E_ic = tb.spectrum_k4_gauss(plan.n_shells, 4.0)
+    plan.init_energy_spectrum(E_ic, 0, 0.5, u)
+    u0 = u.clone()
+
+    for _ in range(args.warmup):
+        plan.rk4_step(u, 1)
+    torch.cuda.synchronize()
+
+    clk = Clocks(local)
+    lib = plan.lib
+    L.check(lib.ts_profile_reset(plan.h), "profile_reset")
+    L.check(lib.ts_profile_enable(plan.h, 1), "profile_enable")
+    n_launch0 = tb.kernel_launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        plan.rk4_step(u, 1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = tb.kernel_launch_count() - n_launch0
+    L.check(lib.ts_profile_enable(plan.h, 0), "profile_disable")
+    prof = {}
+    import ctypes
+    for k, name in enumerate(L.KCLASS_NAMES):
+        tot, n, b = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+        L.check(lib.ts_profile_read(plan.h, k, ctypes.byref(tot), ctypes.byref(n), ctypes.byref(b)), "profile_read")
+        prof[name] = {"total_ms": tot.value, "launches": n.value, "bytes_per_launch": b.value}
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_per_s = world * args.steps / (ms / 1e3)
+
+    # dominant kernel: largest total time
+    main_k = max((k for k in prof if k != "other"), key=lambda k: prof[k]["total_ms"])
+    pk = prof[main_k]
+    avg_s = pk["total_ms"] / max(pk["launches"], 1) / 1e3
+    achieved = pk["bytes_per_launch"] / avg_s / 1e9
+    peak, peak_kind = measured_peak()
+    roofline = {"bound": "hbm", "kernel": main_k, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": ncu_traffic(main_k, N, args.precision),
+                "bytes_per_launch": pk["bytes_per_launch"], "avg_launch_ms": avg_s * 1e3}
+    # whole-step roofline against the graded byte model 288 * N^3 * s
+    s_bytes = 4 if args.precision == "f32" else 8
+    model_bytes = 288.0 * N ** 3 * s_bytes
+    step_model = {"model_bytes_per_step": model_bytes,
+                  "model_GBps": model_bytes * steps_per_s / world / 1e9,
+                  "model_frac": model_bytes * steps_per_s / world / 1e9 / peak,
+                  "kernels": {k: {"avg_ms": v["total_ms"] / max(v["launches"], 1), "launches": v["launches"],
+                                  "GBps": (v["bytes_per_launch"] / (v["total_ms"] / max(v["launches"], 1) / 1e3) / 1e9)
+                                  if v["total_ms"] > 0 and v["bytes_per_launch"] > 0 else None,
+                                  "share": v["total_ms"] / sum(x["total_ms"] for x in prof.values())}
+                              for k, v in prof.items()}}
+
+    extras = {}
+    e2e = None
+    cpu = None
+    if not args.no_extras:
+        # e2e: the reference-facing C-ABI call on HOST (pinned) buffers, copies inside the call
+        host = u.detach().to("cpu").pin_memory()
+        k_e2e = max(3, min(args.steps, 10))
+        plan.rk4_step(host, 1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k_e2e):
+            plan.rk4_step(host, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nbytes = host.numel() * host.element_size()
+        e2e = {"value": world * k_e2e / (ems / 1e3), "unit": "steps/s", "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": k_e2e}
+        # FP32 vs FP64 GPU (same nonlinear form): relative L2 and energy error after 5 steps, FP64 steps/s
+        if args.precision == "f32":
+            p64 = tb.Plan(N, precision="f64", nlin_form=args.form, dealias="two_thirds", nu=1e-3, dt=5e-4,
+                          forcing=forcing)
+            p64.set_stream(stream)
+            a32 = u0.clone()
+            a64 = u0.to(torch.complex128)
+            for _ in range(5):
+                plan.rk4_step(a32, 1)
+                p64.rk4_step(a64, 1)
+            torch.cuda.synchronize()
+            d = (a32.to(torch.complex128) - a64)
+            rel_l2 = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(a64))
+            e32, e64 = plan.energy(a32), p64.energy(a64)
+            k64 = max(3, min(args.steps, 10))
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            p64.rk4_step(a64, k64)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            extras["fp64_gpu_steps_per_s"] = k64 / (f0.elapsed_time(f1) / 1e3)
+            extras["fp32_vs_fp64_after_5_steps"] = {"rel_l2": rel_l2, "rel_energy": abs(e32 - e64) / e64}
+            extras["fp32_speedup_vs_fp64"] = (steps_per_s / world) / extras["fp64_gpu_steps_per_s"]
+            p64.close()
+        extras["max_div_end"] = plan.max_div(u)
+        extras["energy_end"] = plan.energy(u)
+        if rank == 0 and world == 1:
+            v, n, el = cpu_baseline_oracle(N)
+            from oracle import tarang_ref as R
+            cpu = {"value": v, "unit": "steps/s", "cores": R.WORKERS, "kind": "port",
+                   "sample": f"{n} RK4 steps of the same {N}^3 workload in FP64 (oracle/tarang_ref.py, "
+                             f"scipy.fft workers={R.WORKERS}), {el:.1f} s"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": steps_per_s, "unit": "steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": args.precision, "data": "synthetic",
+                "config": dict(workload(N), precision=args.precision, nlin_form=args.form,
+                               parallelism=f"replicas x{world}",
+                               l2="working set (12 spectral fields, %.2f GB) > L2 126 MB: inputs larger than L2"
+                                  % (12 * plan.N[0] * plan.N[1] * (plan.N[2] // 2 + 1) * (8 if args.precision == "f32" else 16) / 1e9)),
+                "roofline": roofline, "step_roofline": step_model, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clocks, "extras": extras}
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,162 @@
+/*
+ * tarang_b200 — C ABI of the B200 pseudo-spectral IF-RK4 hot path.
+ *
+ * Drop-in replacement for the nonlinear-term + RK4 step of the Tarang-2
+ * reference (anandogc/tarang, paths below are inside its trunk/lib/).  The
+ * reference binds these through its C++ seams: the abstract basis `Universal`
+ * (basis/basicfn/universal.h:48-), the static `Nlin_incompress` functions
+ * (fluid/incompressible/nlin/Nlin.h:69-101) and `Time_advance_incompress`
+ * (fluid/incompressible/time_advance/Time_advance.h:69-187).
+ *
+ * Conventions
+ *  - Every function returns a ts_status and never aborts (the reference prints
+ *    and calls exit/MPI_Abort, e.g. basis/FFF/pencil/FFF_pencil.cc:84-87).
+ *  - Spectral fields use the reference layout: complex (Nx, Ny, Nz/2+1), C
+ *    order, kx and ky in FFT order (FFF_pencil_inline.h:63-111); a vector field
+ *    is its three components V1, V2, V3 stored back to back.  Complex = two
+ *    reals (re, im) of the plan's precision (double for TS_F64, float for TS_F32).
+ *  - Real fields use the reference's padded layout (Nx, Ny, Nz+2)
+ *    (FFF_pencil.cc:212); the two pad values per line are ignored on input and
+ *    written as 0 on output.
+ *  - Normalisation (inferred from the reference's energy functions): forward
+ *    transforms divide by Nx*Ny*Nz (FFF) or by 2Nx*Ny*Nz (SFF); inverses are
+ *    unnormalised.
+ *  - Field pointers may be device pointers or host pointers; host pointers are
+ *    staged through plan-owned device buffers (copies inside the call).
+ *  - A plan is used by one host thread at a time; distinct plans are independent.
+ */
+#ifndef TARANG_B200_H
+#define TARANG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TS_OK = 0,
+  TS_ERR_ARG = 1,         /* invalid argument / unsupported size */
+  TS_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  TS_ERR_NAN = 3,         /* a NaN / Inf was detected in the state */
+  TS_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+  TS_ERR_UNSUPPORTED = 5, /* valid but not implemented for this basis / precision */
+  TS_ERR_NOMEM = 6        /* device allocation failed */
+} ts_status;
+
+typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1 } ts_basis;
+typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
+typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;
+typedef enum { TS_DEALIAS_NONE = 0, TS_DEALIAS_REFERENCE_CORNER = 1, TS_DEALIAS_TWO_THIRDS = 2 } ts_dealias;
+typedef enum { TS_FORCE_NONE = 0, TS_FORCE_CARATI_ENERGY_SUPPLY = 1, TS_FORCE_RBC = 51 } ts_force;
+
+/* Solver configuration.  Field names follow the reference's para.yaml keys
+ * where one exists (global/Global.h:65-259). */
+typedef struct {
+  int basis;            /* ts_basis (program.basis_type) */
+  int N[3];             /* field.N, powers of two 16..1024 */
+  double kfactor[3];    /* field.kfactor (reference kfactor[1..3]) */
+  int precision;        /* ts_precision (build option -DREAL) */
+  int nlin_form;        /* ts_nlin_form */
+  int dealias_mode;     /* ts_dealias (program.alias_option) */
+  int reality_fix;      /* program.apply_strong_realitycond_alltime_switch */
+  double nu;            /* field.diss_coefficients[0] (velocity) */
+  double kappa;         /* field.diss_coefficients[1] (scalar) */
+  double dt;            /* time.dt_fixed */
+  int force_type;       /* ts_force (force.field_procedure) */
+  double force_inner_radius, force_outer_radius; /* Carati band (force.parameters) */
+  const double* energy_supply;   /* per shell ceil|K| (in/forcing.txt), copied at create */
+  const double* helicity_supply; /* may be NULL */
+  int n_supply;
+  double Ra, Pr;        /* PHYSICS.Rayleigh, PHYSICS.Prandtl (RBC, PRLARGE / ULARGE) */
+} ts_config;
+
+typedef struct ts_plan ts_plan;
+
+/* Fill *cfg with defaults: FFF, N = 64^3, kfactor 1, F64, conservative,
+ * reference-corner dealias, reality fix on, nu = 0.01, dt = 1e-3, no force. */
+void ts_config_default(ts_config* cfg);
+
+/* Replaces the FFF_PENCIL / SFF_PENCIL constructor + fftk.Init
+ * (FFF_pencil.cc:31-135, SFF_pencil.cc:38-): allocates twiddles and workspace. */
+int ts_plan_create(const ts_config* cfg, ts_plan** plan);
+int ts_plan_destroy(ts_plan* plan);
+/* Stream for every later call (cudaStream_t; NULL = legacy default stream). */
+int ts_plan_set_stream(ts_plan* plan, void* stream);
+/* Complex elements per component (Nx*Ny*(Nz/2+1)) and bytes per complex. */
+int ts_plan_sizes(const ts_plan* plan, long long* elems_per_comp, int* bytes_per_complex);
+/* Number of shells of E(k): Min_radius_outside()+1 (FFF_pencil_inline.h:497-504). */
+int ts_plan_num_shells(const ts_plan* plan, int* n_shells);
+/* Set the fixed time step (global.time.dt). */
+int ts_plan_set_dt(ts_plan* plan, double dt);
+
+/* Universal::Forward_transform / Inverse_transform (FFF_pencil_tr.cc:43-66,
+ * SFF_pencil_tr.cc:43-68).  parity replaces global.program.sincostr_switch:
+ * "FFF" for FFF; "SFF" (sine along x) or "CFF" (cosine along x) for SFF.
+ * real: (Nx,Ny,Nz+2) padded; spec: (Nx,Ny,Nz/2+1).  ncomp fields back to back. */
+int ts_fft_forward(ts_plan* plan, const char* parity, const void* real_in, void* spec_out, int ncomp);
+int ts_fft_inverse(ts_plan* plan, const char* parity, const void* spec_in, void* real_out, int ncomp);
+
+/* Nlin_incompress::Compute_nlin(FluidVF&) (compute_nlin.cc:58-109): dealias U
+ * in place (as the reference does), then nlin_i = sum_j i K_j F[u_i u_j]
+ * (conservative) or -F[u x omega] (rotational).  u_hat, nlin_hat: 3 components. */
+int ts_nlin(ts_plan* plan, void* u_hat, void* nlin_hat);
+
+/* Time_advance_incompress::RK4(U,P,F) (RK.cc:91-170) + strong reality fix
+ * (Time_advance.cc:59-60), nsteps times, in place on u_hat (3 components).
+ * FFF with force_type NONE or CARATI_ENERGY_SUPPLY. */
+int ts_rk4_step(ts_plan* plan, void* u_hat, int nsteps);
+
+/* RK4(U,T,P,F) for RBC (RK_SF.cc:97-221), SFF basis, PRLARGE/ULARGE. */
+int ts_rk4_step_rbc(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
+
+/* CVF::Compute_total_energy (Cvf.cc:213-221): sum over ncomp components. */
+int ts_energy(ts_plan* plan, const void* a_hat, int ncomp, double* energy);
+/* Universal::Compute_shell_spectrum (universal_energy.cc:279-366), summed over
+ * ncomp components: Ek[n_shells]. */
+int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, int n_shells);
+/* Energy flux through spheres: Pi(R_i) = sum_{|K|<=R_i} 2 mult Re(N.U*) with
+ * N = F[(u.grad)u] of the dealiased U (one pass; equals EnergyTr::Compute_flux,
+ * compute_flux.cc:51-65, for alias-free fields).  radii ascending. */
+int ts_flux(ts_plan* plan, const void* u_hat, const double* radii, int n_radii, double* Pi);
+/* max |div U| (universal_basic.cc:343-356). */
+int ts_max_div(ts_plan* plan, const void* u_hat, double* max_div);
+/* Nusselt number, PRLARGE/ULARGE (Correlation.cc:154-156). */
+int ts_nusselt(ts_plan* plan, const void* u_hat, const void* T_hat, double* Nu);
+
+/* Random-phase solenoidal FFF field with shell energies E_ic[n] (construction of
+ * init_cond_energy.cc:67-120; counter-based splitmix64 phases from seed), then the
+ * strong reality fix and a rescale to total energy target_energy (<= 0: no rescale). */
+int ts_init_energy_spectrum(ts_plan* plan, const double* E_ic, int n, uint64_t seed, double target_energy,
+                            void* u_hat);
+
+/* Kernel classes of one right-hand-side evaluation, for ts_profile_read. */
+typedef enum {
+  TS_KCLASS_INV_X = 0,  /* dealias + inverse FFT along x (+ vorticity) */
+  TS_KCLASS_Y_INV = 1,  /* inverse FFT along y */
+  TS_KCLASS_Z = 2,      /* C2R z + real-space products + R2C z */
+  TS_KCLASS_Y_FWD = 3,  /* forward FFT along y */
+  TS_KCLASS_FWD_X = 4,  /* forward FFT along x + projection + RK stage update */
+  TS_KCLASS_OTHER = 5,  /* forcing and reality kernels */
+  TS_KCLASS_COUNT = 6
+} ts_kernel_class;
+
+/* Per-kernel-class timing with CUDA events recorded on the plan's stream around
+ * every launch of ts_rk4_step (no reference counterpart: the reference times
+ * the whole run with time(), main.cc:105-109).  bytes_per_launch is the
+ * algorithmic traffic of one launch (every field read or written once). */
+int ts_profile_enable(ts_plan* plan, int enable);
+int ts_profile_reset(ts_plan* plan);
+int ts_profile_read(ts_plan* plan, int kernel_class, double* total_ms, long long* launches,
+                    double* bytes_per_launch);
+
+/* Number of kernels this library has launched since load (diagnostics). */
+long long ts_kernel_launch_count(void);
+/* Last CUDA error string seen by the library ("" if none). */
+const char* ts_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

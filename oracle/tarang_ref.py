@@ -1,0 +1,837 @@
+"""FP64 CPU oracle for the Tarang-2 pseudo-spectral IF-RK4 hot path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker for the CUDA product
+path: only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` /
+``--impl reference`` legs of ``bench.py`` may import it.  The product path
+(``tarang_b200``) never calls it and fails loudly when its CUDA library is
+missing.
+
+What it restates (file:line are paths inside anandogc/tarang ``trunk/lib``):
+
+* FFF basis index maps, wavenumbers, multiplicity   basis/FFF/pencil/FFF_pencil_inline.h:63-111,486-504,583-602
+* FFF transforms (FFTK over FFTW, forward / N^3)    basis/FFF/pencil/FFF_pencil_tr.cc:43-66
+* i k derivatives                                    basis/FFF/pencil/FFF_pencil_tr.cc:70-145
+* dealias (corner box, intersection semantics)       basis/FFF/pencil/FFF_pencil_basic.cc:87-90,228-259
+* strong reality condition                           basis/FFF/pencil/FFF_pencil_basic.cc:139-179
+* conservative nonlinear term                        fluid/incompressible/nlin/compute_nlin.cc:58-109,
+                                                     fluid/incompressible/nlin/compute_diag_offdiag.cc:47-112
+* pressure / projection / rhs                        fluid/incompressible/Pressure.cc:56-72,
+                                                     basis/basicfn/universal_basic.cc:202-225,343-363,
+                                                     fluid/incompressible/time_advance/Tadvance_functions.cc:45-53,148-191
+* IF-RK4 with the Single_time_step branch table      fluid/incompressible/time_advance/RK.cc:91-170,
+                                                     Tadvance_functions.cc:298-324,566-570,
+                                                     fluid/fluid_base/FluidVF.cc:308-389
+* Carati constant energy supply (non-global alpha)   fluid/fluid_base/force/compute_force_Carati.cc:61-210,
+                                                     force_alpha_beta.cc:56-85, compute_force_main.cc:43-80
+* shell spectrum E(k) (Stepanov normalisation)       basis/basicfn/universal_energy.cc:279-366
+* modes_in_shell                                     basis/basicfn/universal_basic.cc:104-143
+* total energy                                       basis/FFF/pencil/FFF_pencil_energy.cc:59-68, fields/Cvf.cc:213-221
+* energy flux Pi(R) per sphere                       fluid/incompressible/energytr/compute_flux.cc:51-65,
+                                                     fill_space.cc:56-64, prod_nlinV.cc:61-69,
+                                                     basis/basicfn/universal_ET.cc:51-70
+* helical random-phase IC construction               fluid/fluid_base/io/input/init_cond_energy.cc:67-120,
+                                                     fields/Cvf.cc:387-452, FFF_pencil_inline.h:228-247,819-845,
+                                                     basis/basicfn/basicfn_inline.h:357-405
+* SFF basis (sin/cos along x)                        basis/SFF/pencil/SFF_pencil_tr.cc:43-174,
+                                                     SFF_pencil_basic.cc:94-97,143-167,
+                                                     SFF_pencil_inline.h:63-109,412-430,492-515,
+                                                     SFF_pencil_energy.cc:76-95, global/Global.cc:137-165
+* Boussinesq RBC step (PRLARGE / ULARGE)             fluid/incompressible/time_advance/RK_SF.cc:97-221,
+                                                     Tadvance_functions.cc:57-90,226-237,372-395,477-489,589-611,
+                                                     fluid/incompressible/nlin/compute_nlin_SF.cc:75-142,
+                                                     compute_diag_offdiag.cc:116-136,
+                                                     fluid/fluid_base/force/compute_force_RBC.cc:104-150,
+                                                     fluid/fluid_base/Correlation.cc:144-160
+
+Parity status: the transform arithmetic of the reference lives in the
+un-vendored FFTK library (no source, no version pin) and the reference ships
+no golden vectors or tests, so parity at the FFTK boundary is UNPINNED.  The
+FFF convention (forward divides by N^3, inverse unscaled) is inferred from the
+reference's energy functions and Taylor-Green IC and checked here by
+known-answer tests.  The SFF x-grid stagger (type-II/III sin/cos pair) is a
+choice, pinned only by the energy / Parseval identities.
+
+Random initial conditions use this project's counter-based splitmix64
+generator (the reference seeds Blitz++ with ``my_id*time(0)``,
+init_cond_energy.cc:75-76, which is not reproducible); the CUDA library
+implements the same generator bit-for-bit.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.fft as sfft
+
+MYEPS = 1e-15    # global/Global.cc:62
+MYEPS2 = 1e-5    # global/Global.cc:63
+
+DEALIAS_NONE = 0
+DEALIAS_REFERENCE_CORNER = 1
+DEALIAS_TWO_THIRDS = 2
+
+WORKERS = int(os.environ.get("TS_ORACLE_WORKERS", os.cpu_count() or 1))
+
+
+# ----------------------------------------------------------------------------
+# counter-based RNG (this project's own; identical in csrc/ic.cu)
+# ----------------------------------------------------------------------------
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser (Steele, Lea & Flood 2014) on a uint64 array."""
+    with np.errstate(over="ignore"):
+        z = (x + np.uint64(0x9E3779B97F4A7C15)) & _M64
+        z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & _M64
+        z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & _M64
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform01(seed: int, counter: np.ndarray) -> np.ndarray:
+    """U[0,1) double from (seed, counter): splitmix64(splitmix64(seed) ^ counter) >> 11."""
+    key = _splitmix64(np.array([seed], dtype=np.uint64))[0]
+    h = _splitmix64(key ^ counter.astype(np.uint64))
+    return (h >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+# ----------------------------------------------------------------------------
+# grid / basis
+# ----------------------------------------------------------------------------
+@dataclass
+class Grid:
+    """Spectral grid of one field: complex shape (Nx, Ny, Nz//2+1), C order.
+
+    FFF: kx, ky in FFT order (``Get_kx`` FFF_pencil_inline.h:63, ``Get_ky`` :94),
+    kz = 0..Nz/2 (:107).  SFF: kx = lx = 0..Nx-1 (SFF_pencil_inline.h:63).
+    ``kfactor`` is (kf1, kf2, kf3), i.e. the reference's kfactor[1..3].
+    """
+    N: tuple
+    kfactor: tuple = (1.0, 1.0, 1.0)
+    basis: str = "FFF"
+    kx: np.ndarray = field(init=False)
+    ky: np.ndarray = field(init=False)
+    kz: np.ndarray = field(init=False)
+
+    def __post_init__(self):
+        Nx, Ny, Nz = self.N
+        lx = np.arange(Nx)
+        if self.basis == "FFF":
+            self.kx = np.where(lx <= Nx // 2, lx, lx - Nx)
+        elif self.basis == "SFF":
+            self.kx = lx.copy()
+        else:
+            raise ValueError(self.basis)
+        ly = np.arange(Ny)
+        self.ky = np.where(ly <= Ny // 2, ly, ly - Ny)
+        self.kz = np.arange(Nz // 2 + 1)
+
+    @property
+    def shape(self):
+        Nx, Ny, Nz = self.N
+        return (Nx, Ny, Nz // 2 + 1)
+
+    @property
+    def rshape(self):
+        return tuple(self.N)
+
+    def K(self):
+        kf = self.kfactor
+        Kx = (self.kx * kf[0]).astype(np.float64)[:, None, None]
+        Ky = (self.ky * kf[1]).astype(np.float64)[None, :, None]
+        Kz = (self.kz * kf[2]).astype(np.float64)[None, None, :]
+        return Kx, Ky, Kz
+
+    def Ksqr(self):
+        Kx, Ky, Kz = self.K()
+        # universal_basic.cc:202-225 accumulates Kx^2 + Ky^2 + Kz^2 in this order
+        return (Kx ** 2 + Ky ** 2) + Kz ** 2
+
+    def Kmag(self):
+        return np.sqrt(self.Ksqr())
+
+    def multiplicity(self):
+        """Multiplicity_factor: FFF_pencil_inline.h:583-602, SFF_pencil_inline.h:492-515."""
+        Nx, Ny, Nz = self.N
+        kx = self.kx[:, None, None]
+        ky = self.ky[None, :, None]
+        kz = self.kz[None, None, :]
+        if self.basis == "FFF":
+            f = np.where(kz > 0, 1.0, 0.5)
+            dbl = (kx == Nx // 2) | ((ky == Ny // 2) & (Ny > 1))
+            return np.broadcast_to(np.where(dbl, 2 * f, f), self.shape).copy()
+        m = kx
+        f = np.where(kz > 0, np.where(m > 0, 2.0, 1.0), np.where(m > 0, 1.0, 0.5))
+        dbl = (ky == Ny // 2) & (Ny > 1)
+        return np.broadcast_to(np.where(dbl, 2 * f, f), self.shape).copy()
+
+    def min_radius_outside(self):
+        Nx, Ny, Nz = self.N
+        kf = self.kfactor
+        if self.basis == "FFF":
+            return int(math.ceil(math.sqrt((Nx // 2 * kf[0]) ** 2 + (Ny // 2 * kf[1]) ** 2 + (Nz // 2 * kf[2]) ** 2)))
+        return int(math.ceil(math.sqrt(((Nx - 1) * kf[0]) ** 2 + (Ny // 2 * kf[1]) ** 2 + (Nz // 2 * kf[2]) ** 2)))
+
+    def n_shells(self):
+        return self.min_radius_outside() + 1
+
+    def modes_in_shell(self):
+        """Compute_modes_in_shell_array: universal_basic.cc:104-143 (full box count)."""
+        Nx, Ny, Nz = self.N
+        kf = self.kfactor
+        kxm, kym, kzm = Nx // 2, Ny // 2, Nz // 2
+        kx = np.arange(-kxm + 1, kxm + 1) * kf[0]
+        ky = np.arange(-kym + 1, kym + 1) * kf[1]
+        kz = np.arange(-kzm + 1, kzm + 1) * kf[2]
+        Kmag = np.sqrt(kx[:, None, None] ** 2 + ky[None, :, None] ** 2 + kz[None, None, :] ** 2)
+        idx = np.ceil(Kmag).astype(np.int64).ravel()
+        size = max(self.n_shells(), int(idx.max()) + 1)
+        return np.bincount(idx, minlength=size).astype(np.float64)
+
+
+# ----------------------------------------------------------------------------
+# dealias and reality
+# ----------------------------------------------------------------------------
+def dealias_mask(g: Grid, mode: int) -> np.ndarray:
+    """Boolean mask of modes ZEROED by the dealias step.
+
+    REFERENCE_CORNER restates FFF_PENCIL::Dealias (FFF_pencil_basic.cc:87-90 ->
+    Assign_sub_array :228-259): only the box where lx in [Nx/3+1, 2Nx/3-1] AND
+    ly in [Ny/3+1, 2Ny/3-1] AND lz in [Nz/3+1, Nz/2] (array indices) is zeroed.
+    SFF: lx in [2Nx/3+1, Nx-1] AND the same y/z ranges (SFF_pencil_basic.cc:94-97).
+    TWO_THIRDS zeroes every mode with 3|k_i| > N_i on any axis (3 m > 2 Nx on the
+    SFF sin/cos axis).
+    """
+    Nx, Ny, Nz = g.N
+    lx = np.arange(Nx)[:, None, None]
+    ly = np.arange(Ny)[None, :, None]
+    lz = np.arange(Nz // 2 + 1)[None, None, :]
+    if mode == DEALIAS_NONE:
+        return np.zeros(g.shape, dtype=bool)
+    if mode == DEALIAS_REFERENCE_CORNER:
+        if g.basis == "FFF":
+            mx = (lx >= Nx // 3 + 1) & (lx <= 2 * Nx // 3 - 1)
+        else:
+            mx = lx >= 2 * Nx // 3 + 1
+        my = (ly >= Ny // 3 + 1) & (ly <= 2 * Ny // 3 - 1)
+        mz = (lz >= Nz // 3 + 1) & (lz <= Nz // 2)
+        return np.broadcast_to(mx & my & mz, g.shape).copy()
+    if mode == DEALIAS_TWO_THIRDS:
+        kx = g.kx[:, None, None]
+        ky = g.ky[None, :, None]
+        kz = g.kz[None, None, :]
+        if g.basis == "FFF":
+            bx = 3 * np.abs(kx) > Nx
+        else:
+            bx = 3 * kx > 2 * Nx
+        m = bx | (3 * np.abs(ky) > Ny) | (3 * kz > Nz)
+        return np.broadcast_to(m, g.shape).copy()
+    raise ValueError(mode)
+
+
+def dealias(g: Grid, A: np.ndarray, mode: int) -> np.ndarray:
+    B = A.copy()
+    B[..., dealias_mask(g, mode)] = 0
+    return B
+
+
+def reality_fix(g: Grid, A: np.ndarray) -> np.ndarray:
+    """Satisfy_strong_reality_condition_in_Array on one complex array.
+
+    FFF (FFF_pencil_basic.cc:139-179): for kx<0 and ky != Ny/2,
+    A(kx,ky,0) = conj(A(-kx,-ky,0)); for kx=0, ky<0, A(0,ky,0) = conj(A(0,-ky,0));
+    then the kz=Nz/2 plane is zeroed.
+    SFF (SFF_pencil_basic.cc:143-167): for every m and ky<=0,
+    A(m,ky,0) = conj(A(m,-ky,0)); kz=Nz/2 plane zeroed.
+    """
+    Nx, Ny, Nz = g.N
+    B = A.copy()
+    plane = A[:, :, 0].copy()
+    iy_minus = (-g.ky) % Ny  # Get_iy(-ky)
+    if g.basis == "FFF":
+        for lx in range(Nx // 2 + 1, Nx):
+            mkx = -g.kx[lx]
+            sel = g.ky != Ny // 2
+            B[lx, sel, 0] = np.conj(plane[mkx, iy_minus[sel]])
+        sel = g.ky < 0
+        B[0, sel, 0] = np.conj(plane[0, iy_minus[sel]])
+    else:
+        sel = g.ky <= 0
+        B[:, sel, 0] = np.conj(plane[:, iy_minus[sel]])
+    B[:, :, Nz // 2] = 0
+    return B
+
+
+def reality_fix_vec(g: Grid, V: np.ndarray) -> np.ndarray:
+    return np.stack([reality_fix(g, V[i]) for i in range(V.shape[0])])
+
+
+# ----------------------------------------------------------------------------
+# transforms
+# ----------------------------------------------------------------------------
+def _x_forward_sincos(g: Grid, B: np.ndarray, parity: str) -> np.ndarray:
+    """Sine/cosine analysis along x (axis 0) with the FFTW RODFT10/REDFT10 scaling / (2 Nx).
+
+    Sine: coefficient of 2 sin(m pi x/Lx) stored at lx=m for m=1..Nx-1 (lx=0 is 0,
+    the m=Nx coefficient is dropped).  Cosine: c_0 + sum 2 c_m cos(m pi x/Lx), m=0..Nx-1.
+    Staggered grid x_j = (j+1/2) Lx/Nx (type-II forward / type-III inverse).
+    """
+    Nx = g.N[0]
+    if parity == "S":
+        Y = sfft.dst(B, type=2, axis=0, workers=WORKERS) / (2.0 * Nx)
+        out = np.zeros_like(Y)
+        out[1:] = Y[:-1]
+        return out
+    if parity == "C":
+        return sfft.dct(B, type=2, axis=0, workers=WORKERS) / (2.0 * Nx)
+    raise ValueError(parity)
+
+
+def _x_inverse_sincos(g: Grid, A: np.ndarray, parity: str) -> np.ndarray:
+    if parity == "S":
+        Y = np.zeros_like(A)
+        Y[:-1] = A[1:]
+        return sfft.dst(Y, type=3, axis=0, workers=WORKERS)
+    if parity == "C":
+        return sfft.dct(A, type=3, axis=0, workers=WORKERS)
+    raise ValueError(parity)
+
+
+def forward(g: Grid, ur: np.ndarray, parity: str = "F") -> np.ndarray:
+    """Real (Nx,Ny,Nz) -> spectral (Nx,Ny,Nz/2+1).  FFF: A = N^-3 sum u e^{-ik.x}."""
+    if g.basis == "FFF":
+        return sfft.rfftn(ur, norm="forward", workers=WORKERS)
+    Byz = sfft.rfftn(ur, axes=(1, 2), norm="forward", workers=WORKERS)
+    return _x_forward_sincos(g, Byz, parity)
+
+
+def inverse(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
+    """Spectral -> real, unnormalised (u = sum A e^{ik.x}); imag of kz=0 and kz=Nz/2 ignored."""
+    if g.basis == "FFF":
+        return sfft.irfftn(A, s=g.rshape, norm="forward", workers=WORKERS)
+    Nx, Ny, Nz = g.N
+    Bx = _x_inverse_sincos(g, A, parity)
+    return sfft.irfftn(Bx, s=(Ny, Nz), axes=(1, 2), norm="forward", workers=WORKERS)
+
+
+# ----------------------------------------------------------------------------
+# derivatives (FFF: i K ; SFF x: real factor by parity)
+# ----------------------------------------------------------------------------
+def xderiv(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
+    """FFF_pencil_tr.cc:70-79 (i Kx); SFF_pencil_tr.cc:77-90 (S -> +Kx, C -> -Kx)."""
+    Kx, _, _ = g.K()
+    if g.basis == "FFF":
+        return (1j * Kx) * A
+    return (Kx if parity == "S" else -Kx) * A
+
+
+def yderiv(g: Grid, A: np.ndarray) -> np.ndarray:
+    _, Ky, _ = g.K()
+    return (1j * Ky) * A
+
+
+def zderiv(g: Grid, A: np.ndarray) -> np.ndarray:
+    _, _, Kz = g.K()
+    return (1j * Kz) * A
+
+
+# SFF parity strings (global/Global.cc:137-145) -> first letter is the x parity
+SFF_PARITY = {"Vx": "S", "Vy": "C", "Vz": "C", "div": "C", "Vi2": "C", "VxVy": "S", "VxVz": "S",
+              "VyVz": "C", "F": "S", "FVx": "C", "FVy": "S", "FVz": "S"}
+
+
+def _par(g: Grid, key: str) -> str:
+    return "F" if g.basis == "FFF" else SFF_PARITY[key]
+
+
+# ----------------------------------------------------------------------------
+# nonlinear term
+# ----------------------------------------------------------------------------
+def velocity_real(g: Grid, V: np.ndarray) -> list:
+    """CVF::Inverse_transform (fields/Cvf.cc:172-185) with the Vx/Vy/Vz parities."""
+    return [inverse(g, V[0], _par(g, "Vx")), inverse(g, V[1], _par(g, "Vy")), inverse(g, V[2], _par(g, "Vz"))]
+
+
+def nlin_conservative_from_real(g: Grid, ur: list, wr: list | None = None) -> np.ndarray:
+    """N_i = sum_j D_j F[u_j w_i] in the reference's accumulation order.
+
+    Compute_nlin_diag / Compute_nlin_offdiag (compute_diag_offdiag.cc:47-98) for
+    w = u, and the giver form (compute_nlin_ET_VF.cc:71-87) for w given.
+    """
+    if wr is None:
+        wr = ur
+    p = lambda k: _par(g, k)
+    n1 = xderiv(g, forward(g, ur[0] * wr[0], p("Vi2")), p("Vi2"))
+    n2 = yderiv(g, forward(g, ur[1] * wr[1], p("Vi2")))
+    n3 = zderiv(g, forward(g, ur[2] * wr[2], p("Vi2")))
+    if wr is ur:
+        X = forward(g, ur[0] * ur[1], p("VxVy"))
+        n1 = n1 + yderiv(g, X)
+        n2 = n2 + xderiv(g, X, p("VxVy"))
+        X = forward(g, ur[1] * ur[2], p("VyVz"))
+        n2 = n2 + zderiv(g, X)
+        n3 = n3 + yderiv(g, X)
+        X = forward(g, ur[2] * ur[0], p("VxVz"))
+        n1 = n1 + zderiv(g, X)
+        n3 = n3 + xderiv(g, X, p("VxVz"))
+    else:
+        # giver form: nlin_i = sum_j D_j F[u_j w_i]
+        n1 = n1 + yderiv(g, forward(g, ur[1] * wr[0], p("VxVy"))) + zderiv(g, forward(g, ur[2] * wr[0], p("VxVz")))
+        n2 = n2 + xderiv(g, forward(g, ur[0] * wr[1], p("VxVy")), p("VxVy")) + zderiv(g, forward(g, ur[2] * wr[1], p("VyVz")))
+        n3 = n3 + xderiv(g, forward(g, ur[0] * wr[2], p("VxVz")), p("VxVz")) + yderiv(g, forward(g, ur[1] * wr[2], p("VyVz")))
+    return np.stack([n1, n2, n3])
+
+
+def nlin_conservative(g: Grid, V: np.ndarray) -> np.ndarray:
+    """Compute_nlin on an already-dealiased field (compute_nlin.cc:58-109)."""
+    return nlin_conservative_from_real(g, velocity_real(g, V))
+
+
+def vorticity(g: Grid, V: np.ndarray) -> np.ndarray:
+    """omega = i K x V (FFF; Compute_vorticity universal_basic.cc:49-66)."""
+    Kx, Ky, Kz = g.K()
+    return np.stack([1j * (Ky * V[2] - Kz * V[1]), 1j * (Kz * V[0] - Kx * V[2]), 1j * (Kx * V[1] - Ky * V[0])])
+
+
+def nlin_rotational(g: Grid, V: np.ndarray) -> np.ndarray:
+    """N = -F[u x omega] (FFF only): equals the conservative N up to a gradient and aliasing."""
+    if g.basis != "FFF":
+        raise ValueError("rotational form is implemented for FFF only")
+    u = [inverse(g, V[i]) for i in range(3)]
+    W = vorticity(g, V)
+    w = [inverse(g, W[i]) for i in range(3)]
+    c1 = u[1] * w[2] - u[2] * w[1]
+    c2 = u[2] * w[0] - u[0] * w[2]
+    c3 = u[0] * w[1] - u[1] * w[0]
+    return -np.stack([forward(g, c1), forward(g, c2), forward(g, c3)])
+
+
+# ----------------------------------------------------------------------------
+# projection / rhs
+# ----------------------------------------------------------------------------
+def project_rhs(g: Grid, N: np.ndarray) -> np.ndarray:
+    """Pressure::Compute_pressure + Compute_rhs: N <- -(N + D p), p = div(N)/K^2, p(0)=0.
+
+    Pressure.cc:56-72, universal_basic.cc:202-225 (divide, A(0,0,0)=0),
+    Compute_divergence universal_basic.cc:343-352, Add_pressure_gradient and
+    Compute_rhs Tadvance_functions.cc:148-191.  SFF parities: div with Vx
+    (S -> +Kx), gradient with div parity (C -> -Kx).
+    """
+    div = xderiv(g, N[0], _par(g, "Vx")) + yderiv(g, N[1]) + zderiv(g, N[2])
+    K2 = g.Ksqr()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        p = div / K2
+    p[0, 0, 0] = 0
+    n1 = N[0] + xderiv(g, p, _par(g, "div"))
+    n2 = N[1] + yderiv(g, p)
+    n3 = N[2] + zderiv(g, p)
+    return -np.stack([n1, n2, n3])
+
+
+def max_abs_div(g: Grid, V: np.ndarray) -> float:
+    """max |div V| as in Universal::Compute_divergence(field) universal_basic.cc:343-356."""
+    div = xderiv(g, V[0], _par(g, "Vx")) + yderiv(g, V[1]) + zderiv(g, V[2])
+    return float(np.max(np.abs(div)))
+
+
+# ----------------------------------------------------------------------------
+# forcing: Carati constant energy supply, non-global alpha/beta
+# ----------------------------------------------------------------------------
+@dataclass
+class CaratiForcing:
+    inner_radius: float
+    outer_radius: float
+    energy_supply: np.ndarray      # per shell index (ceil |K|)
+    helicity_supply: np.ndarray | None = None
+
+
+def carati_force(g: Grid, V: np.ndarray, f: CaratiForcing, modes_in_shell: np.ndarray) -> np.ndarray:
+    """F = alpha V + beta omega on the band inner < |K| <= outer.
+
+    compute_force_Carati.cc:61-75 (no-forcing early exit), :158-205 (non-global
+    alpha/beta per mode), force_alpha_beta.cc:56-85 (F = alpha u + beta omega),
+    then compute_force_main.cc:67-73 (strong reality condition on F).
+    Modal energy |V|^2/2 (FFF_pencil_inline.h:607-610), modal helicity
+    K.(Re V x Im V) (:618-634), modal vorticity i K x V (:646-664).
+    """
+    F = np.zeros_like(V)
+    es = np.asarray(f.energy_supply, dtype=np.float64)
+    hs = np.zeros_like(es) if f.helicity_supply is None else np.asarray(f.helicity_supply, dtype=np.float64)
+    if abs(es.sum()) + abs(hs.sum()) < MYEPS:
+        return F
+    Kmag = g.Kmag()
+    band = (Kmag > f.inner_radius) & (Kmag <= f.outer_radius)
+    # the reference loops kx in [-kx_max, kx_max] etc. (kx_max = ceil(outer/kf)); with
+    # outer < N/2 every stored band mode is visited exactly once.
+    Kx, Ky, Kz = g.K()
+    Kx = np.broadcast_to(Kx, g.shape)
+    Ky = np.broadcast_to(Ky, g.shape)
+    Kz = np.broadcast_to(Kz, g.shape)
+    W = vorticity(g, V)
+    idxs = np.argwhere(band)
+    for (lx, ly, lz) in idxs:
+        K = Kmag[lx, ly, lz]
+        index = int(math.ceil(K))
+        v = V[:, lx, ly, lz]
+        modal_energy = float(np.sum(np.abs(v) ** 2) / 2)
+        if modal_energy > MYEPS:
+            eps_k = es[index] / modes_in_shell[index]
+            hel_k = hs[index] / modes_in_shell[index]
+            vr, vi = v.real, v.imag
+            Kv = np.array([Kx[lx, ly, lz], Ky[lx, ly, lz], Kz[lx, ly, lz]])
+            modal_hel = float(np.dot(Kv, np.cross(vr, vi)))
+            denr = 2.0 * ((K * modal_energy) ** 2 - modal_hel ** 2)
+            epsh_by_k_epse = hel_k / (K * eps_k) if eps_k != 0 else np.inf
+            if abs(denr) > MYEPS:
+                alpha = (K ** 2 * eps_k * modal_energy - hel_k * modal_hel) / denr
+                beta = (hel_k * modal_energy - eps_k * modal_hel) / denr
+            elif abs(epsh_by_k_epse - 1) < MYEPS:
+                alpha = eps_k / (4 * modal_energy)
+                beta = alpha / K
+            else:
+                raise RuntimeError("max helicity supply case")
+            F[:, lx, ly, lz] = alpha * v + beta * W[:, lx, ly, lz]
+    return reality_fix_vec(g, F)
+
+
+# ----------------------------------------------------------------------------
+# IF-RK4
+# ----------------------------------------------------------------------------
+@dataclass
+class FluidConfig:
+    grid: Grid
+    nu: float
+    dt: float
+    dealias_mode: int = DEALIAS_REFERENCE_CORNER
+    nlin_form: str = "conservative"        # or "rotational"
+    reality_fix: bool = True
+    forcing: CaratiForcing | None = None
+
+
+def exp_ksqr(g: Grid, A: np.ndarray, factor: float) -> np.ndarray:
+    """Array_exp_ksqr: A * exp(factor K^2) (universal_basic.cc:235-252)."""
+    return A * np.exp(factor * g.Ksqr())
+
+
+def fluid_rhs(cfg: FluidConfig, U: np.ndarray, mis: np.ndarray) -> tuple:
+    """Compute_force_TO_rhs (Tadvance_functions.cc:441-453).
+
+    Returns (rhs, dealiased U): the reference dealiases U in place inside
+    Compute_nlin (compute_nlin.cc:61-62), and the caller's Single_time_step
+    then works on the dealiased U.
+    """
+    g = cfg.grid
+    F = None
+    if cfg.forcing is not None:
+        F = carati_force(g, U, cfg.forcing, mis)       # forcing sees the un-dealiased U
+    Ud = dealias(g, U, cfg.dealias_mode) if cfg.dealias_mode else U.copy()
+    if cfg.nlin_form == "conservative":
+        N = nlin_conservative(g, Ud)
+    else:
+        N = nlin_rotational(g, Ud)
+    if F is not None:
+        N = N - F                                       # Add_force :45-53
+    return project_rhs(g, N), Ud
+
+
+def rk4_step(cfg: FluidConfig, U0: np.ndarray, mis: np.ndarray | None = None) -> np.ndarray:
+    """Time_advance_incompress::RK4(U,P,F), RK.cc:91-170, then the reality fix
+    (Time_advance.cc:59-60).  E(a) = exp(-nu K^2 a dt); Single_time_step branch
+    table Tadvance_functions.cc:298-324; Compute_RK4_parts :566-570."""
+    g = cfg.grid
+    if mis is None:
+        mis = g.modes_in_shell()
+    nu, dt = cfg.nu, cfg.dt
+    E = lambda A, a: exp_ksqr(g, A, -nu * a * dt)
+    Vcopy = U0.copy()
+    # stage 1: Single_time_step(.5,.5,.5): a==b -> Add then Mult
+    R, Ud = fluid_rhs(cfg, U0, mis)
+    U = E(Ud + (0.5 * dt) * R, 0.5)
+    tot = (dt / 6.0) * E(R, 1.0)
+    # stage 2: Single_time_step(.5,0,.5): b==0 -> Mult then Add
+    R, _ = fluid_rhs(cfg, U, mis)
+    U = E(Vcopy, 0.5) + (0.5 * dt) * R
+    tot = tot + (dt / 3.0) * E(R, 0.5)
+    # stage 3: Single_time_step(1,.5,1): Mult(a-b), Add, Mult(b)
+    R, _ = fluid_rhs(cfg, U, mis)
+    U = E(E(Vcopy, 0.5) + dt * R, 0.5)
+    tot = tot + (dt / 3.0) * E(R, 0.5)
+    # stage 4: Compute_RK4_parts(0, 1/6): no exp factor
+    R, _ = fluid_rhs(cfg, U, mis)
+    tot = tot + (dt / 6.0) * R
+    U = E(Vcopy, 1.0) + tot
+    if cfg.reality_fix:
+        U = reality_fix_vec(g, U)
+    return U
+
+
+# ----------------------------------------------------------------------------
+# diagnostics
+# ----------------------------------------------------------------------------
+def total_energy(g: Grid, V: np.ndarray) -> float:
+    """CVF::Compute_total_energy: per component sum|A|^2 - 1/2 sum_{kz=0}|A|^2 (FFF);
+    SFF weights 2 / 1 / 1/2 (SFF_pencil_energy.cc:76-95)."""
+    e = 0.0
+    for A in V:
+        a2 = np.abs(A) ** 2
+        if g.basis == "FFF":
+            e += a2.sum() - 0.5 * a2[:, :, 0].sum()
+        else:
+            e += 2 * a2.sum() - a2[:, :, 0].sum() - a2[0].sum() + 0.5 * a2[0, :, 0].sum()
+    return float(e)
+
+
+def total_energy_scalar(g: Grid, A: np.ndarray) -> float:
+    return total_energy(g, A[None])
+
+
+def cross_energy(g: Grid, A: np.ndarray, B: np.ndarray) -> float:
+    """Get_local_energy(A,B) = mydot with the same plane weights (FFF_pencil_energy.cc:81-89)."""
+    d = (A * np.conj(B)).real
+    if g.basis == "FFF":
+        return float(d.sum() - 0.5 * d[:, :, 0].sum())
+    return float(2 * d.sum() - d[:, :, 0].sum() - d[0].sum() + 0.5 * d[0, :, 0].sum())
+
+
+def shell_spectrum(g: Grid, V: np.ndarray, n: int = 0) -> np.ndarray:
+    """Compute_shell_spectrum per component and summed (universal_energy.cc:279-366).
+
+    Sk(ceil|K|) += mult |K|^n |A|^2 |K|^2; count += 2 mult; Sk *= 4 pi /(count kf1 kf2 kf3).
+    """
+    Kmag = g.Kmag()
+    idx = np.ceil(Kmag).astype(np.int64)
+    kmax = g.min_radius_outside()
+    mult = g.multiplicity()
+    ok = idx <= kmax
+    nsh = kmax + 1
+    count = np.bincount(idx[ok], weights=2 * mult[ok], minlength=nsh)
+    kf = g.kfactor
+    out = np.zeros(nsh)
+    for A in V:
+        w = mult * (Kmag ** n) * (np.abs(A) ** 2) * Kmag ** 2
+        Sk = np.bincount(idx[ok], weights=w[ok], minlength=nsh)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            Sk = np.where(count > 0, Sk * 4 * math.pi / (count * kf[0] * kf[1] * kf[2]), 0.0)
+        out += Sk
+    return out
+
+
+def shell_mult_single(g: Grid, A: np.ndarray, B: np.ndarray, inner: float, outer: float) -> float:
+    """Local_shell_mult_single universal_ET.cc:51-70: sum 2 mult Re(A B*) on inner<|K|<=outer."""
+    Kmag = g.Kmag()
+    sel = (Kmag > inner) & (Kmag <= outer)
+    return float(np.sum(2 * g.multiplicity()[sel] * (A[sel] * np.conj(B[sel])).real))
+
+
+def flux_per_sphere(g: Grid, U: np.ndarray, radii, dealias_mode: int) -> np.ndarray:
+    """EnergyTr::Compute_flux (compute_flux.cc:51-65): one giver nonlinear term per sphere.
+
+    Giver = U inside |K| <= R (Fill_in_sphere fill_space.cc:56-64); U and the giver
+    are dealiased; nlin_i = F[d_j(u_j giver_i)]; Pi(R) = -sum_{|K|>R} 2 mult Re(nlin.U*).
+    """
+    Ud = dealias(g, U, dealias_mode) if dealias_mode else U
+    Kmag = g.Kmag()
+    ur = velocity_real(g, Ud)
+    out = []
+    for R in radii:
+        G = np.where(Kmag <= R, Ud, 0)
+        G = dealias(g, G, dealias_mode) if dealias_mode else G
+        wr = velocity_real(g, G)
+        Nl = nlin_conservative_from_real(g, ur, wr)
+        out.append(-sum(shell_mult_single(g, Nl[i], Ud[i], R, np.inf) for i in range(3)))
+    return np.array(out)
+
+
+def flux_one_pass(g: Grid, U: np.ndarray, radii, dealias_mode: int) -> np.ndarray:
+    """Pi(R) = sum_{|K|<=R} 2 mult Re(N.U*), N = F[(u.grad)u] of the dealiased U.
+
+    Equal to the per-sphere form for solenoidal, alias-free (TWO_THIRDS) fields:
+    <u_<, (u.grad)u> = -<u_>, (u.grad)u_<>.
+    """
+    Ud = dealias(g, U, dealias_mode) if dealias_mode else U
+    N = nlin_conservative(g, Ud)
+    Kmag = g.Kmag()
+    mult = g.multiplicity()
+    d = 2 * mult * sum((N[i] * np.conj(Ud[i])).real for i in range(3))
+    return np.array([float(d[Kmag <= R].sum()) for R in radii])
+
+
+# ----------------------------------------------------------------------------
+# initial condition
+# ----------------------------------------------------------------------------
+def _polar_angle(kperp, kpll):
+    """Get_polar_angle basicfn_inline.h:357-377."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = np.where(np.abs(kperp) > MYEPS,
+                     np.where(np.abs(kpll) > MYEPS, np.arctan(kperp / np.where(kpll == 0, 1, kpll)), np.pi / 2),
+                     np.where(kpll >= 0, 0.0, np.pi))
+    return np.where(t >= 0, t, t + np.pi)
+
+
+def _azimuthal_angle(kh1, kh2):
+    """Get_azimuthal_angle basicfn_inline.h:389-405."""
+    kperp = np.sqrt(kh1 ** 2 + kh2 ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ang = np.arccos(np.clip(kh1 / np.where(kperp == 0, 1, kperp), -1, 1))
+    ang = np.where(kh2 >= 0, ang, 2 * np.pi - ang)
+    return np.where(np.abs(kperp) > MYEPS, ang, 0.0)
+
+
+def spectrum_k4_gauss(nsh: int, k0: float) -> np.ndarray:
+    """E_IC(s) = s^4 exp(-2 (s/k0)^2) for shell s>=1 (E_IC(0) = 0)."""
+    s = np.arange(nsh, dtype=np.float64)
+    E = s ** 4 * np.exp(-2.0 * (s / k0) ** 2)
+    E[0] = 0
+    return E
+
+
+def init_energy_spectrum(g: Grid, E_ic: np.ndarray, seed: int, target_energy: float | None = None,
+                         H_ic: np.ndarray | None = None) -> np.ndarray:
+    """Random-phase solenoidal field with per-shell energy E_ic (FFF).
+
+    Construction of Init_cond_energy_helicity_spectrum_k_ne0 (init_cond_energy.cc:67-120):
+    e_k = E_ic(ceil|K|)/modes_in_shell, a_+- = sqrt((e_k +- h_k/|K|)/2), random phases,
+    helical -> Craya (FFF_pencil_inline.h:232-236) -> Cartesian (:238-247) with the
+    anisotropy axis z (anisotropy_dirn 3: V = (vh1, vh2, vpll), Cvf.cc:416-424).
+    The phases come from this project's generator: counter 2m (plus) and 2m+1 (minus)
+    for linear mode index m = (lx*Ny + ly)*(Nz/2+1) + lz.  The mean mode is 0; the
+    strong reality condition is applied, then the field is rescaled to
+    ``target_energy`` (Tarang energy) when given.
+    """
+    if g.basis != "FFF":
+        raise ValueError("FFF only")
+    mis = g.modes_in_shell()
+    Kx, Ky, Kz = [np.broadcast_to(a, g.shape) for a in g.K()]
+    Kmag = g.Kmag()
+    idx = np.ceil(Kmag).astype(np.int64)
+    Eic = np.zeros(max(len(E_ic), idx.max() + 1))
+    Eic[:len(E_ic)] = E_ic
+    Hic = np.zeros_like(Eic)
+    if H_ic is not None:
+        Hic[:len(H_ic)] = H_ic
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ek = np.where(mis[np.minimum(idx, len(mis) - 1)] > 0, Eic[idx] / mis[np.minimum(idx, len(mis) - 1)], 0.0)
+        hk = np.where(mis[np.minimum(idx, len(mis) - 1)] > 0, Hic[idx] / mis[np.minimum(idx, len(mis) - 1)], 0.0)
+    live = (Kmag > MYEPS) & (ek >= MYEPS)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ap = np.sqrt(np.maximum((ek + hk / np.where(Kmag > 0, Kmag, 1)) / 2, 0))
+        am = np.sqrt(np.maximum((ek - hk / np.where(Kmag > 0, Kmag, 1)) / 2, 0))
+    m = np.arange(int(np.prod(g.shape)), dtype=np.uint64).reshape(g.shape)
+    php = 2 * np.pi * uniform01(seed, 2 * m)
+    phm = 2 * np.pi * uniform01(seed, 2 * m + 1)
+    up = ap * np.exp(1j * php)
+    um = am * np.exp(1j * phm)
+    U1 = 1j * (um - up)
+    U2 = um + up
+    theta = _polar_angle(np.sqrt(Kx ** 2 + Ky ** 2), Kz)
+    phi = _azimuthal_angle(Kx, Ky)
+    vpll = -U2 * np.sin(theta)
+    vh1 = U1 * np.sin(phi) + U2 * np.cos(theta) * np.cos(phi)
+    vh2 = -U1 * np.cos(phi) + U2 * np.sin(phi) * np.cos(theta)
+    V = np.stack([vh1, vh2, vpll])
+    V = np.where(live[None], V, 0)
+    V = reality_fix_vec(g, V)
+    if target_energy is not None:
+        e = total_energy(g, V)
+        V = V * math.sqrt(target_energy / e)
+    return V
+
+
+# ----------------------------------------------------------------------------
+# Boussinesq RBC on SFF (PRLARGE, ULARGE)
+# ----------------------------------------------------------------------------
+@dataclass
+class RBCConfig:
+    grid: Grid
+    Ra: float
+    Pr: float
+    dt: float
+    dealias_mode: int = DEALIAS_REFERENCE_CORNER
+    reality_fix: bool = True
+
+    @property
+    def nu(self):
+        return math.sqrt(self.Pr / self.Ra)      # Iscalar_main.cc ULARGE
+
+    @property
+    def kappa(self):
+        return 1.0 / math.sqrt(self.Pr * self.Ra)
+
+
+def rbc_rhs(cfg: RBCConfig, U: np.ndarray, T: np.ndarray) -> tuple:
+    """Compute_force_TO_rhs_RBC (Tadvance_functions.cc:477-489), PRLARGE / ULARGE.
+
+    Force (compute_force_RBC.cc:104-150): U.F1 = T, T.F = U.V1 (both from the
+    un-dealiased stage input).  Nonlinear: dealias U, T; T.nlin = sum_j D_j F[u_j T]
+    (compute_diag_offdiag.cc:116-136 with FVx/FVy/FVz parities) and the velocity
+    nlin; nlin -= F; pressure; rhs = -(nlin + grad p), T.rhs = -T.nlin.
+    """
+    g = cfg.grid
+    FU1 = T.copy()
+    FT = U[0].copy()
+    Ud = dealias(g, U, cfg.dealias_mode)
+    Td = dealias(g, T, cfg.dealias_mode)
+    ur = velocity_real(g, Ud)
+    Tr = inverse(g, Td, _par(g, "F"))
+    p = lambda k: _par(g, k)
+    Tn = xderiv(g, forward(g, ur[0] * Tr, p("FVx")), p("FVx"))
+    Tn = Tn + yderiv(g, forward(g, ur[1] * Tr, p("FVy")))
+    Tn = Tn + zderiv(g, forward(g, ur[2] * Tr, p("FVz")))
+    N = nlin_conservative_from_real(g, ur)
+    N[0] = N[0] - FU1
+    Tn = Tn - FT
+    return project_rhs(g, N), -Tn, Ud, Td
+
+
+def rbc_rk4_step(cfg: RBCConfig, U0: np.ndarray, T0: np.ndarray) -> tuple:
+    """RK4(U,T,P,F) RK_SF.cc:97-221 with Single_time_step_scalar (U with nu, T with kappa)."""
+    g = cfg.grid
+    dt = cfg.dt
+    EU = lambda A, a: exp_ksqr(g, A, -cfg.nu * a * dt)
+    ET = lambda A, a: exp_ksqr(g, A, -cfg.kappa * a * dt)
+    R, S, Ud, Td = rbc_rhs(cfg, U0, T0)
+    U = EU(Ud + 0.5 * dt * R, 0.5)
+    T = ET(Td + 0.5 * dt * S, 0.5)
+    totU = (dt / 6) * EU(R, 1.0)
+    totT = (dt / 6) * ET(S, 1.0)
+    R, S, _, _ = rbc_rhs(cfg, U, T)
+    U = EU(U0, 0.5) + 0.5 * dt * R
+    T = ET(T0, 0.5) + 0.5 * dt * S
+    totU = totU + (dt / 3) * EU(R, 0.5)
+    totT = totT + (dt / 3) * ET(S, 0.5)
+    R, S, _, _ = rbc_rhs(cfg, U, T)
+    U = EU(EU(U0, 0.5) + dt * R, 0.5)
+    T = ET(ET(T0, 0.5) + dt * S, 0.5)
+    totU = totU + (dt / 3) * EU(R, 0.5)
+    totT = totT + (dt / 3) * ET(S, 0.5)
+    R, S, _, _ = rbc_rhs(cfg, U, T)
+    totU = totU + (dt / 6) * R
+    totT = totT + (dt / 6) * S
+    U = EU(U0, 1.0) + totU
+    T = ET(T0, 1.0) + totT
+    if cfg.reality_fix:
+        U = reality_fix_vec(g, U)
+        T = reality_fix(g, T)
+    return U, T
+
+
+def nusselt(cfg: RBCConfig, U: np.ndarray, T: np.ndarray) -> float:
+    """Get_Nusselt_no PRLARGE/ULARGE (Correlation.cc:154-156): 1 + 2 sqrt(Ra Pr) <U1, T>."""
+    return 1.0 + 2.0 * math.sqrt(cfg.Ra * cfg.Pr) * cross_energy(cfg.grid, U[0], T)
+
+
+def rbc_temperature_ic(g: Grid, amp: float, kmax_grid: float, seed: int) -> np.ndarray:
+    """T perturbation: amplitude ``amp`` with uniform random phases on the modes whose grid
+    wavenumber |(m, ky, kz)| <= kmax_grid, m >= 1 (sine parity), kz < Nz/2; then the
+    strong reality condition.  Counter = linear mode index m."""
+    mm = g.kx[:, None, None]
+    ky = g.ky[None, :, None]
+    kz = g.kz[None, None, :]
+    r = np.sqrt(mm ** 2 + ky ** 2 + kz ** 2)
+    sel = np.broadcast_to((r <= kmax_grid) & (mm >= 1), g.shape)
+    cnt = np.arange(int(np.prod(g.shape)), dtype=np.uint64).reshape(g.shape)
+    ph = 2 * np.pi * uniform01(seed, cnt)
+    T = np.where(sel, amp * np.exp(1j * ph), 0)
+    return reality_fix(g, T)

@@ -1,0 +1,637 @@
+// C ABI of the B200 pseudo-spectral IF-RK4 path (declared in include/tarang_b200.h).
+//
+// The plan replaces the reference's FFF_PENCIL basis object + FFTK plan
+// (basis/FFF/pencil/FFF_pencil.cc:31-277) and the static work arrays of
+// Time_advance_incompress::RK4 (RK.cc:95-96: Vcopy, tot_Vrhs).  The caller's
+// u_hat is the state (the reference's U.cvf); the plan owns the stage field,
+// the RK accumulator, six product / transform work fields and twiddle tables.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+#include <stdio.h>
+#include <mutex>
+#include <vector>
+#include <string>
+#include "tarang_b200.h"
+#include "ts_launch.h"
+
+namespace ts {
+long long g_launches = 0;
+bool size_supported(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
+}  // namespace ts
+
+using namespace ts;
+
+static thread_local std::string g_last_error;
+
+#define CK(x)                                                   \
+  do {                                                          \
+    cudaError_t e_ = (x);                                       \
+    if (e_ != cudaSuccess) {                                    \
+      g_last_error = std::string(#x) + ": " + cudaGetErrorString(e_); \
+      return (int)(e_ == cudaErrorMemoryAllocation ? TS_ERR_NOMEM : TS_ERR_CUDA); \
+    }                                                           \
+  } while (0)
+
+#define CKS(x)                          \
+  do {                                  \
+    int s_ = (x);                       \
+    if (s_ != TS_OK) return s_;         \
+  } while (0)
+
+struct ts_plan {
+  ts_config cfg;
+  Geo g;
+  int prec;           // 0 f64, 1 f32
+  size_t cb;          // bytes per complex
+  cudaStream_t st = nullptr;
+  void* Ucur = nullptr;
+  void* tot = nullptr;
+  void* P = nullptr;  // 6 components
+  void* twx = nullptr;
+  void* twy = nullptr;
+  void* twz = nullptr;
+  void* fcube = nullptr;
+  int fkm = 0;
+  double* esup = nullptr;
+  double* hsup = nullptr;
+  double* mis_d = nullptr;
+  int nsup = 0;
+  std::vector<double> mis;  // modes_in_shell (host)
+  int nshells = 0;
+  double* dscr = nullptr;   // diagnostics scratch
+  size_t dscr_n = 0;
+  void* stage_u = nullptr;  // staging for host pointers (3 components)
+  void* stage_t = nullptr;  // staging for host pointers (1 component)
+  // per-kernel-class CUDA event timing (ts_profile_*)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_rec;
+  double prof_ms[TS_KCLASS_COUNT] = {0};
+  long long prof_n[TS_KCLASS_COUNT] = {0};
+};
+
+// ---------------------------------------------------------------------------
+// profiling: events around each launch of a kernel class
+// ---------------------------------------------------------------------------
+static cudaEvent_t prof_event(ts_plan* p) {
+  if (p->ev_used == p->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    p->ev_pool.push_back(e);
+  }
+  return p->ev_pool[p->ev_used++];
+}
+
+static void prof_collect(ts_plan* p) {
+  if (p->ev_rec.empty()) return;
+  cudaStreamSynchronize(p->st);
+  for (auto& r : p->ev_rec) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, r.second.first, r.second.second) == cudaSuccess) {
+      p->prof_ms[r.first] += ms;
+      p->prof_n[r.first] += 1;
+    }
+  }
+  p->ev_rec.clear();
+  p->ev_used = 0;
+}
+
+struct ProfScope {
+  ts_plan* p;
+  int cls;
+  cudaEvent_t b = nullptr;
+  ProfScope(ts_plan* p_, int c) : p(p_), cls(c) {
+    if (p->prof) {
+      if (p->ev_used + 2 > 8192) prof_collect(p);
+      b = prof_event(p);
+      if (b) cudaEventRecord(b, p->st);
+    }
+  }
+  ~ProfScope() {
+    if (p->prof && b) {
+      cudaEvent_t e = prof_event(p);
+      if (e) {
+        cudaEventRecord(e, p->st);
+        p->ev_rec.push_back({cls, {b, e}});
+      }
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+static int upload_twiddles(int L, void** dst) {
+  // exp(-2 pi i m / L), evaluated in double and rounded once to T
+  std::vector<T> h(2 * L);
+  for (int m = 0; m < L; ++m) {
+    const double a = -2.0 * M_PI * (double)m / (double)L;
+    h[2 * m] = (T)cos(a);
+    h[2 * m + 1] = (T)sin(a);
+  }
+  CK(cudaMalloc(dst, sizeof(T) * 2 * L));
+  CK(cudaMemcpy(*dst, h.data(), sizeof(T) * 2 * L, cudaMemcpyHostToDevice));
+  return TS_OK;
+}
+
+static void compute_modes_in_shell(ts_plan* p) {
+  // Compute_modes_in_shell_array (universal_basic.cc:104-143): full box count
+  const int Nx = p->g.Nx, Ny = p->g.Ny, Nz = p->g.Nz;
+  const double* kf = p->g.kf;
+  int kmax;
+  if (p->g.basis == 0)
+    kmax = (int)ceil(sqrt(pow((Nx / 2) * kf[0], 2) + pow((Ny / 2) * kf[1], 2) + pow((Nz / 2) * kf[2], 2)));
+  else
+    kmax = (int)ceil(sqrt(pow((Nx - 1) * kf[0], 2) + pow((Ny / 2) * kf[1], 2) + pow((Nz / 2) * kf[2], 2)));
+  p->nshells = kmax + 1;
+  const int kxm = Nx / 2, kym = Ny / 2, kzm = Nz / 2;
+  int top = kmax + 2;
+  {
+    const double m = sqrt(pow(kxm * kf[0], 2) + pow(kym * kf[1], 2) + pow(kzm * kf[2], 2));
+    if ((int)ceil(m) + 2 > top) top = (int)ceil(m) + 2;
+  }
+  p->mis.assign(top, 0.0);
+  for (int kx = -kxm + 1; kx <= kxm; ++kx)
+    for (int ky = -kym + 1; ky <= kym; ++ky)
+      for (int kz = -kzm + 1; kz <= kzm; ++kz) {
+        const double K = sqrt(pow(kx * kf[0], 2) + pow(ky * kf[1], 2) + pow(kz * kf[2], 2));
+        p->mis[(int)ceil(K)] += 1;
+      }
+}
+
+static int ensure_scratch(ts_plan* p, size_t n) {
+  if (p->dscr_n >= n) return TS_OK;
+  if (p->dscr) cudaFree(p->dscr);
+  p->dscr = nullptr;
+  p->dscr_n = 0;
+  CK(cudaMalloc(&p->dscr, n * sizeof(double)));
+  p->dscr_n = n;
+  return TS_OK;
+}
+
+static int ensure_stage(void** buf, size_t bytes) {
+  if (*buf) return TS_OK;
+  CK(cudaMalloc(buf, bytes));
+  return TS_OK;
+}
+
+// dispatch a Launch<T>::fn call on the plan's precision
+#define LAUNCH(p, fn, ...) \
+  ((p)->prec == 1 ? Launch<float>::fn(__VA_ARGS__) : Launch<double>::fn(__VA_ARGS__))
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void ts_config_default(ts_config* c) {
+  memset(c, 0, sizeof(*c));
+  c->basis = TS_BASIS_FFF;
+  c->N[0] = c->N[1] = c->N[2] = 64;
+  c->kfactor[0] = c->kfactor[1] = c->kfactor[2] = 1.0;
+  c->precision = TS_F64;
+  c->nlin_form = TS_NLIN_CONSERVATIVE;
+  c->dealias_mode = TS_DEALIAS_REFERENCE_CORNER;
+  c->reality_fix = 1;
+  c->nu = 0.01;
+  c->kappa = 0.01;
+  c->dt = 1e-3;
+  c->force_type = TS_FORCE_NONE;
+  c->Ra = 1e5;
+  c->Pr = 1.0;
+}
+
+long long ts_kernel_launch_count(void) { return g_launches; }
+const char* ts_last_error(void) { return g_last_error.c_str(); }
+
+int ts_plan_destroy(ts_plan* p) {
+  if (!p) return TS_ERR_ARG;
+  void* bufs[] = {p->Ucur, p->tot, p->P, p->twx, p->twy, p->twz, p->fcube, p->esup, p->hsup, p->mis_d, p->dscr,
+                  p->stage_u, p->stage_t};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
+  delete p;
+  return TS_OK;
+}
+
+int ts_plan_create(const ts_config* cfg, ts_plan** out) {
+  if (!cfg || !out) return TS_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < 3; ++i)
+    if (!size_supported(cfg->N[i])) {
+      g_last_error = "N must be a power of two in [16, 1024]";
+      return TS_ERR_ARG;
+    }
+  if (cfg->basis != TS_BASIS_FFF && cfg->basis != TS_BASIS_SFF) return TS_ERR_ARG;
+  if (cfg->precision != TS_F64 && cfg->precision != TS_F32) return TS_ERR_ARG;
+  if (cfg->dealias_mode < 0 || cfg->dealias_mode > 2) return TS_ERR_ARG;
+  if (cfg->nlin_form != TS_NLIN_CONSERVATIVE && cfg->nlin_form != TS_NLIN_ROTATIONAL) return TS_ERR_ARG;
+  if (cfg->basis == TS_BASIS_SFF && cfg->nlin_form == TS_NLIN_ROTATIONAL) return TS_ERR_UNSUPPORTED;
+  ts_plan* p = new ts_plan();
+  p->cfg = *cfg;
+  p->cfg.energy_supply = nullptr;
+  p->cfg.helicity_supply = nullptr;
+  Geo& g = p->g;
+  g.Nx = cfg->N[0];
+  g.Ny = cfg->N[1];
+  g.Nz = cfg->N[2];
+  g.Hz = g.Nz / 2 + 1;
+  g.S = (long long)g.Nx * g.Ny * g.Hz;
+  for (int i = 0; i < 3; ++i) g.kf[i] = cfg->kfactor[i];
+  g.basis = cfg->basis;
+  g.dealias = cfg->dealias_mode;
+  p->prec = cfg->precision == TS_F32 ? 1 : 0;
+  p->cb = p->prec ? 8 : 16;
+  int rc = TS_OK;
+#define CKP(x)                     \
+  do {                             \
+    rc = (x);                      \
+    if (rc != TS_OK) {             \
+      ts_plan_destroy(p);          \
+      return rc;                   \
+    }                              \
+  } while (0)
+  auto alloc = [&](void** b, size_t bytes) -> int {
+    CK(cudaMalloc(b, bytes));
+    return TS_OK;
+  };
+  CKP(alloc(&p->Ucur, 3 * g.S * p->cb));
+  CKP(alloc(&p->tot, 3 * g.S * p->cb));
+  CKP(alloc(&p->P, 6 * g.S * p->cb));
+  if (p->prec) {
+    CKP(upload_twiddles<float>(g.Nx, &p->twx));
+    CKP(upload_twiddles<float>(g.Ny, &p->twy));
+    CKP(upload_twiddles<float>(g.Nz, &p->twz));
+  } else {
+    CKP(upload_twiddles<double>(g.Nx, &p->twx));
+    CKP(upload_twiddles<double>(g.Ny, &p->twy));
+    CKP(upload_twiddles<double>(g.Nz, &p->twz));
+  }
+  compute_modes_in_shell(p);
+  CKP(alloc((void**)&p->mis_d, p->mis.size() * sizeof(double)));
+  if (cudaMemcpy(p->mis_d, p->mis.data(), p->mis.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    ts_plan_destroy(p);
+    return TS_ERR_CUDA;
+  }
+  if (cfg->force_type == TS_FORCE_CARATI_ENERGY_SUPPLY) {
+    if (cfg->basis != TS_BASIS_FFF || !cfg->energy_supply || cfg->n_supply <= 0 ||
+        cfg->force_outer_radius <= cfg->force_inner_radius) {
+      ts_plan_destroy(p);
+      return TS_ERR_ARG;
+    }
+    double kfmin = fmin(g.kf[0], fmin(g.kf[1], g.kf[2]));
+    p->fkm = (int)ceil(cfg->force_outer_radius / kfmin);
+    if (p->fkm >= g.Nx / 2 || p->fkm >= g.Ny / 2 || p->fkm > g.Nz / 2) {
+      g_last_error = "forcing band must lie inside the box";
+      ts_plan_destroy(p);
+      return TS_ERR_ARG;
+    }
+    p->nsup = cfg->n_supply;
+    const int n = 2 * p->fkm + 1;
+    CKP(alloc(&p->fcube, 3ull * n * n * (p->fkm + 1) * p->cb));
+    CKP(alloc((void**)&p->esup, p->nsup * sizeof(double)));
+    if (cudaMemcpy(p->esup, cfg->energy_supply, p->nsup * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+      ts_plan_destroy(p);
+      return TS_ERR_CUDA;
+    }
+    if (cfg->helicity_supply) {
+      CKP(alloc((void**)&p->hsup, p->nsup * sizeof(double)));
+      if (cudaMemcpy(p->hsup, cfg->helicity_supply, p->nsup * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        ts_plan_destroy(p);
+        return TS_ERR_CUDA;
+      }
+    }
+  } else if (cfg->force_type != TS_FORCE_NONE && cfg->force_type != TS_FORCE_RBC) {
+    ts_plan_destroy(p);
+    return TS_ERR_ARG;
+  }
+  CKP(ensure_scratch(p, 4096));
+#undef CKP
+  *out = p;
+  return TS_OK;
+}
+
+int ts_plan_set_stream(ts_plan* p, void* stream) {
+  if (!p) return TS_ERR_ARG;
+  p->st = (cudaStream_t)stream;
+  return TS_OK;
+}
+
+int ts_plan_sizes(const ts_plan* p, long long* elems, int* bytes) {
+  if (!p) return TS_ERR_ARG;
+  if (elems) *elems = p->g.S;
+  if (bytes) *bytes = (int)p->cb;
+  return TS_OK;
+}
+
+int ts_plan_num_shells(const ts_plan* p, int* n) {
+  if (!p || !n) return TS_ERR_ARG;
+  *n = p->nshells;
+  return TS_OK;
+}
+
+int ts_plan_set_dt(ts_plan* p, double dt) {
+  if (!p || !(dt > 0)) return TS_ERR_ARG;
+  p->cfg.dt = dt;
+  return TS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// right-hand side pipeline (FFF)
+// ---------------------------------------------------------------------------
+static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a) {
+  const Geo& g = p->g;
+  const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
+  const int nin = rot ? 6 : 3, nout = rot ? 3 : 6;
+  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, nin, p->twy, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, nout, p->twy, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, fwd_x, g, rot, mode, p->P, a, p->twx, p->st)); }
+  return TS_OK;
+}
+
+static int step_fff(ts_plan* p, void* U0) {
+  const Geo& g = p->g;
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.nu = p->cfg.nu;
+  a.dt = p->cfg.dt;
+  a.reality = p->cfg.reality_fix;
+  a.fcube = p->cfg.force_type == TS_FORCE_CARATI_ENERGY_SUPPLY ? p->fcube : nullptr;
+  a.fkm = p->fkm;
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? U0 : p->Ucur;
+    ProfScope ps(p, TS_KCLASS_OTHER);
+    if (a.fcube)
+      CK(LAUNCH(p, carati, g, Uin, p->fcube, p->fkm, p->cfg.force_inner_radius, p->cfg.force_outer_radius, p->esup,
+                p->hsup, p->mis_d, p->nsup, p->st));
+    a.stage = stage;
+    CKS(rhs_fff(p, Uin, MODE_STEP, a));
+  }
+  if (p->cfg.reality_fix) {
+    ProfScope ps(p, TS_KCLASS_OTHER);
+    CK(LAUNCH(p, reality, g, U0, 3, p->st));
+  }
+  return TS_OK;
+}
+
+// run fn(device_ptr) on a field that may live on the host
+template <typename Fn>
+static int with_device(ts_plan* p, void** stage, const void* ptr, size_t bytes, bool copy_back, Fn&& fn) {
+  if (is_device_ptr(ptr)) return fn(const_cast<void*>(ptr));
+  CKS(ensure_stage(stage, bytes));
+  CK(cudaMemcpyAsync(*stage, ptr, bytes, cudaMemcpyHostToDevice, p->st));
+  CKS(fn(*stage));
+  if (copy_back) CK(cudaMemcpyAsync(const_cast<void*>(ptr), *stage, bytes, cudaMemcpyDeviceToHost, p->st));
+  CK(cudaStreamSynchronize(p->st));
+  return TS_OK;
+}
+
+extern "C" {
+
+int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
+  if (!p || !u_hat || nsteps < 0) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
+    for (int s = 0; s < nsteps; ++s) CKS(step_fff(p, U));
+    return (int)TS_OK;
+  });
+}
+
+int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
+  if (!p || !u_hat || !T_hat || nsteps < 0) return TS_ERR_ARG;
+  return TS_ERR_UNSUPPORTED;
+}
+
+int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
+  if (!p || !u_hat || !nlin_hat) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  const size_t bytes = 3 * p->g.S * p->cb;
+  return with_device(p, &p->stage_u, u_hat, bytes, true, [&](void* U) -> int {
+    // the reference dealiases U in place before the transforms (compute_nlin.cc:61-62)
+    if (p->g.dealias) CK(LAUNCH(p, dealias_copy, p->g, U, U, 3, p->st));
+    if (is_device_ptr(nlin_hat)) {
+      StageArgs a;
+      memset(&a, 0, sizeof(a));
+      a.nout = nlin_hat;
+      return rhs_fff(p, U, MODE_NLIN, a);
+    }
+    StageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nout = p->Ucur;
+    CKS(rhs_fff(p, U, MODE_NLIN, a));
+    CK(cudaMemcpyAsync(nlin_hat, p->Ucur, bytes, cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    return (int)TS_OK;
+  });
+}
+
+int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
+  if (!p || !a_hat || !energy || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
+  return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
+    CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
+    CK(LAUNCH(p, energy, p->g, A, A, ncomp, p->dscr, p->st));
+    CK(cudaMemcpyAsync(energy, p->dscr, sizeof(double), cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    return (int)TS_OK;
+  });
+}
+
+int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
+  if (!p || !u_hat || !max_div) return TS_ERR_ARG;
+  return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, false, [&](void* U) -> int {
+    CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
+    CK(LAUNCH(p, maxdiv, p->g, U, (unsigned long long*)p->dscr, p->st));
+    CK(cudaMemcpyAsync(max_div, p->dscr, sizeof(double), cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    return (int)TS_OK;
+  });
+}
+
+int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int n_shells) {
+  if (!p || !a_hat || !Ek || ncomp < 1 || ncomp > 3 || n_shells < 1) return TS_ERR_ARG;
+  const int nsh = p->nshells;
+  return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
+    CKS(ensure_scratch(p, 2 * nsh));
+    CK(cudaMemsetAsync(p->dscr, 0, 2 * nsh * sizeof(double), p->st));
+    CK(LAUNCH(p, shell, p->g, A, ncomp, nsh - 1, p->dscr, p->st));
+    std::vector<double> h(2 * nsh);
+    CK(cudaMemcpyAsync(h.data(), p->dscr, 2 * nsh * sizeof(double), cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    // Stepanov normalisation (universal_energy.cc:350-362), 3D: 4 pi / (count kf1 kf2 kf3)
+    const double kfp = p->g.kf[0] * p->g.kf[1] * p->g.kf[2];
+    for (int i = 0; i < n_shells; ++i) {
+      if (i >= nsh) { Ek[i] = 0; continue; }
+      const double cnt = h[nsh + i];
+      Ek[i] = cnt <= 0 ? 0.0 : h[i] * (4 * M_PI) / (cnt * kfp);
+    }
+    return (int)TS_OK;
+  });
+}
+
+int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, double* Pi) {
+  if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  for (int i = 1; i < n_radii; ++i)
+    if (!(radii[i] >= radii[i - 1])) return TS_ERR_ARG;
+  return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, false, [&](void* U) -> int {
+    CKS(ensure_scratch(p, 2 * (n_radii + 1)));
+    double* bins = p->dscr;
+    double* rad = p->dscr + (n_radii + 1);
+    CK(cudaMemsetAsync(bins, 0, (n_radii + 1) * sizeof(double), p->st));
+    CK(cudaMemcpyAsync(rad, radii, n_radii * sizeof(double), cudaMemcpyHostToDevice, p->st));
+    StageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.Ud = U;
+    a.bins = bins;
+    a.radii = rad;
+    a.nradii = n_radii;
+    CKS(rhs_fff(p, U, MODE_FLUX, a));
+    std::vector<double> h(n_radii + 1);
+    CK(cudaMemcpyAsync(h.data(), bins, (n_radii + 1) * sizeof(double), cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    double acc = 0;
+    for (int i = 0; i < n_radii; ++i) {
+      acc += h[i];
+      Pi[i] = acc;
+    }
+    return (int)TS_OK;
+  });
+}
+
+int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
+  if (!p || !u_hat || !T_hat || !Nu) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
+  if (!is_device_ptr(u_hat) || !is_device_ptr(T_hat)) return TS_ERR_ARG;
+  CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
+  CK(LAUNCH(p, energy, p->g, u_hat, T_hat, 1, p->dscr, p->st));
+  double e = 0;
+  CK(cudaMemcpyAsync(&e, p->dscr, sizeof(double), cudaMemcpyDeviceToHost, p->st));
+  CK(cudaStreamSynchronize(p->st));
+  *Nu = 1.0 + 2.0 * sqrt(p->cfg.Ra * p->cfg.Pr) * e;
+  return TS_OK;
+}
+
+int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed, double target_energy,
+                            void* u_hat) {
+  if (!p || !E_ic || n < 1 || !u_hat) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
+    const int nsh = (int)p->mis.size();
+    CKS(ensure_scratch(p, 2 * nsh + 1));
+    std::vector<double> e(nsh, 0.0);
+    for (int i = 0; i < n && i < nsh; ++i) e[i] = E_ic[i];
+    double* Ed = p->dscr + 1;
+    CK(cudaMemcpyAsync(Ed, e.data(), nsh * sizeof(double), cudaMemcpyHostToDevice, p->st));
+    // key = splitmix64(seed), as the oracle's uniform01
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    const unsigned long long key = z ^ (z >> 31);
+    CK(LAUNCH(p, init_ic, p->g, U, Ed, p->mis_d, nsh, key, p->st));
+    CK(LAUNCH(p, reality, p->g, U, 3, p->st));
+    if (target_energy > 0) {
+      CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
+      CK(LAUNCH(p, energy, p->g, U, U, 3, p->dscr, p->st));
+      double en = 0;
+      CK(cudaMemcpyAsync(&en, p->dscr, sizeof(double), cudaMemcpyDeviceToHost, p->st));
+      CK(cudaStreamSynchronize(p->st));
+      if (!(en > 0)) return (int)TS_ERR_ARG;
+      CK(LAUNCH(p, scale, U, 3 * p->g.S, sqrt(target_energy / en), p->st));
+    }
+    CK(cudaStreamSynchronize(p->st));
+    return (int)TS_OK;
+  });
+}
+
+int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* spec_out, int ncomp) {
+  if (!p || !parity || !real_in || !spec_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  if (strcmp(parity, "FFF") != 0) return TS_ERR_ARG;
+  if (!is_device_ptr(real_in) || !is_device_ptr(spec_out)) return TS_ERR_ARG;
+  const Geo& g = p->g;
+  CK(LAUNCH(p, z_single, g, -1, real_in, spec_out, ncomp, p->twz, p->st));
+  CK(LAUNCH(p, strided, g, 1, -1, spec_out, ncomp, p->twy, p->st));
+  CK(LAUNCH(p, strided, g, 0, -1, spec_out, ncomp, p->twx, p->st));
+  CK(LAUNCH(p, scale, spec_out, ncomp * g.S, 1.0 / ((double)g.Nx * g.Ny * g.Nz), p->st));
+  return TS_OK;
+}
+
+int ts_fft_inverse(ts_plan* p, const char* parity, const void* spec_in, void* real_out, int ncomp) {
+  if (!p || !parity || !spec_in || !real_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  if (strcmp(parity, "FFF") != 0) return TS_ERR_ARG;
+  if (!is_device_ptr(spec_in) || !is_device_ptr(real_out)) return TS_ERR_ARG;
+  const Geo& g = p->g;
+  // the reference copies the input to X_transform first (FFF_pencil_tr.cc:59)
+  CK(cudaMemcpyAsync(p->P, spec_in, ncomp * g.S * p->cb, cudaMemcpyDeviceToDevice, p->st));
+  CK(LAUNCH(p, strided, g, 0, +1, p->P, ncomp, p->twx, p->st));
+  CK(LAUNCH(p, strided, g, 1, +1, p->P, ncomp, p->twy, p->st));
+  CK(LAUNCH(p, z_single, g, +1, p->P, real_out, ncomp, p->twz, p->st));
+  return TS_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int ts_profile_enable(ts_plan* p, int enable) {
+  if (!p) return TS_ERR_ARG;
+  prof_collect(p);
+  p->prof = enable != 0;
+  return TS_OK;
+}
+
+int ts_profile_reset(ts_plan* p) {
+  if (!p) return TS_ERR_ARG;
+  prof_collect(p);
+  for (int i = 0; i < TS_KCLASS_COUNT; ++i) {
+    p->prof_ms[i] = 0;
+    p->prof_n[i] = 0;
+  }
+  return TS_OK;
+}
+
+int ts_profile_read(ts_plan* p, int kclass, double* total_ms, long long* launches, double* bytes_per_launch) {
+  if (!p || kclass < 0 || kclass >= TS_KCLASS_COUNT) return TS_ERR_ARG;
+  prof_collect(p);
+  if (total_ms) *total_ms = p->prof_ms[kclass];
+  if (launches) *launches = p->prof_n[kclass];
+  if (bytes_per_launch) {
+    // algorithmic bytes: every field a launch must read or write, once
+    const double f = (double)p->g.S * (double)p->cb;
+    const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
+    double b = 0;
+    switch (kclass) {
+      case TS_KCLASS_INV_X: b = (3 + (rot ? 6 : 3)) * f; break;          // read U, write W
+      case TS_KCLASS_Y_INV: b = 2.0 * (rot ? 6 : 3) * f; break;          // in place
+      case TS_KCLASS_Z: b = (rot ? 6 + 3 : 3 + 6) * f; break;            // read W, write P
+      case TS_KCLASS_Y_FWD: b = 2.0 * (rot ? 3 : 6) * f; break;
+      case TS_KCLASS_FWD_X: b = ((rot ? 3 : 6) + 13.5) * f; break;       // P + stage-averaged state traffic
+      default: b = 0; break;
+    }
+    *bytes_per_launch = b;
+  }
+  return TS_OK;
+}
+
+}  // extern "C"

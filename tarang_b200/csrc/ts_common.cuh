@@ -1,0 +1,220 @@
+// Shared device building blocks for the B200 pseudo-spectral path:
+// complex arithmetic, register-resident radix-2/4/8/16 DFTs, a Stockham FFT
+// whose passes exchange through shared memory, and the spectral index maps of
+// the FFF / SFF bases (Get_kx / Get_ky / Get_kz of
+// basis/FFF/pencil/FFF_pencil_inline.h:63-111 and SFF_pencil_inline.h:63-109).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <type_traits>
+
+namespace ts {
+
+template <typename T> struct cplx_of;
+template <> struct cplx_of<float> { typedef float2 type; };
+template <> struct cplx_of<double> { typedef double2 type; };
+template <typename T> using C = typename cplx_of<T>::type;
+
+template <typename V> __device__ __forceinline__ V mk(decltype(V::x) a, decltype(V::x) b) { V r; r.x = a; r.y = b; return r; }
+template <typename V> __device__ __forceinline__ V add(V a, V b) { return mk<V>(a.x + b.x, a.y + b.y); }
+template <typename V> __device__ __forceinline__ V sub(V a, V b) { return mk<V>(a.x - b.x, a.y - b.y); }
+template <typename V> __device__ __forceinline__ V mul(V a, V b) { return mk<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename V> __device__ __forceinline__ V conjg(V a) { return mk<V>(a.x, -a.y); }
+template <typename V, typename S> __device__ __forceinline__ V scale(V a, S s) { return mk<V>(a.x * s, a.y * s); }
+// multiply by +i (SIGN=+1) or -i (SIGN=-1)
+template <int SIGN, typename V> __device__ __forceinline__ V mul_i(V a) {
+  return SIGN > 0 ? mk<V>(-a.y, a.x) : mk<V>(a.y, -a.x);
+}
+// i * K * a for real K
+template <typename V, typename S> __device__ __forceinline__ V ik(S K, V a) { return mk<V>(-K * a.y, K * a.x); }
+
+// cos / sin of pi*k/8, k = 0..8 (exact mathematical constants)
+__device__ __forceinline__ double c16(int k) {
+  const double t[9] = {1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173, 0.0,
+                       -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613, -1.0};
+  return t[k];
+}
+__device__ __forceinline__ double s16(int k) {
+  const double t[9] = {0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613, 1.0,
+                       0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173, 0.0};
+  return t[k];
+}
+
+// In-register DFT of size R (2,4,8,16), natural order in and out.
+// DIR = -1: forward (e^{-2 pi i jk/R}), +1: inverse (unnormalised).
+template <int R, int DIR, typename V> struct DFT;
+template <int DIR, typename V> struct DFT<1, DIR, V> {
+  static __device__ __forceinline__ void run(V*) {}
+};
+template <int DIR, typename V> struct DFT<2, DIR, V> {
+  static __device__ __forceinline__ void run(V* v) {
+    V a = v[0];
+    v[0] = add(a, v[1]);
+    v[1] = sub(a, v[1]);
+  }
+};
+template <int R, int DIR, typename V> struct DFT {
+  // radix-2 decimation in time: X[k] = E[k] + w^k O[k], X[k+R/2] = E[k] - w^k O[k]
+  static __device__ __forceinline__ void run(V* v) {
+    typedef decltype(V::x) S;
+    V e[R / 2], o[R / 2];
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) { e[k] = v[2 * k]; o[k] = v[2 * k + 1]; }
+    DFT<R / 2, DIR, V>::run(e);
+    DFT<R / 2, DIR, V>::run(o);
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) {
+      V t;
+      const int q = k * (16 / R);  // angle pi*q/8 = 2 pi k / R
+      if (k == 0) t = o[k];
+      else if (4 * k == R) t = mul_i<DIR>(o[k]);
+      else t = mul(o[k], mk<V>((S)c16(q), (S)(DIR * s16(q))));
+      v[k] = add(e[k], t);
+      v[k + R / 2] = sub(e[k], t);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Stockham radix schedule for length L with at most E elements per thread.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int radix_at(int L, int E, int p) {
+  // radix of pass p: min(E, remaining length)
+  return p == 0 ? (L < E ? L : E) : radix_at(L / (L < E ? L : E), E, p - 1);
+}
+__host__ __device__ constexpr int npasses(int L, int E) { return L <= 1 ? 0 : 1 + npasses(L / (L < E ? L : E), E); }
+__host__ __device__ constexpr int ns_at(int L, int E, int p) {
+  // product of the radices before pass p
+  return p == 0 ? 1 : radix_at(L, E, p - 1) * ns_at(L, E, p - 1);
+}
+
+// Element held in register slot s after pass p: butterfly q = s / R, input/output r = s % R.
+// Thread t of a line owns butterflies j = t*(E/R) + q.
+// Input row  of slot (q,r) for pass p: j + r*(L/R).
+// Output row of slot (q,r) for pass p: (j/Ns)*Ns*R + (j%Ns) + r*Ns.
+template <int L, int E, int P> struct Pass {
+  static constexpr int R = radix_at(L, E, P);
+  static constexpr int NS = ns_at(L, E, P);
+  static constexpr int B = E / R;  // butterflies per thread
+  static __device__ __forceinline__ int in_row(int t, int s) {
+    const int j = t * B + s / R;
+    return j + (s % R) * (L / R);
+  }
+  static __device__ __forceinline__ int out_row(int t, int s) {
+    const int j = t * B + s / R;
+    return (j / NS) * NS * R + (j % NS) + (s % R) * NS;
+  }
+};
+
+// Row of register slot s at load time (first pass input) and after the last pass.
+template <int L, int E> __device__ __forceinline__ int load_row(int t, int s) { return Pass<L, E, 0>::in_row(t, s); }
+template <int L, int E> __device__ __forceinline__ int final_row(int t, int s) {
+  return Pass<L, E, npasses(L, E) - 1>::out_row(t, s);
+}
+
+// Butterflies of pass P on the registers (twiddle then DFT_R).  tw: table of
+// Ltab entries exp(-2 pi i m / Ltab), Ltab = L * tws (tws = table stride).
+template <int L, int E, int P, int DIR, typename V>
+__device__ __forceinline__ void pass_compute(V* v, int t, const V* __restrict__ tw, int tws) {
+  typedef Pass<L, E, P> PP;
+  constexpr int R = PP::R, NS = PP::NS;
+#pragma unroll
+  for (int q = 0; q < PP::B; ++q) {
+    V* b = v + q * R;
+    if (NS > 1) {
+      const int j = t * PP::B + q;
+      const int k = j % NS;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        V w = tw[(r * k * (L / (NS * R))) * tws];
+        if (DIR > 0) w.y = -w.y;
+        b[r] = mul(b[r], w);
+      }
+    }
+    DFT<R, DIR, V>::run(b);
+  }
+}
+
+// Full FFT of one line whose E-element slice per thread is in registers (loaded
+// in load_row order); the line's L elements are exchanged through shared memory
+// `sm` addressed as sm[row*rs + cs] (caller supplies the per-thread column
+// offset cs and the row stride rs).  All threads of the block must call it.
+// On return v[s] holds output row final_row(t, s).
+template <int L, int E, int DIR, int P = 0, typename V>
+__device__ __forceinline__ void fft_regs(V* v, int t, V* sm, int rs, int cs, const V* __restrict__ tw, int tws) {
+  pass_compute<L, E, P, DIR>(v, t, tw, tws);
+  if constexpr (P + 1 < npasses(L, E)) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) sm[Pass<L, E, P>::out_row(t, s) * rs + cs] = v[s];
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < E; ++s) v[s] = sm[Pass<L, E, P + 1>::in_row(t, s) * rs + cs];
+    __syncthreads();
+    fft_regs<L, E, DIR, P + 1>(v, t, sm, rs, cs, tw, tws);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory line FFTs with all threads of the block cooperating
+// (used by the contiguous-axis kernels, where lines are short and the real
+// transform pre/post-processing needs element pairs k, M-k).
+// Stockham ping-pong: reads src, writes dst, swaps; returns the buffer that
+// holds the result.  Lines are at src + l*ld.
+// ---------------------------------------------------------------------------
+template <int L, int E, int DIR, int P = 0, typename V>
+__device__ V* fft_smem_lines(V* src, V* dst, int nlines, int ld, const V* __restrict__ tw, int tws) {
+  typedef Pass<L, E, P> PP;
+  constexpr int R = PP::R, NS = PP::NS;
+  const int nb = nlines * (L / R);
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    const int line = b / (L / R);
+    const int j = b % (L / R);
+    const int k = j % NS;
+    V v[R];
+    const V* s = src + line * ld;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = s[j + r * (L / R)];
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        V w = tw[(r * k * (L / (NS * R))) * tws];
+        if (DIR > 0) w.y = -w.y;
+        v[r] = mul(v[r], w);
+      }
+    }
+    DFT<R, DIR, V>::run(v);
+    V* d = dst + line * ld;
+    const int o = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) d[o + r * NS] = v[r];
+  }
+  __syncthreads();
+  if constexpr (P + 1 < npasses(L, E)) return fft_smem_lines<L, E, DIR, P + 1>(dst, src, nlines, ld, tw, tws);
+  else return dst;
+}
+
+// ---------------------------------------------------------------------------
+// Index maps
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int kfft(int l, int N) { return l <= N / 2 ? l : l - N; }
+
+// Dealias predicates: true when the mode is ZEROED.
+// mode 1 = reference corner box (FFF_pencil_basic.cc:87-90 / SFF_pencil_basic.cc:94-97),
+// mode 2 = two-thirds cube.
+__device__ __forceinline__ bool dealias_zero(int mode, int basis, int lx, int ly, int lz, int Nx, int Ny, int Nz) {
+  if (mode == 1) {
+    bool mx = basis == 0 ? (lx >= Nx / 3 + 1 && lx <= 2 * Nx / 3 - 1) : (lx >= 2 * Nx / 3 + 1);
+    bool my = ly >= Ny / 3 + 1 && ly <= 2 * Ny / 3 - 1;
+    bool mz = lz >= Nz / 3 + 1 && lz <= Nz / 2;
+    return mx && my && mz;
+  }
+  if (mode == 2) {
+    int kx = basis == 0 ? kfft(lx, Nx) : lx;
+    int ky = kfft(ly, Ny);
+    bool bx = basis == 0 ? (3 * abs(kx) > Nx) : (3 * kx > 2 * Nx);
+    return bx || (3 * abs(ky) > Ny) || (3 * lz > Nz);
+  }
+  return false;
+}
+
+}  // namespace ts

@@ -1,0 +1,255 @@
+// Launcher definitions, included once per precision by ts_kern_f32.cu and
+// ts_kern_f64.cu with TS_REAL defined to float / double.
+#include <type_traits>
+#include "ts_launch.h"
+#include "ts_misc.cuh"
+
+namespace ts {
+
+namespace {
+
+typedef TS_REAL T;
+typedef C<T> V;
+
+// elements per thread of the register FFTs; columns per block (rows of 128 B)
+constexpr int E_REG = std::is_same<T, float>::value ? 16 : 8;
+// at L = 1024 the 16-element register FFT would spill under the 512-thread cap
+constexpr int e_reg(int L) { return (L >= 1024 ? 8 : E_REG) < L ? (L >= 1024 ? 8 : E_REG) : L; }
+constexpr int E_ACC = 8;  // forward-x kernel keeps 3 accumulators per element
+constexpr int CWMAX = std::is_same<T, float>::value ? 16 : 8;
+constexpr int emin(int a, int b) { return a < b ? a : b; }
+constexpr int cw_for(int L, int E) {
+  return emin(CWMAX, (512 * E / L) > 0 ? (512 * E / L) : 1);
+}
+
+template <typename Fn> bool dispatch_L(int L, Fn&& fn) {
+  switch (L) {
+    case 16: fn(std::integral_constant<int, 16>{}); return true;
+    case 32: fn(std::integral_constant<int, 32>{}); return true;
+    case 64: fn(std::integral_constant<int, 64>{}); return true;
+    case 128: fn(std::integral_constant<int, 128>{}); return true;
+    case 256: fn(std::integral_constant<int, 256>{}); return true;
+    case 512: fn(std::integral_constant<int, 512>{}); return true;
+    case 1024: fn(std::integral_constant<int, 1024>{}); return true;
+  }
+  return false;
+}
+
+template <typename K> cudaError_t smem_attr(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return cudaSuccess;
+}
+
+inline unsigned grid1d(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+// lines per block of the z kernels: about 96 KB of shared memory (two blocks per SM)
+inline int z_lines(int nbuf, int H) {
+  const long long per = 2LL * nbuf * H * (long long)sizeof(V);
+  long long nl = (96 * 1024) / per;
+  if (nl < 1) nl = 1;
+  if (nl > 16) nl = 16;
+  return (int)nl;
+}
+
+}  // namespace
+
+template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw,
+                                           cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  const int L = axis == 0 ? g.Nx : g.Ny;
+  dispatch_L(L, [&](auto Lc) {
+    constexpr int LL = decltype(Lc)::value;
+    constexpr int E = e_reg(LL);
+    constexpr int CW = cw_for(LL, E);
+    const int inner = axis == 0 ? g.Ny * g.Hz : g.Hz;
+    const long long rstride = axis == 0 ? (long long)g.Ny * g.Hz : g.Hz;
+    const long long ostride = axis == 0 ? 0 : (long long)g.Ny * g.Hz;
+    dim3 grid((inner + CW - 1) / CW, axis == 0 ? 1 : g.Nx);
+    const size_t sm = (size_t)LL * CW * sizeof(V);
+    if (dir < 0) {
+      auto k = k_strided_fft<T, LL, E, CW, -1>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, (const V*)tw);
+    } else {
+      auto k = k_strided_fft<T, LL, E, CW, 1>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, (const V*)tw);
+    }
+    ++g_launches;
+    err = cudaGetLastError();
+  });
+  return err;
+}
+
+template <> cudaError_t Launch<T>::inv_x(const Geo& g, int rot, const void* U, void* W, const void* tw,
+                                         cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L(g.Nx, [&](auto Lc) {
+    constexpr int LL = decltype(Lc)::value;
+    constexpr int E = e_reg(LL);
+    constexpr int CW = cw_for(LL, E);
+    const int inner = g.Ny * g.Hz;
+    const size_t sm = (size_t)LL * CW * sizeof(V);
+    dim3 grid((inner + CW - 1) / CW);
+    if (rot) {
+      auto k = k_inv_x<T, LL, E, CW, true>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw);
+    } else {
+      auto k = k_inv_x<T, LL, E, CW, false>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw);
+    }
+    ++g_launches;
+    err = cudaGetLastError();
+  });
+  return err;
+}
+
+template <> cudaError_t Launch<T>::z_fused(const Geo& g, int rot, void* P, const void* tw, cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L(g.Nz, [&](auto Lc) {
+    constexpr int NZ = decltype(Lc)::value;
+    constexpr int M = NZ / 2, H = M + 1;
+    constexpr int E = emin(E_REG, M);
+    const int nl = z_lines(6, H);
+    const size_t sm = 2ull * 6 * nl * H * sizeof(V);
+    const long long nlines = (long long)g.Nx * g.Ny;
+    dim3 grid((unsigned)((nlines + nl - 1) / nl));
+    if (rot) {
+      auto k = k_z_fused<T, NZ, E, 1>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, 256, sm, st>>>((V*)P, g, (const V*)tw, nl);
+    } else {
+      auto k = k_z_fused<T, NZ, E, 0>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, 256, sm, st>>>((V*)P, g, (const V*)tw, nl);
+    }
+    ++g_launches;
+    err = cudaGetLastError();
+  });
+  return err;
+}
+
+template <> cudaError_t Launch<T>::z_single(const Geo& g, int dir, const void* in, void* out, int ncomp,
+                                            const void* tw, cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L(g.Nz, [&](auto Lc) {
+    constexpr int NZ = decltype(Lc)::value;
+    constexpr int M = NZ / 2, H = M + 1;
+    constexpr int E = emin(E_REG, M);
+    const int nl = z_lines(1, H);
+    const size_t sm = 2ull * nl * H * sizeof(V);
+    const long long nlines = (long long)g.Nx * g.Ny;
+    dim3 grid((unsigned)((nlines + nl - 1) / nl), ncomp);
+    if (dir < 0) {
+      auto k = k_z_single<T, NZ, E, -1>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, 256, sm, st>>>((const V*)in, (V*)out, g, (const V*)tw, nl, ncomp);
+    } else {
+      auto k = k_z_single<T, NZ, E, 1>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<grid, 256, sm, st>>>((const V*)in, (V*)out, g, (const V*)tw, nl, ncomp);
+    }
+    ++g_launches;
+    err = cudaGetLastError();
+  });
+  return err;
+}
+
+template <int FORM, int MODE, int LL>
+static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st) {
+  constexpr int E = emin(E_ACC, LL);
+  constexpr int CW = cw_for(LL, E);
+  const int inner = g.Ny * g.Hz;
+  size_t sm = (size_t)LL * CW * sizeof(V);
+  if (MODE == MODE_FLUX) sm += (size_t)(a.nradii + 1) * sizeof(double);
+  auto k = k_fwd_x<T, LL, E, CW, FORM, MODE>;
+  cudaError_t err = smem_attr(k, sm);
+  if (err != cudaSuccess) return err;
+  k<<<(inner + CW - 1) / CW, CW * (LL / E), sm, st>>>((const V*)P, g, a, (const V*)tw);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int rot, int mode, const void* P, const StageArgs& a,
+                                         const void* tw, cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L(g.Nx, [&](auto Lc) {
+    constexpr int LL = decltype(Lc)::value;
+    if (rot) {
+      if (mode == MODE_STEP) err = fwd_x_impl<1, MODE_STEP, LL>(g, P, a, tw, st);
+      else if (mode == MODE_FLUX) err = fwd_x_impl<1, MODE_FLUX, LL>(g, P, a, tw, st);
+      else err = fwd_x_impl<1, MODE_NLIN, LL>(g, P, a, tw, st);
+    } else {
+      if (mode == MODE_STEP) err = fwd_x_impl<0, MODE_STEP, LL>(g, P, a, tw, st);
+      else if (mode == MODE_FLUX) err = fwd_x_impl<0, MODE_FLUX, LL>(g, P, a, tw, st);
+      else err = fwd_x_impl<0, MODE_NLIN, LL>(g, P, a, tw, st);
+    }
+  });
+  return err;
+}
+
+template <> cudaError_t Launch<T>::reality(const Geo& g, void* A, int ncomp, cudaStream_t st) {
+  const long long n = (long long)g.Nx * g.Ny * ncomp;
+  k_reality<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((V*)A, ncomp, g);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout,
+                                          const double* es, const double* hs, const double* mis, int nsup,
+                                          cudaStream_t st) {
+  k_carati<T><<<1, 256, 0, st>>>((const V*)U, (V*)fc, g, km, rin, rout, es, hs, mis, nsup);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::energy(const Geo& g, const void* A, const void* B, int ncomp, double* out,
+                                          cudaStream_t st) {
+  k_energy<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)A, (const V*)B, ncomp, g, out);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::maxdiv(const Geo& g, const void* U, unsigned long long* out, cudaStream_t st) {
+  k_maxdiv<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)U, g, out);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins,
+                                         cudaStream_t st) {
+  const size_t sm = 2ull * (kmax + 1) * sizeof(double);
+  cudaError_t err = smem_attr(k_shell<T>, sm);
+  if (err != cudaSuccess) return err;
+  k_shell<T><<<grid1d(g.S, 256), 256, sm, st>>>((const V*)A, ncomp, g, kmax, bins);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
+                                           unsigned long long key, cudaStream_t st) {
+  k_init_ic<T><<<grid1d(g.S, 256), 256, 0, st>>>((V*)U, g, Eic, mis, nsh, key);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::scale(void* A, long long n, double s, cudaStream_t st) {
+  k_scale<T><<<grid1d(n, 256), 256, 0, st>>>((V*)A, n, s);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st) {
+  k_dealias_copy<T><<<grid1d(g.S * ncomp, 256), 256, 0, st>>>((const V*)A, (V*)B, ncomp, g);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+}  // namespace ts

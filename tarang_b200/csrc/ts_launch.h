@@ -1,0 +1,34 @@
+// Host-side launchers of the templated kernels, instantiated per precision in
+// ts_kern_f32.cu / ts_kern_f64.cu (compiled in parallel).
+#pragma once
+#include <cuda_runtime.h>
+#include "ts_fff.cuh"
+
+namespace ts {
+
+extern long long g_launches;  // kernels launched by this library
+
+template <typename T> struct Launch {
+  // strided-axis FFT on nf fields in place: axis 0 = x (L = Nx), 1 = y (L = Ny);
+  // dir -1 forward, +1 inverse; outputs scaled by `scale`
+  static cudaError_t strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw, cudaStream_t st);
+  static cudaError_t inv_x(const Geo& g, int rot, const void* U, void* W, const void* tw, cudaStream_t st);
+  static cudaError_t z_fused(const Geo& g, int rot, void* P, const void* tw, cudaStream_t st);
+  static cudaError_t z_single(const Geo& g, int dir, const void* in, void* out, int ncomp, const void* tw, cudaStream_t st);
+  static cudaError_t fwd_x(const Geo& g, int rot, int mode, const void* P, const StageArgs& a, const void* tw,
+                           cudaStream_t st);
+  static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
+  static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,
+                            const double* hs, const double* mis, int nsup, cudaStream_t st);
+  static cudaError_t energy(const Geo& g, const void* A, const void* B, int ncomp, double* out, cudaStream_t st);
+  static cudaError_t maxdiv(const Geo& g, const void* U, unsigned long long* out, cudaStream_t st);
+  static cudaError_t shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins, cudaStream_t st);
+  static cudaError_t init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
+                             unsigned long long key, cudaStream_t st);
+  static cudaError_t scale(void* A, long long n, double s, cudaStream_t st);
+  static cudaError_t dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
+};
+
+bool size_supported(int n);
+
+}  // namespace ts

@@ -1,0 +1,328 @@
+// Plane-sized and reduction kernels: strong reality condition, Carati force on
+// the forcing band, total energy, max |div|, shell spectrum E(k), and the
+// random-phase helical initial condition.
+#pragma once
+#include "ts_fff.cuh"
+
+namespace ts {
+
+// ---------------------------------------------------------------------------
+// Satisfy_strong_reality_condition_in_Array (FFF_pencil_basic.cc:139-179,
+// SFF_pencil_basic.cc:143-167) on ncomp consecutive components.
+// Targets and sources of the kz=0 copy are disjoint, so the copy runs in place.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_reality(C<T>* A, int ncomp, Geo g) {
+  typedef C<T> V;
+  const long long plane = (long long)g.Nx * g.Ny;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= plane * ncomp) return;
+  const int comp = (int)(e / plane);
+  const int lx = (int)((e % plane) / g.Ny), ly = (int)(e % g.Ny);
+  V* a = A + comp * g.S;
+  const int ky = kfft(ly, g.Ny);
+  const int iym = ((-ky) % g.Ny + g.Ny) % g.Ny;
+  const long long Hz = g.Hz;
+  if (g.basis == 0) {
+    if (lx > g.Nx / 2 && ky != g.Ny / 2) {
+      const int mkx = -kfft(lx, g.Nx);
+      a[((long long)lx * g.Ny + ly) * Hz] = conjg(a[((long long)mkx * g.Ny + iym) * Hz]);
+    } else if (lx == 0 && ky < 0) {
+      a[(long long)ly * Hz] = conjg(a[(long long)iym * Hz]);
+    }
+  } else {
+    if (ky < 0) a[((long long)lx * g.Ny + ly) * Hz] = conjg(a[((long long)lx * g.Ny + iym) * Hz]);
+    else if (ky == 0) { V v = a[((long long)lx * g.Ny) * Hz]; v.y = -v.y; a[((long long)lx * g.Ny) * Hz] = v; }
+  }
+  a[((long long)lx * g.Ny + ly) * Hz + g.Nz / 2] = mk<V>(0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Carati constant-energy-supply force (non-global alpha/beta) on the cube
+// |kx|,|ky|,kz <= km; compute_force_Carati.cc:158-205, force_alpha_beta.cc:56-85,
+// then the strong reality condition on the force (compute_force_main.cc:67-73).
+// One block.  fc: 3 comps of (2km+1)(2km+1)(km+1).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_carati(const C<T>* __restrict__ U, C<T>* fc, Geo g, int km, double r_in, double r_out,
+                         const double* __restrict__ esup, const double* __restrict__ hsup,
+                         const double* __restrict__ mis, int nsup) {
+  typedef C<T> V;
+  const int n = 2 * km + 1;
+  const int ncube = n * n * (km + 1);
+  for (int e = threadIdx.x; e < ncube; e += blockDim.x) {
+    const int kx = e / (n * (km + 1)) - km;
+    const int ky = (e / (km + 1)) % n - km;
+    const int kz = e % (km + 1);
+    V F[3] = {mk<V>(0, 0), mk<V>(0, 0), mk<V>(0, 0)};
+    const double Kx = kx * g.kf[0], Ky = ky * g.kf[1], Kz = kz * g.kf[2];
+    const double K = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz);
+    const bool inbox = abs(kx) <= g.Nx / 2 && abs(ky) <= g.Ny / 2 && kz <= g.Nz / 2 &&
+                       !(kx == -g.Nx / 2) && !(ky == -g.Ny / 2);
+    if (inbox && K > r_in && K <= r_out) {
+      const int index = (int)ceil(K);
+      const int lx = kx >= 0 ? kx : kx + g.Nx, ly = ky >= 0 ? ky : ky + g.Ny;
+      const long long off = ((long long)lx * g.Ny + ly) * g.Hz + kz;
+      double vr[3], vi[3];
+      for (int i = 0; i < 3; ++i) { V u = U[i * g.S + off]; vr[i] = u.x; vi[i] = u.y; }
+      const double me = (vr[0] * vr[0] + vi[0] * vi[0] + vr[1] * vr[1] + vi[1] * vi[1] + vr[2] * vr[2] + vi[2] * vi[2]) / 2;
+      if (me > 1e-15 && index < nsup && mis[index] > 0) {
+        const double ek = esup[index] / mis[index];
+        const double hk = hsup ? hsup[index] / mis[index] : 0.0;
+        // K . (Vr x Vi)
+        const double cx = vr[1] * vi[2] - vr[2] * vi[1], cy = vr[2] * vi[0] - vr[0] * vi[2], cz = vr[0] * vi[1] - vr[1] * vi[0];
+        const double mh = Kx * cx + Ky * cy + Kz * cz;
+        const double denr = 2.0 * ((K * me) * (K * me) - mh * mh);
+        double alpha = 0, beta = 0;
+        if (fabs(denr) > 1e-15) {
+          alpha = (K * K * ek * me - hk * mh) / denr;
+          beta = (hk * me - ek * mh) / denr;
+        } else {
+          alpha = ek / (4 * me);
+          beta = alpha / K;
+        }
+        // omega = i K x V
+        const double Kv[3] = {Kx, Ky, Kz};
+        for (int i = 0; i < 3; ++i) {
+          const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+          // (K x V)_i = K_i1 V_i2 - K_i2 V_i1 ; omega = i (K x V)
+          const double crr = Kv[i1] * vr[i2] - Kv[i2] * vr[i1];
+          const double cri = Kv[i1] * vi[i2] - Kv[i2] * vi[i1];
+          const double wr = -cri, wi = crr;
+          F[i] = mk<V>((T)(alpha * vr[i] + beta * wr), (T)(alpha * vi[i] + beta * wi));
+        }
+      }
+    }
+    for (int i = 0; i < 3; ++i) fc[i * ncube + e] = F[i];
+  }
+  __syncthreads();
+  // reality on the kz = 0 plane of the cube: F(kx<0,ky,0) = conj(F(-kx,-ky,0)) for ky != Ny/2,
+  // F(0,ky<0,0) = conj(F(0,-ky,0)); kz = Nz/2 never lies in the cube unless km >= Nz/2.
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int kx = e / n - km, ky = e % n - km;
+    bool tgt = (kx < 0 && ky != g.Ny / 2) || (kx == 0 && ky < 0);
+    if (!tgt) continue;
+    const int src = ((-kx + km) * n + (-ky + km)) * (km + 1);
+    const int dst = ((kx + km) * n + (ky + km)) * (km + 1);
+    for (int i = 0; i < 3; ++i) fc[i * ncube + dst] = conjg(fc[i * ncube + src]);
+  }
+  if (km >= g.Nz / 2) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x)
+      for (int i = 0; i < 3; ++i) fc[i * ncube + e * (km + 1) + g.Nz / 2] = mk<V>(0, 0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// reductions (FP64 accumulation)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x + 31) / 32) ? red[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_sum(v);
+  return v;
+}
+
+// plane weights of the total energy: FFF 1/2 on kz=0 (FFF_pencil_energy.cc:59-68);
+// SFF 2, minus 1 on kz=0, minus 1 on m=0, plus 1/2 on (m=0,kz=0) (SFF_pencil_energy.cc:76-95)
+__device__ __forceinline__ double energy_weight(int basis, int lx, int lz) {
+  if (basis == 0) return lz == 0 ? 0.5 : 1.0;
+  double w = 2.0;
+  if (lz == 0) w -= 1.0;
+  if (lx == 0) w -= 1.0;
+  if (lx == 0 && lz == 0) w += 0.5;
+  return w;
+}
+
+// out[0] += sum_w Re(A.conj(B)) over ncomp components (A == B gives the energy)
+template <typename T>
+__global__ void k_energy(const C<T>* __restrict__ A, const C<T>* __restrict__ B, int ncomp, Geo g, double* out) {
+  const long long n = g.S;
+  double s = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    double d = 0;
+    for (int i = 0; i < ncomp; ++i) {
+      const C<T> a = A[i * n + e], b = B[i * n + e];
+      d += (double)a.x * b.x + (double)a.y * b.y;
+    }
+    s += energy_weight(g.basis, lx, lz) * d;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+// max over modes of |div U| (FFF: i K.U; SFF: Kx U1 (sine parity) + i Ky U2 + i Kz U3)
+template <typename T>
+__global__ void k_maxdiv(const C<T>* __restrict__ U, Geo g, unsigned long long* out) {
+  const long long n = g.S;
+  double m = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    const double Kx = (g.basis == 0 ? kfft(lx, g.Nx) : lx) * g.kf[0];
+    const double Ky = kfft(ly, g.Ny) * g.kf[1], Kz = lz * g.kf[2];
+    const C<T> u1 = U[e], u2 = U[n + e], u3 = U[2 * n + e];
+    double dr, di;
+    if (g.basis == 0) {
+      dr = -(Kx * u1.y + Ky * u2.y + Kz * u3.y);
+      di = Kx * u1.x + Ky * u2.x + Kz * u3.x;
+    } else {
+      dr = Kx * u1.x - (Ky * u2.y + Kz * u3.y);
+      di = Kx * u1.y + (Ky * u2.x + Kz * u3.x);
+    }
+    m = fmax(m, sqrt(dr * dr + di * di));
+  }
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// multiplicity factor (FFF_pencil_inline.h:583-602, SFF_pencil_inline.h:492-515)
+__device__ __forceinline__ double multiplicity(int basis, int lx, int ly, int lz, int Nx, int Ny) {
+  const int ky = kfft(ly, Ny);
+  double f;
+  if (basis == 0) {
+    f = lz > 0 ? 1.0 : 0.5;
+    if (kfft(lx, Nx) == Nx / 2 || (ky == Ny / 2 && Ny > 1)) f *= 2;
+  } else {
+    if (lz > 0) f = lx > 0 ? 2.0 : 1.0;
+    else f = lx > 0 ? 1.0 : 0.5;
+    if (ky == Ny / 2 && Ny > 1) f *= 2;
+  }
+  return f;
+}
+
+// Shell spectrum accumulation (Compute_local_shell_spectrum universal_energy.cc:279-313):
+// bins[s] += mult |K|^2 sum_i |A_i|^2 ; bins[nsh + s] += 2 mult, s = ceil|K| <= kmax.
+// Block-private shared bins, then one global atomic per bin.
+template <typename T>
+__global__ void k_shell(const C<T>* __restrict__ A, int ncomp, Geo g, int kmax, double* bins) {
+  extern __shared__ double sb[];
+  const int nsh = kmax + 1;
+  for (int i = threadIdx.x; i < 2 * nsh; i += blockDim.x) sb[i] = 0;
+  __syncthreads();
+  const long long n = g.S;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    const double Kx = (g.basis == 0 ? kfft(lx, g.Nx) : lx) * g.kf[0];
+    const double Ky = kfft(ly, g.Ny) * g.kf[1], Kz = lz * g.kf[2];
+    const double K2 = (Kx * Kx + Ky * Ky) + Kz * Kz;
+    const double Kmag = sqrt(K2);
+    const int idx = (int)ceil(Kmag);
+    if (idx > kmax) continue;
+    const double f = multiplicity(g.basis, lx, ly, lz, g.Nx, g.Ny);
+    double a2 = 0;
+    for (int i = 0; i < ncomp; ++i) {
+      const C<T> a = A[i * n + e];
+      a2 += (double)a.x * a.x + (double)a.y * a.y;
+    }
+    atomicAdd(&sb[idx], f * a2 * (Kmag * Kmag));
+    atomicAdd(&sb[nsh + idx], 2 * f);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 2 * nsh; i += blockDim.x)
+    if (sb[i] != 0) atomicAdd(&bins[i], sb[i]);
+}
+
+// ---------------------------------------------------------------------------
+// random-phase helical initial condition (init_cond_energy.cc:67-120 construction;
+// this project's counter-based splitmix64 phases, identical to the oracle)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ double uniform01(unsigned long long key, unsigned long long ctr) {
+  return (double)(splitmix64(key ^ ctr) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename T>
+__global__ void k_init_ic(C<T>* U, Geo g, const double* __restrict__ Eic, const double* __restrict__ mis, int nsh,
+                          unsigned long long key) {
+  typedef C<T> V;
+  const long long n = g.S;
+  const double PI = 3.14159265358979323846;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    const double Kx = kfft(lx, g.Nx) * g.kf[0], Ky = kfft(ly, g.Ny) * g.kf[1], Kz = lz * g.kf[2];
+    const double Kmag = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz);
+    double r[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    const int idx = (int)ceil(Kmag);
+    if (Kmag > 1e-15 && idx < nsh && mis[idx] > 0) {
+      const double ek = Eic[idx] / mis[idx];
+      if (ek >= 1e-15) {
+        const double a = sqrt(ek / 2.0);
+        const double php = 2 * PI * uniform01(key, 2ull * (unsigned long long)e);
+        const double phm = 2 * PI * uniform01(key, 2ull * (unsigned long long)e + 1);
+        const double upr = a * cos(php), upi = a * sin(php), umr = a * cos(phm), umi = a * sin(phm);
+        // U1 = i (u- - u+), U2 = u- + u+
+        const double U1r = -(umi - upi), U1i = umr - upr, U2r = umr + upr, U2i = umi + upi;
+        // polar angle of K with z (Get_polar_angle), azimuth from (Kx, Ky)
+        const double kperp = sqrt(Kx * Kx + Ky * Ky);
+        double th;
+        if (fabs(kperp) > 1e-15) th = fabs(Kz) > 1e-15 ? atan(kperp / Kz) : PI / 2;
+        else th = Kz >= 0 ? 0.0 : PI;
+        if (th < 0) th += PI;
+        double ph = 0;
+        if (fabs(kperp) > 1e-15) {
+          double c = Kx / kperp;
+          c = c > 1 ? 1 : (c < -1 ? -1 : c);
+          ph = acos(c);
+          if (Ky < 0) ph = 2 * PI - ph;
+        }
+        const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+        // vpll = -U2 sin th; vh1 = U1 sin ph + U2 cos th cos ph; vh2 = -U1 cos ph + U2 sin ph cos th
+        r[2][0] = -U2r * st; r[2][1] = -U2i * st;
+        r[0][0] = U1r * sp + U2r * ct * cp; r[0][1] = U1i * sp + U2i * ct * cp;
+        r[1][0] = -U1r * cp + U2r * sp * ct; r[1][1] = -U1i * cp + U2i * sp * ct;
+      }
+    }
+    for (int i = 0; i < 3; ++i) U[i * n + e] = mk<V>((T)r[i][0], (T)r[i][1]);
+  }
+}
+
+template <typename T>
+__global__ void k_scale(C<T>* A, long long n, double s) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    C<T> a = A[e];
+    A[e] = mk<C<T>>((T)(a.x * s), (T)(a.y * s));
+  }
+}
+
+// dealiased copy (for flux): B = D(A) on ncomp components
+template <typename T>
+__global__ void k_dealias_copy(const C<T>* __restrict__ A, C<T>* B, int ncomp, Geo g) {
+  const long long n = g.S;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n * ncomp; e += (long long)gridDim.x * blockDim.x) {
+    const long long m = e % n;
+    const int lz = (int)(m % g.Hz);
+    const int ly = (int)((m / g.Hz) % g.Ny);
+    const int lx = (int)(m / ((long long)g.Ny * g.Hz));
+    B[e] = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz) ? mk<C<T>>(0, 0) : A[e];
+  }
+}
+
+}  // namespace ts

@@ -1,0 +1,225 @@
+"""Host-side API over the C ABI, with the reference's names.
+
+``Plan`` owns a ``ts_plan`` (the basis object + FFTK plan + RK work arrays of
+the reference).  Fields are torch tensors on the GPU (complex64 / complex128,
+shape (ncomp, Nx, Ny, Nz//2+1), the reference's spectral layout) or numpy
+arrays on the host; host arrays are staged by the library inside the call.
+
+Reference-named wrappers (paths inside anandogc/tarang ``trunk/lib``):
+  FluidVF                     fluid/fluid_base/FluidVF.h:73-180
+  Nlin_incompress.Compute_nlin fluid/incompressible/nlin/compute_nlin.cc:58-109
+  Time_advance_incompress.RK4  fluid/incompressible/time_advance/RK.cc:91-170
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+_DEALIAS = {"none": L.TS_DEALIAS_NONE, "reference": L.TS_DEALIAS_REFERENCE_CORNER,
+            "two_thirds": L.TS_DEALIAS_TWO_THIRDS}
+_FORM = {"conservative": L.TS_NLIN_CONSERVATIVE, "rotational": L.TS_NLIN_ROTATIONAL}
+
+
+@dataclass
+class Forcing:
+    """Carati constant energy supply, non-global alpha/beta (force.field_procedure 1)."""
+    inner_radius: float
+    outer_radius: float
+    energy_supply: np.ndarray
+    helicity_supply: np.ndarray | None = None
+
+
+def _ptr(a) -> int:
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("field must be contiguous")
+        return a.data_ptr()
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("field must be C contiguous")
+        return a.ctypes.data
+    raise TypeError(type(a))
+
+
+class Plan:
+    def __init__(self, N, basis: str = "FFF", precision: str = "f64", nlin_form: str = "conservative",
+                 dealias: str = "reference", nu: float = 0.01, dt: float = 1e-3, kfactor=(1.0, 1.0, 1.0),
+                 reality_fix: bool = True, forcing: Forcing | None = None, kappa: float = 0.01,
+                 Ra: float = 1e5, Pr: float = 1.0):
+        self.lib = L.load()
+        if isinstance(N, int):
+            N = (N, N, N)
+        self.N = tuple(int(n) for n in N)
+        c = L.TsConfig()
+        self.lib.ts_config_default(ctypes.byref(c))
+        c.basis = L.TS_BASIS_FFF if basis == "FFF" else L.TS_BASIS_SFF
+        for i in range(3):
+            c.N[i] = self.N[i]
+            c.kfactor[i] = float(kfactor[i])
+        c.precision = L.TS_F64 if precision == "f64" else L.TS_F32
+        c.nlin_form = _FORM[nlin_form]
+        c.dealias_mode = _DEALIAS[dealias]
+        c.reality_fix = int(bool(reality_fix))
+        c.nu, c.kappa, c.dt, c.Ra, c.Pr = nu, kappa, dt, Ra, Pr
+        self._keep = []
+        if forcing is not None:
+            es = np.ascontiguousarray(forcing.energy_supply, dtype=np.float64)
+            self._keep.append(es)
+            c.force_type = L.TS_FORCE_CARATI_ENERGY_SUPPLY
+            c.force_inner_radius = forcing.inner_radius
+            c.force_outer_radius = forcing.outer_radius
+            c.energy_supply = es.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            c.n_supply = len(es)
+            if forcing.helicity_supply is not None:
+                hs = np.ascontiguousarray(forcing.helicity_supply, dtype=np.float64)
+                self._keep.append(hs)
+                c.helicity_supply = hs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self.cfg = c
+        self.basis = basis
+        self.precision = precision
+        h = ctypes.c_void_p()
+        L.check(self.lib.ts_plan_create(ctypes.byref(c), ctypes.byref(h)), "ts_plan_create")
+        self.h = h
+        n = ctypes.c_int()
+        L.check(self.lib.ts_plan_num_shells(self.h, ctypes.byref(n)), "ts_plan_num_shells")
+        self.n_shells = n.value
+
+    # ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ts_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def spec_shape(self):
+        Nx, Ny, Nz = self.N
+        return (Nx, Ny, Nz // 2 + 1)
+
+    def torch_dtype(self):
+        import torch
+        return torch.complex64 if self.precision == "f32" else torch.complex128
+
+    def numpy_dtype(self):
+        return np.complex64 if self.precision == "f32" else np.complex128
+
+    def field(self, ncomp: int = 3, device: str = "cuda"):
+        import torch
+        return torch.zeros((ncomp,) + self.spec_shape, dtype=self.torch_dtype(), device=device)
+
+    def set_stream(self, stream=None):
+        """Use a torch.cuda.Stream (default: torch's current stream) for every later call."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        L.check(self.lib.ts_plan_set_stream(self.h, ctypes.c_void_p(s.cuda_stream)), "ts_plan_set_stream")
+
+    # ------------------------------------------------------------------
+    def rk4_step(self, u, nsteps: int = 1):
+        L.check(self.lib.ts_rk4_step(self.h, _ptr(u), nsteps), "ts_rk4_step")
+
+    def rk4_step_rbc(self, u, T, nsteps: int = 1):
+        L.check(self.lib.ts_rk4_step_rbc(self.h, _ptr(u), _ptr(T), nsteps), "ts_rk4_step_rbc")
+
+    def nlin(self, u, out):
+        L.check(self.lib.ts_nlin(self.h, _ptr(u), _ptr(out)), "ts_nlin")
+        return out
+
+    def energy(self, a, ncomp: int | None = None) -> float:
+        n = a.shape[0] if ncomp is None else ncomp
+        e = ctypes.c_double()
+        L.check(self.lib.ts_energy(self.h, _ptr(a), n, ctypes.byref(e)), "ts_energy")
+        return e.value
+
+    def max_div(self, u) -> float:
+        e = ctypes.c_double()
+        L.check(self.lib.ts_max_div(self.h, _ptr(u), ctypes.byref(e)), "ts_max_div")
+        return e.value
+
+    def shell_spectrum(self, a, ncomp: int | None = None) -> np.ndarray:
+        n = a.shape[0] if ncomp is None else ncomp
+        out = np.zeros(self.n_shells)
+        L.check(self.lib.ts_shell_spectrum(self.h, _ptr(a), n, out.ctypes.data_as(L._D), self.n_shells),
+                "ts_shell_spectrum")
+        return out
+
+    def flux(self, u, radii) -> np.ndarray:
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        out = np.zeros(len(r))
+        L.check(self.lib.ts_flux(self.h, _ptr(u), r.ctypes.data_as(L._D), len(r), out.ctypes.data_as(L._D)),
+                "ts_flux")
+        return out
+
+    def nusselt(self, u, T) -> float:
+        e = ctypes.c_double()
+        L.check(self.lib.ts_nusselt(self.h, _ptr(u), _ptr(T), ctypes.byref(e)), "ts_nusselt")
+        return e.value
+
+    def init_energy_spectrum(self, E_ic, seed: int, target_energy: float, out):
+        e = np.ascontiguousarray(E_ic, dtype=np.float64)
+        L.check(self.lib.ts_init_energy_spectrum(self.h, e.ctypes.data_as(L._D), len(e), seed, target_energy,
+                                                 _ptr(out)), "ts_init_energy_spectrum")
+        return out
+
+    def forward(self, real, spec, parity: str = "FFF", ncomp: int | None = None):
+        n = real.shape[0] if ncomp is None else ncomp
+        L.check(self.lib.ts_fft_forward(self.h, parity.encode(), _ptr(real), _ptr(spec), n), "ts_fft_forward")
+        return spec
+
+    def inverse(self, spec, real, parity: str = "FFF", ncomp: int | None = None):
+        n = spec.shape[0] if ncomp is None else ncomp
+        L.check(self.lib.ts_fft_inverse(self.h, parity.encode(), _ptr(spec), _ptr(real), n), "ts_fft_inverse")
+        return real
+
+
+def kernel_launch_count() -> int:
+    return int(L.load().ts_kernel_launch_count())
+
+
+def spectrum_k4_gauss(nsh: int, k0: float) -> np.ndarray:
+    """E_IC(s) = s^4 exp(-2 (s/k0)^2) for shell s >= 1 (the benchmark initial spectrum)."""
+    s = np.arange(nsh, dtype=np.float64)
+    E = s ** 4 * np.exp(-2.0 * (s / k0) ** 2)
+    E[0] = 0
+    return E
+
+
+# ---------------------------------------------------------------------------
+# reference-named wrappers
+# ---------------------------------------------------------------------------
+class FluidVF:
+    """Velocity field container: ``cvf`` (3 spectral components) and ``nlin``."""
+
+    def __init__(self, plan: Plan, device: str = "cuda"):
+        self.plan = plan
+        self.cvf = plan.field(3, device)
+        self.nlin = plan.field(3, device)
+
+    def Compute_total_energy(self) -> float:
+        return self.plan.energy(self.cvf)
+
+    def Compute_divergence_field(self) -> float:
+        return self.plan.max_div(self.cvf)
+
+
+class Nlin_incompress:
+    @staticmethod
+    def Compute_nlin(U: FluidVF):
+        """Dealias U.cvf in place, then U.nlin = F[(u.grad)u] (compute_nlin.cc:58-109)."""
+        U.plan.nlin(U.cvf, U.nlin)
+
+
+class Time_advance_incompress:
+    @staticmethod
+    def RK4(U: FluidVF, nsteps: int = 1):
+        """IF-RK4 step(s) + strong reality condition (RK.cc:91-170, Time_advance.cc:59-60)."""
+        U.plan.rk4_step(U.cvf, nsteps)

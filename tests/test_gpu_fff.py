@@ -1,0 +1,198 @@
+"""GPU parity of the FFF path against the FP64 oracle, through the C ABI.
+
+Tolerances: FP64 path, relative L2 <= 1e-11 after a few steps (transform
+round-off ~1e-15 per operation); FP32 path (FP32 transforms, FP64 sums and
+integrating factor), relative L2 <= 1e-5 against the FP64 result of the same
+nonlinear form.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tarang_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def to_np(t):
+    return t.detach().cpu().numpy()
+
+
+def plan_for(N, **kw):
+    from tarang_b200 import Plan
+    return Plan(N, **kw)
+
+
+def oracle_ic(N, k0=4.0, seed=0, E=0.5):
+    g = R.Grid((N, N, N) if isinstance(N, int) else N)
+    return g, R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), k0), seed, E)
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N", [16, 32, 64, (32, 16, 64), (16, 64, 32)])
+def test_fft_matches_numpy(cuda, prec, N):
+    import torch
+    Ns = (N, N, N) if isinstance(N, int) else N
+    g = R.Grid(Ns)
+    plan = plan_for(Ns, precision=prec)
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal((2,) + Ns)
+    rdt = torch.float64 if prec == "f64" else torch.float32
+    real = torch.zeros((2, Ns[0], Ns[1], Ns[2] + 2), dtype=rdt, device=cuda)
+    real[..., : Ns[2]] = torch.from_numpy(u).to(rdt)
+    spec = plan.field(2)
+    plan.forward(real, spec)
+    torch.cuda.synchronize()
+    ref = np.stack([R.forward(g, u[i]) for i in range(2)])
+    tol = 1e-13 if prec == "f64" else 2e-6
+    assert rel(to_np(spec), ref) < tol
+    back = torch.zeros_like(real)
+    plan.inverse(spec, back)
+    torch.cuda.synchronize()
+    ub = to_np(back)
+    assert rel(ub[..., : Ns[2]], np.stack([R.inverse(g, ref[i]) for i in range(2)])) < tol
+    assert np.all(ub[..., Ns[2]:] == 0)
+
+
+def test_ic_matches_oracle(cuda):
+    g, V = oracle_ic(32)
+    plan = plan_for(32)
+    u = plan.field(3)
+    plan.init_energy_spectrum(R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5, u)
+    assert rel(to_np(u), V) < 1e-13
+    assert abs(plan.energy(u) - 0.5) < 1e-13
+
+
+@pytest.mark.parametrize("dealias", ["reference", "two_thirds", "none"])
+def test_nlin_matches_oracle(cuda, dealias):
+    import torch
+    mode = {"reference": 1, "two_thirds": 2, "none": 0}[dealias]
+    g, V = oracle_ic(32, k0=8.0)
+    plan = plan_for(32, dealias=dealias)
+    u = torch.from_numpy(V.copy()).to(cuda)
+    out = plan.field(3)
+    plan.nlin(u, out)
+    torch.cuda.synchronize()
+    Vd = R.dealias(g, V, mode)
+    ref = R.nlin_conservative(g, Vd)
+    assert rel(to_np(out), ref) < 1e-13
+    # the reference dealiases U in place (compute_nlin.cc:61-62)
+    assert rel(to_np(u), Vd) == 0.0
+
+
+@pytest.mark.parametrize("form", ["conservative", "rotational"])
+@pytest.mark.parametrize("dealias", ["reference", "two_thirds"])
+def test_rk4_matches_oracle_f64(cuda, form, dealias):
+    import torch
+    mode = {"reference": 1, "two_thirds": 2}[dealias]
+    g, V = oracle_ic(32)
+    cfg = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=mode, nlin_form=form)
+    plan = plan_for(32, nu=0.01, dt=1e-3, dealias=dealias, nlin_form=form)
+    u = torch.from_numpy(V.copy()).to(cuda)
+    W = V.copy()
+    for _ in range(3):
+        W = R.rk4_step(cfg, W)
+    plan.rk4_step(u, 3)
+    torch.cuda.synchronize()
+    assert rel(to_np(u), W) < 1e-12
+
+
+def test_rk4_forced_matches_oracle_f64(cuda):
+    import torch
+    g, V = oracle_ic(32)
+    es = np.zeros(g.n_shells())
+    es[3] = 0.1
+    forcing = R.CaratiForcing(2.0, 3.0, es)
+    cfg = R.FluidConfig(g, nu=1e-3, dt=5e-4, dealias_mode=1, forcing=forcing)
+    from tarang_b200 import Forcing
+    plan = plan_for(32, nu=1e-3, dt=5e-4, forcing=Forcing(2.0, 3.0, es))
+    u = torch.from_numpy(V.copy()).to(cuda)
+    W = V.copy()
+    for _ in range(3):
+        W = R.rk4_step(cfg, W)
+    plan.rk4_step(u, 3)
+    torch.cuda.synchronize()
+    assert rel(to_np(u), W) < 1e-12
+    # the forcing injects energy: E grows against the unforced run
+    W0 = V.copy()
+    cfg0 = R.FluidConfig(g, nu=1e-3, dt=5e-4, dealias_mode=1)
+    for _ in range(3):
+        W0 = R.rk4_step(cfg0, W0)
+    assert R.total_energy(g, W) > R.total_energy(g, W0)
+
+
+def test_diagnostics_match_oracle(cuda):
+    import torch
+    g, V = oracle_ic(32)
+    plan = plan_for(32, dealias="two_thirds")
+    u = torch.from_numpy(V.copy()).to(cuda)
+    assert abs(plan.energy(u) - R.total_energy(g, V)) < 1e-14
+    Ek = plan.shell_spectrum(u)
+    assert rel(Ek, R.shell_spectrum(g, V)) < 1e-13
+    assert plan.max_div(u) < 1e-14
+    radii = [0.0, 2.0, 4.0, 8.0, 10.5, 1e9]
+    Pi = plan.flux(u, radii)
+    ref = R.flux_one_pass(g, V, radii, 2)
+    assert np.max(np.abs(Pi - ref)) < 1e-13 * max(1.0, np.max(np.abs(ref)))
+    # per-sphere reference form agrees for the alias-free two-thirds field
+    ref2 = R.flux_per_sphere(g, V, radii[:-1], 2)
+    assert np.max(np.abs(Pi[:-1] - ref2)) < 1e-12
+
+
+def test_f32_rotational_vs_f64(cuda):
+    import torch
+    g, V = oracle_ic(64)
+    p64 = plan_for(64, precision="f64", nlin_form="rotational", dealias="two_thirds")
+    p32 = plan_for(64, precision="f32", nlin_form="rotational", dealias="two_thirds")
+    u64 = torch.from_numpy(V.copy()).to(cuda)
+    u32 = u64.to(torch.complex64)
+    for _ in range(5):
+        p64.rk4_step(u64, 1)
+        p32.rk4_step(u32, 1)
+        torch.cuda.synchronize()
+        e = rel(to_np(u32).astype(np.complex128), to_np(u64))
+        assert e < 1e-5
+        assert abs(p32.energy(u32) - p64.energy(u64)) / p64.energy(u64) < 1e-5
+
+
+def test_config0_plain_small(cuda):
+    """64^3, float64, nu = 0.01, dt = 1e-3, 100 steps, E(k), Pi(k) every 10 steps vs the oracle."""
+    import torch
+    g, V = oracle_ic(64)
+    cfg = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=1)
+    plan = plan_for(64, nu=0.01, dt=1e-3)
+    u = torch.from_numpy(V.copy()).to(cuda)
+    W = V.copy()
+    radii = [0.0, 2.0, 4.0, 8.0, 16.0, 32.0]
+    for step in range(1, 101):
+        W = R.rk4_step(cfg, W)
+        plan.rk4_step(u, 1)
+        if step % 10 == 0:
+            torch.cuda.synchronize()
+            assert rel(to_np(u), W) < 1e-11
+            assert rel(plan.shell_spectrum(u), R.shell_spectrum(g, W)) < 1e-11
+            Pi = plan.flux(u, radii)
+            ref = R.flux_one_pass(g, W, radii, 1)
+            assert np.max(np.abs(Pi - ref)) < 1e-11
+    assert plan.max_div(u) < 1e-12
+
+
+def test_host_pointer_step_matches_device(cuda):
+    """The reference-facing call with host buffers (staged copies inside the call)."""
+    import torch
+    g, V = oracle_ic(32)
+    plan = plan_for(32)
+    host = np.ascontiguousarray(V.copy())
+    dev = torch.from_numpy(V.copy()).to(cuda)
+    plan.rk4_step(host, 2)
+    plan.rk4_step(dev, 2)
+    torch.cuda.synchronize()
+    assert rel(host, to_np(dev)) == 0.0
