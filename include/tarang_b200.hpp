@@ -1,0 +1,150 @@
+// C++ host mirror of the reference's hot-path interface over the C ABI.
+//
+// Same class and method names as anandogc/tarang (paths inside trunk/lib):
+//   FluidVF                         fluid/fluid_base/FluidVF.h:73-180
+//   FFF_PENCIL / SFF_PENCIL         basis/FFF/pencil/FFF_pencil.h:51, basis/SFF/pencil/SFF_pencil.h:52
+//   Nlin_incompress::Compute_nlin   fluid/incompressible/nlin/Nlin.h:79
+//   Time_advance_incompress::RK4    fluid/incompressible/time_advance/Time_advance.h:69-187
+// Differences from the reference, by design: fields live in device memory
+// (one contiguous block per vector field, the reference's (Nx,Ny,Nz/2+1)
+// layout per component), errors throw ts_error instead of exit(1), and the
+// parity string that the reference passes through a global is an argument.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "tarang_b200.h"
+
+namespace tarang_b200 {
+
+struct ts_error : std::runtime_error {
+  int status;
+  ts_error(int s, const std::string& where)
+      : std::runtime_error(where + ": status " + std::to_string(s) + " " + ts_last_error()), status(s) {}
+};
+
+inline void check(int s, const char* where) {
+  if (s != TS_OK) throw ts_error(s, where);
+}
+
+// Owns a ts_plan: the basis object of the reference (FFF_PENCIL / SFF_PENCIL
+// constructor + fftk.Init, FFF_pencil.cc:31-135).
+class Universal {
+ public:
+  explicit Universal(const ts_config& c) : cfg_(c) {
+    check(ts_plan_create(&cfg_, &plan_), "ts_plan_create");
+    long long e = 0;
+    int b = 0;
+    check(ts_plan_sizes(plan_, &e, &b), "ts_plan_sizes");
+    elems_ = e;
+    bytes_ = b;
+    check(ts_plan_num_shells(plan_, &nshells_), "ts_plan_num_shells");
+  }
+  ~Universal() {
+    if (plan_) ts_plan_destroy(plan_);
+  }
+  Universal(const Universal&) = delete;
+  Universal& operator=(const Universal&) = delete;
+
+  ts_plan* plan() const { return plan_; }
+  const ts_config& config() const { return cfg_; }
+  long long elems_per_component() const { return elems_; }
+  int bytes_per_complex() const { return bytes_; }
+  int no_shells() const { return nshells_; }
+
+  // Forward_transform / Inverse_transform (FFF_pencil_tr.cc:43-66): device pointers
+  void Forward_transform(const void* Ar, void* A, const char* parity = "FFF", int ncomp = 1) {
+    check(ts_fft_forward(plan_, parity, Ar, A, ncomp), "Forward_transform");
+  }
+  void Inverse_transform(const void* A, void* Ar, const char* parity = "FFF", int ncomp = 1) {
+    check(ts_fft_inverse(plan_, parity, A, Ar, ncomp), "Inverse_transform");
+  }
+  // Compute_shell_spectrum (universal_energy.cc:279-366), summed over ncomp components
+  std::vector<double> Compute_shell_spectrum(const void* A, int ncomp = 3) {
+    std::vector<double> Ek(nshells_);
+    check(ts_shell_spectrum(plan_, A, ncomp, Ek.data(), nshells_), "Compute_shell_spectrum");
+    return Ek;
+  }
+  double Get_total_energy(const void* A, int ncomp = 1) {
+    double e = 0;
+    check(ts_energy(plan_, A, ncomp, &e), "Get_total_energy");
+    return e;
+  }
+
+ private:
+  ts_config cfg_;
+  ts_plan* plan_ = nullptr;
+  long long elems_ = 0;
+  int bytes_ = 0;
+  int nshells_ = 0;
+};
+
+class FFF_PENCIL : public Universal {
+ public:
+  explicit FFF_PENCIL(ts_config c) : Universal((c.basis = TS_BASIS_FFF, c)) {}
+};
+
+class SFF_PENCIL : public Universal {
+ public:
+  explicit SFF_PENCIL(ts_config c) : Universal((c.basis = TS_BASIS_SFF, c)) {}
+};
+
+// Velocity field: cvf (V1, V2, V3) and nlin (nlin1..3), each a contiguous
+// device block of 3 components.
+class FluidVF {
+ public:
+  explicit FluidVF(Universal& basis) : basis_(basis) {
+    bytes_ = 3ull * basis.elems_per_component() * basis.bytes_per_complex();
+    if (cudaMalloc(&cvf_, bytes_) != cudaSuccess || cudaMalloc(&nlin_, bytes_) != cudaSuccess)
+      throw ts_error(TS_ERR_NOMEM, "FluidVF");
+    cudaMemset(cvf_, 0, bytes_);
+    cudaMemset(nlin_, 0, bytes_);
+  }
+  ~FluidVF() {
+    cudaFree(cvf_);
+    cudaFree(nlin_);
+  }
+  FluidVF(const FluidVF&) = delete;
+  FluidVF& operator=(const FluidVF&) = delete;
+
+  void* cvf() { return cvf_; }
+  void* nlin() { return nlin_; }
+  size_t bytes() const { return bytes_; }
+  Universal& basis() { return basis_; }
+
+  // Init_cond_energy_helicity_spectrum construction (init_cond_energy.cc:67-120)
+  void Init_cond_energy_spectrum(const std::vector<double>& Eic, uint64_t seed, double energy) {
+    check(ts_init_energy_spectrum(basis_.plan(), Eic.data(), (int)Eic.size(), seed, energy, cvf_),
+          "Init_cond_energy_spectrum");
+  }
+  double Compute_total_energy() { return basis_.Get_total_energy(cvf_, 3); }
+  double Compute_divergence_field() {
+    double d = 0;
+    check(ts_max_div(basis_.plan(), cvf_, &d), "Compute_divergence_field");
+    return d;
+  }
+  void Copy_to_host(void* host) { cudaMemcpy(host, cvf_, bytes_, cudaMemcpyDeviceToHost); }
+  void Copy_from_host(const void* host) { cudaMemcpy(cvf_, host, bytes_, cudaMemcpyHostToDevice); }
+
+ private:
+  Universal& basis_;
+  void* cvf_ = nullptr;
+  void* nlin_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+struct Nlin_incompress {
+  // dealias U.cvf in place, U.nlin = F[(u.grad)u] (compute_nlin.cc:58-109)
+  static void Compute_nlin(FluidVF& U) { check(ts_nlin(U.basis().plan(), U.cvf(), U.nlin()), "Compute_nlin"); }
+};
+
+struct Time_advance_incompress {
+  // RK4(U,P,F) + strong reality condition when the plan enables it (RK.cc:91-170, Time_advance.cc:59-60)
+  static void RK4(FluidVF& U, int nsteps = 1) { check(ts_rk4_step(U.basis().plan(), U.cvf(), nsteps), "RK4"); }
+};
+
+}  // namespace tarang_b200

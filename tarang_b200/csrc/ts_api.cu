@@ -380,10 +380,11 @@ static int step_fff(ts_plan* p, void* U0) {
   a.fkm = p->fkm;
   for (int stage = 1; stage <= 4; ++stage) {
     const void* Uin = stage == 1 ? U0 : p->Ucur;
-    ProfScope ps(p, TS_KCLASS_OTHER);
-    if (a.fcube)
+    if (a.fcube) {
+      ProfScope ps(p, TS_KCLASS_OTHER);
       CK(LAUNCH(p, carati, g, Uin, p->fcube, p->fkm, p->cfg.force_inner_radius, p->cfg.force_outer_radius, p->esup,
                 p->hsup, p->mis_d, p->nsup, p->st));
+    }
     a.stage = stage;
     CKS(rhs_fff(p, Uin, MODE_STEP, a));
   }

@@ -140,17 +140,21 @@ __device__ __forceinline__ void pass_compute(V* v, int t, const V* __restrict__ 
 // `sm` addressed as sm[row*rs + cs] (caller supplies the per-thread column
 // offset cs and the row stride rs).  All threads of the block must call it.
 // On return v[s] holds output row final_row(t, s).
-template <int L, int E, int DIR, int P = 0, typename V>
+// padded shared-memory row index: one spare slot every 16 complex values keeps
+// the threads of a line (consecutive rows E apart) on distinct banks
+template <bool PAD> __device__ __forceinline__ int prow(int r) { return PAD ? r + (r >> 4) : r; }
+
+template <int L, int E, int DIR, int P = 0, bool PAD = false, typename V>
 __device__ __forceinline__ void fft_regs(V* v, int t, V* sm, int rs, int cs, const V* __restrict__ tw, int tws) {
   pass_compute<L, E, P, DIR>(v, t, tw, tws);
   if constexpr (P + 1 < npasses(L, E)) {
 #pragma unroll
-    for (int s = 0; s < E; ++s) sm[Pass<L, E, P>::out_row(t, s) * rs + cs] = v[s];
+    for (int s = 0; s < E; ++s) sm[prow<PAD>(Pass<L, E, P>::out_row(t, s)) * rs + cs] = v[s];
     __syncthreads();
 #pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = sm[Pass<L, E, P + 1>::in_row(t, s) * rs + cs];
+    for (int s = 0; s < E; ++s) v[s] = sm[prow<PAD>(Pass<L, E, P + 1>::in_row(t, s)) * rs + cs];
     __syncthreads();
-    fft_regs<L, E, DIR, P + 1>(v, t, sm, rs, cs, tw, tws);
+    fft_regs<L, E, DIR, P + 1, PAD>(v, t, sm, rs, cs, tw, tws);
   }
 }
 

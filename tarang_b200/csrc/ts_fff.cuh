@@ -103,81 +103,97 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1) k
 
 // ---------------------------------------------------------------------------
 // z pass: C2R of the NIN input lines, real-space products, R2C of the NOUT
-// product lines.  Lines are contiguous (Hz complex); a block handles `nl`
-// consecutive (x,y) lines of every component.  In place: outputs overwrite the
-// first NOUT components at the same lines after every input line is loaded.
+// product lines.  Lines are contiguous (Hz = M+1 complex, M = Nz/2); a block
+// handles `nl` consecutive (x,y) lines of every component, with TPL = M/E
+// threads per line.  Each component's line is transformed in registers and
+// exchanged through its own padded shared-memory slot (M + M/16 complex);
+// after the inverse transforms slot c holds the real line of component c
+// packed as M complex (re = even point, im = odd point), the products are
+// formed in place per point, and each product line is transformed forward in
+// its slot and post-processed straight to global memory.
+// In place on P: outputs overwrite the first NOUT components at the same
+// lines, after every input line has been read.
 // FORM 0 (conservative): in u1,u2,u3 -> out u1u1,u2u2,u3u3,u1u2,u2u3,u3u1
 // FORM 1 (rotational):   in u1..3,w1..3 -> out u x w
 // ---------------------------------------------------------------------------
+template <int M> __host__ __device__ constexpr int zslot() { return M + M / 16 + 1; }
+
 template <typename T, int NZ, int E, int FORM>
-__global__ void k_z_fused(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int nl) {
+__global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int nl) {
   typedef C<T> V;
-  constexpr int M = NZ / 2, H = M + 1;
+  constexpr int M = NZ / 2, H = M + 1, TPL = M / E, LDS = zslot<M>();
   constexpr int NIN = FORM == 0 ? 3 : 6, NOUT = FORM == 0 ? 6 : 3;
   extern __shared__ __align__(16) unsigned char smraw[];
-  V* bufA = reinterpret_cast<V*>(smraw);
-  V* bufB = bufA + 6 * nl * H;
+  V* sm = reinterpret_cast<V*>(smraw);
   const long long nlines = (long long)g.Nx * g.Ny;
   const long long line0 = (long long)blockIdx.x * nl;
   const int nh = (int)((nlines - line0) < nl ? (nlines - line0) : nl);
-  // 1. load inputs (contiguous runs of nh*H complex per component)
-  for (int i = 0; i < NIN; ++i) {
-    const V* src = P + i * g.S + line0 * H;
-    V* dst = bufA + i * nl * H;
-    for (int e = threadIdx.x; e < nh * H; e += blockDim.x) dst[e] = src[e];
+  const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const bool live = l < nh;
+  const long long lbase = (line0 + (live ? l : 0)) * H;
+  auto slot = [&](int c, int ll) { return sm + (c * nl + ll) * LDS; };
+
+  // A. inverse: Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]) (imag of X[0], X[M] dropped),
+  //    then the length-M inverse FFT gives z[n] = u[2n] + i u[2n+1]
+  for (int c = 0; c < NIN; ++c) {
+    const V* X = P + c * g.S + lbase;
+    V v[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int k = load_row<M, E>(t, s);
+      V a = mk<V>(0, 0), b = mk<V>(0, 0);
+      if (live) { a = X[k]; b = conjg(X[M - k]); }
+      if (k == 0) { a.y = 0; b.y = 0; }
+      v[s] = add(add(a, b), mul_i<1>(mul(conjg(tw[k]), sub(a, b))));
+    }
+    V* sl = slot(c, l < nl ? l : 0);
+    fft_regs<M, E, 1, 0, true>(v, t, sl, 1, 0, tw, 2);
+#pragma unroll
+    for (int s = 0; s < E; ++s) sl[prow<true>(final_row<M, E>(t, s))] = v[s];
   }
   __syncthreads();
-  // 2. C2R pre-processing into bufB: Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k])
-  for (int e = threadIdx.x; e < NIN * nl * M; e += blockDim.x) {
-    const int li = e / M, k = e % M;
-    const int l = li % nl;
-    if (l >= nh) continue;
-    const V* x = bufA + li * H;
-    V X = x[k], Y = conjg(x[M - k]);
-    if (k == 0) { X.y = 0; Y.y = 0; }
-    const V w = conjg(tw[k]);
-    bufB[li * H + k] = add(add(X, Y), mul_i<1>(mul(w, sub(X, Y))));
-  }
-  __syncthreads();
-  V* r = fft_smem_lines<M, E, 1>(bufB, bufA, NIN * nl, H, tw, 2);
-  V* o = (r == bufA) ? bufB : bufA;
-  // 4. products: real value n of line li is ((T*)(buf + li*H))[n]
-  for (int e = threadIdx.x; e < nl * NZ; e += blockDim.x) {
-    const int l = e / NZ, n = e % NZ;
-    if (l >= nh) continue;
-    auto rv = [&](int comp) { return reinterpret_cast<const T*>(r + (comp * nl + l) * H)[n]; };
-    auto wv = [&](int comp, T val) { reinterpret_cast<T*>(o + (comp * nl + l) * H)[n] = val; };
-    const T u1 = rv(0), u2 = rv(1), u3 = rv(2);
+  // B. products, in place per real point pair
+  for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
+    const int ll = e / M, m = prow<true>(e % M);
+    V in[NIN];
+#pragma unroll
+    for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
     if (FORM == 0) {
-      wv(0, u1 * u1); wv(1, u2 * u2); wv(2, u3 * u3);
-      wv(3, u1 * u2); wv(4, u2 * u3); wv(5, u3 * u1);
+      slot(0, ll)[m] = mk<V>(in[0].x * in[0].x, in[0].y * in[0].y);
+      slot(1, ll)[m] = mk<V>(in[1].x * in[1].x, in[1].y * in[1].y);
+      slot(2, ll)[m] = mk<V>(in[2].x * in[2].x, in[2].y * in[2].y);
+      slot(3, ll)[m] = mk<V>(in[0].x * in[1].x, in[0].y * in[1].y);
+      slot(4, ll)[m] = mk<V>(in[1].x * in[2].x, in[1].y * in[2].y);
+      slot(5, ll)[m] = mk<V>(in[2].x * in[0].x, in[2].y * in[0].y);
     } else {
-      const T w1 = rv(3), w2 = rv(4), w3 = rv(5);
-      wv(0, u2 * w3 - u3 * w2); wv(1, u3 * w1 - u1 * w3); wv(2, u1 * w2 - u2 * w1);
+      slot(0, ll)[m] = mk<V>(in[1].x * in[5].x - in[2].x * in[4].x, in[1].y * in[5].y - in[2].y * in[4].y);
+      slot(1, ll)[m] = mk<V>(in[2].x * in[3].x - in[0].x * in[5].x, in[2].y * in[3].y - in[0].y * in[5].y);
+      slot(2, ll)[m] = mk<V>(in[0].x * in[4].x - in[1].x * in[3].x, in[0].y * in[4].y - in[1].y * in[3].y);
     }
   }
   __syncthreads();
-  V* q = fft_smem_lines<M, E, -1>(o, r, NOUT * nl, H, tw, 2);
-  V* o2 = (q == bufA) ? bufB : bufA;
-  // 6. R2C post-processing: X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]
-  for (int e = threadIdx.x; e < NOUT * nl * H; e += blockDim.x) {
-    const int li = e / H, k = e % H;
-    const int l = li % nl;
-    if (l >= nh) continue;
-    const V* z = q + li * H;
-    const V Z = z[k == M ? 0 : k];
-    const V Zp = conjg(z[k == 0 ? 0 : M - k]);
-    const V w = tw[k == M ? M : k];
-    const V s = scale(add(Z, Zp), (T)0.5);
-    const V d = mul_i<-1>(mul(w, scale(sub(Z, Zp), (T)0.5)));
-    o2[li * H + k] = add(s, d);
-  }
-  __syncthreads();
-  // 7. store
-  for (int i = 0; i < NOUT; ++i) {
-    V* dst = P + i * g.S + line0 * H;
-    const V* src = o2 + i * nl * H;
-    for (int e = threadIdx.x; e < nh * H; e += blockDim.x) dst[e] = src[e];
+  // C. forward: length-M FFT of z[n] = p[2n] + i p[2n+1], then
+  //    X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]
+  for (int c = 0; c < NOUT; ++c) {
+    V* sl = slot(c, l < nl ? l : 0);
+    V v[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) v[s] = sl[prow<true>(load_row<M, E>(t, s))];
+    __syncthreads();
+    fft_regs<M, E, -1, 0, true>(v, t, sl, 1, 0, tw, 2);
+#pragma unroll
+    for (int s = 0; s < E; ++s) sl[prow<true>(final_row<M, E>(t, s))] = v[s];
+    __syncthreads();
+    V* dst = P + c * g.S + line0 * H;
+    for (int e = threadIdx.x; e < nh * H; e += blockDim.x) {
+      const int ll = e / H, k = e % H;
+      const V* z = slot(c, ll);
+      const V Z = z[prow<true>(k == M ? 0 : k)];
+      const V Zp = conjg(z[prow<true>(k == 0 ? 0 : M - k)]);
+      const V s = scale(add(Z, Zp), (T)0.5);
+      const V d = mul_i<-1>(mul(tw[k], scale(sub(Z, Zp), (T)0.5)));
+      dst[e] = add(s, d);
+    }
   }
 }
 

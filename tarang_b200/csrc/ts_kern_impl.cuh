@@ -115,20 +115,24 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int rot, void* P, const
   cudaError_t err = cudaErrorInvalidValue;
   dispatch_L(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
-    constexpr int M = NZ / 2, H = M + 1;
-    constexpr int E = emin(E_REG, M);
-    const int nl = z_lines(6, H);
-    const size_t sm = 2ull * 6 * nl * H * sizeof(V);
+    constexpr int M = NZ / 2;
+    constexpr int E = emin(8, M);
+    constexpr int TPL = M / E;
+    // lines per block: 256 threads, at most ~104 KB of slots (two blocks per SM)
+    int nl = 256 / TPL;
+    while (nl > 1 && 6ull * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
+    const size_t sm = 6ull * nl * zslot<M>() * sizeof(V);
     const long long nlines = (long long)g.Nx * g.Ny;
     dim3 grid((unsigned)((nlines + nl - 1) / nl));
+    const int threads = nl * TPL;
     if (rot) {
       auto k = k_z_fused<T, NZ, E, 1>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<grid, 256, sm, st>>>((V*)P, g, (const V*)tw, nl);
+      k<<<grid, threads, sm, st>>>((V*)P, g, (const V*)tw, nl);
     } else {
       auto k = k_z_fused<T, NZ, E, 0>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<grid, 256, sm, st>>>((V*)P, g, (const V*)tw, nl);
+      k<<<grid, threads, sm, st>>>((V*)P, g, (const V*)tw, nl);
     }
     ++g_launches;
     err = cudaGetLastError();

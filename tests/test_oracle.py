@@ -1,0 +1,233 @@
+"""Known-answer tests of the FP64 oracle (CPU only).
+
+The reference ships no tests or golden vectors (its src/test is commented
+out), so the oracle is pinned by (a) the reference's own analytic initial
+conditions, whose spectral coefficients fix the transform convention
+(ic_model.cc:55-140), and (b) analytic / self-consistency identities.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tarang_ref as R
+
+
+def tg_real(g, k0=1, amp=1.0):
+    N = g.N[0]
+    x = 2 * np.pi * np.arange(N) / N
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    u = amp * np.sin(k0 * X) * np.cos(k0 * Y) * np.cos(k0 * Z)
+    v = -amp * np.cos(k0 * X) * np.sin(k0 * Y) * np.cos(k0 * Z)
+    return np.stack([u, v, np.zeros_like(u)])
+
+
+def fwd(g, ur):
+    return np.stack([R.forward(g, ur[i]) for i in range(ur.shape[0])])
+
+
+def test_taylor_green_coefficients_match_reference_ic():
+    """Setup_Taylor_Green_field FFF (ic_model.cc:84-94): V1(+-k0,+-k0,k0) = -+i amp/8, V2 likewise."""
+    g = R.Grid((16, 16, 16))
+    k0, amp = 2, 0.7
+    V = fwd(g, tg_real(g, k0, amp))
+    ex = np.zeros_like(V)
+    lx = lambda k: k % 16
+    ex[0, lx(k0), lx(k0), k0] = -1j * amp / 8
+    ex[0, lx(k0), lx(-k0), k0] = -1j * amp / 8
+    ex[0, lx(-k0), lx(k0), k0] = 1j * amp / 8
+    ex[0, lx(-k0), lx(-k0), k0] = 1j * amp / 8
+    ex[1, lx(k0), lx(k0), k0] = 1j * amp / 8
+    ex[1, lx(-k0), lx(k0), k0] = 1j * amp / 8
+    ex[1, lx(k0), lx(-k0), k0] = -1j * amp / 8
+    ex[1, lx(-k0), lx(-k0), k0] = -1j * amp / 8
+    assert np.max(np.abs(V - ex)) < 1e-15
+
+
+def test_abc_reference_ic_real_field():
+    """Setup_ABC_field FFF (ic_model.cc:117-129): the kz-only modes carry amp*C, so the inverse
+    transform gives u1 = amp (B cos y + 2 C sin z) (not a Beltrami field)."""
+    g = R.Grid((16, 16, 16))
+    A, B, C, amp = 0.3, 0.5, 0.7, 1.1
+    V = np.zeros((3,) + g.shape, complex)
+    V[0, 0, 1, 0] = amp * B / 2
+    V[0, 0, 15, 0] = amp * B / 2
+    V[0, 0, 0, 1] = -1j * amp * C
+    u1 = R.inverse(g, V[0])
+    x = 2 * np.pi * np.arange(16) / 16
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    assert np.max(np.abs(u1 - amp * (B * np.cos(Y) + 2 * C * np.sin(Z)))) < 1e-14
+
+
+@pytest.mark.parametrize("N", [(16, 16, 16), (8, 16, 32)])
+def test_roundtrip_and_parseval(N):
+    g = R.Grid(N)
+    rng = np.random.default_rng(0)
+    u = rng.standard_normal(N)
+    A = R.forward(g, u)
+    assert np.max(np.abs(R.inverse(g, A) - u)) < 1e-13
+    A[:, :, N[2] // 2] = 0  # Parseval holds for fields without the kz = Nz/2 plane
+    ur = R.inverse(g, A)
+    assert abs(R.total_energy_scalar(g, A) - (ur ** 2).sum() / (2 * np.prod(N))) < 1e-13
+
+
+@pytest.mark.parametrize("par", ["S", "C"])
+def test_sff_roundtrip_and_energy(par):
+    g = R.Grid((16, 8, 16), (math.pi, 2 * math.pi, 2 * math.pi), "SFF")
+    rng = np.random.default_rng(3)
+    A = R.forward(g, rng.standard_normal(g.rshape), par)
+    A[:, :, g.N[2] // 2] = 0
+    ur = R.inverse(g, A, par)
+    A2 = R.forward(g, ur, par)
+    assert np.max(np.abs(A2 - A)) < 1e-13
+    assert abs(R.total_energy_scalar(g, A) - (ur ** 2).sum() / (2 * ur.size)) < 1e-12
+
+
+def test_derivative_of_single_mode():
+    g = R.Grid((16, 16, 16))
+    x = 2 * np.pi * np.arange(16) / 16
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    u = np.sin(3 * X) * np.cos(2 * Z)
+    A = R.forward(g, u)
+    dx = R.inverse(g, R.xderiv(g, A))
+    dz = R.inverse(g, R.zderiv(g, A))
+    assert np.max(np.abs(dx - 3 * np.cos(3 * X) * np.cos(2 * Z))) < 1e-13
+    assert np.max(np.abs(dz + 2 * np.sin(3 * X) * np.sin(2 * Z))) < 1e-13
+
+
+def test_sff_x_derivative_parity():
+    """SFF Xderiv: a sine series differentiates to a cosine series with +Kx (SFF_pencil_tr.cc:77-90)."""
+    g = R.Grid((16, 8, 8), (math.pi, 2 * math.pi, 2 * math.pi), "SFF")
+    xs = (np.arange(16) + 0.5) / 16
+    X = xs[:, None, None] * np.ones((16, 8, 8))
+    u = np.sin(3 * math.pi * X)
+    A = R.forward(g, u, "S")
+    du = R.inverse(g, R.xderiv(g, A, "S"), "C")
+    assert np.max(np.abs(du - 3 * math.pi * np.cos(3 * math.pi * X))) < 1e-12
+
+
+def test_projection_idempotent_and_solenoidal():
+    g = R.Grid((16, 16, 16))
+    rng = np.random.default_rng(1)
+    N = np.stack([R.forward(g, rng.standard_normal((16, 16, 16))) for _ in range(3)])
+    P1 = -R.project_rhs(g, N)
+    P2 = -R.project_rhs(g, P1)
+    assert np.max(np.abs(P1 - P2)) < 1e-15
+    assert R.max_abs_div(g, P1) < 1e-14
+
+
+def test_taylor_green_linear_decay():
+    """Small amplitude TG decays as exp(-2 nu k^2 t) in energy, k^2 = 3 (the IF factor is exact)."""
+    g = R.Grid((16, 16, 16))
+    V = fwd(g, tg_real(g, 1, 1e-7))
+    nu, dt, n = 0.05, 1e-2, 10
+    cfg = R.FluidConfig(g, nu=nu, dt=dt, dealias_mode=R.DEALIAS_TWO_THIRDS)
+    E0 = R.total_energy(g, V)
+    for _ in range(n):
+        V = R.rk4_step(cfg, V)
+    assert abs(R.total_energy(g, V) / E0 - math.exp(-2 * nu * 3 * n * dt)) < 1e-9
+
+
+def test_beltrami_field_decays_exactly():
+    """A k=1 Beltrami field (omega = u) has u x omega = 0: after projection the nonlinear term
+    vanishes, so u(t) = u(0) exp(-nu t)."""
+    g = R.Grid((16, 16, 16))
+    x = 2 * np.pi * np.arange(16) / 16
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    A, B, C = 0.9, 0.6, 0.4
+    u = np.stack([A * np.sin(Z) + C * np.cos(Y), B * np.sin(X) + A * np.cos(Z), C * np.sin(Y) + B * np.cos(X)])
+    V = fwd(g, u)
+    nu, dt, n = 0.02, 1e-2, 5
+    for form in ("conservative", "rotational"):
+        cfg = R.FluidConfig(g, nu=nu, dt=dt, dealias_mode=R.DEALIAS_TWO_THIRDS, nlin_form=form)
+        W = V.copy()
+        for _ in range(n):
+            W = R.rk4_step(cfg, W)
+        assert np.max(np.abs(W - V * math.exp(-nu * n * dt))) < 1e-13
+
+
+def test_nonlinear_term_conserves_energy_two_thirds():
+    """For a two-thirds-dealiased field the projected nonlinear term does no work:
+    sum_w Re(U* . RHS(U)) = 0 (inviscid, unforced), in both forms."""
+    g = R.Grid((32, 32, 32))
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 5, 0.5)
+    V = R.dealias(g, V, R.DEALIAS_TWO_THIRDS)
+    for form in ("conservative", "rotational"):
+        cfg = R.FluidConfig(g, nu=0.0, dt=1e-3, dealias_mode=R.DEALIAS_TWO_THIRDS, nlin_form=form)
+        rhs, _ = R.fluid_rhs(cfg, V, g.modes_in_shell())
+        work = sum(R.cross_energy(g, rhs[i], V[i]) for i in range(3))
+        scale = sum(R.cross_energy(g, np.abs(rhs[i]), np.abs(V[i])) for i in range(3))
+        assert abs(work) < 1e-14 * scale
+
+
+def test_conservative_and_rotational_agree_on_kept_modes():
+    g = R.Grid((16, 16, 16))
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 2, 0.5)
+    Vd = R.dealias(g, V, R.DEALIAS_TWO_THIRDS)
+    Nc = R.project_rhs(g, R.nlin_conservative(g, Vd))
+    Nr = R.project_rhs(g, R.nlin_rotational(g, Vd))
+    keep = ~R.dealias_mask(g, R.DEALIAS_TWO_THIRDS)
+    assert np.max(np.abs((Nc - Nr)[:, keep])) < 1e-14
+
+
+def test_flux_one_pass_equals_per_sphere():
+    g = R.Grid((16, 16, 16))
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 7, 0.5)
+    radii = [0.0, 1.5, 2.0, 3.0, 4.0]
+    a = R.flux_per_sphere(g, V, radii, R.DEALIAS_TWO_THIRDS)
+    b = R.flux_one_pass(g, V, radii, R.DEALIAS_TWO_THIRDS)
+    assert np.max(np.abs(a - b)) < 1e-15
+
+
+def test_ic_shell_energies_and_divergence():
+    """Per shell s < N/2-1 the Tarang-weighted energy equals c E_ic(s) exactly; div = 0."""
+    g = R.Grid((32, 32, 32))
+    E = R.spectrum_k4_gauss(g.n_shells(), 4.0)
+    V = R.init_energy_spectrum(g, E, 11, None)
+    assert R.max_abs_div(g, V) < 1e-15 * 16 * np.abs(V).max()
+    idx = np.ceil(g.Kmag()).astype(int)
+    w = np.where(np.arange(g.shape[2])[None, None, :] == 0, 0.5, 1.0) * np.ones(g.shape)
+    e = (np.abs(V) ** 2).sum(0) * w
+    shells = np.bincount(idx.ravel(), weights=e.ravel())
+    s = np.arange(1, 15)
+    np.testing.assert_allclose(shells[s], E[s], rtol=1e-12)
+    V2 = R.init_energy_spectrum(g, E, 11, 0.5)
+    assert abs(R.total_energy(g, V2) - 0.5) < 1e-14
+
+
+def test_rng_is_counter_based_splitmix64():
+    u = R.uniform01(0, np.arange(4, dtype=np.uint64))
+    assert np.all((u >= 0) & (u < 1))
+    # fixed values of this project's generator (shared with csrc/ts_misc.cuh)
+    assert abs(u[0] - R.uniform01(0, np.array([0], np.uint64))[0]) == 0
+    assert R.uniform01(1, np.arange(4, dtype=np.uint64))[0] != u[0]
+
+
+def test_reality_fix_makes_kz0_plane_hermitian():
+    g = R.Grid((8, 8, 8))
+    rng = np.random.default_rng(4)
+    A = rng.standard_normal(g.shape) + 1j * rng.standard_normal(g.shape)
+    B = R.reality_fix(g, A)
+    assert np.all(B[:, :, 4] == 0)
+    for lx in range(5, 8):
+        for ly in range(8):
+            if g.ky[ly] != 4:
+                assert B[lx, ly, 0] == np.conj(B[(-g.kx[lx]) % 8, (-g.ky[ly]) % 8, 0])
+
+
+def test_rbc_linear_stability():
+    """Free-slip RBC, kfactor (pi, 2pi, 2pi): the lowest mode (m=1, k_perp=2pi) has critical
+    Ra = (pi^2 + 4 pi^2)^3 / (4 pi^2) ~ 3044; a small perturbation decays at Ra=1000 and grows at Ra=1e5."""
+    g = R.Grid((16, 8, 8), (math.pi, 2 * math.pi, 2 * math.pi), "SFF")
+    T0 = R.rbc_temperature_ic(g, 1e-6, 1.5, 3)
+    U0 = np.zeros((3,) + g.shape, complex)
+    out = {}
+    for Ra in (1e3, 1e5):
+        cfg = R.RBCConfig(g, Ra=Ra, Pr=1.0, dt=2e-2)
+        U, T = U0.copy(), T0.copy()
+        E0 = R.total_energy_scalar(g, T)
+        for _ in range(60):
+            U, T = R.rbc_rk4_step(cfg, U, T)
+        out[Ra] = R.total_energy_scalar(g, T) / E0
+    assert out[1e3] < 0.9
+    assert out[1e5] > 1.1
