@@ -151,6 +151,24 @@ int ts_profile_reset(ts_plan* plan);
 int ts_profile_read(ts_plan* plan, int kernel_class, double* total_ms, long long* launches,
                     double* bytes_per_launch);
 
+/* Shell spectrum E(k) without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when they
+ * need the diagnostic (a stepping loop that has reserved nearly all of the GPU's
+ * memory for its fields, or one that must not let cudaMalloc / cudaFree
+ * synchronize the device).  Same result as ts_shell_spectrum, but it needs no
+ * plan: the caller passes the geometry, the device field a_hat (ncomp
+ * components) and a device array Ek[n_shells], which receives the normalised
+ * spectrum.  The shell accumulators are a file-scope __device__ array of
+ * TS_NOALLOC_MAX_SHELLS shells (64 KiB, held on every GPU that loads the
+ * library until exit); more shells than that return TS_ERR_ARG with a message
+ * on stderr.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  Calls share the array and each clears it on `stream`
+ * before use, so calls that overlap on the GPU race: order them. */
+#define TS_NOALLOC_MAX_SHELLS 4096
+int ts_shell_spectrum_noalloc(int basis, int precision, const int N[3], const double kfactor[3], const void* a_hat,
+                              int ncomp, double* Ek, int n_shells, void* stream);
+
 /* Number of kernels this library has launched since load (diagnostics). */
 long long ts_kernel_launch_count(void);
 /* Last CUDA error string seen by the library ("" if none). */

@@ -70,6 +70,8 @@ SIGNATURES = {
     "ts_profile_enable": (ctypes.c_int, [_P, ctypes.c_int]),
     "ts_profile_reset": (ctypes.c_int, [_P]),
     "ts_profile_read": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.POINTER(ctypes.c_longlong), _D]),
+    "ts_shell_spectrum_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _D, _P,
+                                                  ctypes.c_int, _P, ctypes.c_int, _P]),
     "ts_kernel_launch_count": (ctypes.c_longlong, []),
     "ts_last_error": (ctypes.c_char_p, []),
 }

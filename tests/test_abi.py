@@ -17,7 +17,7 @@ def header_functions():
 def test_header_declares_the_entry_points():
     names = header_functions()
     for n in ["ts_plan_create", "ts_rk4_step", "ts_nlin", "ts_fft_forward", "ts_fft_inverse", "ts_shell_spectrum",
-              "ts_flux", "ts_energy", "ts_max_div", "ts_rk4_step_rbc", "ts_nusselt"]:
+              "ts_flux", "ts_energy", "ts_max_div", "ts_rk4_step_rbc", "ts_nusselt", "ts_shell_spectrum_noalloc"]:
         assert n in names
 
 
