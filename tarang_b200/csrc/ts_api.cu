@@ -63,6 +63,9 @@ struct ts_plan {
   size_t dscr_n = 0;
   void* stage_u = nullptr;  // staging for host pointers (3 components)
   void* stage_t = nullptr;  // staging for host pointers (1 component)
+  int* err_d = nullptr;     // device error word (bounded waits that gave up)
+  int* err_h = nullptr;     // pinned copy, refreshed after every step call
+  double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
   // per-kernel-class CUDA event timing (ts_profile_*)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -187,6 +190,27 @@ static int ensure_stage(void** buf, size_t bytes) {
   return TS_OK;
 }
 
+// Integrating-factor tables: E(1/2)(K) = exp(-nu dt K^2 / 2) factorises over the
+// axes, exp(-nu dt/2 Kx^2) exp(-nu dt/2 Ky^2) exp(-nu dt/2 Kz^2) (FP64)
+static int upload_if_tables(ts_plan* p, double nu, double dt) {
+  const Geo& g = p->g;
+  const int n[3] = {g.Nx, g.Ny, g.Hz};
+  for (int ax = 0; ax < 3; ++ax) {
+    std::vector<double> h(n[ax]);
+    for (int l = 0; l < n[ax]; ++l) {
+      int k;
+      if (ax == 0) k = g.basis == 0 ? (l <= g.Nx / 2 ? l : l - g.Nx) : l;
+      else if (ax == 1) k = l <= g.Ny / 2 ? l : l - g.Ny;
+      else k = l;
+      const double K = k * g.kf[ax];
+      h[l] = exp(-nu * 0.5 * dt * (K * K));
+    }
+    if (!p->eax[ax]) CK(cudaMalloc(&p->eax[ax], n[ax] * sizeof(double)));
+    CK(cudaMemcpy(p->eax[ax], h.data(), n[ax] * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return TS_OK;
+}
+
 // dispatch a Launch<T>::fn call on the plan's precision
 #define LAUNCH(p, fn, ...) \
   ((p)->prec == 1 ? Launch<float>::fn(__VA_ARGS__) : Launch<double>::fn(__VA_ARGS__))
@@ -223,6 +247,10 @@ int ts_plan_destroy(ts_plan* p) {
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
+  for (int i = 0; i < 3; ++i)
+    if (p->eax[i]) cudaFree(p->eax[i]);
+  if (p->err_d) cudaFree(p->err_d);
+  if (p->err_h) cudaFreeHost(p->err_h);
   delete p;
   return TS_OK;
 }
@@ -319,6 +347,13 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     return TS_ERR_ARG;
   }
   CKP(ensure_scratch(p, 4096));
+  CKP(alloc((void**)&p->err_d, sizeof(int)));
+  if (cudaMemset(p->err_d, 0, sizeof(int)) != cudaSuccess || cudaMallocHost(&p->err_h, sizeof(int)) != cudaSuccess) {
+    ts_plan_destroy(p);
+    return TS_ERR_CUDA;
+  }
+  *p->err_h = 0;
+  CKP(upload_if_tables(p, cfg->nu, cfg->dt));
 #undef CKP
   *out = p;
   return TS_OK;
@@ -345,8 +380,10 @@ int ts_plan_num_shells(const ts_plan* p, int* n) {
 
 int ts_plan_set_dt(ts_plan* p, double dt) {
   if (!p || !(dt > 0)) return TS_ERR_ARG;
+  if (dt == p->cfg.dt) return TS_OK;
+  CK(cudaStreamSynchronize(p->st));
   p->cfg.dt = dt;
-  return TS_OK;
+  return upload_if_tables(p, p->cfg.nu, dt);
 }
 
 }  // extern "C"
@@ -354,13 +391,18 @@ int ts_plan_set_dt(ts_plan* p, double dt) {
 // ---------------------------------------------------------------------------
 // right-hand side pipeline (FFF)
 // ---------------------------------------------------------------------------
-static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a) {
+static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in) {
   const Geo& g = p->g;
+  StageArgs a = a_in;
+  a.err = p->err_d;
+  a.ex = p->eax[0];
+  a.ey = p->eax[1];
+  a.ez = p->eax[2];
   const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
   const int nin = rot ? 6 : 3, nout = rot ? 3 : 6;
-  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, p->err_d, p->st)); }
   { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, nin, p->twy, p->st)); }
-  { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->err_d, p->st)); }
   { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, nout, p->twy, p->st)); }
   { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, fwd_x, g, rot, mode, p->P, a, p->twx, p->st)); }
   return TS_OK;
@@ -412,10 +454,17 @@ extern "C" {
 int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   if (!p || !u_hat || nsteps < 0) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
-  return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
+  // a bounded device wait that gave up in an earlier call (read without a sync)
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
+    return TS_ERR_TIMEOUT;
+  }
+  int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
     for (int s = 0; s < nsteps; ++s) CKS(step_fff(p, U));
     return (int)TS_OK;
   });
+  if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return rc;
 }
 
 int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {

@@ -88,13 +88,24 @@ __host__ __device__ constexpr int ns_at(int L, int E, int p) {
   return p == 0 ? 1 : radix_at(L, E, p - 1) * ns_at(L, E, p - 1);
 }
 
+// Radix schedule, optionally reversed (REV): running a transform with the
+// reversed schedule makes its input order equal to the output order of the
+// forward schedule and vice versa, so an inverse FFT (forward schedule) can feed
+// a forward FFT (reversed schedule) straight from registers.
+__host__ __device__ constexpr int radix_sched(int L, int E, int p, bool rev) {
+  return rev ? radix_at(L, E, npasses(L, E) - 1 - p) : radix_at(L, E, p);
+}
+__host__ __device__ constexpr int ns_sched(int L, int E, int p, bool rev) {
+  return p == 0 ? 1 : radix_sched(L, E, p - 1, rev) * ns_sched(L, E, p - 1, rev);
+}
+
 // Element held in register slot s after pass p: butterfly q = s / R, input/output r = s % R.
 // Thread t of a line owns butterflies j = t*(E/R) + q.
 // Input row  of slot (q,r) for pass p: j + r*(L/R).
 // Output row of slot (q,r) for pass p: (j/Ns)*Ns*R + (j%Ns) + r*Ns.
-template <int L, int E, int P> struct Pass {
-  static constexpr int R = radix_at(L, E, P);
-  static constexpr int NS = ns_at(L, E, P);
+template <int L, int E, int P, bool REV = false> struct Pass {
+  static constexpr int R = radix_sched(L, E, P, REV);
+  static constexpr int NS = ns_sched(L, E, P, REV);
   static constexpr int B = E / R;  // butterflies per thread
   static __device__ __forceinline__ int in_row(int t, int s) {
     const int j = t * B + s / R;
@@ -107,16 +118,18 @@ template <int L, int E, int P> struct Pass {
 };
 
 // Row of register slot s at load time (first pass input) and after the last pass.
-template <int L, int E> __device__ __forceinline__ int load_row(int t, int s) { return Pass<L, E, 0>::in_row(t, s); }
-template <int L, int E> __device__ __forceinline__ int final_row(int t, int s) {
-  return Pass<L, E, npasses(L, E) - 1>::out_row(t, s);
+template <int L, int E, bool REV = false> __device__ __forceinline__ int load_row(int t, int s) {
+  return Pass<L, E, 0, REV>::in_row(t, s);
+}
+template <int L, int E, bool REV = false> __device__ __forceinline__ int final_row(int t, int s) {
+  return Pass<L, E, npasses(L, E) - 1, REV>::out_row(t, s);
 }
 
 // Butterflies of pass P on the registers (twiddle then DFT_R).  tw: table of
 // Ltab entries exp(-2 pi i m / Ltab), Ltab = L * tws (tws = table stride).
-template <int L, int E, int P, int DIR, typename V>
+template <int L, int E, int P, int DIR, bool REV = false, typename V>
 __device__ __forceinline__ void pass_compute(V* v, int t, const V* __restrict__ tw, int tws) {
-  typedef Pass<L, E, P> PP;
+  typedef Pass<L, E, P, REV> PP;
   constexpr int R = PP::R, NS = PP::NS;
 #pragma unroll
   for (int q = 0; q < PP::B; ++q) {
@@ -135,26 +148,26 @@ __device__ __forceinline__ void pass_compute(V* v, int t, const V* __restrict__ 
   }
 }
 
+// padded shared-memory row index: one spare slot every 16 complex values keeps
+// the threads of a line (consecutive rows E apart) on distinct banks
+template <bool PAD> __device__ __forceinline__ int prow(int r) { return PAD ? r + (r >> 4) : r; }
+
 // Full FFT of one line whose E-element slice per thread is in registers (loaded
 // in load_row order); the line's L elements are exchanged through shared memory
 // `sm` addressed as sm[row*rs + cs] (caller supplies the per-thread column
 // offset cs and the row stride rs).  All threads of the block must call it.
 // On return v[s] holds output row final_row(t, s).
-// padded shared-memory row index: one spare slot every 16 complex values keeps
-// the threads of a line (consecutive rows E apart) on distinct banks
-template <bool PAD> __device__ __forceinline__ int prow(int r) { return PAD ? r + (r >> 4) : r; }
-
-template <int L, int E, int DIR, int P = 0, bool PAD = false, typename V>
+template <int L, int E, int DIR, int P = 0, bool PAD = false, bool REV = false, typename V>
 __device__ __forceinline__ void fft_regs(V* v, int t, V* sm, int rs, int cs, const V* __restrict__ tw, int tws) {
-  pass_compute<L, E, P, DIR>(v, t, tw, tws);
+  pass_compute<L, E, P, DIR, REV>(v, t, tw, tws);
   if constexpr (P + 1 < npasses(L, E)) {
 #pragma unroll
-    for (int s = 0; s < E; ++s) sm[prow<PAD>(Pass<L, E, P>::out_row(t, s)) * rs + cs] = v[s];
+    for (int s = 0; s < E; ++s) sm[prow<PAD>(Pass<L, E, P, REV>::out_row(t, s)) * rs + cs] = v[s];
     __syncthreads();
 #pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = sm[prow<PAD>(Pass<L, E, P + 1>::in_row(t, s)) * rs + cs];
+    for (int s = 0; s < E; ++s) v[s] = sm[prow<PAD>(Pass<L, E, P + 1, REV>::in_row(t, s)) * rs + cs];
     __syncthreads();
-    fft_regs<L, E, DIR, P + 1, PAD>(v, t, sm, rs, cs, tw, tws);
+    fft_regs<L, E, DIR, P + 1, PAD, REV>(v, t, sm, rs, cs, tw, tws);
   }
 }
 
@@ -196,6 +209,18 @@ __device__ V* fft_smem_lines(V* src, V* dst, int nlines, int ld, const V* __rest
   if constexpr (P + 1 < npasses(L, E)) return fft_smem_lines<L, E, DIR, P + 1>(dst, src, nlines, ld, tw, tws);
   else return dst;
 }
+
+// ---------------------------------------------------------------------------
+// asynchronous global -> shared copies (cp.async): each thread stages the
+// elements it will read itself, so a per-thread wait_group is enough.
+// ---------------------------------------------------------------------------
+template <typename V> __device__ __forceinline__ void cp_async(V* dst, const V* src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(V) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+  else asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // ---------------------------------------------------------------------------
 // Index maps

@@ -13,6 +13,7 @@
 //            + the IF-RK4 stage update (or a flux reduction / plain N output)
 #pragma once
 #include "ts_common.cuh"
+#include "ts_tma.cuh"
 
 namespace ts {
 
@@ -26,25 +27,61 @@ struct Geo {
 
 // ---------------------------------------------------------------------------
 // plain strided-axis FFT (x or y axis) over nf fields, in place
-// element (o, row, col) at o*ostride + row*rstride + col, col < inner
+// element (o, row, col) at o*ostride + row*rstride + col, col < inner.
+// Persistent and double-buffered: block b walks the work items
+// w = b, b + G, ... (w -> field, column tile, outer index); while item w is
+// transformed (registers + exchange tile) the tile of its next item streams
+// into the other staging tile with cp.async.
+// Shared memory: 2 staging tiles + 1 exchange tile of L x CW complex.
 // ---------------------------------------------------------------------------
 template <typename T, int L, int E, int CW, int DIR>
-__global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1) k_strided_fft(C<T>* __restrict__ data, int nf, long long fstride,
-                                                               int inner, long long rstride, long long ostride,
-                                                               const C<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
+    k_strided_fft(C<T>* __restrict__ data, int nf, long long fstride, int inner, long long rstride,
+                  long long ostride, int nouter, const C<T>* __restrict__ tw) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
-  V* sm = reinterpret_cast<V*>(smraw);
+  V* stage = reinterpret_cast<V*>(smraw);
+  V* xch = stage + 2 * L * CW;
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
-  const int col = blockIdx.x * CW + c;
-  const bool ok = col < inner;
-  const long long base = (long long)blockIdx.y * ostride + (ok ? col : 0);
-  for (int f = 0; f < nf; ++f) {
-    V* d = data + f * fstride + base;
-    V v[E];
+  const int ntx = (inner + CW - 1) / CW;
+  const long long nwork = (long long)nf * ntx * nouter;
+  // work item -> (pointer of its column, column valid)
+  auto locate = [&](long long w, bool& ok) -> V* {
+    const int f = (int)(w % nf);
+    const long long r = w / nf;
+    const int tx = (int)(r % ntx);
+    const long long o = r / ntx;
+    const int col = tx * CW + c;
+    ok = col < inner;
+    return data + f * fstride + o * ostride + (ok ? col : 0);
+  };
+  auto issue = [&](long long w, int buf) {
+    if (w < nwork) {
+      bool ok;
+      const V* d = locate(w, ok);
+      if (ok) {
+        V* st = stage + buf * L * CW + c;
 #pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = ok ? d[load_row<L, E>(t, s) * rstride] : mk<V>(0, 0);
-    fft_regs<L, E, DIR>(v, t, sm, CW, c, tw, 1);
+        for (int s = 0; s < E; ++s) {
+          const int r = load_row<L, E>(t, s);
+          cp_async(st + r * CW, d + r * rstride);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  int buf = 0;
+  issue(blockIdx.x, 0);
+  for (long long w = blockIdx.x; w < nwork; w += gridDim.x, buf ^= 1) {
+    issue(w + gridDim.x, buf ^ 1);
+    cp_async_wait<1>();
+    bool ok;
+    V* d = locate(w, ok);
+    V v[E];
+    const V* st = stage + buf * L * CW + c;
+#pragma unroll
+    for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
+    fft_regs<L, E, DIR>(v, t, xch, CW, c, tw, 1);
     if (ok) {
 #pragma unroll
       for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
@@ -55,10 +92,104 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1) k
 // ---------------------------------------------------------------------------
 // inverse x pass: W_i = IFFT_x(D(U_i)); rotational form also W_{3+i} = IFFT_x(D(omega_i)),
 // omega = i K x D(U).  col = ly*Hz + lz; row = lx.
+// Persistent over column tiles.  Thread 0 streams the three components of a
+// tile into shared memory with TMA (2-D boxes of CW columns x <=256 rows,
+// mbarrier completion), double buffered so tile k+1 loads while tile k is
+// transformed.  Shared memory: 2 x 3 staging tiles + 1 exchange tile.
 // ---------------------------------------------------------------------------
 template <typename T, int L, int E, int CW, bool ROT>
-__global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1) k_inv_x(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g,
-                                                         const C<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(CW * (L / E), 1)
+    k_inv_x(const __grid_constant__ CUtensorMap mU, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw,
+            int* err) {
+  typedef C<T> V;
+  constexpr int TILE = L * CW, BR = L < 256 ? L : 256, UNITS = (int)sizeof(V) / 8;
+  extern __shared__ __align__(128) unsigned char smraw_[];
+  // TMA destinations: 128-byte aligned (the launcher adds 128 bytes of slack)
+  unsigned char* smraw = smraw_ + ((128 - (smem_u32(smraw_) & 127)) & 127);
+  V* stage = reinterpret_cast<V*>(smraw);  // [2][3][TILE]
+  V* xch = stage + 6 * TILE;
+  __shared__ __align__(8) uint64_t bar[2];
+  const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+  const int inner = g.Ny * g.Hz;
+  const int ntiles = (inner + CW - 1) / CW;
+  const long long rstride = inner;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int tile, int slot) {
+    if (tile >= ntiles) return;
+    mbar_expect_tx(&bar[slot], 3u * TILE * (unsigned)sizeof(V));
+    for (int comp = 0; comp < 3; ++comp)
+      for (int r0 = 0; r0 < L; r0 += BR)
+        tma_load_2d(stage + (slot * 3 + comp) * TILE + r0 * CW, &mU, tile * CW * UNITS, comp * g.Nx + r0, &bar[slot]);
+  };
+  if (threadIdx.x == 0) {
+    issue(blockIdx.x, 0);
+    issue(blockIdx.x + gridDim.x, 1);
+  }
+  uint32_t ph[2] = {0, 0};
+  const int nout = ROT ? 6 : 3;
+  int k = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+    const int slot = k & 1;
+    const bool got = mbar_wait(&bar[slot], ph[slot], err);
+    if (__syncthreads_or(!got)) {
+      // give the copies in flight a second bounded chance to land, then leave
+      if (threadIdx.x == 0) mbar_wait(&bar[slot], ph[slot], nullptr);
+      return;
+    }
+    ph[slot] ^= 1;
+    const int col = tile * CW + c;
+    const bool ok = col < inner;
+    const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
+    const T Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
+    const V* st = stage + slot * 3 * TILE + c;
+    for (int f = 0; f < nout; ++f) {
+      V v[E];
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int lx = load_row<L, E>(t, s);
+        V a = mk<V>(0, 0);
+        if (ok && !dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) {
+          if (f < 3) {
+            a = st[f * TILE + lx * CW];
+          } else {
+            // omega_i = i (K_{i+1} U_{i+2} - K_{i+2} U_{i+1})  (indices mod 3)
+            const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
+            const int i = f - 3, i1 = i == 2 ? 0 : i + 1, i2 = i == 0 ? 2 : i - 1;
+            const T Ka = i1 == 0 ? Kx : (i1 == 1 ? Ky : Kz);
+            const T Kb = i2 == 0 ? Kx : (i2 == 1 ? Ky : Kz);
+            const V ub = st[i2 * TILE + lx * CW], ua = st[i1 * TILE + lx * CW];
+            a = mul_i<1>(sub(scale(ub, Ka), scale(ua, Kb)));
+          }
+        }
+        v[s] = a;
+      }
+      if (f == nout - 1) {
+        // every thread has read this slot: refill it with the tile after next
+        __syncthreads();
+        if (threadIdx.x == 0) issue(tile + 2 * gridDim.x, slot);
+      }
+      fft_regs<L, E, 1>(v, t, xch, CW, c, tw, 1);
+      if (ok) {
+        V* d = W + f * g.S + col;
+#pragma unroll
+        for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// inverse x pass, direct-load variant (one column tile per block, loads straight
+// into registers; two blocks of 256 threads per SM).  Same result as k_inv_x.
+// ---------------------------------------------------------------------------
+template <typename T, int L, int E, int CW, bool ROT>
+__global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
+    k_inv_x_ld(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
@@ -100,6 +231,7 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1) k
     }
   }
 }
+
 
 // ---------------------------------------------------------------------------
 // z pass: C2R of the NIN input lines, real-space products, R2C of the NOUT
@@ -198,6 +330,225 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 }
 
 // ---------------------------------------------------------------------------
+// z pass, register-resident variant (M = Nz/2 <= 256): one line per group of
+// TPL = M/8 consecutive lanes, 8 elements per thread.  The inverse transform
+// (forward radix schedule) leaves every component's real line in registers in
+// the order the forward transform with the reversed schedule expects, so the
+// products are formed in registers and fed straight to the forward FFTs.  The
+// real-transform pair terms X[M-k] come from the partner lane by a warp
+// shuffle; shared memory holds only one exchange line per line group.
+// ---------------------------------------------------------------------------
+// threads per block of k_z_reg: up to six components live in registers, so it
+// runs 128-thread blocks with a 170-register budget (FP32 only; FP64 would spill
+// and uses the shared-memory-slot kernel k_z_fused instead)
+template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 128; }
+
+template <typename T, int NZ, int FORM>
+__global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
+    k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw) {
+  typedef C<T> V;
+  constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
+  static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
+  constexpr int NIN = FORM == 0 ? 3 : 6, NOUT = FORM == 0 ? 6 : 3;
+  constexpr int LPB = zreg_threads<FORM>() / TPL;
+  __shared__ __align__(16) V xch_all[LPB * LDX];
+  const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const int lane = threadIdx.x & 31;
+  const int partner = (lane - t) + (TPL - t) % TPL;  // lane holding row M - k
+  const long long nlines = (long long)g.Nx * g.Ny;
+  const long long line = (long long)blockIdx.x * LPB + l;
+  const bool live = line < nlines;
+  V* xch = xch_all + l * LDX;
+
+  V in[NIN][E];
+#pragma unroll
+  for (int c = 0; c < NIN; ++c) {
+    const V* X = P + c * g.S + (live ? line : 0) * H;
+    V a[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) a[s] = live ? X[t + s * TPL] : mk<V>(0, 0);
+    const V XM = (live && t == 0) ? X[M] : mk<V>(0, 0);
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
+      V b;
+      b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
+      b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
+      if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
+      b = conjg(b);
+      V x = a[s];
+      const int k = t + s * TPL;
+      if (k == 0) { x.y = 0; b.y = 0; }
+      in[c][s] = add(add(x, b), mul_i<1>(mul(conjg(tw[k]), sub(x, b))));
+    }
+    fft_regs<M, E, 1, 0, true, false>(in[c], t, xch, 1, 0, tw, 2);
+  }
+  // real-space products; each complex register holds two real points
+  if (FORM == 1) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const V u1 = in[0][s], u2 = in[1][s], u3 = in[2][s], w1 = in[3][s], w2 = in[4][s], w3 = in[5][s];
+      in[0][s] = mk<V>(u2.x * w3.x - u3.x * w2.x, u2.y * w3.y - u3.y * w2.y);
+      in[1][s] = mk<V>(u3.x * w1.x - u1.x * w3.x, u3.y * w1.y - u1.y * w3.y);
+      in[2][s] = mk<V>(u1.x * w2.x - u2.x * w1.x, u1.y * w2.y - u2.y * w1.y);
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < NOUT; ++f) {
+    V p[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      if (FORM == 1) {
+        p[s] = in[f][s];
+      } else {
+        const int a = f < 3 ? f : f - 3, b = f < 3 ? f : (f == 5 ? 0 : f - 2);
+        p[s] = mk<V>(in[a][s].x * in[b][s].x, in[a][s].y * in[b][s].y);
+      }
+    }
+    fft_regs<M, E, -1, 0, true, true>(p, t, xch, 1, 0, tw, 2);
+    // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL
+    V* Xo = P + f * g.S + (live ? line : 0) * H;
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      V zp;
+      zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
+      zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
+      if (t == 0) zp = p[(E - s) % E];
+      zp = conjg(zp);
+      const int k = t + s * TPL;
+      const V z = p[s];
+      const V o = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[k], scale(sub(z, zp), (T)0.5))));
+      if (live) Xo[k] = o;
+    }
+    if (live && t == 0) {
+      const V z = p[0], zp = conjg(p[0]);
+      Xo[M] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zp), (T)0.5))));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass, bulk-copy variant: persistent over groups of LPB consecutive (x,y)
+// lines.  A group's input lines are contiguous per component (LPB*H complex,
+// 16-byte aligned), so thread 0 fetches each component with one 1-D
+// cp.async.bulk into shared memory, double buffered across groups.  Each line
+// is transformed by TPL = M/E lanes in registers (pair terms X[M-k] read from
+// shared memory on the way in, exchanged by warp shuffles on the way out); the
+// products are formed in registers and fed to the forward FFTs with the
+// reversed radix schedule.  Shared memory: 2 x NIN x LPB x H input + LPB
+// exchange lines.
+// ---------------------------------------------------------------------------
+template <typename T> __host__ __device__ constexpr int ztma_e() { return sizeof(T) == 4 ? 8 : 4; }
+template <typename T, int NZ> __host__ __device__ constexpr int ztma_lpb() { return 256 / ((NZ / 2) / ztma_e<T>()); }
+
+template <typename T, int NZ, int FORM>
+__global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw,
+                                                  int* err) {
+  typedef C<T> V;
+  constexpr int M = NZ / 2, H = M + 1, E = ztma_e<T>(), TPL = M / E, LDX = zslot<M>();
+  constexpr int LPB = ztma_lpb<T, NZ>();
+  static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
+  constexpr int NIN = FORM == 0 ? 3 : 6, NOUT = FORM == 0 ? 6 : 3;
+  constexpr int GRP = LPB * H;  // complex per component per group
+  extern __shared__ __align__(128) unsigned char smraw_[];
+  unsigned char* smraw = smraw_ + ((128 - (smem_u32(smraw_) & 127)) & 127);
+  V* inb = reinterpret_cast<V*>(smraw);  // [2][NIN][GRP]
+  V* xch_all = inb + 2 * NIN * GRP;      // [LPB][LDX]
+  __shared__ __align__(8) uint64_t bar[2];
+  const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const int lane = threadIdx.x & 31;
+  const int partner = (lane - t) + (TPL - t) % TPL;  // lane holding row M - k
+  const long long ngroups = (long long)g.Nx * g.Ny / LPB;
+  V* xch = xch_all + l * LDX;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](long long grp, int slot) {
+    if (grp >= ngroups) return;
+    mbar_expect_tx(&bar[slot], (unsigned)(NIN * GRP * sizeof(V)));
+    for (int c = 0; c < NIN; ++c)
+      bulk_load(inb + (slot * NIN + c) * GRP, P + c * g.S + grp * GRP, (unsigned)(GRP * sizeof(V)), &bar[slot]);
+  };
+  if (threadIdx.x == 0) {
+    issue(blockIdx.x, 0);
+    issue(blockIdx.x + gridDim.x, 1);
+  }
+  uint32_t ph[2] = {0, 0};
+  int k = 0;
+  for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x, ++k) {
+    const int slot = k & 1;
+    const bool got = mbar_wait(&bar[slot], ph[slot], err);
+    if (__syncthreads_or(!got)) {
+      if (threadIdx.x == 0) mbar_wait(&bar[slot], ph[slot], nullptr);
+      return;
+    }
+    ph[slot] ^= 1;
+    V in[NIN][E];
+#pragma unroll
+    for (int c = 0; c < NIN; ++c) {
+      const V* X = inb + (slot * NIN + c) * GRP + l * H;
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
+        const int kk = t + s * TPL;
+        V x = X[kk], b = conjg(X[M - kk]);
+        if (kk == 0) { x.y = 0; b.y = 0; }
+        in[c][s] = add(add(x, b), mul_i<1>(mul(conjg(tw[kk]), sub(x, b))));
+      }
+    }
+    // every thread has read this slot: refill it with the group after next
+    __syncthreads();
+    if (threadIdx.x == 0) issue(grp + 2 * (long long)gridDim.x, slot);
+#pragma unroll
+    for (int c = 0; c < NIN; ++c) fft_regs<M, E, 1, 0, true, false>(in[c], t, xch, 1, 0, tw, 2);
+    if (FORM == 1) {
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const V u1 = in[0][s], u2 = in[1][s], u3 = in[2][s], w1 = in[3][s], w2 = in[4][s], w3 = in[5][s];
+        in[0][s] = mk<V>(u2.x * w3.x - u3.x * w2.x, u2.y * w3.y - u3.y * w2.y);
+        in[1][s] = mk<V>(u3.x * w1.x - u1.x * w3.x, u3.y * w1.y - u1.y * w3.y);
+        in[2][s] = mk<V>(u1.x * w2.x - u2.x * w1.x, u1.y * w2.y - u2.y * w1.y);
+      }
+    }
+    const long long line = grp * LPB + l;
+#pragma unroll
+    for (int f = 0; f < NOUT; ++f) {
+      V p[E];
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        if (FORM == 1) {
+          p[s] = in[f][s];
+        } else {
+          const int a = f < 3 ? f : f - 3, b = f < 3 ? f : (f == 5 ? 0 : f - 2);
+          p[s] = mk<V>(in[a][s].x * in[b][s].x, in[a][s].y * in[b][s].y);
+        }
+      }
+      fft_regs<M, E, -1, 0, true, true>(p, t, xch, 1, 0, tw, 2);
+      // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL
+      V* Xo = P + f * g.S + line * H;
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        V zp;
+        zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
+        zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
+        if (t == 0) zp = p[(E - s) % E];
+        zp = conjg(zp);
+        const int kk = t + s * TPL;
+        const V z = p[s];
+        Xo[kk] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[kk], scale(sub(z, zp), (T)0.5))));
+      }
+      if (t == 0) {
+        const V z = p[0], zp = conjg(p[0]);
+        Xo[M] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zp), (T)0.5))));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // forward x pass + spectral epilogue
 // ---------------------------------------------------------------------------
 struct StageArgs {
@@ -214,149 +565,215 @@ struct StageArgs {
   double nu, dt;
   int stage;         // 1..4
   int reality;       // zero the kz = Nz/2 plane at the end of stage 4
+  int* err;          // set to 1 when a bounded wait gives up
+  const double* ex;  // per-axis integrating factors exp(-nu dt K_i^2 / 2), FP64
+  const double* ey;
+  const double* ez;
 };
 
 enum { MODE_STEP = 0, MODE_FLUX = 1, MODE_NLIN = 2 };
 
+// Persistent over column tiles.  Thread 0 streams the product fields of a tile
+// through two TMA staging tiles (item = (tile, field); item i+2 is issued as
+// soon as every thread has read item i), and the RK state the epilogue needs
+// (U0 and tot, or the flux field) into six state tiles at tile start.
+// Shared memory: 2 product tiles + 1 exchange tile + 6 state tiles (+ flux bins).
 template <typename T, int L, int E, int CW, int FORM, int MODE>
-__global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1) k_fwd_x(const C<T>* __restrict__ P, Geo g, StageArgs a,
-                                                         const C<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(CW * (L / E), 1)
+    k_fwd_x(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mA,
+            const __grid_constant__ CUtensorMap mB, Geo g, StageArgs a, const C<T>* __restrict__ tw) {
   typedef C<T> V;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  V* sm = reinterpret_cast<V*>(smraw);
-  double* sbins = reinterpret_cast<double*>(smraw + (size_t)L * CW * sizeof(V));
+  constexpr int NF = FORM == 0 ? 6 : 3;
+  constexpr int TILE = L * CW, BR = L < 256 ? L : 256, UNITS = (int)sizeof(V) / 8;
+  constexpr int NST = MODE == MODE_NLIN ? 0 : 6;
+  extern __shared__ __align__(128) unsigned char smraw_[];
+  // TMA destinations: 128-byte aligned (the launcher adds 128 bytes of slack)
+  unsigned char* smraw = smraw_ + ((128 - (smem_u32(smraw_) & 127)) & 127);
+  V* pst = reinterpret_cast<V*>(smraw);
+  V* xch = pst + 2 * TILE;
+  V* sst = xch + TILE;
+  double* sbins = reinterpret_cast<double*>(sst + NST * TILE);
+  __shared__ __align__(8) uint64_t bar[3];  // product slots 0, 1; state
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int inner = g.Ny * g.Hz;
-  const int col = blockIdx.x * CW + c;
-  const bool ok = col < inner;
-  const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
-  const int ky = kfft(ly, g.Ny);
-  const double Kyd = ky * g.kf[1], Kzd = lz * g.kf[2];
-  const T Ky = (T)Kyd, Kz = (T)Kzd;
+  const int ntiles = (inner + CW - 1) / CW;
   const long long rstride = inner;
   const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
-  constexpr int NF = FORM == 0 ? 6 : 3;
+  // state tiles: [0,3) = U0 (or the flux field) from map mA, [3,6) = tot from map mB
+  const int nstate = MODE == MODE_FLUX ? 3 : (MODE == MODE_STEP ? (a.stage == 1 ? 3 : 6) : 0);
 
-  V acc[3][E];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int s = 0; s < E; ++s) acc[i][s] = mk<V>(0, 0);
-
-  for (int f = 0; f < NF; ++f) {
-    V v[E];
-    const V* d = P + f * g.S + (ok ? col : 0);
-#pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = ok ? d[load_row<L, E>(t, s) * rstride] : mk<V>(0, 0);
-    fft_regs<L, E, -1>(v, t, sm, CW, c, tw, 1);
-#pragma unroll
-    for (int s = 0; s < E; ++s) {
-      const int lx = final_row<L, E>(t, s);
-      const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
-      const V p = scale(v[s], inv);
-      if (FORM == 0) {
-        // N_i = sum_j i K_j F[u_i u_j]  (compute_diag_offdiag.cc:47-98)
-        switch (f) {
-          case 0: acc[0][s] = add(acc[0][s], ik(Kx, p)); break;
-          case 1: acc[1][s] = add(acc[1][s], ik(Ky, p)); break;
-          case 2: acc[2][s] = add(acc[2][s], ik(Kz, p)); break;
-          case 3: acc[0][s] = add(acc[0][s], ik(Ky, p)); acc[1][s] = add(acc[1][s], ik(Kx, p)); break;
-          case 4: acc[1][s] = add(acc[1][s], ik(Kz, p)); acc[2][s] = add(acc[2][s], ik(Ky, p)); break;
-          default: acc[2][s] = add(acc[2][s], ik(Kx, p)); acc[0][s] = add(acc[0][s], ik(Kz, p)); break;
-        }
-      } else {
-        // N = -F[u x omega]
-        if (f == 0) acc[0][s] = scale(p, (T)-1);
-        else if (f == 1) acc[1][s] = scale(p, (T)-1);
-        else acc[2][s] = scale(p, (T)-1);
-      }
-    }
-  }
-
-  if (MODE == MODE_FLUX) {
+  if (MODE == MODE_FLUX)
     for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x) sbins[i] = 0.0;
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
+    fence_mbar_init();
   }
+  __syncthreads();
+  const long long nitems = (long long)NF * ((ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x);
+  auto issue_item = [&](long long i) {
+    if (i >= nitems) return;
+    const int tile = blockIdx.x + (int)(i / NF) * gridDim.x, f = (int)(i % NF), slot = (int)(i & 1);
+    mbar_expect_tx(&bar[slot], (unsigned)TILE * (unsigned)sizeof(V));
+    for (int r0 = 0; r0 < L; r0 += BR)
+      tma_load_2d(pst + slot * TILE + r0 * CW, &mP, tile * CW * UNITS, f * g.Nx + r0, &bar[slot]);
+  };
+  auto issue_state = [&](int tile) {
+    if (nstate == 0) return;
+    mbar_expect_tx(&bar[2], (unsigned)nstate * TILE * (unsigned)sizeof(V));
+    for (int comp = 0; comp < nstate; ++comp)
+      for (int r0 = 0; r0 < L; r0 += BR)
+        tma_load_2d(sst + comp * TILE + r0 * CW, comp < 3 ? &mA : &mB, tile * CW * UNITS, (comp % 3) * g.Nx + r0,
+                    &bar[2]);
+  };
+  if (threadIdx.x == 0) {
+    issue_item(0);
+    issue_item(1);
+  }
+  uint32_t ph[3] = {0, 0, 0};
+  long long item = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    if (threadIdx.x == 0) issue_state(tile);
+    const int col = tile * CW + c;
+    const bool ok = col < inner;
+    const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
+    const int ky = kfft(ly, g.Ny);
+    const double Kyd = ky * g.kf[1], Kzd = lz * g.kf[2];
+    const T Ky = (T)Kyd, Kz = (T)Kzd;
 
-  if (ok) {
+    V acc[3][E];
 #pragma unroll
-    for (int s = 0; s < E; ++s) {
-      const int lx = final_row<L, E>(t, s);
-      const long long off = lx * rstride + col;
-      const int kx = kfft(lx, g.Nx);
-      const double Kxd = kx * g.kf[0];
-      V N1 = acc[0][s], N2 = acc[1][s], N3 = acc[2][s];
-      if (MODE == MODE_NLIN) {
-        V* no = reinterpret_cast<V*>(a.nout);
-        no[off] = N1; no[g.S + off] = N2; no[2 * g.S + off] = N3;
-        continue;
-      }
-      if (MODE == MODE_FLUX) {
-        // contribution 2 mult Re(N . conj(D(U))) to the first sphere with |K| <= R
-        const V* Ud = reinterpret_cast<const V*>(a.Ud);
-        if (dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) continue;
-        const V u1 = Ud[off], u2 = Ud[g.S + off], u3 = Ud[2 * g.S + off];
-        double re = (double)N1.x * u1.x + (double)N1.y * u1.y + (double)N2.x * u2.x + (double)N2.y * u2.y +
-                    (double)N3.x * u3.x + (double)N3.y * u3.y;
-        double mult = lz > 0 ? 1.0 : 0.5;
-        if (kx == g.Nx / 2 || (ky == g.Ny / 2 && g.Ny > 1)) mult *= 2;
-        const double Kmag = sqrt((Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd);
-        int b = 0;
-        while (b < a.nradii && Kmag > a.radii[b]) ++b;
-        atomicAdd(&sbins[b], 2.0 * mult * re);
-        continue;
-      }
-      // ---- MODE_STEP ----
-      const T Kx = (T)Kxd;
-      if (a.fcube) {
-        const int km = a.fkm;
-        if (abs(kx) <= km && abs(ky) <= km && lz <= km) {
-          const V* fc = reinterpret_cast<const V*>(a.fcube);
-          const int n = 2 * km + 1;
-          const long long fo = ((long long)(kx + km) * n + (ky + km)) * (km + 1) + lz;
-          const long long fs = (long long)n * n * (km + 1);
-          N1 = sub(N1, fc[fo]); N2 = sub(N2, fc[fs + fo]); N3 = sub(N3, fc[2 * fs + fo]);  // Add_force
-        }
-      }
-      // Leray projection: p = (i K . N)/K^2, p(0)=0; N <- -(N + i K p)
-      const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
-      V div = add(add(ik(Kx, N1), ik(Ky, N2)), ik(Kz, N3));
-      const V p = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
-      V R1 = scale(add(N1, ik(Kx, p)), (T)-1);
-      V R2 = scale(add(N2, ik(Ky, p)), (T)-1);
-      V R3 = scale(add(N3, ik(Kz, p)), (T)-1);
-      // IF-RK4 stage update (RK.cc:91-170 with Single_time_step / Compute_RK4_parts)
-      const double eh = exp(-a.nu * 0.5 * a.dt * K2);
-      const double e1 = exp(-a.nu * 1.0 * a.dt * K2);
-      const T Eh = (T)eh, E1 = (T)e1;
-      V* U0 = reinterpret_cast<V*>(a.U0);
-      V* Uc = reinterpret_cast<V*>(a.Ucur);
-      V* tot = reinterpret_cast<V*>(a.tot);
-      const V Rv[3] = {R1, R2, R3};
-      const T dt = (T)a.dt;
-      const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const long long o = i * g.S + off;
-        const V R = Rv[i];
-        if (a.stage == 1) {
-          V u0 = dz ? mk<V>(0, 0) : U0[o];
-          Uc[o] = scale(add(u0, scale(R, (T)(0.5 * a.dt))), Eh);
-          tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
-        } else if (a.stage == 2) {
-          Uc[o] = add(scale(U0[o], Eh), scale(R, (T)(0.5 * a.dt)));
-          tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
-        } else if (a.stage == 3) {
-          Uc[o] = scale(add(scale(U0[o], Eh), scale(R, dt)), Eh);
-          tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      for (int s = 0; s < E; ++s) acc[i][s] = mk<V>(0, 0);
+
+    for (int f = 0; f < NF; ++f, ++item) {
+      const int slot = (int)(item & 1);
+      const bool got = mbar_wait(&bar[slot], ph[slot], a.err);
+      if (__syncthreads_or(!got)) {
+        if (threadIdx.x == 0) mbar_wait(&bar[slot], ph[slot], nullptr);
+        return;
+      }
+      ph[slot] ^= 1;
+      V v[E];
+      const V* st = pst + slot * TILE + c;
+#pragma unroll
+      for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
+      __syncthreads();
+      if (threadIdx.x == 0) issue_item(item + 2);
+      fft_regs<L, E, -1>(v, t, xch, CW, c, tw, 1);
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int lx = final_row<L, E>(t, s);
+        const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
+        const V p = scale(v[s], inv);
+        if (FORM == 0) {
+          // N_i = sum_j i K_j F[u_i u_j]  (compute_diag_offdiag.cc:47-98)
+          switch (f) {
+            case 0: acc[0][s] = add(acc[0][s], ik(Kx, p)); break;
+            case 1: acc[1][s] = add(acc[1][s], ik(Ky, p)); break;
+            case 2: acc[2][s] = add(acc[2][s], ik(Kz, p)); break;
+            case 3: acc[0][s] = add(acc[0][s], ik(Ky, p)); acc[1][s] = add(acc[1][s], ik(Kx, p)); break;
+            case 4: acc[1][s] = add(acc[1][s], ik(Kz, p)); acc[2][s] = add(acc[2][s], ik(Ky, p)); break;
+            default: acc[2][s] = add(acc[2][s], ik(Kx, p)); acc[0][s] = add(acc[0][s], ik(Kz, p)); break;
+          }
         } else {
-          V tt = add(tot[o], scale(R, (T)((1.0 / 6) * a.dt)));
-          V un = add(scale(U0[o], E1), tt);
-          if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
-          U0[o] = un;
+          // N = -F[u x omega]
+          if (f == 0) acc[0][s] = scale(p, (T)-1);
+          else if (f == 1) acc[1][s] = scale(p, (T)-1);
+          else acc[2][s] = scale(p, (T)-1);
         }
       }
     }
+    if (nstate) {
+      const bool got = mbar_wait(&bar[2], ph[2], a.err);
+      if (__syncthreads_or(!got)) {
+        if (threadIdx.x == 0) mbar_wait(&bar[2], ph[2], nullptr);
+        return;
+      }
+      ph[2] ^= 1;
+    }
+    if (ok) {
+      const double exy = MODE == MODE_STEP ? a.ey[ly] * a.ez[lz] : 0.0;
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int lx = final_row<L, E>(t, s);
+        const long long off = lx * rstride + col;
+        const int so = lx * CW + c;
+        const int kx = kfft(lx, g.Nx);
+        const double Kxd = kx * g.kf[0];
+        V N1 = acc[0][s], N2 = acc[1][s], N3 = acc[2][s];
+        if (MODE == MODE_NLIN) {
+          V* no = reinterpret_cast<V*>(a.nout);
+          no[off] = N1; no[g.S + off] = N2; no[2 * g.S + off] = N3;
+          continue;
+        }
+        if (MODE == MODE_FLUX) {
+          // contribution 2 mult Re(N . conj(D(U))) to the first sphere with |K| <= R
+          if (dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) continue;
+          const V u1 = sst[so], u2 = sst[TILE + so], u3 = sst[2 * TILE + so];
+          double re = (double)N1.x * u1.x + (double)N1.y * u1.y + (double)N2.x * u2.x + (double)N2.y * u2.y +
+                      (double)N3.x * u3.x + (double)N3.y * u3.y;
+          double mult = lz > 0 ? 1.0 : 0.5;
+          if (kx == g.Nx / 2 || (ky == g.Ny / 2 && g.Ny > 1)) mult *= 2;
+          const double Kmag = sqrt((Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd);
+          int b = 0;
+          while (b < a.nradii && Kmag > a.radii[b]) ++b;
+          atomicAdd(&sbins[b], 2.0 * mult * re);
+          continue;
+        }
+        // ---- MODE_STEP ----
+        const T Kx = (T)Kxd;
+        if (a.fcube) {
+          const int km = a.fkm;
+          if (abs(kx) <= km && abs(ky) <= km && lz <= km) {
+            const V* fc = reinterpret_cast<const V*>(a.fcube);
+            const int n = 2 * km + 1;
+            const long long fo = ((long long)(kx + km) * n + (ky + km)) * (km + 1) + lz;
+            const long long fs = (long long)n * n * (km + 1);
+            N1 = sub(N1, fc[fo]); N2 = sub(N2, fc[fs + fo]); N3 = sub(N3, fc[2 * fs + fo]);  // Add_force
+          }
+        }
+        // Leray projection: p = (i K . N)/K^2, p(0)=0; N <- -(N + i K p)
+        const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+        const V div = add(add(ik(Kx, N1), ik(Ky, N2)), ik(Kz, N3));
+        const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+        const V Rv[3] = {scale(add(N1, ik(Kx, pr)), (T)-1), scale(add(N2, ik(Ky, pr)), (T)-1),
+                         scale(add(N3, ik(Kz, pr)), (T)-1)};
+        // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
+        const double eh = a.ex[lx] * exy;
+        const double e1 = eh * eh;
+        const T Eh = (T)eh, E1 = (T)e1;
+        V* U0 = reinterpret_cast<V*>(a.U0);
+        V* Uc = reinterpret_cast<V*>(a.Ucur);
+        V* tot = reinterpret_cast<V*>(a.tot);
+        const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+        // IF-RK4 stage update (RK.cc:91-170 with Single_time_step / Compute_RK4_parts)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const long long o = i * g.S + off;
+          const V R = Rv[i];
+          const V u0 = sst[i * TILE + so];
+          if (a.stage == 1) {
+            Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+            tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+          } else {
+            const V tt = sst[(3 + i) * TILE + so];
+            if (a.stage == 2) {
+              Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+              tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+            } else if (a.stage == 3) {
+              Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+              tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+            } else {
+              const V un = add(scale(u0, E1), add(tt, scale(R, (T)((1.0 / 6) * a.dt))));
+              U0[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
+            }
+          }
+        }
+      }
+    }
+    // the next tile's state load overwrites the state tiles
+    __syncthreads();
   }
   if (MODE == MODE_FLUX) {
     __syncthreads();

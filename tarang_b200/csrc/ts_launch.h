@@ -12,9 +12,10 @@ template <typename T> struct Launch {
   // strided-axis FFT on nf fields in place: axis 0 = x (L = Nx), 1 = y (L = Ny);
   // dir -1 forward, +1 inverse; outputs scaled by `scale`
   static cudaError_t strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw, cudaStream_t st);
-  static cudaError_t inv_x(const Geo& g, int rot, const void* U, void* W, const void* tw, cudaStream_t st);
-  static cudaError_t z_fused(const Geo& g, int rot, void* P, const void* tw, cudaStream_t st);
+  static cudaError_t inv_x(const Geo& g, int rot, const void* U, void* W, const void* tw, int* err, cudaStream_t st);
+  static cudaError_t z_fused(const Geo& g, int rot, void* P, const void* tw, int* err, cudaStream_t st);
   static cudaError_t z_single(const Geo& g, int dir, const void* in, void* out, int ncomp, const void* tw, cudaStream_t st);
+  // a.U0 / a.Ud / a.tot must be 16-byte aligned (TMA)
   static cudaError_t fwd_x(const Geo& g, int rot, int mode, const void* P, const StageArgs& a, const void* tw,
                            cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
