@@ -111,6 +111,13 @@ int ts_rk4_step(ts_plan* plan, void* u_hat, int nsteps);
 /* RK4(U,T,P,F) for RBC (RK_SF.cc:97-221), SFF basis, PRLARGE/ULARGE. */
 int ts_rk4_step_rbc(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
 
+/* Temperature perturbation for RBC (SFF): amplitude amp and uniform random
+ * phases (this project's splitmix64 generator, counter = linear mode index) on
+ * the modes with grid radius |(m, ky, kz)| <= kmax and m >= 1, then the strong
+ * reality condition.  The reference's RBC ICs are read from files or set per
+ * mode (init_cond_main.cc:48-78); this is the benchmark's seeded stand-in. */
+int ts_init_temperature_perturbation(ts_plan* plan, double amp, double kmax, uint64_t seed, void* T_hat);
+
 /* CVF::Compute_total_energy (Cvf.cc:213-221): sum over ncomp components. */
 int ts_energy(ts_plan* plan, const void* a_hat, int ncomp, double* energy);
 /* Universal::Compute_shell_spectrum (universal_energy.cc:279-366), summed over

@@ -67,6 +67,7 @@ SIGNATURES = {
     "ts_max_div": (ctypes.c_int, [_P, _P, _D]),
     "ts_nusselt": (ctypes.c_int, [_P, _P, _P, _D]),
     "ts_init_energy_spectrum": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_uint64, ctypes.c_double, _P]),
+    "ts_init_temperature_perturbation": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _P]),
     "ts_profile_enable": (ctypes.c_int, [_P, ctypes.c_int]),
     "ts_profile_reset": (ctypes.c_int, [_P]),
     "ts_profile_read": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.POINTER(ctypes.c_longlong), _D]),

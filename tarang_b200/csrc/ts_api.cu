@@ -66,6 +66,8 @@ struct ts_plan {
   int* err_d = nullptr;     // device error word (bounded waits that gave up)
   int* err_h = nullptr;     // pinned copy, refreshed after every step call
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
+  double* eaxT[3] = {nullptr, nullptr, nullptr}; // per-axis exp(-kappa dt K_i^2 / 2) (SFF scalar)
+  void* twq = nullptr;      // SFF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
   // per-kernel-class CUDA event timing (ts_profile_*)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -192,7 +194,7 @@ static int ensure_stage(void** buf, size_t bytes) {
 
 // Integrating-factor tables: E(1/2)(K) = exp(-nu dt K^2 / 2) factorises over the
 // axes, exp(-nu dt/2 Kx^2) exp(-nu dt/2 Ky^2) exp(-nu dt/2 Kz^2) (FP64)
-static int upload_if_tables(ts_plan* p, double nu, double dt) {
+static int upload_if_tables(ts_plan* p, double nu, double dt, double** tab) {
   const Geo& g = p->g;
   const int n[3] = {g.Nx, g.Ny, g.Hz};
   for (int ax = 0; ax < 3; ++ax) {
@@ -205,8 +207,8 @@ static int upload_if_tables(ts_plan* p, double nu, double dt) {
       const double K = k * g.kf[ax];
       h[l] = exp(-nu * 0.5 * dt * (K * K));
     }
-    if (!p->eax[ax]) CK(cudaMalloc(&p->eax[ax], n[ax] * sizeof(double)));
-    CK(cudaMemcpy(p->eax[ax], h.data(), n[ax] * sizeof(double), cudaMemcpyHostToDevice));
+    if (!tab[ax]) CK(cudaMalloc(&tab[ax], n[ax] * sizeof(double)));
+    CK(cudaMemcpy(tab[ax], h.data(), n[ax] * sizeof(double), cudaMemcpyHostToDevice));
   }
   return TS_OK;
 }
@@ -247,8 +249,11 @@ int ts_plan_destroy(ts_plan* p) {
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
-  for (int i = 0; i < 3; ++i)
+  for (int i = 0; i < 3; ++i) {
     if (p->eax[i]) cudaFree(p->eax[i]);
+    if (p->eaxT[i]) cudaFree(p->eaxT[i]);
+  }
+  if (p->twq) cudaFree(p->twq);
   if (p->err_d) cudaFree(p->err_d);
   if (p->err_h) cudaFreeHost(p->err_h);
   delete p;
@@ -296,9 +301,17 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     CK(cudaMalloc(b, bytes));
     return TS_OK;
   };
-  CKP(alloc(&p->Ucur, 3 * g.S * p->cb));
-  CKP(alloc(&p->tot, 3 * g.S * p->cb));
-  CKP(alloc(&p->P, 6 * g.S * p->cb));
+  // SFF (Boussinesq): stage / accumulator fields carry T as a fourth component,
+  // and the z pass makes nine products
+  const int ncs = cfg->basis == TS_BASIS_SFF ? 4 : 3, nps = cfg->basis == TS_BASIS_SFF ? 9 : 6;
+  if (cfg->basis == TS_BASIS_SFF && g.Nx > 512) {
+    g_last_error = "SFF supports Nx <= 512";
+    ts_plan_destroy(p);
+    return TS_ERR_UNSUPPORTED;
+  }
+  CKP(alloc(&p->Ucur, ncs * g.S * p->cb));
+  CKP(alloc(&p->tot, ncs * g.S * p->cb));
+  CKP(alloc(&p->P, nps * g.S * p->cb));
   if (p->prec) {
     CKP(upload_twiddles<float>(g.Nx, &p->twx));
     CKP(upload_twiddles<float>(g.Ny, &p->twy));
@@ -353,7 +366,12 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     return TS_ERR_CUDA;
   }
   *p->err_h = 0;
-  CKP(upload_if_tables(p, cfg->nu, cfg->dt));
+  CKP(upload_if_tables(p, cfg->nu, cfg->dt, p->eax));
+  if (cfg->basis == TS_BASIS_SFF) {
+    CKP(upload_if_tables(p, cfg->kappa, cfg->dt, p->eaxT));
+    if (p->prec) CKP(upload_twiddles<float>(4 * g.Nx, &p->twq));
+    else CKP(upload_twiddles<double>(4 * g.Nx, &p->twq));
+  }
 #undef CKP
   *out = p;
   return TS_OK;
@@ -383,7 +401,9 @@ int ts_plan_set_dt(ts_plan* p, double dt) {
   if (dt == p->cfg.dt) return TS_OK;
   CK(cudaStreamSynchronize(p->st));
   p->cfg.dt = dt;
-  return upload_if_tables(p, p->cfg.nu, dt);
+  CKS(upload_if_tables(p, p->cfg.nu, dt, p->eax));
+  if (p->cfg.basis == TS_BASIS_SFF) CKS(upload_if_tables(p, p->cfg.kappa, dt, p->eaxT));
+  return TS_OK;
 }
 
 }  // extern "C"
@@ -437,6 +457,42 @@ static int step_fff(ts_plan* p, void* U0) {
   return TS_OK;
 }
 
+// one IF-RK4 step of the Boussinesq system on the SFF basis (RK_SF.cc:97-221)
+static int step_rbc(ts_plan* p, void* U0, void* T0) {
+  const Geo& g = p->g;
+  SffArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.T0 = T0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.dt = p->cfg.dt;
+  a.reality = p->cfg.reality_fix;
+  for (int i = 0; i < 3; ++i) {
+    a.eu[i] = p->eax[i];
+    a.et[i] = p->eaxT[i];
+  }
+  const long long cb = (long long)p->cb;
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? U0 : p->Ucur;
+    const void* Tin = stage == 1 ? T0 : (const void*)((const char*)p->Ucur + 3 * g.S * cb);
+    a.stage = stage;
+    a.U1in = Uin;
+    a.Tin = Tin;
+    { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, sff_inv_x, g, Uin, Tin, p->P, p->twq, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, 4, p->twy, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, 2, p->P, p->twz, p->err_d, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, 9, p->twy, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, sff_fwd_x, g, p->P, a, p->twq, p->st)); }
+  }
+  if (p->cfg.reality_fix) {
+    ProfScope ps(p, TS_KCLASS_OTHER);
+    CK(LAUNCH(p, reality, g, U0, 3, p->st));
+    CK(LAUNCH(p, reality, g, T0, 1, p->st));
+  }
+  return TS_OK;
+}
+
 // run fn(device_ptr) on a field that may live on the host
 template <typename Fn>
 static int with_device(ts_plan* p, void** stage, const void* ptr, size_t bytes, bool copy_back, Fn&& fn) {
@@ -469,7 +525,34 @@ int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
 
 int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   if (!p || !u_hat || !T_hat || nsteps < 0) return TS_ERR_ARG;
-  return TS_ERR_UNSUPPORTED;
+  if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up";
+    return TS_ERR_TIMEOUT;
+  }
+  const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
+  int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
+    return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
+      for (int s = 0; s < nsteps; ++s) CKS(step_rbc(p, U, T));
+      return (int)TS_OK;
+    });
+  });
+  if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return rc;
+}
+
+int ts_init_temperature_perturbation(ts_plan* p, double amp, double kmax, uint64_t seed, void* T_hat) {
+  if (!p || !T_hat || !(amp >= 0) || !(kmax >= 0)) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
+  return with_device(p, &p->stage_t, T_hat, p->g.S * p->cb, true, [&](void* T) -> int {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    CK(LAUNCH(p, init_temp, p->g, T, amp, kmax, z ^ (z >> 31), p->st));
+    CK(LAUNCH(p, reality, p->g, T, 1, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    return (int)TS_OK;
+  });
 }
 
 int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {

@@ -250,11 +250,22 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
 // ---------------------------------------------------------------------------
 template <int M> __host__ __device__ constexpr int zslot() { return M + M / 16 + 1; }
 
+// Real-space product forms of the z pass.
+// FORM 0 (conservative):  in u1,u2,u3       -> u1u1,u2u2,u3u3,u1u2,u2u3,u3u1
+// FORM 1 (rotational):    in u1..3,w1..3    -> u x w
+// FORM 2 (Boussinesq):    in u1,u2,u3,T     -> the six u_i u_j, then u1T,u2T,u3T
+//                         (compute_diag_offdiag.cc:47-136)
+__host__ __device__ constexpr int z_nin(int form) { return form == 0 ? 3 : (form == 1 ? 6 : 4); }
+__host__ __device__ constexpr int z_nout(int form) { return form == 0 ? 6 : (form == 1 ? 3 : 9); }
+// factor indices (a, b) of product output f for FORM 0 / 2
+__host__ __device__ constexpr int z_pa(int f) { return f < 3 ? f : (f < 6 ? f - 3 : f - 6); }
+__host__ __device__ constexpr int z_pb(int f) { return f < 3 ? f : (f < 6 ? (f == 5 ? 0 : f - 2) : 3); }
+
 template <typename T, int NZ, int E, int FORM>
 __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int nl) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, TPL = M / E, LDS = zslot<M>();
-  constexpr int NIN = FORM == 0 ? 3 : 6, NOUT = FORM == 0 ? 6 : 3;
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
   const long long nlines = (long long)g.Nx * g.Ny;
@@ -290,13 +301,10 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
     V in[NIN];
 #pragma unroll
     for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
-    if (FORM == 0) {
-      slot(0, ll)[m] = mk<V>(in[0].x * in[0].x, in[0].y * in[0].y);
-      slot(1, ll)[m] = mk<V>(in[1].x * in[1].x, in[1].y * in[1].y);
-      slot(2, ll)[m] = mk<V>(in[2].x * in[2].x, in[2].y * in[2].y);
-      slot(3, ll)[m] = mk<V>(in[0].x * in[1].x, in[0].y * in[1].y);
-      slot(4, ll)[m] = mk<V>(in[1].x * in[2].x, in[1].y * in[2].y);
-      slot(5, ll)[m] = mk<V>(in[2].x * in[0].x, in[2].y * in[0].y);
+    if (FORM != 1) {
+#pragma unroll
+      for (int f = 0; f < NOUT; ++f)
+        slot(f, ll)[m] = mk<V>(in[z_pa(f)].x * in[z_pb(f)].x, in[z_pa(f)].y * in[z_pb(f)].y);
     } else {
       slot(0, ll)[m] = mk<V>(in[1].x * in[5].x - in[2].x * in[4].x, in[1].y * in[5].y - in[2].y * in[4].y);
       slot(1, ll)[m] = mk<V>(in[2].x * in[3].x - in[0].x * in[5].x, in[2].y * in[3].y - in[0].y * in[5].y);
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
-  constexpr int NIN = FORM == 0 ? 3 : 6, NOUT = FORM == 0 ? 6 : 3;
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   constexpr int LPB = zreg_threads<FORM>() / TPL;
   __shared__ __align__(16) V xch_all[LPB * LDX];
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
@@ -401,7 +409,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
       if (FORM == 1) {
         p[s] = in[f][s];
       } else {
-        const int a = f < 3 ? f : f - 3, b = f < 3 ? f : (f == 5 ? 0 : f - 2);
+        const int a = z_pa(f), b = z_pb(f);
         p[s] = mk<V>(in[a][s].x * in[b][s].x, in[a][s].y * in[b][s].y);
       }
     }
@@ -448,7 +456,7 @@ __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, c
   constexpr int M = NZ / 2, H = M + 1, E = ztma_e<T>(), TPL = M / E, LDX = zslot<M>();
   constexpr int LPB = ztma_lpb<T, NZ>();
   static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
-  constexpr int NIN = FORM == 0 ? 3 : 6, NOUT = FORM == 0 ? 6 : 3;
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   constexpr int GRP = LPB * H;  // complex per component per group
   extern __shared__ __align__(128) unsigned char smraw_[];
   unsigned char* smraw = smraw_ + ((128 - (smem_u32(smraw_) & 127)) & 127);
@@ -522,7 +530,7 @@ __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, c
         if (FORM == 1) {
           p[s] = in[f][s];
         } else {
-          const int a = f < 3 ? f : f - 3, b = f < 3 ? f : (f == 5 ? 0 : f - 2);
+          const int a = z_pa(f), b = z_pb(f);
           p[s] = mk<V>(in[a][s].x * in[b][s].x, in[a][s].y * in[b][s].y);
         }
       }

@@ -127,69 +127,54 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int rot, const void* U, v
   return err_;
 }
 
-template <> cudaError_t Launch<T>::z_fused(const Geo& g, int rot, void* P, const void* tw, int* zerr,
+template <int NZ, int FORM>
+static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr, cudaStream_t st) {
+  constexpr int M = NZ / 2;
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
+  const long long nlines = (long long)g.Nx * g.Ny;
+  cudaError_t err;
+  if constexpr (M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
+    // FP64: bulk-copy variant (whole groups, 16-byte aligned group starts)
+    constexpr int LPB = ztma_lpb<T, NZ>();
+    const size_t sm = 2ull * NIN * LPB * (M + 1) * sizeof(V) + (size_t)LPB * zslot<M>() * sizeof(V) + 128;
+    if (nlines % LPB == 0 && (LPB * (M + 1) * sizeof(V)) % 16 == 0 && sm <= 220 * 1024) {
+      const long long ngroups = nlines / LPB;
+      auto k = k_z_tma<T, NZ, FORM>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
+      k<<<(unsigned)(ngroups < 148 ? ngroups : 148), 256, sm, st>>>((V*)P, g, (const V*)tw, zerr);
+      ++g_launches;
+      return cudaGetLastError();
+    }
+  }
+  if constexpr (M <= 256 && std::is_same<T, float>::value) {
+    // FP32: register-resident variant, lines of M/8 lanes
+    constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
+    k_z_reg<T, NZ, FORM><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
+    ++g_launches;
+    return cudaGetLastError();
+  }
+  // shared-memory slot variant (large lines)
+  constexpr int E = emin(8, M);
+  constexpr int TPL = M / E;
+  constexpr int NSL = NIN > NOUT ? NIN : NOUT;
+  int nl = 256 / TPL;
+  while (nl > 1 && (size_t)NSL * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
+  const size_t sm = (size_t)NSL * nl * zslot<M>() * sizeof(V);
+  auto k = k_z_fused<T, NZ, E, FORM>;
+  if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
+  k<<<(unsigned)((nlines + nl - 1) / nl), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, const void* tw, int* zerr,
                                            cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
   dispatch_L(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
-    constexpr int M = NZ / 2;
-    if constexpr (M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
-      // bulk-copy variant: needs whole groups and 16-byte aligned group starts
-      constexpr int LPB = ztma_lpb<T, NZ>();
-      const long long nlines = (long long)g.Nx * g.Ny;
-      const int nin = rot ? 6 : 3;
-      const size_t sm = 2ull * nin * LPB * (M + 1) * sizeof(V) + (size_t)LPB * zslot<M>() * sizeof(V) + 128;
-      if (nlines % LPB == 0 && (LPB * (M + 1) * sizeof(V)) % 16 == 0 && sm <= 220 * 1024) {
-        const long long ngroups = nlines / LPB;
-        const unsigned blocks = (unsigned)(ngroups < 148 ? ngroups : 148);
-        if (rot) {
-          auto k = k_z_tma<T, NZ, 1>;
-          if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-          k<<<blocks, 256, sm, st>>>((V*)P, g, (const V*)tw, zerr);
-        } else {
-          auto k = k_z_tma<T, NZ, 0>;
-          if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-          k<<<blocks, 256, sm, st>>>((V*)P, g, (const V*)tw, zerr);
-        }
-        ++g_launches;
-        err = cudaGetLastError();
-        return;
-      }
-    }
-    if constexpr (M <= 256 && std::is_same<T, float>::value) {
-      // register-resident variant: lines of M/8 lanes
-      const long long nlines = (long long)g.Nx * g.Ny;
-      if (rot) {
-        constexpr int NT = zreg_threads<1>(), LPB = NT / (M / 8);
-        k_z_reg<T, NZ, 1><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
-      } else {
-        constexpr int NT = zreg_threads<0>(), LPB = NT / (M / 8);
-        k_z_reg<T, NZ, 0><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
-      }
-      ++g_launches;
-      err = cudaGetLastError();
-      return;
-    }
-    constexpr int E = emin(8, M);
-    constexpr int TPL = M / E;
-    // lines per block: 256 threads, at most ~104 KB of slots (two blocks per SM)
-    int nl = 256 / TPL;
-    while (nl > 1 && 6ull * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
-    const size_t sm = 6ull * nl * zslot<M>() * sizeof(V);
-    const long long nlines = (long long)g.Nx * g.Ny;
-    dim3 grid((unsigned)((nlines + nl - 1) / nl));
-    const int threads = nl * TPL;
-    if (rot) {
-      auto k = k_z_fused<T, NZ, E, 1>;
-      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<grid, threads, sm, st>>>((V*)P, g, (const V*)tw, nl);
-    } else {
-      auto k = k_z_fused<T, NZ, E, 0>;
-      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<grid, threads, sm, st>>>((V*)P, g, (const V*)tw, nl);
-    }
-    ++g_launches;
-    err = cudaGetLastError();
+    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st);
+    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st);
+    else err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st);
   });
   return err;
 }
@@ -263,6 +248,49 @@ template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int rot, int mode, const 
   return err;
 }
 
+template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq,
+                                             cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L(g.Nx, [&](auto Lc) {
+    constexpr int NN = decltype(Lc)::value;
+    if constexpr (NN <= 512) {
+      constexpr int L2 = 2 * NN;
+      constexpr int E = e_reg(L2);
+      constexpr int CW = cw_for(L2, E);
+      const int inner = g.Ny * g.Hz;
+      const size_t sm = (size_t)L2 * CW * sizeof(V);
+      auto k = k_sff_inv_x<T, NN, E, CW>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<(inner + CW - 1) / CW, CW * (L2 / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g, (const V*)tq);
+      ++g_launches;
+      err = cudaGetLastError();
+    }
+  });
+  return err;
+}
+
+template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq,
+                                             cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L(g.Nx, [&](auto Lc) {
+    constexpr int NN = decltype(Lc)::value;
+    if constexpr (NN <= 512) {
+      constexpr int L2 = 2 * NN;
+      // four accumulators per element: 8 (FP32) / 4 (FP64) elements per thread
+      constexpr int E = emin(std::is_same<T, float>::value ? 8 : 4, L2);
+      constexpr int CW = cw_for(L2, E);
+      const int inner = g.Ny * g.Hz;
+      const size_t sm = (size_t)L2 * CW * sizeof(V);
+      auto k = k_sff_fwd_x<T, NN, E, CW>;
+      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+      k<<<(inner + CW - 1) / CW, CW * (L2 / E), sm, st>>>((const V*)P, g, a, (const V*)tq);
+      ++g_launches;
+      err = cudaGetLastError();
+    }
+  });
+  return err;
+}
+
 template <> cudaError_t Launch<T>::reality(const Geo& g, void* A, int ncomp, cudaStream_t st) {
   const long long n = (long long)g.Nx * g.Ny * ncomp;
   k_reality<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((V*)A, ncomp, g);
@@ -304,6 +332,13 @@ template <> cudaError_t Launch<T>::shell(const Geo& g, const void* A, int ncomp,
 template <> cudaError_t Launch<T>::init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
                                            unsigned long long key, cudaStream_t st) {
   k_init_ic<T><<<grid1d(g.S, 256), 256, 0, st>>>((V*)U, g, Eic, mis, nsh, key);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::init_temp(const Geo& g, void* A, double amp, double kmax, unsigned long long key,
+                                             cudaStream_t st) {
+  k_init_temp<T><<<grid1d(g.S, 256), 256, 0, st>>>((V*)A, g, amp, kmax, key);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "ts_fff.cuh"
+#include "ts_sff.cuh"
 
 namespace ts {
 
@@ -13,11 +14,16 @@ template <typename T> struct Launch {
   // dir -1 forward, +1 inverse; outputs scaled by `scale`
   static cudaError_t strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw, cudaStream_t st);
   static cudaError_t inv_x(const Geo& g, int rot, const void* U, void* W, const void* tw, int* err, cudaStream_t st);
-  static cudaError_t z_fused(const Geo& g, int rot, void* P, const void* tw, int* err, cudaStream_t st);
+  // form 0 conservative, 1 rotational, 2 Boussinesq (u, T)
+  static cudaError_t z_fused(const Geo& g, int form, void* P, const void* tw, int* err, cudaStream_t st);
   static cudaError_t z_single(const Geo& g, int dir, const void* in, void* out, int ncomp, const void* tw, cudaStream_t st);
   // a.U0 / a.Ud / a.tot must be 16-byte aligned (TMA)
   static cudaError_t fwd_x(const Geo& g, int rot, int mode, const void* P, const StageArgs& a, const void* tw,
                            cudaStream_t st);
+  // SFF x passes (sin/cos along x): inverse of u1,u2,u3,T into P[0..3]; forward of the nine
+  // Boussinesq products + force, projection and the IF-RK4 stage update
+  static cudaError_t sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq, cudaStream_t st);
+  static cudaError_t sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq, cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,
                             const double* hs, const double* mis, int nsup, cudaStream_t st);
@@ -27,6 +33,7 @@ template <typename T> struct Launch {
   static cudaError_t init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
                              unsigned long long key, cudaStream_t st);
   static cudaError_t scale(void* A, long long n, double s, cudaStream_t st);
+  static cudaError_t init_temp(const Geo& g, void* A, double amp, double kmax, unsigned long long key, cudaStream_t st);
   static cudaError_t dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
 };
 

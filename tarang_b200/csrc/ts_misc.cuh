@@ -304,6 +304,27 @@ __global__ void k_init_ic(C<T>* U, Geo g, const double* __restrict__ Eic, const 
   }
 }
 
+// temperature perturbation for RBC: amplitude amp, uniform random phase
+// 2 pi uniform01(key, e) on modes with grid radius |(m, ky, kz)| <= kmax, m >= 1
+template <typename T>
+__global__ void k_init_temp(C<T>* A, Geo g, double amp, double kmax, unsigned long long key) {
+  const long long n = g.S;
+  const double PI = 3.14159265358979323846;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    const int ky = kfft(ly, g.Ny);
+    const double r = sqrt((double)lx * lx + (double)ky * ky + (double)lz * lz);
+    C<T> v = mk<C<T>>(0, 0);
+    if (r <= kmax && lx >= 1) {
+      const double ph = 2 * PI * uniform01(key, (unsigned long long)e);
+      v = mk<C<T>>((T)(amp * cos(ph)), (T)(amp * sin(ph)));
+    }
+    A[e] = v;
+  }
+}
+
 template <typename T>
 __global__ void k_scale(C<T>* A, long long n, double s) {
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {

@@ -159,6 +159,11 @@ class Plan:
                 "ts_flux")
         return out
 
+    def init_temperature_perturbation(self, amp: float, kmax: float, seed: int, out):
+        L.check(self.lib.ts_init_temperature_perturbation(self.h, amp, kmax, seed, _ptr(out)),
+                "ts_init_temperature_perturbation")
+        return out
+
     def nusselt(self, u, T) -> float:
         e = ctypes.c_double()
         L.check(self.lib.ts_nusselt(self.h, _ptr(u), _ptr(T), ctypes.byref(e)), "ts_nusselt")
