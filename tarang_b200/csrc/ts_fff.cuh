@@ -598,8 +598,8 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   // TMA destinations: 128-byte aligned (the launcher adds 128 bytes of slack)
   unsigned char* smraw = smraw_ + ((128 - (smem_u32(smraw_) & 127)) & 127);
   V* pst = reinterpret_cast<V*>(smraw);
-  V* xch = pst + 2 * TILE;
-  V* sst = xch + TILE;
+  V* xch = pst + 2 * TILE;              // exchange tile, row pitch CW + 1 (bank spread)
+  V* sst = xch + L * (CW + 1);
   double* sbins = reinterpret_cast<double*>(sst + NST * TILE);
   __shared__ __align__(8) uint64_t bar[3];  // product slots 0, 1; state
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
       for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
       __syncthreads();
       if (threadIdx.x == 0) issue_item(item + 2);
-      fft_regs<L, E, -1>(v, t, xch, CW, c, tw, 1);
+      fft_regs<L, E, -1>(v, t, xch, CW + 1, c, tw, 1);
 #pragma unroll
       for (int s = 0; s < E; ++s) {
         const int lx = final_row<L, E>(t, s);

@@ -211,7 +211,7 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
   constexpr int CW = xcw(LL);
   const int inner = g.Ny * g.Hz;
   const int ntiles = (inner + CW - 1) / CW;
-  size_t sm = (size_t)(MODE == MODE_NLIN ? 3 : 9) * LL * CW * sizeof(V) + 128;
+  size_t sm = (size_t)(MODE == MODE_NLIN ? 2 : 8) * LL * CW * sizeof(V) + (size_t)LL * (CW + 1) * sizeof(V) + 128;
   if (MODE == MODE_FLUX) sm += (size_t)(a.nradii + 1) * sizeof(double);
   const int per_sm = (int)((220 * 1024) / sm) >= 2 ? 2 : 1;
   const int blocks = ntiles < 148 * per_sm ? ntiles : 148 * per_sm;
