@@ -138,6 +138,29 @@ int ts_nusselt(ts_plan* plan, const void* u_hat, const void* T_hat, double* Nu);
 int ts_init_energy_spectrum(ts_plan* plan, const double* E_ic, int n, uint64_t seed, double target_energy,
                             void* u_hat);
 
+/* Ensemble of independent Boussinesq (RBC, SFF, PRLARGE/ULARGE) runs of uneven
+ * sizes: a batching layer with no reference counterpart (the reference runs one
+ * field per MPI job).  Each member has its own plan (N, Ra, Pr; nu = sqrt(Pr/Ra),
+ * kappa = 1/sqrt(Pr Ra)) and device state; the other settings come from `base`.
+ * ts_ensemble_run advances every member by nsteps; each ensemble step is one
+ * CUDA graph launch whose parallel branches are the members' step sequences.
+ * Asynchronous: ts_ensemble_synchronize / ts_ensemble_nusselt wait for it. */
+typedef struct {
+  int N[3];
+  double Ra, Pr;
+} ts_member;
+typedef struct ts_ensemble ts_ensemble;
+int ts_ensemble_create(const ts_config* base, const ts_member* members, int count, ts_ensemble** ens);
+int ts_ensemble_destroy(ts_ensemble* ens);
+/* the member's plan and its device state u_hat (3 components) and T_hat */
+int ts_ensemble_member(ts_ensemble* ens, int member, ts_plan** plan, void** u_hat, void** T_hat);
+/* u = 0 and a temperature perturbation (ts_init_temperature_perturbation, seed + member) */
+int ts_ensemble_init_temperature(ts_ensemble* ens, double amp, double kmax, uint64_t seed);
+int ts_ensemble_run(ts_ensemble* ens, int nsteps);
+int ts_ensemble_synchronize(ts_ensemble* ens);
+/* Nusselt number of every member (Correlation.cc:154-156) */
+int ts_ensemble_nusselt(ts_ensemble* ens, double* Nu);
+
 /* Kernel classes of one right-hand-side evaluation, for ts_profile_read. */
 typedef enum {
   TS_KCLASS_INV_X = 0,  /* dealias + inverse FFT along x (+ vorticity) */

@@ -22,6 +22,10 @@ TS_FORCE_NONE, TS_FORCE_CARATI_ENERGY_SUPPLY, TS_FORCE_RBC = 0, 1, 51
 KCLASS_NAMES = ["inv_x", "y_inv", "z_fused", "y_fwd", "fwd_x_update", "other"]
 
 
+class TsMember(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int * 3), ("Ra", ctypes.c_double), ("Pr", ctypes.c_double)]
+
+
 class TsConfig(ctypes.Structure):
     _fields_ = [
         ("basis", ctypes.c_int),
@@ -68,6 +72,14 @@ SIGNATURES = {
     "ts_nusselt": (ctypes.c_int, [_P, _P, _P, _D]),
     "ts_init_energy_spectrum": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_uint64, ctypes.c_double, _P]),
     "ts_init_temperature_perturbation": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _P]),
+    "ts_ensemble_create": (ctypes.c_int, [ctypes.POINTER(TsConfig), _P, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "ts_ensemble_destroy": (ctypes.c_int, [_P]),
+    "ts_ensemble_member": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
+    "ts_ensemble_init_temperature": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64]),
+    "ts_ensemble_run": (ctypes.c_int, [_P, ctypes.c_int]),
+    "ts_ensemble_synchronize": (ctypes.c_int, [_P]),
+    "ts_ensemble_nusselt": (ctypes.c_int, [_P, _D]),
     "ts_profile_enable": (ctypes.c_int, [_P, ctypes.c_int]),
     "ts_profile_reset": (ctypes.c_int, [_P]),
     "ts_profile_read": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.POINTER(ctypes.c_longlong), _D]),

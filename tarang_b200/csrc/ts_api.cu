@@ -263,11 +263,14 @@ int ts_plan_destroy(ts_plan* p) {
 int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   if (!cfg || !out) return TS_ERR_ARG;
   *out = nullptr;
-  for (int i = 0; i < 3; ++i)
-    if (!size_supported(cfg->N[i])) {
-      g_last_error = "N must be a power of two in [16, 1024]";
+  for (int i = 0; i < 3; ++i) {
+    // 48 and 96 (factor 3) are supported for the FP32 SFF path
+    const bool mixed = (cfg->N[i] == 48 || cfg->N[i] == 96) && cfg->basis == TS_BASIS_SFF && cfg->precision == TS_F32;
+    if (!size_supported(cfg->N[i]) && !mixed) {
+      g_last_error = "N must be a power of two in [16, 1024] (48 and 96 also for FP32 SFF)";
       return TS_ERR_ARG;
     }
+  }
   if (cfg->basis != TS_BASIS_FFF && cfg->basis != TS_BASIS_SFF) return TS_ERR_ARG;
   if (cfg->precision != TS_F64 && cfg->precision != TS_F32) return TS_ERR_ARG;
   if (cfg->dealias_mode < 0 || cfg->dealias_mode > 2) return TS_ERR_ARG;
@@ -764,6 +767,145 @@ int ts_profile_read(ts_plan* p, int kclass, double* total_ms, long long* launche
     }
     *bytes_per_launch = b;
   }
+  return TS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensemble of independent RBC runs (uneven sizes).  One plan per member; one
+// ensemble step is a single CUDA graph launch whose branches are the members'
+// step sequences (fork on an event of the origin stream, one stream per member,
+// join back), so small members run concurrently and fill the GPU.
+// ---------------------------------------------------------------------------
+struct ts_ensemble {
+  std::vector<ts_plan*> plans;
+  std::vector<void*> U, T;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> done;
+  cudaEvent_t fork = nullptr;
+  cudaStream_t origin = nullptr;
+  bool own_origin = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+int ts_ensemble_destroy(ts_ensemble* e) {
+  if (!e) return TS_ERR_ARG;
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (size_t m = 0; m < e->plans.size(); ++m) {
+    if (e->U[m]) cudaFree(e->U[m]);
+    if (e->T[m]) cudaFree(e->T[m]);
+    if (e->plans[m]) ts_plan_destroy(e->plans[m]);
+    if (e->streams[m]) cudaStreamDestroy(e->streams[m]);
+    if (e->done[m]) cudaEventDestroy(e->done[m]);
+  }
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->own_origin && e->origin) cudaStreamDestroy(e->origin);
+  delete e;
+  return TS_OK;
+}
+
+int ts_ensemble_create(const ts_config* base, const ts_member* members, int count, ts_ensemble** out) {
+  if (!base || !members || count < 1 || !out) return TS_ERR_ARG;
+  *out = nullptr;
+  ts_ensemble* e = new ts_ensemble();
+  auto fail = [&](int rc) {
+    ts_ensemble_destroy(e);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking) != cudaSuccess) return fail(TS_ERR_CUDA);
+  e->own_origin = true;
+  if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) return fail(TS_ERR_CUDA);
+  for (int m = 0; m < count; ++m) {
+    ts_config c = *base;
+    c.basis = TS_BASIS_SFF;
+    c.force_type = TS_FORCE_RBC;
+    for (int i = 0; i < 3; ++i) c.N[i] = members[m].N[i];
+    c.Ra = members[m].Ra;
+    c.Pr = members[m].Pr;
+    // ULARGE: nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra) (Iscalar_main.cc:52-92)
+    c.nu = sqrt(c.Pr / c.Ra);
+    c.kappa = 1.0 / sqrt(c.Pr * c.Ra);
+    ts_plan* p = nullptr;
+    e->plans.push_back(nullptr);
+    e->U.push_back(nullptr);
+    e->T.push_back(nullptr);
+    e->streams.push_back(nullptr);
+    e->done.push_back(nullptr);
+    int rc = ts_plan_create(&c, &p);
+    if (rc != TS_OK) return fail(rc);
+    e->plans[m] = p;
+    if (cudaStreamCreateWithFlags(&e->streams[m], cudaStreamNonBlocking) != cudaSuccess) return fail(TS_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&e->done[m], cudaEventDisableTiming) != cudaSuccess) return fail(TS_ERR_CUDA);
+    p->st = e->streams[m];
+    const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
+    if (cudaMalloc(&e->U[m], bu) != cudaSuccess || cudaMalloc(&e->T[m], bt) != cudaSuccess) return fail(TS_ERR_NOMEM);
+    if (cudaMemset(e->U[m], 0, bu) != cudaSuccess || cudaMemset(e->T[m], 0, bt) != cudaSuccess)
+      return fail(TS_ERR_CUDA);
+  }
+  *out = e;
+  return TS_OK;
+}
+
+int ts_ensemble_member(ts_ensemble* e, int m, ts_plan** plan, void** u_hat, void** T_hat) {
+  if (!e || m < 0 || m >= (int)e->plans.size()) return TS_ERR_ARG;
+  if (plan) *plan = e->plans[m];
+  if (u_hat) *u_hat = e->U[m];
+  if (T_hat) *T_hat = e->T[m];
+  return TS_OK;
+}
+
+int ts_ensemble_init_temperature(ts_ensemble* e, double amp, double kmax, uint64_t seed) {
+  if (!e) return TS_ERR_ARG;
+  for (size_t m = 0; m < e->plans.size(); ++m) {
+    CK(cudaMemset(e->U[m], 0, 3 * e->plans[m]->g.S * e->plans[m]->cb));
+    CKS(ts_init_temperature_perturbation(e->plans[m], amp, kmax, seed + m, e->T[m]));
+  }
+  return TS_OK;
+}
+
+int ts_ensemble_run(ts_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return TS_ERR_ARG;
+  if (!e->exec) {
+    for (ts_plan* p : e->plans) p->prof = false;
+    CK(cudaStreamSynchronize(e->origin));
+    CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeRelaxed));
+    int rc = TS_OK;
+    cudaEventRecord(e->fork, e->origin);
+    for (size_t m = 0; m < e->plans.size() && rc == TS_OK; ++m) {
+      cudaStreamWaitEvent(e->streams[m], e->fork, 0);
+      rc = step_rbc(e->plans[m], e->U[m], e->T[m]);
+      cudaEventRecord(e->done[m], e->streams[m]);
+      cudaStreamWaitEvent(e->origin, e->done[m], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);
+    if (rc != TS_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    CK(ce);
+    e->graph = graph;
+    CK(cudaGraphInstantiate(&e->exec, e->graph, 0));
+  }
+  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(e->exec, e->origin));
+  return TS_OK;
+}
+
+int ts_ensemble_synchronize(ts_ensemble* e) {
+  if (!e) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(e->origin));
+  return TS_OK;
+}
+
+int ts_ensemble_nusselt(ts_ensemble* e, double* Nu) {
+  if (!e || !Nu) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(e->origin));
+  for (size_t m = 0; m < e->plans.size(); ++m) CKS(ts_nusselt(e->plans[m], e->U[m], e->T[m], &Nu[m]));
   return TS_OK;
 }
 

@@ -53,6 +53,18 @@ template <int DIR, typename V> struct DFT<2, DIR, V> {
     v[1] = sub(a, v[1]);
   }
 };
+template <int DIR, typename V> struct DFT<3, DIR, V> {
+  // X1 = a - (b+c)/2 + DIR i (sqrt3/2)(b-c), X2 = a - (b+c)/2 - DIR i (sqrt3/2)(b-c)
+  static __device__ __forceinline__ void run(V* v) {
+    typedef decltype(V::x) S;
+    const V a = v[0], s = add(v[1], v[2]), d = sub(v[1], v[2]);
+    const V t = sub(a, scale(s, (S)0.5));
+    const V u = scale(mul_i<DIR>(d), (S)0.86602540378443864676);
+    v[0] = add(a, s);
+    v[1] = add(t, u);
+    v[2] = sub(t, u);
+  }
+};
 template <int R, int DIR, typename V> struct DFT {
   // radix-2 decimation in time: X[k] = E[k] + w^k O[k], X[k+R/2] = E[k] - w^k O[k]
   static __device__ __forceinline__ void run(V* v) {
@@ -78,11 +90,20 @@ template <int R, int DIR, typename V> struct DFT {
 // ---------------------------------------------------------------------------
 // Stockham radix schedule for length L with at most E elements per thread.
 // ---------------------------------------------------------------------------
-__host__ __device__ constexpr int radix_at(int L, int E, int p) {
-  // radix of pass p: min(E, remaining length)
-  return p == 0 ? (L < E ? L : E) : radix_at(L / (L < E ? L : E), E, p - 1);
+// L = 2^a (or 3 * 2^a): the power-of-two part is split into passes of radix
+// min(lowbit(E), remaining); a factor 3 is one final radix-3 pass.  Every radix
+// divides E, so a thread always owns whole butterflies.
+__host__ __device__ constexpr int lowbit(int x) { return x & (-x); }
+__host__ __device__ constexpr int rad2(int L2, int E2, int p) {
+  return p == 0 ? (L2 < E2 ? L2 : E2) : rad2(L2 / (L2 < E2 ? L2 : E2), E2, p - 1);
 }
-__host__ __device__ constexpr int npasses(int L, int E) { return L <= 1 ? 0 : 1 + npasses(L / (L < E ? L : E), E); }
+__host__ __device__ constexpr int np2(int L2, int E2) { return L2 <= 1 ? 0 : 1 + np2(L2 / (L2 < E2 ? L2 : E2), E2); }
+__host__ __device__ constexpr int radix_at(int L, int E, int p) {
+  return p < np2(lowbit(L), lowbit(E)) ? rad2(lowbit(L), lowbit(E), p) : L / lowbit(L);
+}
+__host__ __device__ constexpr int npasses(int L, int E) {
+  return np2(lowbit(L), lowbit(E)) + (L != lowbit(L) ? 1 : 0);
+}
 __host__ __device__ constexpr int ns_at(int L, int E, int p) {
   // product of the radices before pass p
   return p == 0 ? 1 : radix_at(L, E, p - 1) * ns_at(L, E, p - 1);
@@ -106,6 +127,7 @@ __host__ __device__ constexpr int ns_sched(int L, int E, int p, bool rev) {
 template <int L, int E, int P, bool REV = false> struct Pass {
   static constexpr int R = radix_sched(L, E, P, REV);
   static constexpr int NS = ns_sched(L, E, P, REV);
+  static_assert(E % R == 0 && L % E == 0, "every radix must divide the elements per thread");
   static constexpr int B = E / R;  // butterflies per thread
   static __device__ __forceinline__ int in_row(int t, int s) {
     const int j = t * B + s / R;

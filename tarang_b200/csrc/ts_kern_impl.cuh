@@ -40,6 +40,21 @@ template <typename Fn> bool dispatch_L(int L, Fn&& fn) {
   return false;
 }
 
+// SFF launchers also take the non-power-of-two sizes 48 and 96 (FP32 only):
+// their FFT lengths 3 * 2^k run with 12 elements per thread (radices 4, 2, 3)
+template <typename Fn> bool dispatch_L_sff(int L, Fn&& fn) {
+  if (dispatch_L(L, fn)) return true;
+  if constexpr (std::is_same<T, float>::value) {
+    switch (L) {
+      case 48: fn(std::integral_constant<int, 48>{}); return true;
+      case 96: fn(std::integral_constant<int, 96>{}); return true;
+    }
+  }
+  return false;
+}
+// elements per thread for a length that may carry a factor 3
+constexpr int e_mixed(int L, int e_pow2) { return L % 3 == 0 ? 12 : (e_pow2 < L ? e_pow2 : L); }
+
 template <typename K> cudaError_t smem_attr(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   return cudaSuccess;
@@ -67,9 +82,9 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
                                            cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
   const int L = axis == 0 ? g.Nx : g.Ny;
-  dispatch_L(L, [&](auto Lc) {
+  dispatch_L_sff(L, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
-    constexpr int E = e_reg(LL);
+    constexpr int E = e_mixed(LL, e_reg(LL));
     constexpr int CW = cw_for(LL, E);
     const int inner = axis == 0 ? g.Ny * g.Hz : g.Hz;
     const long long rstride = axis == 0 ? (long long)g.Ny * g.Hz : g.Hz;
@@ -133,7 +148,7 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   const long long nlines = (long long)g.Nx * g.Ny;
   cudaError_t err;
-  if constexpr (M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
+  if constexpr (M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
     // FP64: bulk-copy variant (whole groups, 16-byte aligned group starts)
     constexpr int LPB = ztma_lpb<T, NZ>();
     const size_t sm = 2ull * NIN * LPB * (M + 1) * sizeof(V) + (size_t)LPB * zslot<M>() * sizeof(V) + 128;
@@ -146,15 +161,15 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
       return cudaGetLastError();
     }
   }
-  if constexpr (M <= 256 && std::is_same<T, float>::value) {
+  if constexpr (M % 3 != 0 && M <= 256 && std::is_same<T, float>::value) {
     // FP32: register-resident variant, lines of M/8 lanes
     constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
     k_z_reg<T, NZ, FORM><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
     ++g_launches;
     return cudaGetLastError();
   }
-  // shared-memory slot variant (large lines)
-  constexpr int E = emin(8, M);
+  // shared-memory slot variant (large lines, and line lengths with a factor 3)
+  constexpr int E = e_mixed(M, 8);
   constexpr int TPL = M / E;
   constexpr int NSL = NIN > NOUT ? NIN : NOUT;
   int nl = 256 / TPL;
@@ -170,7 +185,7 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
 template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, const void* tw, int* zerr,
                                            cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
-  dispatch_L(g.Nz, [&](auto Lc) {
+  dispatch_L_sff(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
     if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st);
     else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st);
@@ -251,11 +266,11 @@ template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int rot, int mode, const 
 template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq,
                                              cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
-  dispatch_L(g.Nx, [&](auto Lc) {
+  dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
     if constexpr (NN <= 512) {
       constexpr int L2 = 2 * NN;
-      constexpr int E = e_reg(L2);
+      constexpr int E = e_mixed(L2, e_reg(L2));
       constexpr int CW = cw_for(L2, E);
       const int inner = g.Ny * g.Hz;
       const size_t sm = (size_t)L2 * CW * sizeof(V);
@@ -272,12 +287,12 @@ template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const 
 template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq,
                                              cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
-  dispatch_L(g.Nx, [&](auto Lc) {
+  dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
     if constexpr (NN <= 512) {
       constexpr int L2 = 2 * NN;
       // four accumulators per element: 8 (FP32) / 4 (FP64) elements per thread
-      constexpr int E = emin(std::is_same<T, float>::value ? 8 : 4, L2);
+      constexpr int E = e_mixed(L2, std::is_same<T, float>::value ? 8 : 4);
       constexpr int CW = cw_for(L2, E);
       const int inner = g.Ny * g.Hz;
       const size_t sm = (size_t)L2 * CW * sizeof(V);

@@ -228,3 +228,87 @@ class Time_advance_incompress:
     def RK4(U: FluidVF, nsteps: int = 1):
         """IF-RK4 step(s) + strong reality condition (RK.cc:91-170, Time_advance.cc:59-60)."""
         U.plan.rk4_step(U.cvf, nsteps)
+
+
+class Ensemble:
+    """Independent RBC runs (SFF, PRLARGE/ULARGE) of uneven sizes advanced together:
+    one CUDA graph launch per ensemble step with one parallel branch per member."""
+
+    def __init__(self, members, kfactor=(math.pi, 2 * math.pi, 2 * math.pi), dt: float = 1e-4,
+                 precision: str = "f32", dealias: str = "reference", reality_fix: bool = True):
+        self.lib = L.load()
+        c = L.TsConfig()
+        self.lib.ts_config_default(ctypes.byref(c))
+        c.basis = L.TS_BASIS_SFF
+        for i in range(3):
+            c.kfactor[i] = float(kfactor[i])
+        c.precision = L.TS_F64 if precision == "f64" else L.TS_F32
+        c.dealias_mode = _DEALIAS[dealias]
+        c.reality_fix = int(bool(reality_fix))
+        c.dt = dt
+        c.force_type = L.TS_FORCE_RBC
+        arr = (L.TsMember * len(members))()
+        for m, (N, Ra, Pr) in enumerate(members):
+            N = (N, N, N) if isinstance(N, int) else N
+            for i in range(3):
+                arr[m].N[i] = int(N[i])
+            arr[m].Ra, arr[m].Pr = float(Ra), float(Pr)
+        self.members = [((N, N, N) if isinstance(N, int) else tuple(N), Ra, Pr) for N, Ra, Pr in members]
+        h = ctypes.c_void_p()
+        L.check(self.lib.ts_ensemble_create(ctypes.byref(c), arr, len(members), ctypes.byref(h)), "ts_ensemble_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ts_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def member(self, m):
+        """(plan handle, u_hat pointer, T_hat pointer) of member m (device memory owned by the ensemble)."""
+        p, u, t = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        L.check(self.lib.ts_ensemble_member(self.h, m, ctypes.byref(p), ctypes.byref(u), ctypes.byref(t)),
+                "ts_ensemble_member")
+        return p, u, t
+
+    def init_temperature(self, amp: float, kmax: float, seed: int):
+        L.check(self.lib.ts_ensemble_init_temperature(self.h, amp, kmax, seed), "ts_ensemble_init_temperature")
+
+    def run(self, nsteps: int):
+        L.check(self.lib.ts_ensemble_run(self.h, nsteps), "ts_ensemble_run")
+
+    def synchronize(self):
+        L.check(self.lib.ts_ensemble_synchronize(self.h), "ts_ensemble_synchronize")
+
+    def nusselt(self) -> np.ndarray:
+        out = np.zeros(len(self.members))
+        L.check(self.lib.ts_ensemble_nusselt(self.h, out.ctypes.data_as(L._D)), "ts_ensemble_nusselt")
+        return out
+
+    def energy(self, m: int, which: str = "T") -> float:
+        p, u, t = self.member(m)
+        e = ctypes.c_double()
+        L.check(self.lib.ts_energy(p, t if which == "T" else u, 1 if which == "T" else 3, ctypes.byref(e)), "ts_energy")
+        return e.value
+
+
+def ensemble_members(count: int = 64, sizes=(32, 48, 64, 96, 128), ra_range=(1e5, 1e7), Pr: float = 1.0,
+                     size_seed: int = 1, ra_seed: int = 2):
+    """The benchmark ensemble: sizes drawn uniformly (seed 1) and Ra log-uniform (seed 2) with this
+    project's counter-based generator (splitmix64, as the initial conditions)."""
+    def u01(seed, n):
+        def sm(x):
+            x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+            x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+            x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+            return x ^ (x >> 31)
+        key = sm(seed)
+        return [(sm(key ^ i) >> 11) * (1.0 / 9007199254740992.0) for i in range(n)]
+    su, ru = u01(size_seed, count), u01(ra_seed, count)
+    lo, hi = math.log(ra_range[0]), math.log(ra_range[1])
+    return [(sizes[min(int(a * len(sizes)), len(sizes) - 1)], math.exp(lo + b * (hi - lo)), Pr) for a, b in zip(su, ru)]
