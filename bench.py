@@ -44,7 +44,71 @@ def parse():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--form", default="rotational", choices=["rotational", "conservative"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
+    ap.add_argument("--workload", default="fff256", choices=["fff256", "ensemble", "fff1024"],
+                    help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying 1024^3")
     return ap.parse_args()
+
+
+def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
+    """Config 3: 64 RBC members (SFF, N in {32,48,64,96,128}, Ra log-uniform [1e5,1e7], Pr=1, FP32,
+    dt=1e-4), members greedily packed onto ranks by N^3; returns per-rank timing and model bytes."""
+    import torch
+    import tarang_b200 as tb
+    allm = tb.ensemble_members()
+    members = [allm[i] for i in tb.shard_members(allm, rank, world)]
+    ens = tb.Ensemble(members, dt=1e-4, precision="f32", dealias="reference")
+    ens.init_temperature(1e-3, 4.0, 3)
+    ens.run(warmup)
+    ens.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.run(steps)
+    ens.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    Nu = ens.nusselt()
+    ens.close()
+    model = sum(408.0 * m[0] ** 3 * 4 for m in members)   # SFF RBC byte model per member step, FP32
+    return {"members": len(members), "seconds": wall, "steps": steps, "model_bytes_per_step": model,
+            "nusselt_mean": float(np.mean(Nu)), "nusselt_finite": bool(np.all(np.isfinite(Nu)))}
+
+
+def fff1024_leg(steps: int = 3, warmup: int = 2):
+    """Config 2: FFF 1024^3 decaying turbulence, FP32 rotational, IC k^4 exp(-2(k/8)^2) E=0.5,
+    nu=2e-4, dt=2e-4; steps/s and the per-kernel rates."""
+    import torch
+    import ctypes
+    import tarang_b200 as tb
+    from tarang_b200 import _lib as L
+    plan = tb.Plan(1024, precision="f32", nlin_form="rotational", dealias="two_thirds", nu=2e-4, dt=2e-4)
+    plan.set_stream(torch.cuda.current_stream())   # the timing events below go on this stream
+    u = plan.field(3)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 8.0), 0, 0.5, u)
+    plan.rk4_step(u, warmup)
+    torch.cuda.synchronize()
+    L.check(plan.lib.ts_profile_reset(plan.h), "reset")
+    L.check(plan.lib.ts_profile_enable(plan.h, 1), "enable")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.rk4_step(u, steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    L.check(plan.lib.ts_profile_enable(plan.h, 0), "disable")
+    kern = {}
+    for k, name in enumerate(L.KCLASS_NAMES):
+        tot, n, b = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+        L.check(plan.lib.ts_profile_read(plan.h, k, ctypes.byref(tot), ctypes.byref(n), ctypes.byref(b)), "read")
+        if n.value and b.value:
+            kern[name] = round(b.value / (tot.value / n.value / 1e3) / 1e9, 1)
+    out = {"steps_per_s": steps / (ms / 1e3), "kernel_GBps": kern, "energy": plan.energy(u),
+           "model_frac": 288.0 * 1024 ** 3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
+    plan.close()
+    return out
 
 
 def workload(N):
@@ -187,6 +251,50 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def alt_workload(args, world, rank, local, dev):
+    """The ensemble (config 3) or the 1024^3 decaying run (config 2) as the primary line."""
+    import torch
+    import torch.distributed as dist
+    clk = Clocks(local)
+    clk.start()
+    if args.workload == "ensemble":
+        r = ensemble_leg(rank, world, steps=args.steps, warmup=args.warmup)
+        sec = r["seconds"]
+        mb = r["model_bytes_per_step"]
+        if world > 1:
+            t = torch.tensor([sec, mb], device=dev, dtype=torch.float64)
+            t2 = t.clone()
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t2)
+            sec, mb = float(t[0].item()), float(t2[1].item())
+        value = args.steps / sec
+        line = {"metric": "ensemble RK4 steps/s, 64 RBC members (SFF, N in {32,48,64,96,128}, FP32)",
+                "value": value, "unit": "ensemble-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "64 RBC members, Ra log-uniform [1e5,1e7] (seed 2), sizes seed 1, Pr=1, "
+                                       "kfactor (pi,2pi,2pi), T amp 1e-3 k<=4 (seed 3), dt=1e-4",
+                           "parallelism": f"members packed on {world} GPU(s) by N^3"},
+                "roofline": {"bound": "hbm", "achieved": mb * value / 1e9 / world, "peak": measured_peak()[0],
+                             "unit": "GB/s", "frac": mb * value / 1e9 / world / measured_peak()[0],
+                             "traffic": None, "model": "408 N^3 4 B per member step"},
+                "member_steps_per_s": 64 * value}
+    else:
+        r = fff1024_leg(steps=args.steps, warmup=args.warmup)
+        line = {"metric": "RK4 steps/s, FFF decaying turbulence 1024^3 (FP32 transforms, FP64 sums)",
+                "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 / r["steps_per_s"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "FFF 1024^3 decaying, IC k^4 exp(-2(k/8)^2) E=0.5 seed 0, nu=2e-4, dt=2e-4"},
+                "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "kernel_GBps": r["kernel_GBps"]}}
+    line["clocks"] = clk.stop()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -205,6 +313,9 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    if args.workload != "fff256":
+        return alt_workload(args, world, rank, local, dev)
 
     N = args.N
     nsh = int(math.ceil(math.sqrt(3) * (N // 2))) + 1
@@ -331,6 +442,25 @@ def main():
             p64.close()
         extras["max_div_end"] = plan.max_div(u)
         extras["energy_end"] = plan.energy(u)
+        # config 3: the RBC ensemble (all ranks; members shared out by N^3)
+        plan.close()
+        torch.cuda.empty_cache()
+        ens = ensemble_leg(rank, world, steps=10, warmup=2)
+        esec = ens["seconds"]
+        if world > 1:
+            t = torch.tensor([esec], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            esec = float(t.item())
+            mb = torch.tensor([ens["model_bytes_per_step"]], device=dev, dtype=torch.float64)
+            dist.all_reduce(mb)
+            ens["model_bytes_per_step"] = float(mb.item())
+        extras["ensemble_rbc_64"] = {"ensemble_steps_per_s": ens["steps"] / esec,
+                                     "member_steps_per_s": 64 * ens["steps"] / esec,
+                                     "model_GBps": ens["model_bytes_per_step"] * ens["steps"] / esec / 1e9,
+                                     "nusselt_mean_rank0": ens["nusselt_mean"], "finite": ens["nusselt_finite"],
+                                     "timing": "wall clock around synchronised graph launches, max over ranks"}
+        if world == 1:
+            extras["fff1024_f32"] = fff1024_leg()
         if rank == 0 and world == 1:
             v, n, el = cpu_baseline_oracle(N)
             from oracle import tarang_ref as R
@@ -350,7 +480,8 @@ def main():
                 "roofline": roofline, "step_roofline": step_model, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clocks, "extras": extras}
         print(json.dumps(line), flush=True)
-    plan.close()
+    if plan.h:
+        plan.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

@@ -6,7 +6,7 @@ is the host-side binding.  There is no CPU fallback.
 """
 from ._lib import TsError, load as load_library, lib_path  # noqa: F401
 from .solver import (Ensemble, FluidVF, Forcing, Nlin_incompress, Plan, Time_advance_incompress,  # noqa: F401
-                     ensemble_members, kernel_launch_count, spectrum_k4_gauss)
+                     ensemble_members, kernel_launch_count, shard_members, spectrum_k4_gauss)
 
-__all__ = ["Plan", "Ensemble", "ensemble_members", "Forcing", "FluidVF", "Nlin_incompress", "Time_advance_incompress", "TsError",
+__all__ = ["Plan", "Ensemble", "ensemble_members", "shard_members", "Forcing", "FluidVF", "Nlin_incompress", "Time_advance_incompress", "TsError",
            "load_library", "lib_path", "kernel_launch_count", "spectrum_k4_gauss"]

@@ -25,7 +25,13 @@ constexpr int cw_for(int L, int E) {
 constexpr int UNITS = (int)sizeof(V) / 8;
 // column tile width of the TMA x-pass kernels: 64-byte rows, and at least two
 // 8-byte units so every tile start is 16-byte aligned
-constexpr int xcw(int L) { return std::is_same<T, float>::value ? (L >= 1024 ? 4 : 8) : (L >= 1024 ? 2 : 4); }
+// (the epilogue kernel's 8 tiles + padded exchange tile must fit in 220 KB)
+constexpr int xcw_fit(int L, int cw) {
+  return (cw > (std::is_same<T, float>::value ? 2 : 1) &&
+          (size_t)9 * L * cw * sizeof(V) + (size_t)L * sizeof(V) > 220 * 1024)
+             ? xcw_fit(L, cw / 2) : cw;
+}
+constexpr int xcw(int L) { return xcw_fit(L, std::is_same<T, float>::value ? 8 : 4); }
 
 template <typename Fn> bool dispatch_L(int L, Fn&& fn) {
   switch (L) {
@@ -56,7 +62,11 @@ template <typename Fn> bool dispatch_L_sff(int L, Fn&& fn) {
 constexpr int e_mixed(int L, int e_pow2) { return L % 3 == 0 ? 12 : (e_pow2 < L ? e_pow2 : L); }
 
 template <typename K> cudaError_t smem_attr(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (bytes > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) cudaGetLastError();  // do not leave the error for a later launch to report
+    return e;
+  }
   return cudaSuccess;
 }
 

@@ -312,3 +312,18 @@ def ensemble_members(count: int = 64, sizes=(32, 48, 64, 96, 128), ra_range=(1e5
     su, ru = u01(size_seed, count), u01(ra_seed, count)
     lo, hi = math.log(ra_range[0]), math.log(ra_range[1])
     return [(sizes[min(int(a * len(sizes)), len(sizes) - 1)], math.exp(lo + b * (hi - lo)), Pr) for a, b in zip(su, ru)]
+
+
+def shard_members(members, rank: int, world: int):
+    """Indices of the ensemble members that rank `rank` of `world` advances: greedy bin packing
+    on the per-member cost N^3 (largest first, onto the least-loaded rank).  Members are
+    independent, so ranks exchange nothing while stepping; only diagnostics are gathered."""
+    cost = [int(np.prod((m[0],) * 3 if isinstance(m[0], int) else m[0])) for m in members]
+    order = sorted(range(len(members)), key=lambda i: (-cost[i], i))
+    load = [0] * world
+    owner = [0] * len(members)
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += cost[i]
+        owner[i] = r
+    return [i for i in range(len(members)) if owner[i] == rank]
