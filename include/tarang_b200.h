@@ -161,6 +161,27 @@ int ts_ensemble_synchronize(ts_ensemble* ens);
 /* Nusselt number of every member (Correlation.cc:154-156) */
 int ts_ensemble_nusselt(ts_ensemble* ens, double* Nu);
 
+/* Discrete adjoint of the FFF IF-RK4 step (rotational form, unforced plans).
+ * No reference counterpart: the reference has no adjoint.  Cotangents are
+ * complex fields in the state's layout, in the real inner product
+ * <A, B> = Re sum A conj(B) over the stored half spectrum (torch's convention
+ * for the gradient of a real loss with respect to a complex tensor).
+ * Device pointers only, 16-byte aligned.
+ *
+ * ts_rk4_step_keep: one ts_rk4_step that writes the new state to u_next (may be
+ *   u_hat) and keeps the stage fields U1, U2, U3 (9 components) in `stages`.
+ * ts_adjoint_step: lam_hat <- (d step / d u_hat)^T lam_hat, u_hat = the state
+ *   at the start of the step, `stages` = its stage fields.
+ * ts_adjoint_window: checkpointed form.  Recomputes nsteps steps from u_start,
+ *   keeping every step's state and stage fields in `work`, then runs the nsteps
+ *   adjoint steps backwards: lam_hat enters as the cotangent of the state after
+ *   nsteps and leaves as the cotangent of u_start.
+ * ts_adjoint_work_bytes: size of `work` for nsteps (12 components per step). */
+int ts_rk4_step_keep(ts_plan* plan, const void* u_hat, void* u_next, void* stages);
+int ts_adjoint_step(ts_plan* plan, const void* u_hat, const void* stages, void* lam_hat);
+int ts_adjoint_work_bytes(const ts_plan* plan, int nsteps, size_t* bytes);
+int ts_adjoint_window(ts_plan* plan, const void* u_start, int nsteps, void* lam_hat, void* work, size_t work_bytes);
+
 /* Kernel classes of one right-hand-side evaluation, for ts_profile_read. */
 typedef enum {
   TS_KCLASS_INV_X = 0,  /* dealias + inverse FFT along x (+ vorticity) */

@@ -42,6 +42,8 @@ What it restates (file:line are paths inside anandogc/tarang ``trunk/lib``):
                                                      compute_diag_offdiag.cc:116-136,
                                                      fluid/fluid_base/force/compute_force_RBC.cc:104-150,
                                                      fluid/fluid_base/Correlation.cc:144-160
+* discrete adjoint of the FFF rotational IF-RK4 step  (no reference counterpart: the exact transpose of
+                                                     rk4_step, derived in the adjoint section below)
 
 Parity status: the transform arithmetic of the reference lives in the
 un-vendored FFTK library (no source, no version pin) and the reference ships
@@ -835,3 +837,147 @@ def rbc_temperature_ic(g: Grid, amp: float, kmax_grid: float, seed: int) -> np.n
     ph = 2 * np.pi * uniform01(seed, cnt)
     T = np.where(sel, amp * np.exp(1j * ph), 0)
     return reality_fix(g, T)
+
+
+# ----------------------------------------------------------------------------
+# discrete adjoint of the FFF IF-RK4 step (rotational form, unforced)
+#
+# The reference has no adjoint; this is the exact transpose of rk4_step above
+# (the forward it differentiates follows RK.cc:91-170), derived here:
+#
+#   rhs(U) = g(D U),  g(V) = P F[u x w],  u = I V,  w = I (iK x V)
+#
+# in the real inner product <A, B> = Re sum A conj(B) over the stored
+# half-spectrum arrays (which is also torch's convention for the gradient of a
+# real loss with respect to a complex tensor).  With c = 1 on the kz = 0 and
+# kz = Nz/2 planes and 2 elsewhere (the C2R weights), F^T = N^-3 I c^-1 and
+# I^T = N^3 c F, so
+#
+#   g'(V)^T lam = c [ F(w x mu) + iK x F(mu x u) ],   mu = I(c^-1 P lam),
+#
+# and the IF-RK4 stage recurrences are transposed stage by stage
+# (rk4_step_adjoint).  The strong reality condition is real-linear; its
+# transpose folds the Hermitian-copied half of the kz = 0 plane back onto its
+# source entries (reality_fix_adjoint).
+# ----------------------------------------------------------------------------
+def c2r_weights(g: Grid) -> np.ndarray:
+    """c(kz): 1 on the kz = 0 and kz = Nz/2 planes, 2 on the planes in between."""
+    Nz = g.N[2]
+    c = np.full(g.shape, 2.0)
+    c[:, :, 0] = 1.0
+    c[:, :, Nz // 2] = 1.0
+    return c
+
+
+def leray(g: Grid, N: np.ndarray) -> np.ndarray:
+    """P N = N - K (K.N)/K^2 (identity at K = 0); project_rhs(N) = -P N."""
+    Kx, Ky, Kz = g.K()
+    K2 = g.Ksqr()
+    d = Kx * N[0] + Ky * N[1] + Kz * N[2]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        q = np.where(K2 > 0, d / np.where(K2 > 0, K2, 1.0), 0.0)
+    return np.stack([N[0] - Kx * q, N[1] - Ky * q, N[2] - Kz * q])
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def rhs_rotational_adjoint(g: Grid, V: np.ndarray, lam: np.ndarray) -> np.ndarray:
+    """g'(V)^T lam for g(V) = P F[u x w] (the rotational right-hand side of a dealiased V)."""
+    c = c2r_weights(g)
+    u = [inverse(g, V[i]) for i in range(3)]
+    W = vorticity(g, V)
+    w = [inverse(g, W[i]) for i in range(3)]
+    Pl = leray(g, lam) / c
+    mu = [inverse(g, Pl[i]) for i in range(3)]
+    A = np.stack([forward(g, x) for x in _cross(w, mu)])
+    B = np.stack([forward(g, x) for x in _cross(mu, u)])
+    return c * (A + vorticity(g, B))
+
+
+def reality_fix_adjoint(g: Grid, A: np.ndarray) -> np.ndarray:
+    """Transpose of reality_fix (FFF): each kz = 0 entry that reality_fix overwrites with
+    conj(source) adds its conjugate to the source and becomes 0; the kz = Nz/2 plane is 0."""
+    if g.basis != "FFF":
+        raise ValueError("FFF only")
+    Nx, Ny, Nz = g.N
+    B = A.copy()
+    plane = A[:, :, 0].copy()
+    iy_minus = (-g.ky) % Ny
+    for lx in range(Nx // 2 + 1, Nx):
+        src = -g.kx[lx]
+        sel = g.ky != Ny // 2
+        B[src, iy_minus[sel], 0] += np.conj(plane[lx, sel])
+        B[lx, sel, 0] = 0
+    sel = g.ky < 0
+    B[0, iy_minus[sel], 0] += np.conj(plane[0, sel])
+    B[0, sel, 0] = 0
+    B[:, :, Nz // 2] = 0
+    return B
+
+
+def reality_fix_vec_adjoint(g: Grid, V: np.ndarray) -> np.ndarray:
+    return np.stack([reality_fix_adjoint(g, V[i]) for i in range(V.shape[0])])
+
+
+def rk4_stages(cfg: FluidConfig, U0: np.ndarray) -> list:
+    """The stage inputs [U0, U1, U2, U3] of one rk4_step (each enters rhs dealiased)."""
+    g = cfg.grid
+    if cfg.nlin_form != "rotational" or cfg.forcing is not None or g.basis != "FFF":
+        raise ValueError("adjoint: FFF, rotational form, unforced")
+    mis = g.modes_in_shell()
+    nu, dt = cfg.nu, cfg.dt
+    E = lambda A, a: exp_ksqr(g, A, -nu * a * dt)
+    R, Ud = fluid_rhs(cfg, U0, mis)
+    U1 = E(Ud + (0.5 * dt) * R, 0.5)
+    R, _ = fluid_rhs(cfg, U1, mis)
+    U2 = E(U0, 0.5) + (0.5 * dt) * R
+    R, _ = fluid_rhs(cfg, U2, mis)
+    U3 = E(E(U0, 0.5) + dt * R, 0.5)
+    return [U0, U1, U2, U3]
+
+
+def rk4_step_adjoint(cfg: FluidConfig, U0: np.ndarray, Lam: np.ndarray) -> np.ndarray:
+    """(d rk4_step / d U0)^T Lam: the stage recurrences of rk4_step transposed, last stage first.
+
+    With W_s = D g'(D U_{s-1})^T lam_s (the cotangent of stage input U_{s-1}):
+      L = RF^T Lam;  lam_4 = dt/6 L
+      A  = E1 L + E1 W_4,  lam_3 = dt/3 Eh L + dt Eh W_4
+      A += Eh W_3,         lam_2 = dt/3 Eh L + dt/2 W_3
+      A += Eh W_2,         lam_1 = dt/6 E1 L + dt/2 Eh W_2
+      result = A + W_1
+    """
+    g = cfg.grid
+    dt = cfg.dt
+    stages = rk4_stages(cfg, U0)
+    D = lambda A: dealias(g, A, cfg.dealias_mode) if cfg.dealias_mode else A
+    Eh = np.exp(-cfg.nu * 0.5 * dt * g.Ksqr())
+    E1 = Eh * Eh
+    gT = lambda s, lam: D(rhs_rotational_adjoint(g, D(stages[s]), lam))
+    L = reality_fix_vec_adjoint(g, Lam) if cfg.reality_fix else Lam.copy()
+    W = gT(3, (dt / 6) * L)
+    A = E1 * L + E1 * W
+    lam = (dt / 3) * Eh * L + dt * Eh * W
+    W = gT(2, lam)
+    A = A + Eh * W
+    lam = (dt / 3) * Eh * L + (0.5 * dt) * W
+    W = gT(1, lam)
+    A = A + Eh * W
+    lam = (dt / 6) * E1 * L + (0.5 * dt) * Eh * W
+    W = gT(0, lam)
+    return A + W
+
+
+def energy_weights(g: Grid) -> np.ndarray:
+    """Tarang FFF energy weights per stored mode: 1, and 1/2 on the kz = 0 plane."""
+    w = np.ones(g.shape)
+    w[:, :, 0] = 0.5
+    return w
+
+
+def adjoint_loss(g: Grid, U: np.ndarray, Ut: np.ndarray) -> tuple:
+    """J = 1/2 ||U - Ut||^2 in the energy norm (total_energy of the difference) and dJ/dU."""
+    w = energy_weights(g)
+    d = U - Ut
+    return float(np.sum(w * np.abs(d) ** 2)), 2.0 * w * d

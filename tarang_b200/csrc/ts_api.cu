@@ -47,7 +47,8 @@ struct ts_plan {
   cudaStream_t st = nullptr;
   void* Ucur = nullptr;
   void* tot = nullptr;
-  void* P = nullptr;  // 6 components
+  void* P = nullptr;  // nP components of transform / product work fields
+  int nP = 0;
   void* twx = nullptr;
   void* twy = nullptr;
   void* twz = nullptr;
@@ -315,6 +316,7 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   CKP(alloc(&p->Ucur, ncs * g.S * p->cb));
   CKP(alloc(&p->tot, ncs * g.S * p->cb));
   CKP(alloc(&p->P, nps * g.S * p->cb));
+  p->nP = nps;
   if (p->prec) {
     CKP(upload_twiddles<float>(g.Nx, &p->twx));
     CKP(upload_twiddles<float>(g.Ny, &p->twy));
@@ -423,7 +425,7 @@ static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in)
   a.ez = p->eax[2];
   const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
   const int nin = rot ? 6 : 3, nout = rot ? 3 : 6;
-  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, p->err_d, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, nullptr, 0.0, p->st)); }
   { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, nin, p->twy, p->st)); }
   { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->err_d, p->st)); }
   { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, nout, p->twy, p->st)); }
@@ -431,11 +433,17 @@ static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in)
   return TS_OK;
 }
 
-static int step_fff(ts_plan* p, void* U0) {
+// One IF-RK4 step from U0; stage 4 writes the new state to Uout (nullptr: in
+// place) and the reality fix is applied there.  keep != nullptr: the stage
+// fields U1, U2, U3 are written to keep (9 components) instead of the plan's
+// single stage field; stages_only: stop after stage 3.
+static int step_fff(ts_plan* p, void* U0, void* Uout = nullptr, void* keep = nullptr, bool stages_only = false) {
   const Geo& g = p->g;
+  const long long cs = 3 * g.S * (long long)p->cb;
   StageArgs a;
   memset(&a, 0, sizeof(a));
   a.U0 = U0;
+  a.Uout = Uout ? Uout : U0;
   a.Ucur = p->Ucur;
   a.tot = p->tot;
   a.nu = p->cfg.nu;
@@ -443,8 +451,9 @@ static int step_fff(ts_plan* p, void* U0) {
   a.reality = p->cfg.reality_fix;
   a.fcube = p->cfg.force_type == TS_FORCE_CARATI_ENERGY_SUPPLY ? p->fcube : nullptr;
   a.fkm = p->fkm;
-  for (int stage = 1; stage <= 4; ++stage) {
-    const void* Uin = stage == 1 ? U0 : p->Ucur;
+  for (int stage = 1; stage <= (stages_only ? 3 : 4); ++stage) {
+    const void* Uin = stage == 1 ? U0 : (keep ? (const void*)((const char*)keep + (stage - 2) * cs) : p->Ucur);
+    if (keep && stage <= 3) a.Ucur = (char*)keep + (stage - 1) * cs;
     if (a.fcube) {
       ProfScope ps(p, TS_KCLASS_OTHER);
       CK(LAUNCH(p, carati, g, Uin, p->fcube, p->fkm, p->cfg.force_inner_radius, p->cfg.force_outer_radius, p->esup,
@@ -453,9 +462,66 @@ static int step_fff(ts_plan* p, void* U0) {
     a.stage = stage;
     CKS(rhs_fff(p, Uin, MODE_STEP, a));
   }
+  if (p->cfg.reality_fix && !stages_only) {
+    ProfScope ps(p, TS_KCLASS_OTHER);
+    CK(LAUNCH(p, reality, g, a.Uout, 3, p->st));
+  }
+  return TS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// discrete adjoint of step_fff (rotational form, unforced)
+// ---------------------------------------------------------------------------
+static int adjoint_supported(ts_plan* p) {
+  if (p->cfg.basis != TS_BASIS_FFF || p->cfg.nlin_form != TS_NLIN_ROTATIONAL ||
+      p->cfg.force_type != TS_FORCE_NONE) {
+    g_last_error = "the adjoint step is implemented for FFF, rotational form, unforced plans";
+    return TS_ERR_UNSUPPORTED;
+  }
+  if (p->nP < 9) {
+    // the adjoint right-hand side transforms nine fields (u, w, and the projected cotangent)
+    CK(cudaStreamSynchronize(p->st));
+    CK(cudaFree(p->P));
+    p->P = nullptr;
+    p->nP = 0;
+    CK(cudaMalloc(&p->P, 9 * p->g.S * p->cb));
+    p->nP = 9;
+  }
+  return TS_OK;
+}
+
+// lam <- (d step / d U0)^T lam, with U0 the state at the start of the step and
+// `stages` its stage fields U1, U2, U3 (from step_fff with keep)
+static int adjoint_step_fff(ts_plan* p, const void* U0, const void* stages, void* lam) {
+  const Geo& g = p->g;
+  const long long cs = 3 * g.S * (long long)p->cb;
   if (p->cfg.reality_fix) {
     ProfScope ps(p, TS_KCLASS_OTHER);
-    CK(LAUNCH(p, reality, g, U0, 3, p->st));
+    CK(LAUNCH(p, reality_adj, g, lam, 3, p->st));
+  }
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = lam;
+  a.Uout = lam;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.nu = p->cfg.nu;
+  a.dt = p->cfg.dt;
+  a.err = p->err_d;
+  a.ex = p->eax[0];
+  a.ey = p->eax[1];
+  a.ez = p->eax[2];
+  for (int stage = 4; stage >= 1; --stage) {
+    // the stage's linearisation point: its input U_{stage-1} (dealiased on load)
+    const void* Uin = stage == 1 ? U0 : (const void*)((const char*)stages + (stage - 2) * cs);
+    const void* cot = stage == 4 ? (const void*)lam : (const void*)p->Ucur;
+    const double lsc = stage == 4 ? p->cfg.dt / 6.0 : 1.0;
+    a.stage = stage;
+    { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, 3, Uin, p->P, p->twx, cot, lsc, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, 9, p->twy, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, 3, p->P, p->twz, p->err_d, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, 6, p->twy, p->st)); }
+    { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, fwd_x, g, 3, MODE_ADJ, p->P, a, p->twx, p->st)); }
   }
   return TS_OK;
 }
@@ -524,6 +590,78 @@ int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   });
   if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
   return rc;
+}
+
+static bool aligned16(const void* q) { return ((uintptr_t)q & 15) == 0; }
+
+int ts_rk4_step_keep(ts_plan* p, const void* u_hat, void* u_next, void* stages) {
+  if (!p || !u_hat || !u_next || !stages) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  if (!is_device_ptr(u_hat) || !is_device_ptr(u_next) || !is_device_ptr(stages) || !aligned16(u_hat) ||
+      !aligned16(u_next) || !aligned16(stages)) {
+    g_last_error = "ts_rk4_step_keep: 16-byte aligned device pointers required";
+    return TS_ERR_ARG;
+  }
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
+    return TS_ERR_TIMEOUT;
+  }
+  CKS(step_fff(p, const_cast<void*>(u_hat), u_next, stages));
+  CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return TS_OK;
+}
+
+int ts_adjoint_step(ts_plan* p, const void* u_hat, const void* stages, void* lam_hat) {
+  if (!p || !u_hat || !stages || !lam_hat) return TS_ERR_ARG;
+  CKS(adjoint_supported(p));
+  if (!is_device_ptr(u_hat) || !is_device_ptr(stages) || !is_device_ptr(lam_hat) || !aligned16(lam_hat)) {
+    g_last_error = "ts_adjoint_step: device pointers required (lam_hat 16-byte aligned)";
+    return TS_ERR_ARG;
+  }
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
+    return TS_ERR_TIMEOUT;
+  }
+  CKS(adjoint_step_fff(p, u_hat, stages, lam_hat));
+  CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return TS_OK;
+}
+
+int ts_adjoint_work_bytes(const ts_plan* p, int nsteps, size_t* bytes) {
+  if (!p || nsteps < 1 || !bytes) return TS_ERR_ARG;
+  *bytes = (size_t)nsteps * 12 * (size_t)p->g.S * p->cb;
+  return TS_OK;
+}
+
+int ts_adjoint_window(ts_plan* p, const void* u_start, int nsteps, void* lam_hat, void* work, size_t work_bytes) {
+  if (!p || !u_start || !lam_hat || !work || nsteps < 1) return TS_ERR_ARG;
+  CKS(adjoint_supported(p));
+  size_t need = 0;
+  CKS(ts_adjoint_work_bytes(p, nsteps, &need));
+  if (work_bytes < need) {
+    g_last_error = "ts_adjoint_window: work buffer smaller than ts_adjoint_work_bytes";
+    return TS_ERR_ARG;
+  }
+  if (!is_device_ptr(u_start) || !is_device_ptr(lam_hat) || !is_device_ptr(work) || !aligned16(u_start) ||
+      !aligned16(lam_hat) || !aligned16(work)) {
+    g_last_error = "ts_adjoint_window: 16-byte aligned device pointers required";
+    return TS_ERR_ARG;
+  }
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
+    return TS_ERR_TIMEOUT;
+  }
+  // work slot n = [U_n (3 components), U1, U2, U3 of step n (9)]; U_0 is u_start itself
+  const size_t cs = 3 * (size_t)p->g.S * p->cb, slot = 4 * cs;
+  char* w = (char*)work;
+  auto state = [&](int n) -> void* { return n == 0 ? const_cast<void*>(u_start) : (void*)(w + n * slot); };
+  for (int n = 0; n < nsteps; ++n) {
+    const bool last = n == nsteps - 1;
+    CKS(step_fff(p, state(n), last ? nullptr : state(n + 1), w + n * slot + cs, last));
+  }
+  for (int n = nsteps - 1; n >= 0; --n) CKS(adjoint_step_fff(p, state(n), w + n * slot + cs, lam_hat));
+  CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return TS_OK;
 }
 
 int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {

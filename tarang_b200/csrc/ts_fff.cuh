@@ -186,10 +186,16 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
 // ---------------------------------------------------------------------------
 // inverse x pass, direct-load variant (one column tile per block, loads straight
 // into registers; two blocks of 256 threads per SM).  Same result as k_inv_x.
+// FORM 0: W_0..2 = D U.  FORM 1: also W_3..5 = D omega.  FORM 3 (adjoint of the
+// rotational right-hand side): also W_6..8 = lsc c^-1 P Lam, the Leray-projected
+// cotangent divided by the C2R weight c (2 on the planes 0 < kz < Nz/2, else 1).
 // ---------------------------------------------------------------------------
-template <typename T, int L, int E, int CW, bool ROT>
+__host__ __device__ constexpr int inv_x_nout(int form) { return form == 0 ? 3 : (form == 1 ? 6 : 9); }
+
+template <typename T, int L, int E, int CW, int FORM>
 __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
-    k_inv_x_ld(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw) {
+    k_inv_x_ld(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw,
+               const C<T>* __restrict__ Lam, T lsc) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
@@ -200,7 +206,8 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
   const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
   const T Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
   const long long rstride = inner;
-  const int nout = ROT ? 6 : 3;
+  constexpr int nout = inv_x_nout(FORM);
+  const T lw = (lz > 0 && 2 * lz < g.Nz) ? lsc * (T)0.5 : lsc;
   for (int f = 0; f < nout; ++f) {
     V v[E];
 #pragma unroll
@@ -208,7 +215,19 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
       const int lx = load_row<L, E>(t, s);
       const long long off = lx * rstride + col;
       V a = mk<V>(0, 0);
-      if (ok && !dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) {
+      if (FORM == 3 && f >= 6) {
+        if (ok) {
+          // (P Lam)_i = Lam_i - K_i (K . Lam) / K^2, identity at K = 0
+          const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
+          const V l0 = Lam[off], l1 = Lam[g.S + off], l2 = Lam[2 * g.S + off];
+          const T K2 = (Kx * Kx + Ky * Ky) + Kz * Kz;
+          const V d = add(add(scale(l0, Kx), scale(l1, Ky)), scale(l2, Kz));
+          const V q = K2 > (T)0 ? mk<V>(d.x / K2, d.y / K2) : mk<V>(0, 0);
+          const int i = f - 6;
+          const T Ki = i == 0 ? Kx : (i == 1 ? Ky : Kz);
+          a = scale(sub(i == 0 ? l0 : (i == 1 ? l1 : l2), scale(q, Ki)), lw);
+        }
+      } else if (ok && !dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) {
         if (f < 3) {
           a = U[f * g.S + off];
         } else {
@@ -255,8 +274,15 @@ template <int M> __host__ __device__ constexpr int zslot() { return M + M / 16 +
 // FORM 1 (rotational):    in u1..3,w1..3    -> u x w
 // FORM 2 (Boussinesq):    in u1,u2,u3,T     -> the six u_i u_j, then u1T,u2T,u3T
 //                         (compute_diag_offdiag.cc:47-136)
-__host__ __device__ constexpr int z_nin(int form) { return form == 0 ? 3 : (form == 1 ? 6 : 4); }
-__host__ __device__ constexpr int z_nout(int form) { return form == 0 ? 6 : (form == 1 ? 3 : 9); }
+// FORM 3 (adjoint of the rotational form): in u, w, mu -> mu x u, then w x mu
+__host__ __device__ constexpr int z_nin(int form) { return form == 0 ? 3 : (form == 1 ? 6 : (form == 2 ? 4 : 9)); }
+__host__ __device__ constexpr int z_nout(int form) { return form == 0 ? 6 : (form == 1 ? 3 : (form == 2 ? 9 : 6)); }
+
+// component f of a x b for real points packed two per complex (re, im independent)
+template <typename V> __device__ __forceinline__ V cross_pk(int f, const V* a, const V* b) {
+  const int i = f == 2 ? 0 : f + 1, j = f == 0 ? 2 : f - 1;
+  return mk<V>(a[i].x * b[j].x - a[j].x * b[i].x, a[i].y * b[j].y - a[j].y * b[i].y);
+}
 // factor indices (a, b) of product output f for FORM 0 / 2
 __host__ __device__ constexpr int z_pa(int f) { return f < 3 ? f : (f < 6 ? f - 3 : f - 6); }
 __host__ __device__ constexpr int z_pb(int f) { return f < 3 ? f : (f < 6 ? (f == 5 ? 0 : f - 2) : 3); }
@@ -301,7 +327,13 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
     V in[NIN];
 #pragma unroll
     for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
-    if (FORM != 1) {
+    if (FORM == 3) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        slot(f, ll)[m] = cross_pk(f, in + 6, in);
+        slot(3 + f, ll)[m] = cross_pk(f, in + 3, in + 6);
+      }
+    } else if (FORM != 1) {
 #pragma unroll
       for (int f = 0; f < NOUT; ++f)
         slot(f, ll)[m] = mk<V>(in[z_pa(f)].x * in[z_pb(f)].x, in[z_pa(f)].y * in[z_pb(f)].y);
@@ -351,6 +383,59 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 // and uses the shared-memory-slot kernel k_z_fused instead)
 template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 128; }
 
+// C2R of one line held by TPL lanes (input rows k = t + s*TPL): the pair terms
+// X[M-k] come from the partner lane by a warp shuffle, then the length-M inverse
+// FFT (forward radix schedule) leaves the packed real line in registers
+template <typename T, int M, int E, int TPL>
+__device__ __forceinline__ void zreg_inverse(const C<T>* X, bool live, int t, int partner,
+                                             const C<T>* __restrict__ tw, C<T>* xch, C<T> (&out)[E]) {
+  typedef C<T> V;
+  V a[E];
+#pragma unroll
+  for (int s = 0; s < E; ++s) a[s] = live ? X[t + s * TPL] : mk<V>(0, 0);
+  const V XM = (live && t == 0) ? X[M] : mk<V>(0, 0);
+#pragma unroll
+  for (int s = 0; s < E; ++s) {
+    // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
+    V b;
+    b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
+    b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
+    if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
+    b = conjg(b);
+    V x = a[s];
+    const int k = t + s * TPL;
+    if (k == 0) { x.y = 0; b.y = 0; }
+    out[s] = add(add(x, b), mul_i<1>(mul(conjg(tw[k]), sub(x, b))));
+  }
+  fft_regs<M, E, 1, 0, true, false>(out, t, xch, 1, 0, tw, 2);
+}
+
+// R2C of one packed real line in registers (reversed radix schedule, so the
+// inverse's output order is its input order) and the store of its M+1 rows
+template <typename T, int M, int E, int TPL>
+__device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool live, int t, int partner,
+                                                   const C<T>* __restrict__ tw, C<T>* xch) {
+  typedef C<T> V;
+  fft_regs<M, E, -1, 0, true, true>(p, t, xch, 1, 0, tw, 2);
+  // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL
+#pragma unroll
+  for (int s = 0; s < E; ++s) {
+    V zp;
+    zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
+    zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
+    if (t == 0) zp = p[(E - s) % E];
+    zp = conjg(zp);
+    const int k = t + s * TPL;
+    const V z = p[s];
+    const V o = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[k], scale(sub(z, zp), (T)0.5))));
+    if (live) Xo[k] = o;
+  }
+  if (live && t == 0) {
+    const V z = p[0], zp = conjg(p[0]);
+    Xo[M] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zp), (T)0.5))));
+  }
+}
+
 template <typename T, int NZ, int FORM>
 __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw) {
@@ -358,6 +443,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
   constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
+  static_assert(NIN <= 6, "the adjoint form runs in k_z_reg_adj");
   constexpr int LPB = zreg_threads<FORM>() / TPL;
   __shared__ __align__(16) V xch_all[LPB * LDX];
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
@@ -370,27 +456,8 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
 
   V in[NIN][E];
 #pragma unroll
-  for (int c = 0; c < NIN; ++c) {
-    const V* X = P + c * g.S + (live ? line : 0) * H;
-    V a[E];
-#pragma unroll
-    for (int s = 0; s < E; ++s) a[s] = live ? X[t + s * TPL] : mk<V>(0, 0);
-    const V XM = (live && t == 0) ? X[M] : mk<V>(0, 0);
-#pragma unroll
-    for (int s = 0; s < E; ++s) {
-      // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
-      V b;
-      b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
-      b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
-      if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
-      b = conjg(b);
-      V x = a[s];
-      const int k = t + s * TPL;
-      if (k == 0) { x.y = 0; b.y = 0; }
-      in[c][s] = add(add(x, b), mul_i<1>(mul(conjg(tw[k]), sub(x, b))));
-    }
-    fft_regs<M, E, 1, 0, true, false>(in[c], t, xch, 1, 0, tw, 2);
-  }
+  for (int c = 0; c < NIN; ++c)
+    zreg_inverse<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c]);
   // real-space products; each complex register holds two real points
   if (FORM == 1) {
 #pragma unroll
@@ -413,25 +480,59 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
         p[s] = mk<V>(in[a][s].x * in[b][s].x, in[a][s].y * in[b][s].y);
       }
     }
-    fft_regs<M, E, -1, 0, true, true>(p, t, xch, 1, 0, tw, 2);
-    // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL
-    V* Xo = P + f * g.S + (live ? line : 0) * H;
+    zreg_forward_store<T, M, E, TPL>(p, P + f * g.S + (live ? line : 0) * H, live, t, partner, tw, xch);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass of the adjoint right-hand side, register-resident (FP32, M <= 256).
+// Inputs per line: u (components 0-2), w (3-5), mu (6-8); outputs mu x u into
+// components 0-2 and w x mu into 3-5.  Staged so that at most six components
+// are live: mu and u are inverted, mu x u is transformed and stored over u,
+// then w is inverted into u's registers and w x mu is stored over w.
+// ---------------------------------------------------------------------------
+template <typename T, int NZ>
+__global__ void __launch_bounds__(128, 3) k_z_reg_adj(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw) {
+  typedef C<T> V;
+  constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
+  static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
+  constexpr int LPB = 128 / TPL;
+  __shared__ __align__(16) V xch_all[LPB * LDX];
+  const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const int lane = threadIdx.x & 31;
+  const int partner = (lane - t) + (TPL - t) % TPL;
+  const long long nlines = (long long)g.Nx * g.Ny;
+  const long long line = (long long)blockIdx.x * LPB + l;
+  const bool live = line < nlines;
+  const long long lo = (live ? line : 0) * H;
+  V* xch = xch_all + l * LDX;
+
+  V mu[3][E], w[3][E];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) zreg_inverse<T, M, E, TPL>(P + (6 + c) * g.S + lo, live, t, partner, tw, xch, mu[c]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) zreg_inverse<T, M, E, TPL>(P + c * g.S + lo, live, t, partner, tw, xch, w[c]);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    V p[E];
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      V zp;
-      zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
-      zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
-      if (t == 0) zp = p[(E - s) % E];
-      zp = conjg(zp);
-      const int k = t + s * TPL;
-      const V z = p[s];
-      const V o = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[k], scale(sub(z, zp), (T)0.5))));
-      if (live) Xo[k] = o;
+      const V a[3] = {mu[0][s], mu[1][s], mu[2][s]}, b[3] = {w[0][s], w[1][s], w[2][s]};
+      p[s] = cross_pk(f, a, b);
     }
-    if (live && t == 0) {
-      const V z = p[0], zp = conjg(p[0]);
-      Xo[M] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zp), (T)0.5))));
+    zreg_forward_store<T, M, E, TPL>(p, P + f * g.S + lo, live, t, partner, tw, xch);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) zreg_inverse<T, M, E, TPL>(P + (3 + c) * g.S + lo, live, t, partner, tw, xch, w[c]);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    V p[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const V a[3] = {w[0][s], w[1][s], w[2][s]}, b[3] = {mu[0][s], mu[1][s], mu[2][s]};
+      p[s] = cross_pk(f, a, b);
     }
+    zreg_forward_store<T, M, E, TPL>(p, P + (3 + f) * g.S + lo, live, t, partner, tw, xch);
   }
 }
 
@@ -560,9 +661,10 @@ __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, c
 // forward x pass + spectral epilogue
 // ---------------------------------------------------------------------------
 struct StageArgs {
-  void* U0;          // state (Vcopy), updated in place at stage 4
-  void* Ucur;        // stage field
-  void* tot;         // RK accumulator
+  void* U0;          // state (Vcopy); MODE_ADJ: the adjoint state Lam, overwritten at stage 1
+  void* Uout;        // MODE_STEP: where stage 4 writes the new state (U0 for an in-place step)
+  void* Ucur;        // stage field; MODE_ADJ: the next stage's cotangent lam
+  void* tot;         // RK accumulator; MODE_ADJ: the adjoint accumulator
   void* nout;        // MODE_NLIN: output N (3 comps)
   const void* Ud;    // MODE_FLUX: field whose dealiased copy multiplies N
   double* bins;      // MODE_FLUX: per-sphere accumulators (global)
@@ -579,19 +681,28 @@ struct StageArgs {
   const double* ez;
 };
 
-enum { MODE_STEP = 0, MODE_FLUX = 1, MODE_NLIN = 2 };
+enum { MODE_STEP = 0, MODE_FLUX = 1, MODE_NLIN = 2, MODE_ADJ = 3 };
 
 // Persistent over column tiles.  Thread 0 streams the product fields of a tile
 // through two TMA staging tiles (item = (tile, field); item i+2 is issued as
 // soon as every thread has read item i), and the RK state the epilogue needs
 // (U0 and tot, or the flux field) into six state tiles at tile start.
 // Shared memory: 2 product tiles + 1 exchange tile + 6 state tiles (+ flux bins).
+//
+// FORM 3 / MODE_ADJ (discrete adjoint of the rotational stage; products
+// B = F(mu x u) in fields 0-2 and A = F(w x mu) in 3-5):
+//   W = D c (A + i K x B)  = the cotangent of the stage input, and with
+//   L = Lam (state tiles 0-2), Acc = tot (tiles 3-5), lam = Ucur:
+//   stage 4: Acc = E1 L + E1 W,  lam = dt/3 Eh L + dt Eh W
+//   stage 3: Acc += Eh W,        lam = dt/3 Eh L + dt/2 W
+//   stage 2: Acc += Eh W,        lam = dt/6 E1 L + dt/2 Eh W
+//   stage 1: Lam = Acc + W
 template <typename T, int L, int E, int CW, int FORM, int MODE>
 __global__ void __launch_bounds__(CW * (L / E), 1)
     k_fwd_x(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mA,
             const __grid_constant__ CUtensorMap mB, Geo g, StageArgs a, const C<T>* __restrict__ tw) {
   typedef C<T> V;
-  constexpr int NF = FORM == 0 ? 6 : 3;
+  constexpr int NF = FORM == 1 ? 3 : 6;
   constexpr int TILE = L * CW, BR = L < 256 ? L : 256, UNITS = (int)sizeof(V) / 8;
   constexpr int NST = MODE == MODE_NLIN ? 0 : 6;
   extern __shared__ __align__(128) unsigned char smraw_[];
@@ -607,8 +718,11 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   const int ntiles = (inner + CW - 1) / CW;
   const long long rstride = inner;
   const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
-  // state tiles: [0,3) = U0 (or the flux field) from map mA, [3,6) = tot from map mB
-  const int nstate = MODE == MODE_FLUX ? 3 : (MODE == MODE_STEP ? (a.stage == 1 ? 3 : 6) : 0);
+  // state tiles: [0,3) = U0 (or the flux field) from map mA, [3,6) = tot from map mB;
+  // tiles [sfirst, nstate) are loaded
+  const int nstate = MODE == MODE_FLUX ? 3
+                     : (MODE == MODE_STEP ? (a.stage == 1 ? 3 : 6) : (MODE == MODE_ADJ ? (a.stage == 4 ? 3 : 6) : 0));
+  const int sfirst = (MODE == MODE_ADJ && a.stage == 1) ? 3 : 0;
 
   if (MODE == MODE_FLUX)
     for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x) sbins[i] = 0.0;
@@ -627,8 +741,8 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   };
   auto issue_state = [&](int tile) {
     if (nstate == 0) return;
-    mbar_expect_tx(&bar[2], (unsigned)nstate * TILE * (unsigned)sizeof(V));
-    for (int comp = 0; comp < nstate; ++comp)
+    mbar_expect_tx(&bar[2], (unsigned)(nstate - sfirst) * TILE * (unsigned)sizeof(V));
+    for (int comp = sfirst; comp < nstate; ++comp)
       for (int r0 = 0; r0 < L; r0 += BR)
         tma_load_2d(sst + comp * TILE + r0 * CW, comp < 3 ? &mA : &mB, tile * CW * UNITS, (comp % 3) * g.Nx + r0,
                     &bar[2]);
@@ -684,6 +798,14 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
             case 4: acc[1][s] = add(acc[1][s], ik(Kz, p)); acc[2][s] = add(acc[2][s], ik(Ky, p)); break;
             default: acc[2][s] = add(acc[2][s], ik(Kx, p)); acc[0][s] = add(acc[0][s], ik(Kz, p)); break;
           }
+        } else if (FORM == 3) {
+          // A_i + (i K x B)_i
+          switch (f) {
+            case 0: acc[1][s] = add(acc[1][s], ik(Kz, p)); acc[2][s] = sub(acc[2][s], ik(Ky, p)); break;
+            case 1: acc[2][s] = add(acc[2][s], ik(Kx, p)); acc[0][s] = sub(acc[0][s], ik(Kz, p)); break;
+            case 2: acc[0][s] = add(acc[0][s], ik(Ky, p)); acc[1][s] = sub(acc[1][s], ik(Kx, p)); break;
+            default: acc[f - 3][s] = add(acc[f - 3][s], p); break;
+          }
         } else {
           // N = -F[u x omega]
           if (f == 0) acc[0][s] = scale(p, (T)-1);
@@ -701,7 +823,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
       ph[2] ^= 1;
     }
     if (ok) {
-      const double exy = MODE == MODE_STEP ? a.ey[ly] * a.ez[lz] : 0.0;
+      const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
 #pragma unroll
       for (int s = 0; s < E; ++s) {
         const int lx = final_row<L, E>(t, s);
@@ -729,6 +851,35 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
           atomicAdd(&sbins[b], 2.0 * mult * re);
           continue;
         }
+        if (MODE == MODE_ADJ) {
+          const double eh = a.ex[lx] * exy;
+          const double e1 = eh * eh;
+          const T Eh = (T)eh, E1 = (T)e1;
+          const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+          const T cw = dz ? (T)0 : ((lz > 0 && 2 * lz < g.Nz) ? (T)2 : (T)1);
+          V* Lm = reinterpret_cast<V*>(a.U0);
+          V* lam = reinterpret_cast<V*>(a.Ucur);
+          V* Ac = reinterpret_cast<V*>(a.tot);
+          const V Wv[3] = {scale(N1, cw), scale(N2, cw), scale(N3, cw)};
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            const long long o = i * g.S + off;
+            const V W = Wv[i];
+            if (a.stage == 4) {
+              const V L = sst[i * TILE + so];
+              Ac[o] = add(scale(L, E1), scale(W, E1));
+              lam[o] = add(scale(L, (T)(a.dt / 3 * eh)), scale(W, (T)(a.dt * eh)));
+            } else if (a.stage == 1) {
+              Lm[o] = add(sst[(3 + i) * TILE + so], W);
+            } else {
+              const V L = sst[i * TILE + so], Acc = sst[(3 + i) * TILE + so];
+              Ac[o] = add(Acc, scale(W, Eh));
+              lam[o] = a.stage == 3 ? add(scale(L, (T)(a.dt / 3 * eh)), scale(W, (T)(0.5 * a.dt)))
+                                    : add(scale(L, (T)(a.dt / 6 * e1)), scale(W, (T)(0.5 * a.dt * eh)));
+            }
+          }
+          continue;
+        }
         // ---- MODE_STEP ----
         const T Kx = (T)Kxd;
         if (a.fcube) {
@@ -751,7 +902,6 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
         const double eh = a.ex[lx] * exy;
         const double e1 = eh * eh;
         const T Eh = (T)eh, E1 = (T)e1;
-        V* U0 = reinterpret_cast<V*>(a.U0);
         V* Uc = reinterpret_cast<V*>(a.Ucur);
         V* tot = reinterpret_cast<V*>(a.tot);
         const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
@@ -774,7 +924,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
               tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
             } else {
               const V un = add(scale(u0, E1), add(tt, scale(R, (T)((1.0 / 6) * a.dt))));
-              U0[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
+              reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
             }
           }
         }

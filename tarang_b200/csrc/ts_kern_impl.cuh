@@ -124,8 +124,8 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
   return err;
 }
 
-template <> cudaError_t Launch<T>::inv_x(const Geo& g, int rot, const void* U, void* W, const void* tw, int* err,
-                                         cudaStream_t st) {
+template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
+                                         const void* lam, double lsc, cudaStream_t st) {
   cudaError_t err_ = cudaErrorInvalidValue;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
@@ -136,18 +136,15 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int rot, const void* U, v
     const int inner = g.Ny * g.Hz;
     const size_t sm = (size_t)LL * CW * sizeof(V);
     const unsigned blocks = (unsigned)((inner + CW - 1) / CW);
-    if (rot) {
-      auto k = k_inv_x_ld<T, LL, E, CW, true>;
-      if ((err_ = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw);
-    } else {
-      auto k = k_inv_x_ld<T, LL, E, CW, false>;
-      if ((err_ = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw);
-    }
-    ++g_launches;
-    err_ = cudaGetLastError();
-    (void)err;
+    auto run = [&](auto kern) {
+      if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
+      kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc);
+      ++g_launches;
+      err_ = cudaGetLastError();
+    };
+    if (form == 0) run(k_inv_x_ld<T, LL, E, CW, 0>);
+    else if (form == 1) run(k_inv_x_ld<T, LL, E, CW, 1>);
+    else if (form == 3) run(k_inv_x_ld<T, LL, E, CW, 3>);
   });
   return err_;
 }
@@ -158,7 +155,7 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   const long long nlines = (long long)g.Nx * g.Ny;
   cudaError_t err;
-  if constexpr (M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
+  if constexpr (FORM != 3 && M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
     // FP64: bulk-copy variant (whole groups, 16-byte aligned group starts)
     constexpr int LPB = ztma_lpb<T, NZ>();
     const size_t sm = 2ull * NIN * LPB * (M + 1) * sizeof(V) + (size_t)LPB * zslot<M>() * sizeof(V) + 128;
@@ -174,7 +171,10 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   if constexpr (M % 3 != 0 && M <= 256 && std::is_same<T, float>::value) {
     // FP32: register-resident variant, lines of M/8 lanes
     constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
-    k_z_reg<T, NZ, FORM><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
+    if constexpr (FORM == 3)
+      k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
+    else
+      k_z_reg<T, NZ, FORM><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
     ++g_launches;
     return cudaGetLastError();
   }
@@ -199,7 +199,8 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, cons
     constexpr int NZ = decltype(Lc)::value;
     if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st);
     else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st);
-    else err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st);
+    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st);
+    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st);
   });
   return err;
 }
@@ -244,8 +245,8 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
   CUtensorMap mP, mA, mB;
   cudaError_t err = make_field_map(&mP, P, inner, 6LL * g.Nx, UNITS, CW, br);
   if (err != cudaSuccess) return err;
-  const void* A = MODE == MODE_FLUX ? a.Ud : (MODE == MODE_STEP ? a.U0 : P);
-  const void* B = MODE == MODE_STEP ? a.tot : P;
+  const void* A = MODE == MODE_FLUX ? a.Ud : ((MODE == MODE_STEP || MODE == MODE_ADJ) ? a.U0 : P);
+  const void* B = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.tot : P;
   if ((err = make_field_map(&mA, A, inner, 3LL * g.Nx, UNITS, CW, br)) != cudaSuccess) return err;
   if ((err = make_field_map(&mB, B, inner, 3LL * g.Nx, UNITS, CW, br)) != cudaSuccess) return err;
   auto k = k_fwd_x<T, LL, E, CW, FORM, MODE>;
@@ -255,12 +256,14 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
   return cudaGetLastError();
 }
 
-template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int rot, int mode, const void* P, const StageArgs& a,
+template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int form, int mode, const void* P, const StageArgs& a,
                                          const void* tw, cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
-    if (rot) {
+    if (form == 3) {
+      if (mode == MODE_ADJ) err = fwd_x_impl<3, MODE_ADJ, LL>(g, P, a, tw, st);
+    } else if (form == 1) {
       if (mode == MODE_STEP) err = fwd_x_impl<1, MODE_STEP, LL>(g, P, a, tw, st);
       else if (mode == MODE_FLUX) err = fwd_x_impl<1, MODE_FLUX, LL>(g, P, a, tw, st);
       else err = fwd_x_impl<1, MODE_NLIN, LL>(g, P, a, tw, st);
@@ -319,6 +322,13 @@ template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const 
 template <> cudaError_t Launch<T>::reality(const Geo& g, void* A, int ncomp, cudaStream_t st) {
   const long long n = (long long)g.Nx * g.Ny * ncomp;
   k_reality<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((V*)A, ncomp, g);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st) {
+  const long long n = (long long)g.Nx * g.Ny * ncomp;
+  k_reality_adj<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((V*)A, ncomp, g);
   ++g_launches;
   return cudaGetLastError();
 }

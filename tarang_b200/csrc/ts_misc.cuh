@@ -37,6 +37,33 @@ __global__ void k_reality(C<T>* A, int ncomp, Geo g) {
   a[((long long)lx * g.Ny + ly) * Hz + g.Nz / 2] = mk<V>(0, 0);
 }
 
+// Transpose of k_reality (FFF), in place: every kz = 0 entry that k_reality
+// overwrites with conj(source) adds its conjugate to that source and becomes 0;
+// the kz = Nz/2 plane is zeroed.  One thread per (source, copy) pair, so the
+// pairs are disjoint and no entry is both read and written by two threads.
+template <typename T>
+__global__ void k_reality_adj(C<T>* A, int ncomp, Geo g) {
+  typedef C<T> V;
+  const long long plane = (long long)g.Nx * g.Ny;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= plane * ncomp) return;
+  const int comp = (int)(e / plane);
+  const int lx = (int)((e % plane) / g.Ny), ly = (int)(e % g.Ny);
+  V* a = A + comp * g.S;
+  const int ky = kfft(ly, g.Ny);
+  const int iym = ((-ky) % g.Ny + g.Ny) % g.Ny;
+  const long long Hz = g.Hz;
+  long long cp = -1;  // the copy of this source entry, if any
+  if (lx >= 1 && 2 * lx < g.Nx && ky != g.Ny / 2) cp = ((long long)(g.Nx - lx) * g.Ny + iym) * Hz;
+  else if (lx == 0 && ky > 0 && 2 * ky < g.Ny) cp = (long long)iym * Hz;
+  if (cp >= 0) {
+    const long long so = ((long long)lx * g.Ny + ly) * Hz;
+    a[so] = add(a[so], conjg(a[cp]));
+    a[cp] = mk<V>(0, 0);
+  }
+  a[((long long)lx * g.Ny + ly) * Hz + g.Nz / 2] = mk<V>(0, 0);
+}
+
 // ---------------------------------------------------------------------------
 // Carati constant-energy-supply force (non-global alpha/beta) on the cube
 // |kx|,|ky|,kz <= km; compute_force_Carati.cc:158-205, force_alpha_beta.cc:56-85,
