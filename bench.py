@@ -114,6 +114,44 @@ def fff1024_leg(steps: int = 3, warmup: int = 2):
     return out
 
 
+def adjoint_leg(prec: str, N: int = 128, window: int = 20, reps: int = 3):
+    """Config 4: adjoint/forward cost at 128^3 (nu=5e-3, dt=1e-3, rotational, two-thirds).  Times a
+    forward step, one adjoint step (its four adjoint right-hand sides) and one checkpoint window
+    (recompute `window` steps keeping stages, then `window` adjoint steps), all with CUDA events."""
+    import torch
+    import tarang_b200 as tb
+    plan = tb.Plan(N, precision=prec, nu=5e-3, dt=1e-3, dealias="two_thirds", nlin_form="rotational")
+    plan.set_stream(torch.cuda.current_stream())
+    u = plan.field(3)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 0, 0.5, u)
+    lam = plan.field(3)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 1, 0.5, lam)
+    st = torch.empty((9,) + plan.spec_shape, dtype=u.dtype, device=u.device)
+    un = torch.empty_like(u)
+    work = torch.empty(plan.adjoint_work_bytes(window), dtype=torch.uint8, device=u.device)
+
+    def timed(fn, n):
+        for _ in range(2):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    fwd = timed(lambda: plan.rk4_step(un, 1), 10 * reps)
+    plan.rk4_step_keep(u, un, st)
+    adj = timed(lambda: plan.adjoint_step(u, st, lam), 10 * reps)
+    win = timed(lambda: plan.adjoint_window(u, window, lam, work), reps)
+    plan.close()
+    return {"forward_step_ms": fwd, "adjoint_step_ms": adj, "adjoint_over_forward": adj / fwd,
+            "window_ms": win, "window_steps": window,
+            "adjoint_with_recompute_over_forward": win / (window * fwd)}
+
+
 def workload(N):
     return {"workload": f"FFF {N}^3 forced isotropic turbulence (Carati energy supply shell 3, eps=0.1), "
                         f"nu=1e-3, dt=5e-4, IC k^4 exp(-2(k/4)^2) E=0.5 seed 0",
@@ -464,6 +502,7 @@ def main():
                                      "timing": "wall clock around synchronised graph launches, max over ranks"}
         if world == 1:
             extras["fff1024_f32"] = fff1024_leg()
+            extras["adjoint_128"] = {"f64": adjoint_leg("f64"), "f32": adjoint_leg("f32")}
         if rank == 0 and world == 1:
             v, n, el = cpu_baseline_oracle(N)
             from oracle import tarang_ref as R

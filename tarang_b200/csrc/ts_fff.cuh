@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
     V in[NIN];
 #pragma unroll
     for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
-    if (FORM == 3) {
+    if constexpr (FORM == 3) {
 #pragma unroll
       for (int f = 0; f < 3; ++f) {
         slot(f, ll)[m] = cross_pk(f, in + 6, in);
@@ -866,16 +866,16 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
             const long long o = i * g.S + off;
             const V W = Wv[i];
             if (a.stage == 4) {
-              const V L = sst[i * TILE + so];
-              Ac[o] = add(scale(L, E1), scale(W, E1));
-              lam[o] = add(scale(L, (T)(a.dt / 3 * eh)), scale(W, (T)(a.dt * eh)));
+              const V Lv = sst[i * TILE + so];
+              Ac[o] = add(scale(Lv, E1), scale(W, E1));
+              lam[o] = add(scale(Lv, (T)(a.dt / 3 * eh)), scale(W, (T)(a.dt * eh)));
             } else if (a.stage == 1) {
               Lm[o] = add(sst[(3 + i) * TILE + so], W);
             } else {
-              const V L = sst[i * TILE + so], Acc = sst[(3 + i) * TILE + so];
+              const V Lv = sst[i * TILE + so], Acc = sst[(3 + i) * TILE + so];
               Ac[o] = add(Acc, scale(W, Eh));
-              lam[o] = a.stage == 3 ? add(scale(L, (T)(a.dt / 3 * eh)), scale(W, (T)(0.5 * a.dt)))
-                                    : add(scale(L, (T)(a.dt / 6 * e1)), scale(W, (T)(0.5 * a.dt * eh)));
+              lam[o] = a.stage == 3 ? add(scale(Lv, (T)(a.dt / 3 * eh)), scale(W, (T)(0.5 * a.dt)))
+                                    : add(scale(Lv, (T)(a.dt / 6 * e1)), scale(W, (T)(0.5 * a.dt * eh)));
             }
           }
           continue;

@@ -127,6 +127,28 @@ class Plan:
     def rk4_step(self, u, nsteps: int = 1):
         L.check(self.lib.ts_rk4_step(self.h, _ptr(u), nsteps), "ts_rk4_step")
 
+    def rk4_step_keep(self, u, u_next, stages):
+        """One step u -> u_next (may be u) keeping the stage fields U1, U2, U3 in stages (9 components)."""
+        L.check(self.lib.ts_rk4_step_keep(self.h, _ptr(u), _ptr(u_next), _ptr(stages)), "ts_rk4_step_keep")
+
+    def adjoint_step(self, u, stages, lam):
+        """lam <- (d step / d u)^T lam for the step from u whose stage fields are `stages`."""
+        L.check(self.lib.ts_adjoint_step(self.h, _ptr(u), _ptr(stages), _ptr(lam)), "ts_adjoint_step")
+        return lam
+
+    def adjoint_work_bytes(self, nsteps: int) -> int:
+        b = ctypes.c_size_t()
+        L.check(self.lib.ts_adjoint_work_bytes(self.h, nsteps, ctypes.byref(b)), "ts_adjoint_work_bytes")
+        return b.value
+
+    def adjoint_window(self, u_start, nsteps: int, lam, work):
+        """Recompute nsteps steps from u_start (states and stages kept in `work`), then map lam, the
+        cotangent of the state after nsteps, to the cotangent of u_start (in place)."""
+        nbytes = work.numel() * work.element_size()
+        L.check(self.lib.ts_adjoint_window(self.h, _ptr(u_start), nsteps, _ptr(lam), _ptr(work), nbytes),
+                "ts_adjoint_window")
+        return lam
+
     def rk4_step_rbc(self, u, T, nsteps: int = 1):
         L.check(self.lib.ts_rk4_step_rbc(self.h, _ptr(u), _ptr(T), nsteps), "ts_rk4_step_rbc")
 

@@ -231,3 +231,30 @@ def test_rbc_linear_stability():
         out[Ra] = R.total_energy_scalar(g, T) / E0
     assert out[1e3] < 0.9
     assert out[1e5] > 1.1
+
+
+# ---------------------------------------------------------------------------
+# discrete adjoint: <Phi'(U) d, lam> = <d, Phi'(U)^T lam> with Phi' from central
+# differences of the oracle step (16^3, both reality-fix settings)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("reality", [False, True])
+def test_adjoint_dot_product(reality):
+    g = R.Grid((16, 16, 16))
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    cfg = R.FluidConfig(g, nu=0.01, dt=5e-2, dealias_mode=2, nlin_form="rotational", reality_fix=reality)
+    rng = np.random.default_rng(7)
+    rnd = lambda: rng.standard_normal((3,) + g.shape) + 1j * rng.standard_normal((3,) + g.shape)
+    ip = lambda a, b: float(np.real(np.sum(a * np.conj(b))))
+    d, lam, eps = rnd(), rnd(), 1e-6
+    jd = (R.rk4_step(cfg, V + eps * d) - R.rk4_step(cfg, V - eps * d)) / (2 * eps)
+    lhs, rhs = ip(jd, lam), ip(d, R.rk4_step_adjoint(cfg, V, lam))
+    assert abs(lhs - rhs) < 1e-8 * abs(lhs)
+
+
+def test_reality_fix_adjoint_is_transpose():
+    g = R.Grid((16, 32, 16))
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((3,) + g.shape) + 1j * rng.standard_normal((3,) + g.shape)
+    B = rng.standard_normal((3,) + g.shape) + 1j * rng.standard_normal((3,) + g.shape)
+    ip = lambda a, b: float(np.real(np.sum(a * np.conj(b))))
+    assert abs(ip(R.reality_fix_vec(g, A), B) - ip(A, R.reality_fix_vec_adjoint(g, B))) < 1e-12 * abs(ip(A, B)) + 1e-9
