@@ -32,16 +32,18 @@ struct Geo {
 // w = b, b + G, ... (w -> field, column tile, outer index); while item w is
 // transformed (registers + exchange tile) the tile of its next item streams
 // into the other staging tile with cp.async.
-// Shared memory: 2 staging tiles + 1 exchange tile of L x CW complex.
+// Shared memory: 2 staging tiles + 1 exchange tile of L x CW complex (NT = 3),
+// or 2 staging tiles with the consumed one doubling as the exchange tile
+// (NT = 2: wider column tiles fit, e.g. 8 columns at L = 1024 in FP32).
 // ---------------------------------------------------------------------------
-template <typename T, int L, int E, int CW, int DIR>
+template <typename T, int L, int E, int CW, int DIR, int NT = 3>
 __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     k_strided_fft(C<T>* __restrict__ data, int nf, long long fstride, int inner, long long rstride,
                   long long ostride, int nouter, const C<T>* __restrict__ tw) {
   typedef C<T> V;
+  static_assert(NT == 2 || NT == 3, "two or three tiles");
   extern __shared__ __align__(16) unsigned char smraw[];
   V* stage = reinterpret_cast<V*>(smraw);
-  V* xch = stage + 2 * L * CW;
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int ntx = (inner + CW - 1) / CW;
   const long long nwork = (long long)nf * ntx * nouter;
@@ -81,7 +83,10 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     const V* st = stage + buf * L * CW + c;
 #pragma unroll
     for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
-    fft_regs<L, E, DIR>(v, t, xch, CW, c, tw, 1);
+    // each thread read back only what it staged itself; the barrier is for the
+    // exchange writes into the consumed tile (NT = 2)
+    if (NT == 2) __syncthreads();
+    fft_regs<L, E, DIR>(v, t, NT == 2 ? stage + buf * L * CW : stage + 2 * L * CW, CW, c, tw, 1);
     if (ok) {
 #pragma unroll
       for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
@@ -683,6 +688,149 @@ struct StageArgs {
 
 enum { MODE_STEP = 0, MODE_FLUX = 1, MODE_NLIN = 2, MODE_ADJ = 3 };
 
+// Assembly of the stage's spectral vector from forward-transformed product f
+// (p already scaled by 1/(Nx Ny Nz)):
+//   FORM 0: N_i = sum_j i K_j F[u_i u_j]  (compute_diag_offdiag.cc:47-98)
+//   FORM 1: N = -F[u x omega]
+//   FORM 3: A_i + (i K x B)_i  (adjoint; B = products 0-2, A = products 3-5)
+template <int FORM, typename V, typename S>
+__device__ __forceinline__ void accum_product(int f, V p, S Kx, S Ky, S Kz, V& a0, V& a1, V& a2) {
+  if (FORM == 0) {
+    switch (f) {
+      case 0: a0 = add(a0, ik(Kx, p)); break;
+      case 1: a1 = add(a1, ik(Ky, p)); break;
+      case 2: a2 = add(a2, ik(Kz, p)); break;
+      case 3: a0 = add(a0, ik(Ky, p)); a1 = add(a1, ik(Kx, p)); break;
+      case 4: a1 = add(a1, ik(Kz, p)); a2 = add(a2, ik(Ky, p)); break;
+      default: a2 = add(a2, ik(Kx, p)); a0 = add(a0, ik(Kz, p)); break;
+    }
+  } else if (FORM == 3) {
+    switch (f) {
+      case 0: a1 = add(a1, ik(Kz, p)); a2 = sub(a2, ik(Ky, p)); break;
+      case 1: a2 = add(a2, ik(Kx, p)); a0 = sub(a0, ik(Kz, p)); break;
+      case 2: a0 = add(a0, ik(Ky, p)); a1 = sub(a1, ik(Kx, p)); break;
+      case 3: a0 = add(a0, p); break;
+      case 4: a1 = add(a1, p); break;
+      default: a2 = add(a2, p); break;
+    }
+  } else {
+    if (f == 0) a0 = scale(p, (S)-1);
+    else if (f == 1) a1 = scale(p, (S)-1);
+    else a2 = scale(p, (S)-1);
+  }
+}
+
+// Per-mode epilogue of a right-hand side at spectral element (lx, ly, lz),
+// linear offset `off` in a component.  N1..N3 = the assembled vector; the
+// state the mode reads comes from st0[i * sstr] (U0 / Lam / the flux field)
+// and st1[i * sstr] (tot / the adjoint accumulator), i = component; the
+// fused x kernel passes its shared-memory state tiles, the elementwise
+// epilogue kernel the global arrays.  exy = ey[ly] ez[lz] (MODE_STEP, MODE_ADJ).
+template <typename T, int MODE>
+__device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, int lx, int ly, int lz,
+                                              long long off, double exy, C<T> N1, C<T> N2, C<T> N3,
+                                              const C<T>* st0, const C<T>* st1, long long sstr, double* sbins) {
+  typedef C<T> V;
+  const int kx = kfft(lx, g.Nx), ky = kfft(ly, g.Ny);
+  const double Kxd = kx * g.kf[0], Kyd = ky * g.kf[1], Kzd = lz * g.kf[2];
+  if (MODE == MODE_NLIN) {
+    V* no = reinterpret_cast<V*>(a.nout);
+    no[off] = N1; no[g.S + off] = N2; no[2 * g.S + off] = N3;
+    return;
+  }
+  if (MODE == MODE_FLUX) {
+    // contribution 2 mult Re(N . conj(D(U))) to the first sphere with |K| <= R
+    if (dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) return;
+    const V u1 = st0[0], u2 = st0[sstr], u3 = st0[2 * sstr];
+    double re = (double)N1.x * u1.x + (double)N1.y * u1.y + (double)N2.x * u2.x + (double)N2.y * u2.y +
+                (double)N3.x * u3.x + (double)N3.y * u3.y;
+    double mult = lz > 0 ? 1.0 : 0.5;
+    if (kx == g.Nx / 2 || (ky == g.Ny / 2 && g.Ny > 1)) mult *= 2;
+    const double Kmag = sqrt((Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd);
+    int b = 0;
+    while (b < a.nradii && Kmag > a.radii[b]) ++b;
+    atomicAdd(&sbins[b], 2.0 * mult * re);
+    return;
+  }
+  if (MODE == MODE_ADJ) {
+    const double eh = a.ex[lx] * exy;
+    const double e1 = eh * eh;
+    const T Eh = (T)eh, E1 = (T)e1;
+    const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+    const T cw = dz ? (T)0 : ((lz > 0 && 2 * lz < g.Nz) ? (T)2 : (T)1);
+    V* Lm = reinterpret_cast<V*>(a.U0);
+    V* lam = reinterpret_cast<V*>(a.Ucur);
+    V* Ac = reinterpret_cast<V*>(a.tot);
+    const V Wv[3] = {scale(N1, cw), scale(N2, cw), scale(N3, cw)};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const long long o = i * g.S + off;
+      const V W = Wv[i];
+      if (a.stage == 4) {
+        const V Lv = st0[i * sstr];
+        Ac[o] = add(scale(Lv, E1), scale(W, E1));
+        lam[o] = add(scale(Lv, (T)(a.dt / 3 * eh)), scale(W, (T)(a.dt * eh)));
+      } else if (a.stage == 1) {
+        Lm[o] = add(st1[i * sstr], W);
+      } else {
+        const V Lv = st0[i * sstr], Acc = st1[i * sstr];
+        Ac[o] = add(Acc, scale(W, Eh));
+        lam[o] = a.stage == 3 ? add(scale(Lv, (T)(a.dt / 3 * eh)), scale(W, (T)(0.5 * a.dt)))
+                              : add(scale(Lv, (T)(a.dt / 6 * e1)), scale(W, (T)(0.5 * a.dt * eh)));
+      }
+    }
+    return;
+  }
+  // ---- MODE_STEP ----
+  const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+  if (a.fcube) {
+    const int km = a.fkm;
+    if (abs(kx) <= km && abs(ky) <= km && lz <= km) {
+      const V* fc = reinterpret_cast<const V*>(a.fcube);
+      const int n = 2 * km + 1;
+      const long long fo = ((long long)(kx + km) * n + (ky + km)) * (km + 1) + lz;
+      const long long fs = (long long)n * n * (km + 1);
+      N1 = sub(N1, fc[fo]); N2 = sub(N2, fc[fs + fo]); N3 = sub(N3, fc[2 * fs + fo]);  // Add_force
+    }
+  }
+  // Leray projection: p = (i K . N)/K^2, p(0)=0; N <- -(N + i K p)
+  const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+  const V div = add(add(ik(Kx, N1), ik(Ky, N2)), ik(Kz, N3));
+  const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+  const V Rv[3] = {scale(add(N1, ik(Kx, pr)), (T)-1), scale(add(N2, ik(Ky, pr)), (T)-1),
+                   scale(add(N3, ik(Kz, pr)), (T)-1)};
+  // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
+  const double eh = a.ex[lx] * exy;
+  const double e1 = eh * eh;
+  const T Eh = (T)eh, E1 = (T)e1;
+  V* Uc = reinterpret_cast<V*>(a.Ucur);
+  V* tot = reinterpret_cast<V*>(a.tot);
+  const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+  // IF-RK4 stage update (RK.cc:91-170 with Single_time_step / Compute_RK4_parts)
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const long long o = i * g.S + off;
+    const V R = Rv[i];
+    const V u0 = st0[i * sstr];
+    if (a.stage == 1) {
+      Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+      tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+    } else {
+      const V tt = st1[i * sstr];
+      if (a.stage == 2) {
+        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+        tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else if (a.stage == 3) {
+        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+        tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else {
+        const V un = add(scale(u0, E1), add(tt, scale(R, (T)((1.0 / 6) * a.dt))));
+        reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
+      }
+    }
+  }
+}
+
 // Persistent over column tiles.  Thread 0 streams the product fields of a tile
 // through two TMA staging tiles (item = (tile, field); item i+2 is issued as
 // soon as every thread has read item i), and the RK state the epilogue needs
@@ -788,30 +936,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
         const int lx = final_row<L, E>(t, s);
         const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
         const V p = scale(v[s], inv);
-        if (FORM == 0) {
-          // N_i = sum_j i K_j F[u_i u_j]  (compute_diag_offdiag.cc:47-98)
-          switch (f) {
-            case 0: acc[0][s] = add(acc[0][s], ik(Kx, p)); break;
-            case 1: acc[1][s] = add(acc[1][s], ik(Ky, p)); break;
-            case 2: acc[2][s] = add(acc[2][s], ik(Kz, p)); break;
-            case 3: acc[0][s] = add(acc[0][s], ik(Ky, p)); acc[1][s] = add(acc[1][s], ik(Kx, p)); break;
-            case 4: acc[1][s] = add(acc[1][s], ik(Kz, p)); acc[2][s] = add(acc[2][s], ik(Ky, p)); break;
-            default: acc[2][s] = add(acc[2][s], ik(Kx, p)); acc[0][s] = add(acc[0][s], ik(Kz, p)); break;
-          }
-        } else if (FORM == 3) {
-          // A_i + (i K x B)_i
-          switch (f) {
-            case 0: acc[1][s] = add(acc[1][s], ik(Kz, p)); acc[2][s] = sub(acc[2][s], ik(Ky, p)); break;
-            case 1: acc[2][s] = add(acc[2][s], ik(Kx, p)); acc[0][s] = sub(acc[0][s], ik(Kz, p)); break;
-            case 2: acc[0][s] = add(acc[0][s], ik(Ky, p)); acc[1][s] = sub(acc[1][s], ik(Kx, p)); break;
-            default: acc[f - 3][s] = add(acc[f - 3][s], p); break;
-          }
-        } else {
-          // N = -F[u x omega]
-          if (f == 0) acc[0][s] = scale(p, (T)-1);
-          else if (f == 1) acc[1][s] = scale(p, (T)-1);
-          else acc[2][s] = scale(p, (T)-1);
-        }
+        accum_product<FORM>(f, p, Kx, Ky, Kz, acc[0][s], acc[1][s], acc[2][s]);
       }
     }
     if (nstate) {
@@ -829,109 +954,51 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
         const int lx = final_row<L, E>(t, s);
         const long long off = lx * rstride + col;
         const int so = lx * CW + c;
-        const int kx = kfft(lx, g.Nx);
-        const double Kxd = kx * g.kf[0];
-        V N1 = acc[0][s], N2 = acc[1][s], N3 = acc[2][s];
-        if (MODE == MODE_NLIN) {
-          V* no = reinterpret_cast<V*>(a.nout);
-          no[off] = N1; no[g.S + off] = N2; no[2 * g.S + off] = N3;
-          continue;
-        }
-        if (MODE == MODE_FLUX) {
-          // contribution 2 mult Re(N . conj(D(U))) to the first sphere with |K| <= R
-          if (dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) continue;
-          const V u1 = sst[so], u2 = sst[TILE + so], u3 = sst[2 * TILE + so];
-          double re = (double)N1.x * u1.x + (double)N1.y * u1.y + (double)N2.x * u2.x + (double)N2.y * u2.y +
-                      (double)N3.x * u3.x + (double)N3.y * u3.y;
-          double mult = lz > 0 ? 1.0 : 0.5;
-          if (kx == g.Nx / 2 || (ky == g.Ny / 2 && g.Ny > 1)) mult *= 2;
-          const double Kmag = sqrt((Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd);
-          int b = 0;
-          while (b < a.nradii && Kmag > a.radii[b]) ++b;
-          atomicAdd(&sbins[b], 2.0 * mult * re);
-          continue;
-        }
-        if (MODE == MODE_ADJ) {
-          const double eh = a.ex[lx] * exy;
-          const double e1 = eh * eh;
-          const T Eh = (T)eh, E1 = (T)e1;
-          const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
-          const T cw = dz ? (T)0 : ((lz > 0 && 2 * lz < g.Nz) ? (T)2 : (T)1);
-          V* Lm = reinterpret_cast<V*>(a.U0);
-          V* lam = reinterpret_cast<V*>(a.Ucur);
-          V* Ac = reinterpret_cast<V*>(a.tot);
-          const V Wv[3] = {scale(N1, cw), scale(N2, cw), scale(N3, cw)};
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            const long long o = i * g.S + off;
-            const V W = Wv[i];
-            if (a.stage == 4) {
-              const V Lv = sst[i * TILE + so];
-              Ac[o] = add(scale(Lv, E1), scale(W, E1));
-              lam[o] = add(scale(Lv, (T)(a.dt / 3 * eh)), scale(W, (T)(a.dt * eh)));
-            } else if (a.stage == 1) {
-              Lm[o] = add(sst[(3 + i) * TILE + so], W);
-            } else {
-              const V Lv = sst[i * TILE + so], Acc = sst[(3 + i) * TILE + so];
-              Ac[o] = add(Acc, scale(W, Eh));
-              lam[o] = a.stage == 3 ? add(scale(Lv, (T)(a.dt / 3 * eh)), scale(W, (T)(0.5 * a.dt)))
-                                    : add(scale(Lv, (T)(a.dt / 6 * e1)), scale(W, (T)(0.5 * a.dt * eh)));
-            }
-          }
-          continue;
-        }
-        // ---- MODE_STEP ----
-        const T Kx = (T)Kxd;
-        if (a.fcube) {
-          const int km = a.fkm;
-          if (abs(kx) <= km && abs(ky) <= km && lz <= km) {
-            const V* fc = reinterpret_cast<const V*>(a.fcube);
-            const int n = 2 * km + 1;
-            const long long fo = ((long long)(kx + km) * n + (ky + km)) * (km + 1) + lz;
-            const long long fs = (long long)n * n * (km + 1);
-            N1 = sub(N1, fc[fo]); N2 = sub(N2, fc[fs + fo]); N3 = sub(N3, fc[2 * fs + fo]);  // Add_force
-          }
-        }
-        // Leray projection: p = (i K . N)/K^2, p(0)=0; N <- -(N + i K p)
-        const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
-        const V div = add(add(ik(Kx, N1), ik(Ky, N2)), ik(Kz, N3));
-        const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
-        const V Rv[3] = {scale(add(N1, ik(Kx, pr)), (T)-1), scale(add(N2, ik(Ky, pr)), (T)-1),
-                         scale(add(N3, ik(Kz, pr)), (T)-1)};
-        // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
-        const double eh = a.ex[lx] * exy;
-        const double e1 = eh * eh;
-        const T Eh = (T)eh, E1 = (T)e1;
-        V* Uc = reinterpret_cast<V*>(a.Ucur);
-        V* tot = reinterpret_cast<V*>(a.tot);
-        const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
-        // IF-RK4 stage update (RK.cc:91-170 with Single_time_step / Compute_RK4_parts)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const long long o = i * g.S + off;
-          const V R = Rv[i];
-          const V u0 = sst[i * TILE + so];
-          if (a.stage == 1) {
-            Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-            tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
-          } else {
-            const V tt = sst[(3 + i) * TILE + so];
-            if (a.stage == 2) {
-              Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-              tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
-            } else if (a.stage == 3) {
-              Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-              tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
-            } else {
-              const V un = add(scale(u0, E1), add(tt, scale(R, (T)((1.0 / 6) * a.dt))));
-              reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
-            }
-          }
-        }
+        spec_epilogue<T, MODE>(g, a, lx, ly, lz, off, exy, acc[0][s], acc[1][s], acc[2][s], sst + so,
+                               sst + 3 * TILE + so, TILE, sbins);
       }
     }
     // the next tile's state load overwrites the state tiles
     __syncthreads();
+  }
+  if (MODE == MODE_FLUX) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x)
+      if (sbins[i] != 0.0) atomicAdd(&a.bins[i], sbins[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise spectral epilogue, used where the fused x kernel's column tiles
+// would have rows narrower than 64 bytes (FP32 and FP64 at Nx >= 512): the NF
+// product fields have already been forward-transformed along x in place
+// (k_strided_fft); one thread per spectral element, every array access
+// coalesced.  Same arithmetic as k_fwd_x's epilogue (spec_epilogue).
+// ---------------------------------------------------------------------------
+template <typename T, int FORM, int MODE>
+__global__ void __launch_bounds__(256) k_spec_epi(const C<T>* __restrict__ P, Geo g, StageArgs a) {
+  typedef C<T> V;
+  constexpr int NF = FORM == 1 ? 3 : 6;
+  extern __shared__ double sbins[];  // MODE_FLUX: per-sphere partial sums
+  if (MODE == MODE_FLUX) {
+    for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x) sbins[i] = 0.0;
+    __syncthreads();
+  }
+  const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
+  const V* st0 = reinterpret_cast<const V*>(MODE == MODE_FLUX ? a.Ud : a.U0);
+  const V* st1 = reinterpret_cast<const V*>(a.tot);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]), Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
+    V a0 = mk<V>(0, 0), a1 = mk<V>(0, 0), a2 = mk<V>(0, 0);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) accum_product<FORM>(f, scale(P[f * g.S + e], inv), Kx, Ky, Kz, a0, a1, a2);
+    const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
+    spec_epilogue<T, MODE>(g, a, lx, ly, lz, e, exy, a0, a1, a2, st0 ? st0 + e : nullptr,
+                           st1 ? st1 + e : nullptr, g.S, sbins);
   }
   if (MODE == MODE_FLUX) {
     __syncthreads();

@@ -32,7 +32,7 @@ def setup(N, prec="f64", nu=0.01, dt=1e-2, reality=True):
 
 
 @pytest.mark.parametrize("reality", [True, False])
-@pytest.mark.parametrize("N", [32, (32, 16, 64)])
+@pytest.mark.parametrize("N", [32, (32, 16, 64), (512, 16, 32)])
 def test_adjoint_step_matches_oracle(cuda, N, reality):
     import torch
     g, cfg, plan = setup(N, reality=reality)

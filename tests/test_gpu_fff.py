@@ -213,3 +213,24 @@ def test_rk4_long_axes(cuda, prec, N):
     plan.rk4_step(u, 1)
     torch.cuda.synchronize()
     assert rel(u.cpu().numpy().astype(np.complex128), W) < (1e-12 if prec == "f64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_nlin_and_flux_long_x(cuda, prec):
+    """Nx = 512 runs the split x pass (strided FFT + elementwise epilogue) in every mode."""
+    import torch
+    N = (512, 16, 32)
+    g = R.Grid(N)
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    plan = plan_for(N, precision=prec, dealias="two_thirds")
+    dt = torch.complex128 if prec == "f64" else torch.complex64
+    tol = 1e-12 if prec == "f64" else 2e-5
+    u = torch.from_numpy(V.copy()).to(cuda).to(dt)
+    out = plan.field(3)
+    plan.nlin(u, out)
+    torch.cuda.synchronize()
+    assert rel(to_np(out).astype(np.complex128), R.nlin_conservative(g, R.dealias(g, V, 2))) < tol
+    radii = [0.0, 2.0, 4.0, 8.0, 1e9]
+    Pi = plan.flux(u, radii)
+    ref = R.flux_one_pass(g, V, radii, 2)
+    assert np.max(np.abs(Pi - ref)) < tol * 10 * max(1.0, np.max(np.abs(ref)))
