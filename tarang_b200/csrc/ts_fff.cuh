@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 }
 
 // ---------------------------------------------------------------------------
-// z pass, register-resident variant (M = Nz/2 <= 256): one line per group of
+// z pass, register-resident variant (M = Nz/2 <= 512): one line per group of
 // TPL = M/8 consecutive lanes, 8 elements per thread.  The inverse transform
 // (forward radix schedule) leaves every component's real line in registers in
 // the order the forward transform with the reversed schedule expects, so the
@@ -389,8 +389,10 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 128; }
 
 // C2R of one line held by TPL lanes (input rows k = t + s*TPL): the pair terms
-// X[M-k] come from the partner lane by a warp shuffle, then the length-M inverse
-// FFT (forward radix schedule) leaves the packed real line in registers
+// X[M-k] come from the partner lane by a warp shuffle (TPL <= 32) or straight
+// from global memory (a line spread over several warps; the second read of the
+// line hits L1), then the length-M inverse FFT (forward radix schedule) leaves
+// the packed real line in registers
 template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_inverse(const C<T>* X, bool live, int t, int partner,
                                              const C<T>* __restrict__ tw, C<T>* xch, C<T> (&out)[E]) {
@@ -403,9 +405,13 @@ __device__ __forceinline__ void zreg_inverse(const C<T>* X, bool live, int t, in
   for (int s = 0; s < E; ++s) {
     // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
     V b;
-    b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
-    b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
-    if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
+    if constexpr (TPL <= 32) {
+      b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
+      b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
+      if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
+    } else {
+      b = live ? X[M - (t + s * TPL)] : mk<V>(0, 0);
+    }
     b = conjg(b);
     V x = a[s];
     const int k = t + s * TPL;
@@ -422,13 +428,23 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
                                                    const C<T>* __restrict__ tw, C<T>* xch) {
   typedef C<T> V;
   fft_regs<M, E, -1, 0, true, true>(p, t, xch, 1, 0, tw, 2);
-  // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL
+  // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL.
+  // A line spread over several warps swaps the pair terms through its exchange line.
+  if constexpr (TPL > 32) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) xch[prow<true>(t + s * TPL)] = p[s];
+    __syncthreads();
+  }
 #pragma unroll
   for (int s = 0; s < E; ++s) {
     V zp;
-    zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
-    zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
-    if (t == 0) zp = p[(E - s) % E];
+    if constexpr (TPL <= 32) {
+      zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
+      zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
+      if (t == 0) zp = p[(E - s) % E];
+    } else {
+      zp = xch[prow<true>((M - (t + s * TPL)) % M)];
+    }
     zp = conjg(zp);
     const int k = t + s * TPL;
     const V z = p[s];
@@ -439,6 +455,7 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
     const V z = p[0], zp = conjg(p[0]);
     Xo[M] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zp), (T)0.5))));
   }
+  if constexpr (TPL > 32) __syncthreads();  // the exchange line is reused next
 }
 
 template <typename T, int NZ, int FORM>
@@ -446,7 +463,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
-  static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
+  static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   static_assert(NIN <= 6, "the adjoint form runs in k_z_reg_adj");
   constexpr int LPB = zreg_threads<FORM>() / TPL;
@@ -490,7 +507,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 3)
 }
 
 // ---------------------------------------------------------------------------
-// z pass of the adjoint right-hand side, register-resident (FP32, M <= 256).
+// z pass of the adjoint right-hand side, register-resident (FP32, M <= 512).
 // Inputs per line: u (components 0-2), w (3-5), mu (6-8); outputs mu x u into
 // components 0-2 and w x mu into 3-5.  Staged so that at most six components
 // are live: mu and u are inverted, mu x u is transformed and stored over u,
@@ -500,7 +517,7 @@ template <typename T, int NZ>
 __global__ void __launch_bounds__(128, 3) k_z_reg_adj(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
-  static_assert(TPL >= 1 && TPL <= 32, "line group must fit in a warp");
+  static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int LPB = 128 / TPL;
   __shared__ __align__(16) V xch_all[LPB * LDX];
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;

@@ -142,3 +142,21 @@ def test_adjoint_config4_128(cuda):
     x = u0.to(torch.complex64).requires_grad_(True)
     tb.energy_norm_loss(tb.rk4_evolve(x, p32, 200, 20), tgt.to(torch.complex64)).backward()
     assert rel(np_(x.grad).astype(np.complex128), np_(G64)) < 1e-4
+
+
+@pytest.mark.parametrize("N", [(16, 32, 1024), (1024, 16, 32)])
+def test_adjoint_step_f32_long_axes(cuda, N):
+    """FP32 adjoint on 1024-point axes (two-warp z lines, split x pass) against the FP64 oracle."""
+    import torch
+    g, cfg, _ = setup(N)
+    _, _, plan = setup(N, prec="f32")
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    rng = np.random.default_rng(11)
+    Lam = rng.standard_normal((3,) + g.shape) + 1j * rng.standard_normal((3,) + g.shape)
+    u = torch.from_numpy(V.copy()).to(cuda).to(torch.complex64)
+    st = torch.empty((9,) + g.shape, dtype=u.dtype, device=cuda)
+    plan.rk4_step_keep(u, torch.empty_like(u), st)
+    lam = torch.from_numpy(Lam.copy()).to(cuda).to(torch.complex64)
+    plan.adjoint_step(u, st, lam)
+    torch.cuda.synchronize()
+    assert rel(np_(lam).astype(np.complex128), R.rk4_step_adjoint(cfg, V, Lam)) < 1e-4

@@ -198,15 +198,16 @@ def test_host_pointer_step_matches_device(cuda):
     assert rel(host, to_np(dev)) == 0.0
 
 
+@pytest.mark.parametrize("form", ["rotational", "conservative"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("N", [(1024, 16, 32), (16, 1024, 32), (32, 16, 1024), (512, 32, 16)])
-def test_rk4_long_axes(cuda, prec, N):
+def test_rk4_long_axes(cuda, prec, N, form):
     """1024- and 512-point axes (their own tile widths and kernel variants) against the oracle."""
     import torch
     g = R.Grid(N)
     V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
-    cfg = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=2, nlin_form="rotational")
-    plan = plan_for(N, precision=prec, nu=0.01, dt=1e-3, dealias="two_thirds", nlin_form="rotational")
+    cfg = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=2, nlin_form=form)
+    plan = plan_for(N, precision=prec, nu=0.01, dt=1e-3, dealias="two_thirds", nlin_form=form)
     dt = torch.complex128 if prec == "f64" else torch.complex64
     u = torch.from_numpy(V.copy()).to(cuda).to(dt)
     W = R.rk4_step(cfg, V)
