@@ -88,6 +88,10 @@ int ts_plan_set_stream(ts_plan* plan, void* stream);
 int ts_plan_sizes(const ts_plan* plan, long long* elems_per_comp, int* bytes_per_complex);
 /* Number of shells of E(k): Min_radius_outside()+1 (FFF_pencil_inline.h:497-504). */
 int ts_plan_num_shells(const ts_plan* plan, int* n_shells);
+/* Wait for the plan's stream and report a bounded device wait that gave up in
+ * any earlier call (TS_ERR_TIMEOUT); the stepping calls otherwise report it at
+ * the next call.  No reference counterpart (the reference has no device waits). */
+int ts_plan_status(ts_plan* plan);
 /* Set the fixed time step (global.time.dt). */
 int ts_plan_set_dt(ts_plan* plan, double dt);
 

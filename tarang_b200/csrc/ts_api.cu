@@ -401,6 +401,17 @@ int ts_plan_num_shells(const ts_plan* p, int* n) {
   return TS_OK;
 }
 
+int ts_plan_status(ts_plan* p) {
+  if (!p) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(p->st));
+  CK(cudaMemcpy(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost));
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
+    return TS_ERR_TIMEOUT;
+  }
+  return TS_OK;
+}
+
 int ts_plan_set_dt(ts_plan* p, double dt) {
   if (!p || !(dt > 0)) return TS_ERR_ARG;
   if (dt == p->cfg.dt) return TS_OK;

@@ -123,6 +123,10 @@ class Plan:
         s = stream if stream is not None else torch.cuda.current_stream()
         L.check(self.lib.ts_plan_set_stream(self.h, ctypes.c_void_p(s.cuda_stream)), "ts_plan_set_stream")
 
+    def status(self):
+        """Synchronise the plan's stream; raise TsError if a bounded device wait gave up earlier."""
+        L.check(self.lib.ts_plan_status(self.h), "ts_plan_status")
+
     # ------------------------------------------------------------------
     def rk4_step(self, u, nsteps: int = 1):
         L.check(self.lib.ts_rk4_step(self.h, _ptr(u), nsteps), "ts_rk4_step")
