@@ -374,8 +374,11 @@ template <> cudaError_t Launch<T>::carati(const Geo& g, const void* U, void* fc,
 
 template <> cudaError_t Launch<T>::energy(const Geo& g, const void* A, const void* B, int ncomp, double* out,
                                           cudaStream_t st) {
-  k_energy<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)A, (const V*)B, ncomp, g, out);
-  ++g_launches;
+  // out[0] = the sum; out[1 .. blocks] hold the per-block partial sums (blocks <= 148 * 16)
+  const unsigned blocks = grid1d(g.S, 256);
+  k_energy<T><<<blocks, 256, 0, st>>>((const V*)A, (const V*)B, ncomp, g, out);
+  k_sum_partials<<<1, 256, 0, st>>>(out, (int)blocks);
+  g_launches += 2;
   return cudaGetLastError();
 }
 

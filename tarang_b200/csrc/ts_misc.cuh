@@ -192,7 +192,17 @@ __global__ void k_energy(const C<T>* __restrict__ A, const C<T>* __restrict__ B,
     s += energy_weight(g.basis, lx, lz) * d;
   }
   s = block_sum(s);
-  if (threadIdx.x == 0) atomicAdd(out, s);
+  if (threadIdx.x == 0) out[1 + blockIdx.x] = s;  // partial sums, added in a fixed order by k_sum_partials
+}
+
+// out[0] = sum of the n partial sums out[1..n], in an order that does not depend
+// on scheduling (one block), so energies and the normalised initial condition are
+// reproducible bit for bit
+static __global__ void k_sum_partials(double* out, int n) {
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += out[1 + i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[0] = s;
 }
 
 // max over modes of |div U| (FFF: i K.U; SFF: Kx U1 (sine parity) + i Ky U2 + i Kz U3)
