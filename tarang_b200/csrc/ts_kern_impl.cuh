@@ -313,14 +313,14 @@ template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const 
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
     if constexpr (NN <= 512) {
-      constexpr int L2 = 2 * NN;
-      constexpr int E = e_mixed(L2, e_reg(L2));
-      constexpr int CW = cw_for(L2, E);
+      // one NN-point FFT per column and field, 8 elements per thread
+      constexpr int E = e_mixed(NN, 8);
+      constexpr int CW = cw_for(NN, E);
       const int inner = g.Ny * g.Hz;
-      const size_t sm = (size_t)L2 * CW * sizeof(V);
+      const size_t sm = (size_t)NN * CW * sizeof(V);
       auto k = k_sff_inv_x<T, NN, E, CW>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<(inner + CW - 1) / CW, CW * (L2 / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g, (const V*)tq);
+      k<<<(inner + CW - 1) / CW, CW * (NN / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g, (const V*)tq);
       ++g_launches;
       err = cudaGetLastError();
     }
@@ -334,15 +334,15 @@ template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const 
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
     if constexpr (NN <= 512) {
-      constexpr int L2 = 2 * NN;
-      // four accumulators per element: 8 (FP32) / 4 (FP64) elements per thread
-      constexpr int E = e_mixed(L2, std::is_same<T, float>::value ? 8 : 4);
-      constexpr int CW = cw_for(L2, E);
+      // one NN-point FFT per column and product; four accumulators per element:
+      // 8 (FP32) / 4 (FP64) elements per thread
+      constexpr int E = e_mixed(NN, std::is_same<T, float>::value ? 8 : 4);
+      constexpr int CW = cw_for(NN, E);
       const int inner = g.Ny * g.Hz;
-      const size_t sm = (size_t)L2 * CW * sizeof(V);
+      const size_t sm = 3ull * NN * CW * sizeof(V);
       auto k = k_sff_fwd_x<T, NN, E, CW>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<(inner + CW - 1) / CW, CW * (L2 / E), sm, st>>>((const V*)P, g, a, (const V*)tq);
+      k<<<(inner + CW - 1) / CW, CW * (NN / E), sm, st>>>((const V*)P, g, a, (const V*)tq);
       ++g_launches;
       err = cudaGetLastError();
     }

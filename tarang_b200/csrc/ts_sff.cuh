@@ -5,9 +5,17 @@
 // (SFF_pencil_inline.h:63; sine m = 0 unused, the m = Nx sine term dropped):
 //   C:  u_n = c_0 + 2 sum_m c_m cos(pi m (2n+1)/(2N)),  c_m = (1/N) sum_n u_n cos(...)
 //   S:  u_n =       2 sum_m c_m sin(pi m (2n+1)/(2N)),  c_m = (1/N) sum_n u_n sin(...)
-// Each x transform is a 2N-point complex FFT of the even (C) / odd (S)
-// extension with quarter-step twiddles e^{-i pi k/(2N)} before or after, so it
-// applies to the complex data left by the y and z Fourier passes directly.
+// Each x transform is one N-point complex FFT with O(N) pre/post-processing
+// (the reordering method for the type-II/III cosine transform, applied to the
+// complex data left by the y and z Fourier passes; the transforms are
+// real-linear, so real and imaginary parts ride in one complex FFT):
+//   forward:  v_k = u_{2k} (k < N/2), v_k = +-u_{2(N-1-k)+1} (k >= N/2, minus for S),
+//             Z = FFT_N(v), w_m = e^{-i pi m/(2N)},
+//             C: c_m = (1/2N) (w_m Z_m + conj(w_m) Z_{N-m}),
+//             S: c_m = (i/2N) (w_m Z_m - conj(w_m) Z_{N-m})        (Z_N = Z_0)
+//   inverse:  C: V_m = conj(w_m) (c_m - i c_{N-m}),  S: V_m = conj(w_m) (s_{N-m} - i s_m),
+//             V_0 = c_0 (C) or 0 (S), c_N = 0; v = inverse FFT_N(V) (unscaled);
+//             u_{2k} = v_k, u_{2k+1} = v_{N-1-k}, and u_n *= (-1)^n for S.
 // Parities (global/Global.cc:137-145, sincostr "SFF"): u1 S, u2 C, u3 C, T S;
 // products u1u1 u2u2 u3u3 C, u1u2 S, u2u3 C, u3u1 S, u1T C, u2T S, u3T S.
 // x derivative of a C series is -Kx (result S), of an S series +Kx (result C)
@@ -31,19 +39,25 @@ struct SffArgs {
   int reality;
 };
 
+// blocks per SM the SFF x kernels are compiled for: power-of-two lengths (8
+// elements per thread) stay at or under 128 registers per thread (16+ warps per
+// SM); the 12-element mixed-radix variants need the larger register budget
+__host__ __device__ constexpr int sff_min_blocks(int threads, int e) {
+  return e > 8 ? (threads <= 256 ? 2 : 1) : (threads <= 256 ? 512 / threads : 1);
+}
+
 // parity of product field f: true = sine
 __host__ __device__ constexpr bool sff_prod_sine(int f) { return f == 3 || f == 5 || f == 7 || f == 8; }
 
 // ---------------------------------------------------------------------------
 // inverse x pass: W_f = inverse sin/cos transform of D(field_f), f = u1,u2,u3,T.
-// tq: 4N entries exp(-2 pi i j/(4N)) (its even entries are the 2N-FFT table).
+// tq: 4N entries exp(-2 pi i j/(4N)) (every fourth entry is the N-point FFT table).
 // ---------------------------------------------------------------------------
 template <typename T, int N, int E, int CW>
-__global__ void __launch_bounds__(CW * (2 * N / E), (CW * (2 * N / E)) <= 256 ? 2 : 1)
+__global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     k_sff_inv_x(const C<T>* __restrict__ U, const C<T>* __restrict__ Tf, C<T>* __restrict__ W, Geo g,
                 const C<T>* __restrict__ tq) {
   typedef C<T> V;
-  constexpr int L2 = 2 * N;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
@@ -55,28 +69,33 @@ __global__ void __launch_bounds__(CW * (2 * N / E), (CW * (2 * N / E)) <= 256 ? 
   for (int f = 0; f < 4; ++f) {
     const V* src = (f < 3 ? U + f * g.S : Tf) + (ok ? col : 0);
     const bool sine = f == 0 || f == 3;
+    // coefficient q of the (dealiased) series; 0 outside 0..N-1
+    auto coef = [&](int q) -> V {
+      if (!ok || q <= 0 || q >= N || dealias_zero(g.dealias, 1, q, ly, lz, g.Nx, g.Ny, g.Nz)) return mk<V>(0, 0);
+      return src[q * rstride];
+    };
     V v[E];
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      const int k = load_row<L2, E>(t, s);
-      const int m = k <= N ? k : L2 - k;
-      V z = mk<V>(0, 0);
-      if (ok && k != N && !(sine && m == 0) && !dealias_zero(g.dealias, 1, m, ly, lz, g.Nx, g.Ny, g.Nz)) {
-        const V a = src[m * rstride];
-        if (k == 0) z = a;                                   // cosine c_0
-        else if (k < N) z = mul(conjg(tq[m]), a);            // e^{+i pi m/2N} c_m
-        else z = mul(tq[m], a);                              // e^{-i pi m/2N} c_m
-        if (sine) z = (k < N) ? mul_i<-1>(z) : mul_i<1>(z);  // -i / +i for the sine series
+      const int m = load_row<N, E>(t, s);
+      V z;
+      if (m == 0) {
+        // cosine: V_0 = c_0; sine: V_0 = 0
+        z = (!sine && ok && !dealias_zero(g.dealias, 1, 0, ly, lz, g.Nx, g.Ny, g.Nz)) ? src[0] : mk<V>(0, 0);
+      } else {
+        const V p = sine ? coef(N - m) : coef(m), q = sine ? coef(m) : coef(N - m);
+        z = mul(conjg(tq[m]), sub(p, mul_i<1>(q)));
       }
       v[s] = z;
     }
-    fft_regs<L2, E, 1>(v, t, xch, CW, c, tq, 2);
+    fft_regs<N, E, 1>(v, t, xch, CW, c, tq, 4);
     if (ok) {
       V* d = W + f * g.S + col;
 #pragma unroll
       for (int s = 0; s < E; ++s) {
-        const int n = final_row<L2, E>(t, s);
-        if (n < N) d[n * rstride] = v[s];
+        const int k = final_row<N, E>(t, s);
+        const int n = k < N / 2 ? 2 * k : 2 * (N - 1 - k) + 1;
+        d[n * rstride] = (sine && (n & 1)) ? scale(v[s], (T)-1) : v[s];
       }
     }
   }
@@ -90,13 +109,18 @@ __global__ void __launch_bounds__(CW * (2 * N / E), (CW * (2 * N / E)) <= 256 ? 
 //   N -= F; p = div(N)/K^2; N += grad p; R = -N, RT = -NT; IF-RK4 stage update of U (nu) and T (kappa)
 //   (RK_SF.cc:97-221, Tadvance_functions.cc:57-90,226-237,372-395,589-611).
 // ---------------------------------------------------------------------------
+// The nine product columns stream through two cp.async staging tiles (field
+// f+2 is in flight while f is transformed); each thread stages exactly the
+// elements it reads back, in FFT input order, so the reordering is done by the
+// copy and no barrier guards the staging tiles.
+// Shared memory: exchange tile + 2 staging tiles of N x CW complex.
 template <typename T, int N, int E, int CW>
-__global__ void __launch_bounds__(CW * (2 * N / E), (CW * (2 * N / E)) <= 256 ? 2 : 1)
+__global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     k_sff_fwd_x(const C<T>* __restrict__ P, Geo g, SffArgs a, const C<T>* __restrict__ tq) {
   typedef C<T> V;
-  constexpr int L2 = 2 * N;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
+  V* stage = xch + N * CW;
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int inner = g.Ny * g.Hz;
   const int col = blockIdx.x * CW + c;
@@ -114,27 +138,51 @@ __global__ void __launch_bounds__(CW * (2 * N / E), (CW * (2 * N / E)) <= 256 ? 
 #pragma unroll
     for (int s = 0; s < E; ++s) acc[i][s] = mk<V>(0, 0);
 
+  // field f's column into staging tile buf, row k of the tile = FFT input k
+  // (even points, then odd points reversed)
+  auto issue = [&](int f, int buf) {
+    if (f < 9 && ok) {
+      const V* src = P + f * g.S + col;
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int k = load_row<N, E>(t, s);
+        cp_async(stage + (buf * N + k) * CW + c, src + (k < N / 2 ? 2 * k : 2 * (N - 1 - k) + 1) * rstride);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0, 0);
+  issue(1, 1);
   for (int f = 0; f < 9; ++f) {
     const bool sine = sff_prod_sine(f);
-    const V* src = P + f * g.S + (ok ? col : 0);
+    const int buf = f & 1;
+    cp_async_wait<1>();
     V v[E];
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      const int k = load_row<L2, E>(t, s);
+      const int k = load_row<N, E>(t, s);
       V x = mk<V>(0, 0);
       if (ok) {
-        x = src[(k < N ? k : L2 - 1 - k) * rstride];  // even / odd extension
-        if (sine && k >= N) x = scale(x, (T)-1);
+        x = stage[(buf * N + k) * CW + c];
+        if (sine && k >= N / 2) x = scale(x, (T)-1);
       }
       v[s] = x;
     }
-    fft_regs<L2, E, -1>(v, t, xch, CW, c, tq, 2);
+    issue(f + 2, buf);
+    fft_regs<N, E, -1>(v, t, xch, CW, c, tq, 4);
+    // pair terms Z_{N-m} through the exchange tile
+#pragma unroll
+    for (int s = 0; s < E; ++s) xch[final_row<N, E>(t, s) * CW + c] = v[s];
+    __syncthreads();
+    V zr[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) zr[s] = xch[((N - final_row<N, E>(t, s)) % N) * CW + c];
+    __syncthreads();
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      const int m = final_row<L2, E>(t, s);
-      if (m >= N) continue;
-      V cm = scale(mul(tq[m], v[s]), (T)scl);
-      if (sine) cm = (m == 0) ? mk<V>(0, 0) : mul_i<1>(cm);
+      const int m = final_row<N, E>(t, s);
+      const V wz = mul(tq[m], v[s]), wzr = mul(conjg(tq[m]), zr[s]);
+      const V cm = sine ? mul_i<1>(scale(sub(wz, wzr), (T)scl)) : scale(add(wz, wzr), (T)scl);
       const T Kx = (T)(m * g.kf[0]);
       switch (f) {
         case 0: acc[0][s] = add(acc[0][s], scale(cm, -Kx)); break;
@@ -159,8 +207,7 @@ __global__ void __launch_bounds__(CW * (2 * N / E), (CW * (2 * N / E)) <= 256 ? 
   const double eyz_u = a.eu[1][ly] * a.eu[2][lz], eyz_t = a.et[1][ly] * a.et[2][lz];
 #pragma unroll
   for (int s = 0; s < E; ++s) {
-    const int m = final_row<L2, E>(t, s);
-    if (m >= N) continue;
+    const int m = final_row<N, E>(t, s);
     const long long off = m * rstride + col;
     const double Kxd = m * g.kf[0];
     const T Kx = (T)Kxd;
