@@ -44,8 +44,11 @@ def parse():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--form", default="rotational", choices=["rotational", "conservative"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
-    ap.add_argument("--workload", default="fff256", choices=["fff256", "ensemble", "fff1024"],
-                    help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying 1024^3")
+    ap.add_argument("--workload", default="fff256", choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint"],
+                    help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying "
+                         "1024^3 (or --shape); rbc: one RBC run (SFF, --N, FP32); adjoint: adjoint/forward cost at 128^3")
+    ap.add_argument("--shape", default="1024,1024,1024",
+                    help="grid of the fff1024 workload, Nx,Ny,Nz (smaller shapes exercise the same kernels)")
     return ap.parse_args()
 
 
@@ -76,14 +79,14 @@ def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
             "nusselt_mean": float(np.mean(Nu)), "nusselt_finite": bool(np.all(np.isfinite(Nu)))}
 
 
-def fff1024_leg(steps: int = 3, warmup: int = 2):
+def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024)):
     """Config 2: FFF 1024^3 decaying turbulence, FP32 rotational, IC k^4 exp(-2(k/8)^2) E=0.5,
     nu=2e-4, dt=2e-4; steps/s and the per-kernel rates."""
     import torch
     import ctypes
     import tarang_b200 as tb
     from tarang_b200 import _lib as L
-    plan = tb.Plan(1024, precision="f32", nlin_form="rotational", dealias="two_thirds", nu=2e-4, dt=2e-4)
+    plan = tb.Plan(tuple(shape), precision="f32", nlin_form="rotational", dealias="two_thirds", nu=2e-4, dt=2e-4)
     plan.set_stream(torch.cuda.current_stream())   # the timing events below go on this stream
     u = plan.field(3)
     plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 8.0), 0, 0.5, u)
@@ -108,10 +111,49 @@ def fff1024_leg(steps: int = 3, warmup: int = 2):
         L.check(plan.lib.ts_profile_read(plan.h, k, ctypes.byref(tot), ctypes.byref(n), ctypes.byref(b)), "read")
         if n.value and b.value:
             kern[name] = round(b.value / (tot.value / n.value / 1e3) / 1e9, 1)
+    n3 = float(shape[0]) * shape[1] * shape[2]
     out = {"steps_per_s": steps / (ms / 1e3), "kernel_GBps": kern, "energy": plan.energy(u),
-           "model_frac": 288.0 * 1024 ** 3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
+           "model_frac": 288.0 * n3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
     plan.close()
     return out
+
+
+def rbc_leg(N: int, steps: int, warmup: int):
+    """One Boussinesq (RBC) run on the SFF basis at N^3, FP32, Ra = 1e6, Pr = 1, kfactor (pi, 2pi, 2pi),
+    dt = 1e-4, T perturbation 1e-3 on k <= 4 (seed 3): steps/s and per-kernel rates."""
+    import torch
+    import ctypes
+    import tarang_b200 as tb
+    from tarang_b200 import _lib as L
+    plan = tb.Plan(N, basis="SFF", precision="f32", dealias="reference", Ra=1e6, Pr=1.0, dt=1e-4,
+                   kfactor=(math.pi, 2 * math.pi, 2 * math.pi))
+    plan.set_stream(torch.cuda.current_stream())
+    u, T = plan.field(3), plan.field(1)
+    plan.init_temperature_perturbation(1e-3, 4.0, 3, T)
+    plan.rk4_step_rbc(u, T, warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.rk4_step_rbc(u, T, steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    L.check(plan.lib.ts_profile_reset(plan.h), "reset")
+    L.check(plan.lib.ts_profile_enable(plan.h, 1), "enable")
+    plan.rk4_step_rbc(u, T, 1)
+    torch.cuda.synchronize()
+    L.check(plan.lib.ts_profile_enable(plan.h, 0), "disable")
+    kern = {}
+    for k, name in enumerate(L.KCLASS_NAMES):
+        tot, n, b = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+        L.check(plan.lib.ts_profile_read(plan.h, k, ctypes.byref(tot), ctypes.byref(n), ctypes.byref(b)), "read")
+        if n.value:
+            kern[name] = {"ms_per_step": round(tot.value, 4),
+                          "GBps": round(b.value / (tot.value / n.value / 1e3) / 1e9, 1) if b.value else None}
+    nu = plan.nusselt(u, T)
+    plan.close()
+    return {"steps_per_s": steps / (ms / 1e3), "kernels": kern, "nusselt": nu,
+            "model_frac": 408.0 * N ** 3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
 
 
 def adjoint_leg(prec: str, N: int = 128, window: int = 20, reps: int = 3):
@@ -320,13 +362,32 @@ def alt_workload(args, world, rank, local, dev):
                              "unit": "GB/s", "frac": mb * value / 1e9 / world / measured_peak()[0],
                              "traffic": None, "model": "408 N^3 4 B per member step"},
                 "member_steps_per_s": 64 * value}
-    else:
-        r = fff1024_leg(steps=args.steps, warmup=args.warmup)
-        line = {"metric": "RK4 steps/s, FFF decaying turbulence 1024^3 (FP32 transforms, FP64 sums)",
+    elif args.workload == "rbc":
+        r = rbc_leg(args.N if args.N != 256 else 128, steps=args.steps, warmup=args.warmup)
+        n = args.N if args.N != 256 else 128
+        line = {"metric": f"RK4 steps/s, SFF Boussinesq (RBC) {n}^3 (FP32 transforms, FP64 sums)",
                 "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 / r["steps_per_s"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "FFF 1024^3 decaying, IC k^4 exp(-2(k/8)^2) E=0.5 seed 0, nu=2e-4, dt=2e-4"},
+                "config": {"workload": f"RBC {n}^3, Ra=1e6, Pr=1, kfactor (pi,2pi,2pi), dt=1e-4, T amp 1e-3 k<=4"},
+                "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "kernels": r["kernels"]},
+                "nusselt": r["nusselt"]}
+    elif args.workload == "adjoint":
+        r = {"f64": adjoint_leg("f64"), "f32": adjoint_leg("f32")}
+        line = {"metric": "adjoint step / forward step cost, FFF 128^3 rotational (config 4)",
+                "value": r["f64"]["adjoint_over_forward"], "unit": "ratio", "n_gpus": 1, "steps": 30,
+                "warmup": 2, "ms_per_step": r["f64"]["adjoint_step_ms"], "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "FFF 128^3, nu=5e-3, dt=1e-3, two-thirds, window 20"}, "detail": r}
+    else:
+        shape = tuple(int(x) for x in args.shape.split(","))
+        r = fff1024_leg(steps=args.steps, warmup=args.warmup, shape=shape)
+        sh = "x".join(str(x) for x in shape)
+        line = {"metric": f"RK4 steps/s, FFF decaying turbulence {sh} (FP32 transforms, FP64 sums)",
+                "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 / r["steps_per_s"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"FFF {sh} decaying, IC k^4 exp(-2(k/8)^2) E=0.5 seed 0, nu=2e-4, dt=2e-4"},
                 "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "kernel_GBps": r["kernel_GBps"]}}
     line["clocks"] = clk.stop()
     if rank == 0:
