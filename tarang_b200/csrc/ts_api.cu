@@ -906,6 +906,12 @@ int ts_profile_read(ts_plan* p, int kclass, double* total_ms, long long* launche
     const double f = (double)p->g.S * (double)p->cb;
     const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
     double b = 0;
+    if (p->cfg.basis == TS_BASIS_SFF) {
+      // u1, u2, u3, T in; nine products out; the epilogue's state traffic averages 16 fields over a step
+      const double sff[TS_KCLASS_COUNT] = {8 * f, 8 * f, 13 * f, 18 * f, 25 * f, 0};
+      *bytes_per_launch = kclass < TS_KCLASS_COUNT ? sff[kclass] : 0;
+      return TS_OK;
+    }
     switch (kclass) {
       case TS_KCLASS_INV_X: b = (3 + (rot ? 6 : 3)) * f; break;          // read U, write W
       case TS_KCLASS_Y_INV: b = 2.0 * (rot ? 6 : 3) * f; break;          // in place
@@ -922,16 +928,34 @@ int ts_profile_read(ts_plan* p, int kclass, double* total_ms, long long* launche
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Ensemble of independent RBC runs (uneven sizes).  One plan per member; one
-// ensemble step is a single CUDA graph launch whose branches are the members'
-// step sequences (fork on an event of the origin stream, one stream per member,
-// join back), so small members run concurrently and fill the GPU.
+// Ensemble of independent RBC runs (uneven sizes).  Members of the same grid
+// form a group whose fields sit in contiguous arrays (member stride = its
+// field count x S), so every kernel of a group step covers all of its members
+// in one launch (member = blockIdx.y, or folded into the field / line count);
+// each member keeps its own integrating-factor tables (its Ra sets nu, kappa).
+// One ensemble step = one CUDA graph launch whose parallel branches are the
+// groups' step sequences (fork on the origin stream, one stream per group).
+// Every member also has its own plan, used for diagnostics and for stepping a
+// member on its own; its state is a view into the group arrays.
 // ---------------------------------------------------------------------------
+struct ens_group {
+  std::vector<int> idx;  // member indices
+  ts_plan* gp = nullptr; // the first member's plan: geometry, twiddles, error word
+  void* U = nullptr;     // B x 3S
+  void* T = nullptr;     // B x S
+  void* Ucur = nullptr;  // B x 4S
+  void* tot = nullptr;   // B x 4S
+  void* P = nullptr;     // B x 9S
+  double* eu = nullptr;  // B x (Nx + Ny + Hz): exp(-nu dt K_i^2 / 2) per axis, per member
+  double* et = nullptr;  // same with kappa
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
 struct ts_ensemble {
   std::vector<ts_plan*> plans;
-  std::vector<void*> U, T;
-  std::vector<cudaStream_t> streams;
-  std::vector<cudaEvent_t> done;
+  std::vector<void*> U, T;  // member views into the group arrays
+  std::vector<ens_group> groups;
   cudaEvent_t fork = nullptr;
   cudaStream_t origin = nullptr;
   bool own_origin = false;
@@ -939,19 +963,69 @@ struct ts_ensemble {
   cudaGraphExec_t exec = nullptr;
 };
 
+// one IF-RK4 step of every member of a group (step_rbc with member strides)
+static int step_rbc_group(ens_group& G) {
+  ts_plan* p = G.gp;
+  const Geo& g = p->g;
+  const int B = (int)G.idx.size();
+  const long long S = g.S, cb = (long long)p->cb;
+  const long long TL = (long long)g.Nx + g.Ny + g.Hz;
+  SffArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = G.U;
+  a.T0 = G.T;
+  a.Ucur = G.Ucur;
+  a.tot = G.tot;
+  a.dt = p->cfg.dt;
+  a.reality = p->cfg.reality_fix;
+  const long long aoff[3] = {0, g.Nx, (long long)g.Nx + g.Ny};
+  for (int i = 0; i < 3; ++i) {
+    a.eu[i] = G.eu + aoff[i];
+    a.et[i] = G.et + aoff[i];
+  }
+  a.mtab = TL;
+  a.msU0 = 3 * S;
+  a.msT0 = S;
+  a.msUcur = 4 * S;
+  a.msTot = 4 * S;
+  a.msP = 9 * S;
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? G.U : G.Ucur;
+    const void* Tin = stage == 1 ? G.T : (const void*)((const char*)G.Ucur + 3 * S * cb);
+    const long long msUin = stage == 1 ? 3 * S : 4 * S, msTin = stage == 1 ? S : 4 * S;
+    a.stage = stage;
+    a.U1in = Uin;
+    a.Tin = Tin;
+    a.msU1in = msUin;
+    a.msTin = msTin;
+    CK(LAUNCH(p, sff_inv_x, g, Uin, Tin, G.P, p->twq, G.st, B, msUin, msTin, 9 * S));
+    CK(LAUNCH(p, strided, g, 1, +1, G.P, 4 * B, p->twy, G.st, 4, 9 * S));
+    CK(LAUNCH(p, z_fused, g, 2, G.P, p->twz, p->err_d, G.st, B, 9 * S));
+    CK(LAUNCH(p, strided, g, 1, -1, G.P, 9 * B, p->twy, G.st));
+    CK(LAUNCH(p, sff_fwd_x, g, G.P, a, p->twq, G.st, B));
+  }
+  if (p->cfg.reality_fix) {
+    CK(LAUNCH(p, reality, g, G.U, 3 * B, G.st));
+    CK(LAUNCH(p, reality, g, G.T, B, G.st));
+  }
+  return TS_OK;
+}
+
 extern "C" {
 
 int ts_ensemble_destroy(ts_ensemble* e) {
   if (!e) return TS_ERR_ARG;
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
-  for (size_t m = 0; m < e->plans.size(); ++m) {
-    if (e->U[m]) cudaFree(e->U[m]);
-    if (e->T[m]) cudaFree(e->T[m]);
-    if (e->plans[m]) ts_plan_destroy(e->plans[m]);
-    if (e->streams[m]) cudaStreamDestroy(e->streams[m]);
-    if (e->done[m]) cudaEventDestroy(e->done[m]);
+  for (ens_group& G : e->groups) {
+    void* bufs[] = {G.U, G.T, G.Ucur, G.tot, G.P, G.eu, G.et};
+    for (void* b : bufs)
+      if (b) cudaFree(b);
+    if (G.st) cudaStreamDestroy(G.st);
+    if (G.done) cudaEventDestroy(G.done);
   }
+  for (ts_plan* p : e->plans)
+    if (p) ts_plan_destroy(p);
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->own_origin && e->origin) cudaStreamDestroy(e->origin);
   delete e;
@@ -969,6 +1043,10 @@ int ts_ensemble_create(const ts_config* base, const ts_member* members, int coun
   if (cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking) != cudaSuccess) return fail(TS_ERR_CUDA);
   e->own_origin = true;
   if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) return fail(TS_ERR_CUDA);
+  e->plans.assign(count, nullptr);
+  e->U.assign(count, nullptr);
+  e->T.assign(count, nullptr);
+  std::vector<int> gof(count, -1);
   for (int m = 0; m < count; ++m) {
     ts_config c = *base;
     c.basis = TS_BASIS_SFF;
@@ -976,25 +1054,50 @@ int ts_ensemble_create(const ts_config* base, const ts_member* members, int coun
     for (int i = 0; i < 3; ++i) c.N[i] = members[m].N[i];
     c.Ra = members[m].Ra;
     c.Pr = members[m].Pr;
+    if (!(c.Ra > 0) || !(c.Pr > 0)) return fail(TS_ERR_ARG);
     // ULARGE: nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra) (Iscalar_main.cc:52-92)
     c.nu = sqrt(c.Pr / c.Ra);
     c.kappa = 1.0 / sqrt(c.Pr * c.Ra);
-    ts_plan* p = nullptr;
-    e->plans.push_back(nullptr);
-    e->U.push_back(nullptr);
-    e->T.push_back(nullptr);
-    e->streams.push_back(nullptr);
-    e->done.push_back(nullptr);
-    int rc = ts_plan_create(&c, &p);
+    int rc = ts_plan_create(&c, &e->plans[m]);
     if (rc != TS_OK) return fail(rc);
-    e->plans[m] = p;
-    if (cudaStreamCreateWithFlags(&e->streams[m], cudaStreamNonBlocking) != cudaSuccess) return fail(TS_ERR_CUDA);
-    if (cudaEventCreateWithFlags(&e->done[m], cudaEventDisableTiming) != cudaSuccess) return fail(TS_ERR_CUDA);
-    p->st = e->streams[m];
-    const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
-    if (cudaMalloc(&e->U[m], bu) != cudaSuccess || cudaMalloc(&e->T[m], bt) != cudaSuccess) return fail(TS_ERR_NOMEM);
-    if (cudaMemset(e->U[m], 0, bu) != cudaSuccess || cudaMemset(e->T[m], 0, bt) != cudaSuccess)
+    for (size_t k = 0; k < e->groups.size() && gof[m] < 0; ++k) {
+      const Geo& h = e->groups[k].gp->g;
+      if (h.Nx == c.N[0] && h.Ny == c.N[1] && h.Nz == c.N[2]) gof[m] = (int)k;
+    }
+    if (gof[m] < 0) {
+      e->groups.emplace_back();
+      e->groups.back().gp = e->plans[m];
+      gof[m] = (int)e->groups.size() - 1;
+    }
+    e->groups[gof[m]].idx.push_back(m);
+  }
+  for (ens_group& G : e->groups) {
+    const Geo& g = G.gp->g;
+    const size_t B = G.idx.size(), S = (size_t)g.S, cb = G.gp->cb;
+    const size_t TL = (size_t)g.Nx + g.Ny + g.Hz;
+    if (cudaMalloc(&G.U, B * 3 * S * cb) != cudaSuccess || cudaMalloc(&G.T, B * S * cb) != cudaSuccess ||
+        cudaMalloc(&G.Ucur, B * 4 * S * cb) != cudaSuccess || cudaMalloc(&G.tot, B * 4 * S * cb) != cudaSuccess ||
+        cudaMalloc(&G.P, B * 9 * S * cb) != cudaSuccess || cudaMalloc(&G.eu, B * TL * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&G.et, B * TL * sizeof(double)) != cudaSuccess)
+      return fail(TS_ERR_NOMEM);
+    if (cudaMemset(G.U, 0, B * 3 * S * cb) != cudaSuccess || cudaMemset(G.T, 0, B * S * cb) != cudaSuccess)
       return fail(TS_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&G.st, cudaStreamNonBlocking) != cudaSuccess) return fail(TS_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&G.done, cudaEventDisableTiming) != cudaSuccess) return fail(TS_ERR_CUDA);
+    const size_t n[3] = {(size_t)g.Nx, (size_t)g.Ny, (size_t)g.Hz}, off[3] = {0, (size_t)g.Nx, (size_t)g.Nx + g.Ny};
+    for (size_t j = 0; j < B; ++j) {
+      ts_plan* p = e->plans[G.idx[j]];
+      p->st = G.st;
+      e->U[G.idx[j]] = (char*)G.U + j * 3 * S * cb;
+      e->T[G.idx[j]] = (char*)G.T + j * S * cb;
+      for (int i = 0; i < 3; ++i) {
+        if (cudaMemcpy(G.eu + j * TL + off[i], p->eax[i], n[i] * sizeof(double), cudaMemcpyDeviceToDevice) !=
+                cudaSuccess ||
+            cudaMemcpy(G.et + j * TL + off[i], p->eaxT[i], n[i] * sizeof(double), cudaMemcpyDeviceToDevice) !=
+                cudaSuccess)
+          return fail(TS_ERR_CUDA);
+      }
+    }
   }
   *out = e;
   return TS_OK;
@@ -1010,6 +1113,7 @@ int ts_ensemble_member(ts_ensemble* e, int m, ts_plan** plan, void** u_hat, void
 
 int ts_ensemble_init_temperature(ts_ensemble* e, double amp, double kmax, uint64_t seed) {
   if (!e) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(e->origin));
   for (size_t m = 0; m < e->plans.size(); ++m) {
     CK(cudaMemset(e->U[m], 0, 3 * e->plans[m]->g.S * e->plans[m]->cb));
     CKS(ts_init_temperature_perturbation(e->plans[m], amp, kmax, seed + m, e->T[m]));
@@ -1021,15 +1125,16 @@ int ts_ensemble_run(ts_ensemble* e, int nsteps) {
   if (!e || nsteps < 0) return TS_ERR_ARG;
   if (!e->exec) {
     for (ts_plan* p : e->plans) p->prof = false;
-    CK(cudaStreamSynchronize(e->origin));
+    CK(cudaDeviceSynchronize());
     CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeRelaxed));
     int rc = TS_OK;
     cudaEventRecord(e->fork, e->origin);
-    for (size_t m = 0; m < e->plans.size() && rc == TS_OK; ++m) {
-      cudaStreamWaitEvent(e->streams[m], e->fork, 0);
-      rc = step_rbc(e->plans[m], e->U[m], e->T[m]);
-      cudaEventRecord(e->done[m], e->streams[m]);
-      cudaStreamWaitEvent(e->origin, e->done[m], 0);
+    for (size_t k = 0; k < e->groups.size() && rc == TS_OK; ++k) {
+      ens_group& G = e->groups[k];
+      cudaStreamWaitEvent(G.st, e->fork, 0);
+      rc = step_rbc_group(G);
+      cudaEventRecord(G.done, G.st);
+      cudaStreamWaitEvent(e->origin, G.done, 0);
     }
     cudaGraph_t graph = nullptr;
     cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);

@@ -98,7 +98,8 @@ constexpr int str_cw(int L) { return wide1024(L) ? 8 : cw_for(L, str_e(L)); }
 constexpr int str_nt(int L) { return wide1024(L) ? 2 : 3; }
 
 template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw,
-                                           cudaStream_t st) {
+                                           cudaStream_t st, int per, long long mstride) {
+  if (per <= 0) per = nf;
   cudaError_t err = cudaErrorInvalidValue;
   const int L = axis == 0 ? g.Nx : g.Ny;
   dispatch_L_sff(L, [&](auto Lc) {
@@ -121,12 +122,12 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       auto k = k_strided_fft<T, LL, E, CW, -1, NT>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
       k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
-                                                    (const V*)tw);
+                                                    (const V*)tw, per, mstride);
     } else {
       auto k = k_strided_fft<T, LL, E, CW, 1, NT>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
       k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
-                                                    (const V*)tw);
+                                                    (const V*)tw, per, mstride);
     }
     ++g_launches;
     err = cudaGetLastError();
@@ -160,7 +161,8 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
 }
 
 template <int NZ, int FORM>
-static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr, cudaStream_t st) {
+static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr, cudaStream_t st, int nmem,
+                                long long msP) {
   constexpr int M = NZ / 2;
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   const long long nlines = (long long)g.Nx * g.Ny;
@@ -173,7 +175,7 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
       const long long ngroups = nlines / LPB;
       auto k = k_z_tma<T, NZ, FORM>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
-      k<<<(unsigned)(ngroups < 148 ? ngroups : 148), 256, sm, st>>>((V*)P, g, (const V*)tw, zerr);
+      k<<<dim3((unsigned)(ngroups < 148 ? ngroups : 148), nmem), 256, sm, st>>>((V*)P, g, (const V*)tw, zerr, msP);
       ++g_launches;
       return cudaGetLastError();
     }
@@ -184,7 +186,8 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
     if constexpr (FORM == 3)
       k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
     else
-      k_z_reg<T, NZ, FORM><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
+      k_z_reg<T, NZ, FORM><<<dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), NT, 0, st>>>((V*)P, g, (const V*)tw,
+                                                                                           msP);
     ++g_launches;
     return cudaGetLastError();
   }
@@ -197,20 +200,21 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   const size_t sm = (size_t)NSL * nl * zslot<M>() * sizeof(V);
   auto k = k_z_fused<T, NZ, E, FORM>;
   if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
-  k<<<(unsigned)((nlines + nl - 1) / nl), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl);
+  k<<<dim3((unsigned)((nlines + nl - 1) / nl), nmem), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl, msP);
   ++g_launches;
   return cudaGetLastError();
 }
 
 template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, const void* tw, int* zerr,
-                                           cudaStream_t st) {
+                                           cudaStream_t st, int nmem, long long msP) {
   cudaError_t err = cudaErrorInvalidValue;
+  if (form == 3 && nmem != 1) return err;  // the adjoint z pass has no member batching
   dispatch_L_sff(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
-    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st);
-    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st);
-    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st);
-    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st);
+    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st, nmem, msP);
+    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP);
+    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP);
+    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0);
   });
   return err;
 }
@@ -308,7 +312,7 @@ template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int form, int mode, const
 }
 
 template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq,
-                                             cudaStream_t st) {
+                                             cudaStream_t st, int nmem, long long msU, long long msT, long long msW) {
   cudaError_t err = cudaErrorInvalidValue;
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
@@ -320,7 +324,8 @@ template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const 
       const size_t sm = (size_t)NN * CW * sizeof(V);
       auto k = k_sff_inv_x<T, NN, E, CW>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<(inner + CW - 1) / CW, CW * (NN / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g, (const V*)tq);
+      k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g,
+                                                                   (const V*)tq, msU, msT, msW);
       ++g_launches;
       err = cudaGetLastError();
     }
@@ -329,7 +334,7 @@ template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const 
 }
 
 template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq,
-                                             cudaStream_t st) {
+                                             cudaStream_t st, int nmem) {
   cudaError_t err = cudaErrorInvalidValue;
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
@@ -342,7 +347,7 @@ template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const 
       const size_t sm = 3ull * NN * CW * sizeof(V);
       auto k = k_sff_fwd_x<T, NN, E, CW>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<(inner + CW - 1) / CW, CW * (NN / E), sm, st>>>((const V*)P, g, a, (const V*)tq);
+      k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((const V*)P, g, a, (const V*)tq);
       ++g_launches;
       err = cudaGetLastError();
     }

@@ -12,13 +12,17 @@ extern long long g_launches;  // kernels launched by this library
 template <typename T> struct Launch {
   // strided-axis FFT on nf fields in place: axis 0 = x (L = Nx), 1 = y (L = Ny);
   // dir -1 forward, +1 inverse; outputs scaled by `scale`
-  static cudaError_t strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw, cudaStream_t st);
+  // per > 0: the nf fields are nf / per members of per fields each, members mstride complex apart
+  static cudaError_t strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw, cudaStream_t st,
+                             int per = 0, long long mstride = 0);
   // form 0 conservative (3 fields out), 1 rotational (6), 3 adjoint of the rotational form (9: also
   // lsc c^-1 P lam from the cotangent lam)
   static cudaError_t inv_x(const Geo& g, int form, const void* U, void* W, const void* tw, const void* lam,
                            double lsc, cudaStream_t st);
   // form 0 conservative, 1 rotational, 2 Boussinesq (u, T), 3 adjoint of the rotational form
-  static cudaError_t z_fused(const Geo& g, int form, void* P, const void* tw, int* err, cudaStream_t st);
+  // nmem members, member fields msP complex apart
+  static cudaError_t z_fused(const Geo& g, int form, void* P, const void* tw, int* err, cudaStream_t st,
+                             int nmem = 1, long long msP = 0);
   static cudaError_t z_single(const Geo& g, int dir, const void* in, void* out, int ncomp, const void* tw, cudaStream_t st);
   // a.U0 / a.Ud / a.tot must be 16-byte aligned (TMA)
   // form 0 / 1 / 3 as inv_x; mode MODE_STEP, MODE_FLUX, MODE_NLIN (forms 0, 1) or MODE_ADJ (form 3)
@@ -26,8 +30,11 @@ template <typename T> struct Launch {
                            cudaStream_t st);
   // SFF x passes (sin/cos along x): inverse of u1,u2,u3,T into P[0..3]; forward of the nine
   // Boussinesq products + force, projection and the IF-RK4 stage update
-  static cudaError_t sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq, cudaStream_t st);
-  static cudaError_t sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq, cudaStream_t st);
+  // nmem members: member strides (complex elements) of U, Tf, W; SffArgs carries its own
+  static cudaError_t sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq, cudaStream_t st,
+                               int nmem = 1, long long msU = 0, long long msT = 0, long long msW = 0);
+  static cudaError_t sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq, cudaStream_t st,
+                               int nmem = 1);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,

@@ -37,6 +37,10 @@ struct SffArgs {
   double dt;
   int stage;
   int reality;
+  // batched members (blockIdx.y = member): member strides of each array in
+  // complex elements, and of the integrating-factor tables in doubles (0 for one run)
+  long long msU0, msT0, msUcur, msTot, msU1in, msTin, msP;
+  long long mtab;
 };
 
 // blocks per SM the SFF x kernels are compiled for: power-of-two lengths (8
@@ -56,10 +60,14 @@ __host__ __device__ constexpr bool sff_prod_sine(int f) { return f == 3 || f == 
 template <typename T, int N, int E, int CW>
 __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     k_sff_inv_x(const C<T>* __restrict__ U, const C<T>* __restrict__ Tf, C<T>* __restrict__ W, Geo g,
-                const C<T>* __restrict__ tq) {
+                const C<T>* __restrict__ tq, long long msU, long long msT, long long msW) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
+  // member blockIdx.y of a batch (strides 0 for one run)
+  U += blockIdx.y * msU;
+  Tf += blockIdx.y * msT;
+  W += blockIdx.y * msW;
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int inner = g.Ny * g.Hz;
   const int col = blockIdx.x * CW + c;
@@ -131,6 +139,8 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
   const T Ky = (T)Kyd, Kz = (T)Kzd;
   const long long rstride = inner;
   const double scl = 1.0 / (2.0 * N * (double)g.Ny * g.Nz);
+  const long long mb = blockIdx.y;  // member of a batch
+  P += mb * a.msP;
 
   V acc[4][E];
 #pragma unroll
@@ -198,13 +208,16 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     }
   }
   if (!ok) return;
-  const V* U0 = reinterpret_cast<const V*>(a.U0);
-  const V* T0 = reinterpret_cast<const V*>(a.T0);
-  V* Uc = reinterpret_cast<V*>(a.Ucur);
-  V* tot = reinterpret_cast<V*>(a.tot);
-  const V* U1in = reinterpret_cast<const V*>(a.U1in);
-  const V* Tin = reinterpret_cast<const V*>(a.Tin);
-  const double eyz_u = a.eu[1][ly] * a.eu[2][lz], eyz_t = a.et[1][ly] * a.et[2][lz];
+  const V* U0 = reinterpret_cast<const V*>(a.U0) + mb * a.msU0;
+  const V* T0 = reinterpret_cast<const V*>(a.T0) + mb * a.msT0;
+  V* Uc = reinterpret_cast<V*>(a.Ucur) + mb * a.msUcur;
+  V* tot = reinterpret_cast<V*>(a.tot) + mb * a.msTot;
+  const V* U1in = reinterpret_cast<const V*>(a.U1in) + mb * a.msU1in;
+  const V* Tin = reinterpret_cast<const V*>(a.Tin) + mb * a.msTin;
+  const double* eu0 = a.eu[0] + mb * a.mtab;
+  const double* et0 = a.et[0] + mb * a.mtab;
+  const double eyz_u = a.eu[1][mb * a.mtab + ly] * a.eu[2][mb * a.mtab + lz];
+  const double eyz_t = a.et[1][mb * a.mtab + ly] * a.et[2][mb * a.mtab + lz];
 #pragma unroll
   for (int s = 0; s < E; ++s) {
     const int m = final_row<N, E>(t, s);
@@ -222,7 +235,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     N2 = add(N2, ik(Ky, pr));
     N3 = add(N3, ik(Kz, pr));
     const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
-    const double ehu = a.eu[0][m] * eyz_u, eht = a.et[0][m] * eyz_t;
+    const double ehu = eu0[m] * eyz_u, eht = et0[m] * eyz_t;
     const bool dz = dealias_zero(g.dealias, 1, m, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
