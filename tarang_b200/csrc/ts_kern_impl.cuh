@@ -345,9 +345,15 @@ template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const 
       constexpr int CW = cw_for(NN, E);
       const int inner = g.Ny * g.Hz;
       const size_t sm = 3ull * NN * CW * sizeof(V);
-      auto k = k_sff_fwd_x<T, NN, E, CW>;
+      // from 64 points on, the x kernel writes the assembled vectors and a coalesced
+      // elementwise kernel does the epilogue (its ten state reads stalled the fused form)
+      constexpr bool SPLIT = NN >= 64;
+      auto k = k_sff_fwd_x<T, NN, E, CW, SPLIT>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((const V*)P, g, a, (const V*)tq);
+      k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((V*)P, g, a, (const V*)tq);
+      ++g_launches;
+      if ((err = cudaGetLastError()) != cudaSuccess || !SPLIT) return;
+      k_sff_epi<T><<<dim3(grid1d(g.S, 256), nmem), 256, 0, st>>>((const V*)P, g, a);
       ++g_launches;
       err = cudaGetLastError();
     }

@@ -110,6 +110,80 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 }
 
 // ---------------------------------------------------------------------------
+// Boussinesq epilogue at spectral element (m, ly, lz) of batch member mb (offset
+// `off` in a component): force U.F1 = T, T.F = U.V1 of the stage input, SFF
+// projection, IF-RK4 stage update of U (nu) and T (kappa).  N1..N3, NT = the
+// assembled nonlinear terms (before the force).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, long long mb, int m, int ly, int lz,
+                                             long long off, C<T> N1, C<T> N2, C<T> N3, C<T> NT) {
+  typedef C<T> V;
+  const V* U0 = reinterpret_cast<const V*>(a.U0) + mb * a.msU0;
+  const V* T0 = reinterpret_cast<const V*>(a.T0) + mb * a.msT0;
+  V* Uc = reinterpret_cast<V*>(a.Ucur) + mb * a.msUcur;
+  V* tot = reinterpret_cast<V*>(a.tot) + mb * a.msTot;
+  const V* U1in = reinterpret_cast<const V*>(a.U1in) + mb * a.msU1in;
+  const V* Tin = reinterpret_cast<const V*>(a.Tin) + mb * a.msTin;
+  const long long tb = mb * a.mtab;
+  const double Kxd = m * g.kf[0], Kyd = kfft(ly, g.Ny) * g.kf[1], Kzd = lz * g.kf[2];
+  const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+  // force (ULARGE): U.F1 = T, T.F = U.V1 of the stage input; nlin -= F
+  N1 = sub(N1, Tin[off]);
+  NT = sub(NT, U1in[off]);
+  // projection with SFF parities: div = +Kx N1 + i Ky N2 + i Kz N3; grad_x p = -Kx p
+  const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+  const V div = add(add(scale(N1, Kx), ik(Ky, N2)), ik(Kz, N3));
+  const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+  N1 = add(N1, scale(pr, -Kx));
+  N2 = add(N2, ik(Ky, pr));
+  N3 = add(N3, ik(Kz, pr));
+  const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
+  const double ehu = a.eu[0][tb + m] * a.eu[1][tb + ly] * a.eu[2][tb + lz];
+  const double eht = a.et[0][tb + m] * a.et[1][tb + ly] * a.et[2][tb + lz];
+  const bool dz = dealias_zero(g.dealias, 1, m, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double eh = i < 3 ? ehu : eht;
+    const T Eh = (T)eh, E1 = (T)(eh * eh);
+    const long long o = i * g.S + off;
+    const V R = Rv[i];
+    const V u0 = i < 3 ? U0[o] : T0[off];
+    if (a.stage == 1) {
+      Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+      tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+    } else if (a.stage == 2) {
+      Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+      tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+    } else if (a.stage == 3) {
+      Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+      tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+    } else {
+      V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+      if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
+      if (i < 3) const_cast<V*>(U0)[o] = un;
+      else const_cast<V*>(T0)[off] = un;
+    }
+  }
+}
+
+// Elementwise Boussinesq epilogue (the split form of k_sff_fwd_x): N1..N3, NT
+// in P components 0-3 of member blockIdx.y; one thread per element, every array
+// access coalesced.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sff_epi(const C<T>* __restrict__ P, Geo g, SffArgs a) {
+  const long long mb = blockIdx.y;
+  P += mb * a.msP;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), m = (int)(r / g.Ny);
+    sff_epilogue<T>(g, a, mb, m, ly, lz, e, P[e], P[g.S + e], P[2 * g.S + e], P[3 * g.S + e]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // forward x pass + Boussinesq epilogue (PRLARGE / ULARGE):
 //   N1 = Dx(u1u1) + iKy F[u1u2] + iKz F[u3u1],  N2 = iKy F[u2u2] + Dx(u1u2) + iKz F[u2u3],
 //   N3 = iKz F[u3u3] + iKy F[u2u3] + Dx(u3u1),  NT = Dx(u1T) + iKy F[u2T] + iKz F[u3T]
@@ -122,9 +196,9 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 // elements it reads back, in FFT input order, so the reordering is done by the
 // copy and no barrier guards the staging tiles.
 // Shared memory: exchange tile + 2 staging tiles of N x CW complex.
-template <typename T, int N, int E, int CW>
+template <typename T, int N, int E, int CW, bool SPLIT>
 __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
-    k_sff_fwd_x(const C<T>* __restrict__ P, Geo g, SffArgs a, const C<T>* __restrict__ tq) {
+    k_sff_fwd_x(C<T>* __restrict__ P, Geo g, SffArgs a, const C<T>* __restrict__ tq) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
@@ -208,57 +282,16 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     }
   }
   if (!ok) return;
-  const V* U0 = reinterpret_cast<const V*>(a.U0) + mb * a.msU0;
-  const V* T0 = reinterpret_cast<const V*>(a.T0) + mb * a.msT0;
-  V* Uc = reinterpret_cast<V*>(a.Ucur) + mb * a.msUcur;
-  V* tot = reinterpret_cast<V*>(a.tot) + mb * a.msTot;
-  const V* U1in = reinterpret_cast<const V*>(a.U1in) + mb * a.msU1in;
-  const V* Tin = reinterpret_cast<const V*>(a.Tin) + mb * a.msTin;
-  const double* eu0 = a.eu[0] + mb * a.mtab;
-  const double* et0 = a.et[0] + mb * a.mtab;
-  const double eyz_u = a.eu[1][mb * a.mtab + ly] * a.eu[2][mb * a.mtab + lz];
-  const double eyz_t = a.et[1][mb * a.mtab + ly] * a.et[2][mb * a.mtab + lz];
 #pragma unroll
   for (int s = 0; s < E; ++s) {
     const int m = final_row<N, E>(t, s);
     const long long off = m * rstride + col;
-    const double Kxd = m * g.kf[0];
-    const T Kx = (T)Kxd;
-    // force (ULARGE): U.F1 = T, T.F = U.V1 of the stage input; nlin -= F
-    V N1 = sub(acc[0][s], Tin[off]), N2 = acc[1][s], N3 = acc[2][s];
-    const V NT = sub(acc[3][s], U1in[off]);
-    // projection with SFF parities: div = +Kx N1 + i Ky N2 + i Kz N3; grad_x p = -Kx p
-    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
-    const V div = add(add(scale(N1, Kx), ik(Ky, N2)), ik(Kz, N3));
-    const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
-    N1 = add(N1, scale(pr, -Kx));
-    N2 = add(N2, ik(Ky, pr));
-    N3 = add(N3, ik(Kz, pr));
-    const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
-    const double ehu = eu0[m] * eyz_u, eht = et0[m] * eyz_t;
-    const bool dz = dealias_zero(g.dealias, 1, m, ly, lz, g.Nx, g.Ny, g.Nz);
+    if (SPLIT) {
+      // the assembled vectors replace products 0-3 of this column (every read of them is done)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const double eh = i < 3 ? ehu : eht;
-      const T Eh = (T)eh, E1 = (T)(eh * eh);
-      const long long o = i * g.S + off;
-      const V R = Rv[i];
-      const V u0 = i < 3 ? U0[o] : T0[off];
-      if (a.stage == 1) {
-        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
-      } else if (a.stage == 2) {
-        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
-      } else if (a.stage == 3) {
-        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
-      } else {
-        V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
-        if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
-        if (i < 3) const_cast<V*>(U0)[o] = un;
-        else const_cast<V*>(T0)[off] = un;
-      }
+      for (int i = 0; i < 4; ++i) P[i * g.S + off] = acc[i][s];
+    } else {
+      sff_epilogue<T>(g, a, mb, m, ly, lz, off, acc[0][s], acc[1][s], acc[2][s], acc[3][s]);
     }
   }
 }
