@@ -848,28 +848,50 @@ int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed
   });
 }
 
+// parity string -> x basis: FFF plans take "FFF"; SFF plans take "SFF" (sine
+// along x) or "CFF" (cosine), the first letter of the reference's
+// sincostr_switch entries (global/Global.cc:137-145).  Returns -1 if invalid.
+static int x_parity(const ts_plan* p, const char* parity) {
+  if (p->cfg.basis == TS_BASIS_FFF) return strcmp(parity, "FFF") == 0 ? 0 : -1;
+  if (strcmp(parity, "SFF") == 0) return 1;
+  if (strcmp(parity, "CFF") == 0) return 2;
+  return -1;
+}
+
 int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* spec_out, int ncomp) {
   if (!p || !parity || !real_in || !spec_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
-  if (strcmp(parity, "FFF") != 0) return TS_ERR_ARG;
+  const int xp = x_parity(p, parity);
+  if (xp < 0) {
+    g_last_error = "parity must be \"FFF\" (FFF plan) or \"SFF\" / \"CFF\" (SFF plan)";
+    return TS_ERR_ARG;
+  }
   if (!is_device_ptr(real_in) || !is_device_ptr(spec_out)) return TS_ERR_ARG;
   const Geo& g = p->g;
   CK(LAUNCH(p, z_single, g, -1, real_in, spec_out, ncomp, p->twz, p->st));
   CK(LAUNCH(p, strided, g, 1, -1, spec_out, ncomp, p->twy, p->st));
-  CK(LAUNCH(p, strided, g, 0, -1, spec_out, ncomp, p->twx, p->st));
-  CK(LAUNCH(p, scale, spec_out, ncomp * g.S, 1.0 / ((double)g.Nx * g.Ny * g.Nz), p->st));
+  if (xp == 0) {
+    CK(LAUNCH(p, strided, g, 0, -1, spec_out, ncomp, p->twx, p->st));
+    CK(LAUNCH(p, scale, spec_out, ncomp * g.S, 1.0 / ((double)g.Nx * g.Ny * g.Nz), p->st));
+  } else {
+    // sin/cos analysis / (2 Nx) along x (SFF_pencil_tr.cc:43-55), Fourier / (Ny Nz) along y, z
+    CK(LAUNCH(p, sff_x, g, -1, spec_out, ncomp, xp == 1, 1.0 / (2.0 * g.Nx * (double)g.Ny * g.Nz), p->twq, p->st));
+  }
   return TS_OK;
 }
 
 int ts_fft_inverse(ts_plan* p, const char* parity, const void* spec_in, void* real_out, int ncomp) {
   if (!p || !parity || !spec_in || !real_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
-  if (strcmp(parity, "FFF") != 0) return TS_ERR_ARG;
+  const int xp = x_parity(p, parity);
+  if (xp < 0) {
+    g_last_error = "parity must be \"FFF\" (FFF plan) or \"SFF\" / \"CFF\" (SFF plan)";
+    return TS_ERR_ARG;
+  }
   if (!is_device_ptr(spec_in) || !is_device_ptr(real_out)) return TS_ERR_ARG;
   const Geo& g = p->g;
   // the reference copies the input to X_transform first (FFF_pencil_tr.cc:59)
   CK(cudaMemcpyAsync(p->P, spec_in, ncomp * g.S * p->cb, cudaMemcpyDeviceToDevice, p->st));
-  CK(LAUNCH(p, strided, g, 0, +1, p->P, ncomp, p->twx, p->st));
+  if (xp == 0) CK(LAUNCH(p, strided, g, 0, +1, p->P, ncomp, p->twx, p->st));
+  else CK(LAUNCH(p, sff_x, g, +1, p->P, ncomp, xp == 1, 1.0, p->twq, p->st));
   CK(LAUNCH(p, strided, g, 1, +1, p->P, ncomp, p->twy, p->st));
   CK(LAUNCH(p, z_single, g, +1, p->P, real_out, ncomp, p->twz, p->st));
   return TS_OK;

@@ -361,6 +361,30 @@ template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const 
   return err;
 }
 
+template <> cudaError_t Launch<T>::sff_x(const Geo& g, int dir, void* A, int ncomp, int sine, double scl,
+                                         const void* tq, cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  dispatch_L_sff(g.Nx, [&](auto Lc) {
+    constexpr int NN = decltype(Lc)::value;
+    if constexpr (NN <= 512) {
+      constexpr int E = e_mixed(NN, 8);
+      constexpr int CW = cw_for(NN, E);
+      const int inner = g.Ny * g.Hz;
+      const size_t sm = (size_t)NN * CW * sizeof(V);
+      const dim3 grid((inner + CW - 1) / CW, ncomp);
+      auto run = [&](auto k) {
+        if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+        k<<<grid, CW * (NN / E), sm, st>>>((V*)A, g, (const V*)tq, sine, scl);
+        ++g_launches;
+        err = cudaGetLastError();
+      };
+      if (dir < 0) run(k_sff_x<T, NN, E, CW, -1>);
+      else run(k_sff_x<T, NN, E, CW, 1>);
+    }
+  });
+  return err;
+}
+
 template <> cudaError_t Launch<T>::reality(const Geo& g, void* A, int ncomp, cudaStream_t st) {
   const long long n = (long long)g.Nx * g.Ny * ncomp;
   k_reality<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((V*)A, ncomp, g);

@@ -35,6 +35,9 @@ template <typename T> struct Launch {
                                int nmem = 1, long long msU = 0, long long msT = 0, long long msW = 0);
   static cudaError_t sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq, cudaStream_t st,
                                int nmem = 1);
+  // standalone sin/cos x transform of ncomp components in place (dir -1 forward with scale scl, +1 inverse)
+  static cudaError_t sff_x(const Geo& g, int dir, void* A, int ncomp, int sine, double scl, const void* tq,
+                           cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,

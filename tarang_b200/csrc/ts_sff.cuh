@@ -110,6 +110,80 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 }
 
 // ---------------------------------------------------------------------------
+// Standalone sin/cos transform along x, in place on component blockIdx.y of A
+// (spectral layout: rows lx, columns ly*Hz + lz): the x part of
+// SFF_PENCIL::Forward_transform / Inverse_transform (SFF_pencil_tr.cc:43-68)
+// for one parity (sine != 0: S, else C).
+// DIR = -1: rows hold real-space x points (after the z and y transforms); the
+//           coefficients c_m * (2N * scl) replace them (scl carries the y, z
+//           normalisation as well).
+// DIR = +1: rows hold coefficients; the unscaled synthesis replaces them.
+// Every thread loads its rows before the first barrier inside the FFT and
+// stores after the last one, so the in-place update needs no extra buffer.
+// ---------------------------------------------------------------------------
+template <typename T, int N, int E, int CW, int DIR>
+__global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
+    k_sff_x(C<T>* __restrict__ A, Geo g, const C<T>* __restrict__ tq, int sine, double scl) {
+  typedef C<T> V;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* xch = reinterpret_cast<V*>(smraw);
+  const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+  const int inner = g.Ny * g.Hz;
+  const int col = blockIdx.x * CW + c;
+  const bool ok = col < inner;
+  const long long rstride = inner;
+  V* a = A + blockIdx.y * g.S + (ok ? col : 0);
+  V v[E];
+  if (DIR < 0) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int k = load_row<N, E>(t, s);
+      V x = ok ? a[(k < N / 2 ? 2 * k : 2 * (N - 1 - k) + 1) * rstride] : mk<V>(0, 0);
+      if (sine && k >= N / 2) x = scale(x, (T)-1);
+      v[s] = x;
+    }
+    fft_regs<N, E, -1>(v, t, xch, CW, c, tq, 4);
+#pragma unroll
+    for (int s = 0; s < E; ++s) xch[final_row<N, E>(t, s) * CW + c] = v[s];
+    __syncthreads();
+    V zr[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) zr[s] = xch[((N - final_row<N, E>(t, s)) % N) * CW + c];
+    if (ok) {
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int m = final_row<N, E>(t, s);
+        const V wz = mul(tq[m], v[s]), wzr = mul(conjg(tq[m]), zr[s]);
+        a[m * rstride] = sine ? mul_i<1>(scale(sub(wz, wzr), (T)scl)) : scale(add(wz, wzr), (T)scl);
+      }
+    }
+  } else {
+    auto coef = [&](int q) -> V { return (ok && q > 0 && q < N) ? a[q * rstride] : mk<V>(0, 0); };
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int m = load_row<N, E>(t, s);
+      V z;
+      if (m == 0) {
+        z = (!sine && ok) ? a[0] : mk<V>(0, 0);
+      } else {
+        const V p = sine ? coef(N - m) : coef(m), q = sine ? coef(m) : coef(N - m);
+        z = mul(conjg(tq[m]), sub(p, mul_i<1>(q)));
+      }
+      v[s] = z;
+    }
+    fft_regs<N, E, 1>(v, t, xch, CW, c, tq, 4);
+    if (ok) {
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int k = final_row<N, E>(t, s);
+        const int n = k < N / 2 ? 2 * k : 2 * (N - 1 - k) + 1;
+        a[n * rstride] = (sine && (n & 1)) ? scale(v[s], (T)-1) : v[s];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Boussinesq epilogue at spectral element (m, ly, lz) of batch member mb (offset
 // `off` in a component): force U.F1 = T, T.F = U.V1 of the stage input, SFF
 // projection, IF-RK4 stage update of U (nu) and T (kappa).  N1..N3, NT = the

@@ -95,3 +95,45 @@ def test_rbc_linear_growth_above_critical(cuda):
     plan.rk4_step_rbc(u, T, 60)
     torch.cuda.synchronize()
     assert plan.energy(T) / e0 > 1.1
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("parity", ["SFF", "CFF"])
+@pytest.mark.parametrize("N", [(16, 16, 16), (32, 16, 64), (64, 32, 16), (48, 16, 16)])
+def test_sff_transforms_match_oracle(cuda, N, parity, prec):
+    """SFF_PENCIL::Forward/Inverse_transform through ts_fft_forward / ts_fft_inverse (x parity S or C)."""
+    import torch
+    import tarang_b200 as tb
+    if N[0] % 3 == 0 and prec == "f64":
+        pytest.skip("48- and 96-point SFF plans are FP32")
+    g = R.Grid(N, KF, "SFF")
+    plan = tb.Plan(N, basis="SFF", kfactor=KF, precision=prec)
+    rng = np.random.default_rng(2)
+    u = rng.standard_normal((2,) + N)
+    rdt = torch.float64 if prec == "f64" else torch.float32
+    real = torch.zeros((2, N[0], N[1], N[2] + 2), dtype=rdt, device=cuda)
+    real[..., : N[2]] = torch.from_numpy(u).to(rdt)
+    spec = plan.field(2)
+    plan.forward(real, spec, parity=parity)
+    torch.cuda.synchronize()
+    par = parity[0]
+    ref = np.stack([R.forward(g, u[i], par) for i in range(2)])
+    tol = 1e-13 if prec == "f64" else 2e-6
+    assert rel(spec.cpu().numpy(), ref) < tol
+    back = torch.zeros_like(real)
+    plan.inverse(spec, back, parity=parity)
+    torch.cuda.synchronize()
+    ub = back.cpu().numpy()
+    assert rel(ub[..., : N[2]], np.stack([R.inverse(g, ref[i], par) for i in range(2)])) < tol
+    assert np.all(ub[..., N[2]:] == 0)
+    # the input of the inverse is not modified
+    assert rel(spec.cpu().numpy(), ref) < tol
+
+
+def test_sff_transform_rejects_wrong_parity(cuda):
+    import torch
+    import tarang_b200 as tb
+    plan = tb.Plan((16, 16, 16), basis="SFF", kfactor=KF)
+    real = torch.zeros((1, 16, 16, 18), dtype=torch.float64, device=cuda)
+    with pytest.raises(tb.TsError):
+        plan.forward(real, plan.field(1), parity="FFF")
