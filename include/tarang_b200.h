@@ -131,6 +131,17 @@ int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, i
  * N = F[(u.grad)u] of the dealiased U (one pass; equals EnergyTr::Compute_flux,
  * compute_flux.cc:51-65, for alias-free fields).  radii ascending. */
 int ts_flux(ts_plan* plan, const void* u_hat, const double* radii, int n_radii, double* Pi);
+/* Raw shell sums for the reference's text outputs: sums[k] = sum over modes with
+ * ceil|K| = k of mult K^2 Re(A . conj(B)) (B = NULL: |A|^2), counts[k] = sum of
+ * 2 mult (Compute_local_shell_spectrum / _force, universal_energy.cc:196-229,
+ * 279-310; E(k) = sums 4 pi / (counts kf1 kf2 kf3)).  Device pointers; either
+ * output may be NULL. */
+int ts_shell_sums(ts_plan* plan, const void* a_hat, const void* b_hat, int ncomp, double* sums, double* counts,
+                  int n_shells);
+/* The Carati force of state u_hat (FORCE::Compute_force, compute_force_Carati.cc:158-205)
+ * as a full spectral field f_hat (3 components, zero outside the forcing band);
+ * device pointers. */
+int ts_force_field(ts_plan* plan, const void* u_hat, void* f_hat);
 /* max |div U| (universal_basic.cc:343-356). */
 int ts_max_div(ts_plan* plan, const void* u_hat, double* max_div);
 /* Nusselt number, PRLARGE/ULARGE (Correlation.cc:154-156). */

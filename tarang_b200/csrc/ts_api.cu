@@ -773,6 +773,43 @@ int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int 
   });
 }
 
+int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, double* sums, double* counts,
+                  int n_shells) {
+  if (!p || !a_hat || ncomp < 1 || ncomp > 3 || n_shells < 1 || (!sums && !counts)) return TS_ERR_ARG;
+  if (!is_device_ptr(a_hat) || (b_hat && !is_device_ptr(b_hat))) {
+    g_last_error = "ts_shell_sums: device pointers required";
+    return TS_ERR_ARG;
+  }
+  const int nsh = p->nshells;
+  CKS(ensure_scratch(p, 2 * nsh));
+  CK(cudaMemsetAsync(p->dscr, 0, 2 * nsh * sizeof(double), p->st));
+  CK(LAUNCH(p, shell, p->g, a_hat, ncomp, nsh - 1, p->dscr, p->st, b_hat));
+  std::vector<double> h(2 * nsh);
+  CK(cudaMemcpyAsync(h.data(), p->dscr, 2 * nsh * sizeof(double), cudaMemcpyDeviceToHost, p->st));
+  CK(cudaStreamSynchronize(p->st));
+  for (int i = 0; i < n_shells; ++i) {
+    if (sums) sums[i] = i < nsh ? h[i] : 0.0;
+    if (counts) counts[i] = i < nsh ? h[nsh + i] : 0.0;
+  }
+  return TS_OK;
+}
+
+int ts_force_field(ts_plan* p, const void* u_hat, void* f_hat) {
+  if (!p || !u_hat || !f_hat) return TS_ERR_ARG;
+  if (p->cfg.force_type != TS_FORCE_CARATI_ENERGY_SUPPLY) {
+    g_last_error = "ts_force_field: the plan has no Carati forcing";
+    return TS_ERR_UNSUPPORTED;
+  }
+  if (!is_device_ptr(u_hat) || !is_device_ptr(f_hat)) return TS_ERR_ARG;
+  const Geo& g = p->g;
+  CK(LAUNCH(p, carati, g, u_hat, p->fcube, p->fkm, p->cfg.force_inner_radius, p->cfg.force_outer_radius, p->esup,
+            p->hsup, p->mis_d, p->nsup, p->st));
+  CK(cudaMemsetAsync(f_hat, 0, 3 * g.S * p->cb, p->st));
+  CK(LAUNCH(p, force_scatter, g, p->fcube, f_hat, p->fkm, p->st));
+  CK(cudaStreamSynchronize(p->st));
+  return TS_OK;
+}
+
 int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, double* Pi) {
   if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;

@@ -424,11 +424,18 @@ template <> cudaError_t Launch<T>::maxdiv(const Geo& g, const void* U, unsigned 
 }
 
 template <> cudaError_t Launch<T>::shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins,
-                                         cudaStream_t st) {
+                                         cudaStream_t st, const void* B) {
   const size_t sm = 2ull * (kmax + 1) * sizeof(double);
   cudaError_t err = smem_attr(k_shell<T>, sm);
   if (err != cudaSuccess) return err;
-  k_shell<T><<<grid1d(g.S, 256), 256, sm, st>>>((const V*)A, ncomp, g, kmax, bins);
+  k_shell<T><<<grid1d(g.S, 256), 256, sm, st>>>((const V*)A, ncomp, g, kmax, bins, (const V*)B);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::force_scatter(const Geo& g, const void* fc, void* F, int km, cudaStream_t st) {
+  const long long n = 3LL * (2 * km + 1) * (2 * km + 1) * (km + 1);
+  k_force_scatter<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const V*)fc, (V*)F, g, km);
   ++g_launches;
   return cudaGetLastError();
 }

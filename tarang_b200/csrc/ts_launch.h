@@ -44,7 +44,10 @@ template <typename T> struct Launch {
                             const double* hs, const double* mis, int nsup, cudaStream_t st);
   static cudaError_t energy(const Geo& g, const void* A, const void* B, int ncomp, double* out, cudaStream_t st);
   static cudaError_t maxdiv(const Geo& g, const void* U, unsigned long long* out, cudaStream_t st);
-  static cudaError_t shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins, cudaStream_t st);
+  // B != nullptr: cross spectrum Re(A . conj(B))
+  static cudaError_t shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins, cudaStream_t st,
+                           const void* B = nullptr);
+  static cudaError_t force_scatter(const Geo& g, const void* fc, void* F, int km, cudaStream_t st);
   static cudaError_t init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
                              unsigned long long key, cudaStream_t st);
   static cudaError_t scale(void* A, long long n, double s, cudaStream_t st);

@@ -64,6 +64,21 @@ __global__ void k_reality_adj(C<T>* A, int ncomp, Geo g) {
   a[((long long)lx * g.Ny + ly) * Hz + g.Nz / 2] = mk<V>(0, 0);
 }
 
+// Scatter the force cube (3 components of (2km+1)^2 (km+1) modes, kx, ky = -km..km,
+// kz = 0..km) into a full spectral field F (zeroed by the caller).
+template <typename T>
+__global__ void k_force_scatter(const C<T>* __restrict__ fc, C<T>* __restrict__ F, Geo g, int km) {
+  const int n = 2 * km + 1;
+  const long long ncube = (long long)n * n * (km + 1);
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 3 * ncube) return;
+  const int c = (int)(e / ncube);
+  const long long r = e % ncube;
+  const int kx = (int)(r / (n * (km + 1))) - km, ky = (int)((r / (km + 1)) % n) - km, lz = (int)(r % (km + 1));
+  const int lx = (kx + g.Nx) % g.Nx, ly = (ky + g.Ny) % g.Ny;
+  F[c * g.S + ((long long)lx * g.Ny + ly) * g.Hz + lz] = fc[e];
+}
+
 // ---------------------------------------------------------------------------
 // Carati constant-energy-supply force (non-global alpha/beta) on the cube
 // |kx|,|ky|,kz <= km; compute_force_Carati.cc:158-205, force_alpha_beta.cc:56-85,
@@ -250,7 +265,8 @@ __device__ __forceinline__ double multiplicity(int basis, int lx, int ly, int lz
 // bins[s] += mult |K|^2 sum_i |A_i|^2 ; bins[nsh + s] += 2 mult, s = ceil|K| <= kmax.
 // Block-private shared bins, then one global atomic per bin.
 template <typename T>
-__global__ void k_shell(const C<T>* __restrict__ A, int ncomp, Geo g, int kmax, double* bins) {
+__global__ void k_shell(const C<T>* __restrict__ A, int ncomp, Geo g, int kmax, double* bins,
+                        const C<T>* __restrict__ B = nullptr) {
   extern __shared__ double sb[];
   const int nsh = kmax + 1;
   for (int i = threadIdx.x; i < 2 * nsh; i += blockDim.x) sb[i] = 0;
@@ -267,10 +283,11 @@ __global__ void k_shell(const C<T>* __restrict__ A, int ncomp, Geo g, int kmax, 
     const int idx = (int)ceil(Kmag);
     if (idx > kmax) continue;
     const double f = multiplicity(g.basis, lx, ly, lz, g.Nx, g.Ny);
+    // |A|^2, or Re(A . conj(B)) for a cross spectrum
     double a2 = 0;
     for (int i = 0; i < ncomp; ++i) {
-      const C<T> a = A[i * n + e];
-      a2 += (double)a.x * a.x + (double)a.y * a.y;
+      const C<T> a = A[i * n + e], b = B ? B[i * n + e] : a;
+      a2 += (double)a.x * b.x + (double)a.y * b.y;
     }
     atomicAdd(&sb[idx], f * a2 * (Kmag * Kmag));
     atomicAdd(&sb[nsh + idx], 2 * f);

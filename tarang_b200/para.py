@@ -1,0 +1,317 @@
+"""Run inputs and text outputs in the reference's formats, for the hot-path subset.
+
+Inputs (a reference data directory ``<dir>/in/``):
+
+* ``para.yaml`` — the keys the IF-RK4 step reads (``Global::Read``,
+  global/Global_read.cc:319-450): ``program.kind``, ``program.basis_type``,
+  ``program.alias_option``, ``program.apply_strong_realitycond_alltime_switch``,
+  ``field.N``, ``field.kfactor`` / ``field.L``, ``field.diss_coefficients``,
+  ``time.init / final / dt_fixed``, ``force.U_switch / field_procedure /
+  parameters``, ``PHYSICS.Pr_option / Uscaling / Rayleigh / Prandtl`` and
+  ``energy_transfer.flux.no_spheres / radii``.  Any other kind or basis is
+  refused by name (NotImplementedError), never silently changed.
+* ``initial.txt`` / ``forcing.txt`` — Blitz++ 1-D arrays as text,
+  ``(lb,ub)`` then ``[ v0 v1 ... ]`` (``Global::Read_IC_energy_supply_arrays``,
+  Global_read.cc:822-850): E(k), H(k) of the initial condition and the energy /
+  helicity supply per shell.
+
+Outputs (``<dir>/out/``), in the layouts the reference writes and its
+post-processors read:
+
+* ``spectrum.d`` — per time ``%% Time = t``, a line with one space, then
+  ``%%<label>`` and one tab-separated row per component
+  (``FluidIO::Output_shell_spectrum``, fluid_base/io/output/output_energy.cc:844-868,
+  ``Print_array`` fluid_base/io/FluidIO.h:327-418);
+* ``flux.d`` — per time an empty line, ``%% Time = t``, ``%%flux: U2U `` and the
+  Pi(R) row (``Output_flux``, incompressible/incio/output/output_ET.cc:46-86);
+* ``glob.d`` — one tab-separated row per time (``Global::io::Dump_buffer``,
+  global/Global.cc:447-459) with time, total energy, total dissipation and dt.
+"""
+from __future__ import annotations
+
+import math
+import os
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+INF_RADIUS = 1e9   # the last flux sphere encloses every mode
+
+
+@dataclass
+class RunParams:
+    kind: str
+    basis: str
+    N: tuple
+    kfactor: tuple
+    dealias: str                 # "reference" (alias_option DEALIAS) or "none"
+    reality_fix: bool
+    nu: float
+    kappa: float
+    dt: float
+    t_init: float
+    t_final: float
+    Ra: float | None = None
+    Pr: float | None = None
+    force_on: bool = False
+    force_inner: float | None = None
+    force_outer: float | None = None
+    force_global_alpha_beta: bool = False
+    flux_radii: list = field(default_factory=list)
+
+    @property
+    def nsteps(self) -> int:
+        return int(round((self.t_final - self.t_init) / self.dt))
+
+
+def _flag(v) -> bool:
+    if isinstance(v, bool):
+        return v
+    return str(v).strip().lower() in ("1", "true", "yes", "on")
+
+
+def read_blitz_arrays(path: str) -> list:
+    """All ``(lb,ub) [ ... ]`` 1-D arrays of a Blitz++ text file, in order."""
+    text = open(path).read()
+    out = []
+    for m in re.finditer(r"\(\s*(-?\d+)\s*,\s*(-?\d+)\s*\)\s*\[([^\]]*)\]", text):
+        lb, ub = int(m.group(1)), int(m.group(2))
+        vals = np.array([float(x) for x in m.group(3).split()], dtype=np.float64)
+        if vals.size != ub - lb + 1:
+            raise ValueError(f"{path}: array ({lb},{ub}) holds {vals.size} values")
+        out.append(vals)
+    return out
+
+
+def max_radius_inside(N, kfactor) -> int:
+    """``Max_radius_inside`` for the FFF basis with waveno_switch (FFF_pencil_inline.h:509-539)."""
+    Nx, Ny, Nz = N
+    if Ny > 1:
+        return int(min((Nx // 2) * kfactor[0], (Ny // 2) * kfactor[1], (Nz // 2) * kfactor[2]))
+    return int(min((Nx // 2) * kfactor[0], (Nz // 2) * kfactor[2]))
+
+
+def default_flux_radii(no_spheres: int, rmax: float) -> list:
+    """The sphere radii the reference builds when none are given
+    (Global_process_advanced_vars.cc:133-154): 0, 2, 4, 8, then geometric up to
+    rmax/2, rmax and INF_RADIUS; no_spheres + 1 values."""
+    r = [0.0] * (no_spheres + 1)
+    fixed = [0.0, 2.0, 4.0, 8.0]
+    for i, v in enumerate(fixed):
+        if i <= no_spheres:
+            r[i] = v
+    r[no_spheres - 2] = rmax / 2.0
+    r[no_spheres - 1] = float(rmax)
+    r[no_spheres] = INF_RADIUS
+    if no_spheres > 6:
+        s = math.log2(rmax / 16.0) / (no_spheres - 5)
+        for i in range(4, no_spheres - 2):
+            r[i] = 8 * 2 ** (s * (i - 3))
+    return r
+
+
+def read_para(path: str) -> RunParams:
+    """The hot-path subset of a reference ``para.yaml``."""
+    import yaml
+    with open(path) as f:
+        p = yaml.safe_load(f)
+    prog, fld, tim = p["program"], p["field"], p["time"]
+    kind = str(prog["kind"]).strip()
+    basis = str(prog["basis_type"]).strip()
+    if (kind, basis) not in (("FLUID_INCOMPRESS", "FFF"), ("RBC", "SFF")):
+        raise NotImplementedError(f"program.kind {kind} with basis_type {basis}: this library steps "
+                                  "FLUID_INCOMPRESS on FFF and RBC on SFF")
+    N = tuple(int(n) for n in fld["N"])
+    # kfactor, else from L, else the basis defaults (FFF_pencil.cc:34-66, SFF_pencil.cc:40-80)
+    if fld.get("kfactor") and len(fld["kfactor"]) == 3:
+        kf = tuple(float(k) for k in fld["kfactor"])
+    elif fld.get("L") and len(fld["L"]) == 3:
+        # Fourier directions: 2 pi / L; the sin/cos direction: pi / L
+        L = [float(x) for x in fld["L"]]
+        kf = tuple((math.pi if (basis[i] in "SC") else 2 * math.pi) / L[i] for i in range(3))
+    elif kind == "RBC":
+        kf = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+    else:
+        kf = (1.0, 1.0, 1.0)
+    alias = str(prog.get("alias_option", "DEALIAS")).strip()
+    diss = [float(x) for x in (fld.get("diss_coefficients") or [0.0])]
+    rp = RunParams(kind=kind, basis=basis, N=N, kfactor=kf,
+                   dealias="reference" if alias == "DEALIAS" else "none",
+                   reality_fix=_flag(prog.get("apply_strong_realitycond_alltime_switch", False)),
+                   nu=diss[0], kappa=diss[1] if len(diss) > 1 else 0.0,
+                   dt=float(tim["dt_fixed"]), t_init=float(tim.get("init") or 0.0), t_final=float(tim["final"]))
+    if kind == "RBC":
+        ph = p.get("PHYSICS") or {}
+        pr_opt = str(ph.get("Pr_option", "PRLARGE")).strip()
+        usc = str(ph.get("Uscaling", "USMALL")).strip()
+        if (pr_opt, usc) != ("PRLARGE", "ULARGE"):
+            raise NotImplementedError(f"PHYSICS Pr_option {pr_opt} / Uscaling {usc}: PRLARGE / ULARGE only")
+        rp.Ra = float(ph.get("Rayleigh", 2000.0))
+        rp.Pr = float(ph.get("Prandtl", 1.0))
+        # ULARGE (Iscalar_main.cc:52-92): nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra)
+        rp.nu = math.sqrt(rp.Pr / rp.Ra)
+        rp.kappa = 1.0 / math.sqrt(rp.Pr * rp.Ra)
+    force = p.get("force") or {}
+    if _flag(force.get("U_switch", False)):
+        procs = force.get("field_procedure") or []
+        procs = procs if isinstance(procs, list) else [procs]
+        if kind == "FLUID_INCOMPRESS":
+            if [int(x) for x in procs] != [1]:
+                raise NotImplementedError(f"force.field_procedure {procs}: Carati energy supply (1) only")
+            params = force.get("parameters") or []
+            words = str(params[0] if isinstance(params, list) else params).split()
+            if not words or words[0] != "ENERGY_SUPPLY" or len(words) < 4:
+                raise NotImplementedError(f"force.parameters {params}: 'ENERGY_SUPPLY global inner outer' only")
+            rp.force_on = True
+            rp.force_global_alpha_beta = _flag(words[1])
+            rp.force_inner, rp.force_outer = float(words[2]), float(words[3])
+            if rp.force_global_alpha_beta:
+                raise NotImplementedError("ENERGY_SUPPLY with global_alpha_beta = 1: the non-global branch only")
+    et = p.get("energy_transfer") or {}
+    fl = et.get("flux") or {}
+    if _flag(et.get("turnon", False)) and _flag(fl.get("turnon", False)):
+        ns = int(fl.get("no_spheres") or 0)
+        radii = fl.get("radii")
+        if radii and len(radii) == ns + 1:
+            rp.flux_radii = [float(x) for x in radii]
+        elif ns > 0:
+            rp.flux_radii = default_flux_radii(ns, max_radius_inside(N, kf))
+    return rp
+
+
+def plan_from_dir(data_dir: str, precision: str = "f64", nlin_form: str = "conservative"):
+    """(Plan, RunParams) for a reference data directory (``in/para.yaml`` and, for a
+    forced run, ``in/forcing.txt``)."""
+    from .solver import Forcing, Plan
+    rp = read_para(os.path.join(data_dir, "in", "para.yaml"))
+    forcing = None
+    if rp.force_on:
+        arrs = read_blitz_arrays(os.path.join(data_dir, "in", "forcing.txt"))
+        forcing = Forcing(rp.force_inner, rp.force_outer, arrs[0], arrs[1] if len(arrs) > 1 else None)
+    kw = dict(precision=precision, dealias=rp.dealias, kfactor=rp.kfactor, reality_fix=rp.reality_fix, dt=rp.dt)
+    if rp.kind == "RBC":
+        plan = Plan(rp.N, basis="SFF", nu=rp.nu, kappa=rp.kappa, Ra=rp.Ra, Pr=rp.Pr, **kw)
+    else:
+        plan = Plan(rp.N, nlin_form=nlin_form, nu=rp.nu, forcing=forcing, **kw)
+    return plan, rp
+
+
+# ----------------------------------------------------------------------------
+# text outputs
+# ----------------------------------------------------------------------------
+def _row(values) -> str:
+    """One Print_array row: every value followed by a tab (ostream_iterator with "\\t")."""
+    return "".join(f"{float(v):g}\t" for v in values) + "\n"
+
+
+def write_spectrum(f, t: float, ek: list, dissk: list | None = None, force_k: list | None = None):
+    """One time block of spectrum.d: %%Uek (one row per component), %%UDk, %%(Fv.v)(k)."""
+    f.write(f"%% Time = {t:g}\n \n")
+    for label, rows in (("Uek", ek), ("UDk", dissk), ("(Fv.v)(k)", force_k)):
+        if rows is None:
+            continue
+        f.write(f"%%{label}\n")
+        for r in rows:
+            f.write(_row(r))
+
+
+def write_flux(f, t: float, flux, power_in_sphere=None):
+    """One time block of flux.d: %%flux: U2U  and optionally %%sum(Fv.v)."""
+    f.write(f"\n%% Time = {t:g}\n")
+    f.write("%%flux: U2U \n")
+    f.write(_row(flux))
+    if power_in_sphere is not None:
+        f.write("%%sum(Fv.v)\n")
+        f.write(_row(power_in_sphere))
+
+
+def write_glob_row(f, values):
+    """One glob.d row (Dump_buffer: tab-separated packet, newline)."""
+    f.write(_row(values))
+
+
+def _fff_multiplicity(kx, ky, kz, Nx, Ny):
+    """Multiplicity_factor (FFF_pencil_inline.h:583-602): 1 (kz > 0) or 1/2 (kz = 0),
+    doubled on the kx = Nx/2 and ky = Ny/2 planes."""
+    f = np.where(kz > 0, 1.0, 0.5)
+    return np.where((kx == Nx // 2) | ((ky == Ny // 2) & (Ny > 1)), 2 * f, f)
+
+
+class Output:
+    """Appends out/spectrum.d and out/flux.d for an FFF plan in the reference's layouts.
+
+    spectrum.d (FluidIO::Output_shell_spectrum): %%Uek = per-component shell
+    spectra (Compute_shell_spectrum, n = 0); %%UDk = 2 x per-component raw sums of
+    mult K^2 |A|^2, rescaled by Approx_number_modes_in_shell / count beyond the
+    inscribed sphere (Compute_shell_spectrum_force with n = 2,
+    universal_energy.cc:196-262); for a forced plan %%(Fv.v)(k) = 2 x the
+    component cross spectra of u and the force (Compute_force_shell_spectrum,
+    Correlation.cc:457-469).
+    flux.d (Output_flux): %%flux: U2U = Pi(R_i) (ts_flux) and %%sum(Fv.v) = the
+    power the force puts into the shells between consecutive radii, modes inside
+    the inscribed sphere only (Shell_mult_all, universal_ET.cc:145-176).
+    """
+
+    def __init__(self, plan, out_dir: str, radii=None):
+        if plan.basis != "FFF":
+            raise NotImplementedError("Output writes the FFF fluid layouts")
+        os.makedirs(out_dir, exist_ok=True)
+        self.plan = plan
+        self.out_dir = out_dir
+        self.kf = tuple(plan.cfg.kfactor[i] for i in range(3))
+        self.kmax_inside = max_radius_inside(plan.N, self.kf)
+        self.radii = list(radii) if radii is not None else default_flux_radii(8, self.kmax_inside)
+        self.forced = plan.cfg.force_type != 0
+
+    def _force(self, u):
+        return self.plan.force_field(u, self.plan.field(3)) if self.forced else None
+
+    def spectrum(self, u, t: float):
+        p = self.plan
+        kfp = self.kf[0] * self.kf[1] * self.kf[2]
+        idx = np.arange(p.n_shells, dtype=np.float64)
+        approx = 4 * math.pi * idx ** 2 / kfp    # Approx_number_modes_in_shell (FFF_pencil_inline.h:558-565)
+        ek, dissk, fvk = [], [], None
+        for i in range(3):
+            ui = u[i:i + 1]
+            ek.append(p.shell_spectrum(ui, 1))
+            s, c = p.shell_sums(ui, ncomp=1)
+            d = s.copy()
+            out = (idx > self.kmax_inside) & (c >= 1)
+            d[out] = s[out] * approx[out] / c[out]
+            dissk.append(2 * d)
+        if self.forced:
+            F = self._force(u)
+            fvk = []
+            for i in range(3):
+                s, c = p.shell_sums(u[i:i + 1], F[i:i + 1], ncomp=1)
+                fvk.append(2 * np.where(c > 0, s * 4 * math.pi / np.where(c > 0, c, 1) / kfp, 0.0))
+        with open(os.path.join(self.out_dir, "spectrum.d"), "a") as f:
+            write_spectrum(f, t, ek, dissk, fvk)
+
+    def flux(self, u, t: float):
+        p = self.plan
+        Pi = p.flux(u, self.radii)
+        power = None
+        if self.forced:
+            F = self._force(u)
+            Nx, Ny, Nz = p.N
+            km = int(math.ceil(p.cfg.force_outer_radius / min(self.kf)))
+            kx = np.arange(-km, km + 1)
+            kz = np.arange(0, km + 1)
+            import torch
+            lx = torch.as_tensor(kx % Nx, device=u.device)
+            ly = torch.as_tensor(kx % Ny, device=u.device)
+            Fc = F[:, lx][:, :, ly][..., :km + 1].cpu().numpy()
+            Uc = u[:, lx][:, :, ly][..., :km + 1].cpu().numpy()
+            KX, KY, KZ = np.meshgrid(kx, kx, kz, indexing="ij")
+            K = np.sqrt((KX * self.kf[0]) ** 2 + (KY * self.kf[1]) ** 2 + (KZ * self.kf[2]) ** 2)
+            dot = np.sum((Fc * np.conj(Uc)).real, axis=0)
+            w = 2 * _fff_multiplicity(KX, KY, KZ, Nx, Ny) * dot
+            power = np.zeros(len(self.radii))
+            ins = K <= self.kmax_inside
+            b = np.searchsorted(np.asarray(self.radii), K[ins], side="left")   # first radius >= |K|
+            np.add.at(power, np.minimum(b, len(self.radii) - 1), w[ins])
+        with open(os.path.join(self.out_dir, "flux.d"), "a") as f:
+            write_flux(f, t, Pi, power)

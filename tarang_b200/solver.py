@@ -178,6 +178,20 @@ class Plan:
                 "ts_shell_spectrum")
         return out
 
+    def shell_sums(self, a, b=None, ncomp: int | None = None):
+        """Raw shell sums (sum mult K^2 Re(a . conj(b)), or |a|^2) and counts (sum 2 mult) per shell."""
+        n = a.shape[0] if ncomp is None else ncomp
+        sums, counts = np.zeros(self.n_shells), np.zeros(self.n_shells)
+        L.check(self.lib.ts_shell_sums(self.h, _ptr(a), _ptr(b) if b is not None else None, n,
+                                       sums.ctypes.data_as(L._D), counts.ctypes.data_as(L._D), self.n_shells),
+                "ts_shell_sums")
+        return sums, counts
+
+    def force_field(self, u, out):
+        """The Carati force of state u as a full spectral field (zero outside the band)."""
+        L.check(self.lib.ts_force_field(self.h, _ptr(u), _ptr(out)), "ts_force_field")
+        return out
+
     def flux(self, u, radii) -> np.ndarray:
         r = np.ascontiguousarray(radii, dtype=np.float64)
         out = np.zeros(len(r))

@@ -1,0 +1,157 @@
+"""Reading reference-format run inputs (para.yaml, forcing.txt) and writing the
+reference's text outputs (spectrum.d, flux.d, glob.d).  CPU only, except the last
+test, which steps a run built from a para.yaml on the GPU against the oracle."""
+import io
+import math
+import os
+
+import numpy as np
+import pytest
+
+from tarang_b200 import para
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FFF_DIR = os.path.join(HERE, "golden", "para_fff")
+RBC_DIR = os.path.join(HERE, "golden", "para_rbc")
+
+
+def test_read_para_fff_forced():
+    rp = para.read_para(os.path.join(FFF_DIR, "in", "para.yaml"))
+    assert (rp.kind, rp.basis, rp.N, rp.kfactor) == ("FLUID_INCOMPRESS", "FFF", (32, 32, 32), (1.0, 1.0, 1.0))
+    assert rp.dealias == "reference" and rp.reality_fix
+    assert rp.nu == 0.01 and rp.dt == 0.001 and rp.nsteps == 4
+    assert rp.force_on and (rp.force_inner, rp.force_outer) == (2.0, 3.0) and not rp.force_global_alpha_beta
+    # no radii given: the reference's default spheres for 8 spheres and max radius 16
+    assert rp.flux_radii == [0.0, 2.0, 4.0, 8.0, 8.0, 8.0, 8.0, 16.0, para.INF_RADIUS]
+
+
+def test_read_para_rbc_from_L():
+    rp = para.read_para(os.path.join(RBC_DIR, "in", "para.yaml"))
+    assert rp.kind == "RBC" and rp.basis == "SFF" and rp.N == (32, 16, 16)
+    # L = (1, 2, 2): pi / L along the sin/cos direction, 2 pi / L along the Fourier ones
+    assert np.allclose(rp.kfactor, (math.pi, math.pi, math.pi))
+    assert rp.Ra == 1e5 and rp.Pr == 2.0
+    assert math.isclose(rp.nu, math.sqrt(2.0 / 1e5)) and math.isclose(rp.kappa, 1.0 / math.sqrt(2e5))
+    assert rp.nsteps == 100 and not rp.force_on
+
+
+def test_default_flux_radii_geometric():
+    r = para.default_flux_radii(10, 64)
+    assert r[:4] == [0.0, 2.0, 4.0, 8.0]
+    assert r[8] == 32.0 and r[9] == 64.0 and r[10] == para.INF_RADIUS
+    s = math.log2(64 / 16.0) / 5
+    assert np.allclose(r[4:8], [8 * 2 ** (s * (i - 3)) for i in range(4, 8)])
+    assert all(r[i] <= r[i + 1] for i in range(10))
+
+
+def test_blitz_arrays_and_unsupported(tmp_path):
+    arrs = para.read_blitz_arrays(os.path.join(FFF_DIR, "in", "forcing.txt"))
+    assert len(arrs) == 2 and arrs[0].shape == (7,) and arrs[0][3] == 0.1 and not arrs[1].any()
+    bad = tmp_path / "para.yaml"
+    bad.write_text("program:\n  kind: MHD_INCOMPRESS\n  basis_type: FFF\nfield:\n  N: [8,8,8]\ntime:\n  dt_fixed: 0.1\n  final: 1\n")
+    with pytest.raises(NotImplementedError):
+        para.read_para(str(bad))
+    (tmp_path / "b").write_text("(0,2)\n[ 1 2 ]\n")
+    with pytest.raises(ValueError):
+        para.read_blitz_arrays(str(tmp_path / "b"))
+
+
+def test_output_layouts():
+    f = io.StringIO()
+    ek = [np.arange(4.0), np.arange(4.0) + 1, np.arange(4.0) + 2]
+    para.write_spectrum(f, 0.5, ek, [2 * e for e in ek], [3 * e for e in ek])
+    lines = f.getvalue().split("\n")
+    # 14 lines per time block (+ the empty string after the last newline), as the reference writes them
+    assert len(lines) == 15 and lines[-1] == ""
+    assert lines[0] == "%% Time = 0.5" and lines[1] == " " and lines[2] == "%%Uek" and lines[6] == "%%UDk"
+    assert lines[10] == "%%(Fv.v)(k)"
+    assert lines[3] == "0\t1\t2\t3\t" and [float(x) for x in lines[13].split("\t")[:-1]] == [6, 9, 12, 15]
+    g = io.StringIO()
+    para.write_flux(g, 1.25, [0.0, 0.1, 0.25])
+    assert g.getvalue() == "\n%% Time = 1.25\n%%flux: U2U \n0\t0.1\t0.25\t\n"
+    h = io.StringIO()
+    para.write_glob_row(h, [0.1, 0.5, 2e-3, 1e-3])
+    assert h.getvalue() == "0.1\t0.5\t0.002\t0.001\t\n"
+
+
+@pytest.mark.gpu
+def test_plan_from_para_steps_like_the_oracle(cuda):
+    """A forced FFF run set up from para.yaml + forcing.txt matches the oracle over its 4 steps."""
+    import torch
+    from oracle import tarang_ref as R
+    plan, rp = para.plan_from_dir(FFF_DIR, precision="f64")
+    g = R.Grid(rp.N, rp.kfactor)
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    es = para.read_blitz_arrays(os.path.join(FFF_DIR, "in", "forcing.txt"))[0]
+    cfg = R.FluidConfig(g, nu=rp.nu, dt=rp.dt, dealias_mode=1, forcing=R.CaratiForcing(rp.force_inner, rp.force_outer, es))
+    W = V.copy()
+    for _ in range(rp.nsteps):
+        W = R.rk4_step(cfg, W)
+    u = torch.from_numpy(V.copy()).to(cuda)
+    plan.rk4_step(u, rp.nsteps)
+    torch.cuda.synchronize()
+    d = u.cpu().numpy() - W
+    assert np.linalg.norm(d) / np.linalg.norm(W) < 1e-12
+
+
+def _read_blocks(path, label):
+    """Rows under %%label in every time block of a reference text output."""
+    rows, cur = [], None
+    for line in open(path).read().split("\n"):
+        if line.startswith("%%"):
+            cur = line[2:] == label
+            if cur:
+                rows.append([])
+            continue
+        if cur and line.strip():
+            rows[-1].append(np.array([float(x) for x in line.split("\t")[:-1]]))
+    return rows
+
+
+@pytest.mark.gpu
+def test_output_spectrum_and_flux_match_oracle(cuda, tmp_path):
+    """spectrum.d / flux.d written from a forced 32^3 state against the oracle's quantities."""
+    import torch
+    from oracle import tarang_ref as R
+    plan, rp = para.plan_from_dir(FFF_DIR, precision="f64")
+    g = R.Grid(rp.N, rp.kfactor)
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    u = torch.from_numpy(V.copy()).to(cuda)
+    out = para.Output(plan, str(tmp_path), radii=rp.flux_radii)
+    out.spectrum(u, 0.0)
+    out.flux(u, 0.0)
+    # oracle quantities
+    Kmag = g.Kmag()
+    idx = np.ceil(Kmag).astype(int)
+    mult = g.multiplicity()
+    nsh = g.n_shells()
+    ok = idx < nsh
+    cnt = np.bincount(idx[ok], weights=2 * mult[ok], minlength=nsh)
+    kin = para.max_radius_inside(rp.N, rp.kfactor)
+    sh = np.arange(nsh)
+    es = para.read_blitz_arrays(os.path.join(FFF_DIR, "in", "forcing.txt"))[0]
+    F = R.carati_force(g, V, R.CaratiForcing(rp.force_inner, rp.force_outer, es), g.modes_in_shell())
+    ek = _read_blocks(tmp_path / "spectrum.d", "Uek")[0]
+    ud = _read_blocks(tmp_path / "spectrum.d", "UDk")[0]
+    fv = _read_blocks(tmp_path / "spectrum.d", "(Fv.v)(k)")[0]
+    for i in range(3):
+        ref = R.shell_spectrum(g, V[i:i + 1])
+        assert np.allclose(ek[i], ref, rtol=2e-5, atol=1e-6 * ref.max())
+        raw = np.bincount(idx[ok], weights=(mult * Kmag ** 2 * np.abs(V[i]) ** 2)[ok], minlength=nsh)
+        beyond = (sh > kin) & (cnt >= 1)
+        raw[beyond] *= (4 * np.pi * sh[beyond] ** 2) / cnt[beyond]
+        assert np.allclose(ud[i], 2 * raw, rtol=2e-5, atol=1e-6 * raw.max())
+        cr = np.bincount(idx[ok], weights=(mult * Kmag ** 2 * (V[i] * np.conj(F[i])).real)[ok], minlength=nsh)
+        ref_f = 2 * np.where(cnt > 0, cr * 4 * np.pi / np.where(cnt > 0, cnt, 1), 0.0)
+        assert np.allclose(fv[i], ref_f, rtol=2e-5, atol=1e-6 * np.abs(ref_f).max())
+    flux = _read_blocks(tmp_path / "flux.d", "flux: U2U ")[0][0]
+    assert np.allclose(flux, R.flux_one_pass(g, V, rp.flux_radii, 1), rtol=2e-5, atol=1e-9)
+    power = _read_blocks(tmp_path / "flux.d", "sum(Fv.v)")[0][0]
+    dot = 2 * mult * np.sum((F * np.conj(V)).real, axis=0)
+    ins = Kmag <= kin
+    b = np.searchsorted(np.asarray(rp.flux_radii), Kmag[ins], side="left")
+    ref_p = np.zeros(len(rp.flux_radii))
+    np.add.at(ref_p, b, dot[ins])
+    assert np.allclose(power, ref_p, rtol=2e-5, atol=1e-9)
+    # the total power equals the energy injection 2 sum mult Re(F.u*) = epsilon (0.1) up to 6 digits
+    assert abs(power.sum() - 0.1) < 1e-5
