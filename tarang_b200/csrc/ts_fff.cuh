@@ -214,6 +214,24 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
   const long long rstride = inner;
   constexpr int nout = inv_x_nout(FORM);
   const T lw = (lz > 0 && 2 * lz < g.Nz) ? lsc * (T)0.5 : lsc;
+  // FP32 with up to 8 elements per thread: the three (dealiased) components of U
+  // are loaded once, up front, and every output field is built from registers
+  // (FP64 would spill them)
+  constexpr bool UPFRONT = E <= 8 && sizeof(T) == 4;
+  V u[UPFRONT ? 3 : 1][UPFRONT ? E : 1];
+  if constexpr (UPFRONT) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int lx = load_row<L, E>(t, s);
+      const long long off = lx * rstride + col;
+      const bool z = !ok || dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u[c][s] = z ? mk<V>(0, 0) : U[c * g.S + off];
+    }
+  }
+  // unrolled (register path) so that the register-array indices below are compile-time constants
+  constexpr int kUnroll = UPFRONT ? nout : 1;
+#pragma unroll kUnroll
   for (int f = 0; f < nout; ++f) {
     V v[E];
 #pragma unroll
@@ -221,7 +239,17 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
       const int lx = load_row<L, E>(t, s);
       const long long off = lx * rstride + col;
       V a = mk<V>(0, 0);
-      if (FORM == 3 && f >= 6) {
+      if (UPFRONT && f < 6) {
+        if (f < 3) {
+          a = u[f][s];
+        } else {
+          const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
+          const int i = f - 3, i1 = i == 2 ? 0 : i + 1, i2 = i == 0 ? 2 : i - 1;
+          const T Ka = i1 == 0 ? Kx : (i1 == 1 ? Ky : Kz);
+          const T Kb = i2 == 0 ? Kx : (i2 == 1 ? Ky : Kz);
+          a = mul_i<1>(sub(scale(u[i2][s], Ka), scale(u[i1][s], Kb)));
+        }
+      } else if (FORM == 3 && f >= 6) {
         if (ok) {
           // (P Lam)_i = Lam_i - K_i (K . Lam) / K^2, identity at K = 0
           const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
@@ -398,6 +426,46 @@ template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 64
 // from global memory (a line spread over several warps; the second read of the
 // line hits L1), then the length-M inverse FFT (forward radix schedule) leaves
 // the packed real line in registers
+// rows t + s*TPL of a line (and X[M] on lane t = 0) into registers; issued for
+// every component of a line before any of them is transformed
+template <typename T, int M, int E, int TPL>
+__device__ __forceinline__ void zreg_load(const C<T>* X, bool live, int t, C<T> (&a)[E], C<T>& XM) {
+  typedef C<T> V;
+#pragma unroll
+  for (int s = 0; s < E; ++s) a[s] = live ? X[t + s * TPL] : mk<V>(0, 0);
+  XM = (live && t == 0) ? X[M] : mk<V>(0, 0);
+}
+
+// C2R of a loaded line: a holds rows t + s*TPL, XM = X[M] (lane t = 0); the
+// result (packed real line) replaces a
+template <typename T, int M, int E, int TPL>
+__device__ __forceinline__ void zreg_inverse_loaded(const C<T>* X, bool live, int t, int partner,
+                                                    const C<T>* __restrict__ tw, C<T>* xch, C<T> (&a)[E],
+                                                    const C<T>& XM) {
+  typedef C<T> V;
+  V out[E];
+#pragma unroll
+  for (int s = 0; s < E; ++s) {
+    // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
+    V b;
+    if constexpr (TPL <= 32) {
+      b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
+      b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
+      if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
+    } else {
+      b = live ? X[M - (t + s * TPL)] : mk<V>(0, 0);
+    }
+    b = conjg(b);
+    V x = a[s];
+    const int k = t + s * TPL;
+    if (k == 0) { x.y = 0; b.y = 0; }
+    out[s] = add(add(x, b), mul_i<1>(mul(conjg(tw[k]), sub(x, b))));
+  }
+  fft_regs<M, E, 1, 0, true, false>(out, t, xch, 1, 0, tw, 2);
+#pragma unroll
+  for (int s = 0; s < E; ++s) a[s] = out[s];
+}
+
 template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_inverse(const C<T>* X, bool live, int t, int partner,
                                              const C<T>* __restrict__ tw, C<T>* xch, C<T> (&out)[E]) {
@@ -483,9 +551,19 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), 6)
   V* xch = xch_all + l * LDX;
 
   V in[NIN][E];
+  if constexpr (TPL <= 32) {
+    // lines within a warp: every component's loads are issued before the first transform
+    V XM[NIN];
 #pragma unroll
-  for (int c = 0; c < NIN; ++c)
-    zreg_inverse<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c]);
+    for (int c = 0; c < NIN; ++c) zreg_load<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, in[c], XM[c]);
+#pragma unroll
+    for (int c = 0; c < NIN; ++c)
+      zreg_inverse_loaded<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c], XM[c]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < NIN; ++c)
+      zreg_inverse<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c]);
+  }
   // real-space products; each complex register holds two real points
   if (FORM == 1) {
 #pragma unroll

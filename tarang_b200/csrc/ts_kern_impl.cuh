@@ -142,7 +142,9 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
     constexpr int LL = decltype(Lc)::value;
     // the direct-load kernel measured faster than the TMA-staged k_inv_x on B200
     // (0.19 vs 0.28 ms at 256^3 FP32, rotational); k_inv_x stays available
-    constexpr int E = wide1024(LL) ? 16 : e_reg(LL);
+    // 8 elements per thread (U held in registers across the output fields; 16 at
+    // L = 1024 in FP32, with per-field loads)
+    constexpr int E = wide1024(LL) ? 16 : (std::is_same<T, float>::value ? (8 < LL ? 8 : LL) : e_reg(LL));
     constexpr int CW = wide1024(LL) ? 8 : cw_for(LL, E);
     const int inner = g.Ny * g.Hz;
     const size_t sm = (size_t)LL * CW * sizeof(V);
