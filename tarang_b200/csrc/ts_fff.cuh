@@ -426,18 +426,28 @@ template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 64
 // from global memory (a line spread over several warps; the second read of the
 // line hits L1), then the length-M inverse FFT (forward radix schedule) leaves
 // the packed real line in registers
-// rows t + s*TPL of a line (and X[M] on lane t = 0) into registers; issued for
-// every component of a line before any of them is transformed
+// Register layout of a line: with a first radix equal to E (powers of two), slot
+// s of lane t holds row t + s*TPL on input (forward schedule) and on output
+// (reversed schedule), and the pair terms X[M-k] sit in the partner lane of the
+// same warp (TPL <= 32): warp shuffles.  Otherwise (a line over two warps, or a
+// radix-3 schedule whose rows follow load_row / final_row) the inverse reads the
+// pair terms from global memory (L1 hits) and the forward swaps them through the
+// line's exchange buffer.
+template <int M, int E, int TPL> __host__ __device__ constexpr bool zreg_shfl() {
+  return radix_at(M, E, 0) == E && TPL <= 32;
+}
+
+// rows of a line into registers (and X[M] on lane t = 0 for the shuffle path);
+// issued for every component of a line before any of them is transformed
 template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_load(const C<T>* X, bool live, int t, C<T> (&a)[E], C<T>& XM) {
   typedef C<T> V;
 #pragma unroll
-  for (int s = 0; s < E; ++s) a[s] = live ? X[t + s * TPL] : mk<V>(0, 0);
-  XM = (live && t == 0) ? X[M] : mk<V>(0, 0);
+  for (int s = 0; s < E; ++s) a[s] = live ? X[load_row<M, E>(t, s)] : mk<V>(0, 0);
+  XM = (zreg_shfl<M, E, TPL>() && live && t == 0) ? X[M] : mk<V>(0, 0);
 }
 
-// C2R of a loaded line: a holds rows t + s*TPL, XM = X[M] (lane t = 0); the
-// result (packed real line) replaces a
+// C2R of a loaded line (a, XM from zreg_load); the packed real line replaces a
 template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_inverse_loaded(const C<T>* X, bool live, int t, int partner,
                                                     const C<T>* __restrict__ tw, C<T>* xch, C<T> (&a)[E],
@@ -447,17 +457,17 @@ __device__ __forceinline__ void zreg_inverse_loaded(const C<T>* X, bool live, in
 #pragma unroll
   for (int s = 0; s < E; ++s) {
     // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
+    const int k = load_row<M, E>(t, s);
     V b;
-    if constexpr (TPL <= 32) {
+    if constexpr (zreg_shfl<M, E, TPL>()) {
       b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
       b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
       if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
     } else {
-      b = live ? X[M - (t + s * TPL)] : mk<V>(0, 0);
+      b = live ? X[M - k] : mk<V>(0, 0);
     }
     b = conjg(b);
     V x = a[s];
-    const int k = t + s * TPL;
     if (k == 0) { x.y = 0; b.y = 0; }
     out[s] = add(add(x, b), mul_i<1>(mul(conjg(tw[k]), sub(x, b))));
   }
@@ -470,28 +480,9 @@ template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_inverse(const C<T>* X, bool live, int t, int partner,
                                              const C<T>* __restrict__ tw, C<T>* xch, C<T> (&out)[E]) {
   typedef C<T> V;
-  V a[E];
-#pragma unroll
-  for (int s = 0; s < E; ++s) a[s] = live ? X[t + s * TPL] : mk<V>(0, 0);
-  const V XM = (live && t == 0) ? X[M] : mk<V>(0, 0);
-#pragma unroll
-  for (int s = 0; s < E; ++s) {
-    // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
-    V b;
-    if constexpr (TPL <= 32) {
-      b.x = __shfl_sync(0xffffffffu, a[E - 1 - s].x, partner);
-      b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
-      if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
-    } else {
-      b = live ? X[M - (t + s * TPL)] : mk<V>(0, 0);
-    }
-    b = conjg(b);
-    V x = a[s];
-    const int k = t + s * TPL;
-    if (k == 0) { x.y = 0; b.y = 0; }
-    out[s] = add(add(x, b), mul_i<1>(mul(conjg(tw[k]), sub(x, b))));
-  }
-  fft_regs<M, E, 1, 0, true, false>(out, t, xch, 1, 0, tw, 2);
+  V XM;
+  zreg_load<T, M, E, TPL>(X, live, t, out, XM);
+  zreg_inverse_loaded<T, M, E, TPL>(X, live, t, partner, tw, xch, out, XM);
 }
 
 // R2C of one packed real line in registers (reversed radix schedule, so the
@@ -500,42 +491,48 @@ template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool live, int t, int partner,
                                                    const C<T>* __restrict__ tw, C<T>* xch) {
   typedef C<T> V;
+  constexpr bool SH = zreg_shfl<M, E, TPL>();
   fft_regs<M, E, -1, 0, true, true>(p, t, xch, 1, 0, tw, 2);
-  // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]; rows k = t + s*TPL.
-  // A line spread over several warps swaps the pair terms through its exchange line.
-  if constexpr (TPL > 32) {
+  // X[k] = 1/2 (Z + Z') - i/2 w^k (Z - Z'), Z' = conj(Z[M-k]), Z[M] = Z[0]
+  if constexpr (!SH) {
 #pragma unroll
-    for (int s = 0; s < E; ++s) xch[prow<true>(t + s * TPL)] = p[s];
+    for (int s = 0; s < E; ++s) xch[prow<true>(final_row<M, E, true>(t, s))] = p[s];
     __syncthreads();
   }
 #pragma unroll
   for (int s = 0; s < E; ++s) {
+    const int k = final_row<M, E, true>(t, s);
     V zp;
-    if constexpr (TPL <= 32) {
+    if constexpr (SH) {
       zp.x = __shfl_sync(0xffffffffu, p[E - 1 - s].x, partner);
       zp.y = __shfl_sync(0xffffffffu, p[E - 1 - s].y, partner);
       if (t == 0) zp = p[(E - s) % E];
     } else {
-      zp = xch[prow<true>((M - (t + s * TPL)) % M)];
+      zp = xch[prow<true>((M - k) % M)];
     }
     zp = conjg(zp);
-    const int k = t + s * TPL;
     const V z = p[s];
     const V o = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[k], scale(sub(z, zp), (T)0.5))));
     if (live) Xo[k] = o;
+    if (k == 0 && live) {
+      // X[M] = Re Z[0] + Im Z[0] (Z[M] = Z[0])
+      const V zc = conjg(z);
+      Xo[M] = add(scale(add(z, zc), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zc), (T)0.5))));
+    }
   }
-  if (live && t == 0) {
-    const V z = p[0], zp = conjg(p[0]);
-    Xo[M] = add(scale(add(z, zp), (T)0.5), mul_i<-1>(mul(tw[M], scale(sub(z, zp), (T)0.5))));
-  }
-  if constexpr (TPL > 32) __syncthreads();  // the exchange line is reused next
+  if constexpr (!SH) __syncthreads();  // the exchange line is reused next
 }
 
+// blocks per SM the register z kernel is compiled for: 6 (170 registers), 3 for
+// the 12-element radix-3 lines (which would spill at 170)
+template <int NZ> __host__ __device__ constexpr int zreg_min_blocks() { return (NZ / 2) % 3 == 0 ? 3 : 6; }
+
 template <typename T, int NZ, int FORM>
-__global__ void __launch_bounds__(zreg_threads<FORM>(), 6)
+__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP) {
   typedef C<T> V;
-  constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
+  // 8 elements per thread, 12 for a line length with a factor 3 (radices 4, 2|4, 3)
+  constexpr int M = NZ / 2, H = M + 1, E = (M % 3 == 0) ? 12 : 8, TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   static_assert(NIN <= 6, "the adjoint form runs in k_z_reg_adj");
