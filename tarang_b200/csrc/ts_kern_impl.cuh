@@ -324,7 +324,7 @@ template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const 
       constexpr int E = e_mixed(NN, 8);
       constexpr int CW = cw_for(NN, E);
       const int inner = g.Ny * g.Hz;
-      const size_t sm = (size_t)NN * CW * sizeof(V);
+      const size_t sm = 3ull * NN * CW * sizeof(V);  // exchange + 2 staging tiles
       auto k = k_sff_inv_x<T, NN, E, CW>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
       k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g,

@@ -56,6 +56,10 @@ __host__ __device__ constexpr bool sff_prod_sine(int f) { return f == 3 || f == 
 // ---------------------------------------------------------------------------
 // inverse x pass: W_f = inverse sin/cos transform of D(field_f), f = u1,u2,u3,T.
 // tq: 4N entries exp(-2 pi i j/(4N)) (every fourth entry is the N-point FFT table).
+// The four fields' columns stream through two cp.async staging tiles (field f+2
+// is in flight while f is transformed); the pre-processing pairs rows m and
+// N - m, so a barrier follows each tile's arrival.
+// Shared memory: exchange tile + 2 staging tiles of N x CW complex.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int E, int CW>
 __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
@@ -64,6 +68,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
+  V* stage = xch + N * CW;
   // member blockIdx.y of a batch (strides 0 for one run)
   U += blockIdx.y * msU;
   Tf += blockIdx.y * msT;
@@ -74,13 +79,29 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
   const bool ok = col < inner;
   const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
   const long long rstride = inner;
+  auto issue = [&](int f, int buf) {
+    if (f < 4 && ok) {
+      const V* src = (f < 3 ? U + f * g.S : Tf) + col;
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        const int m = load_row<N, E>(t, s);
+        cp_async(stage + (buf * N + m) * CW + c, src + m * rstride);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0, 0);
+  issue(1, 1);
   for (int f = 0; f < 4; ++f) {
-    const V* src = (f < 3 ? U + f * g.S : Tf) + (ok ? col : 0);
     const bool sine = f == 0 || f == 3;
-    // coefficient q of the (dealiased) series; 0 outside 0..N-1
+    const int buf = f & 1;
+    cp_async_wait<1>();
+    __syncthreads();  // every thread's rows of field f have arrived
+    const V* st = stage + buf * N * CW + c;
+    // coefficient q of the (dealiased) series; 0 outside 1..N-1
     auto coef = [&](int q) -> V {
       if (!ok || q <= 0 || q >= N || dealias_zero(g.dealias, 1, q, ly, lz, g.Nx, g.Ny, g.Nz)) return mk<V>(0, 0);
-      return src[q * rstride];
+      return st[q * CW];
     };
     V v[E];
 #pragma unroll
@@ -89,13 +110,15 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
       V z;
       if (m == 0) {
         // cosine: V_0 = c_0; sine: V_0 = 0
-        z = (!sine && ok && !dealias_zero(g.dealias, 1, 0, ly, lz, g.Nx, g.Ny, g.Nz)) ? src[0] : mk<V>(0, 0);
+        z = (!sine && ok && !dealias_zero(g.dealias, 1, 0, ly, lz, g.Nx, g.Ny, g.Nz)) ? st[0] : mk<V>(0, 0);
       } else {
         const V p = sine ? coef(N - m) : coef(m), q = sine ? coef(m) : coef(N - m);
         z = mul(conjg(tq[m]), sub(p, mul_i<1>(q)));
       }
       v[s] = z;
     }
+    __syncthreads();  // every thread has read tile buf: field f + 2 may overwrite it
+    issue(f + 2, buf);
     fft_regs<N, E, 1>(v, t, xch, CW, c, tq, 4);
     if (ok) {
       V* d = W + f * g.S + col;
