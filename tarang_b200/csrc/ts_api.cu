@@ -436,9 +436,17 @@ static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in)
   a.ez = p->eax[2];
   const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
   const int nin = rot ? 6 : 3, nout = rot ? 3 : 6;
-  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, nullptr, 0.0, p->st)); }
-  { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, nin, p->twy, p->st)); }
-  { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->err_d, p->st)); }
+  // two-thirds dealiasing: after the x inverse only the columns with 3|ky| <= Ny and
+  // 3 kz <= Nz can be nonzero, so the inverse x pass writes only those, the y
+  // inverse transforms only kz <= Nz/3 and reads only the 3|ky| <= Ny rows, and the
+  // z pass reads only kz <= Nz/3 (the skipped memory is never read)
+  const int kept = g.dealias == TS_DEALIAS_TWO_THIRDS;
+  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, nullptr, 0.0, p->st, kept)); }
+  {
+    ProfScope ps(p, TS_KCLASS_Y_INV);
+    CK(LAUNCH(p, strided, g, 1, +1, p->P, nin, p->twy, p->st, 0, 0, kept ? g.Nz / 3 + 1 : 0, kept));
+  }
+  { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->err_d, p->st, 1, 0, kept ? g.Nz / 3 : -1)); }
   { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, nout, p->twy, p->st)); }
   { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, fwd_x, g, rot, mode, p->P, a, p->twx, p->st)); }
   return TS_OK;
@@ -506,6 +514,7 @@ static int adjoint_supported(ts_plan* p) {
 static int adjoint_step_fff(ts_plan* p, const void* U0, const void* stages, void* lam) {
   const Geo& g = p->g;
   const long long cs = 3 * g.S * (long long)p->cb;
+  const int kept = g.dealias == TS_DEALIAS_TWO_THIRDS;
   if (p->cfg.reality_fix) {
     ProfScope ps(p, TS_KCLASS_OTHER);
     CK(LAUNCH(p, reality_adj, g, lam, 3, p->st));
@@ -528,9 +537,23 @@ static int adjoint_step_fff(ts_plan* p, const void* U0, const void* stages, void
     const void* cot = stage == 4 ? (const void*)lam : (const void*)p->Ucur;
     const double lsc = stage == 4 ? p->cfg.dt / 6.0 : 1.0;
     a.stage = stage;
-    { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, 3, Uin, p->P, p->twx, cot, lsc, p->st)); }
-    { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, 9, p->twy, p->st)); }
-    { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, 3, p->P, p->twz, p->err_d, p->st)); }
+    if (kept) {
+      // u, w (fields 0-5) on the kept columns only, as in rhs_fff; the cotangent fields 6-8 are full
+      {
+        ProfScope ps(p, TS_KCLASS_INV_X);
+        CK(LAUNCH(p, inv_x, g, 1, Uin, p->P, p->twx, nullptr, 0.0, p->st, 1));
+        CK(LAUNCH(p, inv_x, g, 4, Uin, p->P, p->twx, cot, lsc, p->st));
+      }
+      {
+        ProfScope ps(p, TS_KCLASS_Y_INV);
+        CK(LAUNCH(p, strided, g, 1, +1, p->P, 6, p->twy, p->st, 0, 0, g.Nz / 3 + 1, 1));
+        CK(LAUNCH(p, strided, g, 1, +1, (char*)p->P + 6 * g.S * (long long)p->cb, 3, p->twy, p->st));
+      }
+    } else {
+      { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, 3, Uin, p->P, p->twx, cot, lsc, p->st)); }
+      { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, 9, p->twy, p->st)); }
+    }
+    { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, 3, p->P, p->twz, p->err_d, p->st, 1, 0, kept ? g.Nz / 3 : -1)); }
     { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, 6, p->twy, p->st)); }
     { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, fwd_x, g, 3, MODE_ADJ, p->P, a, p->twx, p->st)); }
   }

@@ -39,7 +39,8 @@ struct Geo {
 template <typename T, int L, int E, int CW, int DIR, int NT = 3>
 __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     k_strided_fft(C<T>* __restrict__ data, int nf, long long fstride, int inner, long long rstride,
-                  long long ostride, int nouter, const C<T>* __restrict__ tw, int per, long long mstride) {
+                  long long ostride, int nouter, const C<T>* __restrict__ tw, int per, long long mstride,
+                  int zero_hi) {
   typedef C<T> V;
   static_assert(NT == 2 || NT == 3, "two or three tiles");
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
 #pragma unroll
         for (int s = 0; s < E; ++s) {
           const int r = load_row<L, E>(t, s);
-          cp_async(st + r * CW, d + r * rstride);
+          if (!(zero_hi && 3 * (r < L - r ? r : L - r) > L)) cp_async(st + r * CW, d + r * rstride);
         }
       }
     }
@@ -83,7 +84,11 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     V v[E];
     const V* st = stage + buf * L * CW + c;
 #pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
+    for (int s = 0; s < E; ++s) {
+      // zero_hi: rows with 3 |k| > L (two-thirds dealiased) are zero and were not loaded
+      const int r = load_row<L, E>(t, s);
+      v[s] = (ok && !(zero_hi && 3 * (r < L - r ? r : L - r) > L)) ? st[r * CW] : mk<V>(0, 0);
+    }
     // each thread read back only what it staged itself; the barrier is for the
     // exchange writes into the consumed tile (NT = 2)
     if (NT == 2) __syncthreads();
@@ -196,19 +201,34 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
 // rotational right-hand side): also W_6..8 = lsc c^-1 P Lam, the Leray-projected
 // cotangent divided by the C2R weight c (2 on the planes 0 < kz < Nz/2, else 1).
 // ---------------------------------------------------------------------------
+// FORM 4: the cotangent fields 6..8 of FORM 3 only (written at W + 6 S ...)
 __host__ __device__ constexpr int inv_x_nout(int form) { return form == 0 ? 3 : (form == 1 ? 6 : 9); }
+__host__ __device__ constexpr int inv_x_first(int form) { return form == 4 ? 6 : 0; }
 
 template <typename T, int L, int E, int CW, int FORM>
 __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     k_inv_x_ld(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw,
-               const C<T>* __restrict__ Lam, T lsc) {
+               const C<T>* __restrict__ Lam, T lsc, int kept) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int inner = g.Ny * g.Hz;
-  const int col = blockIdx.x * CW + c;
-  const bool ok = col < inner;
+  int col;
+  bool ok;
+  if (kept) {
+    // two-thirds dealiasing: only the columns with 3|ky| <= Ny and 3 kz <= Nz can be
+    // nonzero; block = (kept ly, tile of CW kept lz); the other columns are not
+    // written, and the y and z passes treat them as zero without reading them
+    const int qy = g.Ny / 3, nzk = g.Nz / 3 + 1, ntz = (nzk + CW - 1) / CW;
+    const int iy = blockIdx.x / ntz, lzc = (blockIdx.x % ntz) * CW + c;
+    const int ky = iy <= qy ? iy : iy - (2 * qy + 1);
+    ok = lzc < nzk;
+    col = ((ky + g.Ny) % g.Ny) * g.Hz + (ok ? lzc : 0);
+  } else {
+    col = blockIdx.x * CW + c;
+    ok = col < inner;
+  }
   const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
   const T Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
   const long long rstride = inner;
@@ -217,7 +237,7 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
   // FP32 with up to 8 elements per thread: the three (dealiased) components of U
   // are loaded once, up front, and every output field is built from registers
   // (FP64 would spill them)
-  constexpr bool UPFRONT = E <= 8 && sizeof(T) == 4;
+  constexpr bool UPFRONT = E <= 8 && sizeof(T) == 4 && FORM != 4;
   V u[UPFRONT ? 3 : 1][UPFRONT ? E : 1];
   if constexpr (UPFRONT) {
 #pragma unroll
@@ -232,7 +252,7 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
   // unrolled (register path) so that the register-array indices below are compile-time constants
   constexpr int kUnroll = UPFRONT ? nout : 1;
 #pragma unroll kUnroll
-  for (int f = 0; f < nout; ++f) {
+  for (int f = inv_x_first(FORM); f < nout; ++f) {
     V v[E];
 #pragma unroll
     for (int s = 0; s < E; ++s) {
@@ -249,7 +269,7 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
           const T Kb = i2 == 0 ? Kx : (i2 == 1 ? Ky : Kz);
           a = mul_i<1>(sub(scale(u[i2][s], Ka), scale(u[i1][s], Kb)));
         }
-      } else if (FORM == 3 && f >= 6) {
+      } else if ((FORM == 3 || FORM == 4) && f >= 6) {
         if (ok) {
           // (P Lam)_i = Lam_i - K_i (K . Lam) / K^2, identity at K = 0
           const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
@@ -323,7 +343,7 @@ __host__ __device__ constexpr int z_pb(int f) { return f < 3 ? f : (f < 6 ? (f =
 
 template <typename T, int NZ, int E, int FORM>
 __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int nl,
-                                                 long long msP) {
+                                                 long long msP, int zkeep) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, TPL = M / E, LDS = zslot<M>();
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
@@ -348,7 +368,9 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
     for (int s = 0; s < E; ++s) {
       const int k = load_row<M, E>(t, s);
       V a = mk<V>(0, 0), b = mk<V>(0, 0);
-      if (live) { a = X[k]; b = conjg(X[M - k]); }
+      const int zk = (FORM == 3 && c >= 6) ? M : zkeep;  // the adjoint's cotangent lines are full
+      if (live && k <= zk) a = X[k];
+      if (live && M - k <= zk) b = conjg(X[M - k]);
       if (k == 0) { a.y = 0; b.y = 0; }
       v[s] = add(add(a, b), mul_i<1>(mul(conjg(tw[k]), sub(a, b))));
     }
@@ -439,19 +461,23 @@ template <int M, int E, int TPL> __host__ __device__ constexpr bool zreg_shfl() 
 
 // rows of a line into registers (and X[M] on lane t = 0 for the shuffle path);
 // issued for every component of a line before any of them is transformed
+// (rows above zkeep are zero and not read: two-thirds dealiasing along z)
 template <typename T, int M, int E, int TPL>
-__device__ __forceinline__ void zreg_load(const C<T>* X, bool live, int t, C<T> (&a)[E], C<T>& XM) {
+__device__ __forceinline__ void zreg_load(const C<T>* X, bool live, int t, C<T> (&a)[E], C<T>& XM, int zkeep) {
   typedef C<T> V;
 #pragma unroll
-  for (int s = 0; s < E; ++s) a[s] = live ? X[load_row<M, E>(t, s)] : mk<V>(0, 0);
-  XM = (zreg_shfl<M, E, TPL>() && live && t == 0) ? X[M] : mk<V>(0, 0);
+  for (int s = 0; s < E; ++s) {
+    const int k = load_row<M, E>(t, s);
+    a[s] = (live && k <= zkeep) ? X[k] : mk<V>(0, 0);
+  }
+  XM = (zreg_shfl<M, E, TPL>() && live && t == 0 && M <= zkeep) ? X[M] : mk<V>(0, 0);
 }
 
 // C2R of a loaded line (a, XM from zreg_load); the packed real line replaces a
 template <typename T, int M, int E, int TPL>
 __device__ __forceinline__ void zreg_inverse_loaded(const C<T>* X, bool live, int t, int partner,
                                                     const C<T>* __restrict__ tw, C<T>* xch, C<T> (&a)[E],
-                                                    const C<T>& XM) {
+                                                    const C<T>& XM, int zkeep) {
   typedef C<T> V;
   V out[E];
 #pragma unroll
@@ -464,7 +490,7 @@ __device__ __forceinline__ void zreg_inverse_loaded(const C<T>* X, bool live, in
       b.y = __shfl_sync(0xffffffffu, a[E - 1 - s].y, partner);
       if (t == 0) b = (s == 0) ? XM : a[(E - s) % E];
     } else {
-      b = live ? X[M - k] : mk<V>(0, 0);
+      b = (live && M - k <= zkeep) ? X[M - k] : mk<V>(0, 0);
     }
     b = conjg(b);
     V x = a[s];
@@ -481,8 +507,8 @@ __device__ __forceinline__ void zreg_inverse(const C<T>* X, bool live, int t, in
                                              const C<T>* __restrict__ tw, C<T>* xch, C<T> (&out)[E]) {
   typedef C<T> V;
   V XM;
-  zreg_load<T, M, E, TPL>(X, live, t, out, XM);
-  zreg_inverse_loaded<T, M, E, TPL>(X, live, t, partner, tw, xch, out, XM);
+  zreg_load<T, M, E, TPL>(X, live, t, out, XM, M);
+  zreg_inverse_loaded<T, M, E, TPL>(X, live, t, partner, tw, xch, out, XM, M);
 }
 
 // R2C of one packed real line in registers (reversed radix schedule, so the
@@ -529,7 +555,7 @@ template <int NZ> __host__ __device__ constexpr int zreg_min_blocks() { return (
 
 template <typename T, int NZ, int FORM>
 __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
-    k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP) {
+    k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
   // 8 elements per thread, 12 for a line length with a factor 3 (radices 4, 2|4, 3)
   constexpr int M = NZ / 2, H = M + 1, E = (M % 3 == 0) ? 12 : 8, TPL = M / E, LDX = zslot<M>();
@@ -552,14 +578,20 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
     // lines within a warp: every component's loads are issued before the first transform
     V XM[NIN];
 #pragma unroll
-    for (int c = 0; c < NIN; ++c) zreg_load<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, in[c], XM[c]);
+    for (int c = 0; c < NIN; ++c)
+      zreg_load<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, in[c], XM[c], zkeep);
 #pragma unroll
     for (int c = 0; c < NIN; ++c)
-      zreg_inverse_loaded<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c], XM[c]);
+      zreg_inverse_loaded<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c], XM[c],
+                                        zkeep);
   } else {
 #pragma unroll
-    for (int c = 0; c < NIN; ++c)
-      zreg_inverse<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c]);
+    for (int c = 0; c < NIN; ++c) {
+      V XM;
+      zreg_load<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, in[c], XM, zkeep);
+      zreg_inverse_loaded<T, M, E, TPL>(P + c * g.S + (live ? line : 0) * H, live, t, partner, tw, xch, in[c], XM,
+                                        zkeep);
+    }
   }
   // real-space products; each complex register holds two real points
   if (FORM == 1) {
@@ -596,7 +628,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
 // ---------------------------------------------------------------------------
 template <typename T, int NZ>
 __global__ void __launch_bounds__(zreg_threads<3>(), 6)
-    k_z_reg_adj(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw) {
+    k_z_reg_adj(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int zkeep) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
@@ -615,7 +647,11 @@ __global__ void __launch_bounds__(zreg_threads<3>(), 6)
 #pragma unroll
   for (int c = 0; c < 3; ++c) zreg_inverse<T, M, E, TPL>(P + (6 + c) * g.S + lo, live, t, partner, tw, xch, mu[c]);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) zreg_inverse<T, M, E, TPL>(P + c * g.S + lo, live, t, partner, tw, xch, w[c]);
+  for (int c = 0; c < 3; ++c) {
+    V XM;
+    zreg_load<T, M, E, TPL>(P + c * g.S + lo, live, t, w[c], XM, zkeep);
+    zreg_inverse_loaded<T, M, E, TPL>(P + c * g.S + lo, live, t, partner, tw, xch, w[c], XM, zkeep);
+  }
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
     V p[E];
@@ -627,7 +663,11 @@ __global__ void __launch_bounds__(zreg_threads<3>(), 6)
     zreg_forward_store<T, M, E, TPL>(p, P + f * g.S + lo, live, t, partner, tw, xch);
   }
 #pragma unroll
-  for (int c = 0; c < 3; ++c) zreg_inverse<T, M, E, TPL>(P + (3 + c) * g.S + lo, live, t, partner, tw, xch, w[c]);
+  for (int c = 0; c < 3; ++c) {
+    V XM;
+    zreg_load<T, M, E, TPL>(P + (3 + c) * g.S + lo, live, t, w[c], XM, zkeep);
+    zreg_inverse_loaded<T, M, E, TPL>(P + (3 + c) * g.S + lo, live, t, partner, tw, xch, w[c], XM, zkeep);
+  }
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
     V p[E];
@@ -656,7 +696,7 @@ template <typename T, int NZ> __host__ __device__ constexpr int ztma_lpb() { ret
 
 template <typename T, int NZ, int FORM>
 __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw,
-                                                  int* err, long long msP) {
+                                                  int* err, long long msP, int zkeep) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, E = ztma_e<T>(), TPL = M / E, LDX = zslot<M>();
   constexpr int LPB = ztma_lpb<T, NZ>();
@@ -708,7 +748,7 @@ __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, c
       for (int s = 0; s < E; ++s) {
         // Z[k] = (X + Y) + i conj(w^k)(X - Y), Y = conj(X[M-k]); imag of X[0], X[M] dropped
         const int kk = t + s * TPL;
-        V x = X[kk], b = conjg(X[M - kk]);
+        V x = kk <= zkeep ? X[kk] : mk<V>(0, 0), b = M - kk <= zkeep ? conjg(X[M - kk]) : mk<V>(0, 0);
         if (kk == 0) { x.y = 0; b.y = 0; }
         in[c][s] = add(add(x, b), mul_i<1>(mul(conjg(tw[kk]), sub(x, b))));
       }

@@ -98,7 +98,8 @@ constexpr int str_cw(int L) { return wide1024(L) ? 8 : cw_for(L, str_e(L)); }
 constexpr int str_nt(int L) { return wide1024(L) ? 2 : 3; }
 
 template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw,
-                                           cudaStream_t st, int per, long long mstride) {
+                                           cudaStream_t st, int per, long long mstride, int inner_eff,
+                                           int zero_hi) {
   if (per <= 0) per = nf;
   cudaError_t err = cudaErrorInvalidValue;
   const int L = axis == 0 ? g.Nx : g.Ny;
@@ -107,7 +108,7 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
     constexpr int E = str_e(LL);
     constexpr int CW = str_cw(LL);
     constexpr int NT = str_nt(LL);
-    const int inner = axis == 0 ? g.Ny * g.Hz : g.Hz;
+    const int inner = inner_eff > 0 ? inner_eff : (axis == 0 ? g.Ny * g.Hz : g.Hz);
     const long long rstride = axis == 0 ? (long long)g.Ny * g.Hz : g.Hz;
     const long long ostride = axis == 0 ? 0 : (long long)g.Ny * g.Hz;
     const int nouter = axis == 0 ? 1 : g.Nx;
@@ -122,12 +123,12 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       auto k = k_strided_fft<T, LL, E, CW, -1, NT>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
       k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
-                                                    (const V*)tw, per, mstride);
+                                                    (const V*)tw, per, mstride, zero_hi);
     } else {
       auto k = k_strided_fft<T, LL, E, CW, 1, NT>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return;
       k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
-                                                    (const V*)tw, per, mstride);
+                                                    (const V*)tw, per, mstride, zero_hi);
     }
     ++g_launches;
     err = cudaGetLastError();
@@ -136,7 +137,7 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
 }
 
 template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
-                                         const void* lam, double lsc, cudaStream_t st) {
+                                         const void* lam, double lsc, cudaStream_t st, int kept) {
   cudaError_t err_ = cudaErrorInvalidValue;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
@@ -148,24 +149,28 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
     constexpr int CW = wide1024(LL) ? 8 : cw_for(LL, E);
     const int inner = g.Ny * g.Hz;
     const size_t sm = (size_t)LL * CW * sizeof(V);
-    const unsigned blocks = (unsigned)((inner + CW - 1) / CW);
+    const int nzk = g.Nz / 3 + 1;
+    const unsigned blocks = kept ? (unsigned)((2 * (g.Ny / 3) + 1) * ((nzk + CW - 1) / CW))
+                                 : (unsigned)((inner + CW - 1) / CW);
     auto run = [&](auto kern) {
       if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
-      kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc);
+      kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc, kept);
       ++g_launches;
       err_ = cudaGetLastError();
     };
     if (form == 0) run(k_inv_x_ld<T, LL, E, CW, 0>);
     else if (form == 1) run(k_inv_x_ld<T, LL, E, CW, 1>);
     else if (form == 3) run(k_inv_x_ld<T, LL, E, CW, 3>);
+    else if (form == 4) run(k_inv_x_ld<T, LL, E, CW, 4>);
   });
   return err_;
 }
 
 template <int NZ, int FORM>
 static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr, cudaStream_t st, int nmem,
-                                long long msP) {
+                                long long msP, int zkeep) {
   constexpr int M = NZ / 2;
+  if (zkeep < 0) zkeep = M;
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   const long long nlines = (long long)g.Nx * g.Ny;
   cudaError_t err;
@@ -177,7 +182,8 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
       const long long ngroups = nlines / LPB;
       auto k = k_z_tma<T, NZ, FORM>;
       if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
-      k<<<dim3((unsigned)(ngroups < 148 ? ngroups : 148), nmem), 256, sm, st>>>((V*)P, g, (const V*)tw, zerr, msP);
+      k<<<dim3((unsigned)(ngroups < 148 ? ngroups : 148), nmem), 256, sm, st>>>((V*)P, g, (const V*)tw, zerr, msP,
+                                                                                 zkeep);
       ++g_launches;
       return cudaGetLastError();
     }
@@ -187,10 +193,10 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
     // up to two warps per line)
     constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / ((M % 3 == 0) ? 12 : 8));
     if constexpr (FORM == 3)
-      k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw);
+      k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw, zkeep);
     else
       k_z_reg<T, NZ, FORM><<<dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), NT, 0, st>>>((V*)P, g, (const V*)tw,
-                                                                                           msP);
+                                                                                           msP, zkeep);
     ++g_launches;
     return cudaGetLastError();
   }
@@ -203,21 +209,21 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   const size_t sm = (size_t)NSL * nl * zslot<M>() * sizeof(V);
   auto k = k_z_fused<T, NZ, E, FORM>;
   if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
-  k<<<dim3((unsigned)((nlines + nl - 1) / nl), nmem), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl, msP);
+  k<<<dim3((unsigned)((nlines + nl - 1) / nl), nmem), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl, msP, zkeep);
   ++g_launches;
   return cudaGetLastError();
 }
 
 template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, const void* tw, int* zerr,
-                                           cudaStream_t st, int nmem, long long msP) {
+                                           cudaStream_t st, int nmem, long long msP, int zkeep) {
   cudaError_t err = cudaErrorInvalidValue;
   if (form == 3 && nmem != 1) return err;  // the adjoint z pass has no member batching
   dispatch_L_sff(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
-    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st, nmem, msP);
-    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP);
-    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP);
-    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0);
+    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st, nmem, msP, zkeep);
+    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP, zkeep);
+    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP, zkeep);
+    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0, zkeep);
   });
   return err;
 }

@@ -13,16 +13,20 @@ template <typename T> struct Launch {
   // strided-axis FFT on nf fields in place: axis 0 = x (L = Nx), 1 = y (L = Ny);
   // dir -1 forward, +1 inverse; outputs scaled by `scale`
   // per > 0: the nf fields are nf / per members of per fields each, members mstride complex apart
+  // inner_eff > 0: transform only the first inner_eff columns (y axis: kz < inner_eff);
+  // zero_hi: rows with 3|k| > L are zero and not read (two-thirds dealiased input)
   static cudaError_t strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw, cudaStream_t st,
-                             int per = 0, long long mstride = 0);
+                             int per = 0, long long mstride = 0, int inner_eff = 0, int zero_hi = 0);
   // form 0 conservative (3 fields out), 1 rotational (6), 3 adjoint of the rotational form (9: also
   // lsc c^-1 P lam from the cotangent lam)
+  // kept != 0 (forms 0, 1 with two-thirds dealiasing): write only the columns with 3|ky| <= Ny, 3 kz <= Nz
   static cudaError_t inv_x(const Geo& g, int form, const void* U, void* W, const void* tw, const void* lam,
-                           double lsc, cudaStream_t st);
+                           double lsc, cudaStream_t st, int kept = 0);
   // form 0 conservative, 1 rotational, 2 Boussinesq (u, T), 3 adjoint of the rotational form
   // nmem members, member fields msP complex apart
+  // zkeep >= 0: input rows kz > zkeep are zero and not read
   static cudaError_t z_fused(const Geo& g, int form, void* P, const void* tw, int* err, cudaStream_t st,
-                             int nmem = 1, long long msP = 0);
+                             int nmem = 1, long long msP = 0, int zkeep = -1);
   static cudaError_t z_single(const Geo& g, int dir, const void* in, void* out, int ncomp, const void* tw, cudaStream_t st);
   // a.U0 / a.Ud / a.tot must be 16-byte aligned (TMA)
   // form 0 / 1 / 3 as inv_x; mode MODE_STEP, MODE_FLUX, MODE_NLIN (forms 0, 1) or MODE_ADJ (form 3)
