@@ -442,6 +442,8 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 // would spill and uses the other z kernels).  On B200 at 256^3 the 64-thread
 // blocks streamed 2.88 TB/s against 2.71 for 128-thread blocks.
 template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 64; }
+// lines over two warps (Nz = 1024) run two per 128-thread block (measured faster than one per block)
+template <int FORM, int M> __host__ __device__ constexpr int zreg_block() { return M / 8 > 32 ? 128 : zreg_threads<FORM>(); }
 
 // C2R of one line held by TPL lanes (input rows k = t + s*TPL): the pair terms
 // X[M-k] come from the partner lane by a warp shuffle (TPL <= 32) or straight
@@ -554,7 +556,8 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
 template <int NZ> __host__ __device__ constexpr int zreg_min_blocks() { return (NZ / 2) % 3 == 0 ? 3 : 6; }
 
 template <typename T, int NZ, int FORM>
-__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
+__global__ void __launch_bounds__(zreg_block<FORM, NZ / 2>(), zreg_min_blocks<NZ>() * zreg_threads<FORM>() /
+                                                                  zreg_block<FORM, NZ / 2>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
   // 8 elements per thread, 12 for a line length with a factor 3 (radices 4, 2|4, 3)
@@ -562,7 +565,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   static_assert(NIN <= 6, "the adjoint form runs in k_z_reg_adj");
-  constexpr int LPB = zreg_threads<FORM>() / TPL;
+  constexpr int LPB = zreg_block<FORM, M>() / TPL;
   __shared__ __align__(16) V xch_all[LPB * LDX];
   P += blockIdx.y * msP;  // member blockIdx.y
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
