@@ -442,8 +442,6 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 // would spill and uses the other z kernels).  On B200 at 256^3 the 64-thread
 // blocks streamed 2.88 TB/s against 2.71 for 128-thread blocks.
 template <int FORM> __host__ __device__ constexpr int zreg_threads() { return 64; }
-// lines over two warps (Nz = 1024) run two per 128-thread block (measured faster than one per block)
-template <int FORM, int M> __host__ __device__ constexpr int zreg_block() { return M / 8 > 32 ? 128 : zreg_threads<FORM>(); }
 
 // C2R of one line held by TPL lanes (input rows k = t + s*TPL): the pair terms
 // X[M-k] come from the partner lane by a warp shuffle (TPL <= 32) or straight
@@ -556,8 +554,7 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
 template <int NZ> __host__ __device__ constexpr int zreg_min_blocks() { return (NZ / 2) % 3 == 0 ? 3 : 6; }
 
 template <typename T, int NZ, int FORM>
-__global__ void __launch_bounds__(zreg_block<FORM, NZ / 2>(), zreg_min_blocks<NZ>() * zreg_threads<FORM>() /
-                                                                  zreg_block<FORM, NZ / 2>())
+__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
   // 8 elements per thread, 12 for a line length with a factor 3 (radices 4, 2|4, 3)
@@ -565,7 +562,7 @@ __global__ void __launch_bounds__(zreg_block<FORM, NZ / 2>(), zreg_min_blocks<NZ
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   static_assert(NIN <= 6, "the adjoint form runs in k_z_reg_adj");
-  constexpr int LPB = zreg_block<FORM, M>() / TPL;
+  constexpr int LPB = zreg_threads<FORM>() / TPL;
   __shared__ __align__(16) V xch_all[LPB * LDX];
   P += blockIdx.y * msP;  // member blockIdx.y
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
@@ -623,17 +620,18 @@ __global__ void __launch_bounds__(zreg_block<FORM, NZ / 2>(), zreg_min_blocks<NZ
 }
 
 // ---------------------------------------------------------------------------
-// z pass of the adjoint right-hand side, register-resident (FP32, M <= 512).
+// z pass of the adjoint right-hand side, register-resident (FP32 M <= 512, FP64 M <= 128).
 // Inputs per line: u (components 0-2), w (3-5), mu (6-8); outputs mu x u into
 // components 0-2 and w x mu into 3-5.  Staged so that at most six components
 // are live: mu and u are inverted, mu x u is transformed and stored over u,
 // then w is inverted into u's registers and w x mu is stored over w.
 // ---------------------------------------------------------------------------
 template <typename T, int NZ>
-__global__ void __launch_bounds__(zreg_threads<3>(), 6)
+__global__ void __launch_bounds__(zreg_threads<3>(), sizeof(T) == 8 ? 3 : 6)
     k_z_reg_adj(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int zkeep) {
   typedef C<T> V;
-  constexpr int M = NZ / 2, H = M + 1, E = 8, TPL = M / E, LDX = zslot<M>();
+  // 8 elements per thread in FP32, 4 in FP64 (six components live at once)
+  constexpr int M = NZ / 2, H = M + 1, E = sizeof(T) == 8 ? 4 : 8, TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int LPB = zreg_threads<3>() / TPL;
   __shared__ __align__(16) V xch_all[LPB * LDX];

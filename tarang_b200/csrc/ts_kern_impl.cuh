@@ -188,11 +188,17 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
       return cudaGetLastError();
     }
   }
+  if constexpr (FORM == 3 && !std::is_same<T, float>::value && M % 3 != 0 && M / 4 <= 32) {
+    // FP64 adjoint: register-resident with 4 elements per thread
+    constexpr int NT = zreg_threads<3>(), LPB = NT / (M / 4);
+    k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw, zkeep);
+    ++g_launches;
+    return cudaGetLastError();
+  }
   if constexpr (M <= 512 && (M % 3 != 0 || FORM != 3) && std::is_same<T, float>::value) {
     // FP32: register-resident variant, lines of M/E lanes (E = 8, or 12 with a factor 3;
     // up to two warps per line)
-    constexpr int NT = FORM == 3 ? zreg_threads<FORM>() : zreg_block<FORM, M>();
-    constexpr int LPB = NT / (M / ((M % 3 == 0) ? 12 : 8));
+    constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / ((M % 3 == 0) ? 12 : 8));
     if constexpr (FORM == 3)
       k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw, zkeep);
     else
