@@ -5,6 +5,10 @@
 //   FFF_PENCIL / SFF_PENCIL         basis/FFF/pencil/FFF_pencil.h:51, basis/SFF/pencil/SFF_pencil.h:52
 //   Nlin_incompress::Compute_nlin   fluid/incompressible/nlin/Nlin.h:79
 //   Time_advance_incompress::RK4    fluid/incompressible/time_advance/Time_advance.h:69-187
+//   FluidSF                         fluid/fluid_base/FluidSF.h:42
+//   Correlation::Get_Nusselt_no     fluid/fluid_base/Correlation.cc:144
+//   EnergyTr::Compute_flux          fluid/incompressible/energytr/compute_flux.cc:51
+// Ensemble and Adjoint have no reference counterpart.
 // Differences from the reference, by design: fields live in device memory
 // (one contiguous block per vector field, the reference's (Nx,Ny,Nz/2+1)
 // layout per component), errors throw ts_error instead of exit(1), and the
@@ -142,9 +146,111 @@ struct Nlin_incompress {
   static void Compute_nlin(FluidVF& U) { check(ts_nlin(U.basis().plan(), U.cvf(), U.nlin()), "Compute_nlin"); }
 };
 
+// Scalar field (the RBC temperature): csf F, one device component.
+class FluidSF {
+ public:
+  explicit FluidSF(Universal& basis) : basis_(basis) {
+    bytes_ = basis.elems_per_component() * basis.bytes_per_complex();
+    if (cudaMalloc(&csf_, bytes_) != cudaSuccess) throw ts_error(TS_ERR_NOMEM, "FluidSF");
+    cudaMemset(csf_, 0, bytes_);
+  }
+  ~FluidSF() { cudaFree(csf_); }
+  FluidSF(const FluidSF&) = delete;
+  FluidSF& operator=(const FluidSF&) = delete;
+
+  void* csf() { return csf_; }
+  size_t bytes() const { return bytes_; }
+  Universal& basis() { return basis_; }
+  // amplitude amp, uniform random phases on the modes with |K|/kfactor <= kmax
+  void Init_cond_perturbation(double amp, double kmax, uint64_t seed) {
+    check(ts_init_temperature_perturbation(basis_.plan(), amp, kmax, seed, csf_), "Init_cond_perturbation");
+  }
+  double Compute_total_energy() { return basis_.Get_total_energy(csf_, 1); }
+  void Copy_to_host(void* host) { cudaMemcpy(host, csf_, bytes_, cudaMemcpyDeviceToHost); }
+
+ private:
+  Universal& basis_;
+  void* csf_ = nullptr;
+  size_t bytes_ = 0;
+};
+
 struct Time_advance_incompress {
   // RK4(U,P,F) + strong reality condition when the plan enables it (RK.cc:91-170, Time_advance.cc:59-60)
   static void RK4(FluidVF& U, int nsteps = 1) { check(ts_rk4_step(U.basis().plan(), U.cvf(), nsteps), "RK4"); }
+  // RK4(U,T,P,F) for RBC on the SFF basis (RK_SF.cc:97), PRLARGE / ULARGE
+  static void RK4(FluidVF& U, FluidSF& T, int nsteps = 1) {
+    check(ts_rk4_step_rbc(U.basis().plan(), U.cvf(), T.csf(), nsteps), "RK4");
+  }
+};
+
+struct Correlation {
+  // Get_Nusselt_no (Correlation.cc:144-158, PRLARGE / ULARGE): 1 + 2 sqrt(Ra Pr) <U1, T>
+  static double Get_Nusselt_no(FluidVF& U, FluidSF& T) {
+    double nu = 0;
+    check(ts_nusselt(U.basis().plan(), U.cvf(), T.csf(), &nu), "Get_Nusselt_no");
+    return nu;
+  }
+};
+
+struct EnergyTr {
+  // Compute_flux(U) (compute_flux.cc:51): Pi(R_i) for every sphere radius
+  static std::vector<double> Compute_flux(FluidVF& U, const std::vector<double>& radii) {
+    std::vector<double> Pi(radii.size());
+    check(ts_flux(U.basis().plan(), U.cvf(), radii.data(), (int)radii.size(), Pi.data()), "Compute_flux");
+    return Pi;
+  }
+};
+
+// Many RBC runs of uneven sizes advanced together (no reference counterpart:
+// the reference runs one field per MPI job).
+class Ensemble {
+ public:
+  Ensemble(const ts_config& base, const std::vector<ts_member>& members) {
+    check(ts_ensemble_create(&base, members.data(), (int)members.size(), &ens_), "ts_ensemble_create");
+    n_ = members.size();
+  }
+  ~Ensemble() {
+    if (ens_) ts_ensemble_destroy(ens_);
+  }
+  Ensemble(const Ensemble&) = delete;
+  Ensemble& operator=(const Ensemble&) = delete;
+  void Init_temperature(double amp, double kmax, uint64_t seed) {
+    check(ts_ensemble_init_temperature(ens_, amp, kmax, seed), "Init_temperature");
+  }
+  void Run(int nsteps) { check(ts_ensemble_run(ens_, nsteps), "ts_ensemble_run"); }
+  std::vector<double> Nusselt() {
+    std::vector<double> nu(n_);
+    check(ts_ensemble_nusselt(ens_, nu.data()), "ts_ensemble_nusselt");
+    return nu;
+  }
+
+ private:
+  ts_ensemble* ens_ = nullptr;
+  size_t n_ = 0;
+};
+
+// Discrete adjoint of the FFF rotational IF-RK4 step (no reference counterpart).
+// Window(u_start, n, lam): lam enters as the cotangent of the state n steps after
+// u_start and leaves as the cotangent of u_start; the work buffer is owned here.
+class Adjoint {
+ public:
+  explicit Adjoint(Universal& basis, int window) : basis_(basis), window_(window) {
+    check(ts_adjoint_work_bytes(basis.plan(), window, &bytes_), "ts_adjoint_work_bytes");
+    if (cudaMalloc(&work_, bytes_) != cudaSuccess) throw ts_error(TS_ERR_NOMEM, "Adjoint");
+  }
+  ~Adjoint() { cudaFree(work_); }
+  Adjoint(const Adjoint&) = delete;
+  Adjoint& operator=(const Adjoint&) = delete;
+  void Window(const void* u_start, int nsteps, void* lam) {
+    if (nsteps > window_) throw ts_error(TS_ERR_ARG, "Adjoint::Window: nsteps above the window");
+    check(ts_adjoint_window(basis_.plan(), u_start, nsteps, lam, work_, bytes_), "ts_adjoint_window");
+  }
+
+ private:
+  Universal& basis_;
+  int window_;
+  size_t bytes_ = 0;
+  void* work_ = nullptr;
 };
 
 }  // namespace tarang_b200

@@ -1,39 +1,145 @@
 // Drives the C++ host mirror (include/tarang_b200.hpp) the way the reference's
-// Ifluid_main loop drives its classes: basis, FluidVF, IC, RK4 steps, energy,
-// divergence and E(k).  Prints one JSON line; tests/test_cpp_host.py compares it
-// with the same run through the Python binding.
-#include <cstdio>
-#include <vector>
+// main loops drive their classes: basis, fields, IC, RK4 steps, diagnostics.
+// Usage: host_mirror <mode> [N] [steps], mode one of
+//   fff       FFF_PENCIL + FluidVF: energy, divergence, E(k), Pi(R)
+//   rbc       SFF_PENCIL + FluidVF + FluidSF: energies and Nusselt number
+//   ensemble  two RBC members of different sizes advanced together: Nusselt numbers
+//   adjoint   FFF rotational FP64: cotangent of the start state of an nsteps window
+// Prints one JSON line; tests/test_cpp_host.py compares it with the same run
+// through the Python binding.
 #include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
 
 #include "tarang_b200.hpp"
 
-int main(int argc, char** argv) {
-  using namespace tarang_b200;
-  const int N = argc > 1 ? atoi(argv[1]) : 32;
-  const int steps = argc > 2 ? atoi(argv[2]) : 5;
+using namespace tarang_b200;
+
+static void print_list(const char* key, const std::vector<double>& v, bool last) {
+  printf("\"%s\": [", key);
+  for (size_t i = 0; i < v.size(); ++i) printf("%s%.17g", i ? ", " : "", v[i]);
+  printf("]%s", last ? "" : ", ");
+}
+
+static std::vector<double> k4_gauss(int nsh, double k0) {
+  std::vector<double> E(nsh);
+  for (int s = 1; s < nsh; ++s) E[s] = std::pow((double)s, 4) * std::exp(-2.0 * std::pow(s / k0, 2));
+  return E;
+}
+
+static int run_fff(int N, int steps) {
   ts_config c;
   ts_config_default(&c);
   c.N[0] = c.N[1] = c.N[2] = N;
   c.nu = 0.01;
   c.dt = 1e-3;
+  FFF_PENCIL basis(c);
+  FluidVF U(basis);
+  U.Init_cond_energy_spectrum(k4_gauss(basis.no_shells(), 4.0), 0, 0.5);
+  const double e0 = U.Compute_total_energy();
+  Time_advance_incompress::RK4(U, steps);
+  const double e1 = U.Compute_total_energy();
+  const double div = U.Compute_divergence_field();
+  std::vector<double> Ek = basis.Compute_shell_spectrum(U.cvf(), 3);
+  std::vector<double> Pi = EnergyTr::Compute_flux(U, {2.0, 4.0, 8.0});
+  printf("{\"e0\": %.17g, \"e1\": %.17g, \"div\": %.17g, ", e0, e1, div);
+  print_list("Ek", Ek, false);
+  print_list("Pi", Pi, true);
+  printf("}\n");
+  return 0;
+}
+
+static int run_rbc(int N, int steps) {
+  const double Ra = 1e5, Pr = 1.0;
+  ts_config c;
+  ts_config_default(&c);
+  c.N[0] = c.N[1] = c.N[2] = N;
+  c.kfactor[0] = M_PI;
+  c.kfactor[1] = c.kfactor[2] = 2 * M_PI;
+  c.precision = TS_F32;
+  c.Ra = Ra;
+  c.Pr = Pr;
+  c.nu = std::sqrt(Pr / Ra);
+  c.kappa = 1 / std::sqrt(Pr * Ra);
+  c.dt = 1e-3;
+  SFF_PENCIL basis(c);
+  FluidVF U(basis);
+  FluidSF T(basis);
+  T.Init_cond_perturbation(0.01, 4.0, 3);
+  Time_advance_incompress::RK4(U, T, steps);
+  const double eu = U.Compute_total_energy();
+  const double et = T.Compute_total_energy();
+  const double nu = Correlation::Get_Nusselt_no(U, T);
+  printf("{\"eu\": %.17g, \"eT\": %.17g, \"Nu\": %.17g}\n", eu, et, nu);
+  return 0;
+}
+
+static int run_ensemble(int N, int steps) {
+  ts_config c;
+  ts_config_default(&c);
+  c.basis = TS_BASIS_SFF;
+  c.kfactor[0] = M_PI;
+  c.kfactor[1] = c.kfactor[2] = 2 * M_PI;
+  c.precision = TS_F32;
+  c.dt = 1e-4;
+  c.force_type = TS_FORCE_RBC;
+  std::vector<ts_member> members(2);
+  const int sizes[2] = {N, N + N / 2};
+  const double ra[2] = {1e5, 1e6};
+  for (int m = 0; m < 2; ++m) {
+    for (int i = 0; i < 3; ++i) members[m].N[i] = sizes[m];
+    members[m].Ra = ra[m];
+    members[m].Pr = 1.0;
+  }
+  Ensemble ens(c, members);
+  ens.Init_temperature(0.01, 4.0, 7);
+  ens.Run(steps);
+  printf("{");
+  print_list("Nu", ens.Nusselt(), true);
+  printf("}\n");
+  return 0;
+}
+
+static int run_adjoint(int N, int steps) {
+  ts_config c;
+  ts_config_default(&c);
+  c.N[0] = c.N[1] = c.N[2] = N;
+  c.nlin_form = TS_NLIN_ROTATIONAL;
+  c.dealias_mode = TS_DEALIAS_TWO_THIRDS;
+  c.nu = 0.01;
+  c.dt = 1e-3;
+  FFF_PENCIL basis(c);
+  FluidVF U(basis);
+  FluidVF Lam(basis);
+  U.Init_cond_energy_spectrum(k4_gauss(basis.no_shells(), 4.0), 0, 0.5);
+  // cotangent of the final state: the state itself (the gradient of an energy-like loss)
+  if (cudaMemcpy(Lam.cvf(), U.cvf(), U.bytes(), cudaMemcpyDeviceToDevice) != cudaSuccess)
+    throw ts_error(TS_ERR_CUDA, "cudaMemcpy");
+  Adjoint adj(basis, steps);
+  adj.Window(U.cvf(), steps, Lam.cvf());
+  check(ts_plan_status(basis.plan()), "ts_plan_status");
+  const double el = basis.Get_total_energy(Lam.cvf(), 3);
+  std::vector<double> Ek = basis.Compute_shell_spectrum(Lam.cvf(), 3);
+  printf("{\"elam\": %.17g, ", el);
+  print_list("Ek", Ek, true);
+  printf("}\n");
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  const char* mode = argc > 1 ? argv[1] : "fff";
+  const int N = argc > 2 ? atoi(argv[2]) : 32;
+  const int steps = argc > 3 ? atoi(argv[3]) : 5;
   try {
-    FFF_PENCIL basis(c);
-    FluidVF U(basis);
-    std::vector<double> Eic(basis.no_shells());
-    for (size_t s = 1; s < Eic.size(); ++s) Eic[s] = std::pow((double)s, 4) * std::exp(-2.0 * std::pow(s / 4.0, 2));
-    U.Init_cond_energy_spectrum(Eic, 0, 0.5);
-    const double e0 = U.Compute_total_energy();
-    Time_advance_incompress::RK4(U, steps);
-    const double e1 = U.Compute_total_energy();
-    const double div = U.Compute_divergence_field();
-    std::vector<double> Ek = basis.Compute_shell_spectrum(U.cvf(), 3);
-    printf("{\"e0\": %.17g, \"e1\": %.17g, \"div\": %.17g, \"Ek\": [", e0, e1, div);
-    for (size_t i = 0; i < Ek.size(); ++i) printf("%s%.17g", i ? ", " : "", Ek[i]);
-    printf("]}\n");
+    if (!strcmp(mode, "fff")) return run_fff(N, steps);
+    if (!strcmp(mode, "rbc")) return run_rbc(N, steps);
+    if (!strcmp(mode, "ensemble")) return run_ensemble(N, steps);
+    if (!strcmp(mode, "adjoint")) return run_adjoint(N, steps);
+    fprintf(stderr, "unknown mode %s\n", mode);
+    return 2;
   } catch (const ts_error& e) {
     fprintf(stderr, "%s\n", e.what());
     return 1;
   }
-  return 0;
 }

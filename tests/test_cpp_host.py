@@ -1,6 +1,7 @@
 """The C++ host mirror (include/tarang_b200.hpp) compiles against the C ABI (CPU) and, on a GPU,
 gives the same numbers as the Python binding of the same library."""
 import json
+import math
 import os
 import shutil
 import subprocess
@@ -38,7 +39,7 @@ def test_host_mirror_matches_python_binding(cuda, tmp_path):
     import torch
     import tarang_b200 as tb
     exe = build_driver(tmp_path)
-    r = subprocess.run([str(exe), "32", "5"], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([str(exe), "fff", "32", "5"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     out = json.loads(r.stdout)
     plan = tb.Plan(32, nu=0.01, dt=1e-3)
@@ -51,3 +52,57 @@ def test_host_mirror_matches_python_binding(cuda, tmp_path):
     assert abs(out["e1"] - plan.energy(u)) < 1e-14
     assert np.max(np.abs(np.array(out["Ek"]) - plan.shell_spectrum(u))) < 1e-13
     assert out["div"] < 1e-12
+    assert np.max(np.abs(np.array(out["Pi"]) - plan.flux(u, [2.0, 4.0, 8.0]))) < 1e-14
+
+
+def run_driver(exe, *args):
+    r = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return json.loads(r.stdout)
+
+
+@pytest.mark.gpu
+def test_host_mirror_rbc_matches_python_binding(cuda, tmp_path):
+    import torch
+    import tarang_b200 as tb
+    out = run_driver(build_driver(tmp_path), "rbc", 32, 5)
+    Ra, Pr = 1e5, 1.0
+    plan = tb.Plan(32, basis="SFF", precision="f32", kfactor=(math.pi, 2 * math.pi, 2 * math.pi),
+                   nu=math.sqrt(Pr / Ra), kappa=1 / math.sqrt(Pr * Ra), dt=1e-3, Ra=Ra, Pr=Pr)
+    u, T = plan.field(3), plan.field(1)
+    plan.init_temperature_perturbation(0.01, 4.0, 3, T)
+    plan.rk4_step_rbc(u, T, 5)
+    torch.cuda.synchronize()
+    # same library, same launches: bitwise equal
+    assert out["eu"] == plan.energy(u)
+    assert out["eT"] == plan.energy(T)
+    assert out["Nu"] == plan.nusselt(u, T)
+    assert out["eu"] > 0 and out["Nu"] != 1.0
+
+
+@pytest.mark.gpu
+def test_host_mirror_ensemble_matches_python_binding(cuda, tmp_path):
+    import tarang_b200 as tb
+    out = run_driver(build_driver(tmp_path), "ensemble", 32, 4)
+    ens = tb.Ensemble([(32, 1e5, 1.0), (48, 1e6, 1.0)], dt=1e-4, precision="f32")
+    ens.init_temperature(0.01, 4.0, 7)
+    ens.run(4)
+    assert out["Nu"] == list(ens.nusselt())
+
+
+@pytest.mark.gpu
+def test_host_mirror_adjoint_matches_python_binding(cuda, tmp_path):
+    import torch
+    import tarang_b200 as tb
+    out = run_driver(build_driver(tmp_path), "adjoint", 32, 3)
+    plan = tb.Plan(32, nlin_form="rotational", dealias="two_thirds", nu=0.01, dt=1e-3)
+    u = plan.field(3)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 0, 0.5, u)
+    lam = u.clone()
+    work = torch.empty(plan.adjoint_work_bytes(3), dtype=torch.uint8, device=cuda)
+    plan.adjoint_window(u, 3, lam, work)
+    plan.status()
+    # the two drivers build the initial spectrum with different pow/exp (last-bit differences)
+    assert abs(out["elam"] - plan.energy(lam)) < 1e-13 * out["elam"]
+    assert np.max(np.abs(np.array(out["Ek"]) - plan.shell_spectrum(lam))) < 1e-13 * out["elam"]
+    assert out["elam"] > 0
