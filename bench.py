@@ -47,9 +47,23 @@ def parse():
     ap.add_argument("--workload", default="fff256", choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint"],
                     help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying "
                          "1024^3 (or --shape); rbc: one RBC run (SFF, --N, FP32); adjoint: adjoint/forward cost at 128^3")
+    ap.add_argument("--tune", default="auto", choices=["auto", "off"],
+                    help="auto: pick kernel candidates with the library's autotuner before warm-up "
+                         "(untimed set-up); off: the fixed tile rules")
     ap.add_argument("--shape", default="1024,1024,1024",
                     help="grid of the fff1024 workload, Nx,Ny,Nz (smaller shapes exercise the same kernels)")
     return ap.parse_args()
+
+
+TUNE = {"mode": "auto"}
+
+
+def tune_plan(plan, reps: int = 3) -> dict | None:
+    """Run the library autotuner on a plan (set-up, outside every timed region); returns the picks."""
+    if TUNE["mode"] == "off":
+        return None
+    rep = plan.autotune(reps=reps)
+    return {"tuning": rep["tuning"], "rule_ms_per_step": rep["start_ms"], "tuned_ms_per_step": rep["end_ms"]}
 
 
 def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
@@ -61,6 +75,14 @@ def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
     members = [allm[i] for i in tb.shard_members(allm, rank, world)]
     ens = tb.Ensemble(members, dt=1e-4, precision="f32", dealias="reference")
     ens.init_temperature(1e-3, 4.0, 3)
+    tuned = None
+    if TUNE["mode"] == "auto":
+        rep = ens.autotune(reps=3)
+        tuned = [{"N": gr["N"], "members": gr["members"], "rule_ms": gr["tuning"]["start_ms"],
+                  "tuned_ms": gr["tuning"]["end_ms"],
+                  "variant": [gr["tuning"][c]["variant"] for c in ("x_inv", "y_inv", "z", "y_fwd", "x_fwd")],
+                  "blocks_per_sm": [gr["tuning"][c]["blocks_per_sm"] for c in ("x_inv", "y_inv", "z", "y_fwd", "x_fwd")]}
+                 for gr in rep["groups"]]
     ens.run(warmup)
     ens.synchronize()
     t0 = time.perf_counter()
@@ -76,7 +98,7 @@ def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
     ens.close()
     model = sum(408.0 * m[0] ** 3 * 4 for m in members)   # SFF RBC byte model per member step, FP32
     return {"members": len(members), "seconds": wall, "steps": steps, "model_bytes_per_step": model,
-            "nusselt_mean": float(np.mean(Nu)), "nusselt_finite": bool(np.all(np.isfinite(Nu)))}
+            "nusselt_mean": float(np.mean(Nu)), "nusselt_finite": bool(np.all(np.isfinite(Nu))), "tuning": tuned}
 
 
 def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024)):
@@ -90,6 +112,7 @@ def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024)):
     plan.set_stream(torch.cuda.current_stream())   # the timing events below go on this stream
     u = plan.field(3)
     plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 8.0), 0, 0.5, u)
+    tuned = tune_plan(plan, reps=1)
     plan.rk4_step(u, warmup)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -113,7 +136,7 @@ def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024)):
             kern[name] = round(b.value / (tot.value / n.value / 1e3) / 1e9, 1)
     n3 = float(shape[0]) * shape[1] * shape[2]
     out = {"steps_per_s": steps / (ms / 1e3), "kernel_GBps": kern, "energy": plan.energy(u),
-           "model_frac": 288.0 * n3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
+           "model_frac": 288.0 * n3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0], "tuning": tuned}
     plan.close()
     return out
 
@@ -130,6 +153,7 @@ def rbc_leg(N: int, steps: int, warmup: int):
     plan.set_stream(torch.cuda.current_stream())
     u, T = plan.field(3), plan.field(1)
     plan.init_temperature_perturbation(1e-3, 4.0, 3, T)
+    tuned = tune_plan(plan)
     plan.rk4_step_rbc(u, T, warmup)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -153,7 +177,7 @@ def rbc_leg(N: int, steps: int, warmup: int):
     nu = plan.nusselt(u, T)
     plan.close()
     return {"steps_per_s": steps / (ms / 1e3), "kernels": kern, "nusselt": nu,
-            "model_frac": 408.0 * N ** 3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
+            "model_frac": 408.0 * N ** 3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0], "tuning": tuned}
 
 
 def adjoint_leg(prec: str, N: int = 128, window: int = 20, reps: int = 3):
@@ -362,6 +386,7 @@ def alt_workload(args, world, rank, local, dev):
                              "unit": "GB/s", "frac": mb * value / 1e9 / world / measured_peak()[0],
                              "traffic": None, "model": "408 N^3 4 B per member step"},
                 "member_steps_per_s": 64 * value}
+        line["config"]["tuning"] = r["tuning"]
     elif args.workload == "rbc":
         r = rbc_leg(args.N if args.N != 256 else 128, steps=args.steps, warmup=args.warmup)
         n = args.N if args.N != 256 else 128
@@ -372,6 +397,7 @@ def alt_workload(args, world, rank, local, dev):
                 "config": {"workload": f"RBC {n}^3, Ra=1e6, Pr=1, kfactor (pi,2pi,2pi), dt=1e-4, T amp 1e-3 k<=4"},
                 "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "kernels": r["kernels"]},
                 "nusselt": r["nusselt"]}
+        line["config"]["tuning"] = r["tuning"]
     elif args.workload == "adjoint":
         r = {"f64": adjoint_leg("f64"), "f32": adjoint_leg("f32")}
         line = {"metric": "adjoint step / forward step cost, FFF 128^3 rotational (config 4)",
@@ -389,6 +415,7 @@ def alt_workload(args, world, rank, local, dev):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"FFF {sh} decaying, IC k^4 exp(-2(k/8)^2) E=0.5 seed 0, nu=2e-4, dt=2e-4"},
                 "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "kernel_GBps": r["kernel_GBps"]}}
+        line["config"]["tuning"] = r["tuning"]
     line["clocks"] = clk.stop()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -399,6 +426,7 @@ def alt_workload(args, world, rank, local, dev):
 
 def main():
     args = parse()
+    TUNE["mode"] = args.tune
     if args.impl == "reference":
         return run_reference(args)
 
@@ -431,6 +459,7 @@ def main():
     E_ic = tb.spectrum_k4_gauss(plan.n_shells, 4.0)
     plan.init_energy_spectrum(E_ic, 0, 0.5, u)
     u0 = u.clone()
+    tuned = tune_plan(plan)
 
     for _ in range(args.warmup):
         plan.rk4_step(u, 1)
@@ -522,6 +551,7 @@ def main():
             p64 = tb.Plan(N, precision="f64", nlin_form=args.form, dealias="two_thirds", nu=1e-3, dt=5e-4,
                           forcing=forcing)
             p64.set_stream(stream)
+            extras["fp64_tuning"] = tune_plan(p64)
             a32 = u0.clone()
             a64 = u0.to(torch.complex128)
             for _ in range(5):
@@ -577,7 +607,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": args.precision, "data": "synthetic",
                 "config": dict(workload(N), precision=args.precision, nlin_form=args.form,
-                               parallelism=f"replicas x{world}",
+                               parallelism=f"replicas x{world}", tuning=tuned,
                                l2="working set (12 spectral fields, %.2f GB) > L2 126 MB: inputs larger than L2"
                                   % (12 * plan.N[0] * plan.N[1] * (plan.N[2] // 2 + 1) * (8 if args.precision == "f32" else 16) / 1e9)),
                 "roofline": roofline, "step_roofline": step_model, "cpu_baseline": cpu, "e2e": e2e,

@@ -197,6 +197,48 @@ int ts_adjoint_step(ts_plan* plan, const void* u_hat, const void* stages, void* 
 int ts_adjoint_work_bytes(const ts_plan* plan, int nsteps, size_t* bytes);
 int ts_adjoint_window(ts_plan* plan, const void* u_start, int nsteps, void* lam_hat, void* work, size_t work_bytes);
 
+/* Launch tuning (no reference counterpart: the reference leaves the FFT plan
+ * to FFTW's planner).  Each right-hand side runs five pass classes; for each
+ * the library holds a fixed rule (candidate 0) and up to three other kernel
+ * candidates that change the radix schedule (elements per thread, so the
+ * Stockham passes' radices), the column-tile width, the staging depth, or the
+ * kernel form (z: shared-memory slot kernels; FFF forward x: split x FFF +
+ * elementwise epilogue; SFF forward x: the other fused/split choice), plus a
+ * blocks-per-SM count for the persistent launches (y passes, fused FFF
+ * forward x; 0 = the rule).  Every candidate computes the same transform;
+ * results differ from the rule's in rounding only.
+ * ts_tuning_candidates: bit v of *mask set when candidate v of class cls exists
+ *   for this plan; *blocks != 0 when the class takes a blocks-per-SM count.
+ * ts_plan_set_tuning: TS_ERR_ARG if a candidate does not exist for the plan.
+ * ts_plan_autotune: coordinate descent, class by class: times whole IF-RK4 steps
+ *   of a scratch state on the plan's stream with CUDA events (best of `reps`
+ *   trials, enough steps per trial for about 3 ms), keeps a candidate only when
+ *   it is at least 1 % faster.  The caller's fields are not touched; the plan's
+ *   work buffers are.  report (may be NULL): a JSON summary of every timing.
+ * ts_ensemble_autotune: the same for every size group of an ensemble, timing
+ *   whole ensemble steps (one graph launch each); the members' states are saved
+ *   and restored. */
+typedef enum {
+  TS_TUNE_X_INV = 0,
+  TS_TUNE_Y_INV = 1,
+  TS_TUNE_Z = 2,
+  TS_TUNE_Y_FWD = 3,
+  TS_TUNE_X_FWD = 4,
+  TS_TUNE_NCLASS = 5
+} ts_tune_class;
+typedef struct {
+  int variant[TS_TUNE_NCLASS];
+  int blocks_per_sm[TS_TUNE_NCLASS];
+} ts_tuning;
+int ts_tuning_candidates(const ts_plan* plan, int cls, int* mask, int* blocks);
+int ts_plan_get_tuning(const ts_plan* plan, ts_tuning* tuning);
+int ts_plan_set_tuning(ts_plan* plan, const ts_tuning* tuning);
+int ts_plan_autotune(ts_plan* plan, int reps, char* report, size_t report_len);
+/* the tuning of the size group holding member m (its plan's tuning) */
+int ts_ensemble_get_tuning(ts_ensemble* ens, int member, ts_tuning* tuning);
+int ts_ensemble_set_tuning(ts_ensemble* ens, int member, const ts_tuning* tuning);
+int ts_ensemble_autotune(ts_ensemble* ens, int reps, char* report, size_t report_len);
+
 /* Kernel classes of one right-hand-side evaluation, for ts_profile_read. */
 typedef enum {
   TS_KCLASS_INV_X = 0,  /* dealias + inverse FFT along x (+ vorticity) */

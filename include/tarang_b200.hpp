@@ -78,6 +78,20 @@ class Universal {
     check(ts_energy(plan_, A, ncomp, &e), "Get_total_energy");
     return e;
   }
+  // launch tuning: the fastest kernel candidate per pass class on this GPU
+  // (ts_plan_autotune); returns the JSON timing report
+  std::string Autotune(int reps = 3) {
+    std::string rep(1 << 16, '\0');
+    check(ts_plan_autotune(plan_, reps, &rep[0], rep.size()), "Autotune");
+    rep.resize(rep.find('\0'));
+    return rep;
+  }
+  ts_tuning Get_tuning() const {
+    ts_tuning t;
+    check(ts_plan_get_tuning(plan_, &t), "Get_tuning");
+    return t;
+  }
+  void Set_tuning(const ts_tuning& t) { check(ts_plan_set_tuning(plan_, &t), "Set_tuning"); }
 
  private:
   ts_config cfg_;
@@ -218,6 +232,12 @@ class Ensemble {
     check(ts_ensemble_init_temperature(ens_, amp, kmax, seed), "Init_temperature");
   }
   void Run(int nsteps) { check(ts_ensemble_run(ens_, nsteps), "ts_ensemble_run"); }
+  std::string Autotune(int reps = 3) {
+    std::string rep(1 << 18, '\0');
+    check(ts_ensemble_autotune(ens_, reps, &rep[0], rep.size()), "Ensemble::Autotune");
+    rep.resize(rep.find('\0'));
+    return rep;
+  }
   std::vector<double> Nusselt() {
     std::vector<double> nu(n_);
     check(ts_ensemble_nusselt(ens_, nu.data()), "ts_ensemble_nusselt");

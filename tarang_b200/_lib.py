@@ -26,6 +26,13 @@ class TsMember(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int * 3), ("Ra", ctypes.c_double), ("Pr", ctypes.c_double)]
 
 
+TUNE_CLASSES = ["x_inv", "y_inv", "z", "y_fwd", "x_fwd"]
+
+
+class TsTuning(ctypes.Structure):
+    _fields_ = [("variant", ctypes.c_int * 5), ("blocks_per_sm", ctypes.c_int * 5)]
+
+
 class TsConfig(ctypes.Structure):
     _fields_ = [
         ("basis", ctypes.c_int),
@@ -87,6 +94,14 @@ SIGNATURES = {
     "ts_adjoint_step": (ctypes.c_int, [_P, _P, _P, _P]),
     "ts_adjoint_work_bytes": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "ts_adjoint_window": (ctypes.c_int, [_P, _P, ctypes.c_int, _P, _P, ctypes.c_size_t]),
+    "ts_tuning_candidates": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
+    "ts_plan_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TsTuning)]),
+    "ts_plan_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TsTuning)]),
+    "ts_plan_autotune": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
+    "ts_ensemble_get_tuning": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(TsTuning)]),
+    "ts_ensemble_set_tuning": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(TsTuning)]),
+    "ts_ensemble_autotune": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
     "ts_profile_enable": (ctypes.c_int, [_P, ctypes.c_int]),
     "ts_profile_reset": (ctypes.c_int, [_P]),
     "ts_profile_read": (ctypes.c_int, [_P, ctypes.c_int, _D, ctypes.POINTER(ctypes.c_longlong), _D]),

@@ -1246,3 +1246,315 @@ int ts_ensemble_nusselt(ts_ensemble* e, double* Nu) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// launch tuning: coordinate descent over the five pass classes of a step
+// ---------------------------------------------------------------------------
+namespace {
+
+const char* const kTuneName[TUNE_NCLASS] = {"x_inv", "y_inv", "z", "y_fwd", "x_fwd"};
+
+int plan_form(const ts_plan* p) { return p->cfg.basis == TS_BASIS_SFF ? 2 : p->cfg.nlin_form; }
+
+bool tune_valid(const ts_plan* p, const Geo& g, int cls, int v) {
+  return p->prec == 1 ? Launch<float>::tune_valid(g, plan_form(p), cls, v)
+                      : Launch<double>::tune_valid(g, plan_form(p), cls, v);
+}
+bool tune_blocks(const ts_plan* p, const Geo& g, int cls) {
+  return p->prec == 1 ? Launch<float>::tune_blocks(g, plan_form(p), cls)
+                      : Launch<double>::tune_blocks(g, plan_form(p), cls);
+}
+
+// best over `reps` trials of the time of n calls of fn on stream st, per call
+template <typename Fn> int time_calls(cudaStream_t st, int n, int reps, Fn&& fn, double* ms) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  CK(cudaEventCreate(&a));
+  if (cudaEventCreate(&b) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return TS_ERR_CUDA;
+  }
+  int rc = fn();  // warm-up (first launches of a new kernel candidate)
+  double best = 1e300;
+  for (int r = 0; r < reps && rc == TS_OK; ++r) {
+    cudaEventRecord(a, st);
+    for (int i = 0; i < n && rc == TS_OK; ++i) rc = fn();
+    cudaEventRecord(b, st);
+    float t = 0;
+    if (rc == TS_OK && (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&t, a, b) != cudaSuccess))
+      rc = TS_ERR_CUDA;
+    if (rc == TS_OK && t / n < best) best = t / n;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return rc;
+}
+
+void json_num(std::string& js, double x) {
+  char buf[64];
+  snprintf(buf, sizeof(buf), "%.6g", x);
+  js += buf;
+}
+
+// Tunes g (the geometry a plan's or a group's launches read) class by class;
+// measure(&ms) times the objective with the current g.  Appends a JSON object.
+template <typename Measure> int descend(const ts_plan* p, Geo& g, Measure&& measure, std::string& js) {
+  double best = 0;
+  CKS(measure(&best));
+  js += "{\"start_ms\": ";
+  json_num(js, best);
+  for (int cls = 0; cls < TUNE_NCLASS; ++cls) {
+    js += ", \"";
+    js += kTuneName[cls];
+    js += "\": {\"tried\": [";
+    bool first = true;
+    auto log = [&](int v, int b, double t) {
+      char buf[96];
+      snprintf(buf, sizeof(buf), "%s[%d, %d, %.6g]", first ? "" : ", ", v, b, t);
+      js += buf;
+      first = false;
+    };
+    log(g.tv[cls], g.tb[cls], best);
+    const int v0 = g.tv[cls];
+    int bv = v0;
+    for (int v = 0; v < TUNE_NCAND; ++v) {
+      if (v == v0 || !tune_valid(p, g, cls, v)) continue;
+      g.tv[cls] = (signed char)v;
+      const signed char keep_b = g.tb[cls];
+      if (!tune_blocks(p, g, cls)) g.tb[cls] = 0;
+      double t = 0;
+      const int rc = measure(&t);
+      g.tb[cls] = keep_b;
+      if (rc != TS_OK) {
+        g.tv[cls] = (signed char)bv;
+        return rc;
+      }
+      log(v, tune_blocks(p, g, cls) ? g.tb[cls] : 0, t);
+      if (t < 0.99 * best) {
+        best = t;
+        bv = v;
+      }
+    }
+    g.tv[cls] = (signed char)bv;
+    if (!tune_blocks(p, g, cls)) {
+      g.tb[cls] = 0;
+    } else {
+      const int b0 = g.tb[cls];
+      int bb = b0;
+      for (int b = 0; b <= 4; ++b) {
+        if (b == b0) continue;
+        g.tb[cls] = (signed char)b;
+        double t = 0;
+        const int rc = measure(&t);
+        if (rc != TS_OK) {
+          g.tb[cls] = (signed char)bb;
+          return rc;
+        }
+        log(bv, b, t);
+        if (t < 0.99 * best) {
+          best = t;
+          bb = b;
+        }
+      }
+      g.tb[cls] = (signed char)bb;
+    }
+    char buf[96];
+    snprintf(buf, sizeof(buf), "], \"variant\": %d, \"blocks_per_sm\": %d}", g.tv[cls], g.tb[cls]);
+    js += buf;
+  }
+  js += ", \"end_ms\": ";
+  json_num(js, best);
+  js += "}";
+  return TS_OK;
+}
+
+void copy_report(const std::string& js, char* report, size_t len) {
+  if (!report || len == 0) return;
+  const size_t n = js.size() < len - 1 ? js.size() : len - 1;
+  memcpy(report, js.data(), n);
+  report[n] = 0;
+}
+
+void ens_invalidate(ts_ensemble* e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->exec = nullptr;
+  e->graph = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ts_tuning_candidates(const ts_plan* p, int cls, int* mask, int* blocks) {
+  if (!p || cls < 0 || cls >= TUNE_NCLASS || !mask) return TS_ERR_ARG;
+  int m = 0;
+  for (int v = 0; v < TUNE_NCAND; ++v)
+    if (tune_valid(p, p->g, cls, v)) m |= 1 << v;
+  *mask = m;
+  if (blocks) *blocks = tune_blocks(p, p->g, cls) ? 1 : 0;
+  return TS_OK;
+}
+
+int ts_plan_get_tuning(const ts_plan* p, ts_tuning* t) {
+  if (!p || !t) return TS_ERR_ARG;
+  for (int c = 0; c < TUNE_NCLASS; ++c) {
+    t->variant[c] = p->g.tv[c];
+    t->blocks_per_sm[c] = p->g.tb[c];
+  }
+  return TS_OK;
+}
+
+int ts_plan_set_tuning(ts_plan* p, const ts_tuning* t) {
+  if (!p || !t) return TS_ERR_ARG;
+  Geo g = p->g;
+  for (int c = 0; c < TUNE_NCLASS; ++c) {
+    g.tv[c] = (signed char)t->variant[c];
+    if (t->variant[c] < 0 || t->variant[c] >= TUNE_NCAND || !tune_valid(p, g, c, t->variant[c])) {
+      g_last_error = std::string("ts_plan_set_tuning: candidate ") + std::to_string(t->variant[c]) + " of class " +
+                     kTuneName[c] + " does not exist for this plan";
+      return TS_ERR_ARG;
+    }
+  }
+  for (int c = 0; c < TUNE_NCLASS; ++c) {
+    const int b = t->blocks_per_sm[c];
+    if (b < 0 || b > 8 || (b > 0 && !tune_blocks(p, g, c))) {
+      g_last_error = std::string("ts_plan_set_tuning: blocks_per_sm ") + std::to_string(b) + " not accepted for " +
+                     kTuneName[c];
+      return TS_ERR_ARG;
+    }
+    g.tb[c] = (signed char)b;
+  }
+  CK(cudaStreamSynchronize(p->st));  // launches already queued keep the old tuning
+  p->g = g;
+  return TS_OK;
+}
+
+int ts_plan_autotune(ts_plan* p, int reps, char* report, size_t report_len) {
+  if (!p || reps < 1) return TS_ERR_ARG;
+  const bool sff = p->cfg.basis == TS_BASIS_SFF;
+  const size_t bu = 3 * (size_t)p->g.S * p->cb, bt = (size_t)p->g.S * p->cb;
+  void *U = nullptr, *T = nullptr;
+  CK(cudaStreamSynchronize(p->st));
+  if (cudaMalloc(&U, bu) != cudaSuccess || cudaMalloc(&T, bt) != cudaSuccess) {
+    if (U) cudaFree(U);
+    cudaGetLastError();
+    return TS_ERR_NOMEM;
+  }
+  const bool prof = p->prof;
+  p->prof = false;
+  int rc = TS_OK;
+  auto fail = [&](int r) {
+    p->prof = prof;
+    cudaStreamSynchronize(p->st);
+    cudaFree(U);
+    cudaFree(T);
+    return r;
+  };
+  // scratch state: the benchmark's k^4 exp(-2 (k/4)^2) spectrum (FFF) or a
+  // temperature perturbation from rest (SFF)
+  if (sff) {
+    if (cudaMemsetAsync(U, 0, bu, p->st) != cudaSuccess) return fail(TS_ERR_CUDA);
+    if ((rc = ts_init_temperature_perturbation(p, 1e-3, 4.0, 3, T)) != TS_OK) return fail(rc);
+  } else {
+    std::vector<double> E(p->nshells > 1 ? p->nshells : 2, 0.0);
+    for (size_t k = 1; k < E.size(); ++k) E[k] = pow((double)k, 4) * exp(-2.0 * pow(k / 4.0, 2));
+    if ((rc = ts_init_energy_spectrum(p, E.data(), (int)E.size(), 1, 0.5, U)) != TS_OK) return fail(rc);
+  }
+  auto step = [&]() -> int { return sff ? step_rbc(p, U, T) : step_fff(p, U); };
+  double t1 = 0;
+  if ((rc = time_calls(p->st, 1, 1, step, &t1)) != TS_OK) return fail(rc);
+  int n = t1 > 0 ? (int)ceil(3.0 / t1) : 64;
+  n = n < 1 ? 1 : (n > 64 ? 64 : n);
+  auto measure = [&](double* ms) { return time_calls(p->st, n, reps, step, ms); };
+  std::string js;
+  rc = descend(p, p->g, measure, js);
+  if (rc == TS_OK) copy_report(js, report, report_len);
+  return fail(rc);
+}
+
+int ts_ensemble_get_tuning(ts_ensemble* e, int m, ts_tuning* t) {
+  if (!e || m < 0 || m >= (int)e->plans.size()) return TS_ERR_ARG;
+  for (const ens_group& G : e->groups)
+    for (int i : G.idx)
+      if (i == m) return ts_plan_get_tuning(G.gp, t);
+  return TS_ERR_ARG;
+}
+
+int ts_ensemble_set_tuning(ts_ensemble* e, int m, const ts_tuning* t) {
+  if (!e || m < 0 || m >= (int)e->plans.size()) return TS_ERR_ARG;
+  for (ens_group& G : e->groups)
+    for (int i : G.idx)
+      if (i == m) {
+        CK(cudaStreamSynchronize(e->origin));
+        CKS(ts_plan_set_tuning(G.gp, t));
+        ens_invalidate(e);
+        return TS_OK;
+      }
+  return TS_ERR_ARG;
+}
+
+int ts_ensemble_autotune(ts_ensemble* e, int reps, char* report, size_t report_len) {
+  if (!e || reps < 1) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(e->origin));
+  // save the members' states; tuning steps run on the group arrays
+  std::vector<void*> saved;
+  size_t total = 0;
+  for (const ens_group& G : e->groups) total += 4 * (size_t)G.idx.size() * G.gp->g.S * G.gp->cb;
+  void* save = nullptr;
+  if (cudaMalloc(&save, total) != cudaSuccess) {
+    cudaGetLastError();
+    return TS_ERR_NOMEM;
+  }
+  size_t off = 0;
+  for (const ens_group& G : e->groups) {
+    const size_t B = G.idx.size(), S = (size_t)G.gp->g.S, cb = G.gp->cb;
+    if (cudaMemcpy((char*)save + off, G.U, B * 3 * S * cb, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+        cudaMemcpy((char*)save + off + B * 3 * S * cb, G.T, B * S * cb, cudaMemcpyDeviceToDevice) != cudaSuccess) {
+      cudaFree(save);
+      return TS_ERR_CUDA;
+    }
+    off += 4 * B * S * cb;
+  }
+  auto restore = [&]() -> int {
+    cudaStreamSynchronize(e->origin);
+    size_t o = 0;
+    int r = TS_OK;
+    for (const ens_group& G : e->groups) {
+      const size_t B = G.idx.size(), S = (size_t)G.gp->g.S, cb = G.gp->cb;
+      if (cudaMemcpy(G.U, (char*)save + o, B * 3 * S * cb, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+          cudaMemcpy(G.T, (char*)save + o + B * 3 * S * cb, B * S * cb, cudaMemcpyDeviceToDevice) != cudaSuccess)
+        r = TS_ERR_CUDA;
+      o += 4 * B * S * cb;
+    }
+    cudaFree(save);
+    return r;
+  };
+  auto step = [&]() -> int { return ts_ensemble_run(e, 1); };
+  double t1 = 0;
+  int rc = time_calls(e->origin, 1, 1, step, &t1);
+  int n = t1 > 0 ? (int)ceil(5.0 / t1) : 16;
+  n = n < 1 ? 1 : (n > 16 ? 16 : n);
+  auto measure = [&](double* ms) {
+    ens_invalidate(e);  // the next run re-captures the graph with the current tuning
+    return time_calls(e->origin, n, reps, step, ms);
+  };
+  std::string js = "{\"groups\": [";
+  for (size_t k = 0; k < e->groups.size() && rc == TS_OK; ++k) {
+    ens_group& G = e->groups[k];
+    char buf[128];
+    snprintf(buf, sizeof(buf), "%s{\"N\": [%d, %d, %d], \"members\": %d, \"tuning\": ", k ? ", " : "", G.gp->g.Nx,
+             G.gp->g.Ny, G.gp->g.Nz, (int)G.idx.size());
+    js += buf;
+    rc = descend(G.gp, G.gp->g, measure, js);
+    js += "}";
+  }
+  js += "]}";
+  ens_invalidate(e);
+  const int rr = restore();
+  if (rc == TS_OK) rc = rr;
+  if (rc == TS_OK) copy_report(js, report, report_len);
+  return rc;
+}
+
+}  // extern "C"

@@ -17,12 +17,19 @@
 
 namespace ts {
 
+// pass classes of the launch tuning: inverse x, inverse y, z, forward y, forward x
+enum { TUNE_X_INV = 0, TUNE_Y_INV = 1, TUNE_Z = 2, TUNE_Y_FWD = 3, TUNE_X_FWD = 4, TUNE_NCLASS = 5, TUNE_NCAND = 4 };
+
 struct Geo {
   int Nx, Ny, Nz, Hz;
   long long S;          // complex elements per component
   double kf[3];         // kfactor (reference kfactor[1..3])
   int basis;            // 0 FFF, 1 SFF
   int dealias;          // 0 none, 1 reference corner, 2 two thirds
+  // launch tuning per pass class: kernel candidate (0 = the fixed rule) and
+  // blocks per SM of the persistent launches (0 = the rule)
+  signed char tv[TUNE_NCLASS] = {0, 0, 0, 0, 0};
+  signed char tb[TUNE_NCLASS] = {0, 0, 0, 0, 0};
 };
 
 // ---------------------------------------------------------------------------

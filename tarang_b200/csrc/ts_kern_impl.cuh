@@ -97,83 +97,193 @@ constexpr int str_e(int L) { return wide1024(L) ? 16 : e_mixed(L, e_reg(L)); }
 constexpr int str_cw(int L) { return wide1024(L) ? 8 : cw_for(L, str_e(L)); }
 constexpr int str_nt(int L) { return wide1024(L) ? 2 : 3; }
 
+// ---------------------------------------------------------------------------
+// Launch-tuning candidates.  Candidate 0 of every pass class is the fixed rule;
+// the others change the radix schedule (elements per thread E: the Stockham
+// passes use radix min(E, remaining)), the column-tile width CW or the number of
+// staging tiles NT.  A candidate that does not fit (threads per block, shared
+// memory) or repeats an earlier one is invalid and launches as the rule.
+// ---------------------------------------------------------------------------
+constexpr int NCAND = TUNE_NCAND;
+struct Tile { int E, CW, NT; };
+constexpr bool tile_eq(Tile a, Tile b) { return a.E == b.E && a.CW == b.CW && a.NT == b.NT; }
+constexpr bool tile_fits(int L, Tile c, int tiles) {
+  return c.E > 0 && c.CW > 0 && L % c.E == 0 && c.CW * (L / c.E) <= 1024 && c.CW * (L / c.E) >= 32 &&
+         (size_t)tiles * L * c.CW * sizeof(V) <= 227 * 1024;
+}
+
+// strided passes (y inverse / y forward)
+constexpr Tile str_cand(int L, int v) {
+  return v == 0 ? Tile{str_e(L), str_cw(L), str_nt(L)}
+       : v == 1 ? (L % 3 != 0 && str_e(L) > 4 ? Tile{str_e(L) / 2, str_cw(L), str_nt(L)} : Tile{0, 0, 0})
+       : v == 2 ? (str_cw(L) > 1 ? Tile{str_e(L), str_cw(L) / 2, str_nt(L)} : Tile{0, 0, 0})
+       : v == 3 ? Tile{str_e(L), str_cw(L), 5 - str_nt(L)}
+                : Tile{0, 0, 0};
+}
+constexpr bool str_valid(int L, int v) {
+  return v == 0 || (v < NCAND && tile_fits(L, str_cand(L, v), str_cand(L, v).NT) &&
+                    !tile_eq(str_cand(L, v), str_cand(L, 0)) && (v < 2 || !tile_eq(str_cand(L, v), str_cand(L, 1))) &&
+                    (v < 3 || !tile_eq(str_cand(L, v), str_cand(L, 2))));
+}
+
+template <int L, int VV, typename Fn> void with_str_tile(Fn&& fn) {
+  if constexpr (str_valid(L, VV)) fn(std::integral_constant<int, VV>{});
+  else fn(std::integral_constant<int, 0>{});
+}
+
 template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void* data, int nf, const void* tw,
                                            cudaStream_t st, int per, long long mstride, int inner_eff,
                                            int zero_hi) {
   if (per <= 0) per = nf;
   cudaError_t err = cudaErrorInvalidValue;
   const int L = axis == 0 ? g.Nx : g.Ny;
+  // the y passes follow the tuning of their class; x passes keep the rule
+  const int cls = axis == 1 ? (dir > 0 ? TUNE_Y_INV : TUNE_Y_FWD) : -1;
+  const int v = cls >= 0 ? g.tv[cls] : 0, bps = cls >= 0 ? g.tb[cls] : 0;
   dispatch_L_sff(L, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
-    constexpr int E = str_e(LL);
-    constexpr int CW = str_cw(LL);
-    constexpr int NT = str_nt(LL);
-    const int inner = inner_eff > 0 ? inner_eff : (axis == 0 ? g.Ny * g.Hz : g.Hz);
-    const long long rstride = axis == 0 ? (long long)g.Ny * g.Hz : g.Hz;
-    const long long ostride = axis == 0 ? 0 : (long long)g.Ny * g.Hz;
-    const int nouter = axis == 0 ? 1 : g.Nx;
-    const long long nwork = (long long)nf * ((inner + CW - 1) / CW) * nouter;
-    const size_t sm = (size_t)NT * LL * CW * sizeof(V);
-    // persistent grid: as many blocks as fit on the 148 SMs at once
-    const int per_sm = (int)((227 * 1024) / sm) < ((CW * (LL / E)) <= 256 ? 2 : 1)
-                           ? (int)((227 * 1024) / sm) : ((CW * (LL / E)) <= 256 ? 2 : 1);
-    long long blocks = 148LL * (per_sm > 0 ? per_sm : 1);
-    if (blocks > nwork) blocks = nwork;
-    if (dir < 0) {
-      auto k = k_strided_fft<T, LL, E, CW, -1, NT>;
-      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
-                                                    (const V*)tw, per, mstride, zero_hi);
-    } else {
-      auto k = k_strided_fft<T, LL, E, CW, 1, NT>;
-      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
-                                                    (const V*)tw, per, mstride, zero_hi);
+    auto run = [&](auto vc) {
+      constexpr Tile c = str_cand(LL, decltype(vc)::value);
+      constexpr int E = c.E, CW = c.CW, NT = c.NT;
+      const int inner = inner_eff > 0 ? inner_eff : (axis == 0 ? g.Ny * g.Hz : g.Hz);
+      const long long rstride = axis == 0 ? (long long)g.Ny * g.Hz : g.Hz;
+      const long long ostride = axis == 0 ? 0 : (long long)g.Ny * g.Hz;
+      const int nouter = axis == 0 ? 1 : g.Nx;
+      const long long nwork = (long long)nf * ((inner + CW - 1) / CW) * nouter;
+      const size_t sm = (size_t)NT * LL * CW * sizeof(V);
+      // persistent grid: as many blocks as fit on the 148 SMs at once (or the tuned count)
+      const int cap = (CW * (LL / E)) <= 256 ? 2 : 1;
+      const int fit = (int)((227 * 1024) / sm);
+      const int per_sm = bps > 0 ? bps : (fit < cap ? fit : cap);
+      long long blocks = 148LL * (per_sm > 0 ? per_sm : 1);
+      if (blocks > nwork) blocks = nwork;
+      auto launch = [&](auto k) {
+        if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+        k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
+                                                      (const V*)tw, per, mstride, zero_hi);
+        ++g_launches;
+        err = cudaGetLastError();
+      };
+      if (dir < 0) launch(k_strided_fft<T, LL, E, CW, -1, NT>);
+      else launch(k_strided_fft<T, LL, E, CW, 1, NT>);
+    };
+    switch (v) {
+      case 1: with_str_tile<LL, 1>(run); break;
+      case 2: with_str_tile<LL, 2>(run); break;
+      case 3: with_str_tile<LL, 3>(run); break;
+      default: run(std::integral_constant<int, 0>{});
     }
-    ++g_launches;
-    err = cudaGetLastError();
   });
   return err;
+}
+
+// inverse x pass (FFF forms 0, 1): 8 elements per thread in FP32 (U held in
+// registers across the output fields; 16 at L = 1024 with per-field loads)
+constexpr int ix_e(int L) { return wide1024(L) ? 16 : (std::is_same<T, float>::value ? (8 < L ? 8 : L) : e_reg(L)); }
+constexpr int ix_cw(int L) { return wide1024(L) ? 8 : cw_for(L, ix_e(L)); }
+constexpr int ix_e_alt(int L) {
+  return std::is_same<T, float>::value ? (ix_e(L) == 8 ? (16 <= L ? 16 : 0) : 8) : (ix_e(L) > 4 ? ix_e(L) / 2 : 0);
+}
+constexpr Tile ix_cand(int L, int v) {
+  return v == 0 ? Tile{ix_e(L), ix_cw(L), 1}
+       : v == 1 ? (ix_e_alt(L) > 0 ? Tile{ix_e_alt(L), cw_for(L, ix_e_alt(L)), 1} : Tile{0, 0, 0})
+       : v == 2 ? (ix_cw(L) > 1 ? Tile{ix_e(L), ix_cw(L) / 2, 1} : Tile{0, 0, 0})
+                : Tile{0, 0, 0};
+}
+constexpr bool ix_valid(int L, int v) {
+  return v == 0 || (v < 3 && tile_fits(L, ix_cand(L, v), 1) && !tile_eq(ix_cand(L, v), ix_cand(L, 0)) &&
+                    (v < 2 || !tile_eq(ix_cand(L, v), ix_cand(L, 1))));
 }
 
 template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
                                          const void* lam, double lsc, cudaStream_t st, int kept) {
   cudaError_t err_ = cudaErrorInvalidValue;
+  // forms 0 and 1 follow the tuning; the adjoint forms keep the rule
+  const int v = form <= 1 ? g.tv[TUNE_X_INV] : 0;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
     // the direct-load kernel measured faster than the TMA-staged k_inv_x on B200
     // (0.19 vs 0.28 ms at 256^3 FP32, rotational); k_inv_x stays available
-    // 8 elements per thread (U held in registers across the output fields; 16 at
-    // L = 1024 in FP32, with per-field loads)
-    constexpr int E = wide1024(LL) ? 16 : (std::is_same<T, float>::value ? (8 < LL ? 8 : LL) : e_reg(LL));
-    constexpr int CW = wide1024(LL) ? 8 : cw_for(LL, E);
-    const int inner = g.Ny * g.Hz;
-    const size_t sm = (size_t)LL * CW * sizeof(V);
-    const int nzk = g.Nz / 3 + 1;
-    const unsigned blocks = kept ? (unsigned)((2 * (g.Ny / 3) + 1) * ((nzk + CW - 1) / CW))
-                                 : (unsigned)((inner + CW - 1) / CW);
-    auto run = [&](auto kern) {
-      if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
-      kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc, kept);
-      ++g_launches;
-      err_ = cudaGetLastError();
+    auto tile = [&](auto vc) {
+      constexpr Tile c = ix_cand(LL, decltype(vc)::value);
+      constexpr int E = c.E, CW = c.CW;
+      const int inner = g.Ny * g.Hz;
+      const size_t sm = (size_t)LL * CW * sizeof(V);
+      const int nzk = g.Nz / 3 + 1;
+      const unsigned blocks = kept ? (unsigned)((2 * (g.Ny / 3) + 1) * ((nzk + CW - 1) / CW))
+                                   : (unsigned)((inner + CW - 1) / CW);
+      auto run = [&](auto kern) {
+        if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
+        kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc, kept);
+        ++g_launches;
+        err_ = cudaGetLastError();
+      };
+      if (form == 0) run(k_inv_x_ld<T, LL, E, CW, 0>);
+      else if (form == 1) run(k_inv_x_ld<T, LL, E, CW, 1>);
+      else if constexpr (decltype(vc)::value == 0) {
+        if (form == 3) run(k_inv_x_ld<T, LL, E, CW, 3>);
+        else if (form == 4) run(k_inv_x_ld<T, LL, E, CW, 4>);
+      }
     };
-    if (form == 0) run(k_inv_x_ld<T, LL, E, CW, 0>);
-    else if (form == 1) run(k_inv_x_ld<T, LL, E, CW, 1>);
-    else if (form == 3) run(k_inv_x_ld<T, LL, E, CW, 3>);
-    else if (form == 4) run(k_inv_x_ld<T, LL, E, CW, 4>);
+    if (v == 1 && ix_valid(LL, 1)) {
+      if constexpr (ix_valid(LL, 1)) tile(std::integral_constant<int, 1>{});
+    } else if (v == 2 && ix_valid(LL, 2)) {
+      if constexpr (ix_valid(LL, 2)) tile(std::integral_constant<int, 2>{});
+    } else {
+      tile(std::integral_constant<int, 0>{});
+    }
   });
   return err_;
 }
 
+// shared-memory slot variant of the z pass: E elements per thread, nl lines per
+// block within about 106 KB of shared memory
+template <int NZ, int FORM, int E>
+static cudaError_t z_slots(const Geo& g, void* P, const void* tw, cudaStream_t st, int nmem, long long msP,
+                           int zkeep) {
+  constexpr int M = NZ / 2;
+  constexpr int TPL = M / E;
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
+  constexpr int NSL = NIN > NOUT ? NIN : NOUT;
+  const long long nlines = (long long)g.Nx * g.Ny;
+  int nl = 256 / TPL;
+  while (nl > 1 && (size_t)NSL * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
+  const size_t sm = (size_t)NSL * nl * zslot<M>() * sizeof(V);
+  cudaError_t err;
+  auto k = k_z_fused<T, NZ, E, FORM>;
+  if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
+  k<<<dim3((unsigned)((nlines + nl - 1) / nl), nmem), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl, msP, zkeep);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+// z candidates (forms 0, 1, 2): 1 = the slot kernel with 8 elements per thread
+// (12 with a factor 3), 2 = the slot kernel with 4 (power-of-two lines)
+template <int NZ, int FORM> constexpr bool z_rule_slots() {
+  constexpr int M = NZ / 2;
+  return !(std::is_same<T, float>::value && M <= 512) &&
+         !(!std::is_same<T, float>::value && FORM != 3 && M % 3 != 0 && M / ztma_e<T>() <= 32);
+}
+template <int NZ, int FORM> constexpr bool z_valid(int v) {
+  constexpr int M = NZ / 2;
+  return v == 0 || (FORM <= 2 && ((v == 1 && !z_rule_slots<NZ, FORM>()) ||
+                                  (v == 2 && M % 3 != 0 && M >= 8 && M / 4 <= 256)));
+}
+
 template <int NZ, int FORM>
 static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr, cudaStream_t st, int nmem,
-                                long long msP, int zkeep) {
+                                long long msP, int zkeep, int v) {
   constexpr int M = NZ / 2;
   if (zkeep < 0) zkeep = M;
-  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
+  constexpr int NIN = z_nin(FORM);
   const long long nlines = (long long)g.Nx * g.Ny;
   cudaError_t err;
+  if constexpr (z_valid<NZ, FORM>(1)) {
+    if (v == 1) return z_slots<NZ, FORM, e_mixed(M, 8)>(g, P, tw, st, nmem, msP, zkeep);
+  }
+  if constexpr (z_valid<NZ, FORM>(2)) {
+    if (v == 2) return z_slots<NZ, FORM, 4>(g, P, tw, st, nmem, msP, zkeep);
+  }
   if constexpr (FORM != 3 && M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
     // FP64: bulk-copy variant (whole groups, 16-byte aligned group starts)
     constexpr int LPB = ztma_lpb<T, NZ>();
@@ -208,17 +318,7 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
     return cudaGetLastError();
   }
   // shared-memory slot variant (large lines, and line lengths with a factor 3)
-  constexpr int E = e_mixed(M, 8);
-  constexpr int TPL = M / E;
-  constexpr int NSL = NIN > NOUT ? NIN : NOUT;
-  int nl = 256 / TPL;
-  while (nl > 1 && (size_t)NSL * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
-  const size_t sm = (size_t)NSL * nl * zslot<M>() * sizeof(V);
-  auto k = k_z_fused<T, NZ, E, FORM>;
-  if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
-  k<<<dim3((unsigned)((nlines + nl - 1) / nl), nmem), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, nl, msP, zkeep);
-  ++g_launches;
-  return cudaGetLastError();
+  return z_slots<NZ, FORM, e_mixed(M, 8)>(g, P, tw, st, nmem, msP, zkeep);
 }
 
 template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, const void* tw, int* zerr,
@@ -227,10 +327,11 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, cons
   if (form == 3 && nmem != 1) return err;  // the adjoint z pass has no member batching
   dispatch_L_sff(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
-    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st, nmem, msP, zkeep);
-    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP, zkeep);
-    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP, zkeep);
-    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0, zkeep);
+    const int v = g.tv[TUNE_Z];
+    if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
+    else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
+    else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
+    else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0, zkeep, 0);
   });
   return err;
 }
@@ -264,10 +365,15 @@ template <> cudaError_t Launch<T>::z_single(const Geo& g, int dir, const void* i
 template <int FORM, int MODE, int LL>
 static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st);
 
+// forward x candidates (MODE_STEP): 1 = the split form (strided x FFT, then the
+// elementwise epilogue) where the rule is the fused TMA kernel
+constexpr bool fx_valid(int L, int v) { return v == 0 || (v == 1 && xcw(L) * sizeof(V) >= 64); }
+
 template <int FORM, int MODE, int LL>
 static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st) {
   constexpr int CW = xcw(LL);
-  if constexpr (CW * sizeof(V) < 64) {
+  const bool split = CW * sizeof(V) < 64 || (MODE == MODE_STEP && g.tv[TUNE_X_FWD] == 1);
+  if (split) {
     // tiles narrower than 64-byte rows: forward x FFT in place, then the elementwise epilogue
     constexpr int NF = FORM == 1 ? 3 : 6;
     cudaError_t err = Launch<T>::strided(g, 0, -1, const_cast<void*>(P), NF, tw, st);
@@ -277,9 +383,9 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
     k_spec_epi<T, FORM, MODE><<<grid1d(g.S, 256), 256, sm, st>>>((const V*)P, g, a);
     ++g_launches;
     return cudaGetLastError();
-  } else {
-    return fwd_x_fused<FORM, MODE, LL>(g, P, a, tw, st);
   }
+  if constexpr (CW * sizeof(V) >= 64) return fwd_x_fused<FORM, MODE, LL>(g, P, a, tw, st);
+  return cudaErrorInvalidValue;
 }
 
 template <int FORM, int MODE, int LL>
@@ -290,7 +396,8 @@ static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, 
   const int ntiles = (inner + CW - 1) / CW;
   size_t sm = (size_t)(MODE == MODE_NLIN ? 2 : 8) * LL * CW * sizeof(V) + (size_t)LL * (CW + 1) * sizeof(V) + 128;
   if (MODE == MODE_FLUX) sm += (size_t)(a.nradii + 1) * sizeof(double);
-  const int per_sm = (int)((220 * 1024) / sm) >= 2 ? 2 : 1;
+  const int bps = MODE == MODE_STEP ? g.tb[TUNE_X_FWD] : 0;
+  const int per_sm = bps > 0 ? bps : ((int)((220 * 1024) / sm) >= 2 ? 2 : 1);
   const int blocks = ntiles < 148 * per_sm ? ntiles : 148 * per_sm;
   const int br = LL < 256 ? LL : 256;
   CUtensorMap mP, mA, mB;
@@ -327,23 +434,49 @@ template <> cudaError_t Launch<T>::fwd_x(const Geo& g, int form, int mode, const
   return err;
 }
 
+// SFF x candidates. Inverse: 1 = 4 elements per thread (power-of-two lengths),
+// 2 = half-width column tiles. Forward: 1 = the other split choice (fused
+// epilogue from 64 points on, split below), 2 = half-width column tiles.
+constexpr int sx_e(int N, int dir) { return e_mixed(N, dir > 0 ? 8 : (std::is_same<T, float>::value ? 8 : 4)); }
+constexpr Tile sx_cand(int N, int dir, int v) {
+  return v == 0 ? Tile{sx_e(N, dir), cw_for(N, sx_e(N, dir)), 1}
+       : v == 1 ? (dir > 0 ? (N % 3 != 0 && sx_e(N, dir) > 4 ? Tile{4, cw_for(N, 4), 1} : Tile{0, 0, 0})
+                           : Tile{sx_e(N, dir), cw_for(N, sx_e(N, dir)), 2})
+       : v == 2 ? (cw_for(N, sx_e(N, dir)) > 1 ? Tile{sx_e(N, dir), cw_for(N, sx_e(N, dir)) / 2, 1} : Tile{0, 0, 0})
+                : Tile{0, 0, 0};
+}
+constexpr bool sx_valid(int N, int dir, int v) {
+  return v == 0 || (N <= 512 && v < 3 && tile_fits(N, sx_cand(N, dir, v), 3) &&
+                    !tile_eq(sx_cand(N, dir, v), sx_cand(N, dir, 0)));
+}
+
 template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const void* Tf, void* W, const void* tq,
                                              cudaStream_t st, int nmem, long long msU, long long msT, long long msW) {
   cudaError_t err = cudaErrorInvalidValue;
+  const int v = g.tv[TUNE_X_INV];
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
     if constexpr (NN <= 512) {
       // one NN-point FFT per column and field, 8 elements per thread
-      constexpr int E = e_mixed(NN, 8);
-      constexpr int CW = cw_for(NN, E);
-      const int inner = g.Ny * g.Hz;
-      const size_t sm = 3ull * NN * CW * sizeof(V);  // exchange + 2 staging tiles
-      auto k = k_sff_inv_x<T, NN, E, CW>;
-      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g,
-                                                                   (const V*)tq, msU, msT, msW);
-      ++g_launches;
-      err = cudaGetLastError();
+      auto run = [&](auto vc) {
+        constexpr Tile c = sx_cand(NN, 1, decltype(vc)::value);
+        constexpr int E = c.E, CW = c.CW;
+        const int inner = g.Ny * g.Hz;
+        const size_t sm = 3ull * NN * CW * sizeof(V);  // exchange + 2 staging tiles
+        auto k = k_sff_inv_x<T, NN, E, CW>;
+        if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+        k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((const V*)U, (const V*)Tf, (V*)W, g,
+                                                                     (const V*)tq, msU, msT, msW);
+        ++g_launches;
+        err = cudaGetLastError();
+      };
+      if (v == 1 && sx_valid(NN, 1, 1)) {
+        if constexpr (sx_valid(NN, 1, 1)) run(std::integral_constant<int, 1>{});
+      } else if (v == 2 && sx_valid(NN, 1, 2)) {
+        if constexpr (sx_valid(NN, 1, 2)) run(std::integral_constant<int, 2>{});
+      } else {
+        run(std::integral_constant<int, 0>{});
+      }
     }
   });
   return err;
@@ -352,26 +485,36 @@ template <> cudaError_t Launch<T>::sff_inv_x(const Geo& g, const void* U, const 
 template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq,
                                              cudaStream_t st, int nmem) {
   cudaError_t err = cudaErrorInvalidValue;
+  const int v = g.tv[TUNE_X_FWD];
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
     if constexpr (NN <= 512) {
       // one NN-point FFT per column and product; four accumulators per element:
       // 8 (FP32) / 4 (FP64) elements per thread
-      constexpr int E = e_mixed(NN, std::is_same<T, float>::value ? 8 : 4);
-      constexpr int CW = cw_for(NN, E);
-      const int inner = g.Ny * g.Hz;
-      const size_t sm = 3ull * NN * CW * sizeof(V);
-      // from 64 points on, the x kernel writes the assembled vectors and a coalesced
-      // elementwise kernel does the epilogue (its ten state reads stalled the fused form)
-      constexpr bool SPLIT = NN >= 64;
-      auto k = k_sff_fwd_x<T, NN, E, CW, SPLIT>;
-      if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-      k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((V*)P, g, a, (const V*)tq);
-      ++g_launches;
-      if ((err = cudaGetLastError()) != cudaSuccess || !SPLIT) return;
-      k_sff_epi<T><<<dim3(grid1d(g.S, 256), nmem), 256, 0, st>>>((const V*)P, g, a);
-      ++g_launches;
-      err = cudaGetLastError();
+      auto run = [&](auto vc) {
+        constexpr Tile c = sx_cand(NN, -1, decltype(vc)::value);
+        constexpr int E = c.E, CW = c.CW;
+        const int inner = g.Ny * g.Hz;
+        const size_t sm = 3ull * NN * CW * sizeof(V);
+        // from 64 points on, the x kernel writes the assembled vectors and a coalesced
+        // elementwise kernel does the epilogue (its ten state reads stalled the fused form)
+        constexpr bool SPLIT = (NN >= 64) != (c.NT == 2);
+        auto k = k_sff_fwd_x<T, NN, E, CW, SPLIT>;
+        if ((err = smem_attr(k, sm)) != cudaSuccess) return;
+        k<<<dim3((inner + CW - 1) / CW, nmem), CW * (NN / E), sm, st>>>((V*)P, g, a, (const V*)tq);
+        ++g_launches;
+        if ((err = cudaGetLastError()) != cudaSuccess || !SPLIT) return;
+        k_sff_epi<T><<<dim3(grid1d(g.S, 256), nmem), 256, 0, st>>>((const V*)P, g, a);
+        ++g_launches;
+        err = cudaGetLastError();
+      };
+      if (v == 1 && sx_valid(NN, -1, 1)) {
+        if constexpr (sx_valid(NN, -1, 1)) run(std::integral_constant<int, 1>{});
+      } else if (v == 2 && sx_valid(NN, -1, 2)) {
+        if constexpr (sx_valid(NN, -1, 2)) run(std::integral_constant<int, 2>{});
+      } else {
+        run(std::integral_constant<int, 0>{});
+      }
     }
   });
   return err;
@@ -480,6 +623,44 @@ template <> cudaError_t Launch<T>::dealias_copy(const Geo& g, const void* A, voi
   k_dealias_copy<T><<<grid1d(g.S * ncomp, 256), 256, 0, st>>>((const V*)A, (V*)B, ncomp, g);
   ++g_launches;
   return cudaGetLastError();
+}
+
+template <> bool Launch<T>::tune_valid(const Geo& g, int form, int cls, int v) {
+  if (v == 0) return true;
+  if (v < 0 || v >= NCAND) return false;
+  const bool sff = g.basis == 1;
+  bool ok = false;
+  switch (cls) {
+    case TUNE_Y_INV:
+    case TUNE_Y_FWD:
+      dispatch_L_sff(g.Ny, [&](auto Lc) { ok = str_valid(decltype(Lc)::value, v); });
+      break;
+    case TUNE_X_INV:
+      if (sff) dispatch_L_sff(g.Nx, [&](auto Lc) { ok = sx_valid(decltype(Lc)::value, 1, v); });
+      else if (form <= 1) dispatch_L(g.Nx, [&](auto Lc) { ok = ix_valid(decltype(Lc)::value, v); });
+      break;
+    case TUNE_X_FWD:
+      if (sff) dispatch_L_sff(g.Nx, [&](auto Lc) { ok = sx_valid(decltype(Lc)::value, -1, v); });
+      else if (form <= 1) dispatch_L(g.Nx, [&](auto Lc) { ok = fx_valid(decltype(Lc)::value, v); });
+      break;
+    case TUNE_Z:
+      dispatch_L_sff(g.Nz, [&](auto Lc) {
+        constexpr int NZ = decltype(Lc)::value;
+        ok = form == 0 ? z_valid<NZ, 0>(v) : form == 1 ? z_valid<NZ, 1>(v) : form == 2 ? z_valid<NZ, 2>(v) : false;
+      });
+      break;
+    default:
+      break;
+  }
+  return ok;
+}
+
+template <> bool Launch<T>::tune_blocks(const Geo& g, int form, int cls) {
+  if (cls == TUNE_Y_INV || cls == TUNE_Y_FWD) return true;
+  bool ok = false;
+  if (cls == TUNE_X_FWD && g.basis == 0 && form <= 1)
+    dispatch_L(g.Nx, [&](auto Lc) { ok = xcw(decltype(Lc)::value) * sizeof(V) >= 64 && g.tv[TUNE_X_FWD] == 0; });
+  return ok;
 }
 
 }  // namespace ts

@@ -57,6 +57,11 @@ template <typename T> struct Launch {
   static cudaError_t scale(void* A, long long n, double s, cudaStream_t st);
   static cudaError_t init_temp(const Geo& g, void* A, double amp, double kmax, unsigned long long key, cudaStream_t st);
   static cudaError_t dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
+  // launch tuning (Geo::tv, Geo::tb): whether kernel candidate v (0 = the rule) of pass class
+  // cls exists for this geometry and product form (form as z_fused; the basis selects the
+  // SFF x kernels), and whether the class takes a blocks-per-SM count (persistent launches)
+  static bool tune_valid(const Geo& g, int form, int cls, int v);
+  static bool tune_blocks(const Geo& g, int form, int cls);
 };
 
 bool size_supported(int n);

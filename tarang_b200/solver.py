@@ -13,7 +13,9 @@ Reference-named wrappers (paths inside anandogc/tarang ``trunk/lib``):
 from __future__ import annotations
 
 import ctypes
+import json
 import math
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -32,6 +34,28 @@ class Forcing:
     outer_radius: float
     energy_supply: np.ndarray
     helicity_supply: np.ndarray | None = None
+
+
+def _tuning_struct(tuning: dict) -> L.TsTuning:
+    t = L.TsTuning()
+    for i in range(5):
+        t.variant[i] = int(tuning["variant"][i])
+        t.blocks_per_sm[i] = int(tuning["blocks_per_sm"][i])
+    return t
+
+
+def _cache_put(path: str, key: str, tuning: dict):
+    data = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+    data[key] = tuning
+    d = os.path.dirname(os.path.abspath(path))
+    os.makedirs(d, exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
 
 
 def _ptr(a) -> int:
@@ -126,6 +150,51 @@ class Plan:
     def status(self):
         """Synchronise the plan's stream; raise TsError if a bounded device wait gave up earlier."""
         L.check(self.lib.ts_plan_status(self.h), "ts_plan_status")
+
+    # ------------------------------------------------------------------
+    # launch tuning (candidate kernels per pass class; see ts_plan_autotune)
+    def tuning(self) -> dict:
+        t = L.TsTuning()
+        L.check(self.lib.ts_plan_get_tuning(self.h, ctypes.byref(t)), "ts_plan_get_tuning")
+        return {"variant": list(t.variant), "blocks_per_sm": list(t.blocks_per_sm)}
+
+    def set_tuning(self, tuning: dict):
+        L.check(self.lib.ts_plan_set_tuning(self.h, ctypes.byref(_tuning_struct(tuning))), "ts_plan_set_tuning")
+
+    def tuning_candidates(self) -> dict:
+        """{class: {"variants": [candidate indices], "blocks": takes a blocks-per-SM count}}"""
+        out = {}
+        for c, name in enumerate(L.TUNE_CLASSES):
+            m, b = ctypes.c_int(), ctypes.c_int()
+            L.check(self.lib.ts_tuning_candidates(self.h, c, ctypes.byref(m), ctypes.byref(b)), "ts_tuning_candidates")
+            out[name] = {"variants": [v for v in range(4) if m.value >> v & 1], "blocks": bool(b.value)}
+        return out
+
+    def tuning_key(self) -> str:
+        import torch
+        dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+        c = self.cfg
+        return (f"{dev}|{self.basis}|{'x'.join(map(str, self.N))}|{self.precision}|form{c.nlin_form}"
+                f"|dealias{c.dealias_mode}|force{c.force_type}")
+
+    def autotune(self, reps: int = 3, cache: str | None = None) -> dict:
+        """Pick the fastest kernel candidate of every pass class on this GPU (ts_plan_autotune) and
+        return the timing report.  cache: a JSON file of earlier results keyed by device and plan
+        configuration; a hit applies the stored tuning without timing anything."""
+        key = self.tuning_key()
+        if cache and os.path.exists(cache):
+            with open(cache) as f:
+                hit = json.load(f).get(key)
+            if hit is not None:
+                self.set_tuning(hit)
+                return {"cached": True, "tuning": hit}
+        buf = ctypes.create_string_buffer(1 << 16)
+        L.check(self.lib.ts_plan_autotune(self.h, reps, buf, len(buf)), "ts_plan_autotune")
+        report = json.loads(buf.value.decode())
+        report["tuning"] = self.tuning()
+        if cache:
+            _cache_put(cache, key, report["tuning"])
+        return report
 
     # ------------------------------------------------------------------
     def rk4_step(self, u, nsteps: int = 1):
@@ -330,7 +399,24 @@ class Ensemble:
         L.check(self.lib.ts_ensemble_nusselt(self.h, out.ctypes.data_as(L._D)), "ts_ensemble_nusselt")
         return out
 
+    def tuning(self, m: int) -> dict:
+        """launch tuning of the size group of member m"""
+        t = L.TsTuning()
+        L.check(self.lib.ts_ensemble_get_tuning(self.h, m, ctypes.byref(t)), "ts_ensemble_get_tuning")
+        return {"variant": list(t.variant), "blocks_per_sm": list(t.blocks_per_sm)}
+
+    def set_tuning(self, m: int, tuning: dict):
+        L.check(self.lib.ts_ensemble_set_tuning(self.h, m, ctypes.byref(_tuning_struct(tuning))),
+                "ts_ensemble_set_tuning")
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Tune every size group on whole ensemble steps (ts_ensemble_autotune); states are kept."""
+        buf = ctypes.create_string_buffer(1 << 18)
+        L.check(self.lib.ts_ensemble_autotune(self.h, reps, buf, len(buf)), "ts_ensemble_autotune")
+        return json.loads(buf.value.decode())
+
     def energy(self, m: int, which: str = "T") -> float:
+        self.synchronize()  # ensemble steps run on the ensemble's own stream
         p, u, t = self.member(m)
         e = ctypes.c_double()
         L.check(self.lib.ts_energy(p, t if which == "T" else u, 1 if which == "T" else 3, ctypes.byref(e)), "ts_energy")

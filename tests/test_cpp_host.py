@@ -55,6 +55,15 @@ def test_host_mirror_matches_python_binding(cuda, tmp_path):
     assert np.max(np.abs(np.array(out["Pi"]) - plan.flux(u, [2.0, 4.0, 8.0]))) < 1e-14
 
 
+@pytest.mark.gpu
+def test_host_mirror_autotuned_matches_rule(cuda, tmp_path):
+    exe = build_driver(tmp_path)
+    a = run_driver(exe, "fff", 64, 3)
+    b = run_driver(exe, "fff_tuned", 64, 3)
+    assert abs(a["e1"] - b["e1"]) < 1e-13 * a["e1"]  # FP64: candidates differ in rounding only
+    assert np.max(np.abs(np.array(a["Ek"]) - np.array(b["Ek"]))) < 1e-13 * a["e1"]
+
+
 def run_driver(exe, *args):
     r = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
