@@ -1314,6 +1314,7 @@ template <typename Measure> int descend(const ts_plan* p, Geo& g, Measure&& meas
       js += buf;
       first = false;
     };
+    if (cls > 0) CKS(measure(&best));  // re-time the incumbent: clocks drift between classes
     log(g.tv[cls], g.tb[cls], best);
     const int v0 = g.tv[cls];
     int bv = v0;
@@ -1533,7 +1534,7 @@ int ts_ensemble_autotune(ts_ensemble* e, int reps, char* report, size_t report_l
   auto step = [&]() -> int { return ts_ensemble_run(e, 1); };
   double t1 = 0;
   int rc = time_calls(e->origin, 1, 1, step, &t1);
-  int n = t1 > 0 ? (int)ceil(5.0 / t1) : 16;
+  int n = t1 > 0 ? (int)ceil(30.0 / t1) : 16;
   n = n < 1 ? 1 : (n > 16 ? 16 : n);
   auto measure = [&](double* ms) {
     ens_invalidate(e);  // the next run re-captures the graph with the current tuning

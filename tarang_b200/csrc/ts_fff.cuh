@@ -558,14 +558,18 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
 
 // blocks per SM the register z kernel is compiled for: 6 (170 registers), 3 for
 // the 12-element radix-3 lines (which would spill at 170)
-template <int NZ> __host__ __device__ constexpr int zreg_min_blocks() { return (NZ / 2) % 3 == 0 ? 3 : 6; }
+// (8 for the 4-element variant)
+template <int NZ, int EZ = 0> __host__ __device__ constexpr int zreg_min_blocks() {
+  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : 6);
+}
 
-template <typename T, int NZ, int FORM>
-__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ>())
+// EZ = 0: 8 elements per thread, 12 for a line length with a factor 3 (radices
+// 4, 2|4, 3); EZ = 4: 4 elements per thread (twice the lanes per line)
+template <typename T, int NZ, int FORM, int EZ = 0>
+__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
-  // 8 elements per thread, 12 for a line length with a factor 3 (radices 4, 2|4, 3)
-  constexpr int M = NZ / 2, H = M + 1, E = (M % 3 == 0) ? 12 : 8, TPL = M / E, LDX = zslot<M>();
+  constexpr int M = NZ / 2, H = M + 1, E = EZ ? EZ : ((M % 3 == 0) ? 12 : 8), TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
   static_assert(NIN <= 6, "the adjoint form runs in k_z_reg_adj");

@@ -258,7 +258,8 @@ static cudaError_t z_slots(const Geo& g, void* P, const void* tw, cudaStream_t s
 }
 
 // z candidates (forms 0, 1, 2): 1 = the slot kernel with 8 elements per thread
-// (12 with a factor 3), 2 = the slot kernel with 4 (power-of-two lines)
+// (12 with a factor 3), 2 = the slot kernel with 4 (power-of-two lines), 3 = the
+// FP32 register kernel with 4 elements per thread (lines of up to 256 points)
 template <int NZ, int FORM> constexpr bool z_rule_slots() {
   constexpr int M = NZ / 2;
   return !(std::is_same<T, float>::value && M <= 512) &&
@@ -267,7 +268,8 @@ template <int NZ, int FORM> constexpr bool z_rule_slots() {
 template <int NZ, int FORM> constexpr bool z_valid(int v) {
   constexpr int M = NZ / 2;
   return v == 0 || (FORM <= 2 && ((v == 1 && !z_rule_slots<NZ, FORM>()) ||
-                                  (v == 2 && M % 3 != 0 && M >= 8 && M / 4 <= 256)));
+                                  (v == 2 && M % 3 != 0 && M >= 8 && M / 4 <= 256) ||
+                                  (v == 3 && std::is_same<T, float>::value && M % 3 != 0 && M >= 8 && M / 4 <= 64)));
 }
 
 template <int NZ, int FORM>
@@ -283,6 +285,15 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   }
   if constexpr (z_valid<NZ, FORM>(2)) {
     if (v == 2) return z_slots<NZ, FORM, 4>(g, P, tw, st, nmem, msP, zkeep);
+  }
+  if constexpr (z_valid<NZ, FORM>(3)) {
+    if (v == 3) {
+      constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 4);
+      k_z_reg<T, NZ, FORM, 4><<<dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), NT, 0, st>>>((V*)P, g, (const V*)tw,
+                                                                                              msP, zkeep);
+      ++g_launches;
+      return cudaGetLastError();
+    }
   }
   if constexpr (FORM != 3 && M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
     // FP64: bulk-copy variant (whole groups, 16-byte aligned group starts)
@@ -362,17 +373,32 @@ template <> cudaError_t Launch<T>::z_single(const Geo& g, int dir, const void* i
   return err;
 }
 
-template <int FORM, int MODE, int LL>
+template <int FORM, int MODE, int LL, int E, int CW>
 static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st);
 
 // forward x candidates (MODE_STEP): 1 = the split form (strided x FFT, then the
-// elementwise epilogue) where the rule is the fused TMA kernel
-constexpr bool fx_valid(int L, int v) { return v == 0 || (v == 1 && xcw(L) * sizeof(V) >= 64); }
+// elementwise epilogue) where the rule is the fused TMA kernel; 2 = the fused
+// kernel with half-width column tiles (32-byte rows in FP32; where the rule
+// splits, the fused kernel at the rule's tile width); 3 = the fused kernel with
+// 4 elements per thread (twice the threads)
+constexpr bool fx_rule_fused(int L) { return xcw(L) * sizeof(V) >= 64; }
+constexpr int fx_cw2(int L) { return fx_rule_fused(L) ? xcw(L) / 2 : xcw(L); }
+constexpr bool fx_valid(int L, int v) {
+  return v == 0 || (v == 1 && fx_rule_fused(L)) || (v == 2 && fx_cw2(L) * sizeof(V) >= 16 && fx_cw2(L) * (L / emin(E_ACC, L)) >= 32) ||
+         (v == 3 && fx_rule_fused(L) && L >= 8 && E_ACC > 4);
+}
 
 template <int FORM, int MODE, int LL>
 static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st) {
   constexpr int CW = xcw(LL);
-  const bool split = CW * sizeof(V) < 64 || (MODE == MODE_STEP && g.tv[TUNE_X_FWD] == 1);
+  const int v = MODE == MODE_STEP ? g.tv[TUNE_X_FWD] : 0;
+  if constexpr (fx_valid(LL, 2)) {
+    if (v == 2) return fwd_x_fused<FORM, MODE, LL, emin(E_ACC, LL), fx_cw2(LL)>(g, P, a, tw, st);
+  }
+  if constexpr (fx_valid(LL, 3)) {
+    if (v == 3) return fwd_x_fused<FORM, MODE, LL, 4, CW>(g, P, a, tw, st);
+  }
+  const bool split = CW * sizeof(V) < 64 || v == 1;
   if (split) {
     // tiles narrower than 64-byte rows: forward x FFT in place, then the elementwise epilogue
     constexpr int NF = FORM == 1 ? 3 : 6;
@@ -384,14 +410,12 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
     ++g_launches;
     return cudaGetLastError();
   }
-  if constexpr (CW * sizeof(V) >= 64) return fwd_x_fused<FORM, MODE, LL>(g, P, a, tw, st);
+  if constexpr (CW * sizeof(V) >= 64) return fwd_x_fused<FORM, MODE, LL, emin(E_ACC, LL), CW>(g, P, a, tw, st);
   return cudaErrorInvalidValue;
 }
 
-template <int FORM, int MODE, int LL>
+template <int FORM, int MODE, int LL, int E, int CW>
 static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st) {
-  constexpr int E = emin(E_ACC, LL);
-  constexpr int CW = xcw(LL);
   const int inner = g.Ny * g.Hz;
   const int ntiles = (inner + CW - 1) / CW;
   size_t sm = (size_t)(MODE == MODE_NLIN ? 2 : 8) * LL * CW * sizeof(V) + (size_t)LL * (CW + 1) * sizeof(V) + 128;
@@ -659,7 +683,11 @@ template <> bool Launch<T>::tune_blocks(const Geo& g, int form, int cls) {
   if (cls == TUNE_Y_INV || cls == TUNE_Y_FWD) return true;
   bool ok = false;
   if (cls == TUNE_X_FWD && g.basis == 0 && form <= 1)
-    dispatch_L(g.Nx, [&](auto Lc) { ok = xcw(decltype(Lc)::value) * sizeof(V) >= 64 && g.tv[TUNE_X_FWD] == 0; });
+    dispatch_L(g.Nx, [&](auto Lc) {
+      constexpr int LL = decltype(Lc)::value;
+      const int v = g.tv[TUNE_X_FWD];
+      ok = (v == 0 && fx_rule_fused(LL)) || (v >= 2 && fx_valid(LL, v));
+    });
   return ok;
 }
 

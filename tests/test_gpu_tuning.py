@@ -120,9 +120,9 @@ def test_set_tuning_rejects_missing_candidates(cuda):
         plan.set_tuning(with_class(2, 0, 2))  # z takes no blocks-per-SM count
     with pytest.raises(tb.TsError):
         plan.set_tuning(with_class(0, 7, 0))
-    missing = [v for v in range(4) if v not in cand["x_fwd"]["variants"]]
+    assert 3 not in cand["x_inv"]["variants"]  # the FFF inverse x pass has three candidates
     with pytest.raises(tb.TsError):
-        plan.set_tuning(with_class(4, missing[0], 0))
+        plan.set_tuning(with_class(0, 3, 0))
     assert plan.tuning() == {"variant": [0] * 5, "blocks_per_sm": [0] * 5}
 
 
