@@ -173,23 +173,29 @@ __device__ __forceinline__ void pass_compute(V* v, int t, const V* __restrict__ 
 // padded shared-memory row index: one spare slot every 16 complex values keeps
 // the threads of a line (consecutive rows E apart) on distinct banks
 template <bool PAD> __device__ __forceinline__ int prow(int r) { return PAD ? r + (r >> 4) : r; }
+// exchange row of logical row r: padded (PAD), or with bit 0 flipped by bit SWK
+// (SWK > 0; a permutation of the rows) so that rows 2^SWK apart, which one
+// radix pass stores from neighbouring threads, land on different bank pairs
+template <bool PAD, int SWK> __device__ __forceinline__ int xrow(int r) {
+  return SWK > 0 ? (r ^ ((r >> SWK) & 1)) : prow<PAD>(r);
+}
 
 // Full FFT of one line whose E-element slice per thread is in registers (loaded
 // in load_row order); the line's L elements are exchanged through shared memory
 // `sm` addressed as sm[row*rs + cs] (caller supplies the per-thread column
 // offset cs and the row stride rs).  All threads of the block must call it.
 // On return v[s] holds output row final_row(t, s).
-template <int L, int E, int DIR, int P = 0, bool PAD = false, bool REV = false, typename V>
+template <int L, int E, int DIR, int P = 0, bool PAD = false, bool REV = false, int SWK = 0, typename V>
 __device__ __forceinline__ void fft_regs(V* v, int t, V* sm, int rs, int cs, const V* __restrict__ tw, int tws) {
   pass_compute<L, E, P, DIR, REV>(v, t, tw, tws);
   if constexpr (P + 1 < npasses(L, E)) {
 #pragma unroll
-    for (int s = 0; s < E; ++s) sm[prow<PAD>(Pass<L, E, P, REV>::out_row(t, s)) * rs + cs] = v[s];
+    for (int s = 0; s < E; ++s) sm[xrow<PAD, SWK>(Pass<L, E, P, REV>::out_row(t, s)) * rs + cs] = v[s];
     __syncthreads();
 #pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = sm[prow<PAD>(Pass<L, E, P + 1, REV>::in_row(t, s)) * rs + cs];
+    for (int s = 0; s < E; ++s) v[s] = sm[xrow<PAD, SWK>(Pass<L, E, P + 1, REV>::in_row(t, s)) * rs + cs];
     __syncthreads();
-    fft_regs<L, E, DIR, P + 1, PAD, REV>(v, t, sm, rs, cs, tw, tws);
+    fft_regs<L, E, DIR, P + 1, PAD, REV, SWK>(v, t, sm, rs, cs, tw, tws);
   }
 }
 

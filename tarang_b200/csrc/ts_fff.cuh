@@ -148,18 +148,18 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
     issue(blockIdx.x, 0);
     issue(blockIdx.x + gridDim.x, 1);
   }
-  uint32_t ph[2] = {0, 0};
   const int nout = ROT ? 6 : 3;
   int k = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+    // slots alternate, so slot k & 1 completes its phase (k >> 1) & 1
     const int slot = k & 1;
-    const bool got = mbar_wait(&bar[slot], ph[slot], err);
+    const uint32_t phase = (uint32_t)(k >> 1) & 1u;
+    const bool got = mbar_wait(&bar[slot], phase, err);
     if (__syncthreads_or(!got)) {
       // give the copies in flight a second bounded chance to land, then leave
-      if (threadIdx.x == 0) mbar_wait(&bar[slot], ph[slot], nullptr);
+      if (threadIdx.x == 0) mbar_wait(&bar[slot], phase, nullptr);
       return;
     }
-    ph[slot] ^= 1;
     const int col = tile * CW + c;
     const bool ok = col < inner;
     const int ly = ok ? col / g.Hz : 0, lz = ok ? col % g.Hz : 0;
@@ -742,16 +742,16 @@ __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, c
     issue(blockIdx.x, 0);
     issue(blockIdx.x + gridDim.x, 1);
   }
-  uint32_t ph[2] = {0, 0};
   int k = 0;
   for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x, ++k) {
+    // slots alternate, so slot k & 1 completes its phase (k >> 1) & 1
     const int slot = k & 1;
-    const bool got = mbar_wait(&bar[slot], ph[slot], err);
+    const uint32_t phase = (uint32_t)(k >> 1) & 1u;
+    const bool got = mbar_wait(&bar[slot], phase, err);
     if (__syncthreads_or(!got)) {
-      if (threadIdx.x == 0) mbar_wait(&bar[slot], ph[slot], nullptr);
+      if (threadIdx.x == 0) mbar_wait(&bar[slot], phase, nullptr);
       return;
     }
-    ph[slot] ^= 1;
     V in[NIN][E];
 #pragma unroll
     for (int c = 0; c < NIN; ++c) {
@@ -1009,7 +1009,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   // TMA destinations: 128-byte aligned (the launcher adds 128 bytes of slack)
   unsigned char* smraw = smraw_ + ((128 - (smem_u32(smraw_) & 127)) & 127);
   V* pst = reinterpret_cast<V*>(smraw);
-  V* xch = pst + 2 * TILE;              // exchange tile, row pitch CW + 1 (bank spread)
+  V* xch = pst + 2 * TILE;              // exchange tile, row pitch CW (L x (CW + 1) reserved)
   V* sst = xch + L * (CW + 1);
   double* sbins = reinterpret_cast<double*>(sst + NST * TILE);
   __shared__ __align__(8) uint64_t bar[3];  // product slots 0, 1; state
@@ -1051,7 +1051,9 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
     issue_item(0);
     issue_item(1);
   }
-  uint32_t ph[3] = {0, 0, 0};
+  // mbarrier phases of the two product slots and the state barrier (scalars:
+  // a runtime-indexed array would live in local memory)
+  uint32_t ph0 = 0, ph1 = 0, phs = 0;
   long long item = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     if (threadIdx.x == 0) issue_state(tile);
@@ -1070,19 +1072,25 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
 
     for (int f = 0; f < NF; ++f, ++item) {
       const int slot = (int)(item & 1);
-      const bool got = mbar_wait(&bar[slot], ph[slot], a.err);
+      const uint32_t phase = slot ? ph1 : ph0;
+      const bool got = mbar_wait(&bar[slot], phase, a.err);
       if (__syncthreads_or(!got)) {
-        if (threadIdx.x == 0) mbar_wait(&bar[slot], ph[slot], nullptr);
+        if (threadIdx.x == 0) mbar_wait(&bar[slot], phase, nullptr);
         return;
       }
-      ph[slot] ^= 1;
+      if (slot) ph1 ^= 1;
+      else ph0 ^= 1;
       V v[E];
       const V* st = pst + slot * TILE + c;
 #pragma unroll
       for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
       __syncthreads();
       if (threadIdx.x == 0) issue_item(item + 2);
-      fft_regs<L, E, -1>(v, t, xch, CW + 1, c, tw, 1);
+      // exchange rows of pitch CW, bit 0 of the row flipped by bit 2 (E = 4) or
+      // bit 1 (E = 8): the first pass stores rows 4 (8) apart from neighbouring
+      // threads, which would share bank pairs; modelled shared-memory wavefronts
+      // 1.0x / 1.25x the minimum, against 2.0x / 1.75x with a padded pitch CW + 1
+      fft_regs<L, E, -1, 0, false, false, (E == 4 ? 2 : 1)>(v, t, xch, CW, c, tw, 1);
 #pragma unroll
       for (int s = 0; s < E; ++s) {
         const int lx = final_row<L, E>(t, s);
@@ -1092,12 +1100,12 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
       }
     }
     if (nstate) {
-      const bool got = mbar_wait(&bar[2], ph[2], a.err);
+      const bool got = mbar_wait(&bar[2], phs, a.err);
       if (__syncthreads_or(!got)) {
-        if (threadIdx.x == 0) mbar_wait(&bar[2], ph[2], nullptr);
+        if (threadIdx.x == 0) mbar_wait(&bar[2], phs, nullptr);
         return;
       }
-      ph[2] ^= 1;
+      phs ^= 1;
     }
     if (ok) {
       const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;

@@ -15,7 +15,11 @@ typedef C<T> V;
 constexpr int E_REG = std::is_same<T, float>::value ? 16 : 8;
 // at L = 1024 the 16-element register FFT would spill under the 512-thread cap
 constexpr int e_reg(int L) { return (L >= 1024 ? 8 : E_REG) < L ? (L >= 1024 ? 8 : E_REG) : L; }
-constexpr int E_ACC = 8;  // forward-x kernel keeps 3 accumulators per element
+// forward-x kernel: 4 elements per thread (3 accumulators each); on B200 at 256^3
+// the 512-thread blocks beat the 8-element, 256-thread form by 6 % in FP32 (3.03
+// vs 3.09 ms per step) and 2.5 % in FP64 (6.78 vs 6.96 ms)
+constexpr int E_ACC = 4;
+constexpr int E_ACC_ALT = 8;
 constexpr int CWMAX = std::is_same<T, float>::value ? 16 : 8;
 constexpr int emin(int a, int b) { return a < b ? a : b; }
 constexpr int cw_for(int L, int E) {
@@ -380,12 +384,12 @@ static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, 
 // elementwise epilogue) where the rule is the fused TMA kernel; 2 = the fused
 // kernel with half-width column tiles (32-byte rows in FP32; where the rule
 // splits, the fused kernel at the rule's tile width); 3 = the fused kernel with
-// 4 elements per thread (twice the threads)
+// 8 elements per thread (half the threads)
 constexpr bool fx_rule_fused(int L) { return xcw(L) * sizeof(V) >= 64; }
 constexpr int fx_cw2(int L) { return fx_rule_fused(L) ? xcw(L) / 2 : xcw(L); }
 constexpr bool fx_valid(int L, int v) {
   return v == 0 || (v == 1 && fx_rule_fused(L)) || (v == 2 && fx_cw2(L) * sizeof(V) >= 16 && fx_cw2(L) * (L / emin(E_ACC, L)) >= 32) ||
-         (v == 3 && fx_rule_fused(L) && L >= 8 && E_ACC > 4);
+         (v == 3 && fx_rule_fused(L) && emin(E_ACC_ALT, L) != emin(E_ACC, L));
 }
 
 template <int FORM, int MODE, int LL>
@@ -396,7 +400,7 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
     if (v == 2) return fwd_x_fused<FORM, MODE, LL, emin(E_ACC, LL), fx_cw2(LL)>(g, P, a, tw, st);
   }
   if constexpr (fx_valid(LL, 3)) {
-    if (v == 3) return fwd_x_fused<FORM, MODE, LL, 4, CW>(g, P, a, tw, st);
+    if (v == 3) return fwd_x_fused<FORM, MODE, LL, emin(E_ACC_ALT, LL), CW>(g, P, a, tw, st);
   }
   const bool split = CW * sizeof(V) < 64 || v == 1;
   if (split) {
