@@ -101,18 +101,19 @@ def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
             "nusselt_mean": float(np.mean(Nu)), "nusselt_finite": bool(np.all(np.isfinite(Nu))), "tuning": tuned}
 
 
-def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024)):
-    """Config 2: FFF 1024^3 decaying turbulence, FP32 rotational, IC k^4 exp(-2(k/8)^2) E=0.5,
-    nu=2e-4, dt=2e-4; steps/s and the per-kernel rates."""
+def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024), prec: str = "f32", tune: bool = True):
+    """Config 2: FFF 1024^3 decaying turbulence, rotational, IC k^4 exp(-2(k/8)^2) E=0.5,
+    nu=2e-4, dt=2e-4; steps/s and the per-kernel rates (FP32 by default; FP64 untuned is the
+    plain FP64 GPU path the FP32 rate is compared with)."""
     import torch
     import ctypes
     import tarang_b200 as tb
     from tarang_b200 import _lib as L
-    plan = tb.Plan(tuple(shape), precision="f32", nlin_form="rotational", dealias="two_thirds", nu=2e-4, dt=2e-4)
+    plan = tb.Plan(tuple(shape), precision=prec, nlin_form="rotational", dealias="two_thirds", nu=2e-4, dt=2e-4)
     plan.set_stream(torch.cuda.current_stream())   # the timing events below go on this stream
     u = plan.field(3)
     plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 8.0), 0, 0.5, u)
-    tuned = tune_plan(plan, reps=1)
+    tuned = tune_plan(plan, reps=1) if tune else None
     plan.rk4_step(u, warmup)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -135,10 +136,48 @@ def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024)):
         if n.value and b.value:
             kern[name] = round(b.value / (tot.value / n.value / 1e3) / 1e9, 1)
     n3 = float(shape[0]) * shape[1] * shape[2]
+    sb = 4 if prec == "f32" else 8
     out = {"steps_per_s": steps / (ms / 1e3), "kernel_GBps": kern, "energy": plan.energy(u),
-           "model_frac": 288.0 * n3 * 4 * steps / (ms / 1e3) / 1e9 / measured_peak()[0], "tuning": tuned}
+           "model_frac": 288.0 * n3 * sb * steps / (ms / 1e3) / 1e9 / measured_peak()[0], "tuning": tuned}
     plan.close()
+    del u
+    torch.cuda.empty_cache()
     return out
+
+
+def ensemble_plain_fp64_leg(steps: int = 3, warmup: int = 1):
+    """The 64 ensemble members advanced the plain way: one FP64 plan per member, stepped one
+    after another with ts_rk4_step_rbc (no batching, no graph, the fixed tile rules).  Returns
+    ensemble-steps/s (all 64 members advanced once per ensemble step), CUDA-event timed."""
+    import torch
+    import tarang_b200 as tb
+    members = tb.ensemble_members()
+    plans, states = [], []
+    for (N, Ra, Pr) in members:
+        p = tb.Plan(N, basis="SFF", precision="f64", dealias="reference", Ra=Ra, Pr=Pr, dt=1e-4,
+                    nu=math.sqrt(Pr / Ra), kappa=1 / math.sqrt(Pr * Ra), kfactor=(math.pi, 2 * math.pi, 2 * math.pi))
+        p.set_stream(torch.cuda.current_stream())
+        u, T = p.field(3), p.field(1)
+        p.init_temperature_perturbation(1e-3, 4.0, 3, T)
+        plans.append(p)
+        states.append((u, T))
+    for p, (u, T) in zip(plans, states):
+        p.rk4_step_rbc(u, T, warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        for p, (u, T) in zip(plans, states):
+            p.rk4_step_rbc(u, T, 1)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    for p in plans:
+        p.close()
+    del states
+    torch.cuda.empty_cache()
+    return {"ensemble_steps_per_s": steps / (ms / 1e3), "members": len(members), "steps": steps,
+            "how": "64 FP64 plans stepped one after another, fixed tile rules, CUDA events"}
 
 
 def rbc_leg(N: int, steps: int, warmup: int):
@@ -593,6 +632,14 @@ def main():
                                      "timing": "wall clock around synchronised graph launches, max over ranks"}
         if world == 1:
             extras["fff1024_f32"] = fff1024_leg()
+            # the plain FP64 GPU path at the same sizes: 1024^3 (2 steps) and the ensemble members
+            # one plan at a time; the north-star target is FP32 / plain FP64 >= 3
+            extras["fff1024_f64_plain"] = fff1024_leg(steps=2, warmup=1, prec="f64", tune=False)
+            extras["ensemble_rbc_64_fp64_plain"] = ensemble_plain_fp64_leg()
+            extras["fp32_over_plain_fp64"] = {
+                "fff1024": extras["fff1024_f32"]["steps_per_s"] / extras["fff1024_f64_plain"]["steps_per_s"],
+                "ensemble": extras["ensemble_rbc_64"]["ensemble_steps_per_s"]
+                / extras["ensemble_rbc_64_fp64_plain"]["ensemble_steps_per_s"]}
             extras["adjoint_128"] = {"f64": adjoint_leg("f64"), "f32": adjoint_leg("f32")}
         if rank == 0 and world == 1:
             v, n, el = cpu_baseline_oracle(N)

@@ -265,10 +265,10 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   if (!cfg || !out) return TS_ERR_ARG;
   *out = nullptr;
   for (int i = 0; i < 3; ++i) {
-    // 48 and 96 (factor 3) are supported for the FP32 SFF path
-    const bool mixed = (cfg->N[i] == 48 || cfg->N[i] == 96) && cfg->basis == TS_BASIS_SFF && cfg->precision == TS_F32;
+    // 48 and 96 (factor 3) are supported for the SFF path
+    const bool mixed = (cfg->N[i] == 48 || cfg->N[i] == 96) && cfg->basis == TS_BASIS_SFF;
     if (!size_supported(cfg->N[i]) && !mixed) {
-      g_last_error = "N must be a power of two in [16, 1024] (48 and 96 also for FP32 SFF)";
+      g_last_error = "N must be a power of two in [16, 1024] (48 and 96 also for SFF)";
       return TS_ERR_ARG;
     }
   }
@@ -1437,7 +1437,7 @@ int ts_plan_autotune(ts_plan* p, int reps, char* report, size_t report_len) {
   const size_t bu = 3 * (size_t)p->g.S * p->cb, bt = (size_t)p->g.S * p->cb;
   void *U = nullptr, *T = nullptr;
   CK(cudaStreamSynchronize(p->st));
-  if (cudaMalloc(&U, bu) != cudaSuccess || cudaMalloc(&T, bt) != cudaSuccess) {
+  if (cudaMalloc(&U, bu) != cudaSuccess || (sff && cudaMalloc(&T, bt) != cudaSuccess)) {
     if (U) cudaFree(U);
     cudaGetLastError();
     return TS_ERR_NOMEM;

@@ -50,11 +50,11 @@ template <typename Fn> bool dispatch_L(int L, Fn&& fn) {
   return false;
 }
 
-// SFF launchers also take the non-power-of-two sizes 48 and 96 (FP32 only):
-// their FFT lengths 3 * 2^k run with 12 elements per thread (radices 4, 2, 3)
+// SFF launchers also take the non-power-of-two sizes 48 and 96: their FFT
+// lengths 3 * 2^k run with 12 elements per thread (radices 4, 2, 3)
 template <typename Fn> bool dispatch_L_sff(int L, Fn&& fn) {
   if (dispatch_L(L, fn)) return true;
-  if constexpr (std::is_same<T, float>::value) {
+  {
     switch (L) {
       case 48: fn(std::integral_constant<int, 48>{}); return true;
       case 96: fn(std::integral_constant<int, 96>{}); return true;
@@ -63,7 +63,9 @@ template <typename Fn> bool dispatch_L_sff(int L, Fn&& fn) {
   return false;
 }
 // elements per thread for a length that may carry a factor 3
-constexpr int e_mixed(int L, int e_pow2) { return L % 3 == 0 ? 12 : (e_pow2 < L ? e_pow2 : L); }
+// (6 where the power-of-two choice is 4 or less: the FP64 SFF forward x kernel
+// holds four accumulators per element and spilled at 12)
+constexpr int e_mixed(int L, int e_pow2) { return L % 3 == 0 ? (e_pow2 >= 8 ? 12 : 6) : (e_pow2 < L ? e_pow2 : L); }
 
 template <typename K> cudaError_t smem_attr(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) {

@@ -46,8 +46,10 @@ struct SffArgs {
 // blocks per SM the SFF x kernels are compiled for: power-of-two lengths (8
 // elements per thread) stay at or under 128 registers per thread (16+ warps per
 // SM); the 12-element mixed-radix variants need the larger register budget
+// (the FP64 6-element mixed-radix forward kernel: 3 blocks of 128 threads, a
+// 170-register budget)
 __host__ __device__ constexpr int sff_min_blocks(int threads, int e) {
-  return e > 8 ? (threads <= 256 ? 2 : 1) : (threads <= 256 ? 512 / threads : 1);
+  return e > 8 ? (threads <= 256 ? 2 : 1) : (e == 6 ? (threads <= 128 ? 3 : 1) : (threads <= 256 ? 512 / threads : 1));
 }
 
 // parity of product field f: true = sine

@@ -24,9 +24,10 @@ def test_member_generator_is_deterministic():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "f64"])
 @pytest.mark.parametrize("N", [(48, 48, 48), (96, 32, 48), (32, 96, 96)])
-def test_mixed_radix_rbc_matches_oracle(cuda, N):
-    """FP32 SFF path at sizes with a factor 3 against the FP64 oracle (relative L2 <= 1e-5)."""
+def test_mixed_radix_rbc_matches_oracle(cuda, N, prec):
+    """SFF path at sizes with a factor 3 against the FP64 oracle (relative L2 <= 1e-5 FP32, 1e-12 FP64)."""
     import torch
     import tarang_b200 as tb
     g = R.Grid(N, KF, "SFF")
@@ -35,16 +36,18 @@ def test_mixed_radix_rbc_matches_oracle(cuda, N):
     U0 = np.stack([R.reality_fix(g, 0.3 * R.forward(g, rng.standard_normal(g.rshape), par[i])) for i in range(3)])
     T0 = R.reality_fix(g, 0.3 * R.forward(g, rng.standard_normal(g.rshape), "S"))
     cfg = R.RBCConfig(g, Ra=1e5, Pr=1.0, dt=1e-3, dealias_mode=1)
-    plan = tb.Plan(N, basis="SFF", precision="f32", kfactor=KF, nu=cfg.nu, kappa=cfg.kappa, dt=1e-3)
-    u = torch.from_numpy(U0.copy()).to(cuda).to(torch.complex64)
-    T = torch.from_numpy(T0.copy()).to(cuda).to(torch.complex64)
+    plan = tb.Plan(N, basis="SFF", precision=prec, kfactor=KF, nu=cfg.nu, kappa=cfg.kappa, dt=1e-3)
+    cdt = torch.complex64 if prec == "f32" else torch.complex128
+    u = torch.from_numpy(U0.copy()).to(cuda).to(cdt)
+    T = torch.from_numpy(T0.copy()).to(cuda).to(cdt)
     Uo, To = U0, T0
     for _ in range(3):
         Uo, To = R.rbc_rk4_step(cfg, Uo, To)
     plan.rk4_step_rbc(u, T, 3)
     torch.cuda.synchronize()
-    assert rel(u.cpu().numpy().astype(np.complex128), Uo) < 1e-5
-    assert rel(T.cpu().numpy().astype(np.complex128), To) < 1e-5
+    tol = 1e-5 if prec == "f32" else 1e-12
+    assert rel(u.cpu().numpy().astype(np.complex128), Uo) < tol
+    assert rel(T.cpu().numpy().astype(np.complex128), To) < tol
 
 
 @pytest.mark.gpu

@@ -77,7 +77,8 @@ def test_fff_candidates_match_oracle(cuda, N, prec, form, dealias):
 
 
 SFF_CASES = [((64, 64, 32), "f32", "two_thirds"), ((48, 48, 48), "f32", "reference"),
-             ((32, 32, 32), "f64", "reference"), ((128, 32, 16), "f32", "reference")]
+             ((32, 32, 32), "f64", "reference"), ((128, 32, 16), "f32", "reference"),
+             ((96, 48, 48), "f64", "reference")]
 
 
 @pytest.mark.parametrize("N,prec,dealias", SFF_CASES)
