@@ -139,6 +139,60 @@ template <int L, int E, int P, bool REV = false> struct Pass {
   }
 };
 
+// Modelled shared-memory wavefronts of the exchanges of one fft_regs<L, E> call on
+// a tile of CW columns (row pitch CW, column = thread % CW, element of WB bytes),
+// with the row swizzle xrow<false, k> (k = 0: none): for every store and load
+// request of the first (up to) four warps, the largest number of threads whose
+// element falls in one bank group of WB bytes (128-byte rows of 32 banks).
+// Rows follow Pass::out_row (stores after pass p) and Pass::in_row (loads for p + 1).
+__host__ __device__ constexpr int xch_wavefronts(int L, int E, int CW, int WB, int k) {
+  const int units = 128 / WB;
+  const int threads = CW * (L / E);
+  const int nw = threads >= 128 ? 4 : (threads + 31) / 32;
+  const int np = npasses(L, E);
+  int R[16] = {}, NS[16] = {};
+  for (int p = 0; p < np && p < 16; ++p) {
+    R[p] = radix_at(L, E, p);
+    NS[p] = p == 0 ? 1 : NS[p - 1] * R[p - 1];
+  }
+  int total = 0;
+  for (int w = 0; w < nw; ++w)
+    for (int p = 0; p + 1 < np; ++p)
+      for (int s = 0; s < E; ++s)
+        for (int side = 0; side < 2; ++side) {
+          int cnt[32] = {};
+          int worst = 0;
+          const int pp = side == 0 ? p : p + 1;
+          const int Rr = R[pp], B = E / Rr;
+          for (int i = 0; i < 32; ++i) {
+            const int tid = w * 32 + i;
+            if (tid >= threads) break;
+            const int t = tid / CW, c = tid % CW;
+            const int j = t * B + s / Rr;
+            int r = side == 0 ? (j / NS[pp]) * NS[pp] * Rr + (j % NS[pp]) + (s % Rr) * NS[pp]
+                              : j + (s % Rr) * (L / Rr);
+            if (k > 0) r ^= (r >> k) & 1;
+            const int g = (r * CW + c) % units;
+            if (++cnt[g] > worst) worst = cnt[g];
+          }
+          total += worst;
+        }
+  return total;
+}
+// the row swizzle with the fewest modelled wavefronts (0 unless it saves at least 5 %)
+__host__ __device__ constexpr int best_swk(int L, int E, int CW, int WB) {
+  const int base = xch_wavefronts(L, E, CW, WB, 0);
+  int best = base, bk = 0;
+  for (int k = 1; k <= 6 && (2 << k) <= L; ++k) {
+    const int v = xch_wavefronts(L, E, CW, WB, k);
+    if (v < best) {
+      best = v;
+      bk = k;
+    }
+  }
+  return 20 * best <= 19 * base ? bk : 0;
+}
+
 // Row of register slot s at load time (first pass input) and after the last pass.
 template <int L, int E, bool REV = false> __device__ __forceinline__ int load_row(int t, int s) {
   return Pass<L, E, 0, REV>::in_row(t, s);

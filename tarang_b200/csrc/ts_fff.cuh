@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     // each thread read back only what it staged itself; the barrier is for the
     // exchange writes into the consumed tile (NT = 2)
     if (NT == 2) __syncthreads();
-    fft_regs<L, E, DIR>(v, t, NT == 2 ? stage + buf * L * CW : stage + 2 * L * CW, CW, c, tw, 1);
+    fft_regs<L, E, DIR, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(
+        v, t, NT == 2 ? stage + buf * L * CW : stage + 2 * L * CW, CW, c, tw, 1);
     if (ok) {
 #pragma unroll
       for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
@@ -191,7 +192,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
         __syncthreads();
         if (threadIdx.x == 0) issue(tile + 2 * gridDim.x, slot);
       }
-      fft_regs<L, E, 1>(v, t, xch, CW, c, tw, 1);
+      fft_regs<L, E, 1, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tw, 1);
       if (ok) {
         V* d = W + f * g.S + col;
 #pragma unroll
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
       }
       v[s] = a;
     }
-    fft_regs<L, E, 1>(v, t, sm, CW, c, tw, 1);
+    fft_regs<L, E, 1, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(v, t, sm, CW, c, tw, 1);
     if (ok) {
       V* d = W + f * g.S + col;
 #pragma unroll
@@ -1086,11 +1087,11 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
       for (int s = 0; s < E; ++s) v[s] = ok ? st[load_row<L, E>(t, s) * CW] : mk<V>(0, 0);
       __syncthreads();
       if (threadIdx.x == 0) issue_item(item + 2);
-      // exchange rows of pitch CW, bit 0 of the row flipped by bit 2 (E = 4) or
-      // bit 1 (E = 8): the first pass stores rows 4 (8) apart from neighbouring
-      // threads, which would share bank pairs; modelled shared-memory wavefronts
-      // 1.0x / 1.25x the minimum, against 2.0x / 1.75x with a padded pitch CW + 1
-      fft_regs<L, E, -1, 0, false, false, (E == 4 ? 2 : 1)>(v, t, xch, CW, c, tw, 1);
+      // exchange rows of pitch CW with the modelled best row swizzle (at 4
+      // elements and 8 columns: bit 0 flipped by bit 2, since the first pass stores
+      // rows 4 apart from neighbouring threads; 1.0x the minimum wavefronts against
+      // 2.0x with the earlier padded pitch CW + 1)
+      fft_regs<L, E, -1, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tw, 1);
 #pragma unroll
       for (int s = 0; s < E; ++s) {
         const int lx = final_row<L, E>(t, s);

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
     }
     __syncthreads();  // every thread has read tile buf: field f + 2 may overwrite it
     issue(f + 2, buf);
-    fft_regs<N, E, 1>(v, t, xch, CW, c, tq, 4);
+    fft_regs<N, E, 1, 0, false, false, best_swk(N, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tq, 4);
     if (ok) {
       V* d = W + f * g.S + col;
 #pragma unroll
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
       if (sine && k >= N / 2) x = scale(x, (T)-1);
       v[s] = x;
     }
-    fft_regs<N, E, -1>(v, t, xch, CW, c, tq, 4);
+    fft_regs<N, E, -1, 0, false, false, best_swk(N, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tq, 4);
 #pragma unroll
     for (int s = 0; s < E; ++s) xch[final_row<N, E>(t, s) * CW + c] = v[s];
     __syncthreads();
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
       }
       v[s] = z;
     }
-    fft_regs<N, E, 1>(v, t, xch, CW, c, tq, 4);
+    fft_regs<N, E, 1, 0, false, false, best_swk(N, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tq, 4);
     if (ok) {
 #pragma unroll
       for (int s = 0; s < E; ++s) {
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
       v[s] = x;
     }
     issue(f + 2, buf);
-    fft_regs<N, E, -1>(v, t, xch, CW, c, tq, 4);
+    fft_regs<N, E, -1, 0, false, false, best_swk(N, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tq, 4);
     // pair terms Z_{N-m} through the exchange tile
 #pragma unroll
     for (int s = 0; s < E; ++s) xch[final_row<N, E>(t, s) * CW + c] = v[s];
