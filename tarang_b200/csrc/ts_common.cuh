@@ -21,6 +21,33 @@ template <typename V> __device__ __forceinline__ V sub(V a, V b) { return mk<V>(
 template <typename V> __device__ __forceinline__ V mul(V a, V b) { return mk<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 template <typename V> __device__ __forceinline__ V conjg(V a) { return mk<V>(a.x, -a.y); }
 template <typename V, typename S> __device__ __forceinline__ V scale(V a, S s) { return mk<V>(a.x * s, a.y * s); }
+
+// FP32 complex add / sub / real scale as one paired instruction (add / sub / mul
+// .rn.f32x2, sm_100): each lane rounds exactly as the scalar operation, so the
+// results are unchanged while the FFT butterflies (mostly adds) issue half the
+// floating-point instructions
+#define TS_F32X2(OP)                                                                           \
+  asm("{\n\t.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t" OP \
+      ".rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n\t}"                                  \
+      : "=f"(r.x), "=f"(r.y)                                                                   \
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y))
+template <> __device__ __forceinline__ float2 add<float2>(float2 a, float2 b) {
+  float2 r;
+  TS_F32X2("add");
+  return r;
+}
+template <> __device__ __forceinline__ float2 sub<float2>(float2 a, float2 b) {
+  float2 r;
+  TS_F32X2("sub");
+  return r;
+}
+template <> __device__ __forceinline__ float2 scale<float2, float>(float2 a, float s) {
+  float2 r;
+  const float2 b = make_float2(s, s);
+  TS_F32X2("mul");
+  return r;
+}
+#undef TS_F32X2
 // multiply by +i (SIGN=+1) or -i (SIGN=-1)
 template <int SIGN, typename V> __device__ __forceinline__ V mul_i(V a) {
   return SIGN > 0 ? mk<V>(-a.y, a.x) : mk<V>(a.y, -a.x);

@@ -558,10 +558,11 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
 }
 
 // blocks per SM the register z kernel is compiled for: 6 (170 registers), 3 for
-// the 12-element radix-3 lines (which would spill at 170)
+// the 12-element radix-3 lines (which would spill at 170), 4 for 512-point lines
+// (two warps per line, the pair terms through the exchange line; spilled at 170)
 // (8 for the 4-element variant)
 template <int NZ, int EZ = 0> __host__ __device__ constexpr int zreg_min_blocks() {
-  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : 6);
+  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : (NZ >= 1024 ? 4 : 6));
 }
 
 // EZ = 0: 8 elements per thread, 12 for a line length with a factor 3 (radices
