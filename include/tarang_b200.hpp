@@ -191,9 +191,12 @@ class FluidSF {
 struct Time_advance_incompress {
   // RK4(U,P,F) + strong reality condition when the plan enables it (RK.cc:91-170, Time_advance.cc:59-60)
   static void RK4(FluidVF& U, int nsteps = 1) { check(ts_rk4_step(U.basis().plan(), U.cvf(), nsteps), "RK4"); }
-  // RK4(U,T,P,F) for RBC on the SFF basis (RK_SF.cc:97), PRLARGE / ULARGE
+  // RK4(U,T,P,F) (RK_SF.cc:97): RBC on the SFF basis (PRLARGE / ULARGE), or a
+  // passive scalar (kind INC_SCALAR, no force) on the FFF basis
   static void RK4(FluidVF& U, FluidSF& T, int nsteps = 1) {
-    check(ts_rk4_step_rbc(U.basis().plan(), U.cvf(), T.csf(), nsteps), "RK4");
+    ts_plan* p = U.basis().plan();
+    if (U.basis().config().basis == TS_BASIS_SFF) check(ts_rk4_step_rbc(p, U.cvf(), T.csf(), nsteps), "RK4");
+    else check(ts_rk4_step_scalar(p, U.cvf(), T.csf(), nsteps), "RK4");
   }
 };
 

@@ -762,17 +762,32 @@ class RBCConfig:
         return 1.0 / math.sqrt(self.Pr * self.Ra)
 
 
-def rbc_rhs(cfg: RBCConfig, U: np.ndarray, T: np.ndarray) -> tuple:
-    """Compute_force_TO_rhs_RBC (Tadvance_functions.cc:477-489), PRLARGE / ULARGE.
+@dataclass
+class ScalarConfig:
+    """Incompressible flow with a passive scalar (program.kind INC_SCALAR), no force."""
+    grid: Grid
+    nu: float
+    kappa: float
+    dt: float
+    dealias_mode: int = DEALIAS_REFERENCE_CORNER
+    reality_fix: bool = True
+    buoyancy = False
+
+
+def rbc_rhs(cfg, U: np.ndarray, T: np.ndarray) -> tuple:
+    """Compute_force_TO_rhs_RBC (Tadvance_functions.cc:477-489), PRLARGE / ULARGE, or
+    Compute_force_TO_rhs_scalar (Tadvance_functions.cc:464-474) for a ScalarConfig.
 
     Force (compute_force_RBC.cc:104-150): U.F1 = T, T.F = U.V1 (both from the
-    un-dealiased stage input).  Nonlinear: dealias U, T; T.nlin = sum_j D_j F[u_j T]
+    un-dealiased stage input); none for the passive scalar.  Nonlinear
+    (compute_nlin_SF.cc:75-112): dealias U, T; T.nlin = sum_j D_j F[u_j T]
     (compute_diag_offdiag.cc:116-136 with FVx/FVy/FVz parities) and the velocity
     nlin; nlin -= F; pressure; rhs = -(nlin + grad p), T.rhs = -T.nlin.
     """
     g = cfg.grid
-    FU1 = T.copy()
-    FT = U[0].copy()
+    buoyancy = getattr(cfg, "buoyancy", True)
+    FU1 = T.copy() if buoyancy else np.zeros_like(T)
+    FT = U[0].copy() if buoyancy else np.zeros_like(T)
     Ud = dealias(g, U, cfg.dealias_mode)
     Td = dealias(g, T, cfg.dealias_mode)
     ur = velocity_real(g, Ud)
@@ -787,8 +802,9 @@ def rbc_rhs(cfg: RBCConfig, U: np.ndarray, T: np.ndarray) -> tuple:
     return project_rhs(g, N), -Tn, Ud, Td
 
 
-def rbc_rk4_step(cfg: RBCConfig, U0: np.ndarray, T0: np.ndarray) -> tuple:
-    """RK4(U,T,P,F) RK_SF.cc:97-221 with Single_time_step_scalar (U with nu, T with kappa)."""
+def rbc_rk4_step(cfg, U0: np.ndarray, T0: np.ndarray) -> tuple:
+    """RK4(U,T,P,F) RK_SF.cc:97-221 with Single_time_step_scalar (U with nu, T with kappa);
+    an RBCConfig (SFF, buoyancy) or a ScalarConfig (passive scalar, any basis)."""
     g = cfg.grid
     dt = cfg.dt
     EU = lambda A, a: exp_ksqr(g, A, -cfg.nu * a * dt)

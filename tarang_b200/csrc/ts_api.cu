@@ -49,6 +49,7 @@ struct ts_plan {
   void* tot = nullptr;
   void* P = nullptr;  // nP components of transform / product work fields
   int nP = 0;
+  int nS = 0;         // components of the stage field Ucur and the accumulator tot
   void* twx = nullptr;
   void* twy = nullptr;
   void* twz = nullptr;
@@ -317,6 +318,7 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   CKP(alloc(&p->tot, ncs * g.S * p->cb));
   CKP(alloc(&p->P, nps * g.S * p->cb));
   p->nP = nps;
+  p->nS = ncs;
   if (p->prec) {
     CKP(upload_twiddles<float>(g.Nx, &p->twx));
     CKP(upload_twiddles<float>(g.Ny, &p->twy));
@@ -372,8 +374,9 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   }
   *p->err_h = 0;
   CKP(upload_if_tables(p, cfg->nu, cfg->dt, p->eax));
+  // the scalar's factors: the SFF Boussinesq step and the FFF passive-scalar step
+  CKP(upload_if_tables(p, cfg->kappa, cfg->dt, p->eaxT));
   if (cfg->basis == TS_BASIS_SFF) {
-    CKP(upload_if_tables(p, cfg->kappa, cfg->dt, p->eaxT));
     if (p->prec) CKP(upload_twiddles<float>(4 * g.Nx, &p->twq));
     else CKP(upload_twiddles<double>(4 * g.Nx, &p->twq));
   }
@@ -418,7 +421,7 @@ int ts_plan_set_dt(ts_plan* p, double dt) {
   CK(cudaStreamSynchronize(p->st));
   p->cfg.dt = dt;
   CKS(upload_if_tables(p, p->cfg.nu, dt, p->eax));
-  if (p->cfg.basis == TS_BASIS_SFF) CKS(upload_if_tables(p, p->cfg.kappa, dt, p->eaxT));
+  CKS(upload_if_tables(p, p->cfg.kappa, dt, p->eaxT));
   return TS_OK;
 }
 
@@ -596,6 +599,88 @@ static int step_rbc(ts_plan* p, void* U0, void* T0) {
   return TS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// FFF passive scalar (program.kind INC_SCALAR): RK4(U,T,P,F) with no force
+// ---------------------------------------------------------------------------
+static int scalar_supported(ts_plan* p) {
+  if (p->cfg.basis != TS_BASIS_FFF || p->cfg.force_type != TS_FORCE_NONE ||
+      p->cfg.nlin_form != TS_NLIN_CONSERVATIVE) {
+    g_last_error = "the passive-scalar step is implemented for FFF, conservative form, unforced plans";
+    return TS_ERR_UNSUPPORTED;
+  }
+  // stage and accumulator fields carry T as a fourth component; the z pass makes nine products
+  if (p->nS < 4 || p->nP < 9) {
+    CK(cudaStreamSynchronize(p->st));
+    if (p->nS < 4) {
+      CK(cudaFree(p->Ucur));
+      CK(cudaFree(p->tot));
+      p->Ucur = p->tot = nullptr;
+      p->nS = 0;
+      CK(cudaMalloc(&p->Ucur, 4 * p->g.S * p->cb));
+      CK(cudaMalloc(&p->tot, 4 * p->g.S * p->cb));
+      p->nS = 4;
+    }
+    if (p->nP < 9) {
+      CK(cudaFree(p->P));
+      p->P = nullptr;
+      p->nP = 0;
+      CK(cudaMalloc(&p->P, 9 * p->g.S * p->cb));
+      p->nP = 9;
+    }
+  }
+  return TS_OK;
+}
+
+// one IF-RK4 step of U and the passive scalar T on the FFF basis (RK_SF.cc:97-221 with
+// Compute_force_TO_rhs_scalar, Tadvance_functions.cc:464-474, and Compute_nlin_scalar,
+// compute_nlin_SF.cc:75-112): dealiased u, T to real space, the nine products u_i u_j and
+// u_i T (z pass form 2), forward transforms, then N, NT, the projection and the stage update
+static int step_scalar_fff(ts_plan* p, void* U0, void* T0) {
+  const Geo& g = p->g;
+  SffArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.T0 = T0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.dt = p->cfg.dt;
+  a.reality = p->cfg.reality_fix;
+  for (int i = 0; i < 3; ++i) {
+    a.eu[i] = p->eax[i];
+    a.et[i] = p->eaxT[i];
+  }
+  const long long cb = (long long)p->cb;
+  const int kept = g.dealias == TS_DEALIAS_TWO_THIRDS;
+  void* P3 = (char*)p->P + 3 * g.S * cb;
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? U0 : p->Ucur;
+    const void* Tin = stage == 1 ? T0 : (const void*)((const char*)p->Ucur + 3 * g.S * cb);
+    a.stage = stage;
+    a.U1in = Uin;
+    a.Tin = Tin;
+    {
+      ProfScope ps(p, TS_KCLASS_INV_X);
+      CK(LAUNCH(p, inv_x, g, 0, Uin, p->P, p->twx, nullptr, 0.0, p->st, kept));
+      CK(LAUNCH(p, dealias_copy, g, Tin, P3, 1, p->st));
+      CK(LAUNCH(p, strided, g, 0, +1, P3, 1, p->twx, p->st));
+    }
+    { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, 4, p->twy, p->st, 0, 0, kept ? g.Nz / 3 + 1 : 0, kept)); }
+    { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, 2, p->P, p->twz, p->err_d, p->st, 1, 0, kept ? g.Nz / 3 : -1)); }
+    { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, 9, p->twy, p->st)); }
+    {
+      ProfScope ps(p, TS_KCLASS_FWD_X);
+      CK(LAUNCH(p, strided, g, 0, -1, p->P, 9, p->twx, p->st));
+      CK(LAUNCH(p, scalar_epi, g, p->P, a, p->st));
+    }
+  }
+  if (p->cfg.reality_fix) {
+    ProfScope ps(p, TS_KCLASS_OTHER);
+    CK(LAUNCH(p, reality, g, U0, 3, p->st));
+    CK(LAUNCH(p, reality, g, T0, 1, p->st));
+  }
+  return TS_OK;
+}
+
 // run fn(device_ptr) on a field that may live on the host
 template <typename Fn>
 static int with_device(ts_plan* p, void** stage, const void* ptr, size_t bytes, bool copy_back, Fn&& fn) {
@@ -709,6 +794,24 @@ int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
     return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
       for (int s = 0; s < nsteps; ++s) CKS(step_rbc(p, U, T));
+      return (int)TS_OK;
+    });
+  });
+  if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return rc;
+}
+
+int ts_rk4_step_scalar(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
+  if (!p || !u_hat || !T_hat || nsteps < 0) return TS_ERR_ARG;
+  CKS(scalar_supported(p));
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up";
+    return TS_ERR_TIMEOUT;
+  }
+  const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
+  int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
+    return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
+      for (int s = 0; s < nsteps; ++s) CKS(step_scalar_fff(p, U, T));
       return (int)TS_OK;
     });
   });

@@ -649,6 +649,12 @@ template <> cudaError_t Launch<T>::scale(void* A, long long n, double s, cudaStr
   return cudaGetLastError();
 }
 
+template <> cudaError_t Launch<T>::scalar_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st) {
+  k_scalar_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
 template <> cudaError_t Launch<T>::dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st) {
   k_dealias_copy<T><<<grid1d(g.S * ncomp, 256), 256, 0, st>>>((const V*)A, (V*)B, ncomp, g);
   ++g_launches;

@@ -42,6 +42,8 @@ template <typename T> struct Launch {
   // standalone sin/cos x transform of ncomp components in place (dir -1 forward with scale scl, +1 inverse)
   static cudaError_t sff_x(const Geo& g, int dir, void* A, int ncomp, int sine, double scl, const void* tq,
                            cudaStream_t st);
+  // FFF passive scalar: elementwise epilogue of the nine x-transformed products in P
+  static cudaError_t scalar_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,

@@ -395,4 +395,73 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
   }
 }
 
+// ---------------------------------------------------------------------------
+// FFF passive scalar (program.kind INC_SCALAR), elementwise epilogue after the
+// forward x FFT of the nine products of form 2 (u1u1, u2u2, u3u3, u1u2, u2u3,
+// u3u1, u1T, u2T, u3T; unnormalised):
+//   N_i = sum_j i K_j F[u_j u_i]  (compute_diag_offdiag.cc:47-98, conservative)
+//   NT  = sum_j i K_j F[u_j T]    (compute_diag_offdiag.cc:116-136)
+//   no force (Add_force with F = 0); p = (i K . N)/K^2, N <- N + i K p; R = -N,
+//   RT = -NT; IF-RK4 stage update of U (nu) and T (kappa) as the Boussinesq
+//   epilogue (RK_SF.cc:97-221).  One thread per element, every access coalesced.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, Geo g, SffArgs a) {
+  typedef C<T> V;
+  const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
+  const V* U0 = reinterpret_cast<const V*>(a.U0);
+  const V* T0 = reinterpret_cast<const V*>(a.T0);
+  V* Uc = reinterpret_cast<V*>(a.Ucur);
+  V* tot = reinterpret_cast<V*>(a.tot);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const double Kxd = kfft(lx, g.Nx) * g.kf[0], Kyd = kfft(ly, g.Ny) * g.kf[1], Kzd = lz * g.kf[2];
+    const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+    V p[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) p[f] = scale(P[f * g.S + e], inv);
+    // x, then y, then z derivative terms, as the reference accumulates them
+    V N1 = add(add(ik(Kx, p[0]), ik(Ky, p[3])), ik(Kz, p[5]));
+    V N2 = add(add(ik(Kx, p[3]), ik(Ky, p[1])), ik(Kz, p[4]));
+    V N3 = add(add(ik(Kx, p[5]), ik(Ky, p[4])), ik(Kz, p[2]));
+    const V NT = add(add(ik(Kx, p[6]), ik(Ky, p[7])), ik(Kz, p[8]));
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    const V div = add(add(ik(Kx, N1), ik(Ky, N2)), ik(Kz, N3));
+    const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+    N1 = add(N1, ik(Kx, pr));
+    N2 = add(N2, ik(Ky, pr));
+    N3 = add(N3, ik(Kz, pr));
+    const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
+    const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lz];
+    const double eht = a.et[0][lx] * a.et[1][ly] * a.et[2][lz];
+    const bool dz = dealias_zero(g.dealias, 0, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double eh = i < 3 ? ehu : eht;
+      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const long long o = i * g.S + e;
+      const V R = Rv[i];
+      const V u0 = i < 3 ? U0[o] : T0[e];
+      if (a.stage == 1) {
+        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+      } else if (a.stage == 2) {
+        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else if (a.stage == 3) {
+        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else {
+        V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
+        if (i < 3) const_cast<V*>(U0)[o] = un;
+        else const_cast<V*>(T0)[e] = un;
+      }
+    }
+  }
+}
+
 }  // namespace ts
