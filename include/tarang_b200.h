@@ -119,6 +119,12 @@ int ts_rk4_step_rbc(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
  * plan, conservative form: U with nu, T with kappa; T_hat one component in the
  * state layout.  Replaces that RK4 call for kind INC_SCALAR. */
 int ts_rk4_step_scalar(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
+/* Time_advance_incompress::RK4(U, W, P, F) for incompressible MHD (RK_VF_MHD.cc:126-186,
+ * Compute_nlin(U, W) compute_nlin_VF_MHD.cc:40-95 in Elsasser form) + the strong
+ * reality condition on U and B (Time_advance.cc:126-129), FFF plan, no force:
+ * U with nu, B = W with eta = the plan's kappa (diss_coefficients[1]); b_hat three
+ * components in the state layout. */
+int ts_rk4_step_mhd(ts_plan* plan, void* u_hat, void* b_hat, int nsteps);
 
 /* Temperature perturbation for RBC (SFF): amplitude amp and uniform random
  * phases (this project's splitmix64 generator, counter = linear mode index) on

@@ -191,6 +191,11 @@ class FluidSF {
 struct Time_advance_incompress {
   // RK4(U,P,F) + strong reality condition when the plan enables it (RK.cc:91-170, Time_advance.cc:59-60)
   static void RK4(FluidVF& U, int nsteps = 1) { check(ts_rk4_step(U.basis().plan(), U.cvf(), nsteps), "RK4"); }
+  // RK4(U,W,P,F) for incompressible MHD (RK_VF_MHD.cc:126), W = B, FFF, no force;
+  // eta = the basis config's kappa
+  static void RK4(FluidVF& U, FluidVF& W, int nsteps = 1) {
+    check(ts_rk4_step_mhd(U.basis().plan(), U.cvf(), W.cvf(), nsteps), "RK4");
+  }
   // RK4(U,T,P,F) (RK_SF.cc:97): RBC on the SFF basis (PRLARGE / ULARGE), or a
   // passive scalar (kind INC_SCALAR, no force) on the FFF basis
   static void RK4(FluidVF& U, FluidSF& T, int nsteps = 1) {

@@ -835,6 +835,89 @@ def rbc_rk4_step(cfg, U0: np.ndarray, T0: np.ndarray) -> tuple:
     return U, T
 
 
+# ----------------------------------------------------------------------------
+# incompressible MHD (FFF): RK4(U, W, P, F) with W = B, no force
+# ----------------------------------------------------------------------------
+@dataclass
+class MHDConfig:
+    grid: Grid
+    nu: float
+    eta: float
+    dt: float
+    dealias_mode: int = DEALIAS_REFERENCE_CORNER
+    reality_fix: bool = True
+
+
+def mhd_nlin(g: Grid, U: np.ndarray, B: np.ndarray) -> tuple:
+    """Nlin_incompress::Compute_nlin(U, W) (compute_nlin_VF_MHD.cc:40-95) on dealiased
+    fields: Elsasser real fields Zp = u + b, Zm = u - b (MHD.cc:75-84); diagonal terms
+    Zp.nlin_i = Zm.nlin_i = D_i F[Zp_i Zm_i] (compute_diag_offdiag.cc:139-164), then
+    the six off-diagonal products in the reference's order (:202-258), so that
+    Zp.nlin_i = sum_j D_j F[Zp_i Zm_j] and Zm.nlin_i = sum_j D_j F[Zp_j Zm_i];
+    U.nlin = (Zp.nlin + Zm.nlin)/2, B.nlin = (Zp.nlin - Zm.nlin)/2 (MHD.cc:150-161)."""
+    u = [inverse(g, U[i]) for i in range(3)]
+    b = [inverse(g, B[i]) for i in range(3)]
+    zp = [u[i] + b[i] for i in range(3)]
+    zm = [u[i] - b[i] for i in range(3)]
+    D = [lambda A: xderiv(g, A), lambda A: yderiv(g, A), lambda A: zderiv(g, A)]
+    P = lambda i, j: forward(g, zp[i] * zm[j])
+    npl = [D[i](P(i, i)) for i in range(3)]
+    nmi = [a.copy() for a in npl]
+    X = P(0, 1); npl[0] = npl[0] + D[1](X); nmi[1] = nmi[1] + D[0](X)
+    X = P(1, 0); nmi[0] = nmi[0] + D[1](X); npl[1] = npl[1] + D[0](X)
+    X = P(1, 2); npl[1] = npl[1] + D[2](X); nmi[2] = nmi[2] + D[1](X)
+    X = P(2, 1); nmi[1] = nmi[1] + D[2](X); npl[2] = npl[2] + D[1](X)
+    X = P(2, 0); nmi[0] = nmi[0] + D[2](X); npl[2] = npl[2] + D[0](X)
+    X = P(0, 2); npl[0] = npl[0] + D[2](X); nmi[2] = nmi[2] + D[0](X)
+    NU = np.stack([0.5 * (npl[i] + nmi[i]) for i in range(3)])
+    NB = np.stack([0.5 * (npl[i] - nmi[i]) for i in range(3)])
+    return NU, NB
+
+
+def mhd_rhs(cfg: MHDConfig, U: np.ndarray, B: np.ndarray) -> tuple:
+    """Compute_force_TO_rhs(U, W, P, F) (Tadvance_functions.cc:506-517) with no force:
+    dealias U, B in place, nlin, pressure from U.nlin, U.rhs = -(U.nlin + D p),
+    W.rhs = -W.nlin (Compute_rhs(U, W, P), :259-267)."""
+    g = cfg.grid
+    Ud = dealias(g, U, cfg.dealias_mode) if cfg.dealias_mode else U.copy()
+    Bd = dealias(g, B, cfg.dealias_mode) if cfg.dealias_mode else B.copy()
+    NU, NB = mhd_nlin(g, Ud, Bd)
+    return project_rhs(g, NU), -NB, Ud, Bd
+
+
+def mhd_rk4_step(cfg: MHDConfig, U0: np.ndarray, B0: np.ndarray) -> tuple:
+    """RK4(U, W, P, F) (RK_VF_MHD.cc:126-186): the fluid RK4 stages for U (nu) and
+    W = B (eta), then the strong reality condition on both (Time_advance.cc:126-129)."""
+    g = cfg.grid
+    dt = cfg.dt
+    EU = lambda A, a: exp_ksqr(g, A, -cfg.nu * a * dt)
+    EB = lambda A, a: exp_ksqr(g, A, -cfg.eta * a * dt)
+    R, S, Ud, Bd = mhd_rhs(cfg, U0, B0)
+    U = EU(Ud + 0.5 * dt * R, 0.5)
+    B = EB(Bd + 0.5 * dt * S, 0.5)
+    totU = (dt / 6) * EU(R, 1.0)
+    totB = (dt / 6) * EB(S, 1.0)
+    R, S, _, _ = mhd_rhs(cfg, U, B)
+    U = EU(U0, 0.5) + 0.5 * dt * R
+    B = EB(B0, 0.5) + 0.5 * dt * S
+    totU = totU + (dt / 3) * EU(R, 0.5)
+    totB = totB + (dt / 3) * EB(S, 0.5)
+    R, S, _, _ = mhd_rhs(cfg, U, B)
+    U = EU(EU(U0, 0.5) + dt * R, 0.5)
+    B = EB(EB(B0, 0.5) + dt * S, 0.5)
+    totU = totU + (dt / 3) * EU(R, 0.5)
+    totB = totB + (dt / 3) * EB(S, 0.5)
+    R, S, _, _ = mhd_rhs(cfg, U, B)
+    totU = totU + (dt / 6) * R
+    totB = totB + (dt / 6) * S
+    U = EU(U0, 1.0) + totU
+    B = EB(B0, 1.0) + totB
+    if cfg.reality_fix:
+        U = reality_fix_vec(g, U)
+        B = reality_fix_vec(g, B)
+    return U, B
+
+
 def nusselt(cfg: RBCConfig, U: np.ndarray, T: np.ndarray) -> float:
     """Get_Nusselt_no PRLARGE/ULARGE (Correlation.cc:154-156): 1 + 2 sqrt(Ra Pr) <U1, T>."""
     return 1.0 + 2.0 * math.sqrt(cfg.Ra * cfg.Pr) * cross_energy(cfg.grid, U[0], T)

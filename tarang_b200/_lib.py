@@ -91,6 +91,7 @@ SIGNATURES = {
     "ts_ensemble_synchronize": (ctypes.c_int, [_P]),
     "ts_ensemble_nusselt": (ctypes.c_int, [_P, _D]),
     "ts_rk4_step_scalar": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
+    "ts_rk4_step_mhd": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
     "ts_rk4_step_keep": (ctypes.c_int, [_P, _P, _P, _P]),
     "ts_adjoint_step": (ctypes.c_int, [_P, _P, _P, _P]),
     "ts_adjoint_work_bytes": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),

@@ -65,6 +65,7 @@ struct ts_plan {
   size_t dscr_n = 0;
   void* stage_u = nullptr;  // staging for host pointers (3 components)
   void* stage_t = nullptr;  // staging for host pointers (1 component)
+  void* stage_b = nullptr;  // staging for host pointers (3 components, the MHD field B)
   int* err_d = nullptr;     // device error word (bounded waits that gave up)
   int* err_h = nullptr;     // pinned copy, refreshed after every step call
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
@@ -247,7 +248,7 @@ const char* ts_last_error(void) { return g_last_error.c_str(); }
 int ts_plan_destroy(ts_plan* p) {
   if (!p) return TS_ERR_ARG;
   void* bufs[] = {p->Ucur, p->tot, p->P, p->twx, p->twy, p->twz, p->fcube, p->esup, p->hsup, p->mis_d, p->dscr,
-                  p->stage_u, p->stage_t};
+                  p->stage_u, p->stage_t, p->stage_b};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
@@ -602,6 +603,8 @@ static int step_rbc(ts_plan* p, void* U0, void* T0) {
 // ---------------------------------------------------------------------------
 // FFF passive scalar (program.kind INC_SCALAR): RK4(U,T,P,F) with no force
 // ---------------------------------------------------------------------------
+static int ensure_work(ts_plan* p, int nstage, int nprod);
+
 static int scalar_supported(ts_plan* p) {
   if (p->cfg.basis != TS_BASIS_FFF || p->cfg.force_type != TS_FORCE_NONE ||
       p->cfg.nlin_form != TS_NLIN_CONSERVATIVE) {
@@ -609,26 +612,7 @@ static int scalar_supported(ts_plan* p) {
     return TS_ERR_UNSUPPORTED;
   }
   // stage and accumulator fields carry T as a fourth component; the z pass makes nine products
-  if (p->nS < 4 || p->nP < 9) {
-    CK(cudaStreamSynchronize(p->st));
-    if (p->nS < 4) {
-      CK(cudaFree(p->Ucur));
-      CK(cudaFree(p->tot));
-      p->Ucur = p->tot = nullptr;
-      p->nS = 0;
-      CK(cudaMalloc(&p->Ucur, 4 * p->g.S * p->cb));
-      CK(cudaMalloc(&p->tot, 4 * p->g.S * p->cb));
-      p->nS = 4;
-    }
-    if (p->nP < 9) {
-      CK(cudaFree(p->P));
-      p->P = nullptr;
-      p->nP = 0;
-      CK(cudaMalloc(&p->P, 9 * p->g.S * p->cb));
-      p->nP = 9;
-    }
-  }
-  return TS_OK;
+  return ensure_work(p, 4, 9);
 }
 
 // one IF-RK4 step of U and the passive scalar T on the FFF basis (RK_SF.cc:97-221 with
@@ -677,6 +661,87 @@ static int step_scalar_fff(ts_plan* p, void* U0, void* T0) {
     ProfScope ps(p, TS_KCLASS_OTHER);
     CK(LAUNCH(p, reality, g, U0, 3, p->st));
     CK(LAUNCH(p, reality, g, T0, 1, p->st));
+  }
+  return TS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FFF incompressible MHD: RK4(U, W, P, F) with W = B, no force
+// ---------------------------------------------------------------------------
+static int ensure_work(ts_plan* p, int nstage, int nprod) {
+  if (p->nS >= nstage && p->nP >= nprod) return TS_OK;
+  CK(cudaStreamSynchronize(p->st));
+  if (p->nS < nstage) {
+    CK(cudaFree(p->Ucur));
+    CK(cudaFree(p->tot));
+    p->Ucur = p->tot = nullptr;
+    p->nS = 0;
+    CK(cudaMalloc(&p->Ucur, nstage * p->g.S * p->cb));
+    CK(cudaMalloc(&p->tot, nstage * p->g.S * p->cb));
+    p->nS = nstage;
+  }
+  if (p->nP < nprod) {
+    CK(cudaFree(p->P));
+    p->P = nullptr;
+    p->nP = 0;
+    CK(cudaMalloc(&p->P, nprod * p->g.S * p->cb));
+    p->nP = nprod;
+  }
+  return TS_OK;
+}
+
+static int mhd_supported(ts_plan* p) {
+  if (p->cfg.basis != TS_BASIS_FFF || p->cfg.force_type != TS_FORCE_NONE) {
+    g_last_error = "the MHD step is implemented for FFF, unforced plans";
+    return TS_ERR_UNSUPPORTED;
+  }
+  // stage and accumulator fields carry U and B (6 components); nine Elsasser products
+  return ensure_work(p, 6, 9);
+}
+
+// one IF-RK4 step of U (nu) and B (eta = the plan's kappa) (RK_VF_MHD.cc:126-186,
+// Compute_force_TO_rhs Tadvance_functions.cc:506-517, Compute_nlin(U, W)
+// compute_nlin_VF_MHD.cc:40-95): dealiased u, b to real space, the nine Elsasser
+// products Zp_i Zm_j (z pass form 5), forward transforms, then the MHD epilogue
+static int step_mhd_fff(ts_plan* p, void* U0, void* B0) {
+  const Geo& g = p->g;
+  SffArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.T0 = B0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.dt = p->cfg.dt;
+  a.reality = p->cfg.reality_fix;
+  for (int i = 0; i < 3; ++i) {
+    a.eu[i] = p->eax[i];
+    a.et[i] = p->eaxT[i];
+  }
+  const long long cs = 3 * g.S * (long long)p->cb;
+  const int kept = g.dealias == TS_DEALIAS_TWO_THIRDS;
+  void* P3 = (char*)p->P + cs;
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? U0 : p->Ucur;
+    const void* Bin = stage == 1 ? B0 : (const void*)((const char*)p->Ucur + cs);
+    a.stage = stage;
+    {
+      ProfScope ps(p, TS_KCLASS_INV_X);
+      CK(LAUNCH(p, inv_x, g, 0, Uin, p->P, p->twx, nullptr, 0.0, p->st, kept));
+      CK(LAUNCH(p, inv_x, g, 0, Bin, P3, p->twx, nullptr, 0.0, p->st, kept));
+    }
+    { ProfScope ps(p, TS_KCLASS_Y_INV); CK(LAUNCH(p, strided, g, 1, +1, p->P, 6, p->twy, p->st, 0, 0, kept ? g.Nz / 3 + 1 : 0, kept)); }
+    { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, 5, p->P, p->twz, p->err_d, p->st, 1, 0, kept ? g.Nz / 3 : -1)); }
+    { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, 9, p->twy, p->st)); }
+    {
+      ProfScope ps(p, TS_KCLASS_FWD_X);
+      CK(LAUNCH(p, strided, g, 0, -1, p->P, 9, p->twx, p->st));
+      CK(LAUNCH(p, mhd_epi, g, p->P, a, p->st));
+    }
+  }
+  if (p->cfg.reality_fix) {
+    ProfScope ps(p, TS_KCLASS_OTHER);
+    CK(LAUNCH(p, reality, g, U0, 3, p->st));
+    CK(LAUNCH(p, reality, g, B0, 3, p->st));
   }
   return TS_OK;
 }
@@ -812,6 +877,24 @@ int ts_rk4_step_scalar(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
     return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
       for (int s = 0; s < nsteps; ++s) CKS(step_scalar_fff(p, U, T));
+      return (int)TS_OK;
+    });
+  });
+  if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+  return rc;
+}
+
+int ts_rk4_step_mhd(ts_plan* p, void* u_hat, void* b_hat, int nsteps) {
+  if (!p || !u_hat || !b_hat || nsteps < 0) return TS_ERR_ARG;
+  CKS(mhd_supported(p));
+  if (*p->err_h) {
+    g_last_error = "a bounded device wait gave up";
+    return TS_ERR_TIMEOUT;
+  }
+  const size_t bu = 3 * p->g.S * p->cb;
+  int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
+    return with_device(p, &p->stage_b, b_hat, bu, true, [&](void* B) -> int {
+      for (int s = 0; s < nsteps; ++s) CKS(step_mhd_fff(p, U, B));
       return (int)TS_OK;
     });
   });

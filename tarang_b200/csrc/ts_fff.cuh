@@ -337,8 +337,14 @@ template <int M> __host__ __device__ constexpr int zslot() { return M + M / 16 +
 // FORM 2 (Boussinesq):    in u1,u2,u3,T     -> the six u_i u_j, then u1T,u2T,u3T
 //                         (compute_diag_offdiag.cc:47-136)
 // FORM 3 (adjoint of the rotational form): in u, w, mu -> mu x u, then w x mu
-__host__ __device__ constexpr int z_nin(int form) { return form == 0 ? 3 : (form == 1 ? 6 : (form == 2 ? 4 : 9)); }
-__host__ __device__ constexpr int z_nout(int form) { return form == 0 ? 6 : (form == 1 ? 3 : (form == 2 ? 9 : 6)); }
+// FORM 5 (MHD):           in u1..3, b1..3      -> Zp_i Zm_j (f = 3 i + j), Zp = u + b, Zm = u - b
+//                         (compute_nlin_VF_MHD.cc:40-95, MHD.cc:75-84)
+__host__ __device__ constexpr int z_nin(int form) {
+  return form == 0 ? 3 : (form == 1 ? 6 : (form == 2 ? 4 : (form == 5 ? 6 : 9)));
+}
+__host__ __device__ constexpr int z_nout(int form) {
+  return form == 0 ? 6 : (form == 1 ? 3 : (form == 2 ? 9 : (form == 5 ? 9 : 6)));
+}
 
 // component f of a x b for real points packed two per complex (re, im independent)
 template <typename V> __device__ __forceinline__ V cross_pk(int f, const V* a, const V* b) {
@@ -346,8 +352,24 @@ template <typename V> __device__ __forceinline__ V cross_pk(int f, const V* a, c
   return mk<V>(a[i].x * b[j].x - a[j].x * b[i].x, a[i].y * b[j].y - a[j].y * b[i].y);
 }
 // factor indices (a, b) of product output f for FORM 0 / 2
-__host__ __device__ constexpr int z_pa(int f) { return f < 3 ? f : (f < 6 ? f - 3 : f - 6); }
-__host__ __device__ constexpr int z_pb(int f) { return f < 3 ? f : (f < 6 ? (f == 5 ? 0 : f - 2) : 3); }
+__host__ __device__ constexpr int z_pa(int f, int form = 0) {
+  return form == 5 ? f / 3 : (f < 3 ? f : (f < 6 ? f - 3 : f - 6));
+}
+__host__ __device__ constexpr int z_pb(int f, int form = 0) {
+  return form == 5 ? 3 + f % 3 : (f < 3 ? f : (f < 6 ? (f == 5 ? 0 : f - 2) : 3));
+}
+// FORM 5: the real lines of u and b (packed two points per complex) become the
+// Elsasser lines Zp = u + b, Zm = u - b in place
+template <int FORM, typename V> __device__ __forceinline__ void z_elsasser(V* in) {
+  if constexpr (FORM == 5) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const V u = in[c], b = in[c + 3];
+      in[c] = add(u, b);
+      in[c + 3] = sub(u, b);
+    }
+  }
+}
 
 template <typename T, int NZ, int E, int FORM>
 __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, int nl,
@@ -394,6 +416,7 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
     V in[NIN];
 #pragma unroll
     for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
+    z_elsasser<FORM>(in);
     if constexpr (FORM == 3) {
 #pragma unroll
       for (int f = 0; f < 3; ++f) {
@@ -403,7 +426,7 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
     } else if (FORM != 1) {
 #pragma unroll
       for (int f = 0; f < NOUT; ++f)
-        slot(f, ll)[m] = mk<V>(in[z_pa(f)].x * in[z_pb(f)].x, in[z_pa(f)].y * in[z_pb(f)].y);
+        slot(f, ll)[m] = mk<V>(in[z_pa(f, FORM)].x * in[z_pb(f, FORM)].x, in[z_pa(f, FORM)].y * in[z_pb(f, FORM)].y);
     } else {
       slot(0, ll)[m] = mk<V>(in[1].x * in[5].x - in[2].x * in[4].x, in[1].y * in[5].y - in[2].y * in[4].y);
       slot(1, ll)[m] = mk<V>(in[2].x * in[3].x - in[0].x * in[5].x, in[2].y * in[3].y - in[0].y * in[5].y);
@@ -561,14 +584,15 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
 // the 12-element radix-3 lines (which would spill at 170), 4 for 512-point lines
 // (two warps per line, the pair terms through the exchange line; spilled at 170)
 // (8 for the 4-element variant)
-template <int NZ, int EZ = 0> __host__ __device__ constexpr int zreg_min_blocks() {
-  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : (NZ >= 1024 ? 4 : 6));
+// (4 for the MHD form, which holds six lines while it makes nine products)
+template <int NZ, int EZ = 0, int FORM = 0> __host__ __device__ constexpr int zreg_min_blocks() {
+  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : ((NZ >= 1024 || FORM == 5) ? 4 : 6));
 }
 
 // EZ = 0: 8 elements per thread, 12 for a line length with a factor 3 (radices
 // 4, 2|4, 3); EZ = 4: 4 elements per thread (twice the lanes per line)
 template <typename T, int NZ, int FORM, int EZ = 0>
-__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ>())
+__global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ, FORM>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
   constexpr int M = NZ / 2, H = M + 1, E = EZ ? EZ : ((M % 3 == 0) ? 12 : 8), TPL = M / E, LDX = zslot<M>();
@@ -607,6 +631,17 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ>(
     }
   }
   // real-space products; each complex register holds two real points
+  if constexpr (FORM == 5) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      V col[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) col[c] = in[c][s];
+      z_elsasser<FORM>(col);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) in[c][s] = col[c];
+    }
+  }
   if (FORM == 1) {
 #pragma unroll
     for (int s = 0; s < E; ++s) {
@@ -624,7 +659,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ>(
       if (FORM == 1) {
         p[s] = in[f][s];
       } else {
-        const int a = z_pa(f), b = z_pb(f);
+        const int a = z_pa(f, FORM), b = z_pb(f, FORM);
         p[s] = mk<V>(in[a][s].x * in[b][s].x, in[a][s].y * in[b][s].y);
       }
     }

@@ -269,7 +269,7 @@ static cudaError_t z_slots(const Geo& g, void* P, const void* tw, cudaStream_t s
 template <int NZ, int FORM> constexpr bool z_rule_slots() {
   constexpr int M = NZ / 2;
   return !(std::is_same<T, float>::value && M <= 512) &&
-         !(!std::is_same<T, float>::value && FORM != 3 && M % 3 != 0 && M / ztma_e<T>() <= 32);
+         !(!std::is_same<T, float>::value && FORM <= 2 && M % 3 != 0 && M / ztma_e<T>() <= 32);
 }
 template <int NZ, int FORM> constexpr bool z_valid(int v) {
   constexpr int M = NZ / 2;
@@ -301,7 +301,7 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
       return cudaGetLastError();
     }
   }
-  if constexpr (FORM != 3 && M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
+  if constexpr (FORM <= 2 && M % 3 != 0 && M / ztma_e<T>() <= 32 && !std::is_same<T, float>::value) {
     // FP64: bulk-copy variant (whole groups, 16-byte aligned group starts)
     constexpr int LPB = ztma_lpb<T, NZ>();
     const size_t sm = 2ull * NIN * LPB * (M + 1) * sizeof(V) + (size_t)LPB * zslot<M>() * sizeof(V) + 128;
@@ -348,6 +348,7 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, cons
     if (form == 0) err = z_fused_impl<NZ, 0>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
     else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
     else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
+    else if (form == 5) err = z_fused_impl<NZ, 5>(g, P, tw, zerr, st, nmem, msP, zkeep, 0);
     else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0, zkeep, 0);
   });
   return err;
@@ -651,6 +652,12 @@ template <> cudaError_t Launch<T>::scale(void* A, long long n, double s, cudaStr
 
 template <> cudaError_t Launch<T>::scalar_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st) {
   k_scalar_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::mhd_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st) {
+  k_mhd_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -44,6 +44,8 @@ template <typename T> struct Launch {
                            cudaStream_t st);
   // FFF passive scalar: elementwise epilogue of the nine x-transformed products in P
   static cudaError_t scalar_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
+  // FFF MHD: elementwise epilogue of the nine x-transformed Elsasser products in P
+  static cudaError_t mhd_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,

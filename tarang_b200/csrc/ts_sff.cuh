@@ -464,4 +464,88 @@ __global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// FFF incompressible MHD (RK4(U, W, P, F) with W = B, no force), elementwise
+// epilogue after the forward x FFT of the nine products P_ij = F[Zp_i Zm_j]
+// (f = 3 i + j, unnormalised) of the z pass form 5:
+//   Zp.nlin_i = sum_j D_j P_ij, Zm.nlin_i = sum_j D_j P_ji, accumulated as the
+//   reference does (diagonal term, then the off-diagonal products in the order of
+//   compute_diag_offdiag.cc:202-258); U.nlin = (Zp.nlin + Zm.nlin)/2,
+//   B.nlin = (Zp.nlin - Zm.nlin)/2 (MHD.cc:150-161); pressure from U.nlin;
+//   R_U = -(U.nlin + i K p), R_B = -B.nlin (Tadvance_functions.cc:259-267); IF-RK4
+//   stage update of U (nu, tables eu) and B (eta, tables et), RK_VF_MHD.cc:126-186.
+//   a.U0 = U (3 components), a.T0 = B (3), Ucur and tot carry 6 components.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_mhd_epi(const C<T>* __restrict__ P, Geo g, SffArgs a) {
+  typedef C<T> V;
+  const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
+  const V* U0 = reinterpret_cast<const V*>(a.U0);
+  const V* B0 = reinterpret_cast<const V*>(a.T0);
+  V* Uc = reinterpret_cast<V*>(a.Ucur);
+  V* tot = reinterpret_cast<V*>(a.tot);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const double Kxd = kfft(lx, g.Nx) * g.kf[0], Kyd = kfft(ly, g.Ny) * g.kf[1], Kzd = lz * g.kf[2];
+    const T K[3] = {(T)Kxd, (T)Kyd, (T)Kzd};
+    V q[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) q[f] = scale(P[f * g.S + e], inv);
+    // Zp.nlin (np) and Zm.nlin (nm)
+    V np[3], nm[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) np[i] = nm[i] = ik(K[i], q[4 * i]);
+    np[0] = add(np[0], ik(K[1], q[1])); nm[1] = add(nm[1], ik(K[0], q[1]));   // P01
+    nm[0] = add(nm[0], ik(K[1], q[3])); np[1] = add(np[1], ik(K[0], q[3]));   // P10
+    np[1] = add(np[1], ik(K[2], q[5])); nm[2] = add(nm[2], ik(K[1], q[5]));   // P12
+    nm[1] = add(nm[1], ik(K[2], q[7])); np[2] = add(np[2], ik(K[1], q[7]));   // P21
+    nm[0] = add(nm[0], ik(K[2], q[6])); np[2] = add(np[2], ik(K[0], q[6]));   // P20
+    np[0] = add(np[0], ik(K[2], q[2])); nm[2] = add(nm[2], ik(K[0], q[2]));   // P02
+    V NU[3], NB[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      NU[i] = scale(add(np[i], nm[i]), (T)0.5);
+      NB[i] = scale(sub(np[i], nm[i]), (T)0.5);
+    }
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    const V div = add(add(ik(K[0], NU[0]), ik(K[1], NU[1])), ik(K[2], NU[2]));
+    const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+    V Rv[6];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      Rv[i] = scale(add(NU[i], ik(K[i], pr)), (T)-1);
+      Rv[3 + i] = scale(NB[i], (T)-1);
+    }
+    const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lz];
+    const double ehb = a.et[0][lx] * a.et[1][ly] * a.et[2][lz];
+    const bool dz = dealias_zero(g.dealias, 0, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      const double eh = i < 3 ? ehu : ehb;
+      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const long long o = i * g.S + e;
+      const V R = Rv[i];
+      const V u0 = i < 3 ? U0[o] : B0[(i - 3) * g.S + e];
+      if (a.stage == 1) {
+        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+      } else if (a.stage == 2) {
+        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else if (a.stage == 3) {
+        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else {
+        V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
+        if (i < 3) const_cast<V*>(U0)[o] = un;
+        else const_cast<V*>(B0)[(i - 3) * g.S + e] = un;
+      }
+    }
+  }
+}
+
 }  // namespace ts

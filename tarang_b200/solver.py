@@ -225,6 +225,10 @@ class Plan:
     def rk4_step_rbc(self, u, T, nsteps: int = 1):
         L.check(self.lib.ts_rk4_step_rbc(self.h, _ptr(u), _ptr(T), nsteps), "ts_rk4_step_rbc")
 
+    def rk4_step_mhd(self, u, b, nsteps: int = 1):
+        """RK4(U, W, P, F) for incompressible MHD (FFF, unforced): u with nu, b with eta = the plan's kappa."""
+        L.check(self.lib.ts_rk4_step_mhd(self.h, _ptr(u), _ptr(b), nsteps), "ts_rk4_step_mhd")
+
     def rk4_step_scalar(self, u, T, nsteps: int = 1):
         """RK4(U,T,P,F) with a passive scalar T (FFF, conservative form, unforced; kappa of the plan)."""
         L.check(self.lib.ts_rk4_step_scalar(self.h, _ptr(u), _ptr(T), nsteps), "ts_rk4_step_scalar")

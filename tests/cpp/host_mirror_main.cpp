@@ -6,6 +6,7 @@
 //   rbc       SFF_PENCIL + FluidVF + FluidSF: energies and Nusselt number
 //   ensemble  two RBC members of different sizes advanced together: Nusselt numbers
 //   adjoint   FFF rotational FP64: cotangent of the start state of an nsteps window
+//   mhd       FFF incompressible MHD: energies of U and B, max |div B|
 // Prints one JSON line; tests/test_cpp_host.py compares it with the same run
 // through the Python binding.
 #include <cmath>
@@ -105,6 +106,24 @@ static int run_ensemble(int N, int steps) {
   return 0;
 }
 
+static int run_mhd(int N, int steps) {
+  ts_config c;
+  ts_config_default(&c);
+  c.N[0] = c.N[1] = c.N[2] = N;
+  c.nu = 0.01;
+  c.kappa = 0.02;  // eta
+  c.dt = 1e-3;
+  c.dealias_mode = TS_DEALIAS_TWO_THIRDS;
+  FFF_PENCIL basis(c);
+  FluidVF U(basis), W(basis);
+  U.Init_cond_energy_spectrum(k4_gauss(basis.no_shells(), 4.0), 0, 0.5);
+  W.Init_cond_energy_spectrum(k4_gauss(basis.no_shells(), 3.0), 1, 0.3);
+  Time_advance_incompress::RK4(U, W, steps);
+  printf("{\"eu\": %.17g, \"eb\": %.17g, \"divb\": %.17g}\n", U.Compute_total_energy(), W.Compute_total_energy(),
+         W.Compute_divergence_field());
+  return 0;
+}
+
 static int run_adjoint(int N, int steps) {
   ts_config c;
   ts_config_default(&c);
@@ -141,6 +160,7 @@ int main(int argc, char** argv) {
     if (!strcmp(mode, "rbc")) return run_rbc(N, steps);
     if (!strcmp(mode, "ensemble")) return run_ensemble(N, steps);
     if (!strcmp(mode, "adjoint")) return run_adjoint(N, steps);
+    if (!strcmp(mode, "mhd")) return run_mhd(N, steps);
     fprintf(stderr, "unknown mode %s\n", mode);
     return 2;
   } catch (const ts_error& e) {

@@ -56,6 +56,21 @@ def test_host_mirror_matches_python_binding(cuda, tmp_path):
 
 
 @pytest.mark.gpu
+def test_host_mirror_mhd_matches_python_binding(cuda, tmp_path):
+    import tarang_b200 as tb
+    out = run_driver(build_driver(tmp_path), "mhd", 32, 4)
+    plan = tb.Plan(32, nu=0.01, kappa=0.02, dt=1e-3, dealias="two_thirds")
+    u, b = plan.field(3), plan.field(3)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 0, 0.5, u)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 3.0), 1, 0.3, b)
+    plan.rk4_step_mhd(u, b, 4)
+    # the drivers build the initial spectra with different pow/exp (last-bit differences)
+    assert abs(out["eu"] - plan.energy(u)) < 1e-13 * out["eu"]
+    assert abs(out["eb"] - plan.energy(b)) < 1e-13 * out["eb"]
+    assert out["divb"] < 1e-12
+
+
+@pytest.mark.gpu
 def test_host_mirror_autotuned_matches_rule(cuda, tmp_path):
     exe = build_driver(tmp_path)
     a = run_driver(exe, "fff", 64, 3)
