@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--form", default="rotational", choices=["rotational", "conservative"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
-    ap.add_argument("--workload", default="fff256", choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint"],
+    ap.add_argument("--workload", default="fff256",
+                    choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint", "scalar", "mhd"],
                     help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying "
                          "1024^3 (or --shape); rbc: one RBC run (SFF, --N, FP32); adjoint: adjoint/forward cost at 128^3")
     ap.add_argument("--tune", default="auto", choices=["auto", "off"],
@@ -178,6 +179,54 @@ def ensemble_plain_fp64_leg(steps: int = 3, warmup: int = 1):
     torch.cuda.empty_cache()
     return {"ensemble_steps_per_s": steps / (ms / 1e3), "members": len(members), "steps": steps,
             "how": "64 FP64 plans stepped one after another, fixed tile rules, CUDA events"}
+
+
+def coupled_leg(kind: str, N: int, steps: int, warmup: int, prec: str = "f32"):
+    """FFF passive scalar ("scalar") or incompressible MHD ("mhd") at N^3: decaying, nu = 1e-3,
+    kappa / eta = 1e-3, dt = 5e-4, two-thirds dealias; U (and B) from the k^4 exp(-2(k/4)^2)
+    spectrum (seeds 0, 1), the scalar a copy of u1.  Steps/s (CUDA events) and the per-class
+    kernel times; model bytes 90 (scalar) / 114 (MHD) S s per right-hand side."""
+    import torch
+    import ctypes
+    import tarang_b200 as tb
+    from tarang_b200 import _lib as L
+    plan = tb.Plan(N, precision=prec, nu=1e-3, kappa=1e-3, dt=5e-4, dealias="two_thirds")
+    plan.set_stream(torch.cuda.current_stream())
+    u = plan.field(3)
+    plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 0, 0.5, u)
+    if kind == "mhd":
+        w = plan.field(3)
+        plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 1, 0.3, w)
+        step = lambda n: plan.rk4_step_mhd(u, w, n)
+    else:
+        w = u[0:1].clone()
+        step = lambda n: plan.rk4_step_scalar(u, w, n)
+    step(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    L.check(plan.lib.ts_profile_reset(plan.h), "reset")
+    L.check(plan.lib.ts_profile_enable(plan.h, 1), "enable")
+    step(1)
+    torch.cuda.synchronize()
+    L.check(plan.lib.ts_profile_enable(plan.h, 0), "disable")
+    kern = {}
+    for k, name in enumerate(L.KCLASS_NAMES):
+        tot, n, b = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+        L.check(plan.lib.ts_profile_read(plan.h, k, ctypes.byref(tot), ctypes.byref(n), ctypes.byref(b)), "read")
+        if n.value:
+            kern[name] = round(tot.value, 4)
+    S = N * N * (N // 2 + 1)
+    sb = 8 if prec == "f32" else 16
+    model = (90 if kind == "scalar" else 114) * 4 * S * sb
+    plan.close()
+    return {"steps_per_s": steps / (ms / 1e3), "ms_per_step_by_class": kern,
+            "model_GBps": model * steps / (ms / 1e3) / 1e9,
+            "model_frac": model * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
 
 
 def rbc_leg(N: int, steps: int, warmup: int):
@@ -426,6 +475,17 @@ def alt_workload(args, world, rank, local, dev):
                              "traffic": None, "model": "408 N^3 4 B per member step"},
                 "member_steps_per_s": 64 * value}
         line["config"]["tuning"] = r["tuning"]
+    elif args.workload in ("scalar", "mhd"):
+        n = args.N
+        r = coupled_leg(args.workload, n, steps=args.steps, warmup=args.warmup, prec=args.precision)
+        what = "passive scalar" if args.workload == "scalar" else "incompressible MHD"
+        line = {"metric": f"RK4 steps/s, FFF {what} {n}^3 ({args.precision} transforms, FP64 sums)",
+                "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 / r["steps_per_s"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": f"FFF {what} {n}^3, decaying, nu = kappa/eta = 1e-3, dt = 5e-4, two-thirds"},
+                "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "model_GBps": r["model_GBps"],
+                             "ms_per_step_by_class": r["ms_per_step_by_class"]}}
     elif args.workload == "rbc":
         r = rbc_leg(args.N if args.N != 256 else 128, steps=args.steps, warmup=args.warmup)
         n = args.N if args.N != 256 else 128
@@ -636,6 +696,8 @@ def main():
             # one plan at a time; the north-star target is FP32 / plain FP64 >= 3
             extras["fff1024_f64_plain"] = fff1024_leg(steps=2, warmup=1, prec="f64", tune=False)
             extras["ensemble_rbc_64_fp64_plain"] = ensemble_plain_fp64_leg()
+            extras["scalar_256_f32"] = coupled_leg("scalar", 256, steps=5, warmup=2)
+            extras["mhd_256_f32"] = coupled_leg("mhd", 256, steps=5, warmup=2)
             extras["fp32_over_plain_fp64"] = {
                 "fff1024": extras["fff1024_f32"]["steps_per_s"] / extras["fff1024_f64_plain"]["steps_per_s"],
                 "ensemble": extras["ensemble_rbc_64"]["ensemble_steps_per_s"]
