@@ -475,9 +475,10 @@ __global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, 
 //   R_U = -(U.nlin + i K p), R_B = -B.nlin (Tadvance_functions.cc:259-267); IF-RK4
 //   stage update of U (nu, tables eu) and B (eta, tables et), RK_VF_MHD.cc:126-186.
 //   a.U0 = U (3 components), a.T0 = B (3), Ucur and tot carry 6 components.
+//   Compiled for three blocks per SM (66 registers): with 123 it ran 20 % slower.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_mhd_epi(const C<T>* __restrict__ P, Geo g, SffArgs a) {
+__global__ void __launch_bounds__(256, 3) k_mhd_epi(const C<T>* __restrict__ P, Geo g, SffArgs a) {
   typedef C<T> V;
   const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
   const V* U0 = reinterpret_cast<const V*>(a.U0);
