@@ -258,3 +258,63 @@ def test_reality_fix_adjoint_is_transpose():
     B = rng.standard_normal((3,) + g.shape) + 1j * rng.standard_normal((3,) + g.shape)
     ip = lambda a, b: float(np.real(np.sum(a * np.conj(b))))
     assert abs(ip(R.reality_fix_vec(g, A), B) - ip(A, R.reality_fix_vec_adjoint(g, B))) < 1e-12 * abs(ip(A, B)) + 1e-9
+
+
+# ---------------------------------------------------------------------------
+# passive scalar and MHD (FFF)
+# ---------------------------------------------------------------------------
+def test_scalar_pure_diffusion_is_exact():
+    """u = 0: the passive scalar only diffuses, and the integrating factor makes that exact."""
+    g = R.Grid((16, 16, 16))
+    rng = np.random.default_rng(3)
+    T0 = R.reality_fix(g, R.forward(g, rng.standard_normal(g.rshape)))
+    cfg = R.ScalarConfig(g, nu=0.01, kappa=0.05, dt=1e-2, dealias_mode=0)
+    U, T = np.zeros((3,) + g.shape, complex), T0.copy()
+    for _ in range(5):
+        U, T = R.rbc_rk4_step(cfg, U, T)
+    expect = R.reality_fix(g, T0 * np.exp(-cfg.kappa * g.Ksqr() * 5 * cfg.dt))
+    assert np.max(np.abs(T - expect)) < 1e-14
+    assert np.max(np.abs(U)) == 0
+
+
+def test_scalar_mean_kept_and_variance_decays():
+    g = R.Grid((16, 16, 16))
+    U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 2.0), 0, 0.5)
+    rng = np.random.default_rng(4)
+    T = R.reality_fix(g, R.forward(g, rng.standard_normal(g.rshape)))
+    T[0, 0, 0] = 0.3
+    cfg = R.ScalarConfig(g, nu=0.01, kappa=0.05, dt=2e-3, dealias_mode=2)
+    v0 = R.total_energy_scalar(g, T)
+    for _ in range(5):
+        U, T = R.rbc_rk4_step(cfg, U, T)
+    assert abs(T[0, 0, 0] - 0.3) < 1e-15
+    assert R.total_energy_scalar(g, T) < v0
+
+
+def test_mhd_without_field_is_the_fluid_step():
+    """B = 0: the Elsasser nonlinear terms reduce to the conservative fluid term and B stays 0."""
+    g = R.Grid((16, 16, 16))
+    U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 1, 0.5)
+    fl = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=2, nlin_form="conservative")
+    mh = R.MHDConfig(g, nu=0.01, eta=0.02, dt=1e-3, dealias_mode=2)
+    Uf = R.rk4_step(fl, U.copy())
+    Um, Bm = R.mhd_rk4_step(mh, U.copy(), np.zeros_like(U))
+    assert np.max(np.abs(Bm)) == 0
+    assert np.linalg.norm(Um - Uf) <= 1e-13 * np.linalg.norm(Uf)
+
+
+def test_ideal_mhd_invariants():
+    """nu = eta = 0: total energy and cross helicity conserved to the RK4 error, fields solenoidal."""
+    g = R.Grid((16, 16, 16))
+    U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 2.0), 0, 0.5)
+    B = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 2.0), 1, 0.3)
+    cfg = R.MHDConfig(g, nu=0.0, eta=0.0, dt=1e-3, dealias_mode=2)
+    E0 = R.total_energy(g, U) + R.total_energy(g, B)
+    H0 = sum(R.cross_energy(g, U[i], B[i]) for i in range(3))
+    for _ in range(10):
+        U, B = R.mhd_rk4_step(cfg, U, B)
+    E1 = R.total_energy(g, U) + R.total_energy(g, B)
+    H1 = sum(R.cross_energy(g, U[i], B[i]) for i in range(3))
+    assert abs(E1 - E0) < 1e-6 * E0
+    assert abs(H1 - H0) < 1e-6 * E0
+    assert R.max_abs_div(g, B) < 1e-14 and R.max_abs_div(g, U) < 1e-14
