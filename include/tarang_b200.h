@@ -45,7 +45,10 @@ typedef enum {
   TS_ERR_NOMEM = 6        /* device allocation failed */
 } ts_status;
 
-typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1 } ts_basis;
+/* TS_BASIS_SSF (sin/cos along x and y, Fourier along z; basis/SSF/pencil) offers the
+ * transforms only: ts_fft_forward / ts_fft_inverse with parities "SCF", "CSF", "SSF",
+ * "CCF"; every other call on an SSF plan returns TS_ERR_UNSUPPORTED. */
+typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1, TS_BASIS_SSF = 2 } ts_basis;
 typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
 typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;
 typedef enum { TS_DEALIAS_NONE = 0, TS_DEALIAS_REFERENCE_CORNER = 1, TS_DEALIAS_TWO_THIRDS = 2 } ts_dealias;

@@ -122,12 +122,13 @@ class Grid:
         lx = np.arange(Nx)
         if self.basis == "FFF":
             self.kx = np.where(lx <= Nx // 2, lx, lx - Nx)
-        elif self.basis == "SFF":
+        elif self.basis in ("SFF", "SSF"):
             self.kx = lx.copy()
         else:
             raise ValueError(self.basis)
         ly = np.arange(Ny)
-        self.ky = np.where(ly <= Ny // 2, ly, ly - Ny)
+        # SSF: sin/cos along y as well, ky = ly (SSF_pencil_inline.h Get_ky)
+        self.ky = ly.copy() if self.basis == "SSF" else np.where(ly <= Ny // 2, ly, ly - Ny)
         self.kz = np.arange(Nz // 2 + 1)
 
     @property
@@ -273,31 +274,34 @@ def reality_fix_vec(g: Grid, V: np.ndarray) -> np.ndarray:
 # ----------------------------------------------------------------------------
 # transforms
 # ----------------------------------------------------------------------------
-def _x_forward_sincos(g: Grid, B: np.ndarray, parity: str) -> np.ndarray:
-    """Sine/cosine analysis along x (axis 0) with the FFTW RODFT10/REDFT10 scaling / (2 Nx).
+def _x_forward_sincos(g: Grid, B: np.ndarray, parity: str, axis: int = 0) -> np.ndarray:
+    """Sine/cosine analysis along x (axis 0; y for the SSF basis, axis 1) with the FFTW
+    RODFT10/REDFT10 scaling / (2 N).
 
     Sine: coefficient of 2 sin(m pi x/Lx) stored at lx=m for m=1..Nx-1 (lx=0 is 0,
     the m=Nx coefficient is dropped).  Cosine: c_0 + sum 2 c_m cos(m pi x/Lx), m=0..Nx-1.
     Staggered grid x_j = (j+1/2) Lx/Nx (type-II forward / type-III inverse).
     """
-    Nx = g.N[0]
+    N = g.N[axis]
     if parity == "S":
-        Y = sfft.dst(B, type=2, axis=0, workers=WORKERS) / (2.0 * Nx)
+        Y = sfft.dst(B, type=2, axis=axis, workers=WORKERS) / (2.0 * N)
+        Y = np.moveaxis(Y, axis, 0)
         out = np.zeros_like(Y)
         out[1:] = Y[:-1]
-        return out
+        return np.moveaxis(out, 0, axis)
     if parity == "C":
-        return sfft.dct(B, type=2, axis=0, workers=WORKERS) / (2.0 * Nx)
+        return sfft.dct(B, type=2, axis=axis, workers=WORKERS) / (2.0 * N)
     raise ValueError(parity)
 
 
-def _x_inverse_sincos(g: Grid, A: np.ndarray, parity: str) -> np.ndarray:
+def _x_inverse_sincos(g: Grid, A: np.ndarray, parity: str, axis: int = 0) -> np.ndarray:
     if parity == "S":
-        Y = np.zeros_like(A)
-        Y[:-1] = A[1:]
-        return sfft.dst(Y, type=3, axis=0, workers=WORKERS)
+        Am = np.moveaxis(A, axis, 0)
+        Y = np.zeros_like(Am)
+        Y[:-1] = Am[1:]
+        return sfft.dst(np.moveaxis(Y, 0, axis), type=3, axis=axis, workers=WORKERS)
     if parity == "C":
-        return sfft.dct(A, type=3, axis=0, workers=WORKERS)
+        return sfft.dct(A, type=3, axis=axis, workers=WORKERS)
     raise ValueError(parity)
 
 
@@ -305,6 +309,10 @@ def forward(g: Grid, ur: np.ndarray, parity: str = "F") -> np.ndarray:
     """Real (Nx,Ny,Nz) -> spectral (Nx,Ny,Nz/2+1).  FFF: A = N^-3 sum u e^{-ik.x}."""
     if g.basis == "FFF":
         return sfft.rfftn(ur, norm="forward", workers=WORKERS)
+    if g.basis == "SSF":
+        # SSF_pencil_tr.cc:43-51: sin/cos along x and y by the parity's first two letters
+        Bz = sfft.rfft(ur, axis=2, norm="forward", workers=WORKERS)
+        return _x_forward_sincos(g, _x_forward_sincos(g, Bz, parity[1], axis=1), parity[0])
     Byz = sfft.rfftn(ur, axes=(1, 2), norm="forward", workers=WORKERS)
     return _x_forward_sincos(g, Byz, parity)
 
@@ -314,6 +322,9 @@ def inverse(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
     if g.basis == "FFF":
         return sfft.irfftn(A, s=g.rshape, norm="forward", workers=WORKERS)
     Nx, Ny, Nz = g.N
+    if g.basis == "SSF":
+        Bxy = _x_inverse_sincos(g, _x_inverse_sincos(g, A, parity[0]), parity[1], axis=1)
+        return sfft.irfft(Bxy, n=Nz, axis=2, norm="forward", workers=WORKERS)
     Bx = _x_inverse_sincos(g, A, parity)
     return sfft.irfftn(Bx, s=(Ny, Nz), axes=(1, 2), norm="forward", workers=WORKERS)
 

@@ -70,7 +70,8 @@ struct ts_plan {
   int* err_h = nullptr;     // pinned copy, refreshed after every step call
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
   double* eaxT[3] = {nullptr, nullptr, nullptr}; // per-axis exp(-kappa dt K_i^2 / 2) (SFF scalar)
-  void* twq = nullptr;      // SFF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
+  void* twq = nullptr;      // SFF, SSF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
+  void* twqy = nullptr;     // SSF: exp(-2 pi i j / (4 Ny)), j < 4 Ny
   // per-kernel-class CUDA event timing (ts_profile_*)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -248,7 +249,7 @@ const char* ts_last_error(void) { return g_last_error.c_str(); }
 int ts_plan_destroy(ts_plan* p) {
   if (!p) return TS_ERR_ARG;
   void* bufs[] = {p->Ucur, p->tot, p->P, p->twx, p->twy, p->twz, p->fcube, p->esup, p->hsup, p->mis_d, p->dscr,
-                  p->stage_u, p->stage_t, p->stage_b};
+                  p->stage_u, p->stage_t, p->stage_b, p->twqy};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
@@ -268,17 +269,21 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   *out = nullptr;
   for (int i = 0; i < 3; ++i) {
     // 48 and 96 (factor 3) are supported for the SFF path
-    const bool mixed = (cfg->N[i] == 48 || cfg->N[i] == 96) && cfg->basis == TS_BASIS_SFF;
+    const bool mixed = (cfg->N[i] == 48 || cfg->N[i] == 96) && cfg->basis != TS_BASIS_FFF;
     if (!size_supported(cfg->N[i]) && !mixed) {
       g_last_error = "N must be a power of two in [16, 1024] (48 and 96 also for SFF)";
       return TS_ERR_ARG;
     }
   }
-  if (cfg->basis != TS_BASIS_FFF && cfg->basis != TS_BASIS_SFF) return TS_ERR_ARG;
+  if (cfg->basis != TS_BASIS_FFF && cfg->basis != TS_BASIS_SFF && cfg->basis != TS_BASIS_SSF) return TS_ERR_ARG;
   if (cfg->precision != TS_F64 && cfg->precision != TS_F32) return TS_ERR_ARG;
   if (cfg->dealias_mode < 0 || cfg->dealias_mode > 2) return TS_ERR_ARG;
   if (cfg->nlin_form != TS_NLIN_CONSERVATIVE && cfg->nlin_form != TS_NLIN_ROTATIONAL) return TS_ERR_ARG;
-  if (cfg->basis == TS_BASIS_SFF && cfg->nlin_form == TS_NLIN_ROTATIONAL) return TS_ERR_UNSUPPORTED;
+  if (cfg->basis != TS_BASIS_FFF && cfg->nlin_form == TS_NLIN_ROTATIONAL) return TS_ERR_UNSUPPORTED;
+  if (cfg->basis == TS_BASIS_SSF && (cfg->N[0] > 512 || cfg->N[1] > 512)) {
+    g_last_error = "SSF supports Nx, Ny <= 512";
+    return TS_ERR_UNSUPPORTED;
+  }
   ts_plan* p = new ts_plan();
   p->cfg = *cfg;
   p->cfg.energy_supply = nullptr;
@@ -377,7 +382,12 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   CKP(upload_if_tables(p, cfg->nu, cfg->dt, p->eax));
   // the scalar's factors: the SFF Boussinesq step and the FFF passive-scalar step
   CKP(upload_if_tables(p, cfg->kappa, cfg->dt, p->eaxT));
-  if (cfg->basis == TS_BASIS_SFF) {
+  if (cfg->basis == TS_BASIS_SSF) {
+    // sin/cos along y: the 4 Ny quarter-step table
+    if (p->prec) CKP(upload_twiddles<float>(4 * g.Ny, &p->twqy));
+    else CKP(upload_twiddles<double>(4 * g.Ny, &p->twqy));
+  }
+  if (cfg->basis != TS_BASIS_FFF) {
     if (p->prec) CKP(upload_twiddles<float>(4 * g.Nx, &p->twq));
     else CKP(upload_twiddles<double>(4 * g.Nx, &p->twq));
   }
@@ -746,6 +756,12 @@ static int step_mhd_fff(ts_plan* p, void* U0, void* B0) {
   return TS_OK;
 }
 
+// SSF plans offer the transforms only
+static int ssf_transforms_only() {
+  g_last_error = "SSF plans offer ts_fft_forward / ts_fft_inverse only";
+  return TS_ERR_UNSUPPORTED;
+}
+
 // run fn(device_ptr) on a field that may live on the host
 template <typename Fn>
 static int with_device(ts_plan* p, void** stage, const void* ptr, size_t bytes, bool copy_back, Fn&& fn) {
@@ -917,6 +933,7 @@ int ts_init_temperature_perturbation(ts_plan* p, double amp, double kmax, uint64
 }
 
 int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !u_hat || !nlin_hat) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   const size_t bytes = 3 * p->g.S * p->cb;
@@ -940,6 +957,7 @@ int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
 }
 
 int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !a_hat || !energy || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
   return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
@@ -951,6 +969,7 @@ int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
 }
 
 int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !u_hat || !max_div) return TS_ERR_ARG;
   return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, false, [&](void* U) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
@@ -962,6 +981,7 @@ int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
 }
 
 int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int n_shells) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !a_hat || !Ek || ncomp < 1 || ncomp > 3 || n_shells < 1) return TS_ERR_ARG;
   const int nsh = p->nshells;
   return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
@@ -984,6 +1004,7 @@ int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int 
 
 int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, double* sums, double* counts,
                   int n_shells) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !a_hat || ncomp < 1 || ncomp > 3 || n_shells < 1 || (!sums && !counts)) return TS_ERR_ARG;
   if (!is_device_ptr(a_hat) || (b_hat && !is_device_ptr(b_hat))) {
     g_last_error = "ts_shell_sums: device pointers required";
@@ -1004,6 +1025,7 @@ int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, d
 }
 
 int ts_force_field(ts_plan* p, const void* u_hat, void* f_hat) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !u_hat || !f_hat) return TS_ERR_ARG;
   if (p->cfg.force_type != TS_FORCE_CARATI_ENERGY_SUPPLY) {
     g_last_error = "ts_force_field: the plan has no Carati forcing";
@@ -1020,6 +1042,7 @@ int ts_force_field(ts_plan* p, const void* u_hat, void* f_hat) {
 }
 
 int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, double* Pi) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   for (int i = 1; i < n_radii; ++i)
@@ -1050,6 +1073,7 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
 }
 
 int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !u_hat || !T_hat || !Nu) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
   if (!is_device_ptr(u_hat) || !is_device_ptr(T_hat)) return TS_ERR_ARG;
@@ -1064,6 +1088,7 @@ int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
 
 int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed, double target_energy,
                             void* u_hat) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || !E_ic || n < 1 || !u_hat) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
@@ -1097,22 +1122,53 @@ int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed
 // parity string -> x basis: FFF plans take "FFF"; SFF plans take "SFF" (sine
 // along x) or "CFF" (cosine), the first letter of the reference's
 // sincostr_switch entries (global/Global.cc:137-145).  Returns -1 if invalid.
-static int x_parity(const ts_plan* p, const char* parity) {
+// x parity: 0 Fourier (FFF), 1 sine, 2 cosine; *yp: the y parity of an SSF plan
+// (1 sine, 2 cosine; 0 Fourier otherwise)
+static int x_parity(const ts_plan* p, const char* parity, int* yp = nullptr) {
+  if (yp) *yp = 0;
   if (p->cfg.basis == TS_BASIS_FFF) return strcmp(parity, "FFF") == 0 ? 0 : -1;
+  if (p->cfg.basis == TS_BASIS_SSF) {
+    if (strlen(parity) != 3 || parity[2] != 'F') return -1;
+    const int x = parity[0] == 'S' ? 1 : (parity[0] == 'C' ? 2 : -1);
+    const int y = parity[1] == 'S' ? 1 : (parity[1] == 'C' ? 2 : -1);
+    if (x < 0 || y < 0) return -1;
+    if (yp) *yp = y;
+    return x;
+  }
   if (strcmp(parity, "SFF") == 0) return 1;
   if (strcmp(parity, "CFF") == 0) return 2;
   return -1;
 }
 
+// the geometry that makes the x-axis sin/cos kernel transform along y: every
+// x-plane of every component is one "component" of Ny rows x Hz columns
+static Geo y_as_x(const Geo& g) {
+  Geo h = g;
+  h.Nx = g.Ny;
+  h.Ny = 1;
+  h.S = (long long)g.Ny * g.Hz;
+  h.dealias = 0;
+  return h;
+}
+
 int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* spec_out, int ncomp) {
   if (!p || !parity || !real_in || !spec_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  const int xp = x_parity(p, parity);
+  int yp = 0;
+  const int xp = x_parity(p, parity, &yp);
   if (xp < 0) {
-    g_last_error = "parity must be \"FFF\" (FFF plan) or \"SFF\" / \"CFF\" (SFF plan)";
+    g_last_error = "parity must be \"FFF\" (FFF plan), \"SFF\" / \"CFF\" (SFF plan) or [SC][SC]F (SSF plan)";
     return TS_ERR_ARG;
   }
   if (!is_device_ptr(real_in) || !is_device_ptr(spec_out)) return TS_ERR_ARG;
   const Geo& g = p->g;
+  if (yp) {
+    // SSF (SSF_pencil_tr.cc:43-51): z Fourier, then sin/cos / (2 Ny) along y, sin/cos
+    // / (2 Nx) along x with the z normalisation
+    CK(LAUNCH(p, z_single, g, -1, real_in, spec_out, ncomp, p->twz, p->st));
+    CK(LAUNCH(p, sff_x, y_as_x(g), -1, spec_out, ncomp * g.Nx, yp == 1, 1.0 / (2.0 * g.Ny), p->twqy, p->st));
+    CK(LAUNCH(p, sff_x, g, -1, spec_out, ncomp, xp == 1, 1.0 / (2.0 * g.Nx * (double)g.Nz), p->twq, p->st));
+    return TS_OK;
+  }
   CK(LAUNCH(p, z_single, g, -1, real_in, spec_out, ncomp, p->twz, p->st));
   CK(LAUNCH(p, strided, g, 1, -1, spec_out, ncomp, p->twy, p->st));
   if (xp == 0) {
@@ -1127,15 +1183,22 @@ int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* sp
 
 int ts_fft_inverse(ts_plan* p, const char* parity, const void* spec_in, void* real_out, int ncomp) {
   if (!p || !parity || !spec_in || !real_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  const int xp = x_parity(p, parity);
+  int yp = 0;
+  const int xp = x_parity(p, parity, &yp);
   if (xp < 0) {
-    g_last_error = "parity must be \"FFF\" (FFF plan) or \"SFF\" / \"CFF\" (SFF plan)";
+    g_last_error = "parity must be \"FFF\" (FFF plan), \"SFF\" / \"CFF\" (SFF plan) or [SC][SC]F (SSF plan)";
     return TS_ERR_ARG;
   }
   if (!is_device_ptr(spec_in) || !is_device_ptr(real_out)) return TS_ERR_ARG;
   const Geo& g = p->g;
   // the reference copies the input to X_transform first (FFF_pencil_tr.cc:59)
   CK(cudaMemcpyAsync(p->P, spec_in, ncomp * g.S * p->cb, cudaMemcpyDeviceToDevice, p->st));
+  if (yp) {
+    CK(LAUNCH(p, sff_x, g, +1, p->P, ncomp, xp == 1, 1.0, p->twq, p->st));
+    CK(LAUNCH(p, sff_x, y_as_x(g), +1, p->P, ncomp * g.Nx, yp == 1, 1.0, p->twqy, p->st));
+    CK(LAUNCH(p, z_single, g, +1, p->P, real_out, ncomp, p->twz, p->st));
+    return TS_OK;
+  }
   if (xp == 0) CK(LAUNCH(p, strided, g, 0, +1, p->P, ncomp, p->twx, p->st));
   else CK(LAUNCH(p, sff_x, g, +1, p->P, ncomp, xp == 1, 1.0, p->twq, p->st));
   CK(LAUNCH(p, strided, g, 1, +1, p->P, ncomp, p->twy, p->st));
@@ -1618,6 +1681,7 @@ int ts_plan_set_tuning(ts_plan* p, const ts_tuning* t) {
 }
 
 int ts_plan_autotune(ts_plan* p, int reps, char* report, size_t report_len) {
+  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
   if (!p || reps < 1) return TS_ERR_ARG;
   const bool sff = p->cfg.basis == TS_BASIS_SFF;
   const size_t bu = 3 * (size_t)p->g.S * p->cb, bt = (size_t)p->g.S * p->cb;

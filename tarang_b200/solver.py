@@ -81,7 +81,7 @@ class Plan:
         self.N = tuple(int(n) for n in N)
         c = L.TsConfig()
         self.lib.ts_config_default(ctypes.byref(c))
-        c.basis = L.TS_BASIS_FFF if basis == "FFF" else L.TS_BASIS_SFF
+        c.basis = {"FFF": L.TS_BASIS_FFF, "SFF": L.TS_BASIS_SFF, "SSF": L.TS_BASIS_SSF}[basis]
         for i in range(3):
             c.N[i] = self.N[i]
             c.kfactor[i] = float(kfactor[i])
