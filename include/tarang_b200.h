@@ -46,8 +46,10 @@ typedef enum {
 } ts_status;
 
 /* TS_BASIS_SSF (sin/cos along x and y, Fourier along z; basis/SSF/pencil) offers the
- * transforms only: ts_fft_forward / ts_fft_inverse with parities "SCF", "CSF", "SSF",
- * "CCF"; every other call on an SSF plan returns TS_ERR_UNSUPPORTED. */
+ * transforms (ts_fft_forward / ts_fft_inverse with parities "SCF", "CSF", "SSF", "CCF")
+ * and ts_rk4_step for the conservative, unforced fluid (sincostr_switch "SCF":
+ * Vx = SCF, Vy = CSF, Vz = CCF); every other call on an SSF plan returns
+ * TS_ERR_UNSUPPORTED. */
 typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1, TS_BASIS_SSF = 2 } ts_basis;
 typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
 typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;

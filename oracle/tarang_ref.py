@@ -218,7 +218,11 @@ def dealias_mask(g: Grid, mode: int) -> np.ndarray:
             mx = (lx >= Nx // 3 + 1) & (lx <= 2 * Nx // 3 - 1)
         else:
             mx = lx >= 2 * Nx // 3 + 1
-        my = (ly >= Ny // 3 + 1) & (ly <= 2 * Ny // 3 - 1)
+        if g.basis == "SSF":
+            # SSF_PENCIL::Dealias (SSF_pencil_basic.cc:103-106): lx >= 2Nx/3+1, ly >= 2Ny/3+1, lz >= Nz/3+1
+            my = ly >= 2 * Ny // 3 + 1
+        else:
+            my = (ly >= Ny // 3 + 1) & (ly <= 2 * Ny // 3 - 1)
         mz = (lz >= Nz // 3 + 1) & (lz <= Nz // 2)
         return np.broadcast_to(mx & my & mz, g.shape).copy()
     if mode == DEALIAS_TWO_THIRDS:
@@ -229,7 +233,8 @@ def dealias_mask(g: Grid, mode: int) -> np.ndarray:
             bx = 3 * np.abs(kx) > Nx
         else:
             bx = 3 * kx > 2 * Nx
-        m = bx | (3 * np.abs(ky) > Ny) | (3 * kz > Nz)
+        by = (3 * ky > 2 * Ny) if g.basis == "SSF" else (3 * np.abs(ky) > Ny)
+        m = bx | by | (3 * kz > Nz)
         return np.broadcast_to(m, g.shape).copy()
     raise ValueError(mode)
 
@@ -251,6 +256,8 @@ def reality_fix(g: Grid, A: np.ndarray) -> np.ndarray:
     """
     Nx, Ny, Nz = g.N
     B = A.copy()
+    if g.basis == "SSF":
+        return B  # SSF_pencil_basic.cc:127-130: nothing to do
     plane = A[:, :, 0].copy()
     iy_minus = (-g.ky) % Ny  # Get_iy(-ky)
     if g.basis == "FFF":
@@ -333,15 +340,19 @@ def inverse(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
 # derivatives (FFF: i K ; SFF x: real factor by parity)
 # ----------------------------------------------------------------------------
 def xderiv(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
-    """FFF_pencil_tr.cc:70-79 (i Kx); SFF_pencil_tr.cc:77-90 (S -> +Kx, C -> -Kx)."""
+    """FFF_pencil_tr.cc:70-79 (i Kx); SFF_pencil_tr.cc:77-90 and SSF_pencil_tr.cc:69-90
+    (x parity S -> +Kx, C -> -Kx)."""
     Kx, _, _ = g.K()
     if g.basis == "FFF":
         return (1j * Kx) * A
-    return (Kx if parity == "S" else -Kx) * A
+    return (Kx if parity[0] == "S" else -Kx) * A
 
 
-def yderiv(g: Grid, A: np.ndarray) -> np.ndarray:
+def yderiv(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
+    """i Ky; SSF (SSF_PENCIL::Yderiv): y parity S -> +Ky, C -> -Ky."""
     _, Ky, _ = g.K()
+    if g.basis == "SSF":
+        return (Ky if parity[1] == "S" else -Ky) * A
     return (1j * Ky) * A
 
 
@@ -355,7 +366,14 @@ SFF_PARITY = {"Vx": "S", "Vy": "C", "Vz": "C", "div": "C", "Vi2": "C", "VxVy": "
               "VyVz": "C", "F": "S", "FVx": "C", "FVy": "S", "FVz": "S"}
 
 
+# SSF parity strings for sincostr_switch "SCF" (global/Global.cc:184-191): x, y, z letters
+SSF_PARITY = {"Vx": "SCF", "Vy": "CSF", "Vz": "CCF", "div": "CCF", "Vi2": "CCF", "VxVy": "SSF", "VxVz": "SCF",
+              "VyVz": "CSF"}
+
+
 def _par(g: Grid, key: str) -> str:
+    if g.basis == "SSF":
+        return SSF_PARITY[key]
     return "F" if g.basis == "FFF" else SFF_PARITY[key]
 
 
@@ -377,15 +395,15 @@ def nlin_conservative_from_real(g: Grid, ur: list, wr: list | None = None) -> np
         wr = ur
     p = lambda k: _par(g, k)
     n1 = xderiv(g, forward(g, ur[0] * wr[0], p("Vi2")), p("Vi2"))
-    n2 = yderiv(g, forward(g, ur[1] * wr[1], p("Vi2")))
+    n2 = yderiv(g, forward(g, ur[1] * wr[1], p("Vi2")), p("Vi2"))
     n3 = zderiv(g, forward(g, ur[2] * wr[2], p("Vi2")))
     if wr is ur:
         X = forward(g, ur[0] * ur[1], p("VxVy"))
-        n1 = n1 + yderiv(g, X)
+        n1 = n1 + yderiv(g, X, p("VxVy"))
         n2 = n2 + xderiv(g, X, p("VxVy"))
         X = forward(g, ur[1] * ur[2], p("VyVz"))
         n2 = n2 + zderiv(g, X)
-        n3 = n3 + yderiv(g, X)
+        n3 = n3 + yderiv(g, X, p("VyVz"))
         X = forward(g, ur[2] * ur[0], p("VxVz"))
         n1 = n1 + zderiv(g, X)
         n3 = n3 + xderiv(g, X, p("VxVz"))
@@ -432,20 +450,20 @@ def project_rhs(g: Grid, N: np.ndarray) -> np.ndarray:
     Compute_rhs Tadvance_functions.cc:148-191.  SFF parities: div with Vx
     (S -> +Kx), gradient with div parity (C -> -Kx).
     """
-    div = xderiv(g, N[0], _par(g, "Vx")) + yderiv(g, N[1]) + zderiv(g, N[2])
+    div = xderiv(g, N[0], _par(g, "Vx")) + yderiv(g, N[1], _par(g, "Vy")) + zderiv(g, N[2])
     K2 = g.Ksqr()
     with np.errstate(divide="ignore", invalid="ignore"):
         p = div / K2
     p[0, 0, 0] = 0
     n1 = N[0] + xderiv(g, p, _par(g, "div"))
-    n2 = N[1] + yderiv(g, p)
+    n2 = N[1] + yderiv(g, p, _par(g, "div"))
     n3 = N[2] + zderiv(g, p)
     return -np.stack([n1, n2, n3])
 
 
 def max_abs_div(g: Grid, V: np.ndarray) -> float:
     """max |div V| as in Universal::Compute_divergence(field) universal_basic.cc:343-356."""
-    div = xderiv(g, V[0], _par(g, "Vx")) + yderiv(g, V[1]) + zderiv(g, V[2])
+    div = xderiv(g, V[0], _par(g, "Vx")) + yderiv(g, V[1], _par(g, "Vy")) + zderiv(g, V[2])
     return float(np.max(np.abs(div)))
 
 

@@ -206,7 +206,7 @@ static int upload_if_tables(ts_plan* p, double nu, double dt, double** tab) {
     for (int l = 0; l < n[ax]; ++l) {
       int k;
       if (ax == 0) k = g.basis == 0 ? (l <= g.Nx / 2 ? l : l - g.Nx) : l;
-      else if (ax == 1) k = l <= g.Ny / 2 ? l : l - g.Ny;
+      else if (ax == 1) k = g.basis == TS_BASIS_SSF ? l : (l <= g.Ny / 2 ? l : l - g.Ny);
       else k = l;
       const double K = k * g.kf[ax];
       h[l] = exp(-nu * 0.5 * dt * (K * K));
@@ -762,6 +762,83 @@ static int ssf_transforms_only() {
   return TS_ERR_UNSUPPORTED;
 }
 
+// the geometry that makes the x-axis sin/cos kernel transform along y: every
+// x-plane of every component is one "component" of Ny rows x Hz columns
+static Geo y_as_x(const Geo& g) {
+  Geo h = g;
+  h.Nx = g.Ny;
+  h.Ny = 1;
+  h.S = (long long)g.Ny * g.Hz;
+  h.dealias = 0;
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+// SSF fluid step (sin/cos along x and y; sincostr_switch "SCF"), conservative form,
+// unforced: RK4(U,P,F) (RK.cc:91-170) with standalone transforms.  P holds 12
+// components: [0, 3) spectral scratch, [3, 6) real u, [6, 12) real products; the
+// forward z transform writes the products' spectra into [0, 6).
+// ---------------------------------------------------------------------------
+static int ssf_step_supported(ts_plan* p) {
+  if (p->cfg.basis != TS_BASIS_SSF || p->cfg.nlin_form != TS_NLIN_CONSERVATIVE ||
+      p->cfg.force_type != TS_FORCE_NONE) {
+    g_last_error = "the SSF step is the conservative, unforced fluid step";
+    return TS_ERR_UNSUPPORTED;
+  }
+  return ensure_work(p, 3, 12);
+}
+
+static int step_ssf(ts_plan* p, void* U0) {
+  const Geo& g = p->g;
+  const Geo gy = y_as_x(g);
+  const long long cs = g.S * (long long)p->cb;  // bytes of one component
+  char* P = (char*)p->P;
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.Uout = U0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.dt = p->cfg.dt;
+  a.ex = p->eax[0];
+  a.ey = p->eax[1];
+  a.ez = p->eax[2];
+  // x, y sine (1) / cosine (0) letters of Vx = SCF, Vy = CSF, Vz = CCF and of the products
+  // u1u1, u2u2, u3u3 (Vi2 = CCF), u1u2 (VxVy = SSF), u2u3 (VyVz = CSF), u3u1 (VxVz = SCF)
+  const int vx[3] = {1, 0, 0}, vy[3] = {0, 1, 0};
+  const int qx[6] = {0, 0, 0, 1, 0, 1}, qy[6] = {0, 0, 0, 1, 1, 0};
+  const double sy = 1.0 / (2.0 * g.Ny), sx = 1.0 / (2.0 * g.Nx * (double)g.Nz);
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? U0 : p->Ucur;
+    a.stage = stage;
+    {
+      ProfScope ps(p, TS_KCLASS_INV_X);
+      CK(LAUNCH(p, dealias_copy, g, Uin, P, 3, p->st));
+      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_Y_INV);
+      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_Z);
+      CK(LAUNCH(p, z_single, g, +1, P, P + 3 * cs, 3, p->twz, p->st));
+      CK(LAUNCH(p, real_products, P + 3 * cs, P + 6 * cs, 2 * g.S, p->st));
+      CK(LAUNCH(p, z_single, g, -1, P + 6 * cs, P, 6, p->twz, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_Y_FWD);
+      for (int f = 0; f < 6; ++f) CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], sy, p->twqy, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_FWD_X);
+      for (int f = 0; f < 6; ++f) CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], sx, p->twq, p->st));
+      CK(LAUNCH(p, ssf_epi, g, P, a, p->st));
+    }
+  }
+  return TS_OK;
+}
+
 // run fn(device_ptr) on a field that may live on the host
 template <typename Fn>
 static int with_device(ts_plan* p, void** stage, const void* ptr, size_t bytes, bool copy_back, Fn&& fn) {
@@ -778,6 +855,14 @@ extern "C" {
 
 int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   if (!p || !u_hat || nsteps < 0) return TS_ERR_ARG;
+  if (p->cfg.basis == TS_BASIS_SSF) {
+    CKS(ssf_step_supported(p));
+    int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
+      for (int s = 0; s < nsteps; ++s) CKS(step_ssf(p, U));
+      return (int)TS_OK;
+    });
+    return rc;
+  }
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   // a bounded device wait that gave up in an earlier call (read without a sync)
   if (*p->err_h) {
@@ -1140,16 +1225,6 @@ static int x_parity(const ts_plan* p, const char* parity, int* yp = nullptr) {
   return -1;
 }
 
-// the geometry that makes the x-axis sin/cos kernel transform along y: every
-// x-plane of every component is one "component" of Ny rows x Hz columns
-static Geo y_as_x(const Geo& g) {
-  Geo h = g;
-  h.Nx = g.Ny;
-  h.Ny = 1;
-  h.S = (long long)g.Ny * g.Hz;
-  h.dealias = 0;
-  return h;
-}
 
 int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* spec_out, int ncomp) {
   if (!p || !parity || !real_in || !spec_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;

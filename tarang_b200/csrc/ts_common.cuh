@@ -342,7 +342,8 @@ __device__ __forceinline__ int kfft(int l, int N) { return l <= N / 2 ? l : l - 
 __device__ __forceinline__ bool dealias_zero(int mode, int basis, int lx, int ly, int lz, int Nx, int Ny, int Nz) {
   if (mode == 1) {
     bool mx = basis == 0 ? (lx >= Nx / 3 + 1 && lx <= 2 * Nx / 3 - 1) : (lx >= 2 * Nx / 3 + 1);
-    bool my = ly >= Ny / 3 + 1 && ly <= 2 * Ny / 3 - 1;
+    // SSF (sin/cos along y too): ly >= 2Ny/3 + 1 (SSF_pencil_basic.cc:103-106)
+    bool my = basis == 2 ? (ly >= 2 * Ny / 3 + 1) : (ly >= Ny / 3 + 1 && ly <= 2 * Ny / 3 - 1);
     bool mz = lz >= Nz / 3 + 1 && lz <= Nz / 2;
     return mx && my && mz;
   }
@@ -350,7 +351,8 @@ __device__ __forceinline__ bool dealias_zero(int mode, int basis, int lx, int ly
     int kx = basis == 0 ? kfft(lx, Nx) : lx;
     int ky = kfft(ly, Ny);
     bool bx = basis == 0 ? (3 * abs(kx) > Nx) : (3 * kx > 2 * Nx);
-    return bx || (3 * abs(ky) > Ny) || (3 * lz > Nz);
+    bool by = basis == 2 ? (3 * ly > 2 * Ny) : (3 * abs(ky) > Ny);
+    return bx || by || (3 * lz > Nz);
   }
   return false;
 }

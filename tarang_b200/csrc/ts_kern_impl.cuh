@@ -656,6 +656,18 @@ template <> cudaError_t Launch<T>::scalar_epi(const Geo& g, const void* P, const
   return cudaGetLastError();
 }
 
+template <> cudaError_t Launch<T>::real_products(const void* R, void* Q, long long n, cudaStream_t st) {
+  k_real_products<T><<<grid1d(n, 256), 256, 0, st>>>((const T*)R, (T*)Q, n);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::ssf_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st) {
+  k_ssf_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
 template <> cudaError_t Launch<T>::mhd_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st) {
   k_mhd_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
   ++g_launches;

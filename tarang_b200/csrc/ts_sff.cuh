@@ -549,4 +549,69 @@ __global__ void __launch_bounds__(256, 3) k_mhd_epi(const C<T>* __restrict__ P, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// SSF fluid step (sincostr_switch "SCF": Vx = SCF, Vy = CSF, Vz = CCF), elementwise
+// epilogue after the forward transforms of the six products (normalised; parities
+// Vi2 = CCF for u_i u_i, VxVy = SSF, VyVz = CSF, VxVz = SCF; Global.cc:184-191).
+// Derivatives (SSF_pencil_tr.cc): x and y parity S -> +K, C -> -K; z -> i Kz.
+//   N1 = Dx(u1u1) + Dy(u1u2) + Dz(u3u1), N2 = Dy(u2u2) + Dx(u1u2) + Dz(u2u3),
+//   N3 = Dz(u3u3) + Dy(u2u3) + Dx(u3u1)  (compute_diag_offdiag.cc:47-98)
+//   div = Dx^Vx N1 + Dy^Vy N2 + Dz N3, p = div/K^2, N += (Dx^div p, Dy^div p, Dz p), R = -N;
+//   IF-RK4 stage update as the FFF step (RK.cc:91-170); no reality condition.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo g, StageArgs a) {
+  typedef C<T> V;
+  const V* U0 = reinterpret_cast<const V*>(a.U0);
+  V* Uc = reinterpret_cast<V*>(a.Ucur);
+  V* tot = reinterpret_cast<V*>(a.tot);
+  V* Uo = reinterpret_cast<V*>(a.Uout);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const double Kxd = lx * g.kf[0], Kyd = ly * g.kf[1], Kzd = lz * g.kf[2];
+    const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+    V q[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) q[f] = P[f * g.S + e];
+    // x / y derivative of a sine (+K) or cosine (-K) series
+    auto dS = [](T K, V A) { return scale(A, K); };
+    auto dC = [](T K, V A) { return scale(A, -K); };
+    V N1 = add(add(dC(Kx, q[0]), dS(Ky, q[3])), ik(Kz, q[5]));
+    V N2 = add(add(dC(Ky, q[1]), dS(Kx, q[3])), ik(Kz, q[4]));
+    V N3 = add(add(ik(Kz, q[2]), dS(Ky, q[4])), dS(Kx, q[5]));
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    const V div = add(add(dS(Kx, N1), dS(Ky, N2)), ik(Kz, N3));
+    const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+    N1 = add(N1, dC(Kx, pr));
+    N2 = add(N2, dC(Ky, pr));
+    N3 = add(N3, ik(Kz, pr));
+    const V Rv[3] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1)};
+    const double eh = a.ex[lx] * a.ey[ly] * a.ez[lz];
+    const double e1 = eh * eh;
+    const T Eh = (T)eh, E1 = (T)e1;
+    const bool dz = dealias_zero(g.dealias, 2, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const long long o = i * g.S + e;
+      const V R = Rv[i];
+      const V u0 = U0[o];
+      if (a.stage == 1) {
+        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+      } else if (a.stage == 2) {
+        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else if (a.stage == 3) {
+        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else {
+        Uo[o] = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+      }
+    }
+  }
+}
+
 }  // namespace ts

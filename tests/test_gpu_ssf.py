@@ -46,16 +46,63 @@ def test_ssf_transforms_match_oracle(cuda, N, parity, prec):
     assert rel(spec.cpu().numpy(), ref) < tol
 
 
-def test_ssf_plan_offers_transforms_only(cuda):
+def test_ssf_plan_rejects_other_calls(cuda):
     import tarang_b200 as tb
     plan = tb.Plan(32, basis="SSF", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
         plan.energy(u)
     with pytest.raises(tb.TsError):
-        plan.rk4_step(u, 1)
-    with pytest.raises(tb.TsError):
         plan.rk4_step_rbc(u, plan.field(1), 1)
+    with pytest.raises(tb.TsError):
+        tb.Plan(32, basis="SSF", kfactor=KF, nlin_form="rotational")
     real = plan.field(1)
     with pytest.raises(tb.TsError):
         plan.forward(real, plan.field(1), parity="SFF")
+
+
+def ssf_state(g, seed):
+    """a random solenoidal field with the SSF parities (Vx = SCF, Vy = CSF, Vz = CCF)"""
+    rng = np.random.default_rng(seed)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCF", "CSF", "CCF")])
+    return R.project_rhs(g, U) * -1.0  # the projection keeps the solenoidal part
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,dealias", [((16, 16, 16), "reference"), ((32, 16, 32), "none"),
+                                       ((48, 32, 16), "reference"), ((32, 32, 32), "two_thirds")])
+def test_ssf_step_matches_oracle(cuda, N, dealias, prec):
+    import torch
+    import tarang_b200 as tb
+    mode = {"none": 0, "reference": 1, "two_thirds": 2}[dealias]
+    g = R.Grid(N, KF, "SSF")
+    U0 = 0.3 * ssf_state(g, 2)
+    cfg = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=mode, nlin_form="conservative")
+    W = U0.copy()
+    for _ in range(3):
+        W = R.rk4_step(cfg, W)
+    plan = tb.Plan(N, basis="SSF", kfactor=KF, precision=prec, nu=0.01, dt=1e-3, dealias=dealias)
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    u = torch.from_numpy(U0).to(cuda).to(cdt)
+    plan.rk4_step(u, 3)
+    plan.status()
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel(u.cpu().numpy().astype(np.complex128), W) < tol
+
+
+def test_ssf_taylor_green_decays_exactly(cuda):
+    """u = sin x cos y, v = -cos x sin y (Vx = SCF, Vy = CSF): the nonlinear term is a
+    gradient, so the step is the exact viscous decay exp(-2 nu t)."""
+    import torch
+    import tarang_b200 as tb
+    N = (16, 16, 16)
+    g = R.Grid(N, (1.0, 1.0, 1.0), "SSF")
+    x = (np.arange(16) + 0.5) * np.pi / 16
+    z = 2 * np.pi * np.arange(16) / 16
+    X, Y, Z = np.meshgrid(x, x, z, indexing="ij")
+    U0 = np.stack([R.forward(g, np.sin(X) * np.cos(Y), "SCF"), R.forward(g, -np.cos(X) * np.sin(Y), "CSF"),
+                   R.forward(g, np.zeros_like(X), "CCF")])
+    plan = tb.Plan(N, basis="SSF", kfactor=(1.0, 1.0, 1.0), precision="f64", nu=0.05, dt=1e-2)
+    u = torch.from_numpy(U0).to(cuda)
+    plan.rk4_step(u, 5)
+    assert np.max(np.abs(u.cpu().numpy() - U0 * np.exp(-0.05 * 2 * 5e-2))) < 1e-15
