@@ -64,7 +64,7 @@ def tune_plan(plan, reps: int = 3) -> dict | None:
     if TUNE["mode"] == "off":
         return None
     rep = plan.autotune(reps=reps)
-    return {"tuning": rep["tuning"], "rule_ms_per_step": rep["start_ms"], "tuned_ms_per_step": rep["end_ms"]}
+    return {"tuning": rep["tuning"], "confirm": rep["confirm"]}
 
 
 def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
@@ -79,11 +79,8 @@ def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
     tuned = None
     if TUNE["mode"] == "auto":
         rep = ens.autotune(reps=3)
-        tuned = [{"N": gr["N"], "members": gr["members"], "rule_ms": gr["tuning"]["start_ms"],
-                  "tuned_ms": gr["tuning"]["end_ms"],
-                  "variant": [gr["tuning"][c]["variant"] for c in ("x_inv", "y_inv", "z", "y_fwd", "x_fwd")],
-                  "blocks_per_sm": [gr["tuning"][c]["blocks_per_sm"] for c in ("x_inv", "y_inv", "z", "y_fwd", "x_fwd")]}
-                 for gr in rep["groups"]]
+        tuned = [{"N": gr["N"], "members": gr["members"], "confirm": gr["tuning"]["confirm"],
+                  **gr["tuning"]["final"]} for gr in rep["groups"]]
     ens.run(warmup)
     ens.synchronize()
     t0 = time.perf_counter()

@@ -231,7 +231,9 @@ int ts_adjoint_window(ts_plan* plan, const void* u_start, int nsteps, void* lam_
  *   trials, enough steps per trial for about 3 ms), keeps a candidate only when
  *   it is at least 1 % faster.  The caller's fields are not touched; the plan's
  *   work buffers are.  report (may be NULL): a JSON summary of every timing.
- *   The incumbent is re-timed at the start of every class.
+ *   The incumbent is re-timed at the start of every class, and the picks are
+ *   kept only if, timed twice against the rule (interleaved), they are still at
+ *   least 1 % faster ("confirm" and "final" in the report).
  * ts_ensemble_autotune: the same for every size group of an ensemble, timing
  *   whole ensemble steps (one graph launch each, about 30 ms per trial); the
  *   members' states are saved and restored. */

@@ -1687,6 +1687,34 @@ template <typename Measure> int descend(const ts_plan* p, Geo& g, Measure&& meas
     snprintf(buf, sizeof(buf), "], \"variant\": %d, \"blocks_per_sm\": %d}", g.tv[cls], g.tb[cls]);
     js += buf;
   }
+  // confirm against the rule: time both settings twice, interleaved, and keep the
+  // rule unless the picks are at least 1 % faster on the best of the two trials
+  {
+    const Geo tuned = g;
+    Geo rule = g;
+    for (int c = 0; c < TUNE_NCLASS; ++c) rule.tv[c] = rule.tb[c] = 0;
+    double bt = 1e300, br = 1e300;
+    for (int r = 0; r < 2; ++r) {
+      double t = 0;
+      g = tuned;
+      CKS(measure(&t));
+      if (t < bt) bt = t;
+      g = rule;
+      CKS(measure(&t));
+      if (t < br) br = t;
+    }
+    g = bt < 0.99 * br ? tuned : rule;
+    best = bt < 0.99 * br ? bt : br;
+    js += ", \"confirm\": {\"tuned_ms\": ";
+    json_num(js, bt);
+    js += ", \"rule_ms\": ";
+    json_num(js, br);
+    js += bt < 0.99 * br ? ", \"kept\": \"tuned\"}" : ", \"kept\": \"rule\"}";
+    char buf[160];
+    snprintf(buf, sizeof(buf), ", \"final\": {\"variant\": [%d, %d, %d, %d, %d], \"blocks_per_sm\": [%d, %d, %d, %d, %d]}",
+             g.tv[0], g.tv[1], g.tv[2], g.tv[3], g.tv[4], g.tb[0], g.tb[1], g.tb[2], g.tb[3], g.tb[4]);
+    js += buf;
+  }
   js += ", \"end_ms\": ";
   json_num(js, best);
   js += "}";
