@@ -50,7 +50,10 @@ typedef enum {
  * and ts_rk4_step for the conservative, unforced fluid (sincostr_switch "SCF":
  * Vx = SCF, Vy = CSF, Vz = CCF); every other call on an SSF plan returns
  * TS_ERR_UNSUPPORTED. */
-typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1, TS_BASIS_SSF = 2 } ts_basis;
+/* TS_BASIS_SSS (sin/cos along every axis; basis/SSS/pencil) stores real coefficients in
+ * the padded real layout (Nx, Ny, Nz + 2) of each component (the complex buffer viewed
+ * as reals, as SSS_PENCIL does) and offers the transforms (parities [SC][SC][SC]). */
+typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1, TS_BASIS_SSF = 2, TS_BASIS_SSS = 3 } ts_basis;
 typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
 typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;
 typedef enum { TS_DEALIAS_NONE = 0, TS_DEALIAS_REFERENCE_CORNER = 1, TS_DEALIAS_TWO_THIRDS = 2 } ts_dealias;

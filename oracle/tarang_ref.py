@@ -122,19 +122,20 @@ class Grid:
         lx = np.arange(Nx)
         if self.basis == "FFF":
             self.kx = np.where(lx <= Nx // 2, lx, lx - Nx)
-        elif self.basis in ("SFF", "SSF"):
+        elif self.basis in ("SFF", "SSF", "SSS"):
             self.kx = lx.copy()
         else:
             raise ValueError(self.basis)
         ly = np.arange(Ny)
         # SSF: sin/cos along y as well, ky = ly (SSF_pencil_inline.h Get_ky)
-        self.ky = ly.copy() if self.basis == "SSF" else np.where(ly <= Ny // 2, ly, ly - Ny)
-        self.kz = np.arange(Nz // 2 + 1)
+        self.ky = ly.copy() if self.basis in ("SSF", "SSS") else np.where(ly <= Ny // 2, ly, ly - Ny)
+        # SSS: sin/cos along z as well, real coefficients (Nx, Ny, Nz), kz = lz (SSS_pencil_inline.h)
+        self.kz = np.arange(Nz) if self.basis == "SSS" else np.arange(Nz // 2 + 1)
 
     @property
     def shape(self):
         Nx, Ny, Nz = self.N
-        return (Nx, Ny, Nz // 2 + 1)
+        return (Nx, Ny, Nz) if self.basis == "SSS" else (Nx, Ny, Nz // 2 + 1)
 
     @property
     def rshape(self):
@@ -213,6 +214,10 @@ def dealias_mask(g: Grid, mode: int) -> np.ndarray:
     lz = np.arange(Nz // 2 + 1)[None, None, :]
     if mode == DEALIAS_NONE:
         return np.zeros(g.shape, dtype=bool)
+    if mode == DEALIAS_REFERENCE_CORNER and g.basis == "SSS":
+        # SSS_PENCIL::Dealias (SSS_pencil_basic.cc:129-134): lx >= 2Nx/3+1, ly >= 2Ny/3+1, lz >= Nz/3
+        lzr = np.arange(Nz)[None, None, :]
+        return np.broadcast_to((lx >= 2 * Nx // 3 + 1) & (ly >= 2 * Ny // 3 + 1) & (lzr >= Nz // 3), g.shape).copy()
     if mode == DEALIAS_REFERENCE_CORNER:
         if g.basis == "FFF":
             mx = (lx >= Nx // 3 + 1) & (lx <= 2 * Nx // 3 - 1)
@@ -233,8 +238,9 @@ def dealias_mask(g: Grid, mode: int) -> np.ndarray:
             bx = 3 * np.abs(kx) > Nx
         else:
             bx = 3 * kx > 2 * Nx
-        by = (3 * ky > 2 * Ny) if g.basis == "SSF" else (3 * np.abs(ky) > Ny)
-        m = bx | by | (3 * kz > Nz)
+        by = (3 * ky > 2 * Ny) if g.basis in ("SSF", "SSS") else (3 * np.abs(ky) > Ny)
+        bz = (3 * kz > 2 * Nz) if g.basis == "SSS" else (3 * kz > Nz)
+        m = bx | by | bz
         return np.broadcast_to(m, g.shape).copy()
     raise ValueError(mode)
 
@@ -256,8 +262,8 @@ def reality_fix(g: Grid, A: np.ndarray) -> np.ndarray:
     """
     Nx, Ny, Nz = g.N
     B = A.copy()
-    if g.basis == "SSF":
-        return B  # SSF_pencil_basic.cc:127-130: nothing to do
+    if g.basis in ("SSF", "SSS"):
+        return B  # SSF_pencil_basic.cc:127-130 (and SSS): nothing to do
     plane = A[:, :, 0].copy()
     iy_minus = (-g.ky) % Ny  # Get_iy(-ky)
     if g.basis == "FFF":
@@ -320,6 +326,10 @@ def forward(g: Grid, ur: np.ndarray, parity: str = "F") -> np.ndarray:
         # SSF_pencil_tr.cc:43-51: sin/cos along x and y by the parity's first two letters
         Bz = sfft.rfft(ur, axis=2, norm="forward", workers=WORKERS)
         return _x_forward_sincos(g, _x_forward_sincos(g, Bz, parity[1], axis=1), parity[0])
+    if g.basis == "SSS":
+        # SSS_pencil_tr.cc: sin/cos along every axis, real coefficients
+        B = _x_forward_sincos(g, ur, parity[2], axis=2)
+        return _x_forward_sincos(g, _x_forward_sincos(g, B, parity[1], axis=1), parity[0])
     Byz = sfft.rfftn(ur, axes=(1, 2), norm="forward", workers=WORKERS)
     return _x_forward_sincos(g, Byz, parity)
 
@@ -332,6 +342,9 @@ def inverse(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
     if g.basis == "SSF":
         Bxy = _x_inverse_sincos(g, _x_inverse_sincos(g, A, parity[0]), parity[1], axis=1)
         return sfft.irfft(Bxy, n=Nz, axis=2, norm="forward", workers=WORKERS)
+    if g.basis == "SSS":
+        Bxy = _x_inverse_sincos(g, _x_inverse_sincos(g, A, parity[0]), parity[1], axis=1)
+        return _x_inverse_sincos(g, Bxy, parity[2], axis=2)
     Bx = _x_inverse_sincos(g, A, parity)
     return sfft.irfftn(Bx, s=(Ny, Nz), axes=(1, 2), norm="forward", workers=WORKERS)
 
@@ -351,13 +364,16 @@ def xderiv(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
 def yderiv(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
     """i Ky; SSF (SSF_PENCIL::Yderiv): y parity S -> +Ky, C -> -Ky."""
     _, Ky, _ = g.K()
-    if g.basis == "SSF":
+    if g.basis in ("SSF", "SSS"):
         return (Ky if parity[1] == "S" else -Ky) * A
     return (1j * Ky) * A
 
 
-def zderiv(g: Grid, A: np.ndarray) -> np.ndarray:
+def zderiv(g: Grid, A: np.ndarray, parity: str = "F") -> np.ndarray:
+    """i Kz; SSS (SSS_PENCIL::Zderiv, SSS_pencil_tr.cc:171-189): z parity S -> +Kz, C -> -Kz."""
     _, _, Kz = g.K()
+    if g.basis == "SSS":
+        return (Kz if parity[2] == "S" else -Kz) * A
     return (1j * Kz) * A
 
 
@@ -371,7 +387,14 @@ SSF_PARITY = {"Vx": "SCF", "Vy": "CSF", "Vz": "CCF", "div": "CCF", "Vi2": "CCF",
               "VyVz": "CSF"}
 
 
+# SSS parity strings for sincostr_switch "SCC" (global/Global.cc:221-228)
+SSS_PARITY = {"Vx": "SCC", "Vy": "CSC", "Vz": "CCS", "div": "CCC", "Vi2": "CCC", "VxVy": "SSC", "VxVz": "SCS",
+              "VyVz": "CSS"}
+
+
 def _par(g: Grid, key: str) -> str:
+    if g.basis == "SSS":
+        return SSS_PARITY[key]
     if g.basis == "SSF":
         return SSF_PARITY[key]
     return "F" if g.basis == "FFF" else SFF_PARITY[key]
@@ -396,16 +419,16 @@ def nlin_conservative_from_real(g: Grid, ur: list, wr: list | None = None) -> np
     p = lambda k: _par(g, k)
     n1 = xderiv(g, forward(g, ur[0] * wr[0], p("Vi2")), p("Vi2"))
     n2 = yderiv(g, forward(g, ur[1] * wr[1], p("Vi2")), p("Vi2"))
-    n3 = zderiv(g, forward(g, ur[2] * wr[2], p("Vi2")))
+    n3 = zderiv(g, forward(g, ur[2] * wr[2], p("Vi2")), p("Vi2"))
     if wr is ur:
         X = forward(g, ur[0] * ur[1], p("VxVy"))
         n1 = n1 + yderiv(g, X, p("VxVy"))
         n2 = n2 + xderiv(g, X, p("VxVy"))
         X = forward(g, ur[1] * ur[2], p("VyVz"))
-        n2 = n2 + zderiv(g, X)
+        n2 = n2 + zderiv(g, X, p("VyVz"))
         n3 = n3 + yderiv(g, X, p("VyVz"))
         X = forward(g, ur[2] * ur[0], p("VxVz"))
-        n1 = n1 + zderiv(g, X)
+        n1 = n1 + zderiv(g, X, p("VxVz"))
         n3 = n3 + xderiv(g, X, p("VxVz"))
     else:
         # giver form: nlin_i = sum_j D_j F[u_j w_i]
@@ -450,20 +473,20 @@ def project_rhs(g: Grid, N: np.ndarray) -> np.ndarray:
     Compute_rhs Tadvance_functions.cc:148-191.  SFF parities: div with Vx
     (S -> +Kx), gradient with div parity (C -> -Kx).
     """
-    div = xderiv(g, N[0], _par(g, "Vx")) + yderiv(g, N[1], _par(g, "Vy")) + zderiv(g, N[2])
+    div = xderiv(g, N[0], _par(g, "Vx")) + yderiv(g, N[1], _par(g, "Vy")) + zderiv(g, N[2], _par(g, "Vz"))
     K2 = g.Ksqr()
     with np.errstate(divide="ignore", invalid="ignore"):
         p = div / K2
     p[0, 0, 0] = 0
     n1 = N[0] + xderiv(g, p, _par(g, "div"))
     n2 = N[1] + yderiv(g, p, _par(g, "div"))
-    n3 = N[2] + zderiv(g, p)
+    n3 = N[2] + zderiv(g, p, _par(g, "div"))
     return -np.stack([n1, n2, n3])
 
 
 def max_abs_div(g: Grid, V: np.ndarray) -> float:
     """max |div V| as in Universal::Compute_divergence(field) universal_basic.cc:343-356."""
-    div = xderiv(g, V[0], _par(g, "Vx")) + yderiv(g, V[1], _par(g, "Vy")) + zderiv(g, V[2])
+    div = xderiv(g, V[0], _par(g, "Vx")) + yderiv(g, V[1], _par(g, "Vy")) + zderiv(g, V[2], _par(g, "Vz"))
     return float(np.max(np.abs(div)))
 
 

@@ -14,7 +14,7 @@ _LIB_PATH = Path(__file__).resolve().parent / "libtarang_b200.so"
 TS_OK, TS_ERR_ARG, TS_ERR_CUDA, TS_ERR_NAN, TS_ERR_TIMEOUT, TS_ERR_UNSUPPORTED, TS_ERR_NOMEM = range(7)
 STATUS_NAMES = {0: "TS_OK", 1: "TS_ERR_ARG", 2: "TS_ERR_CUDA", 3: "TS_ERR_NAN", 4: "TS_ERR_TIMEOUT",
                 5: "TS_ERR_UNSUPPORTED", 6: "TS_ERR_NOMEM"}
-TS_BASIS_FFF, TS_BASIS_SFF, TS_BASIS_SSF = 0, 1, 2
+TS_BASIS_FFF, TS_BASIS_SFF, TS_BASIS_SSF, TS_BASIS_SSS = 0, 1, 2, 3
 TS_F64, TS_F32 = 0, 1
 TS_NLIN_CONSERVATIVE, TS_NLIN_ROTATIONAL = 0, 1
 TS_DEALIAS_NONE, TS_DEALIAS_REFERENCE_CORNER, TS_DEALIAS_TWO_THIRDS = 0, 1, 2

@@ -71,7 +71,8 @@ struct ts_plan {
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
   double* eaxT[3] = {nullptr, nullptr, nullptr}; // per-axis exp(-kappa dt K_i^2 / 2) (SFF scalar)
   void* twq = nullptr;      // SFF, SSF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
-  void* twqy = nullptr;     // SSF: exp(-2 pi i j / (4 Ny)), j < 4 Ny
+  void* twqy = nullptr;     // SSF, SSS: exp(-2 pi i j / (4 Ny)), j < 4 Ny
+  void* twqz = nullptr;     // SSS: exp(-2 pi i j / (4 Nz)), j < 4 Nz
   // per-kernel-class CUDA event timing (ts_profile_*)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -249,7 +250,7 @@ const char* ts_last_error(void) { return g_last_error.c_str(); }
 int ts_plan_destroy(ts_plan* p) {
   if (!p) return TS_ERR_ARG;
   void* bufs[] = {p->Ucur, p->tot, p->P, p->twx, p->twy, p->twz, p->fcube, p->esup, p->hsup, p->mis_d, p->dscr,
-                  p->stage_u, p->stage_t, p->stage_b, p->twqy};
+                  p->stage_u, p->stage_t, p->stage_b, p->twqy, p->twqz};
   for (void* b : bufs)
     if (b) cudaFree(b);
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
@@ -275,13 +276,19 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
       return TS_ERR_ARG;
     }
   }
-  if (cfg->basis != TS_BASIS_FFF && cfg->basis != TS_BASIS_SFF && cfg->basis != TS_BASIS_SSF) return TS_ERR_ARG;
+  if (cfg->basis != TS_BASIS_FFF && cfg->basis != TS_BASIS_SFF && cfg->basis != TS_BASIS_SSF &&
+      cfg->basis != TS_BASIS_SSS)
+    return TS_ERR_ARG;
   if (cfg->precision != TS_F64 && cfg->precision != TS_F32) return TS_ERR_ARG;
   if (cfg->dealias_mode < 0 || cfg->dealias_mode > 2) return TS_ERR_ARG;
   if (cfg->nlin_form != TS_NLIN_CONSERVATIVE && cfg->nlin_form != TS_NLIN_ROTATIONAL) return TS_ERR_ARG;
   if (cfg->basis != TS_BASIS_FFF && cfg->nlin_form == TS_NLIN_ROTATIONAL) return TS_ERR_UNSUPPORTED;
-  if (cfg->basis == TS_BASIS_SSF && (cfg->N[0] > 512 || cfg->N[1] > 512)) {
-    g_last_error = "SSF supports Nx, Ny <= 512";
+  if ((cfg->basis == TS_BASIS_SSF || cfg->basis == TS_BASIS_SSS) && (cfg->N[0] > 512 || cfg->N[1] > 512)) {
+    g_last_error = "SSF and SSS support Nx, Ny <= 512";
+    return TS_ERR_UNSUPPORTED;
+  }
+  if (cfg->basis == TS_BASIS_SSS && (cfg->N[2] % 3 == 0)) {
+    g_last_error = "SSS needs a power-of-two Nz";
     return TS_ERR_UNSUPPORTED;
   }
   ts_plan* p = new ts_plan();
@@ -314,7 +321,8 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   };
   // SFF (Boussinesq): stage / accumulator fields carry T as a fourth component,
   // and the z pass makes nine products
-  const int ncs = cfg->basis == TS_BASIS_SFF ? 4 : 3, nps = cfg->basis == TS_BASIS_SFF ? 9 : 6;
+  const int ncs = cfg->basis == TS_BASIS_SFF ? 4 : 3,
+            nps = cfg->basis == TS_BASIS_SFF ? 9 : (cfg->basis == TS_BASIS_SSS ? 12 : 6);
   if (cfg->basis == TS_BASIS_SFF && g.Nx > 512) {
     g_last_error = "SFF supports Nx <= 512";
     ts_plan_destroy(p);
@@ -382,7 +390,12 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   CKP(upload_if_tables(p, cfg->nu, cfg->dt, p->eax));
   // the scalar's factors: the SFF Boussinesq step and the FFF passive-scalar step
   CKP(upload_if_tables(p, cfg->kappa, cfg->dt, p->eaxT));
-  if (cfg->basis == TS_BASIS_SSF) {
+  if (cfg->basis == TS_BASIS_SSS) {
+    // sin/cos along z: the 4 Nz quarter-step table
+    if (p->prec) CKP(upload_twiddles<float>(4 * g.Nz, &p->twqz));
+    else CKP(upload_twiddles<double>(4 * g.Nz, &p->twqz));
+  }
+  if (cfg->basis == TS_BASIS_SSF || cfg->basis == TS_BASIS_SSS) {
     // sin/cos along y: the 4 Ny quarter-step table
     if (p->prec) CKP(upload_twiddles<float>(4 * g.Ny, &p->twqy));
     else CKP(upload_twiddles<double>(4 * g.Ny, &p->twqy));
@@ -758,7 +771,7 @@ static int step_mhd_fff(ts_plan* p, void* U0, void* B0) {
 
 // SSF plans offer the transforms only
 static int ssf_transforms_only() {
-  g_last_error = "SSF plans offer ts_fft_forward / ts_fft_inverse only";
+  g_last_error = "SSF plans offer the transforms and ts_rk4_step, SSS plans the transforms only";
   return TS_ERR_UNSUPPORTED;
 }
 
@@ -1018,7 +1031,7 @@ int ts_init_temperature_perturbation(ts_plan* p, double amp, double kmax, uint64
 }
 
 int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !nlin_hat) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   const size_t bytes = 3 * p->g.S * p->cb;
@@ -1042,7 +1055,7 @@ int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
 }
 
 int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || !energy || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
   return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
@@ -1054,7 +1067,7 @@ int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
 }
 
 int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !max_div) return TS_ERR_ARG;
   return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, false, [&](void* U) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
@@ -1066,7 +1079,7 @@ int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
 }
 
 int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int n_shells) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || !Ek || ncomp < 1 || ncomp > 3 || n_shells < 1) return TS_ERR_ARG;
   const int nsh = p->nshells;
   return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
@@ -1089,7 +1102,7 @@ int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int 
 
 int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, double* sums, double* counts,
                   int n_shells) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || ncomp < 1 || ncomp > 3 || n_shells < 1 || (!sums && !counts)) return TS_ERR_ARG;
   if (!is_device_ptr(a_hat) || (b_hat && !is_device_ptr(b_hat))) {
     g_last_error = "ts_shell_sums: device pointers required";
@@ -1110,7 +1123,7 @@ int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, d
 }
 
 int ts_force_field(ts_plan* p, const void* u_hat, void* f_hat) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !f_hat) return TS_ERR_ARG;
   if (p->cfg.force_type != TS_FORCE_CARATI_ENERGY_SUPPLY) {
     g_last_error = "ts_force_field: the plan has no Carati forcing";
@@ -1127,7 +1140,7 @@ int ts_force_field(ts_plan* p, const void* u_hat, void* f_hat) {
 }
 
 int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, double* Pi) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   for (int i = 1; i < n_radii; ++i)
@@ -1158,7 +1171,7 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
 }
 
 int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !T_hat || !Nu) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
   if (!is_device_ptr(u_hat) || !is_device_ptr(T_hat)) return TS_ERR_ARG;
@@ -1173,7 +1186,7 @@ int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
 
 int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed, double target_energy,
                             void* u_hat) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !E_ic || n < 1 || !u_hat) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
@@ -1209,9 +1222,21 @@ int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed
 // sincostr_switch entries (global/Global.cc:137-145).  Returns -1 if invalid.
 // x parity: 0 Fourier (FFF), 1 sine, 2 cosine; *yp: the y parity of an SSF plan
 // (1 sine, 2 cosine; 0 Fourier otherwise)
-static int x_parity(const ts_plan* p, const char* parity, int* yp = nullptr) {
+static int x_parity(const ts_plan* p, const char* parity, int* yp = nullptr, int* zp = nullptr) {
   if (yp) *yp = 0;
+  if (zp) *zp = 0;
   if (p->cfg.basis == TS_BASIS_FFF) return strcmp(parity, "FFF") == 0 ? 0 : -1;
+  if (p->cfg.basis == TS_BASIS_SSS) {
+    if (strlen(parity) != 3) return -1;
+    int l[3];
+    for (int i = 0; i < 3; ++i) {
+      l[i] = parity[i] == 'S' ? 1 : (parity[i] == 'C' ? 2 : -1);
+      if (l[i] < 0) return -1;
+    }
+    if (yp) *yp = l[1];
+    if (zp) *zp = l[2];
+    return l[0];
+  }
   if (p->cfg.basis == TS_BASIS_SSF) {
     if (strlen(parity) != 3 || parity[2] != 'F') return -1;
     const int x = parity[0] == 'S' ? 1 : (parity[0] == 'C' ? 2 : -1);
@@ -1228,14 +1253,27 @@ static int x_parity(const ts_plan* p, const char* parity, int* yp = nullptr) {
 
 int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* spec_out, int ncomp) {
   if (!p || !parity || !real_in || !spec_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  int yp = 0;
-  const int xp = x_parity(p, parity, &yp);
+  int yp = 0, zp = 0;
+  const int xp = x_parity(p, parity, &yp, &zp);
   if (xp < 0) {
-    g_last_error = "parity must be \"FFF\" (FFF plan), \"SFF\" / \"CFF\" (SFF plan) or [SC][SC]F (SSF plan)";
+    g_last_error = "parity must be \"FFF\" (FFF plan), \"SFF\" / \"CFF\" (SFF plan), [SC][SC]F (SSF plan) or "
+                   "[SC][SC][SC] (SSS plan)";
     return TS_ERR_ARG;
   }
   if (!is_device_ptr(real_in) || !is_device_ptr(spec_out)) return TS_ERR_ARG;
   const Geo& g = p->g;
+  if (zp) {
+    // SSS: sin/cos / (2 Nz) along z on the real lines, then y and x on the coefficient
+    // pairs viewed as complex (each pass acts on both reals of a pair)
+    const long long cs = g.S * (long long)p->cb, nl = (long long)ncomp * g.Nx * g.Ny;
+    char* P = (char*)p->P;
+    CK(LAUNCH(p, sss_zperm_fwd, real_in, P, nl, g.Nz, zp == 1, p->st));
+    CK(LAUNCH(p, z_single, g, -1, P, P + 3 * cs, ncomp, p->twz, p->st));
+    CK(LAUNCH(p, sss_zpost_fwd, P + 3 * cs, spec_out, nl, g.Nz, zp == 1, 1.0 / (2.0 * g.Nz), p->twqz, p->st));
+    CK(LAUNCH(p, sff_x, y_as_x(g), -1, spec_out, ncomp * g.Nx, yp == 1, 1.0 / (2.0 * g.Ny), p->twqy, p->st));
+    CK(LAUNCH(p, sff_x, g, -1, spec_out, ncomp, xp == 1, 1.0 / (2.0 * g.Nx), p->twq, p->st));
+    return TS_OK;
+  }
   if (yp) {
     // SSF (SSF_pencil_tr.cc:43-51): z Fourier, then sin/cos / (2 Ny) along y, sin/cos
     // / (2 Nx) along x with the z normalisation
@@ -1258,16 +1296,27 @@ int ts_fft_forward(ts_plan* p, const char* parity, const void* real_in, void* sp
 
 int ts_fft_inverse(ts_plan* p, const char* parity, const void* spec_in, void* real_out, int ncomp) {
   if (!p || !parity || !spec_in || !real_out || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  int yp = 0;
-  const int xp = x_parity(p, parity, &yp);
+  int yp = 0, zp = 0;
+  const int xp = x_parity(p, parity, &yp, &zp);
   if (xp < 0) {
-    g_last_error = "parity must be \"FFF\" (FFF plan), \"SFF\" / \"CFF\" (SFF plan) or [SC][SC]F (SSF plan)";
+    g_last_error = "parity must be \"FFF\" (FFF plan), \"SFF\" / \"CFF\" (SFF plan), [SC][SC]F (SSF plan) or "
+                   "[SC][SC][SC] (SSS plan)";
     return TS_ERR_ARG;
   }
   if (!is_device_ptr(spec_in) || !is_device_ptr(real_out)) return TS_ERR_ARG;
   const Geo& g = p->g;
   // the reference copies the input to X_transform first (FFF_pencil_tr.cc:59)
   CK(cudaMemcpyAsync(p->P, spec_in, ncomp * g.S * p->cb, cudaMemcpyDeviceToDevice, p->st));
+  if (zp) {
+    const long long cs = g.S * (long long)p->cb, nl = (long long)ncomp * g.Nx * g.Ny;
+    char* P = (char*)p->P;
+    CK(LAUNCH(p, sff_x, g, +1, P, ncomp, xp == 1, 1.0, p->twq, p->st));
+    CK(LAUNCH(p, sff_x, y_as_x(g), +1, P, ncomp * g.Nx, yp == 1, 1.0, p->twqy, p->st));
+    CK(LAUNCH(p, sss_zpre_inv, P, P + 3 * cs, nl, g.Nz, zp == 1, p->twqz, p->st));
+    CK(LAUNCH(p, z_single, g, +1, P + 3 * cs, P + 6 * cs, ncomp, p->twz, p->st));
+    CK(LAUNCH(p, sss_zperm_inv, P + 6 * cs, real_out, nl, g.Nz, zp == 1, p->st));
+    return TS_OK;
+  }
   if (yp) {
     CK(LAUNCH(p, sff_x, g, +1, p->P, ncomp, xp == 1, 1.0, p->twq, p->st));
     CK(LAUNCH(p, sff_x, y_as_x(g), +1, p->P, ncomp * g.Nx, yp == 1, 1.0, p->twqy, p->st));
@@ -1784,7 +1833,7 @@ int ts_plan_set_tuning(ts_plan* p, const ts_tuning* t) {
 }
 
 int ts_plan_autotune(ts_plan* p, int reps, char* report, size_t report_len) {
-  if (p && p->cfg.basis == TS_BASIS_SSF) return ssf_transforms_only();
+  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || reps < 1) return TS_ERR_ARG;
   const bool sff = p->cfg.basis == TS_BASIS_SFF;
   const size_t bu = 3 * (size_t)p->g.S * p->cb, bt = (size_t)p->g.S * p->cb;

@@ -656,6 +656,33 @@ template <> cudaError_t Launch<T>::scalar_epi(const Geo& g, const void* P, const
   return cudaGetLastError();
 }
 
+template <> cudaError_t Launch<T>::sss_zperm_fwd(const void* u, void* v, long long nlines, int N, int sine,
+                                                cudaStream_t st) {
+  k_sss_zperm_fwd<T><<<grid1d(nlines * (N + 2), 256), 256, 0, st>>>((const T*)u, (T*)v, nlines, N, sine);
+  ++g_launches;
+  return cudaGetLastError();
+}
+template <> cudaError_t Launch<T>::sss_zpost_fwd(const void* Z, void* c, long long nlines, int N, int sine, double scl,
+                                                const void* tq, cudaStream_t st) {
+  k_sss_zpost_fwd<T><<<grid1d(nlines * (N + 2), 256), 256, 0, st>>>((const V*)Z, (T*)c, nlines, N, sine, scl,
+                                                                     (const V*)tq);
+  ++g_launches;
+  return cudaGetLastError();
+}
+template <> cudaError_t Launch<T>::sss_zpre_inv(const void* c, void* Vout, long long nlines, int N, int sine,
+                                               const void* tq, cudaStream_t st) {
+  k_sss_zpre_inv<T><<<grid1d(nlines * (N / 2 + 1), 256), 256, 0, st>>>((const T*)c, (V*)Vout, nlines, N, sine,
+                                                                        (const V*)tq);
+  ++g_launches;
+  return cudaGetLastError();
+}
+template <> cudaError_t Launch<T>::sss_zperm_inv(const void* v, void* u, long long nlines, int N, int sine,
+                                                cudaStream_t st) {
+  k_sss_zperm_inv<T><<<grid1d(nlines * (N + 2), 256), 256, 0, st>>>((const T*)v, (T*)u, nlines, N, sine);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
 template <> cudaError_t Launch<T>::real_products(const void* R, void* Q, long long n, cudaStream_t st) {
   k_real_products<T><<<grid1d(n, 256), 256, 0, st>>>((const T*)R, (T*)Q, n);
   ++g_launches;

@@ -44,6 +44,13 @@ template <typename T> struct Launch {
                            cudaStream_t st);
   // FFF passive scalar: elementwise epilogue of the nine x-transformed products in P
   static cudaError_t scalar_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
+  // SSS z sin/cos helpers on nlines lines of N reals (padded to N + 2)
+  static cudaError_t sss_zperm_fwd(const void* u, void* v, long long nlines, int N, int sine, cudaStream_t st);
+  static cudaError_t sss_zpost_fwd(const void* Z, void* c, long long nlines, int N, int sine, double scl,
+                                   const void* tq, cudaStream_t st);
+  static cudaError_t sss_zpre_inv(const void* c, void* Vout, long long nlines, int N, int sine, const void* tq,
+                                  cudaStream_t st);
+  static cudaError_t sss_zperm_inv(const void* v, void* u, long long nlines, int N, int sine, cudaStream_t st);
   // six products u_i u_j of three real fields (n reals each)
   static cudaError_t real_products(const void* R, void* Q, long long n, cudaStream_t st);
   // SSF fluid step: elementwise epilogue of the six forward-transformed products in P

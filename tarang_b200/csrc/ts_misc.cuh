@@ -416,4 +416,86 @@ __global__ void __launch_bounds__(256) k_real_products(const T* __restrict__ R, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// SSS basis: sine/cosine transforms along z of real data (z lines contiguous, the
+// padded real layout of N + 2 values per line).  Same algorithm as the x / y
+// passes (one N-point FFT per line of the reordered sequence v), with the FFT
+// done by the z real-to-complex / complex-to-real kernels and the reordering and
+// the quarter-step twiddles e^{-i pi m / 2N} (tq, 4N entries) in these kernels.
+// ---------------------------------------------------------------------------
+// v_k = u_{2k} (k < N/2), +-u_{2(N-1-k)+1} (k >= N/2; minus for the sine series)
+template <typename T>
+__global__ void k_sss_zperm_fwd(const T* __restrict__ u, T* __restrict__ v, long long nlines, int N, int sine) {
+  const long long n = nlines * (N + 2);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long l = e / (N + 2);
+    const int k = (int)(e % (N + 2));
+    const T* ul = u + l * (N + 2);
+    T x = 0;
+    if (k < N / 2) x = ul[2 * k];
+    else if (k < N) x = sine ? -ul[2 * (N - 1 - k) + 1] : ul[2 * (N - 1 - k) + 1];
+    v[e] = x;
+  }
+}
+// real coefficients from the half spectrum Z of v: c_m = 2 scl Re(w_m Z_m) (cosine),
+// -2 scl Im(w_m Z_m) (sine), Z_m = conj(Z_{N-m}) above N/2
+template <typename T>
+__global__ void k_sss_zpost_fwd(const C<T>* __restrict__ Z, T* __restrict__ c, long long nlines, int N, int sine,
+                                double scl, const C<T>* __restrict__ tq) {
+  typedef C<T> V;
+  const int H = N / 2 + 1;
+  const long long n = nlines * (N + 2);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long l = e / (N + 2);
+    const int m = (int)(e % (N + 2));
+    T out = 0;
+    if (m < N) {
+      const V* Zl = Z + l * H;
+      const V zm = m <= N / 2 ? Zl[m] : conjg(Zl[N - m]);
+      const V t = mul(tq[m], zm);
+      out = sine ? (T)(-2.0 * scl) * t.y : (T)(2.0 * scl) * t.x;
+    }
+    c[e] = out;
+  }
+}
+// half spectrum V of the inverse: V_m = conj(w_m) (c_m - i c_{N-m}) (cosine, V_0 = c_0),
+// conj(w_m) (s_{N-m} - i s_m) (sine, V_0 = 0); c_N = s_N = 0
+template <typename T>
+__global__ void k_sss_zpre_inv(const T* __restrict__ c, C<T>* __restrict__ Vout, long long nlines, int N, int sine,
+                               const C<T>* __restrict__ tq) {
+  typedef C<T> V;
+  const int H = N / 2 + 1;
+  const long long n = nlines * H;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long l = e / H;
+    const int m = (int)(e % H);
+    const T* cl = c + l * (N + 2);
+    V z;
+    if (m == 0) {
+      z = mk<V>(sine ? (T)0 : cl[0], 0);
+    } else {
+      const T a = sine ? cl[N - m] : cl[m], b = sine ? cl[m] : cl[N - m];
+      z = mul(conjg(tq[m]), mk<V>(a, -b));
+    }
+    Vout[e] = z;
+  }
+}
+// u_{2k} = v_k, u_{2k+1} = v_{N-1-k}; the sine series negates the odd points
+template <typename T>
+__global__ void k_sss_zperm_inv(const T* __restrict__ v, T* __restrict__ u, long long nlines, int N, int sine) {
+  const long long n = nlines * (N + 2);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const long long l = e / (N + 2);
+    const int q = (int)(e % (N + 2));
+    T x = 0;
+    if (q < N) {
+      const int h = q >> 1;  // (q - 1) / 2 for odd q, q / 2 for even q
+      const int k = (q & 1) ? N - 1 - h : h;
+      x = v[l * (N + 2) + k];
+      if (sine && (q & 1)) x = -x;
+    }
+    u[e] = x;
+  }
+}
+
 }  // namespace ts

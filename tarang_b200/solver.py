@@ -81,7 +81,7 @@ class Plan:
         self.N = tuple(int(n) for n in N)
         c = L.TsConfig()
         self.lib.ts_config_default(ctypes.byref(c))
-        c.basis = {"FFF": L.TS_BASIS_FFF, "SFF": L.TS_BASIS_SFF, "SSF": L.TS_BASIS_SSF}[basis]
+        c.basis = {"FFF": L.TS_BASIS_FFF, "SFF": L.TS_BASIS_SFF, "SSF": L.TS_BASIS_SSF, "SSS": L.TS_BASIS_SSS}[basis]
         for i in range(3):
             c.N[i] = self.N[i]
             c.kfactor[i] = float(kfactor[i])
