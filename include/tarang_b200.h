@@ -52,7 +52,9 @@ typedef enum {
  * TS_ERR_UNSUPPORTED. */
 /* TS_BASIS_SSS (sin/cos along every axis; basis/SSS/pencil) stores real coefficients in
  * the padded real layout (Nx, Ny, Nz + 2) of each component (the complex buffer viewed
- * as reals, as SSS_PENCIL does) and offers the transforms (parities [SC][SC][SC]). */
+ * as reals, as SSS_PENCIL does) and offers the transforms (parities [SC][SC][SC]) and
+ * ts_rk4_step for the conservative, unforced fluid (sincostr_switch "SCC": Vx = SCC,
+ * Vy = CSC, Vz = CCS). */
 typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1, TS_BASIS_SSF = 2, TS_BASIS_SSS = 3 } ts_basis;
 typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
 typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;

@@ -201,13 +201,14 @@ static int ensure_stage(void** buf, size_t bytes) {
 // axes, exp(-nu dt/2 Kx^2) exp(-nu dt/2 Ky^2) exp(-nu dt/2 Kz^2) (FP64)
 static int upload_if_tables(ts_plan* p, double nu, double dt, double** tab) {
   const Geo& g = p->g;
-  const int n[3] = {g.Nx, g.Ny, g.Hz};
+  // SSS: real z coefficients kz = lz < Nz
+  const int n[3] = {g.Nx, g.Ny, g.basis == TS_BASIS_SSS ? g.Nz : g.Hz};
   for (int ax = 0; ax < 3; ++ax) {
     std::vector<double> h(n[ax]);
     for (int l = 0; l < n[ax]; ++l) {
       int k;
       if (ax == 0) k = g.basis == 0 ? (l <= g.Nx / 2 ? l : l - g.Nx) : l;
-      else if (ax == 1) k = g.basis == TS_BASIS_SSF ? l : (l <= g.Ny / 2 ? l : l - g.Ny);
+      else if (ax == 1) k = g.basis >= TS_BASIS_SSF ? l : (l <= g.Ny / 2 ? l : l - g.Ny);
       else k = l;
       const double K = k * g.kf[ax];
       h[l] = exp(-nu * 0.5 * dt * (K * K));
@@ -771,7 +772,7 @@ static int step_mhd_fff(ts_plan* p, void* U0, void* B0) {
 
 // SSF plans offer the transforms only
 static int ssf_transforms_only() {
-  g_last_error = "SSF plans offer the transforms and ts_rk4_step, SSS plans the transforms only";
+  g_last_error = "SSF and SSS plans offer the transforms and ts_rk4_step only";
   return TS_ERR_UNSUPPORTED;
 }
 
@@ -852,6 +853,81 @@ static int step_ssf(ts_plan* p, void* U0) {
   return TS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// SSS fluid step (sin/cos along every axis; sincostr_switch "SCC"), conservative,
+// unforced, on real coefficients.  P holds 12 components: [0, 6) the coefficient
+// scratch of the inverse and then the six products, [6] and [7] per-line scratch
+// of the z passes, [9, 12) the real velocity.
+// ---------------------------------------------------------------------------
+static int sss_step_supported(ts_plan* p) {
+  if (p->cfg.basis != TS_BASIS_SSS || p->cfg.nlin_form != TS_NLIN_CONSERVATIVE ||
+      p->cfg.force_type != TS_FORCE_NONE) {
+    g_last_error = "the SSS step is the conservative, unforced fluid step";
+    return TS_ERR_UNSUPPORTED;
+  }
+  return ensure_work(p, 3, 12);
+}
+
+static int step_sss(ts_plan* p, void* U0) {
+  const Geo& g = p->g;
+  const Geo gy = y_as_x(g);
+  const long long cs = g.S * (long long)p->cb, nl = (long long)g.Nx * g.Ny;
+  char* P = (char*)p->P;
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.Uout = U0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.dt = p->cfg.dt;
+  a.ex = p->eax[0];
+  a.ey = p->eax[1];
+  a.ez = p->eax[2];
+  // sine (1) / cosine (0) letters: Vx = SCC, Vy = CSC, Vz = CCS; products u1u1, u2u2,
+  // u3u3 (CCC), u1u2 (SSC), u2u3 (CSS), u3u1 (SCS)
+  const int vx[3] = {1, 0, 0}, vy[3] = {0, 1, 0}, vz[3] = {0, 0, 1};
+  const int qx[6] = {0, 0, 0, 1, 0, 1}, qy[6] = {0, 0, 0, 1, 1, 0}, qz[6] = {0, 0, 0, 0, 1, 1};
+  for (int stage = 1; stage <= 4; ++stage) {
+    const void* Uin = stage == 1 ? U0 : p->Ucur;
+    a.stage = stage;
+    {
+      ProfScope ps(p, TS_KCLASS_INV_X);
+      CK(LAUNCH(p, sss_dealias_copy, g, Uin, P, 3, p->st));
+      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_Y_INV);
+      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_Z);
+      for (int c = 0; c < 3; ++c) {
+        CK(LAUNCH(p, sss_zpre_inv, P + c * cs, P + 6 * cs, nl, g.Nz, vz[c], p->twqz, p->st));
+        CK(LAUNCH(p, z_single, g, +1, P + 6 * cs, P + 7 * cs, 1, p->twz, p->st));
+        CK(LAUNCH(p, sss_zperm_inv, P + 7 * cs, P + (9 + c) * cs, nl, g.Nz, vz[c], p->st));
+      }
+      CK(LAUNCH(p, real_products, P + 9 * cs, P, 2 * g.S, p->st));
+      for (int f = 0; f < 6; ++f) {
+        CK(LAUNCH(p, sss_zperm_fwd, P + f * cs, P + 6 * cs, nl, g.Nz, qz[f], p->st));
+        CK(LAUNCH(p, z_single, g, -1, P + 6 * cs, P + 7 * cs, 1, p->twz, p->st));
+        CK(LAUNCH(p, sss_zpost_fwd, P + 7 * cs, P + f * cs, nl, g.Nz, qz[f], 1.0 / (2.0 * g.Nz), p->twqz, p->st));
+      }
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_Y_FWD);
+      for (int f = 0; f < 6; ++f)
+        CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], 1.0 / (2.0 * g.Ny), p->twqy, p->st));
+    }
+    {
+      ProfScope ps(p, TS_KCLASS_FWD_X);
+      for (int f = 0; f < 6; ++f)
+        CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], 1.0 / (2.0 * g.Nx), p->twq, p->st));
+      CK(LAUNCH(p, sss_epi, g, P, a, p->st));
+    }
+  }
+  return TS_OK;
+}
+
 // run fn(device_ptr) on a field that may live on the host
 template <typename Fn>
 static int with_device(ts_plan* p, void** stage, const void* ptr, size_t bytes, bool copy_back, Fn&& fn) {
@@ -868,10 +944,11 @@ extern "C" {
 
 int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   if (!p || !u_hat || nsteps < 0) return TS_ERR_ARG;
-  if (p->cfg.basis == TS_BASIS_SSF) {
-    CKS(ssf_step_supported(p));
+  if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
+    const bool sss = p->cfg.basis == TS_BASIS_SSS;
+    CKS(sss ? sss_step_supported(p) : ssf_step_supported(p));
     int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
-      for (int s = 0; s < nsteps; ++s) CKS(step_ssf(p, U));
+      for (int s = 0; s < nsteps; ++s) CKS(sss ? step_sss(p, U) : step_ssf(p, U));
       return (int)TS_OK;
     });
     return rc;

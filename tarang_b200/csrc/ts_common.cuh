@@ -339,6 +339,15 @@ __device__ __forceinline__ int kfft(int l, int N) { return l <= N / 2 ? l : l - 
 // Dealias predicates: true when the mode is ZEROED.
 // mode 1 = reference corner box (FFF_pencil_basic.cc:87-90 / SFF_pencil_basic.cc:94-97),
 // mode 2 = two-thirds cube.
+// SSS (real coefficients, lzr = real z index < Nz): SSS_PENCIL::Dealias zeroes
+// lx >= 2Nx/3+1, ly >= 2Ny/3+1, lzr >= Nz/3 (SSS_pencil_basic.cc:129-134); two-thirds
+// zeroes 3 k > 2 N on any axis
+__device__ __forceinline__ bool sss_dealias_zero(int mode, int lx, int ly, int lzr, int Nx, int Ny, int Nz) {
+  if (mode == 1) return lx >= 2 * Nx / 3 + 1 && ly >= 2 * Ny / 3 + 1 && lzr >= Nz / 3;
+  if (mode == 2) return 3 * lx > 2 * Nx || 3 * ly > 2 * Ny || 3 * lzr > 2 * Nz;
+  return false;
+}
+
 __device__ __forceinline__ bool dealias_zero(int mode, int basis, int lx, int ly, int lz, int Nx, int Ny, int Nz) {
   if (mode == 1) {
     bool mx = basis == 0 ? (lx >= Nx / 3 + 1 && lx <= 2 * Nx / 3 - 1) : (lx >= 2 * Nx / 3 + 1);

@@ -683,6 +683,18 @@ template <> cudaError_t Launch<T>::sss_zperm_inv(const void* v, void* u, long lo
   return cudaGetLastError();
 }
 
+template <> cudaError_t Launch<T>::sss_dealias_copy(const Geo& g, const void* A, void* B, int ncomp,
+                                                   cudaStream_t st) {
+  k_sss_dealias_copy<T><<<grid1d(2 * g.S * ncomp, 256), 256, 0, st>>>((const T*)A, (T*)B, ncomp, g);
+  ++g_launches;
+  return cudaGetLastError();
+}
+template <> cudaError_t Launch<T>::sss_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st) {
+  k_sss_epi<T><<<grid1d(2 * g.S, 256), 256, 0, st>>>((const T*)P, g, a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
 template <> cudaError_t Launch<T>::real_products(const void* R, void* Q, long long n, cudaStream_t st) {
   k_real_products<T><<<grid1d(n, 256), 256, 0, st>>>((const T*)R, (T*)Q, n);
   ++g_launches;

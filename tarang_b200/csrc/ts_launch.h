@@ -51,6 +51,9 @@ template <typename T> struct Launch {
   static cudaError_t sss_zpre_inv(const void* c, void* Vout, long long nlines, int N, int sine, const void* tq,
                                   cudaStream_t st);
   static cudaError_t sss_zperm_inv(const void* v, void* u, long long nlines, int N, int sine, cudaStream_t st);
+  // SSS fluid step: dealiased copy of real coefficients, and the epilogue
+  static cudaError_t sss_dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
+  static cudaError_t sss_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st);
   // six products u_i u_j of three real fields (n reals each)
   static cudaError_t real_products(const void* R, void* Q, long long n, cudaStream_t st);
   // SSF fluid step: elementwise epilogue of the six forward-transformed products in P

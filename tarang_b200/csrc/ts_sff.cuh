@@ -614,4 +614,75 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
   }
 }
 
+// ---------------------------------------------------------------------------
+// SSS fluid step (sincostr_switch "SCC": Vx = SCC, Vy = CSC, Vz = CCS), on real
+// coefficients in the padded real layout (Nz + 2 reals per line, lzr < Nz used):
+// dealiased copy, and the elementwise epilogue after the forward transforms of the
+// six products (Vi2 = CCC, VxVy = SSC, VyVz = CSS, VxVz = SCS; Global.cc:221-228).
+// Derivatives along every axis: parity S -> +K, C -> -K (SSS_pencil_tr.cc).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_sss_dealias_copy(const T* __restrict__ A, T* __restrict__ B, int ncomp,
+                                                          Geo g) {
+  const long long per = 2 * g.S;  // reals per component
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < per * ncomp;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long m = e % per;
+    const int lzr = (int)(m % (g.Nz + 2));
+    const long long r = m / (g.Nz + 2);
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    B[e] = (lzr >= g.Nz || sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz)) ? (T)0 : A[e];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g, StageArgs a) {
+  const long long per = 2 * g.S;
+  const T* U0 = reinterpret_cast<const T*>(a.U0);
+  T* Uc = reinterpret_cast<T*>(a.Ucur);
+  T* tot = reinterpret_cast<T*>(a.tot);
+  T* Uo = reinterpret_cast<T*>(a.Uout);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < per; e += (long long)gridDim.x * blockDim.x) {
+    const int lzr = (int)(e % (g.Nz + 2));
+    if (lzr >= g.Nz) continue;  // padding
+    const long long r = e / (g.Nz + 2);
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const double Kxd = lx * g.kf[0], Kyd = ly * g.kf[1], Kzd = lzr * g.kf[2];
+    const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+    T q[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) q[f] = P[f * per + e];
+    T N1 = (-Kx * q[0] + Ky * q[3]) + Kz * q[5];
+    T N2 = (-Ky * q[1] + Kx * q[3]) + Kz * q[4];
+    T N3 = (-Kz * q[2] + Ky * q[4]) + Kx * q[5];
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    const T div = (Kx * N1 + Ky * N2) + Kz * N3;
+    const T pr = K2 > 0 ? div / (T)K2 : (T)0;
+    N1 += -Kx * pr;
+    N2 += -Ky * pr;
+    N3 += -Kz * pr;
+    const T Rv[3] = {-N1, -N2, -N3};
+    const double eh = a.ex[lx] * a.ey[ly] * a.ez[lzr];
+    const T Eh = (T)eh, E1 = (T)(eh * eh);
+    const bool dz = sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const long long o = i * per + e;
+      const T R = Rv[i], u0 = U0[o];
+      if (a.stage == 1) {
+        Uc[o] = ((dz ? (T)0 : u0) + (T)(0.5 * a.dt) * R) * Eh;
+        tot[o] = (R * E1) * (T)((1.0 / 6) * a.dt);
+      } else if (a.stage == 2) {
+        Uc[o] = u0 * Eh + (T)(0.5 * a.dt) * R;
+        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+      } else if (a.stage == 3) {
+        Uc[o] = (u0 * Eh + (T)a.dt * R) * Eh;
+        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+      } else {
+        Uo[o] = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
+      }
+    }
+  }
+}
+
 }  // namespace ts

@@ -52,8 +52,63 @@ def test_sss_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSS", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.rk4_step(u, 1)
-    with pytest.raises(tb.TsError):
         plan.energy(u)
     with pytest.raises(tb.TsError):
+        tb.Plan(32, basis="SSS", kfactor=KF, nlin_form="rotational")
+    with pytest.raises(tb.TsError):
         plan.forward(plan.field(1), plan.field(1), parity="SCF")
+
+
+def to_padded(A):
+    """real coefficients (c, Nx, Ny, Nz) -> the padded real layout viewed as complex"""
+    c, Nx, Ny, Nz = A.shape
+    P = np.zeros((c, Nx, Ny, Nz + 2))
+    P[..., :Nz] = A
+    return P.view(np.complex128)
+
+
+def from_padded(t, Nz):
+    import torch
+    a = torch.view_as_real(t).reshape(t.shape[0], t.shape[1], t.shape[2], -1).cpu().numpy().astype(np.float64)
+    return a[..., :Nz]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,dealias", [((16, 16, 16), "reference"), ((32, 16, 32), "none"),
+                                       ((32, 32, 16), "two_thirds")])
+def test_sss_step_matches_oracle(cuda, N, dealias, prec):
+    import torch
+    import tarang_b200 as tb
+    mode = {"none": 0, "reference": 1, "two_thirds": 2}[dealias]
+    g = R.Grid(N, KF, "SSS")
+    rng = np.random.default_rng(4)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCC", "CSC", "CCS")])
+    U0 = -0.3 * R.project_rhs(g, U)
+    cfg = R.FluidConfig(g, nu=0.01, dt=1e-3, dealias_mode=mode, nlin_form="conservative")
+    W = U0.copy()
+    for _ in range(3):
+        W = R.rk4_step(cfg, W)
+    plan = tb.Plan(N, basis="SSS", kfactor=KF, precision=prec, nu=0.01, dt=1e-3, dealias=dealias)
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    u = torch.from_numpy(to_padded(U0)).to(cuda).to(cdt) if prec == "f64" else \
+        torch.view_as_complex(torch.from_numpy(to_padded(U0).view(np.float64).reshape(3, N[0], N[1], N[2] // 2 + 1, 2)
+                                               .astype(np.float32)).contiguous()).to(cuda)
+    plan.rk4_step(u, 3)
+    plan.status()
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel(from_padded(u, N[2]), W) < tol
+
+
+def test_sss_taylor_green_decays_exactly(cuda):
+    import torch
+    import tarang_b200 as tb
+    N = (16, 16, 16)
+    g = R.Grid(N, (1.0, 1.0, 1.0), "SSS")
+    x = (np.arange(16) + 0.5) * np.pi / 16
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    U0 = np.stack([R.forward(g, np.sin(X) * np.cos(Y), "SCC"), R.forward(g, -np.cos(X) * np.sin(Y), "CSC"),
+                   R.forward(g, np.zeros_like(X), "CCS")])
+    plan = tb.Plan(N, basis="SSS", kfactor=(1.0, 1.0, 1.0), precision="f64", nu=0.05, dt=1e-2)
+    u = torch.from_numpy(to_padded(U0)).to(cuda)
+    plan.rk4_step(u, 5)
+    assert np.max(np.abs(from_padded(u, 16) - U0 * np.exp(-0.05 * 2 * 5e-2))) < 1e-15
