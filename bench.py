@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--form", default="rotational", choices=["rotational", "conservative"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
     ap.add_argument("--workload", default="fff256",
-                    choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint", "scalar", "mhd", "ssf"],
+                    choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint", "scalar", "mhd", "ssf", "sss"],
                     help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying "
                          "1024^3 (or --shape); rbc: one RBC run (SFF, --N, FP32); adjoint: adjoint/forward cost at 128^3")
     ap.add_argument("--tune", default="auto", choices=["auto", "off"],
@@ -226,14 +226,15 @@ def coupled_leg(kind: str, N: int, steps: int, warmup: int, prec: str = "f32"):
             "model_frac": model * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
 
 
-def ssf_leg(N: int, steps: int, warmup: int, prec: str = "f32"):
-    """SSF fluid step (sin/cos along x and y) at N^3: conservative, unforced, nu = 1e-3,
-    dt = 5e-4, reference dealias, kfactor (pi, pi, 2 pi); a small seeded random spectral
-    field (amplitude 1e-3; the timing does not depend on the values).  Steps/s, CUDA events."""
+def ssf_leg(N: int, steps: int, warmup: int, prec: str = "f32", basis: str = "SSF"):
+    """SSF (sin/cos along x and y) or SSS (along every axis) fluid step at N^3: conservative,
+    unforced, nu = 1e-3, dt = 5e-4, reference dealias, kfactor (pi, pi, 2 pi) / (pi, pi, pi);
+    a small seeded random spectral field (amplitude 1e-3; the timing does not depend on the
+    values).  Steps/s, CUDA events."""
     import torch
     import tarang_b200 as tb
-    plan = tb.Plan(N, basis="SSF", precision=prec, nu=1e-3, dt=5e-4, dealias="reference",
-                   kfactor=(math.pi, math.pi, 2 * math.pi))
+    plan = tb.Plan(N, basis=basis, precision=prec, nu=1e-3, dt=5e-4, dealias="reference",
+                   kfactor=(math.pi, math.pi, 2 * math.pi if basis == "SSF" else math.pi))
     plan.set_stream(torch.cuda.current_stream())
     gen = torch.Generator(device="cuda").manual_seed(0)
     u = plan.field(3)
@@ -507,14 +508,15 @@ def alt_workload(args, world, rank, local, dev):
                 "config": {"workload": f"FFF {what} {n}^3, decaying, nu = kappa/eta = 1e-3, dt = 5e-4, two-thirds"},
                 "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "model_GBps": r["model_GBps"],
                              "ms_per_step_by_class": r["ms_per_step_by_class"]}}
-    elif args.workload == "ssf":
+    elif args.workload in ("ssf", "sss"):
         n = args.N if args.N != 256 else 128
-        r = ssf_leg(n, steps=args.steps, warmup=args.warmup, prec=args.precision)
-        line = {"metric": f"RK4 steps/s, SSF fluid {n}^3 ({args.precision} transforms)",
+        bas = args.workload.upper()
+        r = ssf_leg(n, steps=args.steps, warmup=args.warmup, prec=args.precision, basis=bas)
+        line = {"metric": f"RK4 steps/s, {bas} fluid {n}^3 ({args.precision} transforms)",
                 "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 / r["steps_per_s"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-                "config": {"workload": f"SSF fluid {n}^3, conservative, unforced, nu = 1e-3, dt = 5e-4, "
+                "config": {"workload": f"{bas} fluid {n}^3, conservative, unforced, nu = 1e-3, dt = 5e-4, "
                                        "reference dealias, standalone sin/cos passes"}}
     elif args.workload == "rbc":
         r = rbc_leg(args.N if args.N != 256 else 128, steps=args.steps, warmup=args.warmup)
