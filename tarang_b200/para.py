@@ -239,7 +239,8 @@ def _fff_multiplicity(kx, ky, kz, Nx, Ny):
 
 
 class Output:
-    """Appends out/spectrum.d and out/flux.d for an FFF plan in the reference's layouts.
+    """Appends out/glob.d, out/spectrum.d and out/flux.d for an FFF plan in the reference's
+    layouts.
 
     spectrum.d (FluidIO::Output_shell_spectrum): %%Uek = per-component shell
     spectra (Compute_shell_spectrum, n = 0); %%UDk = 2 x per-component raw sums of
@@ -289,6 +290,51 @@ class Output:
                 fvk.append(2 * np.where(c > 0, s * 4 * math.pi / np.where(c > 0, c, 1) / kfp, 0.0))
         with open(os.path.join(self.out_dir, "spectrum.d"), "a") as f:
             write_spectrum(f, t, ek, dissk, fvk)
+
+    def glob(self, u, t: float, dt: float, helicity: bool = False):
+        """One row of out/glob.d (FluidIO::Output_global, output_energy.cc:69-117): time,
+        total energy, dissipation nu * total_k2energy (total_k2energy = 2 sum mult K^2 |V|^2,
+        Cvf.cc:224-227), helicity1, helicity2, k2H1, k2H2 (2 mult K.(Vr x Vi) summed, / K^2,
+        and the K^2 moments; FFF_pencil_energy.cc:99-139; zero when helicity is off), the
+        modal-energy entropy in bits (universal_energy.cc:449-473), kmax * Kolmogorov scale,
+        nu, R_lambda = 2 E sqrt(15 / eps), dt, and the three component energies."""
+        import torch
+        p = self.plan
+        nu = float(p.cfg.nu)
+        E = [p.energy(u[i:i + 1], 1) for i in range(3)]
+        Etot = E[0] + E[1] + E[2]
+        k2 = 2 * sum(float(p.shell_sums(u[i:i + 1], ncomp=1)[0].sum()) for i in range(3))
+        eps = nu * k2
+        Nx, Ny, Nz = p.N
+        dev = u.device
+        lx = torch.arange(Nx, device=dev)
+        ly = torch.arange(Ny, device=dev)
+        kx = torch.where(lx <= Nx // 2, lx, lx - Nx).double()[:, None, None]
+        ky = torch.where(ly <= Ny // 2, ly, ly - Ny).double()[None, :, None]
+        kz = torch.arange(Nz // 2 + 1, device=dev).double()[None, None, :]
+        mult = torch.where(kz > 0, 1.0, 0.5) * torch.where((kx == Nx // 2) | ((ky == Ny // 2) & (Ny > 1)), 2.0, 1.0)
+        K = [kx * self.kf[0], ky * self.kf[1], kz * self.kf[2]]
+        K2 = (K[0] ** 2 + K[1] ** 2) + K[2] ** 2
+        v = u.to(torch.complex128)
+        H1 = H2 = k2H1 = k2H2 = 0.0
+        if helicity:
+            vr, vi = v.real, v.imag
+            cr = [vr[1] * vi[2] - vr[2] * vi[1], vr[2] * vi[0] - vr[0] * vi[2], vr[0] * vi[1] - vr[1] * vi[0]]
+            h = 2 * mult * (K[0] * cr[0] + K[1] * cr[1] + K[2] * cr[2])
+            H1 = float(h.sum())
+            H2 = float(torch.where(K2 > 1e-15, h / torch.where(K2 > 1e-15, K2, 1.0), 0.0).sum())
+            k2H1 = 2 * float((K2 * h).sum())
+            k2H2 = 2 * H1
+        modal = mult * (v.abs() ** 2).sum(0)
+        prob = modal / Etot
+        ent = float(torch.where(prob > 1e-15, -prob * torch.log(torch.where(prob > 1e-15, prob, 1.0)) / math.log(2.0),
+                                0.0).sum())
+        kmax_eta = self.kmax_inside * (nu ** 3 / eps) ** 0.25 if eps > 0 else float("inf")
+        rlam = 2 * Etot * math.sqrt(15 / eps) if eps > 0 else float("inf")
+        row = [t, Etot, eps, H1, H2, k2H1, k2H2, ent, kmax_eta, nu, rlam, dt, E[0], E[1], E[2]]
+        with open(os.path.join(self.out_dir, "glob.d"), "a") as f:
+            write_glob_row(f, row)
+        return row
 
     def flux(self, u, t: float):
         p = self.plan

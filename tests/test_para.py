@@ -155,3 +155,40 @@ def test_output_spectrum_and_flux_match_oracle(cuda, tmp_path):
     assert np.allclose(power, ref_p, rtol=2e-5, atol=1e-9)
     # the total power equals the energy injection 2 sum mult Re(F.u*) = epsilon (0.1) up to 6 digits
     assert abs(power.sum() - 0.1) < 1e-5
+
+
+@pytest.mark.gpu
+def test_output_glob_matches_oracle(cuda, tmp_path):
+    """glob.d row (FluidIO::Output_global) from a 32^3 state against numpy sums of the oracle field."""
+    import torch
+    from oracle import tarang_ref as R
+    plan, rp = para.plan_from_dir(FFF_DIR, precision="f64")
+    g = R.Grid(rp.N, rp.kfactor)
+    V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    u = torch.from_numpy(V.copy()).to(cuda)
+    out = para.Output(plan, str(tmp_path), radii=rp.flux_radii)
+    row = out.glob(u, 0.25, 5e-4, helicity=True)
+    text = open(tmp_path / "glob.d").read().split("\n")[0].split("\t")[:-1]
+    assert len(text) == 15
+    mult = g.multiplicity()
+    Kx, Ky, Kz = g.K()
+    K2 = g.Ksqr()
+    E = [float(np.sum(mult * np.abs(V[i]) ** 2)) for i in range(3)]
+    Et = E[0] + E[1] + E[2]
+    k2 = 2 * float(np.sum(mult * K2 * np.sum(np.abs(V) ** 2, axis=0)))
+    nu = plan.cfg.nu
+    eps = nu * k2
+    cr = np.cross(V.real, V.imag, axis=0)
+    h = 2 * mult * (Kx * cr[0] + Ky * cr[1] + Kz * cr[2])
+    H1 = float(h.sum())
+    H2 = float(np.where(K2 > 1e-15, h / np.where(K2 > 1e-15, K2, 1), 0).sum())
+    modal = mult * np.sum(np.abs(V) ** 2, axis=0)
+    p = modal / Et
+    ent = float(np.where(p > 1e-15, -p * np.log2(np.where(p > 1e-15, p, 1)), 0).sum())
+    kin = para.max_radius_inside(rp.N, rp.kfactor)
+    ref = [0.25, Et, eps, H1, H2, 2 * float((K2 * h).sum()), 2 * H1, ent, kin * (nu ** 3 / eps) ** 0.25, nu,
+           2 * Et * math.sqrt(15 / eps), 5e-4, E[0], E[1], E[2]]
+    for a, b in zip(row, ref):
+        assert abs(a - b) <= 1e-10 * max(1.0, abs(b))
+    for a, b in zip(text, ref):
+        assert abs(float(a) - b) <= 1e-5 * max(1e-12, abs(b))
