@@ -3,6 +3,7 @@
 // Same class and method names as anandogc/tarang (paths inside trunk/lib):
 //   FluidVF                         fluid/fluid_base/FluidVF.h:73-180
 //   FFF_PENCIL / SFF_PENCIL         basis/FFF/pencil/FFF_pencil.h:51, basis/SFF/pencil/SFF_pencil.h:52
+//   SSF_PENCIL / SSS_PENCIL         basis/SSF/pencil/SSF_pencil.h, basis/SSS/pencil/SSS_pencil.h
 //   Nlin_incompress::Compute_nlin   fluid/incompressible/nlin/Nlin.h:79
 //   Time_advance_incompress::RK4    fluid/incompressible/time_advance/Time_advance.h:69-187
 //   FluidSF                         fluid/fluid_base/FluidSF.h:42
@@ -109,6 +110,18 @@ class FFF_PENCIL : public Universal {
 class SFF_PENCIL : public Universal {
  public:
   explicit SFF_PENCIL(ts_config c) : Universal((c.basis = TS_BASIS_SFF, c)) {}
+};
+
+// basis/SSF/pencil (sin/cos along x and y): transforms and the fluid RK4
+class SSF_PENCIL : public Universal {
+ public:
+  explicit SSF_PENCIL(ts_config c) : Universal((c.basis = TS_BASIS_SSF, c)) {}
+};
+
+// basis/SSS/pencil (sin/cos along every axis, real coefficients): transforms and the fluid RK4
+class SSS_PENCIL : public Universal {
+ public:
+  explicit SSS_PENCIL(ts_config c) : Universal((c.basis = TS_BASIS_SSS, c)) {}
 };
 
 // Velocity field: cvf (V1, V2, V3) and nlin (nlin1..3), each a contiguous
