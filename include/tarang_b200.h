@@ -124,10 +124,10 @@ int ts_rk4_step(ts_plan* plan, void* u_hat, int nsteps);
 
 /* RK4(U,T,P,F) for RBC (RK_SF.cc:97-221), SFF basis, PRLARGE/ULARGE. */
 int ts_rk4_step_rbc(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
-/* RK4(U,T,P,F) (RK_SF.cc:97-221) with a passive scalar (program.kind INC_SCALAR,
+/* RK4(U,T,P,F) (RK_SF.cc:97-221) with a passive scalar (program.kind SCALAR_INCOMPRESS,
  * Compute_force_TO_rhs_scalar, Tadvance_functions.cc:464-474, no force) on an FFF
  * plan, conservative form: U with nu, T with kappa; T_hat one component in the
- * state layout.  Replaces that RK4 call for kind INC_SCALAR. */
+ * state layout.  Replaces that RK4 call for kind SCALAR_INCOMPRESS. */
 int ts_rk4_step_scalar(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
 /* Time_advance_incompress::RK4(U, W, P, F) for incompressible MHD (RK_VF_MHD.cc:126-186,
  * Compute_nlin(U, W) compute_nlin_VF_MHD.cc:40-95 in Elsasser form) + the strong

@@ -210,7 +210,7 @@ struct Time_advance_incompress {
     check(ts_rk4_step_mhd(U.basis().plan(), U.cvf(), W.cvf(), nsteps), "RK4");
   }
   // RK4(U,T,P,F) (RK_SF.cc:97): RBC on the SFF basis (PRLARGE / ULARGE), or a
-  // passive scalar (kind INC_SCALAR, no force) on the FFF basis
+  // passive scalar (kind SCALAR_INCOMPRESS, no force) on the FFF basis
   static void RK4(FluidVF& U, FluidSF& T, int nsteps = 1) {
     ts_plan* p = U.basis().plan();
     if (U.basis().config().basis == TS_BASIS_SFF) check(ts_rk4_step_rbc(p, U.cvf(), T.csf(), nsteps), "RK4");

@@ -816,7 +816,7 @@ class RBCConfig:
 
 @dataclass
 class ScalarConfig:
-    """Incompressible flow with a passive scalar (program.kind INC_SCALAR), no force."""
+    """Incompressible flow with a passive scalar (program.kind SCALAR_INCOMPRESS), no force."""
     grid: Grid
     nu: float
     kappa: float

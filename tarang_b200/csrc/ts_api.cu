@@ -625,7 +625,7 @@ static int step_rbc(ts_plan* p, void* U0, void* T0) {
 }
 
 // ---------------------------------------------------------------------------
-// FFF passive scalar (program.kind INC_SCALAR): RK4(U,T,P,F) with no force
+// FFF passive scalar (program.kind SCALAR_INCOMPRESS): RK4(U,T,P,F) with no force
 // ---------------------------------------------------------------------------
 static int ensure_work(ts_plan* p, int nstage, int nprod);
 

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 }
 
 // ---------------------------------------------------------------------------
-// FFF passive scalar (program.kind INC_SCALAR), elementwise epilogue after the
+// FFF passive scalar (program.kind SCALAR_INCOMPRESS), elementwise epilogue after the
 // forward x FFT of the nine products of form 2 (u1u1, u2u2, u3u3, u1u2, u2u3,
 // u3u1, u1T, u2T, u3T; unnormalised):
 //   N_i = sum_j i K_j F[u_j u_i]  (compute_diag_offdiag.cc:47-98, conservative)

@@ -6,9 +6,11 @@ Inputs (a reference data directory ``<dir>/in/``):
   global/Global_read.cc:319-450): ``program.kind``, ``program.basis_type``,
   ``program.alias_option``, ``program.apply_strong_realitycond_alltime_switch``,
   ``field.N``, ``field.kfactor`` / ``field.L``, ``field.diss_coefficients``,
-  ``time.init / final / dt_fixed``, ``force.U_switch / field_procedure /
-  parameters``, ``PHYSICS.Pr_option / Uscaling / Rayleigh / Prandtl`` and
-  ``energy_transfer.flux.no_spheres / radii``.  Any other kind or basis is
+  ``time.init / final / dt_fixed``, ``force.U_switch / W_switch / T_switch /
+  field_procedure / parameters``, ``PHYSICS.Pr_option / Uscaling / Rayleigh / Prandtl`` and
+  ``energy_transfer.flux.no_spheres / radii``.  Kinds and bases: FLUID_INCOMPRESS on
+  FFF, SSF and SSS, RBC on SFF, SCALAR_INCOMPRESS and MHD_INCOMPRESS on FFF
+  (``diss_coefficients`` = [nu, kappa] or [nu, eta]).  Any other kind or basis is
   refused by name (NotImplementedError), never silently changed.
 * ``initial.txt`` / ``forcing.txt`` — Blitz++ 1-D arrays as text,
   ``(lb,ub)`` then ``[ v0 v1 ... ]`` (``Global::Read_IC_energy_supply_arrays``,
@@ -37,6 +39,11 @@ from dataclasses import dataclass, field
 import numpy as np
 
 INF_RADIUS = 1e9   # the last flux sphere encloses every mode
+
+# (program.kind, basis_type) pairs this library steps (solvers/main.cc:113-130 picks the
+# solver by kind): the fluid on FFF, SSF and SSS, RBC on SFF, the passive scalar and MHD on FFF
+STEPPED = (("FLUID_INCOMPRESS", "FFF"), ("FLUID_INCOMPRESS", "SSF"), ("FLUID_INCOMPRESS", "SSS"),
+           ("RBC", "SFF"), ("SCALAR_INCOMPRESS", "FFF"), ("MHD_INCOMPRESS", "FFF"))
 
 
 @dataclass
@@ -119,9 +126,9 @@ def read_para(path: str) -> RunParams:
     prog, fld, tim = p["program"], p["field"], p["time"]
     kind = str(prog["kind"]).strip()
     basis = str(prog["basis_type"]).strip()
-    if (kind, basis) not in (("FLUID_INCOMPRESS", "FFF"), ("RBC", "SFF")):
+    if (kind, basis) not in STEPPED:
         raise NotImplementedError(f"program.kind {kind} with basis_type {basis}: this library steps "
-                                  "FLUID_INCOMPRESS on FFF and RBC on SFF")
+                                  + ", ".join(f"{k} on {b}" for k, b in STEPPED))
     N = tuple(int(n) for n in fld["N"])
     # kfactor, else from L, else the basis defaults (FFF_pencil.cc:34-66, SFF_pencil.cc:40-80)
     if fld.get("kfactor") and len(fld["kfactor"]) == 3:
@@ -153,11 +160,16 @@ def read_para(path: str) -> RunParams:
         rp.nu = math.sqrt(rp.Pr / rp.Ra)
         rp.kappa = 1.0 / math.sqrt(rp.Pr * rp.Ra)
     force = p.get("force") or {}
-    if _flag(force.get("U_switch", False)):
-        procs = force.get("field_procedure") or []
-        procs = procs if isinstance(procs, list) else [procs]
-        if kind == "FLUID_INCOMPRESS":
-            if [int(x) for x in procs] != [1]:
+    procs = force.get("field_procedure")
+    procs = [int(x) for x in (procs if isinstance(procs, list) else [procs]) if x is not None]
+    # field_procedure 0 is decay (no force); RBC's buoyancy (51) is part of the RBC step
+    switches = [_flag(force.get(s, False)) for s in ("U_switch", "W_switch", "T_switch")]
+    if kind != "RBC" and any(switches) and procs and any(x != 0 for x in procs):
+        if (kind, basis) != ("FLUID_INCOMPRESS", "FFF") or switches[1] or switches[2]:
+            raise NotImplementedError(f"force.field_procedure {procs} for {kind} on {basis}: "
+                                      "decay (0) only; the forced step is the FFF fluid one")
+        if switches[0]:
+            if procs != [1]:
                 raise NotImplementedError(f"force.field_procedure {procs}: Carati energy supply (1) only")
             params = force.get("parameters") or []
             words = str(params[0] if isinstance(params, list) else params).split()
@@ -192,9 +204,37 @@ def plan_from_dir(data_dir: str, precision: str = "f64", nlin_form: str = "conse
     kw = dict(precision=precision, dealias=rp.dealias, kfactor=rp.kfactor, reality_fix=rp.reality_fix, dt=rp.dt)
     if rp.kind == "RBC":
         plan = Plan(rp.N, basis="SFF", nu=rp.nu, kappa=rp.kappa, Ra=rp.Ra, Pr=rp.Pr, **kw)
+    elif rp.kind in ("SCALAR_INCOMPRESS", "MHD_INCOMPRESS"):
+        # the second dissipation coefficient: kappa of T, or eta of B (stored as the plan's kappa)
+        plan = Plan(rp.N, nlin_form="conservative", nu=rp.nu, kappa=rp.kappa, **kw)
+    elif rp.basis in ("SSF", "SSS"):
+        plan = Plan(rp.N, basis=rp.basis, nlin_form="conservative", nu=rp.nu, **kw)
     else:
         plan = Plan(rp.N, nlin_form=nlin_form, nu=rp.nu, forcing=forcing, **kw)
     return plan, rp
+
+
+def n_fields(kind: str) -> int:
+    """How many fields one step advances: U alone, or U with T (RBC, passive scalar) or B (MHD)."""
+    return 1 if kind == "FLUID_INCOMPRESS" else 2
+
+
+def advance(plan, kind: str, fields, nsteps: int = 1):
+    """nsteps IF-RK4 steps of the fields of a run of this kind, the RK4 the reference's
+    solver for the kind calls (RK_VF.cc, RK_SF.cc, RK_VF_MHD.cc): ``fields`` is (u,) for
+    FLUID_INCOMPRESS, (u, T) for RBC and SCALAR_INCOMPRESS, (u, b) for MHD_INCOMPRESS."""
+    if len(fields) != n_fields(kind):
+        raise ValueError(f"{kind} advances {n_fields(kind)} field(s), got {len(fields)}")
+    if kind == "FLUID_INCOMPRESS":
+        plan.rk4_step(fields[0], nsteps)
+    elif kind == "RBC":
+        plan.rk4_step_rbc(fields[0], fields[1], nsteps)
+    elif kind == "SCALAR_INCOMPRESS":
+        plan.rk4_step_scalar(fields[0], fields[1], nsteps)
+    elif kind == "MHD_INCOMPRESS":
+        plan.rk4_step_mhd(fields[0], fields[1], nsteps)
+    else:
+        raise NotImplementedError(f"program.kind {kind}")
 
 
 # ----------------------------------------------------------------------------

@@ -1,4 +1,4 @@
-"""Passive scalar on the FFF basis (program.kind INC_SCALAR): RK4(U,T,P,F) with no force,
+"""Passive scalar on the FFF basis (program.kind SCALAR_INCOMPRESS): RK4(U,T,P,F) with no force,
 through ts_rk4_step_scalar, against the FP64 oracle (relative L2 <= 1e-12 FP64, 1e-5 FP32)."""
 import numpy as np
 import pytest

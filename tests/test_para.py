@@ -1,6 +1,7 @@
 """Reading reference-format run inputs (para.yaml, forcing.txt) and writing the
-reference's text outputs (spectrum.d, flux.d, glob.d).  CPU only, except the last
-test, which steps a run built from a para.yaml on the GPU against the oracle."""
+reference's text outputs (spectrum.d, flux.d, glob.d).  The gpu-marked tests step
+runs built from a para.yaml (the fluid on FFF, SSF and SSS, MHD, the passive
+scalar) and write outputs on the GPU against the oracle."""
 import io
 import math
 import os
@@ -13,6 +14,7 @@ from tarang_b200 import para
 HERE = os.path.dirname(os.path.abspath(__file__))
 FFF_DIR = os.path.join(HERE, "golden", "para_fff")
 RBC_DIR = os.path.join(HERE, "golden", "para_rbc")
+KIND_DIRS = {k: os.path.join(HERE, "golden", f"para_{k}") for k in ("mhd", "scalar", "ssf", "sss")}
 
 
 def test_read_para_fff_forced():
@@ -35,6 +37,36 @@ def test_read_para_rbc_from_L():
     assert rp.nsteps == 100 and not rp.force_on
 
 
+def test_read_para_other_kinds():
+    """MHD and the passive scalar on FFF take [nu, eta] / [nu, kappa]; decay (field_procedure 0,
+    or a procedure with every switch off) is unforced; SSF / SSS fluids default kfactor to 1."""
+    rp = para.read_para(os.path.join(KIND_DIRS["mhd"], "in", "para.yaml"))
+    assert (rp.kind, rp.basis, rp.N) == ("MHD_INCOMPRESS", "FFF", (32, 16, 32))
+    assert (rp.nu, rp.kappa, rp.nsteps, rp.force_on, rp.reality_fix) == (0.01, 0.02, 3, False, True)
+    rp = para.read_para(os.path.join(KIND_DIRS["scalar"], "in", "para.yaml"))
+    assert (rp.kind, rp.N, rp.nu, rp.kappa, rp.nsteps) == ("SCALAR_INCOMPRESS", (32, 32, 16), 0.01, 0.03, 3)
+    assert np.allclose(rp.kfactor, (1.0, 2.0, 1.0)) and rp.t_init == 0.5 and not rp.force_on
+    rp = para.read_para(os.path.join(KIND_DIRS["ssf"], "in", "para.yaml"))
+    assert (rp.kind, rp.basis, rp.kfactor, rp.nu, rp.nsteps) == ("FLUID_INCOMPRESS", "SSF", (1.0, 1.0, 1.0), 0.02, 3)
+    rp = para.read_para(os.path.join(KIND_DIRS["sss"], "in", "para.yaml"))
+    assert (rp.basis, rp.N, rp.kfactor, rp.dealias) == ("SSS", (16, 32, 16), (1.0, 1.0, 1.0), "reference")
+    assert [para.n_fields(k) for k in ("FLUID_INCOMPRESS", "RBC", "SCALAR_INCOMPRESS", "MHD_INCOMPRESS")] == [1, 2, 2, 2]
+    with pytest.raises(ValueError):
+        para.advance(None, "MHD_INCOMPRESS", (None,), 1)
+
+
+@pytest.mark.parametrize("kind,basis,force", [("FLUID_INCOMPRESS", "SSF", "U_switch: true\n  field_procedure: [1]"),
+                                              ("MHD_INCOMPRESS", "FFF", "W_switch: true\n  field_procedure: 2"),
+                                              ("FLUID_INCOMPRESS", "FFF", "T_switch: true\n  field_procedure: [1]"),
+                                              ("SCALAR_INCOMPRESS", "SFF", "U_switch: false")])
+def test_read_para_refuses_forcings_and_bases(tmp_path, kind, basis, force):
+    f = tmp_path / "para.yaml"
+    f.write_text(f"program:\n  kind: {kind}\n  basis_type: {basis}\nfield:\n  N: [8,8,8]\n"
+                 f"time:\n  dt_fixed: 0.1\n  final: 1\nforce:\n  {force}\n")
+    with pytest.raises(NotImplementedError):
+        para.read_para(str(f))
+
+
 def test_default_flux_radii_geometric():
     r = para.default_flux_radii(10, 64)
     assert r[:4] == [0.0, 2.0, 4.0, 8.0]
@@ -48,7 +80,7 @@ def test_blitz_arrays_and_unsupported(tmp_path):
     arrs = para.read_blitz_arrays(os.path.join(FFF_DIR, "in", "forcing.txt"))
     assert len(arrs) == 2 and arrs[0].shape == (7,) and arrs[0][3] == 0.1 and not arrs[1].any()
     bad = tmp_path / "para.yaml"
-    bad.write_text("program:\n  kind: MHD_INCOMPRESS\n  basis_type: FFF\nfield:\n  N: [8,8,8]\ntime:\n  dt_fixed: 0.1\n  final: 1\n")
+    bad.write_text("program:\n  kind: MHD_INCOMPRESS\n  basis_type: SFF\nfield:\n  N: [8,8,8]\ntime:\n  dt_fixed: 0.1\n  final: 1\n")
     with pytest.raises(NotImplementedError):
         para.read_para(str(bad))
     (tmp_path / "b").write_text("(0,2)\n[ 1 2 ]\n")
@@ -92,6 +124,61 @@ def test_plan_from_para_steps_like_the_oracle(cuda):
     torch.cuda.synchronize()
     d = u.cpu().numpy() - W
     assert np.linalg.norm(d) / np.linalg.norm(W) < 1e-12
+
+
+def _kind_state(g, kind, basis):
+    """a seeded oracle state for a run of this kind: (U,), (U, T) or (U, B)"""
+    from oracle import tarang_ref as R
+    rng = np.random.default_rng(11)
+    if basis in ("SSF", "SSS"):
+        par = R.SSF_PARITY if basis == "SSF" else R.SSS_PARITY
+        U = np.stack([R.forward(g, rng.standard_normal(g.rshape), par[v]) for v in ("Vx", "Vy", "Vz")])
+        return (-0.3 * R.project_rhs(g, U),)
+    U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+    if kind == "MHD_INCOMPRESS":
+        return U, R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 1, 0.3)
+    return U, R.reality_fix(g, 0.3 * R.forward(g, rng.standard_normal(g.rshape)))
+
+
+def _kind_oracle(g, rp, state):
+    from oracle import tarang_ref as R
+    out = [s.copy() for s in state]
+    for _ in range(rp.nsteps):
+        if rp.kind == "FLUID_INCOMPRESS":
+            out = [R.rk4_step(R.FluidConfig(g, nu=rp.nu, dt=rp.dt, dealias_mode=1, nlin_form="conservative"), out[0])]
+        elif rp.kind == "MHD_INCOMPRESS":
+            out = list(R.mhd_rk4_step(R.MHDConfig(g, nu=rp.nu, eta=rp.kappa, dt=rp.dt, dealias_mode=1), *out))
+        else:
+            out = list(R.rbc_rk4_step(R.ScalarConfig(g, nu=rp.nu, kappa=rp.kappa, dt=rp.dt, dealias_mode=1), *out))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["mhd", "scalar", "ssf", "sss"])
+def test_plan_from_para_other_kinds_step_like_the_oracle(cuda, name):
+    """MHD, passive-scalar, SSF and SSS runs set up from a para.yaml, stepped through
+    para.advance, match the FP64 oracle over the run's 3 steps (relative L2 <= 1e-12)."""
+    import torch
+    from oracle import tarang_ref as R
+    plan, rp = para.plan_from_dir(KIND_DIRS[name], precision="f64")
+    g = R.Grid(rp.N, rp.kfactor, rp.basis)
+    state = _kind_state(g, rp.kind, rp.basis)
+    want = _kind_oracle(g, rp, state)
+    Nz = rp.N[2]
+    if rp.basis == "SSS":
+        # real coefficients in the padded real layout (Nx, Ny, Nz + 2), viewed as complex
+        pad = np.zeros(state[0].shape[:3] + (Nz + 2,))
+        pad[..., :Nz] = state[0]
+        fields = [torch.from_numpy(pad.view(np.complex128)).to(cuda)]
+    else:
+        fields = [torch.from_numpy(s.copy()).to(cuda) for s in state]
+    para.advance(plan, rp.kind, fields, rp.nsteps)
+    plan.status()
+    for f, w in zip(fields, want):
+        got = f.cpu().numpy()
+        if rp.basis == "SSS":
+            got = got.view(np.float64)[..., :Nz]
+        assert np.linalg.norm(got - w) / np.linalg.norm(w) < 1e-12
 
 
 def _read_blocks(path, label):
