@@ -122,7 +122,11 @@ int ts_nlin(ts_plan* plan, void* u_hat, void* nlin_hat);
  * FFF with force_type NONE or CARATI_ENERGY_SUPPLY. */
 int ts_rk4_step(ts_plan* plan, void* u_hat, int nsteps);
 
-/* RK4(U,T,P,F) for RBC (RK_SF.cc:97-221), SFF basis, PRLARGE/ULARGE. */
+/* RK4(U,T,P,F) for RBC (RK_SF.cc:97-221), PRLARGE/ULARGE buoyancy
+ * (compute_force_RBC.cc:104-150): on an SFF plan, and on SSF / SSS plans
+ * (conservative, unforced; T takes the Vx parity, SCF / SCC, with the products
+ * u_i T in Vi2 / VxVy / VxVz, Global_process_basic_vars.cc:108-116; on SSS, T_hat
+ * is one component of real coefficients in the padded real layout). */
 int ts_rk4_step_rbc(ts_plan* plan, void* u_hat, void* T_hat, int nsteps);
 /* RK4(U,T,P,F) (RK_SF.cc:97-221) with a passive scalar (program.kind SCALAR_INCOMPRESS,
  * Compute_force_TO_rhs_scalar, Tadvance_functions.cc:464-474, no force) on an FFF

@@ -213,7 +213,7 @@ struct Time_advance_incompress {
   // passive scalar (kind SCALAR_INCOMPRESS, no force) on the FFF basis
   static void RK4(FluidVF& U, FluidSF& T, int nsteps = 1) {
     ts_plan* p = U.basis().plan();
-    if (U.basis().config().basis == TS_BASIS_SFF) check(ts_rk4_step_rbc(p, U.cvf(), T.csf(), nsteps), "RK4");
+    if (U.basis().config().basis != TS_BASIS_FFF) check(ts_rk4_step_rbc(p, U.cvf(), T.csf(), nsteps), "RK4");
     else check(ts_rk4_step_scalar(p, U.cvf(), T.csf(), nsteps), "RK4");
   }
 };

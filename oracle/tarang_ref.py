@@ -391,6 +391,11 @@ SSF_PARITY = {"Vx": "SCF", "Vy": "CSF", "Vz": "CCF", "div": "CCF", "Vi2": "CCF",
 SSS_PARITY = {"Vx": "SCC", "Vy": "CSC", "Vz": "CCS", "div": "CCC", "Vi2": "CCC", "VxVy": "SSC", "VxVz": "SCS",
               "VyVz": "CSS"}
 
+# a scalar F (the temperature) takes the Vx parity on every basis and the products
+# u_x F, u_y F, u_z F take Vi2, VxVy and VxVz (Global_process_basic_vars.cc:108, 114-116)
+for _tab in (SSF_PARITY, SSS_PARITY):
+    _tab.update(F=_tab["Vx"], FVx=_tab["Vi2"], FVy=_tab["VxVy"], FVz=_tab["VxVz"])
+
 
 def _par(g: Grid, key: str) -> str:
     if g.basis == "SSS":
@@ -432,9 +437,12 @@ def nlin_conservative_from_real(g: Grid, ur: list, wr: list | None = None) -> np
         n3 = n3 + xderiv(g, X, p("VxVz"))
     else:
         # giver form: nlin_i = sum_j D_j F[u_j w_i]
-        n1 = n1 + yderiv(g, forward(g, ur[1] * wr[0], p("VxVy"))) + zderiv(g, forward(g, ur[2] * wr[0], p("VxVz")))
-        n2 = n2 + xderiv(g, forward(g, ur[0] * wr[1], p("VxVy")), p("VxVy")) + zderiv(g, forward(g, ur[2] * wr[1], p("VyVz")))
-        n3 = n3 + xderiv(g, forward(g, ur[0] * wr[2], p("VxVz")), p("VxVz")) + yderiv(g, forward(g, ur[1] * wr[2], p("VyVz")))
+        n1 = n1 + yderiv(g, forward(g, ur[1] * wr[0], p("VxVy")), p("VxVy")) \
+            + zderiv(g, forward(g, ur[2] * wr[0], p("VxVz")), p("VxVz"))
+        n2 = n2 + xderiv(g, forward(g, ur[0] * wr[1], p("VxVy")), p("VxVy")) \
+            + zderiv(g, forward(g, ur[2] * wr[1], p("VyVz")), p("VyVz"))
+        n3 = n3 + xderiv(g, forward(g, ur[0] * wr[2], p("VxVz")), p("VxVz")) \
+            + yderiv(g, forward(g, ur[1] * wr[2], p("VyVz")), p("VyVz"))
     return np.stack([n1, n2, n3])
 
 
@@ -794,7 +802,7 @@ def init_energy_spectrum(g: Grid, E_ic: np.ndarray, seed: int, target_energy: fl
 
 
 # ----------------------------------------------------------------------------
-# Boussinesq RBC on SFF (PRLARGE, ULARGE)
+# Boussinesq RBC on SFF, SSF and SSS (PRLARGE, ULARGE)
 # ----------------------------------------------------------------------------
 @dataclass
 class RBCConfig:
@@ -846,8 +854,8 @@ def rbc_rhs(cfg, U: np.ndarray, T: np.ndarray) -> tuple:
     Tr = inverse(g, Td, _par(g, "F"))
     p = lambda k: _par(g, k)
     Tn = xderiv(g, forward(g, ur[0] * Tr, p("FVx")), p("FVx"))
-    Tn = Tn + yderiv(g, forward(g, ur[1] * Tr, p("FVy")))
-    Tn = Tn + zderiv(g, forward(g, ur[2] * Tr, p("FVz")))
+    Tn = Tn + yderiv(g, forward(g, ur[1] * Tr, p("FVy")), p("FVy"))
+    Tn = Tn + zderiv(g, forward(g, ur[2] * Tr, p("FVz")), p("FVz"))
     N = nlin_conservative_from_real(g, ur)
     N[0] = N[0] - FU1
     Tn = Tn - FT
@@ -856,7 +864,7 @@ def rbc_rhs(cfg, U: np.ndarray, T: np.ndarray) -> tuple:
 
 def rbc_rk4_step(cfg, U0: np.ndarray, T0: np.ndarray) -> tuple:
     """RK4(U,T,P,F) RK_SF.cc:97-221 with Single_time_step_scalar (U with nu, T with kappa);
-    an RBCConfig (SFF, buoyancy) or a ScalarConfig (passive scalar, any basis)."""
+    an RBCConfig (SFF, SSF or SSS, buoyancy) or a ScalarConfig (passive scalar)."""
     g = cfg.grid
     dt = cfg.dt
     EU = lambda A, a: exp_ksqr(g, A, -cfg.nu * a * dt)

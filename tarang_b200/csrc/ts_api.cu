@@ -789,23 +789,45 @@ static Geo y_as_x(const Geo& g) {
 
 // ---------------------------------------------------------------------------
 // SSF fluid step (sin/cos along x and y; sincostr_switch "SCF"), conservative form,
-// unforced: RK4(U,P,F) (RK.cc:91-170) with standalone transforms.  P holds 12
-// components: [0, 3) spectral scratch, [3, 6) real u, [6, 12) real products; the
-// forward z transform writes the products' spectra into [0, 6).
+// unforced: RK4(U,P,F) (RK.cc:91-170) with standalone transforms; with a temperature
+// T the Boussinesq step RK4(U,T,P,F) (RK_SF.cc:97-221, PRLARGE / ULARGE buoyancy).
+// With nf = 3 (fluid) or 4 (U, T) fields and np = 6 or 9 products, P holds
+// [0, nf) spectral scratch, [nf, 2 nf) the real fields, [2 nf, 2 nf + np) the real
+// products; the forward z transform writes the products' spectra into [0, np).
 // ---------------------------------------------------------------------------
-static int ssf_step_supported(ts_plan* p) {
-  if (p->cfg.basis != TS_BASIS_SSF || p->cfg.nlin_form != TS_NLIN_CONSERVATIVE ||
+static int ssf_step_supported(ts_plan* p, bool rbc) {
+  const int basis = p->cfg.basis;
+  if ((basis != TS_BASIS_SSF && basis != TS_BASIS_SSS) || p->cfg.nlin_form != TS_NLIN_CONSERVATIVE ||
       p->cfg.force_type != TS_FORCE_NONE) {
-    g_last_error = "the SSF step is the conservative, unforced fluid step";
+    g_last_error = rbc ? "the SSF / SSS Boussinesq step is the conservative, unforced one"
+                       : "the SSF / SSS step is the conservative, unforced fluid step";
     return TS_ERR_UNSUPPORTED;
   }
-  return ensure_work(p, 3, 12);
+  const int nf = rbc ? 4 : 3, np = rbc ? 9 : 6;
+  return ensure_work(p, nf, basis == TS_BASIS_SSS ? np + 3 + nf : 2 * nf + np);
 }
 
-static int step_ssf(ts_plan* p, void* U0) {
+// the RBC epilogue's arguments (U, T in place; stage fields U then T in Ucur, tot)
+static SffArgs ssf_rbc_args(ts_plan* p, void* U0, void* T0) {
+  SffArgs a;
+  memset(&a, 0, sizeof(a));
+  a.U0 = U0;
+  a.T0 = T0;
+  a.Ucur = p->Ucur;
+  a.tot = p->tot;
+  a.dt = p->cfg.dt;
+  for (int i = 0; i < 3; ++i) {
+    a.eu[i] = p->eax[i];
+    a.et[i] = p->eaxT[i];
+  }
+  return a;
+}
+
+static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
   const Geo& g = p->g;
   const Geo gy = y_as_x(g);
   const long long cs = g.S * (long long)p->cb;  // bytes of one component
+  const int nf = T0 ? 4 : 3, np = T0 ? 9 : 6;
   char* P = (char*)p->P;
   StageArgs a;
   memset(&a, 0, sizeof(a));
@@ -817,37 +839,44 @@ static int step_ssf(ts_plan* p, void* U0) {
   a.ex = p->eax[0];
   a.ey = p->eax[1];
   a.ez = p->eax[2];
-  // x, y sine (1) / cosine (0) letters of Vx = SCF, Vy = CSF, Vz = CCF and of the products
-  // u1u1, u2u2, u3u3 (Vi2 = CCF), u1u2 (VxVy = SSF), u2u3 (VyVz = CSF), u3u1 (VxVz = SCF)
-  const int vx[3] = {1, 0, 0}, vy[3] = {0, 1, 0};
-  const int qx[6] = {0, 0, 0, 1, 0, 1}, qy[6] = {0, 0, 0, 1, 1, 0};
+  SffArgs b = ssf_rbc_args(p, U0, T0);
+  // x, y sine (1) / cosine (0) letters of Vx = SCF, Vy = CSF, Vz = CCF, T = SCF and of the
+  // products u1u1, u2u2, u3u3 (Vi2 = CCF), u1u2 (VxVy = SSF), u2u3 (VyVz = CSF),
+  // u3u1 (VxVz = SCF), u1T (CCF), u2T (SSF), u3T (SCF)
+  const int vx[4] = {1, 0, 0, 1}, vy[4] = {0, 1, 0, 0};
+  const int qx[9] = {0, 0, 0, 1, 0, 1, 0, 1, 1}, qy[9] = {0, 0, 0, 1, 1, 0, 0, 1, 0};
   const double sy = 1.0 / (2.0 * g.Ny), sx = 1.0 / (2.0 * g.Nx * (double)g.Nz);
   for (int stage = 1; stage <= 4; ++stage) {
     const void* Uin = stage == 1 ? U0 : p->Ucur;
-    a.stage = stage;
+    const void* Tin = stage == 1 ? (const void*)T0 : (const void*)((const char*)p->Ucur + 3 * cs);
+    a.stage = b.stage = stage;
+    b.U1in = Uin;
+    b.Tin = Tin;
     {
       ProfScope ps(p, TS_KCLASS_INV_X);
       CK(LAUNCH(p, dealias_copy, g, Uin, P, 3, p->st));
-      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
+      if (T0) CK(LAUNCH(p, dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
+      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_INV);
-      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
+      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Z);
-      CK(LAUNCH(p, z_single, g, +1, P, P + 3 * cs, 3, p->twz, p->st));
-      CK(LAUNCH(p, real_products, P + 3 * cs, P + 6 * cs, 2 * g.S, p->st));
-      CK(LAUNCH(p, z_single, g, -1, P + 6 * cs, P, 6, p->twz, p->st));
+      CK(LAUNCH(p, z_single, g, +1, P, P + nf * cs, nf, p->twz, p->st));
+      CK(LAUNCH(p, real_products, P + nf * cs, P + 2 * nf * cs, 2 * g.S, nf, p->st));
+      CK(LAUNCH(p, z_single, g, -1, P + 2 * nf * cs, P, np, p->twz, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_FWD);
-      for (int f = 0; f < 6; ++f) CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], sy, p->twqy, p->st));
+      for (int f = 0; f < np; ++f) CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], sy, p->twqy, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_FWD_X);
-      for (int f = 0; f < 6; ++f) CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], sx, p->twq, p->st));
-      CK(LAUNCH(p, ssf_epi, g, P, a, p->st));
+      for (int f = 0; f < np; ++f) CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], sx, p->twq, p->st));
+      if (T0) CK(LAUNCH(p, ssf_rbc_epi, g, P, b, p->st));
+      else CK(LAUNCH(p, ssf_epi, g, P, a, p->st));
     }
   }
   return TS_OK;
@@ -855,24 +884,19 @@ static int step_ssf(ts_plan* p, void* U0) {
 
 // ---------------------------------------------------------------------------
 // SSS fluid step (sin/cos along every axis; sincostr_switch "SCC"), conservative,
-// unforced, on real coefficients.  P holds 12 components: [0, 6) the coefficient
-// scratch of the inverse and then the six products, [6] and [7] per-line scratch
-// of the z passes, [9, 12) the real velocity.
+// unforced, on real coefficients; with T the Boussinesq step as on SSF.  P holds
+// [0, np) the coefficient scratch of the inverse and then the np products, [np] and
+// [np + 1] per-line scratch of the z passes, [np + 3, np + 3 + nf) the real fields.
 // ---------------------------------------------------------------------------
-static int sss_step_supported(ts_plan* p) {
-  if (p->cfg.basis != TS_BASIS_SSS || p->cfg.nlin_form != TS_NLIN_CONSERVATIVE ||
-      p->cfg.force_type != TS_FORCE_NONE) {
-    g_last_error = "the SSS step is the conservative, unforced fluid step";
-    return TS_ERR_UNSUPPORTED;
-  }
-  return ensure_work(p, 3, 12);
-}
-
-static int step_sss(ts_plan* p, void* U0) {
+static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
   const Geo& g = p->g;
   const Geo gy = y_as_x(g);
   const long long cs = g.S * (long long)p->cb, nl = (long long)g.Nx * g.Ny;
+  const int nf = T0 ? 4 : 3, np = T0 ? 9 : 6;
   char* P = (char*)p->P;
+  char* s0 = P + np * cs;
+  char* s1 = P + (np + 1) * cs;
+  char* Rf = P + (np + 3) * cs;
   StageArgs a;
   memset(&a, 0, sizeof(a));
   a.U0 = U0;
@@ -883,46 +907,53 @@ static int step_sss(ts_plan* p, void* U0) {
   a.ex = p->eax[0];
   a.ey = p->eax[1];
   a.ez = p->eax[2];
-  // sine (1) / cosine (0) letters: Vx = SCC, Vy = CSC, Vz = CCS; products u1u1, u2u2,
-  // u3u3 (CCC), u1u2 (SSC), u2u3 (CSS), u3u1 (SCS)
-  const int vx[3] = {1, 0, 0}, vy[3] = {0, 1, 0}, vz[3] = {0, 0, 1};
-  const int qx[6] = {0, 0, 0, 1, 0, 1}, qy[6] = {0, 0, 0, 1, 1, 0}, qz[6] = {0, 0, 0, 0, 1, 1};
+  SffArgs b = ssf_rbc_args(p, U0, T0);
+  // sine (1) / cosine (0) letters: Vx = SCC, Vy = CSC, Vz = CCS, T = SCC; products u1u1,
+  // u2u2, u3u3 (CCC), u1u2 (SSC), u2u3 (CSS), u3u1 (SCS), u1T (CCC), u2T (SSC), u3T (SCS)
+  const int vx[4] = {1, 0, 0, 1}, vy[4] = {0, 1, 0, 0}, vz[4] = {0, 0, 1, 0};
+  const int qx[9] = {0, 0, 0, 1, 0, 1, 0, 1, 1}, qy[9] = {0, 0, 0, 1, 1, 0, 0, 1, 0};
+  const int qz[9] = {0, 0, 0, 0, 1, 1, 0, 0, 1};
   for (int stage = 1; stage <= 4; ++stage) {
     const void* Uin = stage == 1 ? U0 : p->Ucur;
-    a.stage = stage;
+    const void* Tin = stage == 1 ? (const void*)T0 : (const void*)((const char*)p->Ucur + 3 * cs);
+    a.stage = b.stage = stage;
+    b.U1in = Uin;
+    b.Tin = Tin;
     {
       ProfScope ps(p, TS_KCLASS_INV_X);
       CK(LAUNCH(p, sss_dealias_copy, g, Uin, P, 3, p->st));
-      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
+      if (T0) CK(LAUNCH(p, sss_dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
+      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_INV);
-      for (int c = 0; c < 3; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
+      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Z);
-      for (int c = 0; c < 3; ++c) {
-        CK(LAUNCH(p, sss_zpre_inv, P + c * cs, P + 6 * cs, nl, g.Nz, vz[c], p->twqz, p->st));
-        CK(LAUNCH(p, z_single, g, +1, P + 6 * cs, P + 7 * cs, 1, p->twz, p->st));
-        CK(LAUNCH(p, sss_zperm_inv, P + 7 * cs, P + (9 + c) * cs, nl, g.Nz, vz[c], p->st));
+      for (int c = 0; c < nf; ++c) {
+        CK(LAUNCH(p, sss_zpre_inv, P + c * cs, s0, nl, g.Nz, vz[c], p->twqz, p->st));
+        CK(LAUNCH(p, z_single, g, +1, s0, s1, 1, p->twz, p->st));
+        CK(LAUNCH(p, sss_zperm_inv, s1, Rf + c * cs, nl, g.Nz, vz[c], p->st));
       }
-      CK(LAUNCH(p, real_products, P + 9 * cs, P, 2 * g.S, p->st));
-      for (int f = 0; f < 6; ++f) {
-        CK(LAUNCH(p, sss_zperm_fwd, P + f * cs, P + 6 * cs, nl, g.Nz, qz[f], p->st));
-        CK(LAUNCH(p, z_single, g, -1, P + 6 * cs, P + 7 * cs, 1, p->twz, p->st));
-        CK(LAUNCH(p, sss_zpost_fwd, P + 7 * cs, P + f * cs, nl, g.Nz, qz[f], 1.0 / (2.0 * g.Nz), p->twqz, p->st));
+      CK(LAUNCH(p, real_products, Rf, P, 2 * g.S, nf, p->st));
+      for (int f = 0; f < np; ++f) {
+        CK(LAUNCH(p, sss_zperm_fwd, P + f * cs, s0, nl, g.Nz, qz[f], p->st));
+        CK(LAUNCH(p, z_single, g, -1, s0, s1, 1, p->twz, p->st));
+        CK(LAUNCH(p, sss_zpost_fwd, s1, P + f * cs, nl, g.Nz, qz[f], 1.0 / (2.0 * g.Nz), p->twqz, p->st));
       }
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_FWD);
-      for (int f = 0; f < 6; ++f)
+      for (int f = 0; f < np; ++f)
         CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], 1.0 / (2.0 * g.Ny), p->twqy, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_FWD_X);
-      for (int f = 0; f < 6; ++f)
+      for (int f = 0; f < np; ++f)
         CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], 1.0 / (2.0 * g.Nx), p->twq, p->st));
-      CK(LAUNCH(p, sss_epi, g, P, a, p->st));
+      if (T0) CK(LAUNCH(p, sss_rbc_epi, g, P, b, p->st));
+      else CK(LAUNCH(p, sss_epi, g, P, a, p->st));
     }
   }
   return TS_OK;
@@ -946,7 +977,7 @@ int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   if (!p || !u_hat || nsteps < 0) return TS_ERR_ARG;
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
     const bool sss = p->cfg.basis == TS_BASIS_SSS;
-    CKS(sss ? sss_step_supported(p) : ssf_step_supported(p));
+    CKS(ssf_step_supported(p, false));
     int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
       for (int s = 0; s < nsteps; ++s) CKS(sss ? step_sss(p, U) : step_ssf(p, U));
       return (int)TS_OK;
@@ -1041,6 +1072,17 @@ int ts_adjoint_window(ts_plan* p, const void* u_start, int nsteps, void* lam_hat
 
 int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   if (!p || !u_hat || !T_hat || nsteps < 0) return TS_ERR_ARG;
+  if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
+    const bool sss = p->cfg.basis == TS_BASIS_SSS;
+    CKS(ssf_step_supported(p, true));
+    const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
+    return with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
+      return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
+        for (int s = 0; s < nsteps; ++s) CKS(sss ? step_sss(p, U, T) : step_ssf(p, U, T));
+        return (int)TS_OK;
+      });
+    });
+  }
   if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
   if (*p->err_h) {
     g_last_error = "a bounded device wait gave up";

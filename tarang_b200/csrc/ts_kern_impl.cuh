@@ -695,14 +695,26 @@ template <> cudaError_t Launch<T>::sss_epi(const Geo& g, const void* P, const St
   return cudaGetLastError();
 }
 
-template <> cudaError_t Launch<T>::real_products(const void* R, void* Q, long long n, cudaStream_t st) {
-  k_real_products<T><<<grid1d(n, 256), 256, 0, st>>>((const T*)R, (T*)Q, n);
+template <> cudaError_t Launch<T>::real_products(const void* R, void* Q, long long n, int nf, cudaStream_t st) {
+  k_real_products<T><<<grid1d(n, 256), 256, 0, st>>>((const T*)R, (T*)Q, n, nf);
   ++g_launches;
   return cudaGetLastError();
 }
 
 template <> cudaError_t Launch<T>::ssf_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st) {
   k_ssf_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::ssf_rbc_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st) {
+  k_ssf_rbc_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::sss_rbc_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st) {
+  k_sss_rbc_epi<T><<<grid1d(2 * g.S, 256), 256, 0, st>>>((const T*)P, g, a);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -54,10 +54,13 @@ template <typename T> struct Launch {
   // SSS fluid step: dealiased copy of real coefficients, and the epilogue
   static cudaError_t sss_dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
   static cudaError_t sss_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st);
-  // six products u_i u_j of three real fields (n reals each)
-  static cudaError_t real_products(const void* R, void* Q, long long n, cudaStream_t st);
+  // six products u_i u_j of three real fields (n reals each); nf = 4 adds u_i T of a fourth
+  static cudaError_t real_products(const void* R, void* Q, long long n, int nf, cudaStream_t st);
   // SSF fluid step: elementwise epilogue of the six forward-transformed products in P
   static cudaError_t ssf_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st);
+  // SSF / SSS Boussinesq step: epilogues of the nine forward-transformed products in P
+  static cudaError_t ssf_rbc_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
+  static cudaError_t sss_rbc_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
   // FFF MHD: elementwise epilogue of the nine x-transformed Elsasser products in P
   static cudaError_t mhd_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);

@@ -685,4 +685,140 @@ __global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Boussinesq RBC (PRLARGE, ULARGE) on the SSF and SSS bases: the temperature takes
+// the Vx parity and the products u_x T, u_y T, u_z T take Vi2, VxVy and VxVz
+// (Global_process_basic_vars.cc:108, 114-116).  Epilogues after the forward
+// transforms of the nine products (u1u1, u2u2, u3u3, u1u2, u2u3, u3u1, u1T, u2T,
+// u3T; normalised):
+//   N as the fluid step; NT = Dx(u1T) + Dy(u2T) + Dz(u3T) (compute_diag_offdiag.cc:116-136);
+//   force (compute_force_RBC.cc:104-150): U.F1 = T, T.F = U.V1, both from the
+//   un-dealiased stage input; N1 -= T, NT -= u1 (Add_force); pressure from N;
+//   R = -N, RT = -NT; IF-RK4 stage update of U (nu, tables eu) and T (kappa,
+//   tables et) as RK_SF.cc:97-221, in place at stage 4; no reality condition.
+// SSF: x and y derivatives of a sine series +K, of a cosine series -K; z: i Kz.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_ssf_rbc_epi(const C<T>* __restrict__ P, Geo g, SffArgs a) {
+  typedef C<T> V;
+  V* U0 = const_cast<V*>(reinterpret_cast<const V*>(a.U0));
+  V* T0 = const_cast<V*>(reinterpret_cast<const V*>(a.T0));
+  const V* U1in = reinterpret_cast<const V*>(a.U1in);
+  const V* Tin = reinterpret_cast<const V*>(a.Tin);
+  V* Uc = reinterpret_cast<V*>(a.Ucur);
+  V* tot = reinterpret_cast<V*>(a.tot);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const double Kxd = lx * g.kf[0], Kyd = ly * g.kf[1], Kzd = lz * g.kf[2];
+    const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+    V q[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) q[f] = P[f * g.S + e];
+    auto dS = [](T K, V A) { return scale(A, K); };
+    auto dC = [](T K, V A) { return scale(A, -K); };
+    V N1 = add(add(dC(Kx, q[0]), dS(Ky, q[3])), ik(Kz, q[5]));
+    V N2 = add(add(dC(Ky, q[1]), dS(Kx, q[3])), ik(Kz, q[4]));
+    V N3 = add(add(ik(Kz, q[2]), dS(Ky, q[4])), dS(Kx, q[5]));
+    V NT = add(add(dC(Kx, q[6]), dS(Ky, q[7])), ik(Kz, q[8]));
+    N1 = sub(N1, Tin[e]);
+    NT = sub(NT, U1in[e]);
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    const V div = add(add(dS(Kx, N1), dS(Ky, N2)), ik(Kz, N3));
+    const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
+    N1 = add(N1, dC(Kx, pr));
+    N2 = add(N2, dC(Ky, pr));
+    N3 = add(N3, ik(Kz, pr));
+    const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
+    const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lz];
+    const double eht = a.et[0][lx] * a.et[1][ly] * a.et[2][lz];
+    const bool dz = dealias_zero(g.dealias, 2, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double eh = i < 3 ? ehu : eht;
+      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const long long o = i * g.S + e;
+      const V R = Rv[i];
+      const V u0 = i < 3 ? U0[o] : T0[e];
+      if (a.stage == 1) {
+        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
+        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+      } else if (a.stage == 2) {
+        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else if (a.stage == 3) {
+        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
+        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      } else {
+        const V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        if (i < 3) U0[o] = un;
+        else T0[e] = un;
+      }
+    }
+  }
+}
+
+// SSS: real coefficients in the padded real layout; every axis sine +K, cosine -K.
+// Parities: u1u1..u3u3 CCC, u1u2 SSC, u2u3 CSS, u3u1 SCS, u1T CCC, u2T SSC, u3T SCS.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sss_rbc_epi(const T* __restrict__ P, Geo g, SffArgs a) {
+  const long long per = 2 * g.S;
+  T* U0 = const_cast<T*>(reinterpret_cast<const T*>(a.U0));
+  T* T0 = const_cast<T*>(reinterpret_cast<const T*>(a.T0));
+  const T* U1in = reinterpret_cast<const T*>(a.U1in);
+  const T* Tin = reinterpret_cast<const T*>(a.Tin);
+  T* Uc = reinterpret_cast<T*>(a.Ucur);
+  T* tot = reinterpret_cast<T*>(a.tot);
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < per; e += (long long)gridDim.x * blockDim.x) {
+    const int lzr = (int)(e % (g.Nz + 2));
+    if (lzr >= g.Nz) continue;  // padding
+    const long long r = e / (g.Nz + 2);
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const double Kxd = lx * g.kf[0], Kyd = ly * g.kf[1], Kzd = lzr * g.kf[2];
+    const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
+    T q[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) q[f] = P[f * per + e];
+    T N1 = (-Kx * q[0] + Ky * q[3]) + Kz * q[5];
+    T N2 = (-Ky * q[1] + Kx * q[3]) + Kz * q[4];
+    T N3 = (-Kz * q[2] + Ky * q[4]) + Kx * q[5];
+    T NT = (-Kx * q[6] + Ky * q[7]) + Kz * q[8];
+    N1 -= Tin[e];
+    NT -= U1in[e];
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    const T div = (Kx * N1 + Ky * N2) + Kz * N3;
+    const T pr = K2 > 0 ? div / (T)K2 : (T)0;
+    N1 += -Kx * pr;
+    N2 += -Ky * pr;
+    N3 += -Kz * pr;
+    const T Rv[4] = {-N1, -N2, -N3, -NT};
+    const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lzr];
+    const double eht = a.et[0][lx] * a.et[1][ly] * a.et[2][lzr];
+    const bool dz = sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double eh = i < 3 ? ehu : eht;
+      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const long long o = i * per + e;
+      const T R = Rv[i], u0 = i < 3 ? U0[o] : T0[e];
+      if (a.stage == 1) {
+        Uc[o] = ((dz ? (T)0 : u0) + (T)(0.5 * a.dt) * R) * Eh;
+        tot[o] = (R * E1) * (T)((1.0 / 6) * a.dt);
+      } else if (a.stage == 2) {
+        Uc[o] = u0 * Eh + (T)(0.5 * a.dt) * R;
+        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+      } else if (a.stage == 3) {
+        Uc[o] = (u0 * Eh + (T)a.dt * R) * Eh;
+        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+      } else {
+        const T un = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
+        if (i < 3) U0[o] = un;
+        else T0[e] = un;
+      }
+    }
+  }
+}
+
 }  // namespace ts

@@ -9,8 +9,8 @@ Inputs (a reference data directory ``<dir>/in/``):
   ``time.init / final / dt_fixed``, ``force.U_switch / W_switch / T_switch /
   field_procedure / parameters``, ``PHYSICS.Pr_option / Uscaling / Rayleigh / Prandtl`` and
   ``energy_transfer.flux.no_spheres / radii``.  Kinds and bases: FLUID_INCOMPRESS on
-  FFF, SSF and SSS, RBC on SFF, SCALAR_INCOMPRESS and MHD_INCOMPRESS on FFF
-  (``diss_coefficients`` = [nu, kappa] or [nu, eta]).  Any other kind or basis is
+  FFF, SSF and SSS; RBC on SFF, SSF and SSS; SCALAR_INCOMPRESS and MHD_INCOMPRESS on
+  FFF (``diss_coefficients`` = [nu, kappa] or [nu, eta]).  Any other kind or basis is
   refused by name (NotImplementedError), never silently changed.
 * ``initial.txt`` / ``forcing.txt`` — Blitz++ 1-D arrays as text,
   ``(lb,ub)`` then ``[ v0 v1 ... ]`` (``Global::Read_IC_energy_supply_arrays``,
@@ -41,9 +41,10 @@ import numpy as np
 INF_RADIUS = 1e9   # the last flux sphere encloses every mode
 
 # (program.kind, basis_type) pairs this library steps (solvers/main.cc:113-130 picks the
-# solver by kind): the fluid on FFF, SSF and SSS, RBC on SFF, the passive scalar and MHD on FFF
+# solver by kind): the fluid on FFF, SSF and SSS, RBC on SFF, SSF and SSS, the passive scalar
+# and MHD on FFF
 STEPPED = (("FLUID_INCOMPRESS", "FFF"), ("FLUID_INCOMPRESS", "SSF"), ("FLUID_INCOMPRESS", "SSS"),
-           ("RBC", "SFF"), ("SCALAR_INCOMPRESS", "FFF"), ("MHD_INCOMPRESS", "FFF"))
+           ("RBC", "SFF"), ("RBC", "SSF"), ("RBC", "SSS"), ("SCALAR_INCOMPRESS", "FFF"), ("MHD_INCOMPRESS", "FFF"))
 
 
 @dataclass
@@ -122,7 +123,8 @@ def read_para(path: str) -> RunParams:
     """The hot-path subset of a reference ``para.yaml``."""
     import yaml
     with open(path) as f:
-        p = yaml.safe_load(f)
+        # yaml-cpp accepts trailing tabs and tab-only lines, which PyYAML rejects; strip them
+        p = yaml.safe_load("\n".join(line.rstrip() for line in f.read().split("\n")))
     prog, fld, tim = p["program"], p["field"], p["time"]
     kind = str(prog["kind"]).strip()
     basis = str(prog["basis_type"]).strip()
@@ -130,7 +132,8 @@ def read_para(path: str) -> RunParams:
         raise NotImplementedError(f"program.kind {kind} with basis_type {basis}: this library steps "
                                   + ", ".join(f"{k} on {b}" for k, b in STEPPED))
     N = tuple(int(n) for n in fld["N"])
-    # kfactor, else from L, else the basis defaults (FFF_pencil.cc:34-66, SFF_pencil.cc:40-80)
+    # kfactor, else from L, else the basis defaults (FFF_pencil.cc:34-66, SFF_pencil.cc:40-80,
+    # SSF_pencil.cc:40-80, SSS_pencil.cc:40-80: RBC (pi, pi/sqrt2, pi/sqrt2), otherwise 1)
     if fld.get("kfactor") and len(fld["kfactor"]) == 3:
         kf = tuple(float(k) for k in fld["kfactor"])
     elif fld.get("L") and len(fld["L"]) == 3:
@@ -172,7 +175,7 @@ def read_para(path: str) -> RunParams:
             if procs != [1]:
                 raise NotImplementedError(f"force.field_procedure {procs}: Carati energy supply (1) only")
             params = force.get("parameters") or []
-            words = str(params[0] if isinstance(params, list) else params).split()
+            words = str(params[0] if isinstance(params, list) and params else params or "").split()
             if not words or words[0] != "ENERGY_SUPPLY" or len(words) < 4:
                 raise NotImplementedError(f"force.parameters {params}: 'ENERGY_SUPPLY global inner outer' only")
             rp.force_on = True
@@ -203,7 +206,7 @@ def plan_from_dir(data_dir: str, precision: str = "f64", nlin_form: str = "conse
         forcing = Forcing(rp.force_inner, rp.force_outer, arrs[0], arrs[1] if len(arrs) > 1 else None)
     kw = dict(precision=precision, dealias=rp.dealias, kfactor=rp.kfactor, reality_fix=rp.reality_fix, dt=rp.dt)
     if rp.kind == "RBC":
-        plan = Plan(rp.N, basis="SFF", nu=rp.nu, kappa=rp.kappa, Ra=rp.Ra, Pr=rp.Pr, **kw)
+        plan = Plan(rp.N, basis=rp.basis, nu=rp.nu, kappa=rp.kappa, Ra=rp.Ra, Pr=rp.Pr, **kw)
     elif rp.kind in ("SCALAR_INCOMPRESS", "MHD_INCOMPRESS"):
         # the second dissipation coefficient: kappa of T, or eta of B (stored as the plan's kappa)
         plan = Plan(rp.N, nlin_form="conservative", nu=rp.nu, kappa=rp.kappa, **kw)

@@ -53,7 +53,9 @@ def test_ssf_plan_rejects_other_calls(cuda):
     with pytest.raises(tb.TsError):
         plan.energy(u)
     with pytest.raises(tb.TsError):
-        plan.rk4_step_rbc(u, plan.field(1), 1)
+        plan.rk4_step_scalar(u, plan.field(1), 1)   # the passive-scalar step is FFF only
+    with pytest.raises(tb.TsError):
+        plan.rk4_step_mhd(u, plan.field(3), 1)
     with pytest.raises(tb.TsError):
         tb.Plan(32, basis="SSF", kfactor=KF, nlin_form="rotational")
     real = plan.field(1)
@@ -106,3 +108,54 @@ def test_ssf_taylor_green_decays_exactly(cuda):
     u = torch.from_numpy(U0).to(cuda)
     plan.rk4_step(u, 5)
     assert np.max(np.abs(u.cpu().numpy() - U0 * np.exp(-0.05 * 2 * 5e-2))) < 1e-15
+
+
+KF_RBC = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))   # SSF_PENCIL's RBC default
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,dealias", [((16, 16, 16), "reference"), ((32, 16, 32), "none"),
+                                       ((48, 32, 16), "two_thirds"), ((32, 32, 32), "reference")])
+def test_ssf_rbc_step_matches_oracle(cuda, N, dealias, prec):
+    """RBC on SSF (ts_rk4_step_rbc on an SSF plan; T = SCF) over 3 steps against the oracle."""
+    import torch
+    import tarang_b200 as tb
+    mode = {"none": 0, "reference": 1, "two_thirds": 2}[dealias]
+    g = R.Grid(N, KF_RBC, "SSF")
+    U0 = 0.3 * ssf_state(g, 5)
+    rng = np.random.default_rng(9)
+    T0 = 0.3 * R.forward(g, rng.standard_normal(g.rshape), "SCF")
+    cfg = R.RBCConfig(g, Ra=1e5, Pr=0.7, dt=1e-3, dealias_mode=mode)
+    Uo, To = U0.copy(), T0.copy()
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    plan = tb.Plan(N, basis="SSF", kfactor=KF_RBC, precision=prec, nu=cfg.nu, kappa=cfg.kappa, dt=1e-3,
+                   dealias=dealias, Ra=1e5, Pr=0.7)
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    u = torch.from_numpy(U0).to(cuda).to(cdt)
+    T = torch.from_numpy(T0).to(cuda).to(cdt)
+    plan.rk4_step_rbc(u, T, 3)
+    plan.status()
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel(u.cpu().numpy().astype(np.complex128), Uo) < tol
+    assert rel(T.cpu().numpy().astype(np.complex128), To) < tol
+
+
+def test_ssf_rbc_roll_follows_linear_theory(cuda):
+    """One small roll (u_x, theta in sin(kx x) cos(ky y)) grows or decays as the linear
+    system da/dt = (1 - kx^2/K^2) b - nu K^2 a, db/dt = a - kappa K^2 b predicts."""
+    from scipy.linalg import expm
+    import tarang_b200 as tb
+    N = (16, 16, 16)
+    eps, nu, kappa, dt, n = 1e-9, 0.01, 0.02, 2e-3, 25
+    plan = tb.Plan(N, basis="SSF", kfactor=KF_RBC, nu=nu, kappa=kappa, dt=dt)
+    u, T = plan.field(3), plan.field(1)
+    kx, ky = KF_RBC[0], KF_RBC[1]
+    u[0, 1, 1, 0] = eps
+    u[1, 1, 1, 0] = -kx * eps / ky
+    T.view(N[0], N[1], -1)[1, 1, 0] = 0.5 * eps
+    plan.rk4_step_rbc(u, T, n)
+    K2 = kx * kx + ky * ky
+    a, b = expm(np.array([[-nu * K2, 1 - kx * kx / K2], [1.0, -kappa * K2]]) * n * dt) @ np.array([eps, 0.5 * eps])
+    assert abs(u[0, 1, 1, 0].item() - a) < 1e-7 * eps
+    assert abs(T.view(N[0], N[1], -1)[1, 1, 0].item() - b) < 1e-7 * eps

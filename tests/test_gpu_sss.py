@@ -112,3 +112,64 @@ def test_sss_taylor_green_decays_exactly(cuda):
     u = torch.from_numpy(to_padded(U0)).to(cuda)
     plan.rk4_step(u, 5)
     assert np.max(np.abs(from_padded(u, 16) - U0 * np.exp(-0.05 * 2 * 5e-2))) < 1e-15
+
+
+KF_RBC = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))   # SSS_PENCIL's RBC default
+
+
+def _dev(A, cuda, prec):
+    """real coefficients (c, Nx, Ny, Nz) -> the padded layout on the device, as complex"""
+    import torch
+    c, Nx, Ny, Nz = A.shape
+    t = torch.from_numpy(to_padded(A).view(np.float64).reshape(c, Nx, Ny, Nz // 2 + 1, 2))
+    return torch.view_as_complex(t.to(torch.float64 if prec == "f64" else torch.float32).contiguous()).to(cuda)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,dealias", [((16, 16, 16), "reference"), ((32, 16, 32), "none"),
+                                       ((32, 32, 16), "two_thirds"), ((16, 32, 16), "reference")])
+def test_sss_rbc_step_matches_oracle(cuda, N, dealias, prec):
+    """RBC on SSS (ts_rk4_step_rbc on an SSS plan; T = SCC, real coefficients) over 3 steps."""
+    import tarang_b200 as tb
+    mode = {"none": 0, "reference": 1, "two_thirds": 2}[dealias]
+    g = R.Grid(N, KF_RBC, "SSS")
+    rng = np.random.default_rng(6)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCC", "CSC", "CCS")])
+    U0 = -0.3 * R.project_rhs(g, U)
+    T0 = 0.3 * R.forward(g, rng.standard_normal(g.rshape), "SCC")
+    cfg = R.RBCConfig(g, Ra=1e5, Pr=0.7, dt=1e-3, dealias_mode=mode)
+    Uo, To = U0.copy(), T0.copy()
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    plan = tb.Plan(N, basis="SSS", kfactor=KF_RBC, precision=prec, nu=cfg.nu, kappa=cfg.kappa, dt=1e-3,
+                   dealias=dealias, Ra=1e5, Pr=0.7)
+    u = _dev(U0, cuda, prec)
+    T = _dev(T0[None], cuda, prec)
+    plan.rk4_step_rbc(u, T, 3)
+    plan.status()
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel(from_padded(u, N[2]), Uo) < tol
+    assert rel(from_padded(T, N[2])[0], To) < tol
+
+
+def test_sss_rbc_roll_follows_linear_theory(cuda):
+    """One small roll (u_x, theta in sin(kx x) cos(ky y) cos(kz z)) with u_y balancing the
+    divergence: (a, b) follow da/dt = (1 - kx^2/K^2) b - nu K^2 a, db/dt = a - kappa K^2 b."""
+    from scipy.linalg import expm
+    import tarang_b200 as tb
+    N = (16, 16, 16)
+    eps, nu, kappa, dt, n = 1e-9, 0.01, 0.02, 2e-3, 25
+    g = R.Grid(N, KF_RBC, "SSS")
+    U0 = np.zeros((3,) + g.shape)
+    T0 = np.zeros((1,) + g.shape)
+    kx, ky, kz = KF_RBC
+    U0[0, 1, 1, 1] = eps
+    U0[1, 1, 1, 1] = -kx * eps / ky
+    T0[0, 1, 1, 1] = 0.5 * eps
+    plan = tb.Plan(N, basis="SSS", kfactor=KF_RBC, nu=nu, kappa=kappa, dt=dt)
+    u, T = _dev(U0, cuda, "f64"), _dev(T0, cuda, "f64")
+    plan.rk4_step_rbc(u, T, n)
+    K2 = kx * kx + ky * ky + kz * kz
+    a, b = expm(np.array([[-nu * K2, 1 - kx * kx / K2], [1.0, -kappa * K2]]) * n * dt) @ np.array([eps, 0.5 * eps])
+    assert abs(from_padded(u, N[2])[0, 1, 1, 1] - a) < 1e-7 * eps
+    assert abs(from_padded(T, N[2])[0, 1, 1, 1] - b) < 1e-7 * eps

@@ -359,3 +359,35 @@ def test_sss_transforms_and_taylor_green():
     for _ in range(5):
         U = R.rk4_step(cfg, U)
     assert np.max(np.abs(U - U0 * np.exp(-0.05 * 2 * 5e-2))) < 1e-15
+
+
+@pytest.mark.parametrize("basis", ["SSF", "SSS"])
+def test_rbc_single_roll_follows_linear_theory(basis):
+    """RBC on SSF / SSS (PRLARGE, ULARGE; the temperature takes the Vx parity): one small
+    roll u_x = a sin(kx x) cos(ky y), u_y = c cos(kx x) sin(ky y), theta = b sin(kx x) cos(ky y)
+    obeys da/dt = (1 - kx^2/K^2) b - nu K^2 a, db/dt = a - kappa K^2 b to O(amplitude):
+    compared with the matrix exponential of that system over 20 steps."""
+    from scipy.linalg import expm
+    kf = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+    g = R.Grid((16, 16, 8), kf, basis)
+    eps = 1e-9
+    U0 = np.zeros((3,) + g.shape, np.float64 if basis == "SSS" else complex)
+    T0 = np.zeros(g.shape, U0.dtype)
+    kx, ky = kf[0], kf[1]
+    U0[0, 1, 1, 0] = eps
+    U0[1, 1, 1, 0] = -kx * eps / ky   # kx a + ky c = 0
+    T0[1, 1, 0] = 0.5 * eps
+    cfg = R.RBCConfig(g, Ra=3e4, Pr=0.7, dt=2e-3)
+    U, T = U0.copy(), T0.copy()
+    for _ in range(20):
+        U, T = R.rbc_rk4_step(cfg, U, T)
+    K2 = kx * kx + ky * ky
+    M = np.array([[-cfg.nu * K2, 1 - kx * kx / K2], [1.0, -cfg.kappa * K2]])
+    a, b = expm(M * 20 * cfg.dt) @ np.array([eps, 0.5 * eps])
+    assert abs(U[0, 1, 1, 0] - a) < 1e-7 * eps and abs(T[1, 1, 0] - b) < 1e-7 * eps
+    assert abs(U[0, 1, 1, 0] / U0[0, 1, 1, 0] - 1) > 1e-3   # the buoyancy did act
+    # the roll stays in its mode: kx a + ky c = 0, and nothing else grows at first order
+    assert abs(kx * U[0, 1, 1, 0] + ky * U[1, 1, 1, 0]) < 1e-7 * eps
+    U[:, 1, 1, 0] = 0
+    T[1, 1, 0] = 0
+    assert np.max(np.abs(U)) < 1e-6 * eps and np.max(np.abs(T)) < 1e-6 * eps

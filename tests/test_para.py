@@ -14,7 +14,7 @@ from tarang_b200 import para
 HERE = os.path.dirname(os.path.abspath(__file__))
 FFF_DIR = os.path.join(HERE, "golden", "para_fff")
 RBC_DIR = os.path.join(HERE, "golden", "para_rbc")
-KIND_DIRS = {k: os.path.join(HERE, "golden", f"para_{k}") for k in ("mhd", "scalar", "ssf", "sss")}
+KIND_DIRS = {k: os.path.join(HERE, "golden", f"para_{k}") for k in ("mhd", "scalar", "ssf", "sss", "rbc_sss")}
 
 
 def test_read_para_fff_forced():
@@ -50,6 +50,10 @@ def test_read_para_other_kinds():
     assert (rp.kind, rp.basis, rp.kfactor, rp.nu, rp.nsteps) == ("FLUID_INCOMPRESS", "SSF", (1.0, 1.0, 1.0), 0.02, 3)
     rp = para.read_para(os.path.join(KIND_DIRS["sss"], "in", "para.yaml"))
     assert (rp.basis, rp.N, rp.kfactor, rp.dealias) == ("SSS", (16, 32, 16), (1.0, 1.0, 1.0), "reference")
+    rp = para.read_para(os.path.join(KIND_DIRS["rbc_sss"], "in", "para.yaml"))
+    assert (rp.kind, rp.basis, rp.Ra, rp.Pr, rp.nsteps, rp.force_on) == ("RBC", "SSS", 2e4, 0.7, 3, False)
+    assert np.allclose(rp.kfactor, (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0)))
+    assert math.isclose(rp.nu, math.sqrt(0.7 / 2e4)) and math.isclose(rp.kappa, 1 / math.sqrt(0.7 * 2e4))
     assert [para.n_fields(k) for k in ("FLUID_INCOMPRESS", "RBC", "SCALAR_INCOMPRESS", "MHD_INCOMPRESS")] == [1, 2, 2, 2]
     with pytest.raises(ValueError):
         para.advance(None, "MHD_INCOMPRESS", (None,), 1)
@@ -133,7 +137,10 @@ def _kind_state(g, kind, basis):
     if basis in ("SSF", "SSS"):
         par = R.SSF_PARITY if basis == "SSF" else R.SSS_PARITY
         U = np.stack([R.forward(g, rng.standard_normal(g.rshape), par[v]) for v in ("Vx", "Vy", "Vz")])
-        return (-0.3 * R.project_rhs(g, U),)
+        U = -0.3 * R.project_rhs(g, U)
+        if kind == "RBC":
+            return U, 0.3 * R.forward(g, rng.standard_normal(g.rshape), par["F"])
+        return (U,)
     U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
     if kind == "MHD_INCOMPRESS":
         return U, R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 1, 0.3)
@@ -146,6 +153,8 @@ def _kind_oracle(g, rp, state):
     for _ in range(rp.nsteps):
         if rp.kind == "FLUID_INCOMPRESS":
             out = [R.rk4_step(R.FluidConfig(g, nu=rp.nu, dt=rp.dt, dealias_mode=1, nlin_form="conservative"), out[0])]
+        elif rp.kind == "RBC":
+            out = list(R.rbc_rk4_step(R.RBCConfig(g, Ra=rp.Ra, Pr=rp.Pr, dt=rp.dt, dealias_mode=1), *out))
         elif rp.kind == "MHD_INCOMPRESS":
             out = list(R.mhd_rk4_step(R.MHDConfig(g, nu=rp.nu, eta=rp.kappa, dt=rp.dt, dealias_mode=1), *out))
         else:
@@ -154,10 +163,11 @@ def _kind_oracle(g, rp, state):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["mhd", "scalar", "ssf", "sss"])
+@pytest.mark.parametrize("name", ["mhd", "scalar", "ssf", "sss", "rbc_sss"])
 def test_plan_from_para_other_kinds_step_like_the_oracle(cuda, name):
-    """MHD, passive-scalar, SSF and SSS runs set up from a para.yaml, stepped through
-    para.advance, match the FP64 oracle over the run's 3 steps (relative L2 <= 1e-12)."""
+    """MHD, passive-scalar, SSF and SSS fluid and SSS RBC runs set up from a para.yaml,
+    stepped through para.advance, match the FP64 oracle over the run's 3 steps
+    (relative L2 <= 1e-12)."""
     import torch
     from oracle import tarang_ref as R
     plan, rp = para.plan_from_dir(KIND_DIRS[name], precision="f64")
@@ -167,9 +177,11 @@ def test_plan_from_para_other_kinds_step_like_the_oracle(cuda, name):
     Nz = rp.N[2]
     if rp.basis == "SSS":
         # real coefficients in the padded real layout (Nx, Ny, Nz + 2), viewed as complex
-        pad = np.zeros(state[0].shape[:3] + (Nz + 2,))
-        pad[..., :Nz] = state[0]
-        fields = [torch.from_numpy(pad.view(np.complex128)).to(cuda)]
+        fields = []
+        for s in state:
+            pad = np.zeros(s.shape[:-1] + (Nz + 2,))
+            pad[..., :Nz] = s
+            fields.append(torch.from_numpy(pad.view(np.complex128)).to(cuda))
     else:
         fields = [torch.from_numpy(s.copy()).to(cuda) for s in state]
     para.advance(plan, rp.kind, fields, rp.nsteps)
