@@ -147,7 +147,10 @@ int ts_rk4_step_mhd(ts_plan* plan, void* u_hat, void* b_hat, int nsteps);
  * mode (init_cond_main.cc:48-78); this is the benchmark's seeded stand-in. */
 int ts_init_temperature_perturbation(ts_plan* plan, double amp, double kmax, uint64_t seed, void* T_hat);
 
-/* CVF::Compute_total_energy (Cvf.cc:213-221): sum over ncomp components. */
+/* CVF::Compute_total_energy (Cvf.cc:213-221): sum over ncomp components, with the
+ * basis's weights (FFF_pencil_energy.cc, SFF_pencil_energy.cc:76-95, and on SSF / SSS
+ * the Multiplicity_factor weights 4 / 2 / 1 / 1/2 of SSF_pencil_energy.cc:76-103,
+ * SSS_pencil_energy.cc:69-98; SSS coefficients real in the padded layout). */
 int ts_energy(ts_plan* plan, const void* a_hat, int ncomp, double* energy);
 /* Universal::Compute_shell_spectrum (universal_energy.cc:279-366), summed over
  * ncomp components: Ek[n_shells]. */
@@ -169,7 +172,8 @@ int ts_shell_sums(ts_plan* plan, const void* a_hat, const void* b_hat, int ncomp
 int ts_force_field(ts_plan* plan, const void* u_hat, void* f_hat);
 /* max |div U| (universal_basic.cc:343-356). */
 int ts_max_div(ts_plan* plan, const void* u_hat, double* max_div);
-/* Nusselt number, PRLARGE/ULARGE (Correlation.cc:154-156). */
+/* Nusselt number, PRLARGE/ULARGE (Correlation.cc:154-156): 1 + 2 sqrt(Ra Pr) <U1, T>,
+ * on SFF, SSF and SSS plans. */
 int ts_nusselt(ts_plan* plan, const void* u_hat, const void* T_hat, double* Nu);
 
 /* Random-phase solenoidal FFF field with shell energies E_ic[n] (construction of

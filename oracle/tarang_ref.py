@@ -632,14 +632,30 @@ def rk4_step(cfg: FluidConfig, U0: np.ndarray, mis: np.ndarray | None = None) ->
 # ----------------------------------------------------------------------------
 # diagnostics
 # ----------------------------------------------------------------------------
+def _sincos3_sum(d: np.ndarray, d0: float) -> float:
+    """SSF / SSS Get_local_energy plane sums (SSF_pencil_energy.cc:76-103,
+    SSS_pencil_energy.cc:69-98): 4 sum d, minus 2 on each of the lx = 0, ly = 0 and
+    lz = 0 planes, plus the lines where two of them meet, minus d0 / 2 at the origin
+    (d0 = the product of the real parts there)."""
+    e = 4 * d.sum()
+    e += -2 * d[0].sum() + d[0, :, 0].sum()
+    e += d[0, 0, :].sum() - 0.5 * d0
+    e += -2 * d[:, 0, :].sum() + d[:, 0, 0].sum()
+    e += -2 * d[:, :, 0].sum()
+    return float(e)
+
+
 def total_energy(g: Grid, V: np.ndarray) -> float:
     """CVF::Compute_total_energy: per component sum|A|^2 - 1/2 sum_{kz=0}|A|^2 (FFF);
-    SFF weights 2 / 1 / 1/2 (SFF_pencil_energy.cc:76-95)."""
+    SFF weights 2 / 1 / 1/2 (SFF_pencil_energy.cc:76-95); SSF and SSS weights
+    4 / 2 / 1 / 1/2 by the number of zero indices (_sincos3_sum)."""
     e = 0.0
     for A in V:
         a2 = np.abs(A) ** 2
         if g.basis == "FFF":
             e += a2.sum() - 0.5 * a2[:, :, 0].sum()
+        elif g.basis in ("SSF", "SSS"):
+            e += _sincos3_sum(a2, float(np.real(A[0, 0, 0])) ** 2)
         else:
             e += 2 * a2.sum() - a2[:, :, 0].sum() - a2[0].sum() + 0.5 * a2[0, :, 0].sum()
     return float(e)
@@ -654,6 +670,8 @@ def cross_energy(g: Grid, A: np.ndarray, B: np.ndarray) -> float:
     d = (A * np.conj(B)).real
     if g.basis == "FFF":
         return float(d.sum() - 0.5 * d[:, :, 0].sum())
+    if g.basis in ("SSF", "SSS"):
+        return _sincos3_sum(d, float(np.real(A[0, 0, 0]) * np.real(B[0, 0, 0])))
     return float(2 * d.sum() - d[:, :, 0].sum() - d[0].sum() + 0.5 * d[0, :, 0].sum())
 
 

@@ -1174,7 +1174,6 @@ int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
 }
 
 int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
-  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || !energy || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
   return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
@@ -1290,9 +1289,8 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
 }
 
 int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
-  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !T_hat || !Nu) return TS_ERR_ARG;
-  if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
+  if (p->cfg.basis == TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   if (!is_device_ptr(u_hat) || !is_device_ptr(T_hat)) return TS_ERR_ARG;
   CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
   CK(LAUNCH(p, energy, p->g, u_hat, T_hat, 1, p->dscr, p->st));

@@ -181,9 +181,16 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 
 // plane weights of the total energy: FFF 1/2 on kz=0 (FFF_pencil_energy.cc:59-68);
-// SFF 2, minus 1 on kz=0, minus 1 on m=0, plus 1/2 on (m=0,kz=0) (SFF_pencil_energy.cc:76-95)
-__device__ __forceinline__ double energy_weight(int basis, int lx, int lz) {
+// SFF 2, minus 1 on kz=0, minus 1 on m=0, plus 1/2 on (m=0,kz=0) (SFF_pencil_energy.cc:76-95);
+// SSF and SSS: 4 sum, minus 2 on each of the lx = 0, ly = 0, lz = 0 planes, plus the
+// lines where two meet, minus 1/2 at the origin (SSF_pencil_energy.cc:76-103,
+// SSS_pencil_energy.cc:69-98), i.e. 4, 2, 1, 1/2 for none, one, two, three zero indices
+__device__ __forceinline__ double energy_weight(int basis, int lx, int ly, int lz) {
   if (basis == 0) return lz == 0 ? 0.5 : 1.0;
+  if (basis >= 2) {
+    const int zeros = (lx == 0) + (ly == 0) + (lz == 0);
+    return zeros == 0 ? 4.0 : zeros == 1 ? 2.0 : zeros == 2 ? 1.0 : 0.5;
+  }
   double w = 2.0;
   if (lz == 0) w -= 1.0;
   if (lx == 0) w -= 1.0;
@@ -191,20 +198,32 @@ __device__ __forceinline__ double energy_weight(int basis, int lx, int lz) {
   return w;
 }
 
-// out[0] += sum_w Re(A.conj(B)) over ncomp components (A == B gives the energy)
+// out[0] += sum_w Re(A.conj(B)) over ncomp components (A == B gives the energy).
+// SSS: the coefficients are real, two per complex slot, z index 2 lz and 2 lz + 1
+// (the padding reals at Nz, Nz + 1 are skipped).  SSF: at the origin the reference
+// subtracts half the product of the real parts only (1/2 Re a Re b + Im a Im b).
 template <typename T>
 __global__ void k_energy(const C<T>* __restrict__ A, const C<T>* __restrict__ B, int ncomp, Geo g, double* out) {
   const long long n = g.S;
   double s = 0;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
     const int lx = (int)(e / ((long long)g.Ny * g.Hz));
-    double d = 0;
+    double dr = 0, di = 0;
     for (int i = 0; i < ncomp; ++i) {
       const C<T> a = A[i * n + e], b = B[i * n + e];
-      d += (double)a.x * b.x + (double)a.y * b.y;
+      dr += (double)a.x * b.x;
+      di += (double)a.y * b.y;
     }
-    s += energy_weight(g.basis, lx, lz) * d;
+    if (g.basis == 3) {
+      s += energy_weight(3, lx, ly, 2 * lz) * dr;
+      if (2 * lz + 1 < g.Nz) s += energy_weight(3, lx, ly, 2 * lz + 1) * di;
+    } else if (g.basis == 2 && lx == 0 && ly == 0 && lz == 0) {
+      s += 0.5 * dr + di;
+    } else {
+      s += energy_weight(g.basis, lx, ly, lz) * (dr + di);
+    }
   }
   s = block_sum(s);
   if (threadIdx.x == 0) out[1 + blockIdx.x] = s;  // partial sums, added in a fixed order by k_sum_partials

@@ -51,7 +51,7 @@ def test_ssf_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSF", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.energy(u)
+        plan.max_div(u)
     with pytest.raises(tb.TsError):
         plan.rk4_step_scalar(u, plan.field(1), 1)   # the passive-scalar step is FFF only
     with pytest.raises(tb.TsError):
@@ -159,3 +159,27 @@ def test_ssf_rbc_roll_follows_linear_theory(cuda):
     a, b = expm(np.array([[-nu * K2, 1 - kx * kx / K2], [1.0, -kappa * K2]]) * n * dt) @ np.array([eps, 0.5 * eps])
     assert abs(u[0, 1, 1, 0].item() - a) < 1e-7 * eps
     assert abs(T.view(N[0], N[1], -1)[1, 1, 0].item() - b) < 1e-7 * eps
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_ssf_energy_and_nusselt_match_oracle(cuda, prec):
+    """ts_energy with the SSF weights (Multiplicity_factor 4 / 2 / 1 / 1/2) and the Nusselt
+    number 1 + 2 sqrt(Ra Pr) <U1, T> on an SSF plan, against the oracle."""
+    import torch
+    import tarang_b200 as tb
+    N = (32, 16, 32)
+    g = R.Grid(N, KF_RBC, "SSF")
+    U = 0.3 * ssf_state(g, 3)
+    rng = np.random.default_rng(4)
+    T = 0.3 * R.forward(g, rng.standard_normal(g.rshape), "SCF")
+    cfg = R.RBCConfig(g, Ra=2e5, Pr=0.7, dt=1e-3)
+    plan = tb.Plan(N, basis="SSF", kfactor=KF_RBC, precision=prec, nu=cfg.nu, kappa=cfg.kappa, Ra=2e5, Pr=0.7)
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    u = torch.from_numpy(U).to(cuda).to(cdt)
+    t = torch.from_numpy(T[None]).to(cuda).to(cdt)
+    Ur = u.cpu().numpy().astype(np.complex128)   # the values the device holds
+    Tr = t.cpu().numpy().astype(np.complex128)[0]
+    tol = 1e-12 if prec == "f64" else 1e-6
+    assert abs(plan.energy(u) / R.total_energy(g, Ur) - 1) < tol
+    assert abs(plan.energy(t) / R.total_energy_scalar(g, Tr) - 1) < tol
+    assert abs(plan.nusselt(u, t) - R.nusselt(cfg, Ur, Tr)) < tol * abs(R.nusselt(cfg, Ur, Tr))

@@ -52,7 +52,7 @@ def test_sss_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSS", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.energy(u)
+        plan.max_div(u)
     with pytest.raises(tb.TsError):
         tb.Plan(32, basis="SSS", kfactor=KF, nlin_form="rotational")
     with pytest.raises(tb.TsError):
@@ -173,3 +173,26 @@ def test_sss_rbc_roll_follows_linear_theory(cuda):
     a, b = expm(np.array([[-nu * K2, 1 - kx * kx / K2], [1.0, -kappa * K2]]) * n * dt) @ np.array([eps, 0.5 * eps])
     assert abs(from_padded(u, N[2])[0, 1, 1, 1] - a) < 1e-7 * eps
     assert abs(from_padded(T, N[2])[0, 1, 1, 1] - b) < 1e-7 * eps
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_sss_energy_and_nusselt_match_oracle(cuda, prec):
+    """ts_energy on real SSS coefficients (weights 4 / 2 / 1 / 1/2, padding skipped) and the
+    Nusselt number on an SSS plan, against the oracle; the energy equals <u^2>/2 in real space."""
+    import tarang_b200 as tb
+    N = (16, 32, 16)
+    g = R.Grid(N, KF_RBC, "SSS")
+    rng = np.random.default_rng(8)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCC", "CSC", "CCS")])
+    U = -0.3 * R.project_rhs(g, U)
+    T = 0.3 * R.forward(g, rng.standard_normal(g.rshape), "SCC")
+    cfg = R.RBCConfig(g, Ra=2e5, Pr=0.7, dt=1e-3)
+    plan = tb.Plan(N, basis="SSS", kfactor=KF_RBC, precision=prec, nu=cfg.nu, kappa=cfg.kappa, Ra=2e5, Pr=0.7)
+    u, t = _dev(U, cuda, prec), _dev(T[None], cuda, prec)
+    Ur, Tr = from_padded(u, N[2]), from_padded(t, N[2])[0]   # the values the device holds
+    tol = 1e-12 if prec == "f64" else 1e-6
+    assert abs(plan.energy(u) / R.total_energy(g, Ur) - 1) < tol
+    assert abs(plan.energy(t) / R.total_energy_scalar(g, Tr) - 1) < tol
+    assert abs(plan.nusselt(u, t) - R.nusselt(cfg, Ur, Tr)) < tol * abs(R.nusselt(cfg, Ur, Tr))
+    ur = R.inverse(g, Tr, "SCC")
+    assert abs(plan.energy(t) / (0.5 * np.mean(ur ** 2)) - 1) < tol

@@ -391,3 +391,18 @@ def test_rbc_single_roll_follows_linear_theory(basis):
     U[:, 1, 1, 0] = 0
     T[1, 1, 0] = 0
     assert np.max(np.abs(U)) < 1e-6 * eps and np.max(np.abs(T)) < 1e-6 * eps
+
+
+@pytest.mark.parametrize("basis,parity", [("SSF", "SCF"), ("SSF", "CCF"), ("SSF", "SSF"), ("SSS", "SCC"),
+                                          ("SSS", "CCC"), ("SSS", "SSS"), ("SSS", "CSS")])
+def test_sincos_energy_weights_are_parseval(basis, parity):
+    """The SSF / SSS energy weights (4 / 2 / 1 / 1/2 by the number of zero indices) give
+    <u^2>/2 of the real field; on SSF with the kz = Nz/2 plane empty, which the reference
+    weights like an interior plane."""
+    g = R.Grid((16, 8, 16), (1.0, 1.0, 1.0), basis)
+    A = R.forward(g, np.random.default_rng(2).standard_normal(g.rshape), parity)
+    if basis == "SSF":
+        A[:, :, -1] = 0
+    u = R.inverse(g, A, parity)
+    assert abs(R.total_energy_scalar(g, A) / (0.5 * np.mean(u ** 2)) - 1) < 1e-13
+    assert abs(R.cross_energy(g, A, A) - R.total_energy_scalar(g, A)) < 1e-13
