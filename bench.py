@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--form", default="rotational", choices=["rotational", "conservative"])
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
     ap.add_argument("--workload", default="fff256",
-                    choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint", "scalar", "mhd", "ssf", "sss"],
+                    choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint", "scalar", "mhd", "ssf", "sss",
+                             "rbc_ssf", "rbc_sss"],
                     help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying "
                          "1024^3 (or --shape); rbc: one RBC run (SFF, --N, FP32); adjoint: adjoint/forward cost at 128^3")
     ap.add_argument("--tune", default="auto", choices=["auto", "off"],
@@ -226,29 +227,42 @@ def coupled_leg(kind: str, N: int, steps: int, warmup: int, prec: str = "f32"):
             "model_frac": model * steps / (ms / 1e3) / 1e9 / measured_peak()[0]}
 
 
-def ssf_leg(N: int, steps: int, warmup: int, prec: str = "f32", basis: str = "SSF"):
+def ssf_leg(N: int, steps: int, warmup: int, prec: str = "f32", basis: str = "SSF", rbc: bool = False):
     """SSF (sin/cos along x and y) or SSS (along every axis) fluid step at N^3: conservative,
     unforced, nu = 1e-3, dt = 5e-4, reference dealias, kfactor (pi, pi, 2 pi) / (pi, pi, pi);
     a small seeded random spectral field (amplitude 1e-3; the timing does not depend on the
-    values).  Steps/s, CUDA events."""
+    values).  With rbc, the Boussinesq step (Ra = 1e6, Pr = 1, ULARGE nu / kappa, dt = 1e-4,
+    the basis's RBC kfactor (pi, pi/sqrt2, pi/sqrt2)) with a seeded temperature of the same
+    amplitude.  Steps/s, CUDA events."""
     import torch
     import tarang_b200 as tb
-    plan = tb.Plan(N, basis=basis, precision=prec, nu=1e-3, dt=5e-4, dealias="reference",
-                   kfactor=(math.pi, math.pi, 2 * math.pi if basis == "SSF" else math.pi))
+    if rbc:
+        r2 = math.sqrt(2.0)
+        plan = tb.Plan(N, basis=basis, precision=prec, dealias="reference", Ra=1e6, Pr=1.0, dt=1e-4,
+                       nu=math.sqrt(1.0 / 1e6), kappa=1.0 / math.sqrt(1e6), kfactor=(math.pi, math.pi / r2, math.pi / r2))
+    else:
+        plan = tb.Plan(N, basis=basis, precision=prec, nu=1e-3, dt=5e-4, dealias="reference",
+                       kfactor=(math.pi, math.pi, 2 * math.pi if basis == "SSF" else math.pi))
     plan.set_stream(torch.cuda.current_stream())
     gen = torch.Generator(device="cuda").manual_seed(0)
     u = plan.field(3)
     u.real.copy_(1e-3 * torch.randn(u.shape, generator=gen, device="cuda"))
-    plan.rk4_step(u, warmup)
+    T = plan.field(1)
+    T.real.copy_(1e-3 * torch.randn(T.shape, generator=gen, device="cuda"))
+    step = (lambda n: plan.rk4_step_rbc(u, T, n)) if rbc else (lambda n: plan.rk4_step(u, n))
+    step(warmup)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    plan.rk4_step(u, steps)
+    step(steps)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    out = {"steps_per_s": steps / (ms / 1e3)}
+    if rbc:
+        out["nusselt"] = plan.nusselt(u, T)
     plan.close()
-    return {"steps_per_s": steps / (ms / 1e3)}
+    return out
 
 
 def rbc_leg(N: int, steps: int, warmup: int):
@@ -518,6 +532,17 @@ def alt_workload(args, world, rank, local, dev):
                 "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
                 "config": {"workload": f"{bas} fluid {n}^3, conservative, unforced, nu = 1e-3, dt = 5e-4, "
                                        "reference dealias, standalone sin/cos passes"}}
+    elif args.workload in ("rbc_ssf", "rbc_sss"):
+        n = args.N if args.N != 256 else 128
+        bas = args.workload[4:].upper()
+        r = ssf_leg(n, steps=args.steps, warmup=args.warmup, prec=args.precision, basis=bas, rbc=True)
+        line = {"metric": f"RK4 steps/s, {bas} Boussinesq (RBC) {n}^3 ({args.precision} transforms)",
+                "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 / r["steps_per_s"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": f"RBC on {bas} {n}^3, Ra=1e6, Pr=1, kfactor (pi, pi/sqrt2, pi/sqrt2), "
+                                       "dt=1e-4, reference dealias, standalone sin/cos passes"},
+                "nusselt": r["nusselt"]}
     elif args.workload == "rbc":
         r = rbc_leg(args.N if args.N != 256 else 128, steps=args.steps, warmup=args.warmup)
         n = args.N if args.N != 256 else 128
@@ -730,6 +755,7 @@ def main():
             extras["ensemble_rbc_64_fp64_plain"] = ensemble_plain_fp64_leg()
             extras["scalar_256_f32"] = coupled_leg("scalar", 256, steps=5, warmup=2)
             extras["mhd_256_f32"] = coupled_leg("mhd", 256, steps=5, warmup=2)
+            extras["rbc_sss_128_f32"] = ssf_leg(128, steps=10, warmup=3, basis="SSS", rbc=True)
             extras["fp32_over_plain_fp64"] = {
                 "fff1024": extras["fff1024_f32"]["steps_per_s"] / extras["fff1024_f64_plain"]["steps_per_s"],
                 "ensemble": extras["ensemble_rbc_64"]["ensemble_steps_per_s"]

@@ -150,7 +150,8 @@ int ts_init_temperature_perturbation(ts_plan* plan, double amp, double kmax, uin
 /* CVF::Compute_total_energy (Cvf.cc:213-221): sum over ncomp components, with the
  * basis's weights (FFF_pencil_energy.cc, SFF_pencil_energy.cc:76-95, and on SSF / SSS
  * the Multiplicity_factor weights 4 / 2 / 1 / 1/2 of SSF_pencil_energy.cc:76-103,
- * SSS_pencil_energy.cc:69-98; SSS coefficients real in the padded layout). */
+ * SSS_pencil_energy.cc:69-98; SSS coefficients real in the padded layout, whose two
+ * padding reals per line are not summed). */
 int ts_energy(ts_plan* plan, const void* a_hat, int ncomp, double* energy);
 /* Universal::Compute_shell_spectrum (universal_energy.cc:279-366), summed over
  * ncomp components: Ek[n_shells]. */
@@ -170,7 +171,8 @@ int ts_shell_sums(ts_plan* plan, const void* a_hat, const void* b_hat, int ncomp
  * as a full spectral field f_hat (3 components, zero outside the forcing band);
  * device pointers. */
 int ts_force_field(ts_plan* plan, const void* u_hat, void* f_hat);
-/* max |div U| (universal_basic.cc:343-356). */
+/* max |div U| (universal_basic.cc:343-356), with the basis's derivatives (SSF / SSS:
+ * sine +K, cosine -K along the sin/cos axes; SSS padding reals skipped). */
 int ts_max_div(ts_plan* plan, const void* u_hat, double* max_div);
 /* Nusselt number, PRLARGE/ULARGE (Correlation.cc:154-156): 1 + 2 sqrt(Ra Pr) <U1, T>,
  * on SFF, SSF and SSS plans. */

@@ -791,9 +791,9 @@ static Geo y_as_x(const Geo& g) {
 // SSF fluid step (sin/cos along x and y; sincostr_switch "SCF"), conservative form,
 // unforced: RK4(U,P,F) (RK.cc:91-170) with standalone transforms; with a temperature
 // T the Boussinesq step RK4(U,T,P,F) (RK_SF.cc:97-221, PRLARGE / ULARGE buoyancy).
-// With nf = 3 (fluid) or 4 (U, T) fields and np = 6 or 9 products, P holds
-// [0, nf) spectral scratch, [nf, 2 nf) the real fields, [2 nf, 2 nf + np) the real
-// products; the forward z transform writes the products' spectra into [0, np).
+// With nf = 3 (fluid) or 4 (U, T) fields and np = 6 or 9 products, P holds [0, np):
+// the nf spectra after the x and y inverses, which the fused z pass turns into the
+// np product spectra in place.
 // ---------------------------------------------------------------------------
 static int ssf_step_supported(ts_plan* p, bool rbc) {
   const int basis = p->cfg.basis;
@@ -804,7 +804,7 @@ static int ssf_step_supported(ts_plan* p, bool rbc) {
     return TS_ERR_UNSUPPORTED;
   }
   const int nf = rbc ? 4 : 3, np = rbc ? 9 : 6;
-  return ensure_work(p, nf, basis == TS_BASIS_SSS ? np + 3 + nf : 2 * nf + np);
+  return ensure_work(p, nf, basis == TS_BASIS_SSS ? np + 3 + nf : np);
 }
 
 // the RBC epilogue's arguments (U, T in place; stage fields U then T in Ucur, tot)
@@ -863,10 +863,11 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
       for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
     }
     {
+      // z is a Fourier axis as on FFF: the fused z pass (inverse, the products of form 0
+      // or 2 in real space, forward; unnormalised) reads the nf spectra and writes the
+      // np product spectra in place
       ProfScope ps(p, TS_KCLASS_Z);
-      CK(LAUNCH(p, z_single, g, +1, P, P + nf * cs, nf, p->twz, p->st));
-      CK(LAUNCH(p, real_products, P + nf * cs, P + 2 * nf * cs, 2 * g.S, nf, p->st));
-      CK(LAUNCH(p, z_single, g, -1, P + 2 * nf * cs, P, np, p->twz, p->st));
+      CK(LAUNCH(p, z_fused, g, T0 ? 2 : 0, P, p->twz, p->err_d, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_FWD);
@@ -978,10 +979,15 @@ int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
     const bool sss = p->cfg.basis == TS_BASIS_SSS;
     CKS(ssf_step_supported(p, false));
+    if (*p->err_h) {
+      g_last_error = "a bounded device wait gave up";
+      return TS_ERR_TIMEOUT;
+    }
     int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
       for (int s = 0; s < nsteps; ++s) CKS(sss ? step_sss(p, U) : step_ssf(p, U));
       return (int)TS_OK;
     });
+    if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
     return rc;
   }
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
@@ -1075,13 +1081,19 @@ int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
     const bool sss = p->cfg.basis == TS_BASIS_SSS;
     CKS(ssf_step_supported(p, true));
+    if (*p->err_h) {
+      g_last_error = "a bounded device wait gave up";
+      return TS_ERR_TIMEOUT;
+    }
     const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
-    return with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
+    int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
       return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
         for (int s = 0; s < nsteps; ++s) CKS(sss ? step_sss(p, U, T) : step_ssf(p, U, T));
         return (int)TS_OK;
       });
     });
+    if (rc == TS_OK) CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
+    return rc;
   }
   if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
   if (*p->err_h) {
@@ -1185,7 +1197,6 @@ int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
 }
 
 int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
-  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !max_div) return TS_ERR_ARG;
   return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, false, [&](void* U) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));

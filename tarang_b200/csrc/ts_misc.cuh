@@ -217,7 +217,7 @@ __global__ void k_energy(const C<T>* __restrict__ A, const C<T>* __restrict__ B,
       di += (double)a.y * b.y;
     }
     if (g.basis == 3) {
-      s += energy_weight(3, lx, ly, 2 * lz) * dr;
+      if (2 * lz < g.Nz) s += energy_weight(3, lx, ly, 2 * lz) * dr;
       if (2 * lz + 1 < g.Nz) s += energy_weight(3, lx, ly, 2 * lz + 1) * di;
     } else if (g.basis == 2 && lx == 0 && ly == 0 && lz == 0) {
       s += 0.5 * dr + di;
@@ -239,7 +239,9 @@ static __global__ void k_sum_partials(double* out, int n) {
   if (threadIdx.x == 0) out[0] = s;
 }
 
-// max over modes of |div U| (FFF: i K.U; SFF: Kx U1 (sine parity) + i Ky U2 + i Kz U3)
+// max over modes of |div U| (FFF: i K.U; SFF: Kx U1 (sine parity) + i Ky U2 + i Kz U3;
+// SSF (Vx = SCF, Vy = CSF, Vz = CCF): Kx U1 + Ky U2 + i Kz U3; SSS (real, Vx = SCC,
+// Vy = CSC, Vz = CCS): Kx U1 + Ky U2 + Kz U3 per real coefficient, z index 2 lz, 2 lz + 1)
 template <typename T>
 __global__ void k_maxdiv(const C<T>* __restrict__ U, Geo g, unsigned long long* out) {
   const long long n = g.S;
@@ -249,15 +251,24 @@ __global__ void k_maxdiv(const C<T>* __restrict__ U, Geo g, unsigned long long* 
     const int ly = (int)((e / g.Hz) % g.Ny);
     const int lx = (int)(e / ((long long)g.Ny * g.Hz));
     const double Kx = (g.basis == 0 ? kfft(lx, g.Nx) : lx) * g.kf[0];
-    const double Ky = kfft(ly, g.Ny) * g.kf[1], Kz = lz * g.kf[2];
+    const double Ky = (g.basis >= 2 ? ly : kfft(ly, g.Ny)) * g.kf[1], Kz = lz * g.kf[2];
     const C<T> u1 = U[e], u2 = U[n + e], u3 = U[2 * n + e];
     double dr, di;
     if (g.basis == 0) {
       dr = -(Kx * u1.y + Ky * u2.y + Kz * u3.y);
       di = Kx * u1.x + Ky * u2.x + Kz * u3.x;
-    } else {
+    } else if (g.basis == 1) {
       dr = Kx * u1.x - (Ky * u2.y + Kz * u3.y);
       di = Kx * u1.y + (Ky * u2.x + Kz * u3.x);
+    } else if (g.basis == 2) {
+      dr = Kx * u1.x + Ky * u2.x - Kz * u3.y;
+      di = Kx * u1.y + Ky * u2.y + Kz * u3.x;
+    } else {
+      // two real coefficients per slot: z wavenumbers 2 lz and 2 lz + 1 (padding skipped)
+      dr = (2 * lz < g.Nz) ? fabs(Kx * u1.x + Ky * u2.x + 2.0 * Kz * u3.x) : 0.0;
+      di = (2 * lz + 1 < g.Nz) ? fabs(Kx * u1.y + Ky * u2.y + (2 * lz + 1) * g.kf[2] * u3.y) : 0.0;
+      m = fmax(m, fmax(dr, di));
+      continue;
     }
     m = fmax(m, sqrt(dr * dr + di * di));
   }

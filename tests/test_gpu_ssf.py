@@ -51,7 +51,7 @@ def test_ssf_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSF", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.max_div(u)
+        plan.shell_spectrum(u, 3)
     with pytest.raises(tb.TsError):
         plan.rk4_step_scalar(u, plan.field(1), 1)   # the passive-scalar step is FFF only
     with pytest.raises(tb.TsError):
@@ -183,3 +183,17 @@ def test_ssf_energy_and_nusselt_match_oracle(cuda, prec):
     assert abs(plan.energy(u) / R.total_energy(g, Ur) - 1) < tol
     assert abs(plan.energy(t) / R.total_energy_scalar(g, Tr) - 1) < tol
     assert abs(plan.nusselt(u, t) - R.nusselt(cfg, Ur, Tr)) < tol * abs(R.nusselt(cfg, Ur, Tr))
+
+
+def test_ssf_max_div_matches_oracle(cuda):
+    """ts_max_div on an SSF plan: ~0 for a projected field, the oracle's value for a random one."""
+    import torch
+    import tarang_b200 as tb
+    N = (32, 16, 32)
+    g = R.Grid(N, KF, "SSF")
+    rng = np.random.default_rng(12)
+    V = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCF", "CSF", "CCF")])
+    plan = tb.Plan(N, basis="SSF", kfactor=KF)
+    assert abs(plan.max_div(torch.from_numpy(V).to(cuda)) / R.max_abs_div(g, V) - 1) < 1e-12
+    W = -R.project_rhs(g, V)
+    assert plan.max_div(torch.from_numpy(W).to(cuda)) < 1e-12 * R.max_abs_div(g, V)

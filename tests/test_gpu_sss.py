@@ -52,7 +52,7 @@ def test_sss_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSS", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.max_div(u)
+        plan.shell_spectrum(u, 3)
     with pytest.raises(tb.TsError):
         tb.Plan(32, basis="SSS", kfactor=KF, nlin_form="rotational")
     with pytest.raises(tb.TsError):
@@ -196,3 +196,23 @@ def test_sss_energy_and_nusselt_match_oracle(cuda, prec):
     assert abs(plan.nusselt(u, t) - R.nusselt(cfg, Ur, Tr)) < tol * abs(R.nusselt(cfg, Ur, Tr))
     ur = R.inverse(g, Tr, "SCC")
     assert abs(plan.energy(t) / (0.5 * np.mean(ur ** 2)) - 1) < tol
+
+
+def test_sss_max_div_and_padding(cuda):
+    """ts_max_div on an SSS plan against the oracle (~0 after projection), and the two padding
+    reals per line change neither the energy nor the divergence."""
+    import torch
+    import tarang_b200 as tb
+    N = (16, 32, 16)
+    g = R.Grid(N, KF, "SSS")
+    rng = np.random.default_rng(13)
+    V = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCC", "CSC", "CCS")])
+    plan = tb.Plan(N, basis="SSS", kfactor=KF)
+    v = _dev(V, cuda, "f64")
+    d0, e0 = plan.max_div(v), plan.energy(v)
+    assert abs(d0 / R.max_abs_div(g, V) - 1) < 1e-12
+    w = _dev(-R.project_rhs(g, V), cuda, "f64")
+    assert plan.max_div(w) < 1e-12 * d0
+    vr = torch.view_as_real(v).reshape(3, N[0], N[1], N[2] + 2)
+    vr[..., N[2]:] = 7.0
+    assert plan.max_div(v) == d0 and plan.energy(v) == e0
