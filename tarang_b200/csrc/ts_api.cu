@@ -804,7 +804,7 @@ static int ssf_step_supported(ts_plan* p, bool rbc) {
     return TS_ERR_UNSUPPORTED;
   }
   const int nf = rbc ? 4 : 3, np = rbc ? 9 : 6;
-  return ensure_work(p, nf, basis == TS_BASIS_SSS ? np + 3 + nf : np);
+  return ensure_work(p, nf, np);
 }
 
 // the RBC epilogue's arguments (U, T in place; stage fields U then T in Ucur, tot)
@@ -886,18 +886,15 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
 // ---------------------------------------------------------------------------
 // SSS fluid step (sin/cos along every axis; sincostr_switch "SCC"), conservative,
 // unforced, on real coefficients; with T the Boussinesq step as on SSF.  P holds
-// [0, np) the coefficient scratch of the inverse and then the np products, [np] and
-// [np + 1] per-line scratch of the z passes, [np + 3, np + 3 + nf) the real fields.
+// [0, np): the nf coefficient lines after the x and y inverses, which the fused SSS
+// z pass turns into the np product coefficients in place.
 // ---------------------------------------------------------------------------
 static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
   const Geo& g = p->g;
   const Geo gy = y_as_x(g);
-  const long long cs = g.S * (long long)p->cb, nl = (long long)g.Nx * g.Ny;
+  const long long cs = g.S * (long long)p->cb;
   const int nf = T0 ? 4 : 3, np = T0 ? 9 : 6;
   char* P = (char*)p->P;
-  char* s0 = P + np * cs;
-  char* s1 = P + (np + 1) * cs;
-  char* Rf = P + (np + 3) * cs;
   StageArgs a;
   memset(&a, 0, sizeof(a));
   a.U0 = U0;
@@ -931,18 +928,12 @@ static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
       for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
     }
     {
+      // the fused z pass: sin/cos inverse of the nf lines, the products, sin/cos forward
       ProfScope ps(p, TS_KCLASS_Z);
-      for (int c = 0; c < nf; ++c) {
-        CK(LAUNCH(p, sss_zpre_inv, P + c * cs, s0, nl, g.Nz, vz[c], p->twqz, p->st));
-        CK(LAUNCH(p, z_single, g, +1, s0, s1, 1, p->twz, p->st));
-        CK(LAUNCH(p, sss_zperm_inv, s1, Rf + c * cs, nl, g.Nz, vz[c], p->st));
-      }
-      CK(LAUNCH(p, real_products, Rf, P, 2 * g.S, nf, p->st));
-      for (int f = 0; f < np; ++f) {
-        CK(LAUNCH(p, sss_zperm_fwd, P + f * cs, s0, nl, g.Nz, qz[f], p->st));
-        CK(LAUNCH(p, z_single, g, -1, s0, s1, 1, p->twz, p->st));
-        CK(LAUNCH(p, sss_zpost_fwd, s1, P + f * cs, nl, g.Nz, qz[f], 1.0 / (2.0 * g.Nz), p->twqz, p->st));
-      }
+      int zin = 0, zout = 0;
+      for (int c = 0; c < nf; ++c) zin |= vz[c] << c;
+      for (int f = 0; f < np; ++f) zout |= qz[f] << f;
+      CK(LAUNCH(p, sss_z_fused, g, T0 ? 2 : 0, P, p->twz, p->twqz, zin, zout, p->st));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_FWD);

@@ -460,6 +460,115 @@ __global__ void __launch_bounds__(256) k_z_fused(C<T>* __restrict__ P, Geo g, co
 }
 
 // ---------------------------------------------------------------------------
+// SSS z pass, fused: per z line of real coefficients (N + 2 reals, the padded real
+// layout), the sin/cos inverse of the NIN inputs, the real products of FORM 0 / 2,
+// and the sin/cos forward of the NOUT products, in place.  The sin/cos transforms are
+// the x / y passes' algorithm along z: a quarter-step twiddle (tq = e^{-i pi m / 2N})
+// on the half spectrum of the reordered line v (v_k = u_2k, v_{N-1-k} = +-u_{2k+1},
+// minus for a sine series) and one real FFT of length N, the same real FFT and slot
+// layout as k_z_fused.  The lines are never put back in natural order: the product of
+// two reordered lines is the reordered product with the product's own sign pattern
+// (sine x sine = cosine, sine x cosine = sine, and the sign flips multiply), so the
+// forward transform takes it as it is.  zin / zout: bit c set = input / output c is a
+// sine series along z; scl = 1 / (2N).
+//   inverse: V_m = conj(w_m) (c_m - i c_{N-m}) (cosine, V_0 = c_0),
+//            conj(w_m) (s_{N-m} - i s_m) (sine, V_0 = 0); real inverse FFT of V
+//   forward: Z = real FFT of v; c_m = 2 scl Re(w_m Z_m) (cosine), -2 scl Im(w_m Z_m)
+//            (sine), Z_m = conj(Z_{N-m}) above N/2; the two padding reals written 0
+// ---------------------------------------------------------------------------
+template <typename T, int NZ, int E, int FORM>
+__global__ void __launch_bounds__(256) k_sss_z_fused(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw,
+                                                     const C<T>* __restrict__ tq, int nl, int zin, int zout,
+                                                     T scl) {
+  typedef C<T> V;
+  constexpr int N = NZ, M = NZ / 2, H = M + 1, TPL = M / E, LDS = zslot<M>();
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
+  static_assert(FORM == 0 || FORM == 2, "SSS z pass: conservative products, with or without T");
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* sm = reinterpret_cast<V*>(smraw);
+  const long long nlines = (long long)g.Nx * g.Ny;
+  const long long line0 = (long long)blockIdx.x * nl;
+  const int nh = (int)((nlines - line0) < nl ? (nlines - line0) : nl);
+  const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const bool live = l < nh;
+  const long long lbase = (line0 + (live ? l : 0)) * H;
+  auto slot = [&](int c, int ll) { return sm + (c * nl + ll) * LDS; };
+
+  // A. inverse of each input line into its slot (real points packed two per complex)
+  for (int c = 0; c < NIN; ++c) {
+    const T* cl = reinterpret_cast<const T*>(P + c * g.S + lbase);  // reals 0 .. N-1 of the line
+    const bool sine = (zin >> c) & 1;
+    auto half = [&](int m) -> V {  // V_m, 0 <= m <= M
+      if (m == 0) return mk<V>(sine ? (T)0 : cl[0], (T)0);
+      const T a = sine ? cl[N - m] : cl[m], b = sine ? cl[m] : cl[N - m];
+      return mul(conjg(tq[m]), mk<V>(a, -b));
+    };
+    V v[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int k = load_row<M, E>(t, s);
+      V a = mk<V>(0, 0), b = mk<V>(0, 0);
+      if (live) {
+        a = half(k);
+        b = conjg(half(M - k));
+      }
+      if (k == 0) { a.y = 0; b.y = 0; }
+      v[s] = add(add(a, b), mul_i<1>(mul(conjg(tw[k]), sub(a, b))));
+    }
+    V* sl = slot(c, l < nl ? l : 0);
+    fft_regs<M, E, 1, 0, true>(v, t, sl, 1, 0, tw, 2);
+#pragma unroll
+    for (int s = 0; s < E; ++s) sl[prow<true>(final_row<M, E>(t, s))] = v[s];
+  }
+  __syncthreads();
+  // B. products, in place per real point pair
+  for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
+    const int ll = e / M, m = prow<true>(e % M);
+    V in[NIN];
+#pragma unroll
+    for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
+#pragma unroll
+    for (int f = 0; f < NOUT; ++f)
+      slot(f, ll)[m] = mk<V>(in[z_pa(f, FORM)].x * in[z_pb(f, FORM)].x, in[z_pa(f, FORM)].y * in[z_pb(f, FORM)].y);
+  }
+  __syncthreads();
+  // C. forward of each product line, then the real sin/cos coefficients
+  for (int c = 0; c < NOUT; ++c) {
+    V* sl = slot(c, l < nl ? l : 0);
+    V v[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) v[s] = sl[prow<true>(load_row<M, E>(t, s))];
+    __syncthreads();
+    fft_regs<M, E, -1, 0, true>(v, t, sl, 1, 0, tw, 2);
+#pragma unroll
+    for (int s = 0; s < E; ++s) sl[prow<true>(final_row<M, E>(t, s))] = v[s];
+    __syncthreads();
+    const bool sine = (zout >> c) & 1;
+    V* dst = P + c * g.S + line0 * H;  // complex slot j holds reals 2j, 2j + 1
+    for (int e = threadIdx.x; e < nh * H; e += blockDim.x) {
+      const int ll = e / H, j = e % H;
+      const V* z = slot(c, ll);
+      T o[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int m = 2 * j + h;
+        o[h] = (T)0;
+        if (m < N) {
+          const int k = m <= M ? m : N - m;
+          const V Z = z[prow<true>(k == M ? 0 : k)];
+          const V Zp = conjg(z[prow<true>(k == 0 ? 0 : M - k)]);
+          V X = add(scale(add(Z, Zp), (T)0.5), mul_i<-1>(mul(tw[k], scale(sub(Z, Zp), (T)0.5))));
+          if (m > M) X = conjg(X);
+          const V w = mul(tq[m], X);
+          o[h] = sine ? (T)-2 * scl * w.y : (T)2 * scl * w.x;
+        }
+      }
+      dst[e] = mk<V>(o[0], o[1]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // z pass, register-resident variant (M = Nz/2 <= 512): one line per group of
 // TPL = M/8 consecutive lanes, 8 elements per thread.  The inverse transform
 // (forward radix schedule) leaves every component's real line in registers in

@@ -354,6 +354,40 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, cons
   return err;
 }
 
+// SSS fused z pass (form 0 or 2): the slot layout of the FFF slot kernel, lines per
+// block within about 106 KB of shared memory
+template <int NZ, int FORM>
+static cudaError_t sss_z_slots(const Geo& g, void* P, const void* tw, const void* tq, int zin, int zout,
+                               cudaStream_t st) {
+  constexpr int M = NZ / 2;
+  constexpr int E = e_mixed(M, 8);
+  constexpr int TPL = M / E;
+  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
+  constexpr int NSL = NIN > NOUT ? NIN : NOUT;
+  const long long nlines = (long long)g.Nx * g.Ny;
+  int nl = 256 / TPL;
+  while (nl > 1 && (size_t)NSL * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
+  const size_t sm = (size_t)NSL * nl * zslot<M>() * sizeof(V);
+  cudaError_t err;
+  auto k = k_sss_z_fused<T, NZ, E, FORM>;
+  if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
+  k<<<(unsigned)((nlines + nl - 1) / nl), nl * TPL, sm, st>>>((V*)P, g, (const V*)tw, (const V*)tq, nl, zin, zout,
+                                                              (T)(1.0 / (2.0 * NZ)));
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::sss_z_fused(const Geo& g, int form, void* P, const void* tw, const void* tq, int zin,
+                                               int zout, cudaStream_t st) {
+  cudaError_t err = cudaErrorInvalidValue;
+  if (form != 0 && form != 2) return err;
+  dispatch_L(g.Nz, [&](auto Lc) {
+    constexpr int NZ = decltype(Lc)::value;
+    err = form == 0 ? sss_z_slots<NZ, 0>(g, P, tw, tq, zin, zout, st) : sss_z_slots<NZ, 2>(g, P, tw, tq, zin, zout, st);
+  });
+  return err;
+}
+
 template <> cudaError_t Launch<T>::z_single(const Geo& g, int dir, const void* in, void* out, int ncomp,
                                             const void* tw, cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
@@ -695,11 +729,6 @@ template <> cudaError_t Launch<T>::sss_epi(const Geo& g, const void* P, const St
   return cudaGetLastError();
 }
 
-template <> cudaError_t Launch<T>::real_products(const void* R, void* Q, long long n, int nf, cudaStream_t st) {
-  k_real_products<T><<<grid1d(n, 256), 256, 0, st>>>((const T*)R, (T*)Q, n, nf);
-  ++g_launches;
-  return cudaGetLastError();
-}
 
 template <> cudaError_t Launch<T>::ssf_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st) {
   k_ssf_epi<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)P, g, a);

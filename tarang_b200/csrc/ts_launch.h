@@ -28,6 +28,9 @@ template <typename T> struct Launch {
   static cudaError_t z_fused(const Geo& g, int form, void* P, const void* tw, int* err, cudaStream_t st,
                              int nmem = 1, long long msP = 0, int zkeep = -1);
   static cudaError_t z_single(const Geo& g, int dir, const void* in, void* out, int ncomp, const void* tw, cudaStream_t st);
+  // SSS: the fused z pass on real coefficients (form 0 / 2 products; zin / zout sine masks)
+  static cudaError_t sss_z_fused(const Geo& g, int form, void* P, const void* tw, const void* tq, int zin, int zout,
+                                 cudaStream_t st);
   // a.U0 / a.Ud / a.tot must be 16-byte aligned (TMA)
   // form 0 / 1 / 3 as inv_x; mode MODE_STEP, MODE_FLUX, MODE_NLIN (forms 0, 1) or MODE_ADJ (form 3)
   static cudaError_t fwd_x(const Geo& g, int form, int mode, const void* P, const StageArgs& a, const void* tw,
@@ -54,8 +57,6 @@ template <typename T> struct Launch {
   // SSS fluid step: dealiased copy of real coefficients, and the epilogue
   static cudaError_t sss_dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
   static cudaError_t sss_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st);
-  // six products u_i u_j of three real fields (n reals each); nf = 4 adds u_i T of a fourth
-  static cudaError_t real_products(const void* R, void* Q, long long n, int nf, cudaStream_t st);
   // SSF fluid step: elementwise epilogue of the six forward-transformed products in P
   static cudaError_t ssf_epi(const Geo& g, const void* P, const StageArgs& a, cudaStream_t st);
   // SSF / SSS Boussinesq step: epilogues of the nine forward-transformed products in P

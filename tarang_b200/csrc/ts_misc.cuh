@@ -430,30 +430,6 @@ __global__ void k_dealias_copy(const C<T>* __restrict__ A, C<T>* B, int ncomp, G
   }
 }
 
-// the six products u_i u_j (order u1u1, u2u2, u3u3, u1u2, u2u3, u3u1) of three real
-// fields of n values each (the padded real layout), pointwise; with a fourth field T
-// (nf = 4) also u1T, u2T, u3T as products 6, 7, 8
-template <typename T>
-__global__ void __launch_bounds__(256) k_real_products(const T* __restrict__ R, T* __restrict__ Q, long long n,
-                                                       int nf) {
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-    const T u1 = R[e], u2 = R[n + e], u3 = R[2 * n + e];
-    Q[e] = u1 * u1;
-    Q[n + e] = u2 * u2;
-    Q[2 * n + e] = u3 * u3;
-    Q[3 * n + e] = u1 * u2;
-    Q[4 * n + e] = u2 * u3;
-    Q[5 * n + e] = u3 * u1;
-    if (nf == 4) {
-      const T t = R[3 * n + e];
-      Q[6 * n + e] = u1 * t;
-      Q[7 * n + e] = u2 * t;
-      Q[8 * n + e] = u3 * t;
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // SSS basis: sine/cosine transforms along z of real data (z lines contiguous, the
 // padded real layout of N + 2 values per line).  Same algorithm as the x / y
