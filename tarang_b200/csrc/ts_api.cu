@@ -846,6 +846,10 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
   const int vx[4] = {1, 0, 0, 1}, vy[4] = {0, 1, 0, 0};
   const int qx[9] = {0, 0, 0, 1, 0, 1, 0, 1, 1}, qy[9] = {0, 0, 0, 1, 1, 0, 0, 1, 0};
   const double sy = 1.0 / (2.0 * g.Ny), sx = 1.0 / (2.0 * g.Nx * (double)g.Nz);
+  // the same letters as bit masks (bit c = field c), one batched launch per pass
+  int mx_in = 0, my_in = 0, mx_out = 0, my_out = 0;
+  for (int c = 0; c < nf; ++c) mx_in |= vx[c] << c, my_in |= vy[c] << c;
+  for (int f = 0; f < np; ++f) mx_out |= qx[f] << f, my_out |= qy[f] << f;
   for (int stage = 1; stage <= 4; ++stage) {
     const void* Uin = stage == 1 ? U0 : p->Ucur;
     const void* Tin = stage == 1 ? (const void*)T0 : (const void*)((const char*)p->Ucur + 3 * cs);
@@ -856,11 +860,11 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
       ProfScope ps(p, TS_KCLASS_INV_X);
       CK(LAUNCH(p, dealias_copy, g, Uin, P, 3, p->st));
       if (T0) CK(LAUNCH(p, dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
-      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
+      CK(LAUNCH(p, sff_x, g, +1, P, 1, mx_in, 1.0, p->twq, p->st, nf, g.S));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_INV);
-      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
+      CK(LAUNCH(p, sff_x, gy, +1, P, g.Nx, my_in, 1.0, p->twqy, p->st, nf, g.S));
     }
     {
       // z is a Fourier axis as on FFF: the fused z pass (inverse, the products of form 0
@@ -871,11 +875,11 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_FWD);
-      for (int f = 0; f < np; ++f) CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], sy, p->twqy, p->st));
+      CK(LAUNCH(p, sff_x, gy, -1, P, g.Nx, my_out, sy, p->twqy, p->st, np, g.S));
     }
     {
       ProfScope ps(p, TS_KCLASS_FWD_X);
-      for (int f = 0; f < np; ++f) CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], sx, p->twq, p->st));
+      CK(LAUNCH(p, sff_x, g, -1, P, 1, mx_out, sx, p->twq, p->st, np, g.S));
       if (T0) CK(LAUNCH(p, ssf_rbc_epi, g, P, b, p->st));
       else CK(LAUNCH(p, ssf_epi, g, P, a, p->st));
     }
@@ -911,6 +915,10 @@ static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
   const int vx[4] = {1, 0, 0, 1}, vy[4] = {0, 1, 0, 0}, vz[4] = {0, 0, 1, 0};
   const int qx[9] = {0, 0, 0, 1, 0, 1, 0, 1, 1}, qy[9] = {0, 0, 0, 1, 1, 0, 0, 1, 0};
   const int qz[9] = {0, 0, 0, 0, 1, 1, 0, 0, 1};
+  // the same letters as bit masks (bit c = field c), one batched launch per pass
+  int mx_in = 0, my_in = 0, mx_out = 0, my_out = 0;
+  for (int c = 0; c < nf; ++c) mx_in |= vx[c] << c, my_in |= vy[c] << c;
+  for (int f = 0; f < np; ++f) mx_out |= qx[f] << f, my_out |= qy[f] << f;
   for (int stage = 1; stage <= 4; ++stage) {
     const void* Uin = stage == 1 ? U0 : p->Ucur;
     const void* Tin = stage == 1 ? (const void*)T0 : (const void*)((const char*)p->Ucur + 3 * cs);
@@ -921,11 +929,11 @@ static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
       ProfScope ps(p, TS_KCLASS_INV_X);
       CK(LAUNCH(p, sss_dealias_copy, g, Uin, P, 3, p->st));
       if (T0) CK(LAUNCH(p, sss_dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
-      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, g, +1, P + c * cs, 1, vx[c], 1.0, p->twq, p->st));
+      CK(LAUNCH(p, sff_x, g, +1, P, 1, mx_in, 1.0, p->twq, p->st, nf, g.S));
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_INV);
-      for (int c = 0; c < nf; ++c) CK(LAUNCH(p, sff_x, gy, +1, P + c * cs, g.Nx, vy[c], 1.0, p->twqy, p->st));
+      CK(LAUNCH(p, sff_x, gy, +1, P, g.Nx, my_in, 1.0, p->twqy, p->st, nf, g.S));
     }
     {
       // the fused z pass: sin/cos inverse of the nf lines, the products, sin/cos forward
@@ -937,13 +945,11 @@ static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
     }
     {
       ProfScope ps(p, TS_KCLASS_Y_FWD);
-      for (int f = 0; f < np; ++f)
-        CK(LAUNCH(p, sff_x, gy, -1, P + f * cs, g.Nx, qy[f], 1.0 / (2.0 * g.Ny), p->twqy, p->st));
+      CK(LAUNCH(p, sff_x, gy, -1, P, g.Nx, my_out, 1.0 / (2.0 * g.Ny), p->twqy, p->st, np, g.S));
     }
     {
       ProfScope ps(p, TS_KCLASS_FWD_X);
-      for (int f = 0; f < np; ++f)
-        CK(LAUNCH(p, sff_x, g, -1, P + f * cs, 1, qx[f], 1.0 / (2.0 * g.Nx), p->twq, p->st));
+      CK(LAUNCH(p, sff_x, g, -1, P, 1, mx_out, 1.0 / (2.0 * g.Nx), p->twq, p->st, np, g.S));
       if (T0) CK(LAUNCH(p, sss_rbc_epi, g, P, b, p->st));
       else CK(LAUNCH(p, sss_epi, g, P, a, p->st));
     }

@@ -586,7 +586,7 @@ template <> cudaError_t Launch<T>::sff_fwd_x(const Geo& g, const void* P, const 
 }
 
 template <> cudaError_t Launch<T>::sff_x(const Geo& g, int dir, void* A, int ncomp, int sine, double scl,
-                                         const void* tq, cudaStream_t st) {
+                                         const void* tq, cudaStream_t st, int nbatch, long long bstride) {
   cudaError_t err = cudaErrorInvalidValue;
   dispatch_L_sff(g.Nx, [&](auto Lc) {
     constexpr int NN = decltype(Lc)::value;
@@ -595,10 +595,10 @@ template <> cudaError_t Launch<T>::sff_x(const Geo& g, int dir, void* A, int nco
       constexpr int CW = cw_for(NN, E);
       const int inner = g.Ny * g.Hz;
       const size_t sm = (size_t)NN * CW * sizeof(V);
-      const dim3 grid((inner + CW - 1) / CW, ncomp);
+      const dim3 grid((inner + CW - 1) / CW, ncomp, nbatch);
       auto run = [&](auto k) {
         if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-        k<<<grid, CW * (NN / E), sm, st>>>((V*)A, g, (const V*)tq, sine, scl);
+        k<<<grid, CW * (NN / E), sm, st>>>((V*)A, g, (const V*)tq, sine, scl, bstride);
         ++g_launches;
         err = cudaGetLastError();
       };

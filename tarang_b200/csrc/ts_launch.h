@@ -42,9 +42,10 @@ template <typename T> struct Launch {
                                int nmem = 1, long long msU = 0, long long msT = 0, long long msW = 0);
   static cudaError_t sff_fwd_x(const Geo& g, const void* P, const SffArgs& a, const void* tq, cudaStream_t st,
                                int nmem = 1);
-  // standalone sin/cos x transform of ncomp components in place (dir -1 forward with scale scl, +1 inverse)
+  // standalone sin/cos x transform of ncomp components in place (dir -1 forward with scale scl, +1 inverse);
+  // nbatch > 1 repeats it on the fields at A + b * bstride (complex elements), field b with parity bit b of sine
   static cudaError_t sff_x(const Geo& g, int dir, void* A, int ncomp, int sine, double scl, const void* tq,
-                           cudaStream_t st);
+                           cudaStream_t st, int nbatch = 1, long long bstride = 0);
   // FFF passive scalar: elementwise epilogue of the nine x-transformed products in P
   static cudaError_t scalar_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
   // SSS z sin/cos helpers on nlines lines of N reals (padded to N + 2)

@@ -146,9 +146,11 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 // Every thread loads its rows before the first barrier inside the FFT and
 // stores after the last one, so the in-place update needs no extra buffer.
 // ---------------------------------------------------------------------------
+// Batches: blockIdx.z = b runs the pass on the field at A + b * bstride, whose parity
+// is bit b of smask (one field: b = 0, smask = 0 or 1).
 template <typename T, int N, int E, int CW, int DIR>
 __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
-    k_sff_x(C<T>* __restrict__ A, Geo g, const C<T>* __restrict__ tq, int sine, double scl) {
+    k_sff_x(C<T>* __restrict__ A, Geo g, const C<T>* __restrict__ tq, int smask, double scl, long long bstride) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
@@ -157,7 +159,8 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
   const int col = blockIdx.x * CW + c;
   const bool ok = col < inner;
   const long long rstride = inner;
-  V* a = A + blockIdx.y * g.S + (ok ? col : 0);
+  const int sine = (smask >> blockIdx.z) & 1;
+  V* a = A + blockIdx.y * g.S + blockIdx.z * bstride + (ok ? col : 0);
   V v[E];
   if (DIR < 0) {
 #pragma unroll

@@ -4,6 +4,8 @@
 //   fff       FFF_PENCIL + FluidVF: energy, divergence, E(k), Pi(R)
 //   fff_tuned the same after Universal::Autotune
 //   rbc       SFF_PENCIL + FluidVF + FluidSF: energies and Nusselt number
+//   rbc_sss   SSS_PENCIL + FluidVF + FluidSF (FP64): a roll set from the host, RK4(U, T),
+//             energies and Nusselt number
 //   ensemble  two RBC members of different sizes advanced together: Nusselt numbers
 //   adjoint   FFF rotational FP64: cotangent of the start state of an nsteps window
 //   mhd       FFF incompressible MHD: energies of U and B, max |div B|
@@ -13,6 +15,8 @@
 #include <cstdio>
 #include <cstring>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "tarang_b200.hpp"
 
@@ -72,6 +76,45 @@ static int run_rbc(int N, int steps) {
   FluidVF U(basis);
   FluidSF T(basis);
   T.Init_cond_perturbation(0.01, 4.0, 3);
+  Time_advance_incompress::RK4(U, T, steps);
+  const double eu = U.Compute_total_energy();
+  const double et = T.Compute_total_energy();
+  const double nu = Correlation::Get_Nusselt_no(U, T);
+  printf("{\"eu\": %.17g, \"eT\": %.17g, \"Nu\": %.17g}\n", eu, et, nu);
+  return 0;
+}
+
+// RBC on the SSS basis: real coefficients in the padded layout (N + 2 reals per z line),
+// u_x = 0.1 and theta = 0.05 on mode (1, 1, 1), u_y balancing the divergence, and a
+// second theta mode (2, 1, 0), copied in from the host
+static int run_rbc_sss(int N, int steps) {
+  const double Ra = 1e5, Pr = 1.0;
+  ts_config c;
+  ts_config_default(&c);
+  c.N[0] = c.N[1] = c.N[2] = N;
+  c.kfactor[0] = M_PI;
+  c.kfactor[1] = c.kfactor[2] = M_PI / std::sqrt(2.0);
+  c.precision = TS_F64;
+  c.Ra = Ra;
+  c.Pr = Pr;
+  c.nu = std::sqrt(Pr / Ra);
+  c.kappa = 1 / std::sqrt(Pr * Ra);
+  c.dt = 1e-3;
+  SSS_PENCIL basis(c);
+  FluidVF U(basis);
+  FluidSF T(basis);
+  const size_t line = N + 2, nreal = (size_t)N * N * line;
+  std::vector<double> u(3 * nreal, 0.0), t(nreal, 0.0);
+  auto at = [&](int lx, int ly, int lz) { return ((size_t)lx * N + ly) * line + lz; };
+  u[at(1, 1, 1)] = 0.1;
+  u[nreal + at(1, 1, 1)] = -0.1 * c.kfactor[0] / c.kfactor[1];
+  t[at(1, 1, 1)] = 0.05;
+  t[at(2, 1, 0)] = 0.02;
+  if (cudaMemcpy(U.cvf(), u.data(), u.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(T.csf(), t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    fprintf(stderr, "cudaMemcpy failed\n");
+    return 1;
+  }
   Time_advance_incompress::RK4(U, T, steps);
   const double eu = U.Compute_total_energy();
   const double et = T.Compute_total_energy();
@@ -158,6 +201,7 @@ int main(int argc, char** argv) {
     if (!strcmp(mode, "fff")) return run_fff(N, steps, false);
     if (!strcmp(mode, "fff_tuned")) return run_fff(N, steps, true);
     if (!strcmp(mode, "rbc")) return run_rbc(N, steps);
+    if (!strcmp(mode, "rbc_sss")) return run_rbc_sss(N, steps);
     if (!strcmp(mode, "ensemble")) return run_ensemble(N, steps);
     if (!strcmp(mode, "adjoint")) return run_adjoint(N, steps);
     if (!strcmp(mode, "mhd")) return run_mhd(N, steps);

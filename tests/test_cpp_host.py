@@ -105,6 +105,33 @@ def test_host_mirror_rbc_matches_python_binding(cuda, tmp_path):
 
 
 @pytest.mark.gpu
+def test_host_mirror_rbc_sss_matches_python_binding(cuda, tmp_path):
+    """RBC on SSS through SSS_PENCIL, FluidVF, FluidSF and Time_advance_incompress::RK4(U, T)
+    gives the Python binding's energies and Nusselt number bit for bit."""
+    import torch
+    import tarang_b200 as tb
+    N, steps = 32, 4
+    out = run_driver(build_driver(tmp_path), "rbc_sss", N, steps)
+    Ra, Pr = 1e5, 1.0
+    kf = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+    plan = tb.Plan(N, basis="SSS", precision="f64", kfactor=kf, nu=math.sqrt(Pr / Ra), kappa=1 / math.sqrt(Pr * Ra),
+                   dt=1e-3, Ra=Ra, Pr=Pr)
+    u = np.zeros((3, N, N, N + 2))
+    t = np.zeros((1, N, N, N + 2))
+    u[0, 1, 1, 1] = 0.1
+    u[1, 1, 1, 1] = -0.1 * kf[0] / kf[1]
+    t[0, 1, 1, 1] = 0.05
+    t[0, 2, 1, 0] = 0.02
+    ud = torch.from_numpy(u.view(np.complex128)).to(cuda)
+    td = torch.from_numpy(t.view(np.complex128)).to(cuda)
+    plan.rk4_step_rbc(ud, td, steps)
+    torch.cuda.synchronize()
+    assert out["eu"] == plan.energy(ud) and out["eT"] == plan.energy(td)
+    assert out["Nu"] == plan.nusselt(ud, td)
+    assert out["eu"] > 0 and out["Nu"] != 1.0
+
+
+@pytest.mark.gpu
 def test_host_mirror_ensemble_matches_python_binding(cuda, tmp_path):
     import tarang_b200 as tb
     out = run_driver(build_driver(tmp_path), "ensemble", 32, 4)
