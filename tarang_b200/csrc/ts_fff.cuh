@@ -521,24 +521,22 @@ __global__ void __launch_bounds__(256) k_sss_z_fused(C<T>* __restrict__ P, Geo g
     for (int s = 0; s < E; ++s) sl[prow<true>(final_row<M, E>(t, s))] = v[s];
   }
   __syncthreads();
-  // B. products, in place per real point pair
-  for (int e = threadIdx.x; e < nl * M; e += blockDim.x) {
-    const int ll = e / M, m = prow<true>(e % M);
-    V in[NIN];
-#pragma unroll
-    for (int c = 0; c < NIN; ++c) in[c] = slot(c, ll)[m];
-#pragma unroll
-    for (int f = 0; f < NOUT; ++f)
-      slot(f, ll)[m] = mk<V>(in[z_pa(f, FORM)].x * in[z_pb(f, FORM)].x, in[z_pa(f, FORM)].y * in[z_pb(f, FORM)].y);
-  }
-  __syncthreads();
-  // C. forward of each product line, then the real sin/cos coefficients
+  // B + C. per product: the product of two input lines formed as the forward FFT loads
+  // it (the input slots stay intact), the FFT in the line's work slot, then the real
+  // sin/cos coefficients.  NIN + 1 slots per line instead of max(NIN, NOUT) keep more
+  // lines, and so more warps, per SM.
+  const int lw = l < nl ? l : 0;
   for (int c = 0; c < NOUT; ++c) {
-    V* sl = slot(c, l < nl ? l : 0);
+    V* sl = slot(NIN, lw);
+    const V* sa = slot(z_pa(c, FORM), lw);
+    const V* sb = slot(z_pb(c, FORM), lw);
     V v[E];
 #pragma unroll
-    for (int s = 0; s < E; ++s) v[s] = sl[prow<true>(load_row<M, E>(t, s))];
-    __syncthreads();
+    for (int s = 0; s < E; ++s) {
+      const int r = prow<true>(load_row<M, E>(t, s));
+      v[s] = mk<V>(sa[r].x * sb[r].x, sa[r].y * sb[r].y);
+    }
+    __syncthreads();  // the previous product's coefficients have been read from the work slot
     fft_regs<M, E, -1, 0, true>(v, t, sl, 1, 0, tw, 2);
 #pragma unroll
     for (int s = 0; s < E; ++s) sl[prow<true>(final_row<M, E>(t, s))] = v[s];
@@ -547,7 +545,7 @@ __global__ void __launch_bounds__(256) k_sss_z_fused(C<T>* __restrict__ P, Geo g
     V* dst = P + c * g.S + line0 * H;  // complex slot j holds reals 2j, 2j + 1
     for (int e = threadIdx.x; e < nh * H; e += blockDim.x) {
       const int ll = e / H, j = e % H;
-      const V* z = slot(c, ll);
+      const V* z = slot(NIN, ll);
       T o[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {

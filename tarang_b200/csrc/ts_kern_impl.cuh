@@ -354,16 +354,16 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, cons
   return err;
 }
 
-// SSS fused z pass (form 0 or 2): the slot layout of the FFF slot kernel, lines per
-// block within about 106 KB of shared memory
+// SSS fused z pass (form 0 or 2): the slot layout of the FFF slot kernel with NIN
+// input slots and one work slot per line, lines per block within about 106 KB of
+// shared memory
 template <int NZ, int FORM>
 static cudaError_t sss_z_slots(const Geo& g, void* P, const void* tw, const void* tq, int zin, int zout,
                                cudaStream_t st) {
   constexpr int M = NZ / 2;
   constexpr int E = e_mixed(M, 8);
   constexpr int TPL = M / E;
-  constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
-  constexpr int NSL = NIN > NOUT ? NIN : NOUT;
+  constexpr int NSL = z_nin(FORM) + 1;
   const long long nlines = (long long)g.Nx * g.Ny;
   int nl = 256 / TPL;
   while (nl > 1 && (size_t)NSL * nl * zslot<M>() * sizeof(V) > 106 * 1024) nl /= 2;
