@@ -858,8 +858,12 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
     b.Tin = Tin;
     {
       ProfScope ps(p, TS_KCLASS_INV_X);
-      CK(LAUNCH(p, dealias_copy, g, Uin, P, 3, p->st));
-      if (T0) CK(LAUNCH(p, dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
+      if (T0 && stage > 1) {
+        CK(LAUNCH(p, dealias_copy, g, Uin, P, 4, p->st));  // U and T are adjacent in Ucur
+      } else {
+        CK(LAUNCH(p, dealias_copy, g, Uin, P, 3, p->st));
+        if (T0) CK(LAUNCH(p, dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
+      }
       CK(LAUNCH(p, sff_x, g, +1, P, 1, mx_in, 1.0, p->twq, p->st, nf, g.S));
     }
     {
@@ -927,8 +931,12 @@ static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
     b.Tin = Tin;
     {
       ProfScope ps(p, TS_KCLASS_INV_X);
-      CK(LAUNCH(p, sss_dealias_copy, g, Uin, P, 3, p->st));
-      if (T0) CK(LAUNCH(p, sss_dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
+      if (T0 && stage > 1) {
+        CK(LAUNCH(p, sss_dealias_copy, g, Uin, P, 4, p->st));  // U and T are adjacent in Ucur
+      } else {
+        CK(LAUNCH(p, sss_dealias_copy, g, Uin, P, 3, p->st));
+        if (T0) CK(LAUNCH(p, sss_dealias_copy, g, Tin, P + 3 * cs, 1, p->st));
+      }
       CK(LAUNCH(p, sff_x, g, +1, P, 1, mx_in, 1.0, p->twq, p->st, nf, g.S));
     }
     {

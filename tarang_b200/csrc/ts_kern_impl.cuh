@@ -719,7 +719,7 @@ template <> cudaError_t Launch<T>::sss_zperm_inv(const void* v, void* u, long lo
 
 template <> cudaError_t Launch<T>::sss_dealias_copy(const Geo& g, const void* A, void* B, int ncomp,
                                                    cudaStream_t st) {
-  k_sss_dealias_copy<T><<<grid1d(2 * g.S * ncomp, 256), 256, 0, st>>>((const T*)A, (T*)B, ncomp, g);
+  k_sss_dealias_copy<T><<<dim3(grid1d(g.S, 256), ncomp), 256, 0, st>>>((const T*)A, (T*)B, ncomp, g);
   ++g_launches;
   return cudaGetLastError();
 }
@@ -755,7 +755,7 @@ template <> cudaError_t Launch<T>::mhd_epi(const Geo& g, const void* P, const Sf
 }
 
 template <> cudaError_t Launch<T>::dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st) {
-  k_dealias_copy<T><<<grid1d(g.S * ncomp, 256), 256, 0, st>>>((const V*)A, (V*)B, ncomp, g);
+  k_dealias_copy<T><<<dim3(grid1d(g.S, 256), ncomp), 256, 0, st>>>((const V*)A, (V*)B, ncomp, g);
   ++g_launches;
   return cudaGetLastError();
 }

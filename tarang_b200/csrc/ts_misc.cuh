@@ -420,13 +420,13 @@ __global__ void k_scale(C<T>* A, long long n, double s) {
 // dealiased copy (for flux): B = D(A) on ncomp components
 template <typename T>
 __global__ void k_dealias_copy(const C<T>* __restrict__ A, C<T>* B, int ncomp, Geo g) {
-  const long long n = g.S;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n * ncomp; e += (long long)gridDim.x * blockDim.x) {
-    const long long m = e % n;
-    const int lz = (int)(m % g.Hz);
-    const int ly = (int)((m / g.Hz) % g.Ny);
-    const int lx = (int)(m / ((long long)g.Ny * g.Hz));
-    B[e] = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz) ? mk<C<T>>(0, 0) : A[e];
+  // component blockIdx.y; 32-bit index arithmetic (a component holds < 2^31 modes)
+  const int n = (int)g.S;
+  const long long off = (long long)blockIdx.y * g.S;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    const int lz = m % g.Hz, r = m / g.Hz;
+    const int ly = r % g.Ny, lx = r / g.Ny;
+    B[off + m] = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz) ? mk<C<T>>(0, 0) : A[off + m];
   }
 }
 

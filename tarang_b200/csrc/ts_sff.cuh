@@ -627,14 +627,20 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
 template <typename T>
 __global__ void __launch_bounds__(256) k_sss_dealias_copy(const T* __restrict__ A, T* __restrict__ B, int ncomp,
                                                           Geo g) {
-  const long long per = 2 * g.S;  // reals per component
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < per * ncomp;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long m = e % per;
-    const int lzr = (int)(m % (g.Nz + 2));
-    const long long r = m / (g.Nz + 2);
-    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
-    B[e] = (lzr >= g.Nz || sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz)) ? (T)0 : A[e];
+  // component blockIdx.y; one pair of reals (z indices 2 lz, 2 lz + 1) per element, 32-bit
+  // index arithmetic (a component holds < 2^31 pairs)
+  typedef C<T> V;
+  const V* a = reinterpret_cast<const V*>(A);
+  V* b = reinterpret_cast<V*>(B);
+  const int n = (int)g.S;
+  const long long off = (long long)blockIdx.y * g.S;
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    const int lz = m % g.Hz, r = m / g.Hz;
+    const int ly = r % g.Ny, lx = r / g.Ny;
+    V x = a[off + m];
+    if (2 * lz >= g.Nz || sss_dealias_zero(g.dealias, lx, ly, 2 * lz, g.Nx, g.Ny, g.Nz)) x.x = (T)0;
+    if (2 * lz + 1 >= g.Nz || sss_dealias_zero(g.dealias, lx, ly, 2 * lz + 1, g.Nx, g.Ny, g.Nz)) x.y = (T)0;
+    b[off + m] = x;
   }
 }
 
