@@ -755,6 +755,8 @@ def main():
             extras["ensemble_rbc_64_fp64_plain"] = ensemble_plain_fp64_leg()
             extras["scalar_256_f32"] = coupled_leg("scalar", 256, steps=5, warmup=2)
             extras["mhd_256_f32"] = coupled_leg("mhd", 256, steps=5, warmup=2)
+            extras["ssf_128_f32"] = ssf_leg(128, steps=10, warmup=3, basis="SSF")
+            extras["sss_128_f32"] = ssf_leg(128, steps=10, warmup=3, basis="SSS")
             extras["rbc_sss_128_f32"] = ssf_leg(128, steps=10, warmup=3, basis="SSS", rbc=True)
             extras["fp32_over_plain_fp64"] = {
                 "fff1024": extras["fff1024_f32"]["steps_per_s"] / extras["fff1024_f64_plain"]["steps_per_s"],
