@@ -98,6 +98,12 @@ int ts_plan_set_stream(ts_plan* plan, void* stream);
 int ts_plan_sizes(const ts_plan* plan, long long* elems_per_comp, int* bytes_per_complex);
 /* Number of shells of E(k): Min_radius_outside()+1 (FFF_pencil_inline.h:497-504). */
 int ts_plan_num_shells(const ts_plan* plan, int* n_shells);
+/* A zeroed device field of ncomp components in the plan's spectral layout
+ * (ncomp * elems_per_comp complex elements of the plan's precision), the storage
+ * PlainCVF / CVF allocate for their V1..V3 (fields/plainCvf.cc:52) and CSF for F.
+ * The caller owns it and releases it with ts_free_field. */
+int ts_alloc_field(const ts_plan* plan, int ncomp, void** field);
+int ts_free_field(void* field);
 /* Wait for the plan's stream and report a bounded device wait that gave up in
  * any earlier call (TS_ERR_TIMEOUT); the stepping calls otherwise report it at
  * the next call.  No reference counterpart (the reference has no device waits). */

@@ -66,6 +66,8 @@ SIGNATURES = {
     "ts_plan_set_stream": (ctypes.c_int, [_P, _P]),
     "ts_plan_sizes": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]),
     "ts_plan_num_shells": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    "ts_alloc_field": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "ts_free_field": (ctypes.c_int, [ctypes.c_void_p]),
     "ts_plan_set_dt": (ctypes.c_int, [_P, ctypes.c_double]),
     "ts_plan_status": (ctypes.c_int, [_P]),
     "ts_fft_forward": (ctypes.c_int, [_P, ctypes.c_char_p, _P, _P, ctypes.c_int]),

@@ -429,6 +429,27 @@ int ts_plan_num_shells(const ts_plan* p, int* n) {
   return TS_OK;
 }
 
+int ts_alloc_field(const ts_plan* p, int ncomp, void** field) {
+  if (!p || !field || ncomp < 1) return TS_ERR_ARG;
+  *field = nullptr;
+  const size_t bytes = (size_t)ncomp * (size_t)p->g.S * p->cb;
+  void* f = nullptr;
+  CK(cudaMalloc(&f, bytes));
+  cudaError_t e = cudaMemset(f, 0, bytes);
+  if (e != cudaSuccess) {
+    cudaFree(f);
+    g_last_error = std::string("ts_alloc_field: ") + cudaGetErrorString(e);
+    return TS_ERR_CUDA;
+  }
+  *field = f;
+  return TS_OK;
+}
+
+int ts_free_field(void* field) {
+  if (field) CK(cudaFree(field));
+  return TS_OK;
+}
+
 int ts_plan_status(ts_plan* p) {
   if (!p) return TS_ERR_ARG;
   CK(cudaStreamSynchronize(p->st));

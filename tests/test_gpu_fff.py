@@ -258,3 +258,34 @@ def test_bitwise_reproducible(cuda, prec):
     assert outs[0][0] == outs[1][0]
     assert torch.equal(outs[0][1], outs[1][1])
     assert outs[0][2] == outs[1][2]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_alloc_field_is_a_zeroed_plan_field(cuda, prec):
+    """ts_alloc_field returns a zeroed device field of the plan's layout: energy 0, and the
+    same initial condition and three steps on it as on a torch field, bit for bit; ts_free_field
+    releases it; ncomp < 1 is refused."""
+    import ctypes
+    import torch
+    import tarang_b200 as tb
+    from tarang_b200 import _lib as L
+    plan = plan_for(32, precision=prec, nlin_form="rotational", dealias="two_thirds")
+    lib = plan.lib
+    f = ctypes.c_void_p()
+    L.check(lib.ts_alloc_field(plan.h, 3, ctypes.byref(f)), "ts_alloc_field")
+    assert f.value
+    e = ctypes.c_double(-1.0)
+    L.check(lib.ts_energy(plan.h, f, 3, ctypes.byref(e)), "ts_energy")
+    assert e.value == 0.0
+    E = np.ascontiguousarray(R.spectrum_k4_gauss(plan.n_shells, 4.0))
+    L.check(lib.ts_init_energy_spectrum(plan.h, E.ctypes.data_as(L._D), len(E), 5, 0.5, f), "ts_init_energy_spectrum")
+    L.check(lib.ts_rk4_step(plan.h, f, 3), "ts_rk4_step")
+    L.check(lib.ts_energy(plan.h, f, 3, ctypes.byref(e)), "ts_energy")
+    u = plan.field(3)
+    plan.init_energy_spectrum(E, 5, 0.5, u)
+    plan.rk4_step(u, 3)
+    torch.cuda.synchronize()
+    assert e.value == plan.energy(u) and e.value > 0
+    L.check(lib.ts_free_field(f), "ts_free_field")
+    g = ctypes.c_void_p()
+    assert lib.ts_alloc_field(plan.h, 0, ctypes.byref(g)) == L.TS_ERR_ARG and not g.value
