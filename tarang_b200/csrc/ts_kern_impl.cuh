@@ -361,7 +361,9 @@ template <int NZ, int FORM>
 static cudaError_t sss_z_slots(const Geo& g, void* P, const void* tw, const void* tq, int zin, int zout,
                                cudaStream_t st) {
   constexpr int M = NZ / 2;
-  constexpr int E = e_mixed(M, 8);
+  // 4 elements per thread: twice the threads per z line of the 8-element form, and half
+  // the shared memory per block, so more warps per SM for this latency-bound pass
+  constexpr int E = (M % 3 != 0 && M >= 8) ? 4 : e_mixed(M, 8);
   constexpr int TPL = M / E;
   constexpr int NSL = z_nin(FORM) + 1;
   const long long nlines = (long long)g.Nx * g.Ny;
