@@ -597,10 +597,10 @@ template <> cudaError_t Launch<T>::sff_x(const Geo& g, int dir, void* A, int nco
       constexpr int CW = cw_for(NN, E);
       const int inner = g.Ny * g.Hz;
       const size_t sm = (size_t)NN * CW * sizeof(V);
-      const dim3 grid((inner + CW - 1) / CW, ncomp, nbatch);
+      const dim3 grid((unsigned)(((long long)ncomp * inner + CW - 1) / CW), 1, nbatch);
       auto run = [&](auto k) {
         if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-        k<<<grid, CW * (NN / E), sm, st>>>((V*)A, g, (const V*)tq, sine, scl, bstride);
+        k<<<grid, CW * (NN / E), sm, st>>>((V*)A, g, (const V*)tq, sine, scl, bstride, ncomp);
         ++g_launches;
         err = cudaGetLastError();
       };

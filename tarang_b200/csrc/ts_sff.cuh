@@ -146,21 +146,25 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 // Every thread loads its rows before the first barrier inside the FFT and
 // stores after the last one, so the in-place update needs no extra buffer.
 // ---------------------------------------------------------------------------
-// Batches: blockIdx.z = b runs the pass on the field at A + b * bstride, whose parity
-// is bit b of smask (one field: b = 0, smask = 0 or 1).
+// Planes: the nplanes planes of g.S elements (components, or the x-planes of a y pass)
+// are one run of nplanes * Ny * Hz columns, so no column tile straddles idle columns
+// at a plane's end.  Batches: blockIdx.z = b runs the pass on the planes at
+// A + b * bstride, whose parity is bit b of smask (one batch: b = 0, smask = 0 or 1).
 template <typename T, int N, int E, int CW, int DIR>
 __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
-    k_sff_x(C<T>* __restrict__ A, Geo g, const C<T>* __restrict__ tq, int smask, double scl, long long bstride) {
+    k_sff_x(C<T>* __restrict__ A, Geo g, const C<T>* __restrict__ tq, int smask, double scl, long long bstride,
+            int nplanes) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* xch = reinterpret_cast<V*>(smraw);
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int inner = g.Ny * g.Hz;
-  const int col = blockIdx.x * CW + c;
-  const bool ok = col < inner;
+  const int col = blockIdx.x * CW + c;  // plane col / inner, column col % inner
+  const bool ok = col < nplanes * inner;
   const long long rstride = inner;
   const int sine = (smask >> blockIdx.z) & 1;
-  V* a = A + blockIdx.y * g.S + blockIdx.z * bstride + (ok ? col : 0);
+  const int pl = ok ? col / inner : 0, cc = ok ? col % inner : 0;
+  V* a = A + (long long)pl * g.S + blockIdx.z * bstride + cc;
   V v[E];
   if (DIR < 0) {
 #pragma unroll
