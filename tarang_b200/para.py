@@ -274,6 +274,13 @@ def write_glob_row(f, values):
     f.write(_row(values))
 
 
+def sff_max_radius_inside(N, kfactor) -> int:
+    """``Max_radius_inside`` for the SFF basis with waveno_switch (SFF_pencil_inline.h:436-452):
+    min((Nx - 1) Kx, (Ny/2) Ky, (Nz/2) Kz), truncated."""
+    Nx, Ny, Nz = N
+    return int(min((Nx - 1) * kfactor[0], (Ny // 2) * kfactor[1], (Nz // 2) * kfactor[2]))
+
+
 def _fff_multiplicity(kx, ky, kz, Nx, Ny):
     """Multiplicity_factor (FFF_pencil_inline.h:583-602): 1 (kz > 0) or 1/2 (kz = 0),
     doubled on the kx = Nx/2 and ky = Ny/2 planes."""
@@ -298,13 +305,14 @@ class Output:
     """
 
     def __init__(self, plan, out_dir: str, radii=None):
-        if plan.basis != "FFF":
-            raise NotImplementedError("Output writes the FFF fluid layouts")
+        if plan.basis not in ("FFF", "SFF"):
+            raise NotImplementedError("Output writes the FFF fluid layouts and the SFF RBC glob.d")
         os.makedirs(out_dir, exist_ok=True)
         self.plan = plan
         self.out_dir = out_dir
         self.kf = tuple(plan.cfg.kfactor[i] for i in range(3))
-        self.kmax_inside = max_radius_inside(plan.N, self.kf)
+        self.kmax_inside = (max_radius_inside(plan.N, self.kf) if plan.basis == "FFF"
+                            else sff_max_radius_inside(plan.N, self.kf))
         self.radii = list(radii) if radii is not None else default_flux_radii(8, self.kmax_inside)
         self.forced = plan.cfg.force_type != 0
 
@@ -312,6 +320,8 @@ class Output:
         return self.plan.force_field(u, self.plan.field(3)) if self.forced else None
 
     def spectrum(self, u, t: float):
+        if self.plan.basis != "FFF":
+            raise NotImplementedError("this output is written for FFF fluid runs")
         p = self.plan
         kfp = self.kf[0] * self.kf[1] * self.kf[2]
         idx = np.arange(p.n_shells, dtype=np.float64)
@@ -341,6 +351,8 @@ class Output:
         and the K^2 moments; FFF_pencil_energy.cc:99-139; zero when helicity is off), the
         modal-energy entropy in bits (universal_energy.cc:449-473), kmax * Kolmogorov scale,
         nu, R_lambda = 2 E sqrt(15 / eps), dt, and the three component energies."""
+        if self.plan.basis != "FFF":
+            raise NotImplementedError("this output is written for FFF fluid runs")
         import torch
         p = self.plan
         nu = float(p.cfg.nu)
@@ -380,6 +392,8 @@ class Output:
         return row
 
     def flux(self, u, t: float):
+        if self.plan.basis != "FFF":
+            raise NotImplementedError("this output is written for FFF fluid runs")
         p = self.plan
         Pi = p.flux(u, self.radii)
         power = None
@@ -404,3 +418,54 @@ class Output:
             np.add.at(power, np.minimum(b, len(self.radii) - 1), w[ins])
         with open(os.path.join(self.out_dir, "flux.d"), "a") as f:
             write_flux(f, t, Pi, power)
+
+    def glob_rbc(self, u, T, t: float, dt: float):
+        """One row of out/glob.d for an RBC run on SFF (FluidIO::Output_global_RBC,
+        output_energy.cc:214-303; helicity_switch off, so the four helicity columns
+        are 0): time, E_u, E_T, nu k2E_u, kappa k2E_T (k2E = 2 sum mult K^2 |A|^2,
+        Get_total_Sn universal_energy.cc:106-141; no hyperviscosity), Nusselt
+        (Correlation.cc:154-156), H1, H2, k2H1, k2H2, the modal entropies of u and T in
+        bits (universal_energy.cc:449-537), kmax eta_1 = kmax (nu^3/eps)^(1/4),
+        kmax eta_2 = kmax eta_1 (nu/kappa)^(1/4) / (nu/kappa), nu, kappa,
+        R_lambda = 2 E_u sqrt(15/eps), dt, and the three component energies of u.
+        kmax = Max_radius_inside of SFF; mult = SFF Multiplicity_factor
+        (SFF_pencil_inline.h:492-515)."""
+        import torch
+        p = self.plan
+        if p.basis != "SFF":
+            raise NotImplementedError("glob_rbc writes RBC runs on the SFF basis")
+        nu, kappa = float(p.cfg.nu), float(p.cfg.kappa)
+        Nx, Ny, Nz = p.N
+        dev = u.device
+        lx = torch.arange(Nx, device=dev).double()[:, None, None]
+        ly = torch.arange(Ny, device=dev)
+        ky = torch.where(ly <= Ny // 2, ly, ly - Ny).double()[None, :, None]
+        lz = torch.arange(Nz // 2 + 1, device=dev).double()[None, None, :]
+        mult = torch.where(lz > 0, torch.where(lx > 0, 2.0, 1.0), torch.where(lx > 0, 1.0, 0.5))
+        mult = mult * torch.where((ky == Ny // 2) & (Ny > 1), 2.0, 1.0)
+        K2 = (lx * self.kf[0]) ** 2 + (ky * self.kf[1]) ** 2 + (lz * self.kf[2]) ** 2
+        v = u.to(torch.complex128)
+        th = T.to(torch.complex128).reshape(1, Nx, Ny, Nz // 2 + 1)
+        E = [p.energy(u[i:i + 1], 1) for i in range(3)]
+        Eu = E[0] + E[1] + E[2]
+        ET = p.energy(T, 1)
+        k2u = 2 * float((mult * K2 * (v.abs() ** 2).sum(0)).sum())
+        k2T = 2 * float((mult * K2 * (th.abs() ** 2).sum(0)).sum())
+        eps, epsT = nu * k2u, kappa * k2T
+        Nu = p.nusselt(u, T)
+
+        def entropy(a, etot):
+            prob = mult * (a.abs() ** 2).sum(0) / etot
+            return float(torch.where(prob > 1e-15, -prob * torch.log(torch.where(prob > 1e-15, prob, 1.0))
+                                     / math.log(2.0), 0.0).sum())
+
+        kmax = self.kmax_inside
+        keta1 = kmax * (nu ** 3 / eps) ** 0.25 if eps > 0 else float("inf")
+        r = nu / kappa
+        keta2 = keta1 * r ** 0.25 / r
+        rlam = 2 * Eu * math.sqrt(15 / eps) if eps > 0 else float("inf")
+        row = [t, Eu, ET, eps, epsT, Nu, 0.0, 0.0, 0.0, 0.0, entropy(v, Eu), entropy(th, ET), keta1, keta2,
+               nu, kappa, rlam, dt, E[0], E[1], E[2]]
+        with open(os.path.join(self.out_dir, "glob.d"), "a") as f:
+            write_glob_row(f, row)
+        return row

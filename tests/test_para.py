@@ -291,3 +291,49 @@ def test_output_glob_matches_oracle(cuda, tmp_path):
         assert abs(a - b) <= 1e-10 * max(1.0, abs(b))
     for a, b in zip(text, ref):
         assert abs(float(a) - b) <= 1e-5 * max(1e-12, abs(b))
+
+
+@pytest.mark.gpu
+def test_output_glob_rbc_matches_oracle(cuda, tmp_path):
+    """glob.d for an RBC run on SFF (Output_global_RBC's 21 columns) against numpy sums of
+    the oracle fields: energies, k^2 energies (SFF multiplicity), Nusselt, entropies,
+    kmax eta_1 / eta_2, R_lambda and the component energies (relative 1e-10, FP64)."""
+    import torch
+    import tarang_b200 as tb
+    from oracle import tarang_ref as R
+    N, kf, Ra, Pr = (32, 16, 16), (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0)), 2e5, 0.7
+    g = R.Grid(N, kf, "SFF")
+    rng = np.random.default_rng(21)
+    U = np.stack([R.reality_fix(g, 0.3 * R.forward(g, rng.standard_normal(g.rshape), p)) for p in ("S", "C", "C")])
+    T = R.reality_fix(g, 0.2 * R.forward(g, rng.standard_normal(g.rshape), "S"))
+    cfg = R.RBCConfig(g, Ra=Ra, Pr=Pr, dt=1e-3)
+    plan = tb.Plan(N, basis="SFF", kfactor=kf, nu=cfg.nu, kappa=cfg.kappa, Ra=Ra, Pr=Pr, dt=1e-3)
+    out = para.Output(plan, str(tmp_path))
+    row = out.glob_rbc(torch.from_numpy(U).to(cuda), torch.from_numpy(T[None]).to(cuda), 0.25, 1e-3)
+    # numpy restatement
+    lx = np.arange(N[0])[:, None, None]
+    ky = np.fft.fftfreq(N[1], 1.0 / N[1])[None, :, None]
+    lz = np.arange(N[2] // 2 + 1)[None, None, :]
+    mult = np.where(lz > 0, np.where(lx > 0, 2.0, 1.0), np.where(lx > 0, 1.0, 0.5))
+    mult = mult * np.where(np.abs(ky) == N[1] // 2, 2.0, 1.0)
+    K2 = (lx * kf[0]) ** 2 + (ky * kf[1]) ** 2 + (lz * kf[2]) ** 2
+    Eu, ET = R.total_energy(g, U), R.total_energy_scalar(g, T)
+    eps = cfg.nu * 2 * (mult * K2 * (np.abs(U) ** 2).sum(0)).sum()
+    epsT = cfg.kappa * 2 * (mult * K2 * np.abs(T) ** 2).sum()
+
+    def ent(a2, e):
+        pr = mult * a2 / e
+        pr = pr[pr > 1e-15]
+        return float((-pr * np.log(pr) / np.log(2.0)).sum())
+
+    kmax = int(min((N[0] - 1) * kf[0], (N[1] // 2) * kf[1], (N[2] // 2) * kf[2]))
+    k1 = kmax * (cfg.nu ** 3 / eps) ** 0.25
+    r = cfg.nu / cfg.kappa
+    want = [0.25, Eu, ET, eps, epsT, R.nusselt(cfg, U, T), 0, 0, 0, 0, ent((np.abs(U) ** 2).sum(0), Eu),
+            ent(np.abs(T) ** 2, ET), k1, k1 * r ** 0.25 / r, cfg.nu, cfg.kappa, 2 * Eu * math.sqrt(15 / eps), 1e-3,
+            R.total_energy(g, U[:1]), R.total_energy(g, U[1:2]), R.total_energy(g, U[2:])]
+    assert len(row) == 21
+    for i, (a, b) in enumerate(zip(row, want)):
+        assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
+    line = open(tmp_path / "glob.d").read()
+    assert line.endswith("\t\n") and len(line.split("\t")) == 22
