@@ -430,19 +430,37 @@ class Output:
         R_lambda = 2 E_u sqrt(15/eps), dt, and the three component energies of u.
         kmax = Max_radius_inside of SFF; mult = SFF Multiplicity_factor
         (SFF_pencil_inline.h:492-515)."""
+        if self.plan.basis != "SFF":
+            raise NotImplementedError("glob_rbc writes RBC runs on the SFF basis")
+        return self._glob_uT(u, T, t, dt, nusselt=True)
+
+    def glob_scalar(self, u, T, t: float, dt: float):
+        """One row of out/glob.d for a passive-scalar run on FFF (FluidIO::Output_global_scalar,
+        output_energy.cc:134-205): the RBC row without the Nusselt column (20 columns),
+        with the FFF multiplicity (FFF_pencil_inline.h:583-602) and Max_radius_inside.
+        (The reference's Output_global(U, T) picks this row for program.kind INC_SCALAR,
+        output_energy.cc:125, while its solver runs kind SCALAR_INCOMPRESS, main.cc:116.)"""
+        if self.plan.basis != "FFF":
+            raise NotImplementedError("glob_scalar writes passive-scalar runs on the FFF basis")
+        return self._glob_uT(u, T, t, dt, nusselt=False)
+
+    def _glob_uT(self, u, T, t: float, dt: float, nusselt: bool):
         import torch
         p = self.plan
-        if p.basis != "SFF":
-            raise NotImplementedError("glob_rbc writes RBC runs on the SFF basis")
         nu, kappa = float(p.cfg.nu), float(p.cfg.kappa)
         Nx, Ny, Nz = p.N
         dev = u.device
-        lx = torch.arange(Nx, device=dev).double()[:, None, None]
+        lxi = torch.arange(Nx, device=dev)
         ly = torch.arange(Ny, device=dev)
         ky = torch.where(ly <= Ny // 2, ly, ly - Ny).double()[None, :, None]
         lz = torch.arange(Nz // 2 + 1, device=dev).double()[None, None, :]
-        mult = torch.where(lz > 0, torch.where(lx > 0, 2.0, 1.0), torch.where(lx > 0, 1.0, 0.5))
-        mult = mult * torch.where((ky == Ny // 2) & (Ny > 1), 2.0, 1.0)
+        if p.basis == "SFF":
+            lx = lxi.double()[:, None, None]
+            mult = torch.where(lz > 0, torch.where(lx > 0, 2.0, 1.0), torch.where(lx > 0, 1.0, 0.5))
+            mult = mult * torch.where((ky == Ny // 2) & (Ny > 1), 2.0, 1.0)
+        else:
+            lx = torch.where(lxi <= Nx // 2, lxi, lxi - Nx).double()[:, None, None]
+            mult = torch.where(lz > 0, 1.0, 0.5) * torch.where((lx == Nx // 2) | ((ky == Ny // 2) & (Ny > 1)), 2.0, 1.0)
         K2 = (lx * self.kf[0]) ** 2 + (ky * self.kf[1]) ** 2 + (lz * self.kf[2]) ** 2
         v = u.to(torch.complex128)
         th = T.to(torch.complex128).reshape(1, Nx, Ny, Nz // 2 + 1)
@@ -452,7 +470,7 @@ class Output:
         k2u = 2 * float((mult * K2 * (v.abs() ** 2).sum(0)).sum())
         k2T = 2 * float((mult * K2 * (th.abs() ** 2).sum(0)).sum())
         eps, epsT = nu * k2u, kappa * k2T
-        Nu = p.nusselt(u, T)
+        Nu = [p.nusselt(u, T)] if nusselt else []
 
         def entropy(a, etot):
             prob = mult * (a.abs() ** 2).sum(0) / etot
@@ -464,8 +482,8 @@ class Output:
         r = nu / kappa
         keta2 = keta1 * r ** 0.25 / r
         rlam = 2 * Eu * math.sqrt(15 / eps) if eps > 0 else float("inf")
-        row = [t, Eu, ET, eps, epsT, Nu, 0.0, 0.0, 0.0, 0.0, entropy(v, Eu), entropy(th, ET), keta1, keta2,
-               nu, kappa, rlam, dt, E[0], E[1], E[2]]
+        row = [t, Eu, ET, eps, epsT] + Nu + [0.0, 0.0, 0.0, 0.0, entropy(v, Eu), entropy(th, ET), keta1, keta2,
+                                            nu, kappa, rlam, dt, E[0], E[1], E[2]]
         with open(os.path.join(self.out_dir, "glob.d"), "a") as f:
             write_glob_row(f, row)
         return row

@@ -337,3 +337,42 @@ def test_output_glob_rbc_matches_oracle(cuda, tmp_path):
         assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
     line = open(tmp_path / "glob.d").read()
     assert line.endswith("\t\n") and len(line.split("\t")) == 22
+
+
+@pytest.mark.gpu
+def test_output_glob_scalar_matches_oracle(cuda, tmp_path):
+    """glob.d for a passive-scalar run on FFF (Output_global_scalar's 20 columns: the RBC row
+    without Nusselt) with the FFF multiplicity, against numpy sums of the oracle fields."""
+    import torch
+    import tarang_b200 as tb
+    from oracle import tarang_ref as R
+    N, nu, kappa = (32, 16, 32), 0.01, 0.03
+    g = R.Grid(N)
+    U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 2, 0.5)
+    T = R.reality_fix(g, 0.2 * R.forward(g, np.random.default_rng(22).standard_normal(g.rshape)))
+    plan = tb.Plan(N, nu=nu, kappa=kappa, dt=1e-3)
+    out = para.Output(plan, str(tmp_path))
+    row = out.glob_scalar(torch.from_numpy(U).to(cuda), torch.from_numpy(T[None]).to(cuda), 1.5, 1e-3)
+    kx = np.fft.fftfreq(N[0], 1.0 / N[0])[:, None, None]
+    ky = np.fft.fftfreq(N[1], 1.0 / N[1])[None, :, None]
+    kz = np.arange(N[2] // 2 + 1)[None, None, :]
+    mult = np.where(kz > 0, 1.0, 0.5) * np.where((np.abs(kx) == N[0] // 2) | (np.abs(ky) == N[1] // 2), 2.0, 1.0)
+    K2 = kx ** 2 + ky ** 2 + kz ** 2
+    Eu, ET = R.total_energy(g, U), R.total_energy_scalar(g, T)
+    eps = nu * 2 * (mult * K2 * (np.abs(U) ** 2).sum(0)).sum()
+    epsT = kappa * 2 * (mult * K2 * np.abs(T) ** 2).sum()
+
+    def ent(a2, e):
+        pr = mult * a2 / e
+        pr = pr[pr > 1e-15]
+        return float((-pr * np.log(pr) / np.log(2.0)).sum())
+
+    kmax = para.max_radius_inside(N, (1.0, 1.0, 1.0))
+    k1 = kmax * (nu ** 3 / eps) ** 0.25
+    r = nu / kappa
+    want = [1.5, Eu, ET, eps, epsT, 0, 0, 0, 0, ent((np.abs(U) ** 2).sum(0), Eu), ent(np.abs(T) ** 2, ET), k1,
+            k1 * r ** 0.25 / r, nu, kappa, 2 * Eu * math.sqrt(15 / eps), 1e-3,
+            R.total_energy(g, U[:1]), R.total_energy(g, U[1:2]), R.total_energy(g, U[2:])]
+    assert len(row) == 20
+    for i, (a, b) in enumerate(zip(row, want)):
+        assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
