@@ -444,12 +444,56 @@ class Output:
             raise NotImplementedError("glob_scalar writes passive-scalar runs on the FFF basis")
         return self._glob_uT(u, T, t, dt, nusselt=False)
 
-    def _glob_uT(self, u, T, t: float, dt: float, nusselt: bool):
+    def glob_mhd(self, u, b, t: float, dt: float):
+        """One row of out/glob.d for an MHD run on FFF (FluidIO::Output_global(U, W),
+        output_energy.cc:404-499; helicity_switch off, so the eight helicity columns are
+        0): time, E_u, E_b, nu k2E_u, eta k2E_b, the cross helicity Hc = sum_i <u_i, b_i>
+        (Correlation.cc:225-230), ((nu + eta)/2) k2Hc (k2Hc = 2 sum mult K^2 Re(u . b*),
+        Cvf.cc:235-238), 8 helicity columns, the entropies of u and b, kmax eta_1,
+        kmax eta_2 (with nu / eta), nu, eta, R_lambda, dt, and the component energies of
+        u and of b: 29 columns.  eta is the plan's kappa."""
         import torch
         p = self.plan
-        nu, kappa = float(p.cfg.nu), float(p.cfg.kappa)
+        if p.basis != "FFF":
+            raise NotImplementedError("glob_mhd writes MHD runs on the FFF basis")
+        nu, eta = float(p.cfg.nu), float(p.cfg.kappa)
+        mult, K2 = self._mult_K2(u.device)
+        v, w = u.to(torch.complex128), b.to(torch.complex128)
+        Eu_c = [p.energy(u[i:i + 1], 1) for i in range(3)]
+        Eb_c = [p.energy(b[i:i + 1], 1) for i in range(3)]
+        Eu, Eb = sum(Eu_c), sum(Eb_c)
+        d = (v * w.conj()).real.sum(0)
+        Hc = float(d.sum() - 0.5 * d[:, :, 0].sum())   # FFF plane weights of Get_local_energy(A, B)
+        k2u = 2 * float((mult * K2 * (v.abs() ** 2).sum(0)).sum())
+        k2b = 2 * float((mult * K2 * (w.abs() ** 2).sum(0)).sum())
+        k2Hc = 2 * float((mult * K2 * d).sum())
+        eps, epsb = nu * k2u, eta * k2b
+        kmax = self.kmax_inside
+        keta1 = kmax * (nu ** 3 / eps) ** 0.25 if eps > 0 else float("inf")
+        r = nu / eta
+        keta2 = keta1 * r ** 0.25 / r
+        rlam = 2 * Eu * math.sqrt(15 / eps) if eps > 0 else float("inf")
+        row = ([t, Eu, Eb, eps, epsb, Hc, 0.5 * (nu + eta) * k2Hc] + [0.0] * 8 +
+               [self._entropy(mult, v, Eu), self._entropy(mult, w, Eb), keta1, keta2, nu, eta, rlam, dt] +
+               Eu_c + Eb_c)
+        with open(os.path.join(self.out_dir, "glob.d"), "a") as f:
+            write_glob_row(f, row)
+        return row
+
+    @staticmethod
+    def _entropy(mult, a, etot):
+        """modal-energy entropy in bits, mult |A|^2 / E as the probabilities (universal_energy.cc:449-537)"""
+        import torch
+        prob = mult * (a.abs() ** 2).sum(0) / etot
+        return float(torch.where(prob > 1e-15, -prob * torch.log(torch.where(prob > 1e-15, prob, 1.0))
+                                 / math.log(2.0), 0.0).sum())
+
+    def _mult_K2(self, dev):
+        """Multiplicity_factor (FFF_pencil_inline.h:583-602, SFF_pencil_inline.h:492-515) and K^2
+        per stored mode of the plan's basis"""
+        import torch
+        p = self.plan
         Nx, Ny, Nz = p.N
-        dev = u.device
         lxi = torch.arange(Nx, device=dev)
         ly = torch.arange(Ny, device=dev)
         ky = torch.where(ly <= Ny // 2, ly, ly - Ny).double()[None, :, None]
@@ -462,6 +506,14 @@ class Output:
             lx = torch.where(lxi <= Nx // 2, lxi, lxi - Nx).double()[:, None, None]
             mult = torch.where(lz > 0, 1.0, 0.5) * torch.where((lx == Nx // 2) | ((ky == Ny // 2) & (Ny > 1)), 2.0, 1.0)
         K2 = (lx * self.kf[0]) ** 2 + (ky * self.kf[1]) ** 2 + (lz * self.kf[2]) ** 2
+        return mult, K2
+
+    def _glob_uT(self, u, T, t: float, dt: float, nusselt: bool):
+        import torch
+        p = self.plan
+        nu, kappa = float(p.cfg.nu), float(p.cfg.kappa)
+        Nx, Ny, Nz = p.N
+        mult, K2 = self._mult_K2(u.device)
         v = u.to(torch.complex128)
         th = T.to(torch.complex128).reshape(1, Nx, Ny, Nz // 2 + 1)
         E = [p.energy(u[i:i + 1], 1) for i in range(3)]
@@ -472,18 +524,14 @@ class Output:
         eps, epsT = nu * k2u, kappa * k2T
         Nu = [p.nusselt(u, T)] if nusselt else []
 
-        def entropy(a, etot):
-            prob = mult * (a.abs() ** 2).sum(0) / etot
-            return float(torch.where(prob > 1e-15, -prob * torch.log(torch.where(prob > 1e-15, prob, 1.0))
-                                     / math.log(2.0), 0.0).sum())
-
         kmax = self.kmax_inside
         keta1 = kmax * (nu ** 3 / eps) ** 0.25 if eps > 0 else float("inf")
         r = nu / kappa
         keta2 = keta1 * r ** 0.25 / r
         rlam = 2 * Eu * math.sqrt(15 / eps) if eps > 0 else float("inf")
-        row = [t, Eu, ET, eps, epsT] + Nu + [0.0, 0.0, 0.0, 0.0, entropy(v, Eu), entropy(th, ET), keta1, keta2,
-                                            nu, kappa, rlam, dt, E[0], E[1], E[2]]
+        row = [t, Eu, ET, eps, epsT] + Nu + [0.0, 0.0, 0.0, 0.0, self._entropy(mult, v, Eu),
+                                            self._entropy(mult, th, ET), keta1, keta2, nu, kappa, rlam, dt,
+                                            E[0], E[1], E[2]]
         with open(os.path.join(self.out_dir, "glob.d"), "a") as f:
             write_glob_row(f, row)
         return row

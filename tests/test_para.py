@@ -376,3 +376,46 @@ def test_output_glob_scalar_matches_oracle(cuda, tmp_path):
     assert len(row) == 20
     for i, (a, b) in enumerate(zip(row, want)):
         assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
+
+
+@pytest.mark.gpu
+def test_output_glob_mhd_matches_oracle(cuda, tmp_path):
+    """glob.d for an MHD run on FFF (Output_global(U, W)'s 29 columns: energies,
+    dissipations, cross helicity and its dissipation, entropies, kmax eta_1 / eta_2,
+    R_lambda, component energies) against numpy sums of the oracle fields."""
+    import torch
+    import tarang_b200 as tb
+    from oracle import tarang_ref as R
+    N, nu, eta = (32, 32, 16), 0.01, 0.02
+    g = R.Grid(N)
+    U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 3, 0.5)
+    B = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 4, 0.3)
+    plan = tb.Plan(N, nu=nu, kappa=eta, dt=1e-3)
+    out = para.Output(plan, str(tmp_path))
+    row = out.glob_mhd(torch.from_numpy(U).to(cuda), torch.from_numpy(B).to(cuda), 2.0, 1e-3)
+    kx = np.fft.fftfreq(N[0], 1.0 / N[0])[:, None, None]
+    ky = np.fft.fftfreq(N[1], 1.0 / N[1])[None, :, None]
+    kz = np.arange(N[2] // 2 + 1)[None, None, :]
+    mult = np.where(kz > 0, 1.0, 0.5) * np.where((np.abs(kx) == N[0] // 2) | (np.abs(ky) == N[1] // 2), 2.0, 1.0)
+    K2 = kx ** 2 + ky ** 2 + kz ** 2
+    Eu, Eb = R.total_energy(g, U), R.total_energy(g, B)
+    Hc = sum(R.cross_energy(g, U[i], B[i]) for i in range(3))
+    eps = nu * 2 * (mult * K2 * (np.abs(U) ** 2).sum(0)).sum()
+    epsb = eta * 2 * (mult * K2 * (np.abs(B) ** 2).sum(0)).sum()
+    k2Hc = 2 * (mult * K2 * (U * B.conj()).real.sum(0)).sum()
+
+    def ent(a2, e):
+        pr = mult * a2 / e
+        pr = pr[pr > 1e-15]
+        return float((-pr * np.log(pr) / np.log(2.0)).sum())
+
+    kmax = para.max_radius_inside(N, (1.0, 1.0, 1.0))
+    k1 = kmax * (nu ** 3 / eps) ** 0.25
+    r = nu / eta
+    want = ([2.0, Eu, Eb, eps, epsb, Hc, 0.5 * (nu + eta) * k2Hc] + [0] * 8 +
+            [ent((np.abs(U) ** 2).sum(0), Eu), ent((np.abs(B) ** 2).sum(0), Eb), k1, k1 * r ** 0.25 / r, nu, eta,
+             2 * Eu * math.sqrt(15 / eps), 1e-3] +
+            [R.total_energy(g, U[i:i + 1]) for i in range(3)] + [R.total_energy(g, B[i:i + 1]) for i in range(3)])
+    assert len(row) == 29
+    for i, (a, b) in enumerate(zip(row, want)):
+        assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
