@@ -434,24 +434,28 @@ class Output:
             raise NotImplementedError("glob_rbc writes RBC runs on the SFF basis")
         return self._glob_uT(u, T, t, dt, nusselt=True)
 
-    def glob_scalar(self, u, T, t: float, dt: float):
+    def glob_scalar(self, u, T, t: float, dt: float, helicity: bool = False):
         """One row of out/glob.d for a passive-scalar run on FFF (FluidIO::Output_global_scalar,
         output_energy.cc:134-205): the RBC row without the Nusselt column (20 columns),
         with the FFF multiplicity (FFF_pencil_inline.h:583-602) and Max_radius_inside.
         (The reference's Output_global(U, T) picks this row for program.kind INC_SCALAR,
-        output_energy.cc:125, while its solver runs kind SCALAR_INCOMPRESS, main.cc:116.)"""
+        output_energy.cc:125, while its solver runs kind SCALAR_INCOMPRESS, main.cc:116.)
+        With helicity (the reference's helicity_switch), columns 6-9 hold H1, H2, k2H1, k2H2
+        of u."""
         if self.plan.basis != "FFF":
             raise NotImplementedError("glob_scalar writes passive-scalar runs on the FFF basis")
-        return self._glob_uT(u, T, t, dt, nusselt=False)
+        return self._glob_uT(u, T, t, dt, nusselt=False, helicity=helicity)
 
-    def glob_mhd(self, u, b, t: float, dt: float):
+    def glob_mhd(self, u, b, t: float, dt: float, helicity: bool = False):
         """One row of out/glob.d for an MHD run on FFF (FluidIO::Output_global(U, W),
         output_energy.cc:404-499; helicity_switch off, so the eight helicity columns are
         0): time, E_u, E_b, nu k2E_u, eta k2E_b, the cross helicity Hc = sum_i <u_i, b_i>
         (Correlation.cc:225-230), ((nu + eta)/2) k2Hc (k2Hc = 2 sum mult K^2 Re(u . b*),
         Cvf.cc:235-238), 8 helicity columns, the entropies of u and b, kmax eta_1,
         kmax eta_2 (with nu / eta), nu, eta, R_lambda, dt, and the component energies of
-        u and of b: 29 columns.  eta is the plan's kappa."""
+        u and of b: 29 columns.  eta is the plan's kappa.  With helicity (the reference's
+        helicity_switch) the helicity columns hold H1_u, H2_u, H1_b, H2_b, k2H1_u, k2H2_u,
+        k2H1_b, k2H2_b."""
         import torch
         p = self.plan
         if p.basis != "FFF":
@@ -473,12 +477,35 @@ class Output:
         r = nu / eta
         keta2 = keta1 * r ** 0.25 / r
         rlam = 2 * Eu * math.sqrt(15 / eps) if eps > 0 else float("inf")
-        row = ([t, Eu, Eb, eps, epsb, Hc, 0.5 * (nu + eta) * k2Hc] + [0.0] * 8 +
+        hu = self._helicity(v) if helicity else [0.0] * 4
+        hb = self._helicity(w) if helicity else [0.0] * 4
+        row = ([t, Eu, Eb, eps, epsb, Hc, 0.5 * (nu + eta) * k2Hc] + hu[:2] + hb[:2] + hu[2:] + hb[2:] +
                [self._entropy(mult, v, Eu), self._entropy(mult, w, Eb), keta1, keta2, nu, eta, rlam, dt] +
                Eu_c + Eb_c)
         with open(os.path.join(self.out_dir, "glob.d"), "a") as f:
             write_glob_row(f, row)
         return row
+
+    def _helicity(self, v):
+        """H1, H2, k2H1, k2H2 of a spectral vector field on FFF (FFF_pencil_energy.cc:99-139):
+        h = 2 mult K . (Vr x Vi) summed, / K^2, and the K^2 moments"""
+        import torch
+        p = self.plan
+        if p.basis != "FFF":
+            raise NotImplementedError("helicity columns are written for FFF runs")
+        Nx, Ny, Nz = p.N
+        dev = v.device
+        lx, ly = torch.arange(Nx, device=dev), torch.arange(Ny, device=dev)
+        K = [torch.where(lx <= Nx // 2, lx, lx - Nx).double()[:, None, None] * self.kf[0],
+             torch.where(ly <= Ny // 2, ly, ly - Ny).double()[None, :, None] * self.kf[1],
+             torch.arange(Nz // 2 + 1, device=dev).double()[None, None, :] * self.kf[2]]
+        mult, K2 = self._mult_K2(dev)
+        vr, vi = v.real, v.imag
+        cr = [vr[1] * vi[2] - vr[2] * vi[1], vr[2] * vi[0] - vr[0] * vi[2], vr[0] * vi[1] - vr[1] * vi[0]]
+        h = 2 * mult * (K[0] * cr[0] + K[1] * cr[1] + K[2] * cr[2])
+        H1 = float(h.sum())
+        H2 = float(torch.where(K2 > 1e-15, h / torch.where(K2 > 1e-15, K2, 1.0), 0.0).sum())
+        return [H1, H2, 2 * float((K2 * h).sum()), 2 * H1]
 
     @staticmethod
     def _entropy(mult, a, etot):
@@ -508,7 +535,7 @@ class Output:
         K2 = (lx * self.kf[0]) ** 2 + (ky * self.kf[1]) ** 2 + (lz * self.kf[2]) ** 2
         return mult, K2
 
-    def _glob_uT(self, u, T, t: float, dt: float, nusselt: bool):
+    def _glob_uT(self, u, T, t: float, dt: float, nusselt: bool, helicity: bool = False):
         import torch
         p = self.plan
         nu, kappa = float(p.cfg.nu), float(p.cfg.kappa)
@@ -529,7 +556,8 @@ class Output:
         r = nu / kappa
         keta2 = keta1 * r ** 0.25 / r
         rlam = 2 * Eu * math.sqrt(15 / eps) if eps > 0 else float("inf")
-        row = [t, Eu, ET, eps, epsT] + Nu + [0.0, 0.0, 0.0, 0.0, self._entropy(mult, v, Eu),
+        hel = self._helicity(v) if helicity else [0.0] * 4
+        row = [t, Eu, ET, eps, epsT] + Nu + hel + [self._entropy(mult, v, Eu),
                                             self._entropy(mult, th, ET), keta1, keta2, nu, kappa, rlam, dt,
                                             E[0], E[1], E[2]]
         with open(os.path.join(self.out_dir, "glob.d"), "a") as f:

@@ -334,9 +334,19 @@ def test_output_glob_rbc_matches_oracle(cuda, tmp_path):
             R.total_energy(g, U[:1]), R.total_energy(g, U[1:2]), R.total_energy(g, U[2:])]
     assert len(row) == 21
     for i, (a, b) in enumerate(zip(row, want)):
-        assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
+        assert abs(a - b) <= max(1e-10 * abs(b), 1e-12), (i, a, b)
     line = open(tmp_path / "glob.d").read()
     assert line.endswith("\t\n") and len(line.split("\t")) == 22
+
+
+def _helicity_np(V, kx, ky, kz, mult):
+    """H1, H2, k2H1, k2H2 on FFF with kfactor 1: h = 2 mult K . (Vr x Vi)"""
+    cr = np.cross(V.real, V.imag, axis=0)
+    h = 2 * mult * (kx * cr[0] + ky * cr[1] + kz * cr[2])
+    K2 = kx ** 2 + ky ** 2 + kz ** 2
+    H1 = float(h.sum())
+    return [H1, float(np.where(K2 > 1e-15, h / np.where(K2 > 1e-15, K2, 1.0), 0.0).sum()),
+            2 * float((K2 * h).sum()), 2 * H1]
 
 
 @pytest.mark.gpu
@@ -352,7 +362,7 @@ def test_output_glob_scalar_matches_oracle(cuda, tmp_path):
     T = R.reality_fix(g, 0.2 * R.forward(g, np.random.default_rng(22).standard_normal(g.rshape)))
     plan = tb.Plan(N, nu=nu, kappa=kappa, dt=1e-3)
     out = para.Output(plan, str(tmp_path))
-    row = out.glob_scalar(torch.from_numpy(U).to(cuda), torch.from_numpy(T[None]).to(cuda), 1.5, 1e-3)
+    row = out.glob_scalar(torch.from_numpy(U).to(cuda), torch.from_numpy(T[None]).to(cuda), 1.5, 1e-3, helicity=True)
     kx = np.fft.fftfreq(N[0], 1.0 / N[0])[:, None, None]
     ky = np.fft.fftfreq(N[1], 1.0 / N[1])[None, :, None]
     kz = np.arange(N[2] // 2 + 1)[None, None, :]
@@ -370,12 +380,13 @@ def test_output_glob_scalar_matches_oracle(cuda, tmp_path):
     kmax = para.max_radius_inside(N, (1.0, 1.0, 1.0))
     k1 = kmax * (nu ** 3 / eps) ** 0.25
     r = nu / kappa
-    want = [1.5, Eu, ET, eps, epsT, 0, 0, 0, 0, ent((np.abs(U) ** 2).sum(0), Eu), ent(np.abs(T) ** 2, ET), k1,
+    want = [1.5, Eu, ET, eps, epsT] + _helicity_np(U, kx, ky, kz, mult) + [ent((np.abs(U) ** 2).sum(0), Eu),
+                                                                         ent(np.abs(T) ** 2, ET), k1,
             k1 * r ** 0.25 / r, nu, kappa, 2 * Eu * math.sqrt(15 / eps), 1e-3,
             R.total_energy(g, U[:1]), R.total_energy(g, U[1:2]), R.total_energy(g, U[2:])]
     assert len(row) == 20
     for i, (a, b) in enumerate(zip(row, want)):
-        assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
+        assert abs(a - b) <= max(1e-10 * abs(b), 1e-12), (i, a, b)
 
 
 @pytest.mark.gpu
@@ -392,7 +403,7 @@ def test_output_glob_mhd_matches_oracle(cuda, tmp_path):
     B = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 4, 0.3)
     plan = tb.Plan(N, nu=nu, kappa=eta, dt=1e-3)
     out = para.Output(plan, str(tmp_path))
-    row = out.glob_mhd(torch.from_numpy(U).to(cuda), torch.from_numpy(B).to(cuda), 2.0, 1e-3)
+    row = out.glob_mhd(torch.from_numpy(U).to(cuda), torch.from_numpy(B).to(cuda), 2.0, 1e-3, helicity=True)
     kx = np.fft.fftfreq(N[0], 1.0 / N[0])[:, None, None]
     ky = np.fft.fftfreq(N[1], 1.0 / N[1])[None, :, None]
     kz = np.arange(N[2] // 2 + 1)[None, None, :]
@@ -412,10 +423,11 @@ def test_output_glob_mhd_matches_oracle(cuda, tmp_path):
     kmax = para.max_radius_inside(N, (1.0, 1.0, 1.0))
     k1 = kmax * (nu ** 3 / eps) ** 0.25
     r = nu / eta
-    want = ([2.0, Eu, Eb, eps, epsb, Hc, 0.5 * (nu + eta) * k2Hc] + [0] * 8 +
+    hu, hb = _helicity_np(U, kx, ky, kz, mult), _helicity_np(B, kx, ky, kz, mult)
+    want = ([2.0, Eu, Eb, eps, epsb, Hc, 0.5 * (nu + eta) * k2Hc] + hu[:2] + hb[:2] + hu[2:] + hb[2:] +
             [ent((np.abs(U) ** 2).sum(0), Eu), ent((np.abs(B) ** 2).sum(0), Eb), k1, k1 * r ** 0.25 / r, nu, eta,
              2 * Eu * math.sqrt(15 / eps), 1e-3] +
             [R.total_energy(g, U[i:i + 1]) for i in range(3)] + [R.total_energy(g, B[i:i + 1]) for i in range(3)])
     assert len(row) == 29
     for i, (a, b) in enumerate(zip(row, want)):
-        assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (i, a, b)
+        assert abs(a - b) <= max(1e-10 * abs(b), 1e-12), (i, a, b)
