@@ -104,10 +104,22 @@ int ts_plan_num_shells(const ts_plan* plan, int* n_shells);
  * The caller owns it and releases it with ts_free_field. */
 int ts_alloc_field(const ts_plan* plan, int ncomp, void** field);
 int ts_free_field(void* field);
-/* Wait for the plan's stream and report a bounded device wait that gave up in
- * any earlier call (TS_ERR_TIMEOUT); the stepping calls otherwise report it at
- * the next call.  No reference counterpart (the reference has no device waits). */
+/* Wait for the plan's stream and report the plan's health word: a bounded device
+ * wait that gave up in any earlier call (TS_ERR_TIMEOUT), else a NaN or Inf that a
+ * step wrote into the state (TS_ERR_NAN; every step's stage-4 store checks the
+ * values it writes, the device-side form of the reference's abort on a NaN total
+ * energy, Ifluid_main.cc:127-129).  The stepping calls report the same at their
+ * next call, without stepping.  The word stays set until ts_plan_clear_status. */
 int ts_plan_status(ts_plan* plan);
+/* Clear the plan's health word (after the caller has replaced a bad state).  No
+ * reference counterpart. */
+int ts_plan_clear_status(ts_plan* plan);
+/* Test of the timeout path: one block waits, with the library's bounded wait and
+ * `polls` polls, on an mbarrier that nothing arrives on and no copy completes, so
+ * the wait gives up, sets the plan's timeout bit and the kernel returns.  Then
+ * ts_plan_status reports TS_ERR_TIMEOUT and the context stays usable.  No
+ * reference counterpart. */
+int ts_plan_expire_wait(ts_plan* plan, int polls);
 /* Set the fixed time step (global.time.dt). */
 int ts_plan_set_dt(ts_plan* plan, double dt);
 
@@ -162,10 +174,20 @@ int ts_energy(ts_plan* plan, const void* a_hat, int ncomp, double* energy);
 /* Universal::Compute_shell_spectrum (universal_energy.cc:279-366), summed over
  * ncomp components: Ek[n_shells]. */
 int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, int n_shells);
-/* Energy flux through spheres: Pi(R_i) = sum_{|K|<=R_i} 2 mult Re(N.U*) with
- * N = F[(u.grad)u] of the dealiased U (one pass; equals EnergyTr::Compute_flux,
- * compute_flux.cc:51-65, for alias-free fields).  radii ascending. */
+/* EnergyTr::Compute_flux(U) (compute_flux.cc:51-65): the energy flux Pi(R_i) out of
+ * each sphere |K| <= R_i, radii ascending, at most 63.  Corner-box or no dealiasing:
+ * the reference's per-sphere algorithm, one giver nonlinear term per sphere
+ * (Fill_in_sphere fill_space.cc:56-64, Compute_nlin(U, Giver) compute_nlin_ET_VF.cc:
+ * 71-87) and Pi(R) = -sum_{|K| > R} 2 mult Re(N . conj(D U)) (prod_nlinV.cc:61-69).
+ * Two-thirds dealiasing: the same value from one nonlinear term, Pi(R) =
+ * sum_{|K| <= R} 2 mult Re(N . conj(D U)), N = F[(u.grad)u] (there the products
+ * alias only onto modes D U does not hold, so the two forms agree).  FP64 sums in a
+ * fixed order.  u_hat is not modified (the reference dealiases U in place here:
+ * call ts_dealias_field first to reproduce that side effect). */
 int ts_flux(ts_plan* plan, const void* u_hat, const double* radii, int n_radii, double* Pi);
+/* Universal::Dealias on ncomp components in place (FFF_pencil_basic.cc:87-90 corner
+ * box, or the plan's two-thirds rule; nothing for dealias NONE). */
+int ts_dealias_field(ts_plan* plan, void* a_hat, int ncomp);
 /* Raw shell sums for the reference's text outputs: sums[k] = sum over modes with
  * ceil|K| = k of mult K^2 Re(A . conj(B)) (B = NULL: |A|^2), counts[k] = sum of
  * 2 mult (Compute_local_shell_spectrum / _force, universal_energy.cc:196-229,
@@ -212,6 +234,12 @@ int ts_ensemble_run(ts_ensemble* ens, int nsteps);
 int ts_ensemble_synchronize(ts_ensemble* ens);
 /* Nusselt number of every member (Correlation.cc:154-156) */
 int ts_ensemble_nusselt(ts_ensemble* ens, double* Nu);
+/* Per-member health after the steps run so far (waits for them): status[m] =
+ * TS_OK, TS_ERR_NAN (the member's step wrote a NaN or Inf into its U or T) or
+ * TS_ERR_TIMEOUT (a bounded wait of its size group gave up).  Members are
+ * independent: a bad member does not change the others.  clear != 0 resets the
+ * words afterwards.  No reference counterpart (one run per reference process). */
+int ts_ensemble_health(ts_ensemble* ens, int* status, int clear);
 
 /* Discrete adjoint of the FFF IF-RK4 step (rotational form, unforced plans).
  * No reference counterpart: the reference has no adjoint.  Cotangents are
@@ -306,13 +334,15 @@ int ts_profile_read(ts_plan* plan, int kernel_class, double* total_ms, long long
  * synchronize the device).  Same result as ts_shell_spectrum, but it needs no
  * plan: the caller passes the geometry, the device field a_hat (ncomp
  * components) and a device array Ek[n_shells], which receives the normalised
- * spectrum.  The shell accumulators are a file-scope __device__ array of
- * TS_NOALLOC_MAX_SHELLS shells (64 KiB, held on every GPU that loads the
+ * spectrum.  The shell accumulators (the result and the per-block partial
+ * sums of the shell kernel's 32 blocks) are a file-scope __device__ array for
+ * TS_NOALLOC_MAX_SHELLS shells (2.06 MiB, held on every GPU that loads the
  * library until exit); more shells than that return TS_ERR_ARG with a message
  * on stderr.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call before
- * any stream capture.  Calls share the array and each clears it on `stream`
- * before use, so calls that overlap on the GPU race: order them. */
+ * any stream capture.  Calls share the array and each overwrites what it
+ * reads on `stream` before reading it, so calls that overlap on the GPU race:
+ * order them.  The sums are added in a fixed order (same field, same bits). */
 #define TS_NOALLOC_MAX_SHELLS 4096
 int ts_shell_spectrum_noalloc(int basis, int precision, const int N[3], const double kfactor[3], const void* a_hat,
                               int ncomp, double* Ek, int n_shells, void* stream);

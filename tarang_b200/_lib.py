@@ -70,6 +70,8 @@ SIGNATURES = {
     "ts_free_field": (ctypes.c_int, [ctypes.c_void_p]),
     "ts_plan_set_dt": (ctypes.c_int, [_P, ctypes.c_double]),
     "ts_plan_status": (ctypes.c_int, [_P]),
+    "ts_plan_clear_status": (ctypes.c_int, [_P]),
+    "ts_plan_expire_wait": (ctypes.c_int, [_P, ctypes.c_int]),
     "ts_fft_forward": (ctypes.c_int, [_P, ctypes.c_char_p, _P, _P, ctypes.c_int]),
     "ts_fft_inverse": (ctypes.c_int, [_P, ctypes.c_char_p, _P, _P, ctypes.c_int]),
     "ts_nlin": (ctypes.c_int, [_P, _P, _P]),
@@ -78,6 +80,7 @@ SIGNATURES = {
     "ts_energy": (ctypes.c_int, [_P, _P, ctypes.c_int, _D]),
     "ts_shell_spectrum": (ctypes.c_int, [_P, _P, ctypes.c_int, _D, ctypes.c_int]),
     "ts_flux": (ctypes.c_int, [_P, _P, _D, ctypes.c_int, _D]),
+    "ts_dealias_field": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "ts_max_div": (ctypes.c_int, [_P, _P, _D]),
     "ts_shell_sums": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _D, _D, ctypes.c_int]),
     "ts_force_field": (ctypes.c_int, [_P, _P, _P]),
@@ -92,6 +95,7 @@ SIGNATURES = {
     "ts_ensemble_run": (ctypes.c_int, [_P, ctypes.c_int]),
     "ts_ensemble_synchronize": (ctypes.c_int, [_P]),
     "ts_ensemble_nusselt": (ctypes.c_int, [_P, _D]),
+    "ts_ensemble_health": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     "ts_rk4_step_scalar": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
     "ts_rk4_step_mhd": (ctypes.c_int, [_P, _P, _P, ctypes.c_int]),
     "ts_rk4_step_keep": (ctypes.c_int, [_P, _P, _P, _P]),

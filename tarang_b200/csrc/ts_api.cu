@@ -77,9 +77,16 @@ struct ts_plan {
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_rec;
+  struct ProfRec {
+    int cls;
+    double bytes;  // algorithmic bytes of the bracketed launches (< 0: the class's static model)
+    cudaEvent_t b, e;
+  };
+  std::vector<ProfRec> ev_rec;
   double prof_ms[TS_KCLASS_COUNT] = {0};
   long long prof_n[TS_KCLASS_COUNT] = {0};
+  double prof_bytes[TS_KCLASS_COUNT] = {0};  // summed per-launch algorithmic bytes
+  long long prof_nb[TS_KCLASS_COUNT] = {0};  // launches whose bytes were recorded
 };
 
 // ---------------------------------------------------------------------------
@@ -99,20 +106,27 @@ static void prof_collect(ts_plan* p) {
   cudaStreamSynchronize(p->st);
   for (auto& r : p->ev_rec) {
     float ms = 0;
-    if (cudaEventElapsedTime(&ms, r.second.first, r.second.second) == cudaSuccess) {
-      p->prof_ms[r.first] += ms;
-      p->prof_n[r.first] += 1;
+    if (cudaEventElapsedTime(&ms, r.b, r.e) == cudaSuccess) {
+      p->prof_ms[r.cls] += ms;
+      p->prof_n[r.cls] += 1;
+      if (r.bytes >= 0) {
+        p->prof_bytes[r.cls] += r.bytes;
+        p->prof_nb[r.cls] += 1;
+      }
     }
   }
   p->ev_rec.clear();
   p->ev_used = 0;
 }
 
+// bytes: the algorithmic bytes of the launches the scope brackets (every field
+// element they must read or write, once); < 0 leaves the class's static model
 struct ProfScope {
   ts_plan* p;
   int cls;
+  double bytes;
   cudaEvent_t b = nullptr;
-  ProfScope(ts_plan* p_, int c) : p(p_), cls(c) {
+  ProfScope(ts_plan* p_, int c, double by = -1.0) : p(p_), cls(c), bytes(by) {
     if (p->prof) {
       if (p->ev_used + 2 > 8192) prof_collect(p);
       b = prof_event(p);
@@ -124,7 +138,7 @@ struct ProfScope {
       cudaEvent_t e = prof_event(p);
       if (e) {
         cudaEventRecord(e, p->st);
-        p->ev_rec.push_back({cls, {b, e}});
+        p->ev_rec.push_back({cls, bytes, b, e});
       }
     }
   }
@@ -133,6 +147,18 @@ struct ProfScope {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+// the status of the plan's health word as last copied to the host (err_h)
+static int health_status(ts_plan* p) {
+  if (*p->err_h & HEALTH_TIMEOUT) {
+    g_last_error = "a bounded device wait gave up (a bulk copy never arrived)";
+    return TS_ERR_TIMEOUT;
+  }
+  if (*p->err_h & HEALTH_NONFINITE) {
+    g_last_error = "a step wrote a NaN or Inf into the state";
+    return TS_ERR_NAN;
+  }
+  return TS_OK;
+}
 static bool is_device_ptr(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -454,10 +480,21 @@ int ts_plan_status(ts_plan* p) {
   if (!p) return TS_ERR_ARG;
   CK(cudaStreamSynchronize(p->st));
   CK(cudaMemcpy(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost));
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
-    return TS_ERR_TIMEOUT;
-  }
+  return health_status(p);
+}
+
+int ts_plan_clear_status(ts_plan* p) {
+  if (!p) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(p->st));
+  CK(cudaMemset(p->err_d, 0, sizeof(int)));
+  *p->err_h = 0;
+  return TS_OK;
+}
+
+int ts_plan_expire_wait(ts_plan* p, int polls) {
+  if (!p || polls < 1 || polls > (1 << 22)) return TS_ERR_ARG;
+  CK(LAUNCH(p, expire_wait, p->err_d, polls, p->st));
+  CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
   return TS_OK;
 }
 
@@ -476,6 +513,52 @@ int ts_plan_set_dt(ts_plan* p, double dt) {
 // ---------------------------------------------------------------------------
 // right-hand side pipeline (FFF)
 // ---------------------------------------------------------------------------
+// Algorithmic bytes of each pass of one FFF right-hand side: every element the pass
+// must read or write, once, with the dealias skipping counted as it runs.  Two
+// thirds (kept): the x inverse reads the nxk x nyk x nzk modes that can be nonzero
+// and writes all Nx rows of the nyk x nzk kept columns; the y inverse reads their
+// nyk rows and writes all Ny rows of the nzk kept z planes; the z pass reads those
+// planes and writes full lines.  Other modes: the x inverse does not read the
+// corner box's zeros.  fwd_x: the products plus the state fields of the mode and
+// stage (stage 1 reads U0 and writes Ucur, tot; stages 2-3 also read tot; stage 4
+// reads U0, tot and writes Uout).
+static double fff_pass_bytes(const ts_plan* p, int cls, int nin, int nout, int kept, int mode = MODE_STEP,
+                             int stage = 1) {
+  const Geo& g = p->g;
+  auto kept_count = [](int N, bool half) {
+    int n = 0;
+    for (int l = 0; l < (half ? N / 2 + 1 : N); ++l) {
+      const int k = half ? l : (l <= N / 2 ? l : l - N);
+      n += 3 * (k < 0 ? -k : k) <= N;
+    }
+    return (double)n;
+  };
+  const double S = (double)g.S, Nx = g.Nx, Ny = g.Ny, cb = (double)p->cb;
+  const double nxk = kept_count(g.Nx, false), nyk = kept_count(g.Ny, false), nzk = kept_count(g.Nz, true);
+  double nz_read = S;  // modes of a component the x inverse reads
+  if (!kept && g.dealias == TS_DEALIAS_REFERENCE_CORNER) {
+    const double bx = (double)((2 * g.Nx / 3 - 1) - (g.Nx / 3 + 1) + 1), by = (double)((2 * g.Ny / 3 - 1) - (g.Ny / 3 + 1) + 1);
+    const double bz = (double)(g.Nz / 2 - (g.Nz / 3 + 1) + 1);
+    nz_read = S - (bx > 0 ? bx : 0) * (by > 0 ? by : 0) * (bz > 0 ? bz : 0);
+  }
+  double e = 0;
+  switch (cls) {
+    case TS_KCLASS_INV_X: e = kept ? 3 * nxk * nyk * nzk + nin * Nx * nyk * nzk : 3 * nz_read + nin * S; break;
+    case TS_KCLASS_Y_INV: e = kept ? nin * (Nx * nyk * nzk + Nx * Ny * nzk) : 2.0 * nin * S; break;
+    case TS_KCLASS_Z: e = kept ? nin * Nx * Ny * nzk + nout * S : (nin + nout) * S; break;
+    case TS_KCLASS_Y_FWD: e = 2.0 * nout * S; break;
+    case TS_KCLASS_FWD_X: {
+      double st = 3;  // MODE_FLUX reads the field, MODE_NLIN writes N
+      if (mode == MODE_STEP) st = (stage == 1 || stage == 4) ? 9 : 12;
+      if (mode == MODE_ADJ) st = stage == 1 ? 6 : (stage == 4 ? 9 : 12);
+      e = (nout + st) * S;
+      break;
+    }
+    default: break;
+  }
+  return e * cb;
+}
+
 static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in) {
   const Geo& g = p->g;
   StageArgs a = a_in;
@@ -490,14 +573,21 @@ static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in)
   // inverse transforms only kz <= Nz/3 and reads only the 3|ky| <= Ny rows, and the
   // z pass reads only kz <= Nz/3 (the skipped memory is never read)
   const int kept = g.dealias == TS_DEALIAS_TWO_THIRDS;
-  { ProfScope ps(p, TS_KCLASS_INV_X); CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, nullptr, 0.0, p->st, kept)); }
+  auto by = [&](int cls) { return p->prof ? fff_pass_bytes(p, cls, nin, nout, kept, mode, a.stage) : -1.0; };
   {
-    ProfScope ps(p, TS_KCLASS_Y_INV);
+    ProfScope ps(p, TS_KCLASS_INV_X, by(TS_KCLASS_INV_X));
+    CK(LAUNCH(p, inv_x, g, rot, Uin, p->P, p->twx, nullptr, 0.0, p->st, kept));
+  }
+  {
+    ProfScope ps(p, TS_KCLASS_Y_INV, by(TS_KCLASS_Y_INV));
     CK(LAUNCH(p, strided, g, 1, +1, p->P, nin, p->twy, p->st, 0, 0, kept ? g.Nz / 3 + 1 : 0, kept));
   }
-  { ProfScope ps(p, TS_KCLASS_Z); CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->err_d, p->st, 1, 0, kept ? g.Nz / 3 : -1)); }
-  { ProfScope ps(p, TS_KCLASS_Y_FWD); CK(LAUNCH(p, strided, g, 1, -1, p->P, nout, p->twy, p->st)); }
-  { ProfScope ps(p, TS_KCLASS_FWD_X); CK(LAUNCH(p, fwd_x, g, rot, mode, p->P, a, p->twx, p->st)); }
+  {
+    ProfScope ps(p, TS_KCLASS_Z, by(TS_KCLASS_Z));
+    CK(LAUNCH(p, z_fused, g, rot, p->P, p->twz, p->err_d, p->st, 1, 0, kept ? g.Nz / 3 : -1));
+  }
+  { ProfScope ps(p, TS_KCLASS_Y_FWD, by(TS_KCLASS_Y_FWD)); CK(LAUNCH(p, strided, g, 1, -1, p->P, nout, p->twy, p->st)); }
+  { ProfScope ps(p, TS_KCLASS_FWD_X, by(TS_KCLASS_FWD_X)); CK(LAUNCH(p, fwd_x, g, rot, mode, p->P, a, p->twx, p->st)); }
   return TS_OK;
 }
 
@@ -614,6 +704,7 @@ static int step_rbc(ts_plan* p, void* U0, void* T0) {
   const Geo& g = p->g;
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.health = p->err_d;
   a.U0 = U0;
   a.T0 = T0;
   a.Ucur = p->Ucur;
@@ -668,6 +759,7 @@ static int step_scalar_fff(ts_plan* p, void* U0, void* T0) {
   const Geo& g = p->g;
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.health = p->err_d;
   a.U0 = U0;
   a.T0 = T0;
   a.Ucur = p->Ucur;
@@ -752,6 +844,7 @@ static int step_mhd_fff(ts_plan* p, void* U0, void* B0) {
   const Geo& g = p->g;
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.health = p->err_d;
   a.U0 = U0;
   a.T0 = B0;
   a.Ucur = p->Ucur;
@@ -832,6 +925,7 @@ static int ssf_step_supported(ts_plan* p, bool rbc) {
 static SffArgs ssf_rbc_args(ts_plan* p, void* U0, void* T0) {
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.health = p->err_d;
   a.U0 = U0;
   a.T0 = T0;
   a.Ucur = p->Ucur;
@@ -857,6 +951,7 @@ static int step_ssf(ts_plan* p, void* U0, void* T0 = nullptr) {
   a.Ucur = p->Ucur;
   a.tot = p->tot;
   a.dt = p->cfg.dt;
+  a.err = p->err_d;
   a.ex = p->eax[0];
   a.ey = p->eax[1];
   a.ez = p->eax[2];
@@ -931,6 +1026,7 @@ static int step_sss(ts_plan* p, void* U0, void* T0 = nullptr) {
   a.Ucur = p->Ucur;
   a.tot = p->tot;
   a.dt = p->cfg.dt;
+  a.err = p->err_d;
   a.ex = p->eax[0];
   a.ey = p->eax[1];
   a.ez = p->eax[2];
@@ -1005,10 +1101,8 @@ int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
     const bool sss = p->cfg.basis == TS_BASIS_SSS;
     CKS(ssf_step_supported(p, false));
-    if (*p->err_h) {
-      g_last_error = "a bounded device wait gave up";
-      return TS_ERR_TIMEOUT;
-    }
+    // the health word of earlier calls (copied back without a sync)
+    if (*p->err_h) return health_status(p);
     int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
       for (int s = 0; s < nsteps; ++s) CKS(sss ? step_sss(p, U) : step_ssf(p, U));
       return (int)TS_OK;
@@ -1018,10 +1112,8 @@ int ts_rk4_step(ts_plan* p, void* u_hat, int nsteps) {
   }
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
   // a bounded device wait that gave up in an earlier call (read without a sync)
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   int rc = with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, true, [&](void* U) -> int {
     for (int s = 0; s < nsteps; ++s) CKS(step_fff(p, U));
     return (int)TS_OK;
@@ -1040,10 +1132,8 @@ int ts_rk4_step_keep(ts_plan* p, const void* u_hat, void* u_next, void* stages) 
     g_last_error = "ts_rk4_step_keep: 16-byte aligned device pointers required";
     return TS_ERR_ARG;
   }
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   CKS(step_fff(p, const_cast<void*>(u_hat), u_next, stages));
   CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
   return TS_OK;
@@ -1056,10 +1146,8 @@ int ts_adjoint_step(ts_plan* p, const void* u_hat, const void* stages, void* lam
     g_last_error = "ts_adjoint_step: device pointers required (lam_hat 16-byte aligned)";
     return TS_ERR_ARG;
   }
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   CKS(adjoint_step_fff(p, u_hat, stages, lam_hat));
   CK(cudaMemcpyAsync(p->err_h, p->err_d, sizeof(int), cudaMemcpyDeviceToHost, p->st));
   return TS_OK;
@@ -1085,10 +1173,8 @@ int ts_adjoint_window(ts_plan* p, const void* u_start, int nsteps, void* lam_hat
     g_last_error = "ts_adjoint_window: 16-byte aligned device pointers required";
     return TS_ERR_ARG;
   }
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up (TMA tile never arrived)";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   // work slot n = [U_n (3 components), U1, U2, U3 of step n (9)]; U_0 is u_start itself
   const size_t cs = 3 * (size_t)p->g.S * p->cb, slot = 4 * cs;
   char* w = (char*)work;
@@ -1107,10 +1193,8 @@ int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
     const bool sss = p->cfg.basis == TS_BASIS_SSS;
     CKS(ssf_step_supported(p, true));
-    if (*p->err_h) {
-      g_last_error = "a bounded device wait gave up";
-      return TS_ERR_TIMEOUT;
-    }
+    // the health word of earlier calls (copied back without a sync)
+    if (*p->err_h) return health_status(p);
     const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
     int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
       return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
@@ -1122,10 +1206,8 @@ int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
     return rc;
   }
   if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
   int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
     return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
@@ -1140,10 +1222,8 @@ int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
 int ts_rk4_step_scalar(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   if (!p || !u_hat || !T_hat || nsteps < 0) return TS_ERR_ARG;
   CKS(scalar_supported(p));
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
   int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
     return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
@@ -1158,10 +1238,8 @@ int ts_rk4_step_scalar(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
 int ts_rk4_step_mhd(ts_plan* p, void* u_hat, void* b_hat, int nsteps) {
   if (!p || !u_hat || !b_hat || nsteps < 0) return TS_ERR_ARG;
   CKS(mhd_supported(p));
-  if (*p->err_h) {
-    g_last_error = "a bounded device wait gave up";
-    return TS_ERR_TIMEOUT;
-  }
+  // the health word of earlier calls (copied back without a sync)
+  if (*p->err_h) return health_status(p);
   const size_t bu = 3 * p->g.S * p->cb;
   int rc = with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
     return with_device(p, &p->stage_b, b_hat, bu, true, [&](void* B) -> int {
@@ -1213,7 +1291,7 @@ int ts_nlin(ts_plan* p, void* u_hat, void* nlin_hat) {
 
 int ts_energy(ts_plan* p, const void* a_hat, int ncomp, double* energy) {
   if (!p || !a_hat || !energy || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
+  return with_device(p, &p->stage_u, a_hat, (size_t)ncomp * p->g.S * p->cb, false, [&](void* A) -> int {
     CK(cudaMemsetAsync(p->dscr, 0, sizeof(double), p->st));
     CK(LAUNCH(p, energy, p->g, A, A, ncomp, p->dscr, p->st));
     CK(cudaMemcpyAsync(energy, p->dscr, sizeof(double), cudaMemcpyDeviceToHost, p->st));
@@ -1237,10 +1315,9 @@ int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int 
   if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || !Ek || ncomp < 1 || ncomp > 3 || n_shells < 1) return TS_ERR_ARG;
   const int nsh = p->nshells;
-  return with_device(p, &p->stage_u, a_hat, 3 * p->g.S * p->cb, false, [&](void* A) -> int {
-    CKS(ensure_scratch(p, 2 * nsh));
-    CK(cudaMemsetAsync(p->dscr, 0, 2 * nsh * sizeof(double), p->st));
-    CK(LAUNCH(p, shell, p->g, A, ncomp, nsh - 1, p->dscr, p->st));
+  return with_device(p, &p->stage_u, a_hat, (size_t)ncomp * p->g.S * p->cb, false, [&](void* A) -> int {
+    CKS(ensure_scratch(p, 2ull * nsh * (1 + shell_blocks(p->g, SHELL_MAX_BLOCKS))));
+    CK(LAUNCH(p, shell, p->g, A, ncomp, nsh, p->dscr, p->st));
     std::vector<double> h(2 * nsh);
     CK(cudaMemcpyAsync(h.data(), p->dscr, 2 * nsh * sizeof(double), cudaMemcpyDeviceToHost, p->st));
     CK(cudaStreamSynchronize(p->st));
@@ -1264,9 +1341,8 @@ int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, d
     return TS_ERR_ARG;
   }
   const int nsh = p->nshells;
-  CKS(ensure_scratch(p, 2 * nsh));
-  CK(cudaMemsetAsync(p->dscr, 0, 2 * nsh * sizeof(double), p->st));
-  CK(LAUNCH(p, shell, p->g, a_hat, ncomp, nsh - 1, p->dscr, p->st, b_hat));
+  CKS(ensure_scratch(p, 2ull * nsh * (1 + shell_blocks(p->g, SHELL_MAX_BLOCKS))));
+  CK(LAUNCH(p, shell, p->g, a_hat, ncomp, nsh, p->dscr, p->st, b_hat));
   std::vector<double> h(2 * nsh);
   CK(cudaMemcpyAsync(h.data(), p->dscr, 2 * nsh * sizeof(double), cudaMemcpyDeviceToHost, p->st));
   CK(cudaStreamSynchronize(p->st));
@@ -1298,29 +1374,73 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
   if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
   if (p->cfg.basis != TS_BASIS_FFF) return TS_ERR_UNSUPPORTED;
+  if (n_radii >= FLUX_MAX_BINS) {
+    g_last_error = "ts_flux: at most " + std::to_string(FLUX_MAX_BINS - 1) + " radii";
+    return TS_ERR_ARG;
+  }
   for (int i = 1; i < n_radii; ++i)
     if (!(radii[i] >= radii[i - 1])) return TS_ERR_ARG;
-  return with_device(p, &p->stage_u, u_hat, 3 * p->g.S * p->cb, false, [&](void* U) -> int {
-    CKS(ensure_scratch(p, 2 * (n_radii + 1)));
-    double* bins = p->dscr;
-    double* rad = p->dscr + (n_radii + 1);
-    CK(cudaMemsetAsync(bins, 0, (n_radii + 1) * sizeof(double), p->st));
-    CK(cudaMemcpyAsync(rad, radii, n_radii * sizeof(double), cudaMemcpyHostToDevice, p->st));
-    StageArgs a;
-    memset(&a, 0, sizeof(a));
-    a.Ud = U;
-    a.bins = bins;
-    a.radii = rad;
-    a.nradii = n_radii;
-    CKS(rhs_fff(p, U, MODE_FLUX, a));
+  const Geo& g = p->g;
+  const long long nb = 1 + 148 * 16;  // a result plus the per-block partials of one reduction
+  return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false, [&](void* U) -> int {
     std::vector<double> h(n_radii + 1);
-    CK(cudaMemcpyAsync(h.data(), bins, (n_radii + 1) * sizeof(double), cudaMemcpyDeviceToHost, p->st));
-    CK(cudaStreamSynchronize(p->st));
-    double acc = 0;
-    for (int i = 0; i < n_radii; ++i) {
-      acc += h[i];
-      Pi[i] = acc;
+    if (g.dealias == TS_DEALIAS_TWO_THIRDS) {
+      // one pass: with two-thirds dealiasing the products of kept modes alias only onto
+      // modes the dealiased field does not hold, so <u_<, (u.grad)u> = -<u_>, (u.grad)u_<>
+      // and Pi(R) = sum_{|K| <= R} 2 mult Re(N . conj(D U)) from one nonlinear term
+      CKS(ensure_scratch(p, (size_t)(n_radii + 1) * nb + n_radii));
+      double* bins = p->dscr;
+      double* rad = p->dscr + (n_radii + 1) * nb;
+      CK(cudaMemcpyAsync(rad, radii, n_radii * sizeof(double), cudaMemcpyHostToDevice, p->st));
+      StageArgs a;
+      memset(&a, 0, sizeof(a));
+      a.Ud = U;
+      a.bins = bins;
+      a.radii = rad;
+      a.nradii = n_radii;
+      CKS(rhs_fff(p, U, MODE_FLUX, a));
+      CK(cudaMemcpyAsync(h.data(), bins, (n_radii + 1) * sizeof(double), cudaMemcpyDeviceToHost, p->st));
+      CK(cudaStreamSynchronize(p->st));
+      double acc = 0;
+      for (int i = 0; i < n_radii; ++i) {
+        acc += h[i];
+        Pi[i] = acc;
+      }
+      return (int)TS_OK;
     }
+    // the reference's per-sphere form (EnergyTr::Compute_flux, compute_flux.cc:51-65), which
+    // under the corner-box (or no) dealiasing differs from the one-pass form by the aliased
+    // part of the products: per radius R, the giver G = D U inside |K| <= R (Fill_in_sphere),
+    // the giver nonlinear term N_i = sum_j D_j F[u_j G_i] (Compute_nlin(U, Giver)) and
+    // Pi(R) = -sum_{|K| > R} 2 mult Re(N . conj(D U))
+    CKS(ensure_work(p, p->nS, 9));
+    CKS(ensure_scratch(p, (size_t)n_radii * nb));
+    for (int i = 0; i < n_radii; ++i) {
+      CK(LAUNCH(p, inv_x, g, 5, U, p->P, p->twx, nullptr, 0.0, p->st, 0, radii[i]));
+      CK(LAUNCH(p, strided, g, 1, +1, p->P, 6, p->twy, p->st));
+      CK(LAUNCH(p, z_fused, g, 6, p->P, p->twz, p->err_d, p->st));
+      CK(LAUNCH(p, strided, g, 1, -1, p->P, 9, p->twy, p->st));
+      CK(LAUNCH(p, strided, g, 0, -1, p->P, 9, p->twx, p->st));
+      CK(LAUNCH(p, flux_outside, g, p->P, U, radii[i], p->dscr + i * nb, p->st));
+    }
+    for (int i = 0; i < n_radii; ++i)
+      CK(cudaMemcpyAsync(&h[i], p->dscr + i * nb, sizeof(double), cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    for (int i = 0; i < n_radii; ++i) Pi[i] = -h[i];
+    return (int)TS_OK;
+  });
+}
+
+int ts_dealias_field(ts_plan* p, void* a_hat, int ncomp) {
+  if (!p || !a_hat || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
+  if (p->cfg.basis == TS_BASIS_SSS) {
+    g_last_error = "ts_dealias_field: SSS plans hold real coefficients (use the step's own dealiasing)";
+    return TS_ERR_UNSUPPORTED;
+  }
+  if (!p->g.dealias) return TS_OK;
+  return with_device(p, &p->stage_u, a_hat, (size_t)ncomp * p->g.S * p->cb, true, [&](void* A) -> int {
+    CK(LAUNCH(p, dealias_copy, p->g, A, A, ncomp, p->st));
+    CK(cudaStreamSynchronize(p->st));
     return (int)TS_OK;
   });
 }
@@ -1501,6 +1621,8 @@ int ts_profile_reset(ts_plan* p) {
   for (int i = 0; i < TS_KCLASS_COUNT; ++i) {
     p->prof_ms[i] = 0;
     p->prof_n[i] = 0;
+    p->prof_bytes[i] = 0;
+    p->prof_nb[i] = 0;
   }
   return TS_OK;
 }
@@ -1510,8 +1632,11 @@ int ts_profile_read(ts_plan* p, int kclass, double* total_ms, long long* launche
   prof_collect(p);
   if (total_ms) *total_ms = p->prof_ms[kclass];
   if (launches) *launches = p->prof_n[kclass];
-  if (bytes_per_launch) {
-    // algorithmic bytes: every field a launch must read or write, once
+  if (bytes_per_launch && p->prof_nb[kclass] > 0 && p->prof_nb[kclass] == p->prof_n[kclass]) {
+    // every launch recorded its own algorithmic bytes (the FFF step and the adjoint)
+    *bytes_per_launch = p->prof_bytes[kclass] / (double)p->prof_nb[kclass];
+  } else if (bytes_per_launch) {
+    // static model: every field a launch must read or write, once
     const double f = (double)p->g.S * (double)p->cb;
     const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
     double b = 0;
@@ -1559,12 +1684,14 @@ struct ens_group {
   double* et = nullptr;  // same with kappa
   cudaStream_t st = nullptr;
   cudaEvent_t done = nullptr;
+  int* health = nullptr;  // B health words (a slice of the ensemble's array), member j at j
 };
 
 struct ts_ensemble {
   std::vector<ts_plan*> plans;
   std::vector<void*> U, T;  // member views into the group arrays
   std::vector<ens_group> groups;
+  int* health = nullptr;    // one health word per member, in group order (ens_group::health)
   cudaEvent_t fork = nullptr;
   cudaStream_t origin = nullptr;
   bool own_origin = false;
@@ -1593,6 +1720,7 @@ static int step_rbc_group(ens_group& G) {
     a.et[i] = G.et + aoff[i];
   }
   a.mtab = TL;
+  a.health = G.health;
   a.msU0 = 3 * S;
   a.msT0 = S;
   a.msUcur = 4 * S;
@@ -1635,6 +1763,7 @@ int ts_ensemble_destroy(ts_ensemble* e) {
   }
   for (ts_plan* p : e->plans)
     if (p) ts_plan_destroy(p);
+  if (e->health) cudaFree(e->health);
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->own_origin && e->origin) cudaStreamDestroy(e->origin);
   delete e;
@@ -1679,6 +1808,13 @@ int ts_ensemble_create(const ts_config* base, const ts_member* members, int coun
       gof[m] = (int)e->groups.size() - 1;
     }
     e->groups[gof[m]].idx.push_back(m);
+  }
+  if (cudaMalloc(&e->health, count * sizeof(int)) != cudaSuccess) return fail(TS_ERR_NOMEM);
+  if (cudaMemset(e->health, 0, count * sizeof(int)) != cudaSuccess) return fail(TS_ERR_CUDA);
+  size_t hoff = 0;
+  for (ens_group& G : e->groups) {
+    G.health = e->health + hoff;
+    hoff += G.idx.size();
   }
   for (ens_group& G : e->groups) {
     const Geo& g = G.gp->g;
@@ -1762,6 +1898,30 @@ int ts_ensemble_run(ts_ensemble* e, int nsteps) {
 int ts_ensemble_synchronize(ts_ensemble* e) {
   if (!e) return TS_ERR_ARG;
   CK(cudaStreamSynchronize(e->origin));
+  return TS_OK;
+}
+
+int ts_ensemble_health(ts_ensemble* e, int* status, int clear) {
+  if (!e || !status) return TS_ERR_ARG;
+  CK(cudaStreamSynchronize(e->origin));
+  std::vector<int> h(e->plans.size(), 0);
+  CK(cudaMemcpy(h.data(), e->health, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  size_t off = 0;
+  for (ens_group& G : e->groups) {
+    // a bounded wait that gave up in a group's launch counts against all its members
+    int ge = 0;
+    CK(cudaMemcpy(&ge, G.gp->err_d, sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t j = 0; j < G.idx.size(); ++j) {
+      const int w = h[off + j] | ge;
+      status[G.idx[j]] = (w & HEALTH_TIMEOUT) ? TS_ERR_TIMEOUT : ((w & HEALTH_NONFINITE) ? TS_ERR_NAN : TS_OK);
+    }
+    off += G.idx.size();
+    if (clear) {
+      CK(cudaMemset(G.gp->err_d, 0, sizeof(int)));
+      *G.gp->err_h = 0;
+    }
+  }
+  if (clear) CK(cudaMemset(e->health, 0, e->plans.size() * sizeof(int)));
   return TS_OK;
 }
 

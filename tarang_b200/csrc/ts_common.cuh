@@ -366,4 +366,52 @@ __device__ __forceinline__ bool dealias_zero(int mode, int basis, int lx, int ly
   return false;
 }
 
+// ---------------------------------------------------------------------------
+// FP64 reductions in a fixed order (butterfly within a warp, warps in index order),
+// so that every sum built from them is reproducible bit for bit
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// every thread of the block must call it; thread 0 (warp 0) holds the sum
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x + 31) / 32) ? red[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_sum(v);
+  return v;
+}
+
+// out[i] = sum over b = 0..nblocks-1 of part[b * n + i], b in increasing order:
+// the fixed-order final sum of per-block partial bins
+static __global__ void k_bins_finish(const double* __restrict__ part, int nblocks, int n, double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part[(long long)b * n + i];
+    out[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// health word of a plan (or of one ensemble member): bit HEALTH_TIMEOUT = a bounded
+// wait gave up, bit HEALTH_NONFINITE = a step wrote a NaN or Inf into the state
+// (the reference aborts on a NaN total energy, Ifluid_main.cc:127-129)
+// ---------------------------------------------------------------------------
+constexpr int HEALTH_TIMEOUT = 1, HEALTH_NONFINITE = 2;
+__device__ __forceinline__ void health_mark(bool bad, int* hw) {
+  if (bad && hw && !(*(volatile int*)hw & HEALTH_NONFINITE)) atomicOr(hw, HEALTH_NONFINITE);
+}
+template <typename V> __device__ __forceinline__ bool nonfinite(const V& v) { return !(isfinite(v.x) && isfinite(v.y)); }
+
 }  // namespace ts

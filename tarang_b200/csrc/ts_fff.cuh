@@ -32,6 +32,9 @@ struct Geo {
   signed char tb[TUNE_NCLASS] = {0, 0, 0, 0, 0};
 };
 
+// warps per block of the shell-sum kernel k_shell (each warp walks whole z lines)
+constexpr int SHELL_WARPS = 4;
+
 // ---------------------------------------------------------------------------
 // plain strided-axis FFT (x or y axis) over nf fields, in place
 // element (o, row, col) at o*ostride + row*rstride + col, col < inner.
@@ -157,8 +160,13 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
     const uint32_t phase = (uint32_t)(k >> 1) & 1u;
     const bool got = mbar_wait(&bar[slot], phase, err);
     if (__syncthreads_or(!got)) {
-      // give the copies in flight a second bounded chance to land, then leave
-      if (threadIdx.x == 0) mbar_wait(&bar[slot], phase, nullptr);
+      // give every copy in flight (this tile's and the next tile's, issued into the
+      // other slot) a second bounded chance to land before the block's shared memory
+      // goes away, then leave
+      if (threadIdx.x == 0) {
+        mbar_wait(&bar[slot], phase, nullptr);
+        if (tile + (int)gridDim.x < ntiles) mbar_wait(&bar[slot ^ 1], (uint32_t)((k + 1) >> 1) & 1u, nullptr);
+      }
       return;
     }
     const int col = tile * CW + c;
@@ -210,13 +218,15 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
 // cotangent divided by the C2R weight c (2 on the planes 0 < kz < Nz/2, else 1).
 // ---------------------------------------------------------------------------
 // FORM 4: the cotangent fields 6..8 of FORM 3 only (written at W + 6 S ...)
-__host__ __device__ constexpr int inv_x_nout(int form) { return form == 0 ? 3 : (form == 1 ? 6 : 9); }
+// FORM 5 (the giver of the per-sphere energy flux): W_0..2 = D U and W_3..5 = D U
+// inside the sphere |K| <= rad (Fill_in_sphere, fill_space.cc:56-64), zero outside
+__host__ __device__ constexpr int inv_x_nout(int form) { return form == 0 ? 3 : ((form == 1 || form == 5) ? 6 : 9); }
 __host__ __device__ constexpr int inv_x_first(int form) { return form == 4 ? 6 : 0; }
 
 template <typename T, int L, int E, int CW, int FORM>
 __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     k_inv_x_ld(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw,
-               const C<T>* __restrict__ Lam, T lsc, int kept) {
+               const C<T>* __restrict__ Lam, T lsc, int kept, double rad) {
   typedef C<T> V;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
@@ -242,6 +252,12 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
   const long long rstride = inner;
   constexpr int nout = inv_x_nout(FORM);
   const T lw = (lz > 0 && 2 * lz < g.Nz) ? lsc * (T)0.5 : lsc;
+  // FORM 5: |K| <= rad with |K| = sqrt((Kx^2 + Ky^2) + Kz^2) in FP64 (Kmagnitude)
+  const double Kyd = kfft(ly, g.Ny) * g.kf[1], Kzd = lz * g.kf[2];
+  auto in_sphere = [&](int lx) {
+    const double Kxd = kfft(lx, g.Nx) * g.kf[0];
+    return sqrt((Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd) <= rad;
+  };
   // FP32 with up to 8 elements per thread: the three (dealiased) components of U
   // are loaded once, up front, and every output field is built from registers
   // (FP64 would spill them)
@@ -270,6 +286,8 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
       if (UPFRONT && f < 6) {
         if (f < 3) {
           a = u[f][s];
+        } else if (FORM == 5) {
+          a = in_sphere(lx) ? u[f - 3][s] : mk<V>(0, 0);
         } else {
           const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
           const int i = f - 3, i1 = i == 2 ? 0 : i + 1, i2 = i == 0 ? 2 : i - 1;
@@ -292,6 +310,8 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
       } else if (ok && !dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) {
         if (f < 3) {
           a = U[f * g.S + off];
+        } else if (FORM == 5) {
+          a = in_sphere(lx) ? U[(f - 3) * g.S + off] : mk<V>(0, 0);
         } else {
           // omega_i = i (K_{i+1} U_{i+2} - K_{i+2} U_{i+1})  (indices mod 3)
           const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
@@ -339,11 +359,13 @@ template <int M> __host__ __device__ constexpr int zslot() { return M + M / 16 +
 // FORM 3 (adjoint of the rotational form): in u, w, mu -> mu x u, then w x mu
 // FORM 5 (MHD):           in u1..3, b1..3      -> Zp_i Zm_j (f = 3 i + j), Zp = u + b, Zm = u - b
 //                         (compute_nlin_VF_MHD.cc:40-95, MHD.cc:75-84)
+// FORM 6 (flux giver):    in u1..3, g1..3      -> u_i g_j (f = 3 i + j), for the giver nonlinear
+//                         term N_i = sum_j D_j F[u_j g_i] (compute_nlin_ET_VF.cc:71-87)
 __host__ __device__ constexpr int z_nin(int form) {
-  return form == 0 ? 3 : (form == 1 ? 6 : (form == 2 ? 4 : (form == 5 ? 6 : 9)));
+  return form == 0 ? 3 : (form == 1 ? 6 : (form == 2 ? 4 : ((form == 5 || form == 6) ? 6 : 9)));
 }
 __host__ __device__ constexpr int z_nout(int form) {
-  return form == 0 ? 6 : (form == 1 ? 3 : (form == 2 ? 9 : (form == 5 ? 9 : 6)));
+  return form == 0 ? 6 : (form == 1 ? 3 : (form == 2 ? 9 : ((form == 5 || form == 6) ? 9 : 6)));
 }
 
 // component f of a x b for real points packed two per complex (re, im independent)
@@ -353,10 +375,10 @@ template <typename V> __device__ __forceinline__ V cross_pk(int f, const V* a, c
 }
 // factor indices (a, b) of product output f for FORM 0 / 2
 __host__ __device__ constexpr int z_pa(int f, int form = 0) {
-  return form == 5 ? f / 3 : (f < 3 ? f : (f < 6 ? f - 3 : f - 6));
+  return (form == 5 || form == 6) ? f / 3 : (f < 3 ? f : (f < 6 ? f - 3 : f - 6));
 }
 __host__ __device__ constexpr int z_pb(int f, int form = 0) {
-  return form == 5 ? 3 + f % 3 : (f < 3 ? f : (f < 6 ? (f == 5 ? 0 : f - 2) : 3));
+  return (form == 5 || form == 6) ? 3 + f % 3 : (f < 3 ? f : (f < 6 ? (f == 5 ? 0 : f - 2) : 3));
 }
 // FORM 5: the real lines of u and b (packed two points per complex) become the
 // Elsasser lines Zp = u + b, Zm = u - b in place
@@ -691,9 +713,9 @@ __device__ __forceinline__ void zreg_forward_store(C<T> (&p)[E], C<T>* Xo, bool 
 // the 12-element radix-3 lines (which would spill at 170), 4 for 512-point lines
 // (two warps per line, the pair terms through the exchange line; spilled at 170)
 // (8 for the 4-element variant)
-// (4 for the MHD form, which holds six lines while it makes nine products)
+// (4 for the MHD and flux-giver forms, which hold six lines while they make nine products)
 template <int NZ, int EZ = 0, int FORM = 0> __host__ __device__ constexpr int zreg_min_blocks() {
-  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : ((NZ >= 1024 || FORM == 5) ? 4 : 6));
+  return EZ == 4 ? 8 : ((NZ / 2) % 3 == 0 ? 3 : ((NZ >= 1024 || FORM == 5 || FORM == 6) ? 4 : 6));
 }
 
 // EZ = 0: 8 elements per thread, 12 for a line length with a factor 3 (radices
@@ -893,7 +915,11 @@ __global__ void __launch_bounds__(256, 1) k_z_tma(C<T>* __restrict__ P, Geo g, c
     const uint32_t phase = (uint32_t)(k >> 1) & 1u;
     const bool got = mbar_wait(&bar[slot], phase, err);
     if (__syncthreads_or(!got)) {
-      if (threadIdx.x == 0) mbar_wait(&bar[slot], phase, nullptr);
+      // drain this group's copies and the next group's (other slot), each wait bounded
+      if (threadIdx.x == 0) {
+        mbar_wait(&bar[slot], phase, nullptr);
+        if (grp + (long long)gridDim.x < ngroups) mbar_wait(&bar[slot ^ 1], (uint32_t)((k + 1) >> 1) & 1u, nullptr);
+      }
       return;
     }
     V in[NIN][E];
@@ -968,7 +994,7 @@ struct StageArgs {
   void* tot;         // RK accumulator; MODE_ADJ: the adjoint accumulator
   void* nout;        // MODE_NLIN: output N (3 comps)
   const void* Ud;    // MODE_FLUX: field whose dealiased copy multiplies N
-  double* bins;      // MODE_FLUX: per-sphere accumulators (global)
+  double* bins;      // MODE_FLUX: nradii + 1 sums, then per-block partial sums, nradii + 1 per block
   const double* radii;
   int nradii;
   const void* fcube; // force cube (3 comps of (2km+1)^2 (km+1)), nullptr = no force
@@ -983,6 +1009,8 @@ struct StageArgs {
 };
 
 enum { MODE_STEP = 0, MODE_FLUX = 1, MODE_NLIN = 2, MODE_ADJ = 3 };
+// MODE_FLUX: at most FLUX_MAX_BINS - 1 radii (each thread keeps one FP64 partial per sphere)
+constexpr int FLUX_MAX_BINS = 64;
 
 // Assembly of the stage's spectral vector from forward-transformed product f
 // (p already scaled by 1/(Nx Ny Nz)):
@@ -1045,7 +1073,7 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
     const double Kmag = sqrt((Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd);
     int b = 0;
     while (b < a.nradii && Kmag > a.radii[b]) ++b;
-    atomicAdd(&sbins[b], 2.0 * mult * re);
+    sbins[b] += 2.0 * mult * re;  // the calling thread's own partials, in a fixed element order
     return;
   }
   if (MODE == MODE_ADJ) {
@@ -1122,6 +1150,7 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
       } else {
         const V un = add(scale(u0, E1), add(tt, scale(R, (T)((1.0 / 6) * a.dt))));
         reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
+        health_mark(nonfinite(un), a.err);
       }
     }
   }
@@ -1155,7 +1184,9 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   V* pst = reinterpret_cast<V*>(smraw);
   V* xch = pst + 2 * TILE;              // exchange tile, row pitch CW (L x (CW + 1) reserved)
   V* sst = xch + L * (CW + 1);
-  double* sbins = reinterpret_cast<double*>(sst + NST * TILE);
+  // MODE_FLUX: per-thread FP64 partials of the spheres (thread-local, fixed element order;
+  // summed over the block by block_sum and over blocks by k_bins_finish: reproducible)
+  double tb[MODE == MODE_FLUX ? FLUX_MAX_BINS : 1];
   __shared__ __align__(8) uint64_t bar[3];  // product slots 0, 1; state
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
   const int inner = g.Ny * g.Hz;
@@ -1169,7 +1200,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   const int sfirst = (MODE == MODE_ADJ && a.stage == 1) ? 3 : 0;
 
   if (MODE == MODE_FLUX)
-    for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x) sbins[i] = 0.0;
+    for (int i = 0; i <= a.nradii; ++i) tb[i] = 0.0;
   if (threadIdx.x == 0) {
     for (int i = 0; i < 3; ++i) mbar_init(&bar[i], 1);
     fence_mbar_init();
@@ -1199,6 +1230,14 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
   // a runtime-indexed array would live in local memory)
   uint32_t ph0 = 0, ph1 = 0, phs = 0;
   long long item = 0;
+  // after a wait gave up: a second bounded wait on every copy still in flight (the
+  // product items `item` and item + 1, and this tile's state tiles if pending), so no
+  // bulk copy lands in the shared memory of a block that has left
+  auto drain = [&](bool state_pending) {
+    if (threadIdx.x != 0) return;
+    for (long long i = item; i < item + 2 && i < nitems; ++i) mbar_wait(&bar[i & 1], (i & 1) ? ph1 : ph0, nullptr);
+    if (state_pending) mbar_wait(&bar[2], phs, nullptr);
+  };
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     if (threadIdx.x == 0) issue_state(tile);
     const int col = tile * CW + c;
@@ -1219,7 +1258,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
       const uint32_t phase = slot ? ph1 : ph0;
       const bool got = mbar_wait(&bar[slot], phase, a.err);
       if (__syncthreads_or(!got)) {
-        if (threadIdx.x == 0) mbar_wait(&bar[slot], phase, nullptr);
+        drain(nstate > 0);
         return;
       }
       if (slot) ph1 ^= 1;
@@ -1246,7 +1285,7 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
     if (nstate) {
       const bool got = mbar_wait(&bar[2], phs, a.err);
       if (__syncthreads_or(!got)) {
-        if (threadIdx.x == 0) mbar_wait(&bar[2], phs, nullptr);
+        drain(true);
         return;
       }
       phs ^= 1;
@@ -1259,16 +1298,17 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
         const long long off = lx * rstride + col;
         const int so = lx * CW + c;
         spec_epilogue<T, MODE>(g, a, lx, ly, lz, off, exy, acc[0][s], acc[1][s], acc[2][s], sst + so,
-                               sst + 3 * TILE + so, TILE, sbins);
+                               sst + 3 * TILE + so, TILE, tb);
       }
     }
     // the next tile's state load overwrites the state tiles
     __syncthreads();
   }
   if (MODE == MODE_FLUX) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x)
-      if (sbins[i] != 0.0) atomicAdd(&a.bins[i], sbins[i]);
+    for (int i = 0; i <= a.nradii; ++i) {
+      const double v = block_sum(tb[i]);
+      if (threadIdx.x == 0) a.bins[(long long)(blockIdx.x + 1) * (a.nradii + 1) + i] = v;
+    }
   }
 }
 
@@ -1283,11 +1323,9 @@ template <typename T, int FORM, int MODE>
 __global__ void __launch_bounds__(256) k_spec_epi(const C<T>* __restrict__ P, Geo g, StageArgs a) {
   typedef C<T> V;
   constexpr int NF = FORM == 1 ? 3 : 6;
-  extern __shared__ double sbins[];  // MODE_FLUX: per-sphere partial sums
-  if (MODE == MODE_FLUX) {
-    for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x) sbins[i] = 0.0;
-    __syncthreads();
-  }
+  double tb[MODE == MODE_FLUX ? FLUX_MAX_BINS : 1];  // MODE_FLUX: per-thread sphere partials
+  if (MODE == MODE_FLUX)
+    for (int i = 0; i <= a.nradii; ++i) tb[i] = 0.0;
   const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
   const V* st0 = reinterpret_cast<const V*>(MODE == MODE_FLUX ? a.Ud : a.U0);
   const V* st1 = reinterpret_cast<const V*>(a.tot);
@@ -1302,12 +1340,13 @@ __global__ void __launch_bounds__(256) k_spec_epi(const C<T>* __restrict__ P, Ge
     for (int f = 0; f < NF; ++f) accum_product<FORM>(f, scale(P[f * g.S + e], inv), Kx, Ky, Kz, a0, a1, a2);
     const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
     spec_epilogue<T, MODE>(g, a, lx, ly, lz, e, exy, a0, a1, a2, st0 ? st0 + e : nullptr,
-                           st1 ? st1 + e : nullptr, g.S, sbins);
+                           st1 ? st1 + e : nullptr, g.S, tb);
   }
   if (MODE == MODE_FLUX) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < a.nradii + 1; i += blockDim.x)
-      if (sbins[i] != 0.0) atomicAdd(&a.bins[i], sbins[i]);
+    for (int i = 0; i <= a.nradii; ++i) {
+      const double v = block_sum(tb[i]);
+      if (threadIdx.x == 0) a.bins[(long long)(blockIdx.x + 1) * (a.nradii + 1) + i] = v;
+    }
   }
 }
 

@@ -202,7 +202,7 @@ constexpr bool ix_valid(int L, int v) {
 }
 
 template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
-                                         const void* lam, double lsc, cudaStream_t st, int kept) {
+                                         const void* lam, double lsc, cudaStream_t st, int kept, double rad) {
   cudaError_t err_ = cudaErrorInvalidValue;
   // forms 0 and 1 follow the tuning; the adjoint forms keep the rule
   const int v = form <= 1 ? g.tv[TUNE_X_INV] : 0;
@@ -220,7 +220,8 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
                                    : (unsigned)((inner + CW - 1) / CW);
       auto run = [&](auto kern) {
         if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
-        kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc, kept);
+        kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc, kept,
+                                                 rad);
         ++g_launches;
         err_ = cudaGetLastError();
       };
@@ -229,6 +230,7 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
       else if constexpr (decltype(vc)::value == 0) {
         if (form == 3) run(k_inv_x_ld<T, LL, E, CW, 3>);
         else if (form == 4) run(k_inv_x_ld<T, LL, E, CW, 4>);
+        else if (form == 5) run(k_inv_x_ld<T, LL, E, CW, 5>);
       }
     };
     if (v == 1 && ix_valid(LL, 1)) {
@@ -349,6 +351,7 @@ template <> cudaError_t Launch<T>::z_fused(const Geo& g, int form, void* P, cons
     else if (form == 1) err = z_fused_impl<NZ, 1>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
     else if (form == 2) err = z_fused_impl<NZ, 2>(g, P, tw, zerr, st, nmem, msP, zkeep, v);
     else if (form == 5) err = z_fused_impl<NZ, 5>(g, P, tw, zerr, st, nmem, msP, zkeep, 0);
+    else if (form == 6) err = z_fused_impl<NZ, 6>(g, P, tw, zerr, st, nmem, msP, zkeep, 0);
     else if constexpr (NZ % 3 != 0) err = z_fused_impl<NZ, 3>(g, P, tw, zerr, st, 1, 0, zkeep, 0);
   });
   return err;
@@ -447,10 +450,13 @@ static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, c
     constexpr int NF = FORM == 1 ? 3 : 6;
     cudaError_t err = Launch<T>::strided(g, 0, -1, const_cast<void*>(P), NF, tw, st);
     if (err != cudaSuccess) return err;
-    const size_t sm = MODE == MODE_FLUX ? (size_t)(a.nradii + 1) * sizeof(double) : 0;
-    if ((err = smem_attr(k_spec_epi<T, FORM, MODE>, sm)) != cudaSuccess) return err;
-    k_spec_epi<T, FORM, MODE><<<grid1d(g.S, 256), 256, sm, st>>>((const V*)P, g, a);
+    const unsigned blocks = grid1d(g.S, 256);
+    k_spec_epi<T, FORM, MODE><<<blocks, 256, 0, st>>>((const V*)P, g, a);
     ++g_launches;
+    if (MODE == MODE_FLUX) {
+      k_bins_finish<<<1, 64, 0, st>>>(a.bins + (a.nradii + 1), (int)blocks, a.nradii + 1, a.bins);
+      ++g_launches;
+    }
     return cudaGetLastError();
   }
   if constexpr (CW * sizeof(V) >= 64) return fwd_x_fused<FORM, MODE, LL, emin(E_ACC, LL), CW>(g, P, a, tw, st);
@@ -462,7 +468,6 @@ static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, 
   const int inner = g.Ny * g.Hz;
   const int ntiles = (inner + CW - 1) / CW;
   size_t sm = (size_t)(MODE == MODE_NLIN ? 2 : 8) * LL * CW * sizeof(V) + (size_t)LL * (CW + 1) * sizeof(V) + 128;
-  if (MODE == MODE_FLUX) sm += (size_t)(a.nradii + 1) * sizeof(double);
   const int bps = MODE == MODE_STEP ? g.tb[TUNE_X_FWD] : 0;
   const int per_sm = bps > 0 ? bps : ((int)((220 * 1024) / sm) >= 2 ? 2 : 1);
   const int blocks = ntiles < 148 * per_sm ? ntiles : 148 * per_sm;
@@ -478,6 +483,10 @@ static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, 
   if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
   k<<<blocks, CW * (LL / E), sm, st>>>(mP, mA, mB, g, a, (const V*)tw);
   ++g_launches;
+  if (MODE == MODE_FLUX) {
+    k_bins_finish<<<1, 64, 0, st>>>(a.bins + (a.nradii + 1), blocks, a.nradii + 1, a.bins);
+    ++g_launches;
+  }
   return cudaGetLastError();
 }
 
@@ -649,13 +658,31 @@ template <> cudaError_t Launch<T>::maxdiv(const Geo& g, const void* U, unsigned 
   return cudaGetLastError();
 }
 
-template <> cudaError_t Launch<T>::shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins,
-                                         cudaStream_t st, const void* B) {
-  const size_t sm = 2ull * (kmax + 1) * sizeof(double);
+template <> cudaError_t Launch<T>::shell(const Geo& g, const void* A, int ncomp, int nbins, double* bins,
+                                         cudaStream_t st, const void* B, unsigned cap) {
+  const size_t sm = (size_t)(SHELL_WARPS + 1) * nbins * sizeof(double);
+  if (sm > 220 * 1024) return cudaErrorInvalidValue;
   cudaError_t err = smem_attr(k_shell<T>, sm);
   if (err != cudaSuccess) return err;
-  k_shell<T><<<grid1d(g.S, 256), 256, sm, st>>>((const V*)A, ncomp, g, kmax, bins, (const V*)B);
+  const unsigned blocks = shell_blocks(g, cap);
+  k_shell<T><<<blocks, 32 * SHELL_WARPS, sm, st>>>((const V*)A, (const V*)B, ncomp, g, nbins, bins + 2 * nbins);
+  k_bins_finish<<<(2 * nbins + 255) / 256, 256, 0, st>>>(bins + 2 * nbins, (int)blocks, 2 * nbins, bins);
+  g_launches += 2;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::expire_wait(int* err, int polls, cudaStream_t st) {
+  k_expire_wait<<<1, 32, 0, st>>>(err, polls);
   ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::flux_outside(const Geo& g, const void* P, const void* U, double R, double* out,
+                                                cudaStream_t st) {
+  const unsigned blocks = grid1d(g.S, 256);
+  k_flux_outside<T><<<blocks, 256, 0, st>>>((const V*)P, (const V*)U, g, R, out);
+  k_sum_partials<<<1, 256, 0, st>>>(out, (int)blocks);
+  g_launches += 2;
   return cudaGetLastError();
 }
 

@@ -8,6 +8,14 @@
 namespace ts {
 
 extern long long g_launches;  // kernels launched by this library
+constexpr unsigned SHELL_MAX_BLOCKS = 4 * 148;  // blocks of the plan's shell-sum kernel
+// blocks of k_shell for a geometry and a cap (the sums' rounding depends on it, so a
+// geometry and cap always give the same blocks)
+inline unsigned shell_blocks(const Geo& g, unsigned cap) {
+  const long long lines = (long long)g.Nx * g.Ny;
+  const long long b = (lines + SHELL_WARPS - 1) / SHELL_WARPS;
+  return (unsigned)(b < (long long)cap ? b : (long long)cap);
+}
 
 template <typename T> struct Launch {
   // strided-axis FFT on nf fields in place: axis 0 = x (L = Nx), 1 = y (L = Ny);
@@ -20,9 +28,11 @@ template <typename T> struct Launch {
   // form 0 conservative (3 fields out), 1 rotational (6), 3 adjoint of the rotational form (9: also
   // lsc c^-1 P lam from the cotangent lam)
   // kept != 0 (forms 0, 1 with two-thirds dealiasing): write only the columns with 3|ky| <= Ny, 3 kz <= Nz
+  // form 5: u and the giver u inside |K| <= rad (6 fields) for the per-sphere energy flux
   static cudaError_t inv_x(const Geo& g, int form, const void* U, void* W, const void* tw, const void* lam,
-                           double lsc, cudaStream_t st, int kept = 0);
-  // form 0 conservative, 1 rotational, 2 Boussinesq (u, T), 3 adjoint of the rotational form
+                           double lsc, cudaStream_t st, int kept = 0, double rad = 0.0);
+  // form 0 conservative, 1 rotational, 2 Boussinesq (u, T), 3 adjoint of the rotational form,
+  // 5 MHD (Elsasser products), 6 flux giver (u_i g_j)
   // nmem members, member fields msP complex apart
   // zkeep >= 0: input rows kz > zkeep are zero and not read
   static cudaError_t z_fused(const Geo& g, int form, void* P, const void* tw, int* err, cudaStream_t st,
@@ -71,15 +81,23 @@ template <typename T> struct Launch {
                             const double* hs, const double* mis, int nsup, cudaStream_t st);
   static cudaError_t energy(const Geo& g, const void* A, const void* B, int ncomp, double* out, cudaStream_t st);
   static cudaError_t maxdiv(const Geo& g, const void* U, unsigned long long* out, cudaStream_t st);
-  // B != nullptr: cross spectrum Re(A . conj(B))
-  static cudaError_t shell(const Geo& g, const void* A, int ncomp, int kmax, double* bins, cudaStream_t st,
-                           const void* B = nullptr);
+  // shell sums of the shells s = ceil|K| < nbins into bins[0, nbins) and the counts into bins[nbins, 2 nbins);
+  // B != nullptr: cross spectrum Re(A . conj(B)).  bins must hold 2 nbins (1 + shell_blocks(g, cap))
+  // doubles (the per-block partials follow the result); the sums are reproducible bit for bit
+  static cudaError_t shell(const Geo& g, const void* A, int ncomp, int nbins, double* bins, cudaStream_t st,
+                           const void* B = nullptr, unsigned cap = SHELL_MAX_BLOCKS);
+  // per-sphere energy flux: out[0] = sum over |K| > R of 2 mult Re(N . conj(D U)), N from the
+  // nine x-forward-transformed giver products in P; out must hold 1 + 148 * 16 doubles
+  static cudaError_t flux_outside(const Geo& g, const void* P, const void* U, double R, double* out,
+                                  cudaStream_t st);
   static cudaError_t force_scatter(const Geo& g, const void* fc, void* F, int km, cudaStream_t st);
   static cudaError_t init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
                              unsigned long long key, cudaStream_t st);
   static cudaError_t scale(void* A, long long n, double s, cudaStream_t st);
   static cudaError_t init_temp(const Geo& g, void* A, double amp, double kmax, unsigned long long key, cudaStream_t st);
   static cudaError_t dealias_copy(const Geo& g, const void* A, void* B, int ncomp, cudaStream_t st);
+  // one block whose bounded wait gives up after `polls` polls (test of the timeout path)
+  static cudaError_t expire_wait(int* err, int polls, cudaStream_t st);
   // launch tuning (Geo::tv, Geo::tb): whether kernel candidate v (0 = the rule) of pass class
   // cls exists for this geometry and product form (form as z_fused; the basis selects the
   // SFF x kernels), and whether the class takes a blocks-per-SM count (persistent launches)

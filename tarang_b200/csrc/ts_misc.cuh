@@ -156,29 +156,23 @@ __global__ void k_carati(const C<T>* __restrict__ U, C<T>* fc, Geo g, int km, do
 }
 
 // ---------------------------------------------------------------------------
-// reductions (FP64 accumulation)
+// Test of the bounded-wait path (ts_plan_expire_wait): one thread waits on an
+// mbarrier that expects one arrival which never comes, with no bulk copy in flight,
+// so mbar_wait gives up after `polls` polls, sets the timeout bit of *err and the
+// kernel returns.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
+static __global__ void k_expire_wait(int* err, int polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_wait(&bar, 0, err, polls);  // phase 0 never completes
+  }
 }
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-__device__ __forceinline__ double block_sum(double v) {
-  __shared__ double red[32];
-  v = warp_sum(v);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  v = (threadIdx.x < (blockDim.x + 31) / 32) ? red[threadIdx.x] : 0.0;
-  if (w == 0) v = warp_sum(v);
-  return v;
-}
+
+// ---------------------------------------------------------------------------
+// reductions (FP64 accumulation; warp_sum / block_sum are in ts_common.cuh)
+// ---------------------------------------------------------------------------
 
 // plane weights of the total energy: FFF 1/2 on kz=0 (FFF_pencil_energy.cc:59-68);
 // SFF 2, minus 1 on kz=0, minus 1 on m=0, plus 1/2 on (m=0,kz=0) (SFF_pencil_energy.cc:76-95);
@@ -292,39 +286,115 @@ __device__ __forceinline__ double multiplicity(int basis, int lx, int ly, int lz
 }
 
 // Shell spectrum accumulation (Compute_local_shell_spectrum universal_energy.cc:279-313):
-// bins[s] += mult |K|^2 sum_i |A_i|^2 ; bins[nsh + s] += 2 mult, s = ceil|K| <= kmax.
-// Block-private shared bins, then one global atomic per bin.
+// for every shell s = ceil|K| < nbins, sums[s] = sum mult |K|^2 sum_i Re(A_i conj(B_i)) (B = A:
+// |A|^2) and counts[s] = sum 2 mult.  Reproducible bit for bit, without atomics on the sums:
+// each warp walks whole z lines (|K| grows along a line, so the modes of one shell sit in
+// adjacent lanes of a 32-mode chunk), adds a chunk by a segmented scan whose segment tails
+// update the warp's own shared bins, and the block writes its partial bins (warps added in
+// index order) to part[blockIdx.x][2 nbins] (sums, then counts) for k_bins_finish.  The
+// counts are sums of small integers, exact in any order (shared atomics).
 template <typename T>
-__global__ void k_shell(const C<T>* __restrict__ A, int ncomp, Geo g, int kmax, double* bins,
-                        const C<T>* __restrict__ B = nullptr) {
-  extern __shared__ double sb[];
-  const int nsh = kmax + 1;
-  for (int i = threadIdx.x; i < 2 * nsh; i += blockDim.x) sb[i] = 0;
+__global__ void __launch_bounds__(32 * SHELL_WARPS)
+    k_shell(const C<T>* __restrict__ A, const C<T>* __restrict__ B, int ncomp, Geo g, int nbins,
+            double* __restrict__ part) {
+  extern __shared__ double sb[];  // [SHELL_WARPS][nbins] sums, then [nbins] counts
+  double* cnt = sb + SHELL_WARPS * nbins;
+  for (int i = threadIdx.x; i < (SHELL_WARPS + 1) * nbins; i += blockDim.x) sb[i] = 0;
   __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* wb = sb + w * nbins;
+  const long long n = g.S, nlines = (long long)g.Nx * g.Ny;
+  if (!B) B = A;
+  for (long long line = (long long)blockIdx.x * SHELL_WARPS + w; line < nlines;
+       line += (long long)gridDim.x * SHELL_WARPS) {
+    const int lx = (int)(line / g.Ny), ly = (int)(line % g.Ny);
+    const double Kx = (g.basis == 0 ? kfft(lx, g.Nx) : lx) * g.kf[0];
+    const double Ky = kfft(ly, g.Ny) * g.kf[1];
+    for (int z0 = 0; z0 < g.Hz; z0 += 32) {
+      const int lz = z0 + lane;
+      int key = 0x7fffffff;
+      double v = 0, c = 0;
+      if (lz < g.Hz) {
+        const double Kz = lz * g.kf[2];
+        const double Kmag = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz);
+        const int idx = (int)ceil(Kmag);
+        if (idx < nbins) {
+          const long long e = line * g.Hz + lz;
+          const double f = multiplicity(g.basis, lx, ly, lz, g.Nx, g.Ny);
+          double a2 = 0;
+          for (int i = 0; i < ncomp; ++i) {
+            const C<T> a = A[i * n + e], b = B[i * n + e];
+            a2 += (double)a.x * b.x + (double)a.y * b.y;
+          }
+          key = idx;
+          v = f * a2 * (Kmag * Kmag);
+          c = 2 * f;
+        }
+      }
+      // keys do not decrease along the chunk: inclusive scan within runs of equal keys
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double vo = __shfl_up_sync(0xffffffffu, v, o), co = __shfl_up_sync(0xffffffffu, c, o);
+        const int ko = __shfl_up_sync(0xffffffffu, key, o);
+        if (lane >= o && ko == key) {
+          v += vo;
+          c += co;
+        }
+      }
+      const int kn = __shfl_down_sync(0xffffffffu, key, 1);
+      if (key != 0x7fffffff && (lane == 31 || kn != key)) {
+        wb[key] += v;
+        atomicAdd(&cnt[key], c);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+    double t = 0;
+    for (int k = 0; k < SHELL_WARPS; ++k) t += sb[k * nbins + i];
+    part[(long long)blockIdx.x * 2 * nbins + i] = t;
+    part[(long long)blockIdx.x * 2 * nbins + nbins + i] = cnt[i];
+  }
+}
+
+// Energy flux out of one sphere, per-sphere form (EnergyTr::Compute_flux compute_flux.cc:51-65):
+// P holds the nine x-forward-transformed giver products F[u_a g_b] (component 3 a + b,
+// unnormalised), so N_i = sum_j i K_j F[u_j g_i] / (Nx Ny Nz) (compute_nlin_ET_VF.cc:71-87);
+// out[1 + block] = sum over the modes with |K| > R of 2 mult Re(N . conj(D U))
+// (Prod_out_sphere_nlinV prod_nlinV.cc:61-69, Local_shell_mult_single universal_ET.cc:51-70),
+// D = the dealias mask; k_sum_partials adds the blocks in a fixed order.
+template <typename T>
+__global__ void k_flux_outside(const C<T>* __restrict__ P, const C<T>* __restrict__ U, Geo g, double R,
+                               double* __restrict__ out) {
   const long long n = g.S;
+  const double inv = 1.0 / ((double)g.Nx * g.Ny * g.Nz);
+  double s = 0;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int lz = (int)(e % g.Hz);
     const int ly = (int)((e / g.Hz) % g.Ny);
     const int lx = (int)(e / ((long long)g.Ny * g.Hz));
-    const double Kx = (g.basis == 0 ? kfft(lx, g.Nx) : lx) * g.kf[0];
-    const double Ky = kfft(ly, g.Ny) * g.kf[1], Kz = lz * g.kf[2];
-    const double K2 = (Kx * Kx + Ky * Ky) + Kz * Kz;
-    const double Kmag = sqrt(K2);
-    const int idx = (int)ceil(Kmag);
-    if (idx > kmax) continue;
-    const double f = multiplicity(g.basis, lx, ly, lz, g.Nx, g.Ny);
-    // |A|^2, or Re(A . conj(B)) for a cross spectrum
-    double a2 = 0;
-    for (int i = 0; i < ncomp; ++i) {
-      const C<T> a = A[i * n + e], b = B ? B[i * n + e] : a;
-      a2 += (double)a.x * b.x + (double)a.y * b.y;
+    if (dealias_zero(g.dealias, 0, lx, ly, lz, g.Nx, g.Ny, g.Nz)) continue;
+    const double K[3] = {kfft(lx, g.Nx) * g.kf[0], kfft(ly, g.Ny) * g.kf[1], lz * g.kf[2]};
+    const double Kmag = sqrt((K[0] * K[0] + K[1] * K[1]) + K[2] * K[2]);
+    if (!(Kmag > R)) continue;
+    double re = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double nr = 0, ni = 0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const C<T> q = P[(3 * j + i) * n + e];
+        nr -= K[j] * (double)q.y;
+        ni += K[j] * (double)q.x;
+      }
+      const C<T> u = U[i * n + e];
+      re += (nr * inv) * (double)u.x + (ni * inv) * (double)u.y;
     }
-    atomicAdd(&sb[idx], f * a2 * (Kmag * Kmag));
-    atomicAdd(&sb[nsh + idx], 2 * f);
+    s += 2.0 * multiplicity(0, lx, ly, lz, g.Nx, g.Ny) * re;
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 2 * nsh; i += blockDim.x)
-    if (sb[i] != 0) atomicAdd(&bins[i], sb[i]);
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[1 + blockIdx.x] = s;
 }
 
 // ---------------------------------------------------------------------------

@@ -8,12 +8,15 @@
 // __device__ array instead of plan scratch: this entry point calls no
 // cudaMalloc, cudaFree or other allocating routine and needs no plan.
 //
-// The array holds TS_NOALLOC_MAX_SHELLS shells (2 doubles each: sum and mode
-// count, 64 KiB) on every GPU that loads the library, until the process exits.
-// Every call on a device shares it and it keeps the previous call's contents;
-// each call clears it on its stream before use, so calls that overlap on the
-// GPU (different streams, or different host threads) race and must be ordered
-// by the caller.
+// The array holds, for up to TS_NOALLOC_MAX_SHELLS shells, the result (sum and
+// mode count per shell) and the per-block partial sums of the shell kernel's
+// kNoallocBlocks blocks: 2 x 4096 x (1 + 32) doubles, 2.06 MiB, on every GPU that
+// loads the library, until the process exits.  Every call on a device shares it
+// and it keeps the previous call's contents; each call overwrites every entry it
+// reads before reading it (the partials of every block, then the result), so
+// calls that overlap on the GPU (different streams, or different host threads)
+// race and must be ordered by the caller.  The sums are added in a fixed order,
+// so two calls on the same field give the same bits.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -24,7 +27,9 @@
 
 namespace {
 
-static __device__ __align__(256) double g_noalloc_bins[2 * TS_NOALLOC_MAX_SHELLS];
+// blocks of the shell kernel on this path (its partial sums live in the static array)
+constexpr unsigned kNoallocBlocks = 32;
+static __device__ __align__(256) double g_noalloc_bins[2 * TS_NOALLOC_MAX_SHELLS * (1 + kNoallocBlocks)];
 
 constexpr int kMaxDevices = 64;
 double* g_bins_addr[kMaxDevices] = {nullptr};
@@ -77,17 +82,10 @@ template <typename T>
 int run(const ts::Geo& g, const void* a, int ncomp, int kmax, double* bins, double* Ek, int n_shells, double kfp,
         cudaStream_t st) {
   const int nsh = kmax + 1;
-  const size_t sm = 2ull * nsh * sizeof(double);
-  cudaError_t e = cudaMemsetAsync(bins, 0, sm, st);
-  if (e != cudaSuccess) { set_err("cudaMemsetAsync", e); return TS_ERR_CUDA; }
-  if (sm > 48 * 1024) {
-    e = cudaFuncSetAttribute(ts::k_shell<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) { set_err("cudaFuncSetAttribute", e); return TS_ERR_CUDA; }
-  }
-  long long blocks = (g.S + 255) / 256;
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  ts::k_shell<T><<<(unsigned)blocks, 256, sm, st>>>((const ts::C<T>*)a, ncomp, g, kmax, bins);
-  ++ts::g_launches;
+  // the shell kernel writes every block's partial bins, then the fixed-order sum
+  // writes bins[0, 2 nsh): nothing is read before this call has written it
+  cudaError_t e = ts::Launch<T>::shell(g, a, ncomp, nsh, bins, st, nullptr, kNoallocBlocks);
+  if (e != cudaSuccess) { set_err("shell kernel launch", e); return TS_ERR_CUDA; }
   k_shell_finish<<<(n_shells + 255) / 256, 256, 0, st>>>(bins, nsh, kfp, Ek, n_shells);
   ++ts::g_launches;
   e = cudaGetLastError();

@@ -41,6 +41,9 @@ struct SffArgs {
   // complex elements, and of the integrating-factor tables in doubles (0 for one run)
   long long msU0, msT0, msUcur, msTot, msU1in, msTin, msP;
   long long mtab;
+  // health words, one per member (the member index of the batch): a NaN or Inf written
+  // into the state at stage 4 sets HEALTH_NONFINITE (nullptr: no check)
+  int* health;
 };
 
 // blocks per SM the SFF x kernels are compiled for: power-of-two lengths (8
@@ -269,6 +272,7 @@ __device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, lon
       if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
       if (i < 3) const_cast<V*>(U0)[o] = un;
       else const_cast<V*>(T0)[off] = un;
+      health_mark(nonfinite(un), a.health ? a.health + mb : nullptr);
     }
   }
 }
@@ -466,6 +470,7 @@ __global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, 
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(T0)[e] = un;
+        health_mark(nonfinite(un), a.health);
       }
     }
   }
@@ -551,6 +556,7 @@ __global__ void __launch_bounds__(256, 3) k_mhd_epi(const C<T>* __restrict__ P, 
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(B0)[(i - 3) * g.S + e] = un;
+        health_mark(nonfinite(un), a.health);
       }
     }
   }
@@ -615,7 +621,9 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
         Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
         tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
       } else {
-        Uo[o] = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        const V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        Uo[o] = un;
+        health_mark(nonfinite(un), a.err);
       }
     }
   }
@@ -692,7 +700,9 @@ __global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g,
         Uc[o] = (u0 * Eh + (T)a.dt * R) * Eh;
         tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
       } else {
-        Uo[o] = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
+        const T un = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
+        Uo[o] = un;
+        health_mark(!isfinite(un), a.err);
       }
     }
   }
@@ -768,6 +778,7 @@ __global__ void __launch_bounds__(256) k_ssf_rbc_epi(const C<T>* __restrict__ P,
         const V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
         if (i < 3) U0[o] = un;
         else T0[e] = un;
+        health_mark(nonfinite(un), a.health);
       }
     }
   }
@@ -829,6 +840,7 @@ __global__ void __launch_bounds__(256) k_sss_rbc_epi(const T* __restrict__ P, Ge
         const T un = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
+        health_mark(!isfinite(un), a.health);
       }
     }
   }

@@ -35,12 +35,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after ~2^22 polls (each try_wait may suspend briefly),
-// records the failure in *err and returns false.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  for (int i = 0; i < (1 << 22); ++i)
+// Bounded wait: gives up after `polls` polls (default 2^22; each try_wait may
+// suspend briefly), sets the timeout bit of *err and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int polls = 1 << 22) {
+  for (int i = 0; i < polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
-  if (err) atomicExch(err, 1);
+  if (err) atomicOr(err, 1);
   return false;
 }
 // 1-D bulk copy global -> shared (16-byte aligned addresses, size multiple of 16)

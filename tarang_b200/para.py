@@ -299,7 +299,8 @@ class Output:
     universal_energy.cc:196-262); for a forced plan %%(Fv.v)(k) = 2 x the
     component cross spectra of u and the force (Compute_force_shell_spectrum,
     Correlation.cc:457-469).
-    flux.d (Output_flux): %%flux: U2U = Pi(R_i) (ts_flux) and %%sum(Fv.v) = the
+    flux.d (Output_flux): %%flux: U2U = Pi(R_i) (ts_flux, after dealiasing u in place
+    as the reference's Compute_flux does) and %%sum(Fv.v) = the
     power the force puts into the shells between consecutive radii, modes inside
     the inscribed sphere only (Shell_mult_all, universal_ET.cc:145-176).
     """
@@ -395,7 +396,14 @@ class Output:
         if self.plan.basis != "FFF":
             raise NotImplementedError("this output is written for FFF fluid runs")
         p = self.plan
-        Pi = p.flux(u, self.radii)
+        # Compute_flux runs Compute_nlin(U, Giver), which dealiases U in place
+        # (compute_nlin_ET_VF.cc:73-76): the run goes on from the dealiased state
+        p.dealias(u)
+        # spheres 1..no_spheres; the entry at radii[0] is never computed and stays 0
+        # (flux_self = 0.0, compute_flux.cc:55-64)
+        Pi = np.zeros(len(self.radii))
+        if len(self.radii) > 1:
+            Pi[1:] = p.flux(u, self.radii[1:])
         power = None
         if self.forced:
             F = self._force(u)

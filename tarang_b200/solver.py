@@ -148,8 +148,16 @@ class Plan:
         L.check(self.lib.ts_plan_set_stream(self.h, ctypes.c_void_p(s.cuda_stream)), "ts_plan_set_stream")
 
     def status(self):
-        """Synchronise the plan's stream; raise TsError if a bounded device wait gave up earlier."""
+        """Synchronise the plan's stream; raise TsError (status TS_ERR_TIMEOUT or TS_ERR_NAN) if a
+        bounded device wait gave up or a step wrote a NaN / Inf into the state earlier."""
         L.check(self.lib.ts_plan_status(self.h), "ts_plan_status")
+
+    def status_code(self) -> int:
+        """ts_plan_status without raising: TS_OK, TS_ERR_TIMEOUT or TS_ERR_NAN."""
+        return int(self.lib.ts_plan_status(self.h))
+
+    def clear_status(self):
+        L.check(self.lib.ts_plan_clear_status(self.h), "ts_plan_clear_status")
 
     # ------------------------------------------------------------------
     # launch tuning (candidate kernels per pass class; see ts_plan_autotune)
@@ -269,6 +277,12 @@ class Plan:
         L.check(self.lib.ts_force_field(self.h, _ptr(u), _ptr(out)), "ts_force_field")
         return out
 
+    def dealias(self, a, ncomp: int | None = None):
+        """Universal::Dealias in place (the plan's dealias mode)."""
+        n = a.shape[0] if ncomp is None else ncomp
+        L.check(self.lib.ts_dealias_field(self.h, _ptr(a), n), "ts_dealias_field")
+        return a
+
     def flux(self, u, radii) -> np.ndarray:
         r = np.ascontiguousarray(radii, dtype=np.float64)
         out = np.zeros(len(r))
@@ -371,6 +385,7 @@ class Ensemble:
                 arr[m].N[i] = int(N[i])
             arr[m].Ra, arr[m].Pr = float(Ra), float(Pr)
         self.members = [((N, N, N) if isinstance(N, int) else tuple(N), Ra, Pr) for N, Ra, Pr in members]
+        self.precision = precision
         h = ctypes.c_void_p()
         L.check(self.lib.ts_ensemble_create(ctypes.byref(c), arr, len(members), ctypes.byref(h)), "ts_ensemble_create")
         self.h = h
@@ -407,6 +422,13 @@ class Ensemble:
         L.check(self.lib.ts_ensemble_nusselt(self.h, out.ctypes.data_as(L._D)), "ts_ensemble_nusselt")
         return out
 
+    def health(self, clear: bool = False) -> np.ndarray:
+        """Per-member status after the steps so far: TS_OK, TS_ERR_NAN or TS_ERR_TIMEOUT."""
+        out = np.zeros(len(self.members), dtype=np.int32)
+        L.check(self.lib.ts_ensemble_health(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(clear)),
+                "ts_ensemble_health")
+        return out
+
     def tuning(self, m: int) -> dict:
         """launch tuning of the size group of member m"""
         t = L.TsTuning()
@@ -422,6 +444,23 @@ class Ensemble:
         buf = ctypes.create_string_buffer(1 << 18)
         L.check(self.lib.ts_ensemble_autotune(self.h, reps, buf, len(buf)), "ts_ensemble_autotune")
         return json.loads(buf.value.decode())
+
+    def view(self, m: int, which: str = "T"):
+        """A torch tensor viewing member m's device state in place: U (3, Nx, Ny, Nz/2+1) or
+        T (1, Nx, Ny, Nz/2+1), complex64 / complex128 by the ensemble's precision.  Call
+        synchronize() before reading it after run()."""
+        import torch
+        p, u, t = self.member(m)
+        Nx, Ny, Nz = self.members[m][0]
+        ncomp = 3 if which == "U" else 1
+        f64 = self.precision == "f64"
+
+        class _Dev:
+            pass
+        d = _Dev()
+        d.__cuda_array_interface__ = {"shape": (ncomp, Nx, Ny, Nz // 2 + 1), "typestr": "<c16" if f64 else "<c8",
+                                      "data": ((t if which == "T" else u).value, False), "version": 3}
+        return torch.as_tensor(d, device="cuda")
 
     def energy(self, m: int, which: str = "T") -> float:
         self.synchronize()  # ensemble steps run on the ensemble's own stream

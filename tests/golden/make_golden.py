@@ -3,7 +3,8 @@
 The reference ships no golden vectors (its tests are commented out), so these
 fixtures pin the oracle itself: a 16^3 FFF field from this project's seeded
 initial condition, one forced IF-RK4 step (reference-corner dealias), its
-shell spectrum and sphere fluxes.  The CPU tests check that the oracle still
+shell spectrum and sphere fluxes (the reference's per-sphere form,
+compute_flux.cc:51-65).  The CPU tests check that the oracle still
 reproduces them; the GPU tests check the CUDA path against them.
 Usage: python tests/golden/make_golden.py
 """
@@ -29,7 +30,7 @@ def compute():
                         forcing=R.CaratiForcing(CASE["f_in"], CASE["f_out"], es))
     V1 = R.rk4_step(cfg, V0)
     return dict(V0=V0, V1=V1, Ek1=R.shell_spectrum(g, V1), energy_supply=es,
-                Pi1=R.flux_one_pass(g, V1, CASE["radii"], R.DEALIAS_REFERENCE_CORNER),
+                Pi1=R.flux_per_sphere(g, V1, CASE["radii"], R.DEALIAS_REFERENCE_CORNER),
                 radii=np.array(CASE["radii"]))
 
 

@@ -180,8 +180,9 @@ def test_config0_plain_small(cuda):
             assert rel(to_np(u), W) < 1e-11
             assert rel(plan.shell_spectrum(u), R.shell_spectrum(g, W)) < 1e-11
             Pi = plan.flux(u, radii)
-            ref = R.flux_one_pass(g, W, radii, 1)
-            assert np.max(np.abs(Pi - ref)) < 1e-11
+            # the reference's per-sphere form (the configuration's corner-box dealiasing)
+            ref = R.flux_per_sphere(g, W, radii, 1)
+            assert np.max(np.abs(Pi - ref)) < 1e-11 * max(1.0, np.max(np.abs(ref)))
     assert plan.max_div(u) < 1e-12
 
 
@@ -258,6 +259,63 @@ def test_bitwise_reproducible(cuda, prec):
     assert outs[0][0] == outs[1][0]
     assert torch.equal(outs[0][1], outs[1][1])
     assert outs[0][2] == outs[1][2]
+
+
+@pytest.mark.parametrize("dealias", ["two_thirds", "reference"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_shell_and_flux_sums_bitwise_reproducible(cuda, prec, dealias):
+    """E(k), the raw shell sums and Pi(R) are added in a fixed order (no atomics on the sums):
+    repeated calls, and fresh plans, give the same bits."""
+    import torch
+    radii = [0.0, 2.0, 4.0, 8.0, 12.0, 1e9]
+    res = []
+    for _ in range(2):
+        plan = plan_for(64, precision=prec, dealias=dealias)
+        u = plan.field(3)
+        plan.init_energy_spectrum(R.spectrum_k4_gauss(plan.n_shells, 6.0), 11, 0.5, u)
+        for _ in range(3):
+            res.append((plan.shell_spectrum(u), plan.shell_sums(u)[0], plan.flux(u, radii)))
+        plan.close()
+        torch.cuda.empty_cache()
+    for r in res[1:]:
+        for a, b in zip(res[0], r):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("N,k0", [(32, 8.0), ((32, 16, 64), 4.0)])
+@pytest.mark.parametrize("mode", [1, 0])
+def test_flux_per_sphere_matches_oracle(cuda, N, k0, mode):
+    """Pi(R) under the reference's corner-box dealiasing (and none) is the per-sphere algorithm of
+    EnergyTr::Compute_flux (compute_flux.cc:51-65): one giver nonlinear term per sphere.  There the
+    one-pass form differs from it by the aliased part of the products (about 8 % of max|Pi| at
+    32^3, k0 = 8), so the test also checks that the GPU result is not the one-pass value."""
+    import torch
+    g, V = oracle_ic(N, k0=k0, seed=3)
+    radii = [0.0, 2.0, 4.0, 8.0, 12.0, 1e9]
+    ref = R.flux_per_sphere(g, V, radii, mode)
+    one = R.flux_one_pass(g, V, radii, mode)
+    scale = np.max(np.abs(ref))
+    dl = {1: "reference", 0: "none"}[mode]
+    for prec, tol in (("f64", 1e-12), ("f32", 2e-6)):
+        plan = plan_for(N, precision=prec, dealias=dl)
+        dt = torch.complex128 if prec == "f64" else torch.complex64
+        u = torch.from_numpy(V.copy()).to(cuda).to(dt)
+        Pi = plan.flux(u, radii)
+        assert np.max(np.abs(Pi - ref)) < tol * scale, (prec, Pi, ref)
+        # the state is not modified by the diagnostic
+        assert torch.equal(u, torch.from_numpy(V.copy()).to(cuda).to(dt))
+        plan.close()
+    if mode == 1 and N == 32:
+        assert np.max(np.abs(one - ref)) > 0.05 * scale
+
+
+def test_flux_radii_limit(cuda):
+    """At most 63 radii: more are refused with TS_ERR_ARG, not truncated."""
+    plan = plan_for(16, precision="f64", dealias="two_thirds")
+    u = plan.field(3)
+    with pytest.raises(RuntimeError):
+        plan.flux(u, np.arange(64, dtype=np.float64))
+    assert len(plan.flux(u, np.arange(63, dtype=np.float64))) == 63
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])

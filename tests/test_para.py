@@ -244,7 +244,12 @@ def test_output_spectrum_and_flux_match_oracle(cuda, tmp_path):
         ref_f = 2 * np.where(cnt > 0, cr * 4 * np.pi / np.where(cnt > 0, cnt, 1), 0.0)
         assert np.allclose(fv[i], ref_f, rtol=2e-5, atol=1e-6 * np.abs(ref_f).max())
     flux = _read_blocks(tmp_path / "flux.d", "flux: U2U ")[0][0]
-    assert np.allclose(flux, R.flux_one_pass(g, V, rp.flux_radii, 1), rtol=2e-5, atol=1e-9)
+    # the reference's per-sphere algorithm (corner-box dealiasing), with radii[0] never computed
+    ref_pi = R.flux_per_sphere(g, V, rp.flux_radii, 1)
+    ref_pi[0] = 0.0
+    assert np.allclose(flux, ref_pi, rtol=1e-10, atol=1e-12 * np.max(np.abs(ref_pi)))
+    # Compute_flux dealiases U in place, and so does the output
+    assert np.array_equal(u.cpu().numpy(), R.dealias(g, V, 1))
     power = _read_blocks(tmp_path / "flux.d", "sum(Fv.v)")[0][0]
     dot = 2 * mult * np.sum((F * np.conj(V)).real, axis=0)
     ins = Kmag <= kin
