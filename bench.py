@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 comparison, e2e and CPU baseline legs")
     ap.add_argument("--workload", default="fff256",
                     choices=["fff256", "ensemble", "fff1024", "rbc", "adjoint", "scalar", "mhd", "ssf", "sss",
-                             "rbc_ssf", "rbc_sss"],
+                             "rbc_ssf", "rbc_sss", "c1_trajectory", "c2_error"],
                     help="fff256: forced 256^3 (default headline); ensemble: 64 RBC members; fff1024: decaying "
                          "1024^3 (or --shape); rbc: one RBC run (SFF, --N, FP32); adjoint: adjoint/forward cost at 128^3")
     ap.add_argument("--tune", default="auto", choices=["auto", "off"],
@@ -142,6 +142,91 @@ def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024), prec:
     del u
     torch.cuda.empty_cache()
     return out
+
+
+def c1_trajectory_leg(steps: int = 2000, every: int = 10, N: int = 256, form: str = "rotational"):
+    """Config 1's error report: FP32 and FP64 GPU runs of the forced 256^3 workload (same IC,
+    same nonlinear form) advanced side by side; every `every` steps the relative L2 difference
+    of the velocity fields, the relative energy difference and max |div u| of each run.  The
+    FP64 run is the reference the FP32 path is held to (rel err <= 1e-5); forced turbulence
+    is chaotic, so the difference grows with time, and the report says where it crosses 1e-5."""
+    import torch
+    import tarang_b200 as tb
+    nsh = int(math.ceil(math.sqrt(3) * (N // 2))) + 1
+    forcing = tb.Forcing(2.0, 3.0, energy_supply(nsh))
+    kw = dict(nlin_form=form, dealias="two_thirds", nu=1e-3, dt=5e-4, forcing=forcing)
+    p32, p64 = tb.Plan(N, precision="f32", **kw), tb.Plan(N, precision="f64", **kw)
+    st = torch.cuda.current_stream()
+    p32.set_stream(st)
+    p64.set_stream(st)
+    u64 = p64.field(3)
+    p64.init_energy_spectrum(tb.spectrum_k4_gauss(p64.n_shells, 4.0), 0, 0.5, u64)
+    u32 = u64.to(torch.complex64)
+    rows = []
+    t0 = time.perf_counter()
+    for s in range(1, steps + 1):
+        p32.rk4_step(u32, 1)
+        p64.rk4_step(u64, 1)
+        if s % every == 0 or s == 1:
+            d = float(torch.linalg.vector_norm(u32.to(torch.complex128) - u64) / torch.linalg.vector_norm(u64))
+            e32, e64 = p32.energy(u32), p64.energy(u64)
+            rows.append([s, d, abs(e32 - e64) / e64, p32.max_div(u32), p64.max_div(u64), e64])
+    p32.status()
+    p64.status()
+    wall = time.perf_counter() - t0
+    first = next((r[0] for r in rows if r[1] > 1e-5), None)
+    first_e = next((r[0] for r in rows if r[2] > 1e-5), None)
+    out = {"steps": steps, "every": every, "N": N, "form": form,
+           "columns": ["step", "rel_l2_u", "rel_energy", "max_div_f32", "max_div_f64", "energy_f64"],
+           "series": rows, "first_step_rel_l2_above_1e-5": first, "first_step_rel_energy_above_1e-5": first_e,
+           "final": dict(zip(["step", "rel_l2_u", "rel_energy", "max_div_f32", "max_div_f64", "energy_f64"], rows[-1])),
+           "max_div_f32_max": max(r[3] for r in rows), "wall_s": wall}
+    p32.close()
+    p64.close()
+    del u32, u64
+    torch.cuda.empty_cache()
+    return out
+
+
+def c2_error_leg(steps: int = 200, every: int = 10, shape=(1024, 1024, 1024)):
+    """Config 2's error report: the 1024^3 decaying run (rotational, two-thirds, nu = 2e-4,
+    dt = 2e-4, IC k^4 exp(-2 (k/8)^2), E = 0.5) in FP32 and then in FP64 (the two do not fit
+    on one GPU together: the FP32 state waits in host memory), energies every `every` steps
+    and, at the end, the relative L2 difference of the velocity fields."""
+    import torch
+    import tarang_b200 as tb
+    kw = dict(nlin_form="rotational", dealias="two_thirds", nu=2e-4, dt=2e-4)
+    energies = {}
+    final32 = None
+    for prec in ("f32", "f64"):
+        plan = tb.Plan(tuple(shape), precision=prec, **kw)
+        plan.set_stream(torch.cuda.current_stream())
+        u = plan.field(3)
+        plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 8.0), 0, 0.5, u)
+        es = [[0, plan.energy(u)]]
+        t0 = time.perf_counter()
+        for s in range(1, steps + 1):
+            plan.rk4_step(u, 1)
+            if s % every == 0:
+                es.append([s, plan.energy(u)])
+        plan.status()
+        energies[prec] = {"series": es, "wall_s": time.perf_counter() - t0, "max_div": plan.max_div(u)}
+        if prec == "f32":
+            final32 = u.cpu()
+            plan.close()
+            del u
+            torch.cuda.empty_cache()
+        else:
+            num = 0.0
+            for c in range(3):
+                num += float(torch.linalg.vector_norm(final32[c].to("cuda").to(torch.complex128) - u[c]) ** 2)
+            rel_l2 = math.sqrt(num) / float(torch.linalg.vector_norm(u))
+            plan.close()
+            del u
+            torch.cuda.empty_cache()
+    rel_e = [[a[0], abs(a[1] - b[1]) / b[1]] for a, b in zip(energies["f32"]["series"], energies["f64"]["series"])]
+    return {"steps": steps, "shape": list(shape), "rel_l2_u_final": rel_l2, "rel_energy": rel_e,
+            "max_rel_energy": max(r[1] for r in rel_e), "energies": energies}
 
 
 def ensemble_plain_fp64_leg(steps: int = 3, warmup: int = 1):
@@ -554,6 +639,18 @@ def alt_workload(args, world, rank, local, dev):
                 "roofline": {"bound": "hbm", "model_frac": r["model_frac"], "kernels": r["kernels"]},
                 "nusselt": r["nusselt"]}
         line["config"]["tuning"] = r["tuning"]
+    elif args.workload in ("c1_trajectory", "c2_error"):
+        if args.workload == "c1_trajectory":
+            r = c1_trajectory_leg(steps=args.steps if args.steps != 30 else 2000)
+            what = "FP32 vs FP64 GPU, FFF 256^3 forced, rel L2 of u after the run"
+            v = r["final"]["rel_l2_u"]
+        else:
+            r = c2_error_leg(steps=args.steps if args.steps != 30 else 200)
+            what = "FP32 vs FP64 GPU, FFF 1024^3 decaying, rel L2 of u after the run"
+            v = r["rel_l2_u_final"]
+        line = {"metric": what, "value": v, "unit": "relative L2", "n_gpus": 1, "steps": r["steps"],
+                "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 vs f64", "data": "synthetic", "config": {"workload": args.workload}, "detail": r}
     elif args.workload == "adjoint":
         r = {"f64": adjoint_leg("f64"), "f32": adjoint_leg("f32")}
         line = {"metric": "adjoint step / forward step cost, FFF 128^3 rotational (config 4)",

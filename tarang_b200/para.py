@@ -67,6 +67,7 @@ class RunParams:
     force_outer: float | None = None
     force_global_alpha_beta: bool = False
     flux_radii: list = field(default_factory=list)
+    input_field_procedure: int = 5   # io.input_field_procedure (1: read complex fields from in/)
 
     @property
     def nsteps(self) -> int:
@@ -183,6 +184,9 @@ def read_para(path: str) -> RunParams:
             rp.force_inner, rp.force_outer = float(words[2]), float(words[3])
             if rp.force_global_alpha_beta:
                 raise NotImplementedError("ENERGY_SUPPLY with global_alpha_beta = 1: the non-global branch only")
+    io = p.get("io") or {}
+    if io.get("input_field_procedure") is not None:
+        rp.input_field_procedure = int(io["input_field_procedure"])
     et = p.get("energy_transfer") or {}
     fl = et.get("flux") or {}
     if _flag(et.get("turnon", False)) and _flag(fl.get("turnon", False)):
@@ -238,6 +242,102 @@ def advance(plan, kind: str, fields, nsteps: int = 1):
         plan.rk4_step_mhd(fields[0], fields[1], nsteps)
     else:
         raise NotImplementedError(f"program.kind {kind}")
+
+
+# ----------------------------------------------------------------------------
+# complex-field checkpoints (restart)
+# ----------------------------------------------------------------------------
+STATE_FORMAT = "tarang_b200 spectral state 1"
+
+
+def field_layout(kind: str) -> list:
+    """(field name, component names) of the fields a run of this kind advances, named as the
+    reference names its complex-field datasets (CVF::Write_complex_field Cvf.cc:494-508:
+    U.V1, U.V2, U.V3; a scalar field's F: T.F; the second vector field of MHD: W.V1..V3)."""
+    if kind == "FLUID_INCOMPRESS":
+        return [("U", ("V1", "V2", "V3"))]
+    if kind in ("RBC", "SCALAR_INCOMPRESS"):
+        return [("U", ("V1", "V2", "V3")), ("T", ("F",))]
+    if kind == "MHD_INCOMPRESS":
+        return [("U", ("V1", "V2", "V3")), ("W", ("V1", "V2", "V3"))]
+    raise NotImplementedError(f"program.kind {kind}")
+
+
+def save_state(folder: str, plan, kind: str, fields, t: float, step: int = 0) -> str:
+    """Write the state of a run (the fields of ``advance``) as one raw little-endian file per
+    component, ``<name>.<comp>.bin`` (the component's spectral array, C order, the plan's
+    precision: complex (Nx, Ny, Nz/2+1), or on SSS the real coefficients in the padded
+    (Nx, Ny, Nz+2) layout), plus ``state.json`` (format, kind, basis, N, kfactor, precision,
+    dt, t, step, files).  The reference writes the same components as HDF5 datasets into
+    out/time_<t>/ (Cvf.cc:494-508); no HDF5 library is used here."""
+    import json
+    os.makedirs(folder, exist_ok=True)
+    layout = field_layout(kind)
+    if len(fields) != len(layout):
+        raise ValueError(f"{kind} has {len(layout)} field(s), got {len(fields)}")
+    files = []
+    for (name, comps), f in zip(layout, fields):
+        if f.shape[0] != len(comps):
+            raise ValueError(f"field {name}: {len(comps)} components expected, got {f.shape[0]}")
+        host = f.detach().to("cpu").contiguous().numpy()
+        for c, cn in enumerate(comps):
+            fn = f"{name}.{cn}.bin"
+            np.ascontiguousarray(host[c]).astype(host.dtype.newbyteorder("<"), copy=False).tofile(
+                os.path.join(folder, fn))
+            files.append({"field": name, "component": cn, "file": fn, "shape": list(host.shape[1:]),
+                          "dtype": str(host.dtype)})
+    cfg = plan.cfg
+    head = {"format": STATE_FORMAT, "kind": kind, "basis": plan.basis, "N": list(plan.N),
+            "kfactor": [float(cfg.kfactor[i]) for i in range(3)],
+            "precision": "f64" if fields[0].dtype.itemsize == 16 else "f32",
+            "dt": float(cfg.dt), "t": float(t), "step": int(step), "files": files}
+    with open(os.path.join(folder, "state.json"), "w") as fh:
+        json.dump(head, fh, indent=1)
+    return folder
+
+
+def load_state(folder: str, plan, kind: str, device: str = "cuda"):
+    """(fields, t, step) from a folder written by ``save_state``: device tensors in the plan's
+    precision (an FP64 state is rounded once for an FP32 plan).  The geometry, basis and kind
+    must match the plan's, else ValueError (Read_complex_field reads into the run's own
+    arrays, which fixes their shape)."""
+    import json
+    import torch
+    with open(os.path.join(folder, "state.json")) as fh:
+        head = json.load(fh)
+    if head.get("format") != STATE_FORMAT:
+        raise ValueError(f"{folder}: not a {STATE_FORMAT!r} folder")
+    if head["kind"] != kind or head["basis"] != plan.basis or tuple(head["N"]) != tuple(plan.N):
+        raise ValueError(f"{folder}: state of {head['kind']} on {head['basis']} {head['N']}, "
+                         f"run is {kind} on {plan.basis} {list(plan.N)}")
+    kf = [float(plan.cfg.kfactor[i]) for i in range(3)]
+    if any(abs(a - b) > 1e-12 * max(1.0, abs(b)) for a, b in zip(head["kfactor"], kf)):
+        raise ValueError(f"{folder}: kfactor {head['kfactor']} differs from the run's {kf}")
+    by = {(f["field"], f["component"]): f for f in head["files"]}
+    want = torch.complex64 if plan.precision == "f32" else torch.complex128
+    out = []
+    for name, comps in field_layout(kind):
+        arrs = []
+        for cn in comps:
+            f = by.get((name, cn))
+            if f is None:
+                raise ValueError(f"{folder}: {name}.{cn} missing")
+            a = np.fromfile(os.path.join(folder, f["file"]), dtype=np.dtype(f["dtype"]).newbyteorder("<"))
+            arrs.append(a.reshape(f["shape"]))
+        t = torch.from_numpy(np.stack(arrs)).to(want).to(device)
+        out.append(t.contiguous())
+    return out, float(head["t"]), int(head["step"])
+
+
+def read_init_cond(data_dir: str, plan, rp: RunParams):
+    """FluidIO::Read_init_cond for ``io.input_field_procedure: 1`` (init_cond_main.cc:48-56,
+    Init_cond_complex_field init_cond_field.cc:49-58): the run's complex fields from
+    ``<data_dir>/in/`` as ``save_state`` writes them.  Returns (fields, t, step); the run
+    continues from time t.  Other procedures are refused by name."""
+    if rp.input_field_procedure != 1:
+        raise NotImplementedError(f"io.input_field_procedure {rp.input_field_procedure}: "
+                                  "1 (complex fields from in/) only; seeded spectra use Plan.init_energy_spectrum")
+    return load_state(os.path.join(data_dir, "in"), plan, rp.kind)
 
 
 # ----------------------------------------------------------------------------
@@ -316,6 +416,11 @@ class Output:
                             else sff_max_radius_inside(plan.N, self.kf))
         self.radii = list(radii) if radii is not None else default_flux_radii(8, self.kmax_inside)
         self.forced = plan.cfg.force_type != 0
+
+    def save(self, kind: str, fields, t: float, step: int = 0) -> str:
+        """The run's complex fields into out/time_<t>/ (CVF::Write_complex_field, Cvf.cc:494-508,
+        folder "time_" + time.now) in ``save_state``'s format; ``read_init_cond`` restarts from it."""
+        return save_state(os.path.join(self.out_dir, f"time_{t:g}"), self.plan, kind, fields, t, step)
 
     def _force(self, u):
         return self.plan.force_field(u, self.plan.field(3)) if self.forced else None

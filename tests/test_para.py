@@ -247,7 +247,8 @@ def test_output_spectrum_and_flux_match_oracle(cuda, tmp_path):
     # the reference's per-sphere algorithm (corner-box dealiasing), with radii[0] never computed
     ref_pi = R.flux_per_sphere(g, V, rp.flux_radii, 1)
     ref_pi[0] = 0.0
-    assert np.allclose(flux, ref_pi, rtol=1e-10, atol=1e-12 * np.max(np.abs(ref_pi)))
+    # flux.d holds %g values (six significant digits, Print_array)
+    assert np.allclose(flux, ref_pi, rtol=2e-5, atol=1e-9)
     # Compute_flux dealiases U in place, and so does the output
     assert np.array_equal(u.cpu().numpy(), R.dealias(g, V, 1))
     power = _read_blocks(tmp_path / "flux.d", "sum(Fv.v)")[0][0]
@@ -436,3 +437,119 @@ def test_output_glob_mhd_matches_oracle(cuda, tmp_path):
     assert len(row) == 29
     for i, (a, b) in enumerate(zip(row, want)):
         assert abs(a - b) <= max(1e-10 * abs(b), 1e-12), (i, a, b)
+
+
+# ---------------------------------------------------------------------------
+# restart: complex-field checkpoints (Cvf.cc:494-528) and input_field_procedure 1
+# ---------------------------------------------------------------------------
+def _fake_plan(N=(16, 8, 12), basis="FFF", precision="f64", kf=(1.0, 2.0, 1.0)):
+    from types import SimpleNamespace
+    return SimpleNamespace(N=N, basis=basis, precision=precision,
+                           cfg=SimpleNamespace(kfactor=list(kf), dt=1e-3))
+
+
+@pytest.mark.parametrize("kind", ["FLUID_INCOMPRESS", "RBC", "MHD_INCOMPRESS"])
+def test_state_round_trip_bit_exact(tmp_path, kind):
+    """save_state -> load_state returns the same bits; one raw file per component named as the
+    reference's datasets (U.V1 ... T.F, W.V1 ...), plus the JSON header."""
+    import json
+    import torch
+    plan = _fake_plan()
+    g = torch.Generator().manual_seed(5)
+    shape = (16, 8, 7)
+    fields = [torch.complex(torch.randn((len(c),) + shape, generator=g, dtype=torch.float64),
+                            torch.randn((len(c),) + shape, generator=g, dtype=torch.float64))
+              for _, c in para.field_layout(kind)]
+    para.save_state(str(tmp_path / "s"), plan, kind, fields, 0.25, 250)
+    head = json.load(open(tmp_path / "s" / "state.json"))
+    assert head["t"] == 0.25 and head["step"] == 250 and head["N"] == [16, 8, 12] and head["precision"] == "f64"
+    names = sorted(f["file"] for f in head["files"])
+    want = {"FLUID_INCOMPRESS": ["U.V1.bin", "U.V2.bin", "U.V3.bin"],
+            "RBC": ["T.F.bin", "U.V1.bin", "U.V2.bin", "U.V3.bin"],
+            "MHD_INCOMPRESS": ["U.V1.bin", "U.V2.bin", "U.V3.bin", "W.V1.bin", "W.V2.bin", "W.V3.bin"]}[kind]
+    assert names == want
+    # component files hold the component's C-order array, little endian
+    raw = np.fromfile(tmp_path / "s" / "U.V2.bin", dtype="<c16").reshape(shape)
+    assert np.array_equal(raw, fields[0][1].numpy())
+    back, t, step = para.load_state(str(tmp_path / "s"), plan, kind, device="cpu")
+    assert (t, step) == (0.25, 250)
+    for a, b in zip(back, fields):
+        assert torch.equal(a, b)
+    # an FP64 state into an FP32 run is rounded once
+    back32, _, _ = para.load_state(str(tmp_path / "s"), _fake_plan(precision="f32"), kind, device="cpu")
+    assert torch.equal(back32[0], fields[0].to(torch.complex64))
+
+
+def test_state_refuses_other_geometry_and_kind(tmp_path):
+    import torch
+    plan = _fake_plan()
+    u = torch.zeros((3, 16, 8, 7), dtype=torch.complex128)
+    para.save_state(str(tmp_path / "s"), plan, "FLUID_INCOMPRESS", [u], 0.0)
+    with pytest.raises(ValueError):
+        para.load_state(str(tmp_path / "s"), _fake_plan(N=(16, 8, 16)), "FLUID_INCOMPRESS", device="cpu")
+    with pytest.raises(ValueError):
+        para.load_state(str(tmp_path / "s"), plan, "RBC", device="cpu")
+    with pytest.raises(ValueError):
+        para.load_state(str(tmp_path / "s"), _fake_plan(kf=(1.0, 1.0, 1.0)), "FLUID_INCOMPRESS", device="cpu")
+    with pytest.raises(ValueError):
+        para.save_state(str(tmp_path / "t"), plan, "RBC", [u], 0.0)
+
+
+def test_read_para_input_field_procedure(tmp_path):
+    text = open(os.path.join(FFF_DIR, "in", "para.yaml")).read()
+    assert para.read_para(os.path.join(FFF_DIR, "in", "para.yaml")).input_field_procedure == 5
+    (tmp_path / "in").mkdir()
+    (tmp_path / "in" / "para.yaml").write_text(text.replace("io:\n", "io:\n    input_field_procedure: 1\n"))
+    rp = para.read_para(str(tmp_path / "in" / "para.yaml"))
+    assert rp.input_field_procedure == 1
+    rp.input_field_procedure = 4
+    with pytest.raises(NotImplementedError):
+        para.read_init_cond(str(tmp_path), None, rp)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("name", ["fff", "rbc"])
+def test_restart_continues_bit_for_bit(cuda, tmp_path, name, precision):
+    """Save after 2 steps into out/time_<t>/, restart a second run from it through
+    input_field_procedure 1 (the saved folder as the new run's in/), step 2 more: the state equals
+    4 unbroken steps bit for bit."""
+    import shutil
+    import torch
+    from oracle import tarang_ref as R
+    src = FFF_DIR if name == "fff" else RBC_DIR
+    plan, rp = para.plan_from_dir(src, precision=precision)
+    if name == "fff":
+        g = R.Grid(rp.N, rp.kfactor)
+        V = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
+        fields = [torch.from_numpy(V).to(cuda).to(plan.torch_dtype())]
+    else:
+        u, T = plan.field(3), plan.field(1)
+        plan.init_temperature_perturbation(1e-2, 4.0, 3, T)
+        fields = [u, T]
+    ref = [f.clone() for f in fields]
+    para.advance(plan, rp.kind, ref, 4)
+    para.advance(plan, rp.kind, fields, 2)
+    out = para.Output(plan, str(tmp_path / "run1" / "out"))
+    folder = out.save(rp.kind, fields, rp.t_init + 2 * rp.dt, 2)
+    assert os.path.basename(folder) == f"time_{rp.t_init + 2 * rp.dt:g}"
+    # the second run: its in/ holds the para.yaml (input_field_procedure 1) and the saved fields
+    run2 = tmp_path / "run2"
+    shutil.copytree(folder, run2 / "in")
+    text = open(os.path.join(src, "in", "para.yaml")).read()
+    if "io:\n" in text:
+        text = text.replace("io:\n", "io:\n    input_field_procedure: 1\n")
+    else:
+        text += "\nio:\n    input_field_procedure: 1\n"
+    (run2 / "in" / "para.yaml").write_text(text)
+    for extra in ("forcing.txt",):
+        if os.path.exists(os.path.join(src, "in", extra)):
+            shutil.copy(os.path.join(src, "in", extra), run2 / "in" / extra)
+    plan2, rp2 = para.plan_from_dir(str(run2), precision=precision)
+    assert rp2.input_field_procedure == 1
+    fields2, t, step = para.read_init_cond(str(run2), plan2, rp2)
+    assert step == 2 and abs(t - (rp.t_init + 2 * rp.dt)) < 1e-15
+    para.advance(plan2, rp2.kind, fields2, 2)
+    torch.cuda.synchronize()
+    for a, b in zip(fields2, ref):
+        assert torch.equal(a, b)
