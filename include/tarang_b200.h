@@ -60,6 +60,12 @@ typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
 typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;
 typedef enum { TS_DEALIAS_NONE = 0, TS_DEALIAS_REFERENCE_CORNER = 1, TS_DEALIAS_TWO_THIRDS = 2 } ts_dealias;
 typedef enum { TS_FORCE_NONE = 0, TS_FORCE_CARATI_ENERGY_SUPPLY = 1, TS_FORCE_RBC = 51 } ts_force;
+/* PHYSICS.Pr_option and PHYSICS.Uscaling of an RBC run (Global_read.cc; the
+ * coefficients of compute_force_RBC.cc:104-150 and Correlation.cc:144-176).  PRZERO and
+ * PRINFTY (one field slaved to the other, Tadvance_functions.cc:380-395) are refused
+ * with TS_ERR_UNSUPPORTED. */
+typedef enum { TS_PR_LARGE = 0, TS_PR_SMALL = 1, TS_PR_ZERO = 2, TS_PR_INFTY = 3 } ts_pr_option;
+typedef enum { TS_U_LARGE = 0, TS_U_SMALL = 1 } ts_uscaling;
 
 /* Solver configuration.  Field names follow the reference's para.yaml keys
  * where one exists (global/Global.h:65-259). */
@@ -79,7 +85,9 @@ typedef struct {
   const double* energy_supply;   /* per shell ceil|K| (in/forcing.txt), copied at create */
   const double* helicity_supply; /* may be NULL */
   int n_supply;
-  double Ra, Pr;        /* PHYSICS.Rayleigh, PHYSICS.Prandtl (RBC, PRLARGE / ULARGE) */
+  double Ra, Pr;        /* PHYSICS.Rayleigh, PHYSICS.Prandtl (RBC) */
+  int Pr_option;        /* ts_pr_option (RBC; default PRLARGE) */
+  int Uscaling;         /* ts_uscaling (RBC; default ULARGE) */
 } ts_config;
 
 typedef struct ts_plan ts_plan;

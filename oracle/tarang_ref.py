@@ -820,8 +820,30 @@ def init_energy_spectrum(g: Grid, E_ic: np.ndarray, seed: int, target_energy: fl
 
 
 # ----------------------------------------------------------------------------
-# Boussinesq RBC on SFF, SSF and SSS (PRLARGE, ULARGE)
+# Boussinesq RBC on SFF, SSF and SSS (Pr_option PRLARGE / PRSMALL, Uscaling ULARGE / USMALL)
 # ----------------------------------------------------------------------------
+def rbc_coefficients(pr_option: str, uscaling: str, Ra: float, Pr: float) -> dict:
+    """The scaling-dependent coefficients of an RBC run (non-Chebyshev bases):
+
+    * nu, kappa: diss_coefficients (src/solvers/iscalar/Iscalar_main.cc:52-92);
+    * cu, cT: U.Force1 += cu T and T.Force += cT U.V1 (compute_force_RBC.cc:104-150);
+    * nu0, nuc: Nu = nu0 + nuc <U.V1, T> (Correlation::Get_Nusselt_no, Correlation.cc:144-176).
+
+    PRZERO (T slaved to U) and PRINFTY (U slaved to T) change the step itself
+    (Single_time_step_RBC, Tadvance_functions.cc:380-395) and are not restated here."""
+    if pr_option == "PRLARGE":
+        if uscaling == "USMALL":
+            return dict(nu=Pr, kappa=1.0, cu=Ra * Pr, cT=1.0, nu0=1.0, nuc=2.0)
+        return dict(nu=math.sqrt(Pr / Ra), kappa=1.0 / math.sqrt(Pr * Ra), cu=1.0, cT=1.0, nu0=1.0,
+                    nuc=2.0 * math.sqrt(Ra * Pr))
+    if pr_option == "PRSMALL":
+        if uscaling == "USMALL":
+            return dict(nu=1.0, kappa=1.0 / Pr, cu=Ra, cT=1.0 / Pr, nu0=1.0, nuc=2.0 * Pr ** 2)
+        return dict(nu=math.sqrt(Pr / Ra), kappa=1.0 / math.sqrt(Pr * Ra), cu=Pr, cT=1.0 / Pr, nu0=1.0,
+                    nuc=2.0 * Pr * math.sqrt(Ra * Pr))
+    raise NotImplementedError(f"Pr_option {pr_option}: PRLARGE and PRSMALL are restated")
+
+
 @dataclass
 class RBCConfig:
     grid: Grid
@@ -830,14 +852,20 @@ class RBCConfig:
     dt: float
     dealias_mode: int = DEALIAS_REFERENCE_CORNER
     reality_fix: bool = True
+    pr_option: str = "PRLARGE"
+    uscaling: str = "ULARGE"
+
+    @property
+    def coeffs(self):
+        return rbc_coefficients(self.pr_option, self.uscaling, self.Ra, self.Pr)
 
     @property
     def nu(self):
-        return math.sqrt(self.Pr / self.Ra)      # Iscalar_main.cc ULARGE
+        return self.coeffs["nu"]
 
     @property
     def kappa(self):
-        return 1.0 / math.sqrt(self.Pr * self.Ra)
+        return self.coeffs["kappa"]
 
 
 @dataclass
@@ -864,8 +892,9 @@ def rbc_rhs(cfg, U: np.ndarray, T: np.ndarray) -> tuple:
     """
     g = cfg.grid
     buoyancy = getattr(cfg, "buoyancy", True)
-    FU1 = T.copy() if buoyancy else np.zeros_like(T)
-    FT = U[0].copy() if buoyancy else np.zeros_like(T)
+    co = cfg.coeffs if buoyancy else None
+    FU1 = co["cu"] * T if buoyancy else np.zeros_like(T)
+    FT = co["cT"] * U[0] if buoyancy else np.zeros_like(T)
     Ud = dealias(g, U, cfg.dealias_mode)
     Td = dealias(g, T, cfg.dealias_mode)
     ur = velocity_real(g, Ud)
@@ -997,8 +1026,10 @@ def mhd_rk4_step(cfg: MHDConfig, U0: np.ndarray, B0: np.ndarray) -> tuple:
 
 
 def nusselt(cfg: RBCConfig, U: np.ndarray, T: np.ndarray) -> float:
-    """Get_Nusselt_no PRLARGE/ULARGE (Correlation.cc:154-156): 1 + 2 sqrt(Ra Pr) <U1, T>."""
-    return 1.0 + 2.0 * math.sqrt(cfg.Ra * cfg.Pr) * cross_energy(cfg.grid, U[0], T)
+    """Get_Nusselt_no (Correlation.cc:144-176): nu0 + nuc <U1, T> with the scaling's factors
+    (PRLARGE / ULARGE: 1 + 2 sqrt(Ra Pr) <U1, T>)."""
+    co = cfg.coeffs
+    return co["nu0"] + co["nuc"] * cross_energy(cfg.grid, U[0], T)
 
 
 def rbc_temperature_ic(g: Grid, amp: float, kmax_grid: float, seed: int) -> np.ndarray:

@@ -12,6 +12,8 @@ from pathlib import Path
 _LIB_PATH = Path(__file__).resolve().parent / "libtarang_b200.so"
 
 TS_OK, TS_ERR_ARG, TS_ERR_CUDA, TS_ERR_NAN, TS_ERR_TIMEOUT, TS_ERR_UNSUPPORTED, TS_ERR_NOMEM = range(7)
+TS_PR_LARGE, TS_PR_SMALL, TS_PR_ZERO, TS_PR_INFTY = range(4)
+TS_U_LARGE, TS_U_SMALL = range(2)
 STATUS_NAMES = {0: "TS_OK", 1: "TS_ERR_ARG", 2: "TS_ERR_CUDA", 3: "TS_ERR_NAN", 4: "TS_ERR_TIMEOUT",
                 5: "TS_ERR_UNSUPPORTED", 6: "TS_ERR_NOMEM"}
 TS_BASIS_FFF, TS_BASIS_SFF, TS_BASIS_SSF, TS_BASIS_SSS = 0, 1, 2, 3
@@ -53,6 +55,8 @@ class TsConfig(ctypes.Structure):
         ("n_supply", ctypes.c_int),
         ("Ra", ctypes.c_double),
         ("Pr", ctypes.c_double),
+        ("Pr_option", ctypes.c_int),
+        ("Uscaling", ctypes.c_int),
     ]
 
 

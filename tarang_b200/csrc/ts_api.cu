@@ -68,6 +68,8 @@ struct ts_plan {
   void* stage_b = nullptr;  // staging for host pointers (3 components, the MHD field B)
   int* err_d = nullptr;     // device error word (bounded waits that gave up)
   int* err_h = nullptr;     // pinned copy, refreshed after every step call
+  double rbc_cu = 1, rbc_cT = 1;    // RBC buoyancy coefficients U.F1 = cu T, T.F = cT U.V1
+  double rbc_nu0 = 1, rbc_nuc = 0;  // Nusselt number nu0 + nuc <U.V1, T>
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
   double* eaxT[3] = {nullptr, nullptr, nullptr}; // per-axis exp(-kappa dt K_i^2 / 2) (SFF scalar)
   void* twq = nullptr;      // SFF, SSF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
@@ -147,6 +149,40 @@ struct ProfScope {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+// Scaling-dependent RBC coefficients (non-Chebyshev bases): diss_coefficients nu, kappa
+// (Iscalar_main.cc:52-92), buoyancy U.Force1 += cu T, T.Force += cT U.V1
+// (compute_force_RBC.cc:104-150) and the Nusselt number nu0 + nuc <U.V1, T>
+// (Correlation::Get_Nusselt_no, Correlation.cc:144-176).  PRZERO / PRINFTY slave one
+// field to the other (Single_time_step_RBC, Tadvance_functions.cc:380-395): refused.
+static int rbc_coefficients(int pr_option, int uscaling, double Ra, double Pr, double* nu, double* kappa, double* cu,
+                            double* cT, double* nu0, double* nuc) {
+  if (uscaling != TS_U_LARGE && uscaling != TS_U_SMALL) return TS_ERR_ARG;
+  const bool small = uscaling == TS_U_SMALL;
+  if (pr_option == TS_PR_LARGE) {
+    *nu = small ? Pr : sqrt(Pr / Ra);
+    *kappa = small ? 1.0 : 1.0 / sqrt(Pr * Ra);
+    *cu = small ? Ra * Pr : 1.0;
+    *cT = 1.0;
+    *nu0 = 1.0;
+    *nuc = small ? 2.0 : 2.0 * sqrt(Ra * Pr);
+    return TS_OK;
+  }
+  if (pr_option == TS_PR_SMALL) {
+    *nu = small ? 1.0 : sqrt(Pr / Ra);
+    *kappa = small ? 1.0 / Pr : 1.0 / sqrt(Pr * Ra);
+    *cu = small ? Ra : Pr;
+    *cT = 1.0 / Pr;
+    *nu0 = 1.0;
+    *nuc = small ? 2.0 * Pr * Pr : 2.0 * Pr * sqrt(Ra * Pr);
+    return TS_OK;
+  }
+  if (pr_option == TS_PR_ZERO || pr_option == TS_PR_INFTY) {
+    g_last_error = "Pr_option PRZERO / PRINFTY (a slaved field) is not implemented";
+    return TS_ERR_UNSUPPORTED;
+  }
+  return TS_ERR_ARG;
+}
+
 // the status of the plan's health word as last copied to the host (err_h)
 static int health_status(ts_plan* p) {
   if (*p->err_h & HEALTH_TIMEOUT) {
@@ -318,8 +354,18 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     g_last_error = "SSS needs a power-of-two Nz";
     return TS_ERR_UNSUPPORTED;
   }
+  double rbc_nu = 0, rbc_kappa = 0, rbc_cu = 1, rbc_cT = 1, rbc_nu0 = 1, rbc_nuc = 0;
+  if (cfg->force_type == TS_FORCE_RBC || cfg->basis == TS_BASIS_SFF) {
+    const int rc0 = rbc_coefficients(cfg->Pr_option, cfg->Uscaling, cfg->Ra, cfg->Pr, &rbc_nu, &rbc_kappa, &rbc_cu,
+                                     &rbc_cT, &rbc_nu0, &rbc_nuc);
+    if (rc0 != TS_OK) return rc0;
+  }
   ts_plan* p = new ts_plan();
   p->cfg = *cfg;
+  p->rbc_cu = rbc_cu;
+  p->rbc_cT = rbc_cT;
+  p->rbc_nu0 = rbc_nu0;
+  p->rbc_nuc = rbc_nuc;
   p->cfg.energy_supply = nullptr;
   p->cfg.helicity_supply = nullptr;
   Geo& g = p->g;
@@ -704,6 +750,8 @@ static int step_rbc(ts_plan* p, void* U0, void* T0) {
   const Geo& g = p->g;
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.cu = p->rbc_cu;
+  a.cT = p->rbc_cT;
   a.health = p->err_d;
   a.U0 = U0;
   a.T0 = T0;
@@ -925,6 +973,8 @@ static int ssf_step_supported(ts_plan* p, bool rbc) {
 static SffArgs ssf_rbc_args(ts_plan* p, void* U0, void* T0) {
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.cu = p->rbc_cu;
+  a.cT = p->rbc_cT;
   a.health = p->err_d;
   a.U0 = U0;
   a.T0 = T0;
@@ -1454,7 +1504,7 @@ int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
   double e = 0;
   CK(cudaMemcpyAsync(&e, p->dscr, sizeof(double), cudaMemcpyDeviceToHost, p->st));
   CK(cudaStreamSynchronize(p->st));
-  *Nu = 1.0 + 2.0 * sqrt(p->cfg.Ra * p->cfg.Pr) * e;
+  *Nu = p->rbc_nu0 + p->rbc_nuc * e;
   return TS_OK;
 }
 
@@ -1708,6 +1758,8 @@ static int step_rbc_group(ens_group& G) {
   const long long TL = (long long)g.Nx + g.Ny + g.Hz;
   SffArgs a;
   memset(&a, 0, sizeof(a));
+  a.cu = G.gp->rbc_cu;
+  a.cT = G.gp->rbc_cT;
   a.U0 = G.U;
   a.T0 = G.T;
   a.Ucur = G.Ucur;
@@ -1793,9 +1845,10 @@ int ts_ensemble_create(const ts_config* base, const ts_member* members, int coun
     c.Ra = members[m].Ra;
     c.Pr = members[m].Pr;
     if (!(c.Ra > 0) || !(c.Pr > 0)) return fail(TS_ERR_ARG);
-    // ULARGE: nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra) (Iscalar_main.cc:52-92)
-    c.nu = sqrt(c.Pr / c.Ra);
-    c.kappa = 1.0 / sqrt(c.Pr * c.Ra);
+    // nu, kappa of the scaling (Iscalar_main.cc:52-92; ULARGE: sqrt(Pr/Ra), 1/sqrt(Pr Ra))
+    double cu, cT, nu0, nuc;
+    const int rs = rbc_coefficients(c.Pr_option, c.Uscaling, c.Ra, c.Pr, &c.nu, &c.kappa, &cu, &cT, &nu0, &nuc);
+    if (rs != TS_OK) return fail(rs);
     int rc = ts_plan_create(&c, &e->plans[m]);
     if (rc != TS_OK) return fail(rc);
     for (size_t k = 0; k < e->groups.size() && gof[m] < 0; ++k) {
@@ -1809,6 +1862,14 @@ int ts_ensemble_create(const ts_config* base, const ts_member* members, int coun
     }
     e->groups[gof[m]].idx.push_back(m);
   }
+  // one launch covers a group's members with the group's buoyancy coefficients: they must
+  // agree (they do for PRLARGE / ULARGE, cu = cT = 1; other scalings carry Ra or Pr)
+  for (ens_group& G : e->groups)
+    for (int m : G.idx)
+      if (e->plans[m]->rbc_cu != G.gp->rbc_cu || e->plans[m]->rbc_cT != G.gp->rbc_cT) {
+        g_last_error = "ensemble members of one grid size need equal buoyancy coefficients (PRLARGE / ULARGE)";
+        return fail(TS_ERR_UNSUPPORTED);
+      }
   if (cudaMalloc(&e->health, count * sizeof(int)) != cudaSuccess) return fail(TS_ERR_NOMEM);
   if (cudaMemset(e->health, 0, count * sizeof(int)) != cudaSuccess) return fail(TS_ERR_CUDA);
   size_t hoff = 0;

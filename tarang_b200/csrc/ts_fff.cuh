@@ -1126,7 +1126,6 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
   // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
   const double eh = a.ex[lx] * exy;
   const double e1 = eh * eh;
-  const T Eh = (T)eh, E1 = (T)e1;
   V* Uc = reinterpret_cast<V*>(a.Ucur);
   V* tot = reinterpret_cast<V*>(a.tot);
   const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
@@ -1137,18 +1136,18 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
     const V R = Rv[i];
     const V u0 = st0[i * sstr];
     if (a.stage == 1) {
-      Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-      tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
     } else {
       const V tt = st1[i * sstr];
       if (a.stage == 2) {
-        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-        tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-        tot[o] = add(tt, scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
       } else {
-        const V un = add(scale(u0, E1), add(tt, scale(R, (T)((1.0 / 6) * a.dt))));
+        const V un = rk_u4_c(u0, tt, R, e1, (1.0 / 6) * a.dt);
         reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
         health_mark(nonfinite(un), a.err);
       }

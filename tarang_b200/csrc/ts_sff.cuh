@@ -41,6 +41,8 @@ struct SffArgs {
   // complex elements, and of the integrating-factor tables in doubles (0 for one run)
   long long msU0, msT0, msUcur, msTot, msU1in, msTin, msP;
   long long mtab;
+  // buoyancy coefficients U.Force1 = cu T, T.Force = cT U.V1 (compute_force_RBC.cc:104-150)
+  double cu, cT;
   // health words, one per member (the member index of the batch): a NaN or Inf written
   // into the state at stage 4 sets HEALTH_NONFINITE (nullptr: no check)
   int* health;
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(CW * (N / E), sff_min_blocks(CW * (N / E), E))
 
 // ---------------------------------------------------------------------------
 // Boussinesq epilogue at spectral element (m, ly, lz) of batch member mb (offset
-// `off` in a component): force U.F1 = T, T.F = U.V1 of the stage input, SFF
+// `off` in a component): force U.F1 = cu T, T.F = cT U.V1 of the stage input, SFF
 // projection, IF-RK4 stage update of U (nu) and T (kappa).  N1..N3, NT = the
 // assembled nonlinear terms (before the force).
 // ---------------------------------------------------------------------------
@@ -237,9 +239,10 @@ __device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, lon
   const long long tb = mb * a.mtab;
   const double Kxd = m * g.kf[0], Kyd = kfft(ly, g.Ny) * g.kf[1], Kzd = lz * g.kf[2];
   const T Kx = (T)Kxd, Ky = (T)Kyd, Kz = (T)Kzd;
-  // force (ULARGE): U.F1 = T, T.F = U.V1 of the stage input; nlin -= F
-  N1 = sub(N1, Tin[off]);
-  NT = sub(NT, U1in[off]);
+  // force (compute_force_RBC.cc:104-150): U.F1 = cu T, T.F = cT U.V1 of the stage input
+  // (cu = cT = 1 for PRLARGE / ULARGE); nlin -= F
+  N1 = sub(N1, scale(Tin[off], (T)a.cu));
+  NT = sub(NT, scale(U1in[off], (T)a.cT));
   // projection with SFF parities: div = +Kx N1 + i Ky N2 + i Kz N3; grad_x p = -Kx p
   const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
   const V div = add(add(scale(N1, Kx), ik(Ky, N2)), ik(Kz, N3));
@@ -254,21 +257,21 @@ __device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, lon
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const double eh = i < 3 ? ehu : eht;
-    const T Eh = (T)eh, E1 = (T)(eh * eh);
+    const double e1 = eh * eh;
     const long long o = i * g.S + off;
     const V R = Rv[i];
     const V u0 = i < 3 ? U0[o] : T0[off];
     if (a.stage == 1) {
-      Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-      tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
     } else if (a.stage == 2) {
-      Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-      tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+      tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
     } else if (a.stage == 3) {
-      Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-      tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+      Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+      tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
     } else {
-      V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+      V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
       if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
       if (i < 3) const_cast<V*>(U0)[o] = un;
       else const_cast<V*>(T0)[off] = un;
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(256) k_sff_epi(const C<T>* __restrict__ P, Geo
 // forward x pass + Boussinesq epilogue (PRLARGE / ULARGE):
 //   N1 = Dx(u1u1) + iKy F[u1u2] + iKz F[u3u1],  N2 = iKy F[u2u2] + Dx(u1u2) + iKz F[u2u3],
 //   N3 = iKz F[u3u3] + iKy F[u2u3] + Dx(u3u1),  NT = Dx(u1T) + iKy F[u2T] + iKz F[u3T]
-//   (compute_diag_offdiag.cc:47-136); force U.F1 = T, T.F = U.V1 (compute_force_RBC.cc:104-150);
+//   (compute_diag_offdiag.cc:47-136); force U.F1 = cu T, T.F = cT U.V1 (compute_force_RBC.cc:104-150);
 //   N -= F; p = div(N)/K^2; N += grad p; R = -N, RT = -NT; IF-RK4 stage update of U (nu) and T (kappa)
 //   (RK_SF.cc:97-221, Tadvance_functions.cc:57-90,226-237,372-395,589-611).
 // ---------------------------------------------------------------------------
@@ -452,21 +455,21 @@ __global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, 
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const double eh = i < 3 ? ehu : eht;
-      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const double e1 = eh * eh;
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(T0)[e] = un;
@@ -538,21 +541,21 @@ __global__ void __launch_bounds__(256, 3) k_mhd_epi(const C<T>* __restrict__ P, 
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       const double eh = i < 3 ? ehu : ehb;
-      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const double e1 = eh * eh;
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : B0[(i - 3) * g.S + e];
       if (a.stage == 1) {
-        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(B0)[(i - 3) * g.S + e] = un;
@@ -604,7 +607,6 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
     const V Rv[3] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1)};
     const double eh = a.ex[lx] * a.ey[ly] * a.ez[lz];
     const double e1 = eh * eh;
-    const T Eh = (T)eh, E1 = (T)e1;
     const bool dz = dealias_zero(g.dealias, 2, lx, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -612,16 +614,16 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
       const V R = Rv[i];
       const V u0 = U0[o];
       if (a.stage == 1) {
-        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        const V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         Uo[o] = un;
         health_mark(nonfinite(un), a.err);
       }
@@ -684,23 +686,23 @@ __global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g,
     N3 += -Kz * pr;
     const T Rv[3] = {-N1, -N2, -N3};
     const double eh = a.ex[lx] * a.ey[ly] * a.ez[lzr];
-    const T Eh = (T)eh, E1 = (T)(eh * eh);
+    const double e1 = eh * eh;
     const bool dz = sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const long long o = i * per + e;
       const T R = Rv[i], u0 = U0[o];
       if (a.stage == 1) {
-        Uc[o] = ((dz ? (T)0 : u0) + (T)(0.5 * a.dt) * R) * Eh;
-        tot[o] = (R * E1) * (T)((1.0 / 6) * a.dt);
+        Uc[o] = rk_u1(dz ? (T)0 : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = u0 * Eh + (T)(0.5 * a.dt) * R;
-        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+        Uc[o] = rk_u2(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = (u0 * Eh + (T)a.dt * R) * Eh;
-        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+        Uc[o] = rk_u3(u0, R, eh, a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const T un = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
+        const T un = rk_u4(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         Uo[o] = un;
         health_mark(!isfinite(un), a.err);
       }
@@ -715,7 +717,7 @@ __global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g,
 // transforms of the nine products (u1u1, u2u2, u3u3, u1u2, u2u3, u3u1, u1T, u2T,
 // u3T; normalised):
 //   N as the fluid step; NT = Dx(u1T) + Dy(u2T) + Dz(u3T) (compute_diag_offdiag.cc:116-136);
-//   force (compute_force_RBC.cc:104-150): U.F1 = T, T.F = U.V1, both from the
+//   force (compute_force_RBC.cc:104-150): U.F1 = cu T, T.F = cT U.V1, both from the
 //   un-dealiased stage input; N1 -= T, NT -= u1 (Add_force); pressure from N;
 //   R = -N, RT = -NT; IF-RK4 stage update of U (nu, tables eu) and T (kappa,
 //   tables et) as RK_SF.cc:97-221, in place at stage 4; no reality condition.
@@ -746,8 +748,8 @@ __global__ void __launch_bounds__(256) k_ssf_rbc_epi(const C<T>* __restrict__ P,
     V N2 = add(add(dC(Ky, q[1]), dS(Kx, q[3])), ik(Kz, q[4]));
     V N3 = add(add(ik(Kz, q[2]), dS(Ky, q[4])), dS(Kx, q[5]));
     V NT = add(add(dC(Kx, q[6]), dS(Ky, q[7])), ik(Kz, q[8]));
-    N1 = sub(N1, Tin[e]);
-    NT = sub(NT, U1in[e]);
+    N1 = sub(N1, scale(Tin[e], (T)a.cu));
+    NT = sub(NT, scale(U1in[e], (T)a.cT));
     const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
     const V div = add(add(dS(Kx, N1), dS(Ky, N2)), ik(Kz, N3));
     const V pr = (K2 > 0) ? mk<V>(div.x / (T)K2, div.y / (T)K2) : mk<V>(0, 0);
@@ -761,21 +763,21 @@ __global__ void __launch_bounds__(256) k_ssf_rbc_epi(const C<T>* __restrict__ P,
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const double eh = i < 3 ? ehu : eht;
-      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const double e1 = eh * eh;
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = scale(add(dz ? mk<V>(0, 0) : u0, scale(R, (T)(0.5 * a.dt))), Eh);
-        tot[o] = scale(scale(R, E1), (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = add(scale(u0, Eh), scale(R, (T)(0.5 * a.dt)));
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = scale(add(scale(u0, Eh), scale(R, (T)a.dt)), Eh);
-        tot[o] = add(tot[o], scale(scale(R, Eh), (T)((1.0 / 3) * a.dt)));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const V un = add(scale(u0, E1), add(tot[o], scale(R, (T)((1.0 / 6) * a.dt))));
+        const V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
         health_mark(nonfinite(un), a.health);
@@ -809,8 +811,8 @@ __global__ void __launch_bounds__(256) k_sss_rbc_epi(const T* __restrict__ P, Ge
     T N2 = (-Ky * q[1] + Kx * q[3]) + Kz * q[4];
     T N3 = (-Kz * q[2] + Ky * q[4]) + Kx * q[5];
     T NT = (-Kx * q[6] + Ky * q[7]) + Kz * q[8];
-    N1 -= Tin[e];
-    NT -= U1in[e];
+    N1 -= (T)a.cu * Tin[e];
+    NT -= (T)a.cT * U1in[e];
     const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
     const T div = (Kx * N1 + Ky * N2) + Kz * N3;
     const T pr = K2 > 0 ? div / (T)K2 : (T)0;
@@ -824,20 +826,20 @@ __global__ void __launch_bounds__(256) k_sss_rbc_epi(const T* __restrict__ P, Ge
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const double eh = i < 3 ? ehu : eht;
-      const T Eh = (T)eh, E1 = (T)(eh * eh);
+      const double e1 = eh * eh;
       const long long o = i * per + e;
       const T R = Rv[i], u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = ((dz ? (T)0 : u0) + (T)(0.5 * a.dt) * R) * Eh;
-        tot[o] = (R * E1) * (T)((1.0 / 6) * a.dt);
+        Uc[o] = rk_u1(dz ? (T)0 : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = u0 * Eh + (T)(0.5 * a.dt) * R;
-        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+        Uc[o] = rk_u2(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = (u0 * Eh + (T)a.dt * R) * Eh;
-        tot[o] = tot[o] + (R * Eh) * (T)((1.0 / 3) * a.dt);
+        Uc[o] = rk_u3(u0, R, eh, a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const T un = u0 * E1 + (tot[o] + (T)((1.0 / 6) * a.dt) * R);
+        const T un = rk_u4(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
         health_mark(!isfinite(un), a.health);

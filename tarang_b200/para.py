@@ -68,6 +68,8 @@ class RunParams:
     force_global_alpha_beta: bool = False
     flux_radii: list = field(default_factory=list)
     input_field_procedure: int = 5   # io.input_field_procedure (1: read complex fields from in/)
+    pr_option: str = "PRLARGE"       # PHYSICS.Pr_option (RBC)
+    uscaling: str = "ULARGE"         # PHYSICS.Uscaling (RBC)
 
     @property
     def nsteps(self) -> int:
@@ -156,13 +158,15 @@ def read_para(path: str) -> RunParams:
         ph = p.get("PHYSICS") or {}
         pr_opt = str(ph.get("Pr_option", "PRLARGE")).strip()
         usc = str(ph.get("Uscaling", "USMALL")).strip()
-        if (pr_opt, usc) != ("PRLARGE", "ULARGE"):
-            raise NotImplementedError(f"PHYSICS Pr_option {pr_opt} / Uscaling {usc}: PRLARGE / ULARGE only")
+        if pr_opt not in ("PRLARGE", "PRSMALL") or usc not in ("ULARGE", "USMALL"):
+            raise NotImplementedError(f"PHYSICS Pr_option {pr_opt} / Uscaling {usc}: PRLARGE / PRSMALL with "
+                                      "ULARGE / USMALL (PRZERO and PRINFTY slave one field to the other)")
+        rp.pr_option, rp.uscaling = pr_opt, usc
         rp.Ra = float(ph.get("Rayleigh", 2000.0))
         rp.Pr = float(ph.get("Prandtl", 1.0))
-        # ULARGE (Iscalar_main.cc:52-92): nu = sqrt(Pr/Ra), kappa = 1/sqrt(Pr Ra)
-        rp.nu = math.sqrt(rp.Pr / rp.Ra)
-        rp.kappa = 1.0 / math.sqrt(rp.Pr * rp.Ra)
+        # diss_coefficients of the scaling (Iscalar_main.cc:52-92; ULARGE: sqrt(Pr/Ra), 1/sqrt(Pr Ra))
+        from .solver import rbc_diss_coefficients
+        rp.nu, rp.kappa = rbc_diss_coefficients(pr_opt, usc, rp.Ra, rp.Pr)
     force = p.get("force") or {}
     procs = force.get("field_procedure")
     procs = [int(x) for x in (procs if isinstance(procs, list) else [procs]) if x is not None]
@@ -210,7 +214,8 @@ def plan_from_dir(data_dir: str, precision: str = "f64", nlin_form: str = "conse
         forcing = Forcing(rp.force_inner, rp.force_outer, arrs[0], arrs[1] if len(arrs) > 1 else None)
     kw = dict(precision=precision, dealias=rp.dealias, kfactor=rp.kfactor, reality_fix=rp.reality_fix, dt=rp.dt)
     if rp.kind == "RBC":
-        plan = Plan(rp.N, basis=rp.basis, nu=rp.nu, kappa=rp.kappa, Ra=rp.Ra, Pr=rp.Pr, **kw)
+        plan = Plan(rp.N, basis=rp.basis, nu=rp.nu, kappa=rp.kappa, Ra=rp.Ra, Pr=rp.Pr, Pr_option=rp.pr_option,
+                    Uscaling=rp.uscaling, **kw)
     elif rp.kind in ("SCALAR_INCOMPRESS", "MHD_INCOMPRESS"):
         # the second dissipation coefficient: kappa of T, or eta of B (stored as the plan's kappa)
         plan = Plan(rp.N, nlin_form="conservative", nu=rp.nu, kappa=rp.kappa, **kw)

@@ -70,11 +70,26 @@ def _ptr(a) -> int:
     raise TypeError(type(a))
 
 
+# PHYSICS.Pr_option / PHYSICS.Uscaling of an RBC run
+_PR_OPTION = {"PRLARGE": 0, "PRSMALL": 1, "PRZERO": 2, "PRINFTY": 3}
+_USCALING = {"ULARGE": 0, "USMALL": 1}
+
+
+def rbc_diss_coefficients(pr_option: str, uscaling: str, Ra: float, Pr: float) -> tuple:
+    """(nu, kappa) of an RBC run (Iscalar_main.cc:52-92) for Pr_option PRLARGE / PRSMALL."""
+    small = uscaling == "USMALL"
+    if pr_option == "PRLARGE":
+        return (Pr, 1.0) if small else (math.sqrt(Pr / Ra), 1.0 / math.sqrt(Pr * Ra))
+    if pr_option == "PRSMALL":
+        return (1.0, 1.0 / Pr) if small else (math.sqrt(Pr / Ra), 1.0 / math.sqrt(Pr * Ra))
+    raise NotImplementedError(f"Pr_option {pr_option}: PRLARGE / PRSMALL only")
+
+
 class Plan:
     def __init__(self, N, basis: str = "FFF", precision: str = "f64", nlin_form: str = "conservative",
                  dealias: str = "reference", nu: float = 0.01, dt: float = 1e-3, kfactor=(1.0, 1.0, 1.0),
                  reality_fix: bool = True, forcing: Forcing | None = None, kappa: float = 0.01,
-                 Ra: float = 1e5, Pr: float = 1.0):
+                 Ra: float = 1e5, Pr: float = 1.0, Pr_option: str = "PRLARGE", Uscaling: str = "ULARGE"):
         self.lib = L.load()
         if isinstance(N, int):
             N = (N, N, N)
@@ -90,6 +105,8 @@ class Plan:
         c.dealias_mode = _DEALIAS[dealias]
         c.reality_fix = int(bool(reality_fix))
         c.nu, c.kappa, c.dt, c.Ra, c.Pr = nu, kappa, dt, Ra, Pr
+        c.Pr_option = _PR_OPTION[Pr_option]
+        c.Uscaling = _USCALING[Uscaling]
         self._keep = []
         if forcing is not None:
             es = np.ascontiguousarray(forcing.energy_supply, dtype=np.float64)

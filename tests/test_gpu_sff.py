@@ -135,3 +135,56 @@ def test_sff_transform_rejects_wrong_parity(cuda):
     real = torch.zeros((1, 16, 16, 18), dtype=torch.float64, device=cuda)
     with pytest.raises(tb.TsError):
         plan.forward(real, plan.field(1), parity="FFF")
+
+
+SCALINGS = [("PRLARGE", "USMALL"), ("PRSMALL", "ULARGE"), ("PRSMALL", "USMALL")]
+
+
+@pytest.mark.parametrize("pr,us", SCALINGS)
+@pytest.mark.parametrize("basis", ["SFF", "SSF"])
+def test_rbc_scalings_match_oracle(cuda, basis, pr, us):
+    """The other Pr_option / Uscaling combinations: buoyancy coefficients (compute_force_RBC.cc:
+    104-150), nu and kappa (Iscalar_main.cc:52-92) and the Nusselt factors (Correlation.cc:
+    144-176) against the oracle: FP64 <= 1e-12 after 3 steps, FP32 <= 1e-5, Nusselt to 1e-12."""
+    import torch
+    import tarang_b200 as tb
+    from tarang_b200.solver import rbc_diss_coefficients
+    N = (16, 16, 16)
+    kf = KF if basis == "SFF" else (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+    g = R.Grid(N, kf, basis)
+    Ra, Pr = 3e4, 0.7
+    cfg = R.RBCConfig(g, Ra=Ra, Pr=Pr, dt=1e-5 if us == "USMALL" else 1e-3, dealias_mode=1, pr_option=pr,
+                      uscaling=us)
+    if basis == "SFF":
+        U0, T0 = random_state(g, 0.3, 7)
+    else:
+        rng = np.random.default_rng(7)
+        f = [0.3 * R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCF", "CSF", "CCF", "SCF")]
+        U0, T0 = np.stack(f[:3]), f[3]
+    Uo, To = U0, T0
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    nu, kappa = rbc_diss_coefficients(pr, us, Ra, Pr)
+    assert (nu, kappa) == (cfg.nu, cfg.kappa)
+    for prec, tol in (("f64", 1e-12), ("f32", 1e-5)):
+        plan = tb.Plan(N, basis=basis, precision=prec, kfactor=kf, dealias="reference", nu=nu, kappa=kappa,
+                       dt=cfg.dt, Ra=Ra, Pr=Pr, Pr_option=pr, Uscaling=us)
+        u = torch.from_numpy(np.ascontiguousarray(U0)).to(cuda).to(plan.torch_dtype())
+        T = torch.from_numpy(np.ascontiguousarray(T0)[None]).to(cuda).to(plan.torch_dtype())
+        plan.rk4_step_rbc(u, T, 3)
+        plan.status()
+        assert rel(u.cpu().numpy().astype(np.complex128), Uo) < tol
+        assert rel(T[0].cpu().numpy().astype(np.complex128), To) < tol
+        if prec == "f64" and basis == "SFF":
+            ref = R.nusselt(cfg, Uo, To)
+            assert abs(plan.nusselt(u, T) - ref) < 1e-12 * max(1.0, abs(ref))
+        plan.close()
+
+
+def test_rbc_slaved_scalings_are_refused(cuda):
+    """PRZERO and PRINFTY slave one field to the other (Single_time_step_RBC,
+    Tadvance_functions.cc:380-395): refused at plan creation, not run as something else."""
+    import tarang_b200 as tb
+    for pr in ("PRZERO", "PRINFTY"):
+        with pytest.raises(tb.TsError):
+            tb.Plan((16, 16, 16), basis="SFF", kfactor=KF, Pr_option=pr)

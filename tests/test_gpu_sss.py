@@ -216,3 +216,28 @@ def test_sss_max_div_and_padding(cuda):
     vr = torch.view_as_real(v).reshape(3, N[0], N[1], N[2] + 2)
     vr[..., N[2]:] = 7.0
     assert plan.max_div(v) == d0 and plan.energy(v) == e0
+
+
+@pytest.mark.parametrize("pr,us", [("PRLARGE", "USMALL"), ("PRSMALL", "ULARGE"), ("PRSMALL", "USMALL")])
+def test_sss_rbc_scalings_match_oracle(cuda, pr, us):
+    """RBC on SSS under the other Pr_option / Uscaling combinations, FP64 <= 1e-12 after 3 steps."""
+    import tarang_b200 as tb
+    N = (16, 16, 16)
+    g = R.Grid(N, KF_RBC, "SSS")
+    rng = np.random.default_rng(8)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in ("SCC", "CSC", "CCS")])
+    U0 = -0.3 * R.project_rhs(g, U)
+    T0 = 0.3 * R.forward(g, rng.standard_normal(g.rshape), "SCC")
+    cfg = R.RBCConfig(g, Ra=3e4, Pr=0.7, dt=1e-5 if us == "USMALL" else 1e-3, dealias_mode=1, pr_option=pr,
+                      uscaling=us)
+    Uo, To = U0.copy(), T0.copy()
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    plan = tb.Plan(N, basis="SSS", kfactor=KF_RBC, precision="f64", nu=cfg.nu, kappa=cfg.kappa, dt=cfg.dt,
+                   dealias="reference", Ra=3e4, Pr=0.7, Pr_option=pr, Uscaling=us)
+    u = _dev(U0, cuda, "f64")
+    T = _dev(T0[None], cuda, "f64")
+    plan.rk4_step_rbc(u, T, 3)
+    plan.status()
+    assert rel(from_padded(u, N[2]), Uo) < 1e-12
+    assert rel(from_padded(T, N[2])[0], To) < 1e-12

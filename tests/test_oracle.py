@@ -422,3 +422,48 @@ def test_sincos_energy_weights_are_parseval(basis, parity):
     u = R.inverse(g, A, parity)
     assert abs(R.total_energy_scalar(g, A) / (0.5 * np.mean(u ** 2)) - 1) < 1e-13
     assert abs(R.cross_energy(g, A, A) - R.total_energy_scalar(g, A)) < 1e-13
+
+
+SCALINGS = [("PRLARGE", "ULARGE"), ("PRLARGE", "USMALL"), ("PRSMALL", "ULARGE"), ("PRSMALL", "USMALL")]
+
+
+@pytest.mark.parametrize("pr,us", SCALINGS)
+def test_rbc_scalings_are_one_physics(pr, us):
+    """Every scaling of compute_force_RBC.cc / Iscalar_main.cc describes the same Boussinesq
+    system in other units: cu cT / (nu kappa) = Ra and nu / kappa = Pr."""
+    Ra, Pr = 3.7e5, 0.3
+    c = R.rbc_coefficients(pr, us, Ra, Pr)
+    assert abs(c["cu"] * c["cT"] / (c["nu"] * c["kappa"]) / Ra - 1) < 1e-14
+    assert abs(c["nu"] / c["kappa"] / Pr - 1) < 1e-14
+    with pytest.raises(NotImplementedError):
+        R.rbc_coefficients("PRZERO", us, Ra, Pr)
+
+
+@pytest.mark.parametrize("pr,us", SCALINGS)
+def test_rbc_roll_follows_the_linear_system_every_scaling(pr, us):
+    """One small free-slip roll on SFF under each scaling follows the exact linear system
+    da/dt = cu (1 - kx^2/K^2) b - nu K^2 a, db/dt = cT a - kappa K^2 b to 1e-7 of its amplitude
+    over 20 steps, and the Nusselt number is nu0 + nuc <u1, T>."""
+    from scipy.linalg import expm
+    kf = (math.pi, 2 * math.pi, 2 * math.pi)
+    g = R.Grid((16, 8, 8), kf, "SFF")
+    eps = 1e-9
+    U0 = np.zeros((3,) + g.shape, complex)
+    T0 = np.zeros(g.shape, complex)
+    kx, kz = kf[0], kf[2]
+    # mode m = 1, kz = 1: u1 sine, u3 cosine with kx a + kz c = 0 (divergence Kx U1 + i Kz U3 = 0)
+    U0[0, 1, 0, 1] = eps
+    U0[2, 1, 0, 1] = 1j * kx * eps / kz
+    T0[1, 0, 1] = 0.5 * eps
+    cfg = R.RBCConfig(g, Ra=2e4, Pr=0.7, dt=5e-5 if us == "USMALL" else 2e-3, pr_option=pr, uscaling=us)
+    co = cfg.coeffs
+    U, T = U0.copy(), T0.copy()
+    for _ in range(20):
+        U, T = R.rbc_rk4_step(cfg, U, T)
+    K2 = kx * kx + kz * kz
+    M = np.array([[-cfg.nu * K2, co["cu"] * (1 - kx * kx / K2)], [co["cT"], -cfg.kappa * K2]])
+    a, b = expm(M * 20 * cfg.dt) @ np.array([eps, 0.5 * eps])
+    assert abs(U[0, 1, 0, 1] - a) < 1e-7 * eps and abs(T[1, 0, 1] - b) < 1e-7 * eps
+    assert abs(U[0, 1, 0, 1] / eps - 1) > 1e-5   # the state moved
+    nu = R.nusselt(cfg, U, T)
+    assert nu == co["nu0"] + co["nuc"] * R.cross_energy(g, U[0], T)

@@ -553,3 +553,22 @@ def test_restart_continues_bit_for_bit(cuda, tmp_path, name, precision):
     torch.cuda.synchronize()
     for a, b in zip(fields2, ref):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("pr,us", [("PRSMALL", "USMALL"), ("PRLARGE", "USMALL"), ("PRSMALL", "ULARGE")])
+def test_read_para_rbc_scalings(tmp_path, pr, us):
+    """Pr_option PRLARGE / PRSMALL with Uscaling ULARGE / USMALL set nu and kappa as
+    Iscalar_main.cc:52-92; PRZERO / PRINFTY are refused by name."""
+    from tarang_b200.solver import rbc_diss_coefficients
+    text = open(os.path.join(RBC_DIR, "in", "para.yaml")).read()
+    (tmp_path / "in").mkdir()
+    (tmp_path / "in" / "para.yaml").write_text(text.replace("Pr_option: PRLARGE", f"Pr_option: {pr}")
+                                                .replace("Uscaling: ULARGE", f"Uscaling: {us}"))
+    rp = para.read_para(str(tmp_path / "in" / "para.yaml"))
+    assert (rp.pr_option, rp.uscaling) == (pr, us)
+    assert (rp.nu, rp.kappa) == rbc_diss_coefficients(pr, us, rp.Ra, rp.Pr)
+    if us == "USMALL":
+        assert rp.nu == (rp.Pr if pr == "PRLARGE" else 1.0)
+    (tmp_path / "in" / "para.yaml").write_text(text.replace("Pr_option: PRLARGE", "Pr_option: PRZERO"))
+    with pytest.raises(NotImplementedError):
+        para.read_para(str(tmp_path / "in" / "para.yaml"))
