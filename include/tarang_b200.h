@@ -272,9 +272,10 @@ int ts_adjoint_window(ts_plan* plan, const void* u_start, int nsteps, void* lam_
 
 /* Launch tuning (no reference counterpart: the reference leaves the FFT plan
  * to FFTW's planner).  Each right-hand side runs five pass classes; for each
- * the library holds a fixed rule (candidate 0) and up to three other kernel
+ * the library holds a fixed rule (candidate 0) and up to four other kernel
  * candidates that change the radix schedule (elements per thread, so the
- * Stockham passes' radices), the column-tile width, the staging depth, or the
+ * Stockham passes' radices), the column-tile width, the staging depth (y passes:
+ * candidate 4 keeps two items in flight ahead of the one transformed), or the
  * kernel form (z: shared-memory slot kernels; FFF forward x: split x FFF +
  * elementwise epilogue; SFF forward x: the other fused/split choice), plus a
  * blocks-per-SM count for the persistent launches (y passes, fused FFF

@@ -354,8 +354,9 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     g_last_error = "SSS needs a power-of-two Nz";
     return TS_ERR_UNSUPPORTED;
   }
+  // the RBC coefficients of the plan's scaling (any basis: ts_rk4_step_rbc and ts_nusselt use them)
   double rbc_nu = 0, rbc_kappa = 0, rbc_cu = 1, rbc_cT = 1, rbc_nu0 = 1, rbc_nuc = 0;
-  if (cfg->force_type == TS_FORCE_RBC || cfg->basis == TS_BASIS_SFF) {
+  {
     const int rc0 = rbc_coefficients(cfg->Pr_option, cfg->Uscaling, cfg->Ra, cfg->Pr, &rbc_nu, &rbc_kappa, &rbc_cu,
                                      &rbc_cT, &rbc_nu0, &rbc_nuc);
     if (rc0 != TS_OK) return rc0;

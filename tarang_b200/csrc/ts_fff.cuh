@@ -18,7 +18,7 @@
 namespace ts {
 
 // pass classes of the launch tuning: inverse x, inverse y, z, forward y, forward x
-enum { TUNE_X_INV = 0, TUNE_Y_INV = 1, TUNE_Z = 2, TUNE_Y_FWD = 3, TUNE_X_FWD = 4, TUNE_NCLASS = 5, TUNE_NCAND = 4 };
+enum { TUNE_X_INV = 0, TUNE_Y_INV = 1, TUNE_Z = 2, TUNE_Y_FWD = 3, TUNE_X_FWD = 4, TUNE_NCLASS = 5, TUNE_NCAND = 5 };
 
 struct Geo {
   int Nx, Ny, Nz, Hz;
@@ -44,15 +44,20 @@ constexpr int SHELL_WARPS = 4;
 // into the other staging tile with cp.async.
 // Shared memory: 2 staging tiles + 1 exchange tile of L x CW complex (NT = 3),
 // or 2 staging tiles with the consumed one doubling as the exchange tile
-// (NT = 2: wider column tiles fit, e.g. 8 columns at L = 1024 in FP32).
+// (NT = 2: wider column tiles fit, e.g. 8 columns at L = 1024 in FP32), or
+// 3 staging tiles with the consumed one as the exchange tile (NT = 4: the tiles of
+// the next two items stream in while one is transformed).
 // ---------------------------------------------------------------------------
+__host__ __device__ constexpr int str_tiles(int nt) { return nt == 4 ? 3 : nt; }
 template <typename T, int L, int E, int CW, int DIR, int NT = 3>
 __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     k_strided_fft(C<T>* __restrict__ data, int nf, long long fstride, int inner, long long rstride,
                   long long ostride, int nouter, const C<T>* __restrict__ tw, int per, long long mstride,
                   int zero_hi) {
   typedef C<T> V;
-  static_assert(NT == 2 || NT == 3, "two or three tiles");
+  static_assert(NT == 2 || NT == 3 || NT == 4, "two or three staging tiles");
+  constexpr int NBUF = NT == 4 ? 3 : 2;  // staging tiles: items in flight = NBUF - 1 ahead
+  constexpr bool XC = NT != 3;           // exchange in the consumed staging tile
   extern __shared__ __align__(16) unsigned char smraw[];
   V* stage = reinterpret_cast<V*>(smraw);
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
@@ -84,11 +89,15 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     }
     cp_async_commit();
   };
-  int buf = 0;
+  // the first NBUF - 1 items; every issue commits one cp.async group (empty past the end)
   issue(blockIdx.x, 0);
-  for (long long w = blockIdx.x; w < nwork; w += gridDim.x, buf ^= 1) {
-    issue(w + gridDim.x, buf ^ 1);
-    cp_async_wait<1>();
+  if (NBUF == 3) issue(blockIdx.x + gridDim.x, 1);
+  int buf = 0;
+  for (long long w = blockIdx.x; w < nwork; w += gridDim.x, buf = (buf + 1 == NBUF ? 0 : buf + 1)) {
+    // item w + (NBUF-1) G into the tile item w - G used (every thread passed the
+    // barrier after its last exchange read), then wait for item w's group
+    issue(w + (NBUF - 1) * (long long)gridDim.x, buf == 0 ? NBUF - 1 : buf - 1);
+    cp_async_wait<NBUF - 1>();
     bool ok;
     V* d = locate(w, ok);
     V v[E];
@@ -100,10 +109,10 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
       v[s] = (ok && !(zero_hi && 3 * (r < L - r ? r : L - r) > L)) ? st[r * CW] : mk<V>(0, 0);
     }
     // each thread read back only what it staged itself; the barrier is for the
-    // exchange writes into the consumed tile (NT = 2)
-    if (NT == 2) __syncthreads();
+    // exchange writes into the consumed tile (NT = 2, 4)
+    if (XC) __syncthreads();
     fft_regs<L, E, DIR, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(
-        v, t, NT == 2 ? stage + buf * L * CW : stage + 2 * L * CW, CW, c, tw, 1);
+        v, t, XC ? stage + buf * L * CW : stage + 2 * L * CW, CW, c, tw, 1);
     if (ok) {
 #pragma unroll
       for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
@@ -1126,6 +1135,7 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
   // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
   const double eh = a.ex[lx] * exy;
   const double e1 = eh * eh;
+  const Fac<T> Feh(eh), Fe1(e1);
   V* Uc = reinterpret_cast<V*>(a.Ucur);
   V* tot = reinterpret_cast<V*>(a.tot);
   const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
@@ -1136,18 +1146,18 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
     const V R = Rv[i];
     const V u0 = st0[i * sstr];
     if (a.stage == 1) {
-      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
+      tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
     } else {
       const V tt = st1[i * sstr];
       if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
+        tot[o] = rk_tacc_c(tt, R, Feh, (T)((1.0 / 3) * a.dt));
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
-        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
+        tot[o] = rk_tacc_c(tt, R, Feh, (T)((1.0 / 3) * a.dt));
       } else {
-        const V un = rk_u4_c(u0, tt, R, e1, (1.0 / 6) * a.dt);
+        const V un = rk_u4_c(u0, tt, R, Fe1, (T)((1.0 / 6) * a.dt));
         reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
         health_mark(nonfinite(un), a.err);
       }

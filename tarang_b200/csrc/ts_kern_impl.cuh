@@ -124,12 +124,14 @@ constexpr Tile str_cand(int L, int v) {
        : v == 1 ? (L % 3 != 0 && str_e(L) > 4 ? Tile{str_e(L) / 2, str_cw(L), str_nt(L)} : Tile{0, 0, 0})
        : v == 2 ? (str_cw(L) > 1 ? Tile{str_e(L), str_cw(L) / 2, str_nt(L)} : Tile{0, 0, 0})
        : v == 3 ? Tile{str_e(L), str_cw(L), 5 - str_nt(L)}
+       : v == 4 ? Tile{str_e(L), str_cw(L), 4}
                 : Tile{0, 0, 0};
 }
 constexpr bool str_valid(int L, int v) {
-  return v == 0 || (v < NCAND && tile_fits(L, str_cand(L, v), str_cand(L, v).NT) &&
+  return v == 0 || (v < NCAND && tile_fits(L, str_cand(L, v), str_tiles(str_cand(L, v).NT)) &&
                     !tile_eq(str_cand(L, v), str_cand(L, 0)) && (v < 2 || !tile_eq(str_cand(L, v), str_cand(L, 1))) &&
-                    (v < 3 || !tile_eq(str_cand(L, v), str_cand(L, 2))));
+                    (v < 3 || !tile_eq(str_cand(L, v), str_cand(L, 2))) &&
+                    (v < 4 || !tile_eq(str_cand(L, v), str_cand(L, 3))));
 }
 
 template <int L, int VV, typename Fn> void with_str_tile(Fn&& fn) {
@@ -156,7 +158,7 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       const long long ostride = axis == 0 ? 0 : (long long)g.Ny * g.Hz;
       const int nouter = axis == 0 ? 1 : g.Nx;
       const long long nwork = (long long)nf * ((inner + CW - 1) / CW) * nouter;
-      const size_t sm = (size_t)NT * LL * CW * sizeof(V);
+      const size_t sm = (size_t)str_tiles(NT) * LL * CW * sizeof(V);
       // persistent grid: as many blocks as fit on the 148 SMs at once (or the tuned count)
       const int cap = (CW * (LL / E)) <= 256 ? 2 : 1;
       const int fit = (int)((227 * 1024) / sm);
@@ -177,6 +179,7 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       case 1: with_str_tile<LL, 1>(run); break;
       case 2: with_str_tile<LL, 2>(run); break;
       case 3: with_str_tile<LL, 3>(run); break;
+      case 4: with_str_tile<LL, 4>(run); break;
       default: run(std::integral_constant<int, 0>{});
     }
   });

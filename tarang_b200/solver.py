@@ -192,7 +192,7 @@ class Plan:
         for c, name in enumerate(L.TUNE_CLASSES):
             m, b = ctypes.c_int(), ctypes.c_int()
             L.check(self.lib.ts_tuning_candidates(self.h, c, ctypes.byref(m), ctypes.byref(b)), "ts_tuning_candidates")
-            out[name] = {"variants": [v for v in range(4) if m.value >> v & 1], "blocks": bool(b.value)}
+            out[name] = {"variants": [v for v in range(8) if m.value >> v & 1], "blocks": bool(b.value)}
         return out
 
     def tuning_key(self) -> str:
