@@ -416,54 +416,40 @@ template <typename V> __device__ __forceinline__ bool nonfinite(const V& v) { re
 
 // ---------------------------------------------------------------------------
 // IF-RK4 stage arithmetic of one mode (RK.cc:91-170: Single_time_step,
-// Compute_RK4_parts).  eh = E(1/2) = exp(-nu dt K^2 / 2) and e1 = E(1) come from the
-// FP64 tables; c = the stage's dt factor.  A factor rounded to FP32 once would scale
-// the mode by the same wrong amount every step, a bias that grows linearly with the
-// step count (2000 steps: 5.5e-5 relative against the FP64 run), so in FP32 each
-// factor is applied as an unevaluated sum hi + lo of two FP32 numbers, a*hi + a*lo
-// (one FMA): the product is rounded once, like an FP64 factor, with no conversion
-// per element.  In FP64 the factors are plain doubles.
+// Compute_RK4_parts), every product and sum in FP64 and one rounding per stored
+// value.  eh = E(1/2) = exp(-nu dt K^2 / 2), e1 = E(1) (FP64 tables); c = the dt factor.
+// In the FP32 path a factor rounded to FP32 (eh or e1 to 24 bits) would scale a mode by
+// the same wrong amount every step, a bias that grows linearly with the step count; in
+// FP64 these are the plain expressions.
 // ---------------------------------------------------------------------------
-template <typename S> struct Fac;
-template <> struct Fac<double> {
-  double v;
-  __device__ __forceinline__ explicit Fac(double x) : v(x) {}
-  __device__ __forceinline__ double mul(double a) const { return a * v; }
-};
-template <> struct Fac<float> {
-  float hi, lo;
-  __device__ __forceinline__ explicit Fac(double x) : hi((float)x), lo((float)(x - (double)(float)x)) {}
-  __device__ __forceinline__ float mul(float a) const { return fmaf(a, hi, a * lo); }
-};
-template <typename S> __device__ __forceinline__ S rk_u1(S u0, S R, const Fac<S>& eh, S c) {
-  return eh.mul(u0 + R * c);                  // (u0 + R dt/2) E(1/2)
+template <typename S> __device__ __forceinline__ S rk_u1(S u0, S R, double eh, double c) {
+  return (S)(((double)u0 + (double)R * c) * eh);      // (u0 + R dt/2) E(1/2)
 }
-template <typename S> __device__ __forceinline__ S rk_t1(S R, const Fac<S>& e1, S c) {
-  return e1.mul(R) * c;                       // (R E(1)) dt/6
+template <typename S> __device__ __forceinline__ S rk_t1(S R, double e1, double c) {
+  return (S)(((double)R * e1) * c);                   // (R E(1)) dt/6
 }
-template <typename S> __device__ __forceinline__ S rk_u2(S u0, S R, const Fac<S>& eh, S c) {
-  return eh.mul(u0) + R * c;                  // u0 E(1/2) + R dt/2
+template <typename S> __device__ __forceinline__ S rk_u2(S u0, S R, double eh, double c) {
+  return (S)((double)u0 * eh + (double)R * c);        // u0 E(1/2) + R dt/2
 }
-template <typename S> __device__ __forceinline__ S rk_tacc(S tt, S R, const Fac<S>& eh, S c) {
-  return tt + eh.mul(R) * c;                  // tot + (R E(1/2)) dt/3
+template <typename S> __device__ __forceinline__ S rk_tacc(S tt, S R, double eh, double c) {
+  return (S)((double)tt + ((double)R * eh) * c);      // tot + (R E(1/2)) dt/3
 }
-template <typename S> __device__ __forceinline__ S rk_u3(S u0, S R, const Fac<S>& eh, S c) {
-  return eh.mul(eh.mul(u0) + R * c);          // (u0 E(1/2) + R dt) E(1/2)
+template <typename S> __device__ __forceinline__ S rk_u3(S u0, S R, double eh, double c) {
+  return (S)(((double)u0 * eh + (double)R * c) * eh); // (u0 E(1/2) + R dt) E(1/2)
 }
-template <typename S> __device__ __forceinline__ S rk_u4(S u0, S tt, S R, const Fac<S>& e1, S c) {
-  return e1.mul(u0) + (tt + R * c);           // u0 E(1) + (tot + R dt/6)
+template <typename S> __device__ __forceinline__ S rk_u4(S u0, S tt, S R, double e1, double c) {
+  return (S)((double)u0 * e1 + ((double)tt + (double)R * c));  // u0 E(1) + (tot + R dt/6)
 }
-// complex forms (component-wise); S = the component type of V
 #define TS_RK_CPLX(NAME, ...) \
-  template <typename V, typename S = decltype(V::x)> __device__ __forceinline__ V NAME##_c(__VA_ARGS__)
-TS_RK_CPLX(rk_u1, V u0, V R, const Fac<S>& eh, S c) { return mk<V>(rk_u1(u0.x, R.x, eh, c), rk_u1(u0.y, R.y, eh, c)); }
-TS_RK_CPLX(rk_t1, V R, const Fac<S>& e1, S c) { return mk<V>(rk_t1(R.x, e1, c), rk_t1(R.y, e1, c)); }
-TS_RK_CPLX(rk_u2, V u0, V R, const Fac<S>& eh, S c) { return mk<V>(rk_u2(u0.x, R.x, eh, c), rk_u2(u0.y, R.y, eh, c)); }
-TS_RK_CPLX(rk_tacc, V tt, V R, const Fac<S>& eh, S c) {
+  template <typename V> __device__ __forceinline__ V NAME##_c(__VA_ARGS__)
+TS_RK_CPLX(rk_u1, V u0, V R, double eh, double c) { return mk<V>(rk_u1(u0.x, R.x, eh, c), rk_u1(u0.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_t1, V R, double e1, double c) { return mk<V>(rk_t1(R.x, e1, c), rk_t1(R.y, e1, c)); }
+TS_RK_CPLX(rk_u2, V u0, V R, double eh, double c) { return mk<V>(rk_u2(u0.x, R.x, eh, c), rk_u2(u0.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_tacc, V tt, V R, double eh, double c) {
   return mk<V>(rk_tacc(tt.x, R.x, eh, c), rk_tacc(tt.y, R.y, eh, c));
 }
-TS_RK_CPLX(rk_u3, V u0, V R, const Fac<S>& eh, S c) { return mk<V>(rk_u3(u0.x, R.x, eh, c), rk_u3(u0.y, R.y, eh, c)); }
-TS_RK_CPLX(rk_u4, V u0, V tt, V R, const Fac<S>& e1, S c) {
+TS_RK_CPLX(rk_u3, V u0, V R, double eh, double c) { return mk<V>(rk_u3(u0.x, R.x, eh, c), rk_u3(u0.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_u4, V u0, V tt, V R, double e1, double c) {
   return mk<V>(rk_u4(u0.x, tt.x, R.x, e1, c), rk_u4(u0.y, tt.y, R.y, e1, c));
 }
 #undef TS_RK_CPLX

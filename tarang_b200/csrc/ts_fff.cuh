@@ -344,6 +344,104 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
 
 
 // ---------------------------------------------------------------------------
+// inverse x pass, persistent with a prefetch (FP32, FORM 0 / 1): each block walks the
+// column tiles tile = blockIdx.x + k G; every thread stages the dealiased U rows it
+// owns (rows load_row(t, s) of its column) with cp.async into its own slots of a
+// staging tile, moves them to registers, issues the copies of its next tile into the
+// same slots (only it reads them, so no barrier is needed) and then transforms the
+// output fields of the current tile from registers while the next tile streams in.
+// Same result as k_inv_x_ld.  Shared memory: the staging tile (3 L CW) + the
+// exchange tile (L CW).
+// ---------------------------------------------------------------------------
+template <typename T, int L, int E, int CW, int FORM>
+__global__ void __launch_bounds__(CW * (L / E), 1)
+    k_inv_x_pf(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw, int kept) {
+  typedef C<T> V;
+  static_assert(FORM == 0 || FORM == 1, "the fluid forms");
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* xch = reinterpret_cast<V*>(smraw);  // exchange tile, L x CW
+  V* stg = xch + L * CW;                  // staging tile, 3 x L x CW
+  const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+  const int inner = g.Ny * g.Hz;
+  const long long rstride = inner;
+  const int qy = g.Ny / 3, nzk = g.Nz / 3 + 1, ntz = (nzk + CW - 1) / CW;
+  const int ntiles = kept ? (2 * qy + 1) * ntz : (inner + CW - 1) / CW;
+  // column of this thread in tile `tile` (the mapping of k_inv_x_ld's blocks)
+  auto column = [&](int tile, bool& ok) -> int {
+    if (kept) {
+      const int iy = tile / ntz, lzc = (tile % ntz) * CW + c;
+      const int ky = iy <= qy ? iy : iy - (2 * qy + 1);
+      ok = lzc < nzk;
+      return ((ky + g.Ny) % g.Ny) * g.Hz + (ok ? lzc : 0);
+    }
+    const int col = tile * CW + c;
+    ok = col < inner;
+    return ok ? col : 0;
+  };
+  auto issue = [&](int tile) {
+    if (tile < ntiles) {
+      bool ok;
+      const int col = column(tile, ok);
+      if (ok) {
+        const int ly = col / g.Hz, lz = col % g.Hz;
+#pragma unroll
+        for (int s = 0; s < E; ++s) {
+          const int lx = load_row<L, E>(t, s);
+          if (!dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz))
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cp_async(stg + (q * L + lx) * CW + c, U + q * g.S + lx * rstride + col);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  constexpr int nout = FORM == 0 ? 3 : 6;
+  issue(blockIdx.x);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait<0>();
+    bool ok;
+    const int col = column(tile, ok);
+    const int ly = col / g.Hz, lz = col % g.Hz;
+    const T Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
+    V u[3][E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int lx = load_row<L, E>(t, s);
+      const bool z = !ok || dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) u[q][s] = z ? mk<V>(0, 0) : stg[(q * L + lx) * CW + c];
+    }
+    // the slots are this thread's own: the next tile may stream into them now
+    issue(tile + gridDim.x);
+#pragma unroll
+    for (int f = 0; f < nout; ++f) {
+      V v[E];
+#pragma unroll
+      for (int s = 0; s < E; ++s) {
+        if (f < 3) {
+          v[s] = u[f][s];
+        } else {
+          // omega_i = i (K_{i+1} U_{i+2} - K_{i+2} U_{i+1})  (indices mod 3)
+          const int lx = load_row<L, E>(t, s);
+          const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
+          const int i = f - 3, i1 = i == 2 ? 0 : i + 1, i2 = i == 0 ? 2 : i - 1;
+          const T Ka = i1 == 0 ? Kx : (i1 == 1 ? Ky : Kz);
+          const T Kb = i2 == 0 ? Kx : (i2 == 1 ? Ky : Kz);
+          v[s] = mul_i<1>(sub(scale(u[i2][s], Ka), scale(u[i1][s], Kb)));
+        }
+      }
+      fft_regs<L, E, 1, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tw, 1);
+      if (ok) {
+        V* d = W + f * g.S + col;
+#pragma unroll
+        for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
+      }
+    }
+  }
+  cp_async_wait<0>();  // nothing in flight when the block leaves
+}
+
+// ---------------------------------------------------------------------------
 // z pass: C2R of the NIN input lines, real-space products, R2C of the NOUT
 // product lines.  Lines are contiguous (Hz = M+1 complex, M = Nz/2); a block
 // handles `nl` consecutive (x,y) lines of every component, with TPL = M/E
@@ -1135,7 +1233,6 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
   // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
   const double eh = a.ex[lx] * exy;
   const double e1 = eh * eh;
-  const Fac<T> Feh(eh), Fe1(e1);
   V* Uc = reinterpret_cast<V*>(a.Ucur);
   V* tot = reinterpret_cast<V*>(a.tot);
   const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
@@ -1146,18 +1243,18 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
     const V R = Rv[i];
     const V u0 = st0[i * sstr];
     if (a.stage == 1) {
-      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
-      tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
+      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
     } else {
       const V tt = st1[i * sstr];
       if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc_c(tt, R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc_c(tt, R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
       } else {
-        const V un = rk_u4_c(u0, tt, R, Fe1, (T)((1.0 / 6) * a.dt));
+        const V un = rk_u4_c(u0, tt, R, e1, (1.0 / 6) * a.dt);
         reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
         health_mark(nonfinite(un), a.err);
       }

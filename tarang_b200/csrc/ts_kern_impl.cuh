@@ -193,15 +193,19 @@ constexpr int ix_cw(int L) { return wide1024(L) ? 8 : cw_for(L, ix_e(L)); }
 constexpr int ix_e_alt(int L) {
   return std::is_same<T, float>::value ? (ix_e(L) == 8 ? (16 <= L ? 16 : 0) : 8) : (ix_e(L) > 4 ? ix_e(L) / 2 : 0);
 }
+// candidate 3 (FP32): the persistent prefetching kernel k_inv_x_pf, 8 elements per thread
+// (the three components of U held in registers), staging + exchange tiles (NT = 4 tiles)
 constexpr Tile ix_cand(int L, int v) {
   return v == 0 ? Tile{ix_e(L), ix_cw(L), 1}
        : v == 1 ? (ix_e_alt(L) > 0 ? Tile{ix_e_alt(L), cw_for(L, ix_e_alt(L)), 1} : Tile{0, 0, 0})
        : v == 2 ? (ix_cw(L) > 1 ? Tile{ix_e(L), ix_cw(L) / 2, 1} : Tile{0, 0, 0})
+       : v == 3 ? (std::is_same<T, float>::value ? Tile{8, cw_for(L, 8), 4} : Tile{0, 0, 0})
                 : Tile{0, 0, 0};
 }
 constexpr bool ix_valid(int L, int v) {
-  return v == 0 || (v < 3 && tile_fits(L, ix_cand(L, v), 1) && !tile_eq(ix_cand(L, v), ix_cand(L, 0)) &&
-                    (v < 2 || !tile_eq(ix_cand(L, v), ix_cand(L, 1))));
+  return v == 0 || (v < 4 && tile_fits(L, ix_cand(L, v), ix_cand(L, v).NT == 4 ? 4 : 1) &&
+                    !tile_eq(ix_cand(L, v), ix_cand(L, 0)) && (v < 2 || !tile_eq(ix_cand(L, v), ix_cand(L, 1))) &&
+                    (v < 3 || !tile_eq(ix_cand(L, v), ix_cand(L, 2))));
 }
 
 template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
@@ -211,6 +215,27 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
   const int v = form <= 1 ? g.tv[TUNE_X_INV] : 0;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
+    if constexpr (ix_valid(LL, 3)) {
+      if (v == 3) {
+        // persistent, prefetching form: one block per SM
+        constexpr Tile c = ix_cand(LL, 3);
+        constexpr int E = c.E, CW = c.CW;
+        const size_t sm = 4ull * LL * CW * sizeof(V);
+        const int nzk = g.Nz / 3 + 1;
+        const long long ntiles = kept ? (long long)(2 * (g.Ny / 3) + 1) * ((nzk + CW - 1) / CW)
+                                      : (long long)((g.Ny * g.Hz + CW - 1) / CW);
+        const unsigned blocks = (unsigned)(ntiles < 148 ? ntiles : 148);
+        auto run = [&](auto kern) {
+          if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
+          kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, kept);
+          ++g_launches;
+          err_ = cudaGetLastError();
+        };
+        if (form == 0) run(k_inv_x_pf<T, LL, E, CW, 0>);
+        else if (form == 1) run(k_inv_x_pf<T, LL, E, CW, 1>);
+        return;
+      }
+    }
     // the direct-load kernel measured faster than the TMA-staged k_inv_x on B200
     // (0.19 vs 0.28 ms at 256^3 FP32, rotational); k_inv_x stays available
     auto tile = [&](auto vc) {

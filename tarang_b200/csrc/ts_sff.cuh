@@ -258,21 +258,20 @@ __device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, lon
   for (int i = 0; i < 4; ++i) {
     const double eh = i < 3 ? ehu : eht;
     const double e1 = eh * eh;
-    const Fac<T> Feh(eh), Fe1(e1);
     const long long o = i * g.S + off;
     const V R = Rv[i];
     const V u0 = i < 3 ? U0[o] : T0[off];
     if (a.stage == 1) {
-      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
-      tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
+      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
     } else if (a.stage == 2) {
-      Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
-      tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+      Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+      tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
     } else if (a.stage == 3) {
-      Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
-      tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+      Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+      tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
     } else {
-      V un = rk_u4_c(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+      V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
       if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
       if (i < 3) const_cast<V*>(U0)[o] = un;
       else const_cast<V*>(T0)[off] = un;
@@ -457,21 +456,20 @@ __global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, 
     for (int i = 0; i < 4; ++i) {
       const double eh = i < 3 ? ehu : eht;
       const double e1 = eh * eh;
-      const Fac<T> Feh(eh), Fe1(e1);
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        V un = rk_u4_c(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+        V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(T0)[e] = un;
@@ -544,21 +542,20 @@ __global__ void __launch_bounds__(256, 3) k_mhd_epi(const C<T>* __restrict__ P, 
     for (int i = 0; i < 6; ++i) {
       const double eh = i < 3 ? ehu : ehb;
       const double e1 = eh * eh;
-      const Fac<T> Feh(eh), Fe1(e1);
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : B0[(i - 3) * g.S + e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        V un = rk_u4_c(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+        V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(B0)[(i - 3) * g.S + e] = un;
@@ -610,7 +607,6 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
     const V Rv[3] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1)};
     const double eh = a.ex[lx] * a.ey[ly] * a.ez[lz];
     const double e1 = eh * eh;
-    const Fac<T> Feh(eh), Fe1(e1);
     const bool dz = dealias_zero(g.dealias, 2, lx, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -618,16 +614,16 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
       const V R = Rv[i];
       const V u0 = U0[o];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const V un = rk_u4_c(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+        const V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         Uo[o] = un;
         health_mark(nonfinite(un), a.err);
       }
@@ -691,23 +687,22 @@ __global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g,
     const T Rv[3] = {-N1, -N2, -N3};
     const double eh = a.ex[lx] * a.ey[ly] * a.ez[lzr];
     const double e1 = eh * eh;
-    const Fac<T> Feh(eh), Fe1(e1);
     const bool dz = sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const long long o = i * per + e;
       const T R = Rv[i], u0 = U0[o];
       if (a.stage == 1) {
-        Uc[o] = rk_u1(dz ? (T)0 : u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_t1(R, Fe1, (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1(dz ? (T)0 : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3(u0, R, eh, a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const T un = rk_u4(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+        const T un = rk_u4(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         Uo[o] = un;
         health_mark(!isfinite(un), a.err);
       }
@@ -769,21 +764,20 @@ __global__ void __launch_bounds__(256) k_ssf_rbc_epi(const C<T>* __restrict__ P,
     for (int i = 0; i < 4; ++i) {
       const double eh = i < 3 ? ehu : eht;
       const double e1 = eh * eh;
-      const Fac<T> Feh(eh), Fe1(e1);
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_t1_c(R, Fe1, (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc_c(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const V un = rk_u4_c(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+        const V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
         health_mark(nonfinite(un), a.health);
@@ -833,20 +827,19 @@ __global__ void __launch_bounds__(256) k_sss_rbc_epi(const T* __restrict__ P, Ge
     for (int i = 0; i < 4; ++i) {
       const double eh = i < 3 ? ehu : eht;
       const double e1 = eh * eh;
-      const Fac<T> Feh(eh), Fe1(e1);
       const long long o = i * per + e;
       const T R = Rv[i], u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1(dz ? (T)0 : u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_t1(R, Fe1, (T)((1.0 / 6) * a.dt));
+        Uc[o] = rk_u1(dz ? (T)0 : u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_t1(R, e1, (1.0 / 6) * a.dt);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2(u0, R, Feh, (T)(0.5 * a.dt));
-        tot[o] = rk_tacc(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u2(u0, R, eh, 0.5 * a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3(u0, R, Feh, (T)(a.dt));
-        tot[o] = rk_tacc(tot[o], R, Feh, (T)((1.0 / 3) * a.dt));
+        Uc[o] = rk_u3(u0, R, eh, a.dt);
+        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
       } else {
-        const T un = rk_u4(u0, tot[o], R, Fe1, (T)((1.0 / 6) * a.dt));
+        const T un = rk_u4(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
         health_mark(!isfinite(un), a.health);

@@ -121,9 +121,10 @@ def test_set_tuning_rejects_missing_candidates(cuda):
         plan.set_tuning(with_class(2, 0, 2))  # z takes no blocks-per-SM count
     with pytest.raises(tb.TsError):
         plan.set_tuning(with_class(0, 7, 0))
-    assert 3 not in cand["x_inv"]["variants"]  # the FFF inverse x pass has three candidates
+    # the FFF inverse x pass has four candidates in FP32 (3: the prefetching kernel), none at 4
+    assert 3 in cand["x_inv"]["variants"] and 4 not in cand["x_inv"]["variants"]
     with pytest.raises(tb.TsError):
-        plan.set_tuning(with_class(0, 3, 0))
+        plan.set_tuning(with_class(0, 4, 0))
     assert plan.tuning() == {"variant": [0] * 5, "blocks_per_sm": [0] * 5}
 
 
