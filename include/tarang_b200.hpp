@@ -209,7 +209,7 @@ struct Time_advance_incompress {
   static void RK4(FluidVF& U, FluidVF& W, int nsteps = 1) {
     check(ts_rk4_step_mhd(U.basis().plan(), U.cvf(), W.cvf(), nsteps), "RK4");
   }
-  // RK4(U,T,P,F) (RK_SF.cc:97): RBC on the SFF basis (PRLARGE / ULARGE), or a
+  // RK4(U,T,P,F) (RK_SF.cc:97): RBC on the SFF basis (the plan's Pr_option / Uscaling), or a
   // passive scalar (kind SCALAR_INCOMPRESS, no force) on the FFF basis
   static void RK4(FluidVF& U, FluidSF& T, int nsteps = 1) {
     ts_plan* p = U.basis().plan();
@@ -219,7 +219,8 @@ struct Time_advance_incompress {
 };
 
 struct Correlation {
-  // Get_Nusselt_no (Correlation.cc:144-158, PRLARGE / ULARGE): 1 + 2 sqrt(Ra Pr) <U1, T>
+  // Get_Nusselt_no (Correlation.cc:144-176): nu0 + nuc <U1, T> with the factors of the plan's
+  // scaling (PRLARGE / ULARGE: 1 + 2 sqrt(Ra Pr) <U1, T>)
   static double Get_Nusselt_no(FluidVF& U, FluidSF& T) {
     double nu = 0;
     check(ts_nusselt(U.basis().plan(), U.cvf(), T.csf(), &nu), "Get_Nusselt_no");

@@ -166,16 +166,28 @@ class Grid:
             f = np.where(kz > 0, 1.0, 0.5)
             dbl = (kx == Nx // 2) | ((ky == Ny // 2) & (Ny > 1))
             return np.broadcast_to(np.where(dbl, 2 * f, f), self.shape).copy()
+        if self.basis in ("SSF", "SSS"):
+            # SSF_pencil_inline.h:512-532, SSS_pencil_inline.h:537-556: 1/2 at the origin, 1 with
+            # two zero indices, 2 with one, 4 with none (grid indices kx = lx, ly, lz)
+            zeros = (kx == 0).astype(int) + (ky == 0).astype(int) + (kz == 0).astype(int)
+            f = np.choose(np.minimum(zeros, 3), [4.0, 2.0, 1.0, 0.5])
+            return np.broadcast_to(f, self.shape).copy()
         m = kx
         f = np.where(kz > 0, np.where(m > 0, 2.0, 1.0), np.where(m > 0, 1.0, 0.5))
         dbl = (ky == Ny // 2) & (Ny > 1)
         return np.broadcast_to(np.where(dbl, 2 * f, f), self.shape).copy()
 
     def min_radius_outside(self):
+        """Min_radius_outside: FFF_pencil_inline.h:497-504, SFF_pencil_inline.h:423-430,
+        SSF_pencil_inline.h:444-451, SSS_pencil_inline.h:469-476."""
         Nx, Ny, Nz = self.N
         kf = self.kfactor
         if self.basis == "FFF":
             return int(math.ceil(math.sqrt((Nx // 2 * kf[0]) ** 2 + (Ny // 2 * kf[1]) ** 2 + (Nz // 2 * kf[2]) ** 2)))
+        if self.basis == "SSF":
+            return int(math.ceil(math.sqrt(((Nx - 1) * kf[0]) ** 2 + ((Ny - 1) * kf[1]) ** 2 + (Nz // 2 * kf[2]) ** 2)))
+        if self.basis == "SSS":
+            return int(math.ceil(math.sqrt(((Nx - 1) * kf[0]) ** 2 + ((Ny - 1) * kf[1]) ** 2 + ((Nz - 1) * kf[2]) ** 2)))
         return int(math.ceil(math.sqrt(((Nx - 1) * kf[0]) ** 2 + (Ny // 2 * kf[1]) ** 2 + (Nz // 2 * kf[2]) ** 2)))
 
     def n_shells(self):
@@ -675,15 +687,33 @@ def cross_energy(g: Grid, A: np.ndarray, B: np.ndarray) -> float:
     return float(2 * d.sum() - d[:, :, 0].sum() - d[0].sum() + 0.5 * d[0, :, 0].sum())
 
 
+def sss_complex_view(g: Grid, V: np.ndarray) -> tuple:
+    """The complex view the reference's shell loop takes of SSS real coefficients: the pair
+    (2 lz, 2 lz + 1) of a z line is one complex slot lz < Nz/2 (the loop runs over the complex
+    array shape, universal_energy.cc:276-306, with kz = Get_kz(lz) = lz); returns the
+    complex array and the Grid of that view (kz = 0 .. Nz/2 - 1)."""
+    Nx, Ny, Nz = g.N
+    A = V[..., 0:Nz:2] + 1j * V[..., 1:Nz:2]
+    gc = Grid(g.N, g.kfactor, "SSS")
+    gc.kz = np.arange(Nz // 2)
+    return A, gc
+
+
 def shell_spectrum(g: Grid, V: np.ndarray, n: int = 0) -> np.ndarray:
     """Compute_shell_spectrum per component and summed (universal_energy.cc:279-366).
 
     Sk(ceil|K|) += mult |K|^n |A|^2 |K|^2; count += 2 mult; Sk *= 4 pi /(count kf1 kf2 kf3).
+    SSS: over the complex view of the real coefficients (``sss_complex_view``).
     """
+    if g.basis == "SSS":
+        V, gc = sss_complex_view(g, V)
+        kmax = g.min_radius_outside()
+        g = gc
+    else:
+        kmax = g.min_radius_outside()
     Kmag = g.Kmag()
     idx = np.ceil(Kmag).astype(np.int64)
-    kmax = g.min_radius_outside()
-    mult = g.multiplicity()
+    mult = np.broadcast_to(g.multiplicity(), Kmag.shape) if g.basis != "SSS" else _sss_mult(g)
     ok = idx <= kmax
     nsh = kmax + 1
     count = np.bincount(idx[ok], weights=2 * mult[ok], minlength=nsh)
@@ -696,6 +726,15 @@ def shell_spectrum(g: Grid, V: np.ndarray, n: int = 0) -> np.ndarray:
             Sk = np.where(count > 0, Sk * 4 * math.pi / (count * kf[0] * kf[1] * kf[2]), 0.0)
         out += Sk
     return out
+
+
+def _sss_mult(g: Grid) -> np.ndarray:
+    """SSS Multiplicity_factor on the complex view (kz = lz < Nz/2)."""
+    kx = g.kx[:, None, None]
+    ky = g.ky[None, :, None]
+    kz = g.kz[None, None, :]
+    zeros = (kx == 0).astype(int) + (ky == 0).astype(int) + (kz == 0).astype(int)
+    return np.choose(np.minimum(zeros, 3), [4.0, 2.0, 1.0, 0.5]).astype(np.float64)
 
 
 def shell_mult_single(g: Grid, A: np.ndarray, B: np.ndarray, inner: float, outer: float) -> float:

@@ -222,9 +222,15 @@ static void compute_modes_in_shell(ts_plan* p) {
   // Compute_modes_in_shell_array (universal_basic.cc:104-143): full box count
   const int Nx = p->g.Nx, Ny = p->g.Ny, Nz = p->g.Nz;
   const double* kf = p->g.kf;
+  // Min_radius_outside of the basis (FFF_pencil_inline.h:497-504, SFF_pencil_inline.h:423-430,
+  // SSF_pencil_inline.h:444-451, SSS_pencil_inline.h:469-476)
   int kmax;
   if (p->g.basis == 0)
     kmax = (int)ceil(sqrt(pow((Nx / 2) * kf[0], 2) + pow((Ny / 2) * kf[1], 2) + pow((Nz / 2) * kf[2], 2)));
+  else if (p->g.basis == 2)
+    kmax = (int)ceil(sqrt(pow((Nx - 1) * kf[0], 2) + pow((Ny - 1) * kf[1], 2) + pow((Nz / 2) * kf[2], 2)));
+  else if (p->g.basis == 3)
+    kmax = (int)ceil(sqrt(pow((Nx - 1) * kf[0], 2) + pow((Ny - 1) * kf[1], 2) + pow((Nz - 1) * kf[2], 2)));
   else
     kmax = (int)ceil(sqrt(pow((Nx - 1) * kf[0], 2) + pow((Ny / 2) * kf[1], 2) + pow((Nz / 2) * kf[2], 2)));
   p->nshells = kmax + 1;
@@ -1363,7 +1369,6 @@ int ts_max_div(ts_plan* p, const void* u_hat, double* max_div) {
 }
 
 int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int n_shells) {
-  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || !Ek || ncomp < 1 || ncomp > 3 || n_shells < 1) return TS_ERR_ARG;
   const int nsh = p->nshells;
   return with_device(p, &p->stage_u, a_hat, (size_t)ncomp * p->g.S * p->cb, false, [&](void* A) -> int {
@@ -1385,7 +1390,6 @@ int ts_shell_spectrum(ts_plan* p, const void* a_hat, int ncomp, double* Ek, int 
 
 int ts_shell_sums(ts_plan* p, const void* a_hat, const void* b_hat, int ncomp, double* sums, double* counts,
                   int n_shells) {
-  if (p && (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS)) return ssf_transforms_only();
   if (!p || !a_hat || ncomp < 1 || ncomp > 3 || n_shells < 1 || (!sums && !counts)) return TS_ERR_ARG;
   if (!is_device_ptr(a_hat) || (b_hat && !is_device_ptr(b_hat))) {
     g_last_error = "ts_shell_sums: device pointers required";

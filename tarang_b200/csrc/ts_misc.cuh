@@ -271,7 +271,13 @@ __global__ void k_maxdiv(const C<T>* __restrict__ U, Geo g, unsigned long long* 
 }
 
 // multiplicity factor (FFF_pencil_inline.h:583-602, SFF_pencil_inline.h:492-515)
+// SSF / SSS (SSF_pencil_inline.h:512-532, SSS_pencil_inline.h:537-556): 1/2 at the
+// origin, 1 with two zero grid indices, 2 with one, 4 with none (indices lx, ly, lz)
 __device__ __forceinline__ double multiplicity(int basis, int lx, int ly, int lz, int Nx, int Ny) {
+  if (basis >= 2) {
+    const int zeros = (lx == 0) + (ly == 0) + (lz == 0);
+    return zeros == 0 ? 4.0 : zeros == 1 ? 2.0 : zeros == 2 ? 1.0 : 0.5;
+  }
   const int ky = kfft(ly, Ny);
   double f;
   if (basis == 0) {
@@ -285,8 +291,8 @@ __device__ __forceinline__ double multiplicity(int basis, int lx, int ly, int lz
   return f;
 }
 
-// Shell spectrum accumulation (Compute_local_shell_spectrum universal_energy.cc:279-313):
-// for every shell s = ceil|K| < nbins, sums[s] = sum mult |K|^2 sum_i Re(A_i conj(B_i)) (B = A:
+// Shell spectrum accumulation (Compute_local_shell_spectrum universal_energy.cc:279-313), on
+// every basis over the complex array shape: for every shell s = ceil|K| < nbins, sums[s] = sum mult |K|^2 sum_i Re(A_i conj(B_i)) (B = A:
 // |A|^2) and counts[s] = sum 2 mult.  Reproducible bit for bit, without atomics on the sums:
 // each warp walks whole z lines (|K| grows along a line, so the modes of one shell sit in
 // adjacent lanes of a 32-mode chunk), adds a chunk by a segmented scan whose segment tails
@@ -309,12 +315,15 @@ __global__ void __launch_bounds__(32 * SHELL_WARPS)
        line += (long long)gridDim.x * SHELL_WARPS) {
     const int lx = (int)(line / g.Ny), ly = (int)(line % g.Ny);
     const double Kx = (g.basis == 0 ? kfft(lx, g.Nx) : lx) * g.kf[0];
-    const double Ky = kfft(ly, g.Ny) * g.kf[1];
+    const double Ky = (g.basis >= 2 ? ly : kfft(ly, g.Ny)) * g.kf[1];
+    // SSS: the complex view of the real coefficients, pair (2 lz, 2 lz + 1) as slot lz < Nz/2
+    // with kz = lz (the padding slot lz = Nz/2 is not a mode)
+    const int nz = g.basis == 3 ? g.Nz / 2 : g.Hz;
     for (int z0 = 0; z0 < g.Hz; z0 += 32) {
       const int lz = z0 + lane;
       int key = 0x7fffffff;
       double v = 0, c = 0;
-      if (lz < g.Hz) {
+      if (lz < nz) {
         const double Kz = lz * g.kf[2];
         const double Kmag = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz);
         const int idx = (int)ceil(Kmag);
