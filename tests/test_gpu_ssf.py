@@ -51,8 +51,6 @@ def test_ssf_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSF", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.shell_spectrum(u, 3)
-    with pytest.raises(tb.TsError):
         plan.rk4_step_scalar(u, plan.field(1), 1)   # the passive-scalar step is FFF only
     with pytest.raises(tb.TsError):
         plan.rk4_step_mhd(u, plan.field(3), 1)
@@ -197,3 +195,33 @@ def test_ssf_max_div_matches_oracle(cuda):
     assert abs(plan.max_div(torch.from_numpy(V).to(cuda)) / R.max_abs_div(g, V) - 1) < 1e-12
     W = -R.project_rhs(g, V)
     assert plan.max_div(torch.from_numpy(W).to(cuda)) < 1e-12 * R.max_abs_div(g, V)
+
+
+@pytest.mark.parametrize("basis,N", [("SSF", (16, 32, 16)), ("SSF", (32, 16, 32)), ("SSS", (16, 32, 16)),
+                                     ("SSS", (32, 16, 32))])
+def test_sincos_shell_spectrum_matches_oracle(cuda, basis, N):
+    """E(k) on SSF and SSS: the reference's shell loop over the complex array shape
+    (universal_energy.cc:276-306) with the basis's grid wavenumbers (kx = lx, ky = ly, kz = lz),
+    Multiplicity_factor (4 / 2 / 1 / 1/2) and Min_radius_outside; on SSS each pair of real z
+    coefficients is one complex slot at kz = lz.  FP64 <= 1e-13, FP32 <= 1e-6."""
+    import torch
+    import tarang_b200 as tb
+    kf = (math.pi, math.pi / math.sqrt(2.0), 0.7 * math.pi)
+    g = R.Grid(N, kf, basis)
+    rng = np.random.default_rng(4)
+    par = ("SCF", "CSF", "CCF") if basis == "SSF" else ("SCC", "CSC", "CCS")
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), p) for p in par])
+    ref = R.shell_spectrum(g, U)
+    for prec, tol in (("f64", 1e-13), ("f32", 1e-6)):
+        plan = tb.Plan(N, basis=basis, precision=prec, kfactor=kf)
+        assert plan.n_shells == len(ref)
+        if basis == "SSS":
+            P = np.zeros((3, N[0], N[1], N[2] + 2))
+            P[..., :N[2]] = U
+            u = torch.view_as_complex(torch.from_numpy(P.reshape(3, N[0], N[1], N[2] // 2 + 1, 2)).to(
+                torch.float64 if prec == "f64" else torch.float32).contiguous()).to(cuda)
+        else:
+            u = torch.from_numpy(U).to(cuda).to(plan.torch_dtype())
+        got = plan.shell_spectrum(u)
+        assert rel(got, ref) < tol, (prec, rel(got, ref))
+        plan.close()

@@ -52,8 +52,6 @@ def test_sss_plan_rejects_other_calls(cuda):
     plan = tb.Plan(32, basis="SSS", kfactor=KF)
     u = plan.field(3)
     with pytest.raises(tb.TsError):
-        plan.shell_spectrum(u, 3)
-    with pytest.raises(tb.TsError):
         tb.Plan(32, basis="SSS", kfactor=KF, nlin_form="rotational")
     with pytest.raises(tb.TsError):
         plan.forward(plan.field(1), plan.field(1), parity="SCF")
