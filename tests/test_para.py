@@ -572,3 +572,43 @@ def test_read_para_rbc_scalings(tmp_path, pr, us):
     (tmp_path / "in" / "para.yaml").write_text(text.replace("Pr_option: PRLARGE", "Pr_option: PRZERO"))
     with pytest.raises(NotImplementedError):
         para.read_para(str(tmp_path / "in" / "para.yaml"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sign", [1, -1])
+def test_glob_helicity_of_a_beltrami_mode(cuda, tmp_path, sign):
+    """Known answer for the helicity columns, with a non-unit kfactor: one Beltrami mode stored
+    as V = a (1, sign i, 0) at (kx, ky, kz) = (0, 0, 3), i.e. u = 2a (cos Kz z, -sign sin Kz z, 0),
+    whose vorticity is sign Kz u; the reference's helicity 1/2 <u . omega> (FFF_pencil_energy.cc:
+    99-139) is then H1 = sign Kz E and H2 = H1 / Kz^2 = sign E / Kz, E the Tarang energy,
+    Kz = 3 kfactor_z; then an oblique mode (ky = 2, kz = 1) with |K| from both kfactors."""
+    import torch
+    import tarang_b200 as tb
+    kf = (1.0, 2.0, 1.5)
+    plan = tb.Plan((16, 16, 16), precision="f64", kfactor=kf, dealias="none")
+    u = plan.field(3)
+    a = 0.3
+    u[0, 0, 0, 3] = a
+    u[1, 0, 0, 3] = sign * 1j * a
+    out = para.Output(plan, str(tmp_path))
+    row = out.glob(u, 0.0, 1e-3, helicity=True)
+    E = plan.energy(u)
+    Kz = 3 * kf[2]
+    assert abs(E - 2 * a * a) < 1e-15
+    assert abs(row[1] - E) < 1e-15
+    assert abs(row[3] - sign * Kz * E) < 1e-14
+    assert abs(row[4] - sign * E / Kz) < 1e-14
+    # a mode along y (ky = 2, kz = 1): K = (0, 2 kf_y, kf_z); a Beltrami vector e1 + sign i e2 with
+    # e1, e2 unit vectors perpendicular to K and e1 x e2 = K / |K|
+    u.zero_()
+    K = np.array([0.0, 2 * kf[1], 1 * kf[2]])
+    Km = np.linalg.norm(K)
+    e1 = np.array([1.0, 0.0, 0.0])
+    e2 = np.cross(K / Km, e1)
+    V = a * (e1 + sign * 1j * e2)
+    for i in range(3):
+        u[i, 0, 2, 1] = complex(V[i])
+    row = out.glob(u, 0.0, 1e-3, helicity=True)
+    E = plan.energy(u)
+    assert abs(row[3] - sign * Km * E) < 1e-13 * Km * E
+    assert abs(row[4] - sign * E / Km) < 1e-13 * E / Km
