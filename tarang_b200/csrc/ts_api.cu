@@ -1750,9 +1750,15 @@ struct ts_ensemble {
   cudaEvent_t fork = nullptr;
   cudaStream_t origin = nullptr;
   bool own_origin = false;
-  cudaGraph_t graph = nullptr;
+  cudaGraph_t graph = nullptr;      // one ensemble step
   cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graphK = nullptr;     // kEnsSteps ensemble steps, each group a chain of its own
+  cudaGraphExec_t execK = nullptr;
 };
+// ensemble steps per launch of the multi-step graph: the size groups advance this many
+// steps between one fork and one join, so a group does not wait for the slowest one
+// after every step
+constexpr int kEnsSteps = 8;
 
 // one IF-RK4 step of every member of a group (step_rbc with member strides)
 static int step_rbc_group(ens_group& G) {
@@ -1811,6 +1817,8 @@ int ts_ensemble_destroy(ts_ensemble* e) {
   if (!e) return TS_ERR_ARG;
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->execK) cudaGraphExecDestroy(e->execK);
+  if (e->graphK) cudaGraphDestroy(e->graphK);
   for (ens_group& G : e->groups) {
     void* bufs[] = {G.U, G.T, G.Ucur, G.tot, G.P, G.eu, G.et};
     for (void* b : bufs)
@@ -1932,32 +1940,39 @@ int ts_ensemble_init_temperature(ts_ensemble* e, double amp, double kmax, uint64
   return TS_OK;
 }
 
+// captures `steps` ensemble steps into one graph: a fork on the origin stream, each
+// size group's steps as one chain on its own stream, a join
+static int ens_capture(ts_ensemble* e, int steps, cudaGraph_t* graph_out, cudaGraphExec_t* exec_out) {
+  for (ts_plan* p : e->plans) p->prof = false;
+  CK(cudaDeviceSynchronize());
+  CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeRelaxed));
+  int rc = TS_OK;
+  cudaEventRecord(e->fork, e->origin);
+  for (size_t k = 0; k < e->groups.size() && rc == TS_OK; ++k) {
+    ens_group& G = e->groups[k];
+    cudaStreamWaitEvent(G.st, e->fork, 0);
+    for (int s = 0; s < steps && rc == TS_OK; ++s) rc = step_rbc_group(G);
+    cudaEventRecord(G.done, G.st);
+    cudaStreamWaitEvent(e->origin, G.done, 0);
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);
+  if (rc != TS_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  CK(ce);
+  *graph_out = graph;
+  CK(cudaGraphInstantiate(exec_out, graph, 0));
+  return TS_OK;
+}
+
 int ts_ensemble_run(ts_ensemble* e, int nsteps) {
   if (!e || nsteps < 0) return TS_ERR_ARG;
-  if (!e->exec) {
-    for (ts_plan* p : e->plans) p->prof = false;
-    CK(cudaDeviceSynchronize());
-    CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeRelaxed));
-    int rc = TS_OK;
-    cudaEventRecord(e->fork, e->origin);
-    for (size_t k = 0; k < e->groups.size() && rc == TS_OK; ++k) {
-      ens_group& G = e->groups[k];
-      cudaStreamWaitEvent(G.st, e->fork, 0);
-      rc = step_rbc_group(G);
-      cudaEventRecord(G.done, G.st);
-      cudaStreamWaitEvent(e->origin, G.done, 0);
-    }
-    cudaGraph_t graph = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);
-    if (rc != TS_OK) {
-      if (graph) cudaGraphDestroy(graph);
-      return rc;
-    }
-    CK(ce);
-    e->graph = graph;
-    CK(cudaGraphInstantiate(&e->exec, e->graph, 0));
-  }
-  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(e->exec, e->origin));
+  if (nsteps >= kEnsSteps && !e->execK) CKS(ens_capture(e, kEnsSteps, &e->graphK, &e->execK));
+  if (nsteps % kEnsSteps && !e->exec) CKS(ens_capture(e, 1, &e->graph, &e->exec));
+  for (int s = 0; s < nsteps / kEnsSteps; ++s) CK(cudaGraphLaunch(e->execK, e->origin));
+  for (int s = 0; s < nsteps % kEnsSteps; ++s) CK(cudaGraphLaunch(e->exec, e->origin));
   return TS_OK;
 }
 
@@ -2160,8 +2175,12 @@ void copy_report(const std::string& js, char* report, size_t len) {
 void ens_invalidate(ts_ensemble* e) {
   if (e->exec) cudaGraphExecDestroy(e->exec);
   if (e->graph) cudaGraphDestroy(e->graph);
+  if (e->execK) cudaGraphExecDestroy(e->execK);
+  if (e->graphK) cudaGraphDestroy(e->graphK);
   e->exec = nullptr;
   e->graph = nullptr;
+  e->execK = nullptr;
+  e->graphK = nullptr;
 }
 
 }  // namespace
