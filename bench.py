@@ -827,6 +827,14 @@ def main():
             p64.close()
         extras["max_div_end"] = plan.max_div(u)
         extras["energy_end"] = plan.energy(u)
+        if args.precision == "f32" and world == 1:
+            # config 1's error report over the full 2000-step run (FP32 vs the FP64 GPU run)
+            tr = c1_trajectory_leg(steps=2000, every=100, N=N, form=args.form)
+            extras["c1_fp32_vs_fp64_2000_steps"] = {
+                "final": tr["final"], "first_step_rel_l2_above_1e-5": tr["first_step_rel_l2_above_1e-5"],
+                "first_step_rel_energy_above_1e-5": tr["first_step_rel_energy_above_1e-5"],
+                "max_div_f32_max": tr["max_div_f32_max"], "columns": tr["columns"], "every_100_steps": tr["series"],
+                "wall_s": tr["wall_s"]}
         # config 3: the RBC ensemble (all ranks; members shared out by N^3)
         plan.close()
         torch.cuda.empty_cache()

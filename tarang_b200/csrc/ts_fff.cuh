@@ -1435,18 +1435,42 @@ __global__ void __launch_bounds__(256) k_spec_epi(const C<T>* __restrict__ P, Ge
   const T inv = (T)(1.0 / ((double)g.Nx * g.Ny * g.Nz));
   const V* st0 = reinterpret_cast<const V*>(MODE == MODE_FLUX ? a.Ud : a.U0);
   const V* st1 = reinterpret_cast<const V*>(a.tot);
+  // the state fields the epilogue reads at this stage (U0 / Lam / the flux field; tot)
+  const bool ld0 = MODE != MODE_NLIN && !(MODE == MODE_ADJ && a.stage == 1);
+  const bool ld1 = (MODE == MODE_STEP && a.stage > 1) || (MODE == MODE_ADJ && a.stage != 4);
+  // two elements per thread and iteration (e and e + stride): every load of both is
+  // issued before either is used, twice the loads in flight of one element at a time
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
-    const int lz = (int)(e % g.Hz);
-    const long long r = e / g.Hz;
-    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
-    const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]), Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
-    V a0 = mk<V>(0, 0), a1 = mk<V>(0, 0), a2 = mk<V>(0, 0);
+  for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < g.S; e0 += 2 * stride) {
+    const bool has1 = e0 + stride < g.S;
+    V pv[2][NF], s0[2][3], s1[2][3];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) accum_product<FORM>(f, scale(P[f * g.S + e], inv), Kx, Ky, Kz, a0, a1, a2);
-    const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
-    spec_epilogue<T, MODE>(g, a, lx, ly, lz, e, exy, a0, a1, a2, st0 ? st0 + e : nullptr,
-                           st1 ? st1 + e : nullptr, g.S, tb);
+    for (int j = 0; j < 2; ++j) {
+      const long long e = e0 + j * stride;
+      if (j == 0 || has1) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) pv[j][f] = P[f * g.S + e];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          s0[j][i] = ld0 ? st0[i * g.S + e] : mk<V>(0, 0);
+          s1[j][i] = ld1 ? st1[i * g.S + e] : mk<V>(0, 0);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const long long e = e0 + j * stride;
+      if (j == 1 && !has1) break;
+      const int lz = (int)(e % g.Hz);
+      const long long r = e / g.Hz;
+      const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+      const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]), Ky = (T)(kfft(ly, g.Ny) * g.kf[1]), Kz = (T)(lz * g.kf[2]);
+      V a0 = mk<V>(0, 0), a1 = mk<V>(0, 0), a2 = mk<V>(0, 0);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) accum_product<FORM>(f, scale(pv[j][f], inv), Kx, Ky, Kz, a0, a1, a2);
+      const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
+      spec_epilogue<T, MODE>(g, a, lx, ly, lz, e, exy, a0, a1, a2, s0[j], s1[j], 1, tb);
+    }
   }
   if (MODE == MODE_FLUX) {
     for (int i = 0; i <= a.nradii; ++i) {
