@@ -402,7 +402,7 @@ def adjoint_leg(prec: str, N: int = 128, window: int = 20, reps: int = 3):
     lam = plan.field(3)
     plan.init_energy_spectrum(tb.spectrum_k4_gauss(plan.n_shells, 4.0), 1, 0.5, lam)
     st = torch.empty((9,) + plan.spec_shape, dtype=u.dtype, device=u.device)
-    un = torch.empty_like(u)
+    un = u.clone()
     work = torch.empty(plan.adjoint_work_bytes(window), dtype=torch.uint8, device=u.device)
 
     def timed(fn, n):
