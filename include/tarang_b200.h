@@ -62,8 +62,11 @@ typedef enum { TS_DEALIAS_NONE = 0, TS_DEALIAS_REFERENCE_CORNER = 1, TS_DEALIAS_
 typedef enum { TS_FORCE_NONE = 0, TS_FORCE_CARATI_ENERGY_SUPPLY = 1, TS_FORCE_RBC = 51 } ts_force;
 /* PHYSICS.Pr_option and PHYSICS.Uscaling of an RBC run (Global_read.cc; the
  * coefficients of compute_force_RBC.cc:104-150 and Correlation.cc:144-176).  PRZERO and
- * PRINFTY (one field slaved to the other, Tadvance_functions.cc:380-395) are refused
- * with TS_ERR_UNSUPPORTED. */
+ * PRINFTY slave one field to the other (Single_time_step_RBC, Tadvance_functions.cc:
+ * 380-395): under PRZERO only U is advanced and T = U.V1 / K^2 after every stage; under
+ * PRINFTY only T is advanced and U = vs P(T x) / K^2 (FluidVF.cc:228-272).  They step on
+ * SFF plans (ts_rk4_step_rbc); SSF / SSS plans and ensembles refuse them with
+ * TS_ERR_UNSUPPORTED. */
 typedef enum { TS_PR_LARGE = 0, TS_PR_SMALL = 1, TS_PR_ZERO = 2, TS_PR_INFTY = 3 } ts_pr_option;
 typedef enum { TS_U_LARGE = 0, TS_U_SMALL = 1 } ts_uscaling;
 
@@ -210,9 +213,16 @@ int ts_force_field(ts_plan* plan, const void* u_hat, void* f_hat);
 /* max |div U| (universal_basic.cc:343-356), with the basis's derivatives (SSF / SSS:
  * sine +K, cosine -K along the sin/cos axes; SSS padding reals skipped). */
 int ts_max_div(ts_plan* plan, const void* u_hat, double* max_div);
-/* Nusselt number, PRLARGE/ULARGE (Correlation.cc:154-156): 1 + 2 sqrt(Ra Pr) <U1, T>,
- * on SFF, SSF and SSS plans. */
+/* Nusselt number nu0 + nuc <U1, T> with the factors of the plan's scaling
+ * (Correlation.cc:144-176; PRLARGE/ULARGE: 1 + 2 sqrt(Ra Pr) <U1, T>; PRZERO reports
+ * 2 <U1, T>), on SFF, SSF and SSS plans. */
 int ts_nusselt(ts_plan* plan, const void* u_hat, const void* T_hat, double* Nu);
+/* The slaved field of a PRZERO / PRINFTY state on an SFF plan, in place: PRZERO sets
+ * T_hat = U.V1 / K^2 (Zero_Prandtl_number_compute_temperature, FluidVF.cc:228-232);
+ * PRINFTY sets u_hat = vs P(T x) / K^2 (Infinite_Prandtl_number_compute_velocity,
+ * FluidVF.cc:235-272) -- what the reference does after an initial condition
+ * (init_cond_energy.cc:242-258).  TS_ERR_ARG for the other scalings. */
+int ts_rbc_slave(ts_plan* plan, void* u_hat, void* T_hat);
 
 /* Random-phase solenoidal FFF field with shell energies E_ic[n] (construction of
  * init_cond_energy.cc:67-120; counter-based splitmix64 phases from seed), then the
@@ -220,12 +230,13 @@ int ts_nusselt(ts_plan* plan, const void* u_hat, const void* T_hat, double* Nu);
 int ts_init_energy_spectrum(ts_plan* plan, const double* E_ic, int n, uint64_t seed, double target_energy,
                             void* u_hat);
 
-/* Ensemble of independent Boussinesq (RBC, SFF, PRLARGE/ULARGE) runs of uneven
- * sizes: a batching layer with no reference counterpart (the reference runs one
- * field per MPI job).  Each member has its own plan (N, Ra, Pr; nu = sqrt(Pr/Ra),
- * kappa = 1/sqrt(Pr Ra)) and device state; the other settings come from `base`.
- * ts_ensemble_run advances every member by nsteps; each ensemble step is one
- * CUDA graph launch whose parallel branches are the members' step sequences.
+/* Ensemble of independent Boussinesq (RBC, SFF) runs of uneven sizes: a batching
+ * layer with no reference counterpart (the reference runs one field per MPI job).
+ * Each member has its own plan (N, Ra, Pr; nu and kappa of base.Pr_option / base.Uscaling,
+ * PRLARGE or PRSMALL: PRZERO / PRINFTY return TS_ERR_UNSUPPORTED) and device state; the
+ * other settings come from `base`.  Members of one grid size advance as one batch;
+ * ts_ensemble_run advances every member by nsteps with one CUDA graph launch per eight
+ * steps (plus one per remaining step), whose parallel branches are the size groups.
  * Asynchronous: ts_ensemble_synchronize / ts_ensemble_nusselt wait for it. */
 typedef struct {
   int N[3];

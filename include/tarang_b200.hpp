@@ -126,6 +126,8 @@ class SSS_PENCIL : public Universal {
 
 // Velocity field: cvf (V1, V2, V3) and nlin (nlin1..3), each a contiguous
 // device block of 3 components.
+class FluidSF;
+
 class FluidVF {
  public:
   explicit FluidVF(Universal& basis) : basis_(basis) {
@@ -160,6 +162,9 @@ class FluidVF {
   }
   void Copy_to_host(void* host) { cudaMemcpy(host, cvf_, bytes_, cudaMemcpyDeviceToHost); }
   void Copy_from_host(const void* host) { cudaMemcpy(cvf_, host, bytes_, cudaMemcpyHostToDevice); }
+  // the slaved field of a PRZERO / PRINFTY run (FluidVF.cc:228-272); defined after FluidSF
+  inline void Zero_Prandtl_number_compute_temperature(FluidSF& T);
+  inline void Infinite_Prandtl_number_compute_velocity(FluidSF& T);
 
  private:
   Universal& basis_;
@@ -200,6 +205,15 @@ class FluidSF {
   void* csf_ = nullptr;
   size_t bytes_ = 0;
 };
+
+// T = U.V1 / K^2 (the plan's Pr_option must be PRZERO)
+inline void FluidVF::Zero_Prandtl_number_compute_temperature(FluidSF& T) {
+  check(ts_rbc_slave(basis_.plan(), cvf_, T.csf()), "Zero_Prandtl_number_compute_temperature");
+}
+// U = vs P(T x) / K^2 (the plan's Pr_option must be PRINFTY)
+inline void FluidVF::Infinite_Prandtl_number_compute_velocity(FluidSF& T) {
+  check(ts_rbc_slave(basis_.plan(), cvf_, T.csf()), "Infinite_Prandtl_number_compute_velocity");
+}
 
 struct Time_advance_incompress {
   // RK4(U,P,F) + strong reality condition when the plan enables it (RK.cc:91-170, Time_advance.cc:59-60)

@@ -866,10 +866,19 @@ def rbc_coefficients(pr_option: str, uscaling: str, Ra: float, Pr: float) -> dic
 
     * nu, kappa: diss_coefficients (src/solvers/iscalar/Iscalar_main.cc:52-92);
     * cu, cT: U.Force1 += cu T and T.Force += cT U.V1 (compute_force_RBC.cc:104-150);
-    * nu0, nuc: Nu = nu0 + nuc <U.V1, T> (Correlation::Get_Nusselt_no, Correlation.cc:144-176).
+    * nu0, nuc: Nu = nu0 + nuc <U.V1, T> (Correlation::Get_Nusselt_no, Correlation.cc:144-176);
+    * vs: PRINFTY only, the factor of the slaved velocity (FluidVF.cc:259-271).
 
-    PRZERO (T slaved to U) and PRINFTY (U slaved to T) change the step itself
-    (Single_time_step_RBC, Tadvance_functions.cc:380-395) and are not restated here."""
+    PRZERO (T slaved to U: only U is advanced, kappa = 0, no T force) and PRINFTY (U slaved
+    to T: only T is advanced, no U force) step through rbc_rk4_step_slaved."""
+    if pr_option == "PRZERO":
+        # PRZERO shares the PRSMALL branch of the buoyancy; Nu reports 2 <U.V1, T> (no 1 +)
+        return dict(nu=1.0, kappa=0.0, cu=Ra if uscaling == "USMALL" else Pr, cT=0.0, nu0=0.0, nuc=2.0)
+    if pr_option == "PRINFTY":
+        if uscaling == "USMALL":
+            return dict(nu=Pr, kappa=1.0, cu=0.0, cT=1.0, nu0=1.0, nuc=2.0, vs=Ra)
+        return dict(nu=1.0 / math.sqrt(Ra), kappa=1.0 / math.sqrt(Ra), cu=0.0, cT=1.0, nu0=1.0,
+                    nuc=2.0 * math.sqrt(Ra), vs=math.sqrt(Ra))
     if pr_option == "PRLARGE":
         if uscaling == "USMALL":
             return dict(nu=Pr, kappa=1.0, cu=Ra * Pr, cT=1.0, nu0=1.0, nuc=2.0)
@@ -880,7 +889,33 @@ def rbc_coefficients(pr_option: str, uscaling: str, Ra: float, Pr: float) -> dic
             return dict(nu=1.0, kappa=1.0 / Pr, cu=Ra, cT=1.0 / Pr, nu0=1.0, nuc=2.0 * Pr ** 2)
         return dict(nu=math.sqrt(Pr / Ra), kappa=1.0 / math.sqrt(Pr * Ra), cu=Pr, cT=1.0 / Pr, nu0=1.0,
                     nuc=2.0 * Pr * math.sqrt(Ra * Pr))
-    raise NotImplementedError(f"Pr_option {pr_option}: PRLARGE and PRSMALL are restated")
+    raise ValueError(f"Pr_option {pr_option}")
+
+
+def divide_ksqr(g: Grid, A: np.ndarray) -> np.ndarray:
+    """Array_divide_ksqr (universal_basic.cc:202-225): A / K^2 with A(0,0,0) = 0."""
+    K2 = g.Ksqr()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        B = A / K2
+    B[0, 0, 0] = 0.0
+    return B
+
+
+def rbc_slave_temperature(g: Grid, U: np.ndarray) -> np.ndarray:
+    """Zero_Prandtl_number_compute_temperature (FluidVF.cc:228-232): T = U.V1 / K^2."""
+    return divide_ksqr(g, U[0])
+
+
+def rbc_slave_velocity(g: Grid, T: np.ndarray, vs: float) -> np.ndarray:
+    """Infinite_Prandtl_number_compute_velocity (FluidVF.cc:235-272): X = Dx(T) / K^2 (T with
+    the Vx parity), V2 = Dy(X) / K^2, V3 = Dz(X) / K^2, V1 = (Dx(X) + T) / K^2 (X with the
+    divergence parity), all times vs (sqrt(Ra) for ULARGE, Ra for USMALL)."""
+    p = lambda k: _par(g, k)
+    X = divide_ksqr(g, xderiv(g, T, p("Vx")))
+    V2 = divide_ksqr(g, yderiv(g, X, p("div")))
+    V3 = divide_ksqr(g, zderiv(g, X, p("div")))
+    V1 = divide_ksqr(g, xderiv(g, X, p("div")) + T)
+    return vs * np.stack([V1, V2, V3])
 
 
 @dataclass
@@ -951,6 +986,8 @@ def rbc_rhs(cfg, U: np.ndarray, T: np.ndarray) -> tuple:
 def rbc_rk4_step(cfg, U0: np.ndarray, T0: np.ndarray) -> tuple:
     """RK4(U,T,P,F) RK_SF.cc:97-221 with Single_time_step_scalar (U with nu, T with kappa);
     an RBCConfig (SFF, SSF or SSS, buoyancy) or a ScalarConfig (passive scalar)."""
+    if getattr(cfg, "pr_option", "") in ("PRZERO", "PRINFTY"):
+        return rbc_rk4_step_slaved(cfg, U0, T0)
     g = cfg.grid
     dt = cfg.dt
     EU = lambda A, a: exp_ksqr(g, A, -cfg.nu * a * dt)
@@ -975,6 +1012,77 @@ def rbc_rk4_step(cfg, U0: np.ndarray, T0: np.ndarray) -> tuple:
     totT = totT + (dt / 6) * S
     U = EU(U0, 1.0) + totU
     T = ET(T0, 1.0) + totT
+    if cfg.reality_fix:
+        U = reality_fix_vec(g, U)
+        T = reality_fix(g, T)
+    return U, T
+
+
+def rbc_rk4_step_slaved(cfg: RBCConfig, U0: np.ndarray, T0: np.ndarray) -> tuple:
+    """RK4(U,T,P,F) (RK_SF.cc:97-221) under PRZERO or PRINFTY, where one field is slaved to
+    the other (Single_time_step_RBC / Compute_RK4_parts_RBC, Tadvance_functions.cc:380-395,
+    :598-609; final assembly RK_SF.cc:196-213).
+
+    PRZERO: force U.F1 = cu T of the stage input, no T force (compute_force_RBC.cc:117-153);
+    nlin of U only (compute_nlin_SF.cc:266-268); pressure and rhs of U; U advanced with nu
+    and T = U.V1 / K^2 after every stage and after the final assembly.
+    PRINFTY: force T.F = cT U.V1 of the stage input (before the nonlinear term); nlin:
+    dealias T, U = slave(T) (so the products use the dealiased T and the velocity slaved to
+    it), T.nlin = sum_j D_j F[u_j T] (compute_nlin_SF.cc:271-299); no pressure; T advanced
+    with kappa and U = slave(T) after every stage and after the final assembly."""
+    g = cfg.grid
+    dt = cfg.dt
+    co = cfg.coeffs
+    p = lambda k: _par(g, k)
+    if cfg.pr_option == "PRZERO":
+        EU = lambda A, a: exp_ksqr(g, A, -co["nu"] * a * dt)
+
+        def rhs(U, T):
+            FU1 = co["cu"] * T
+            Ud = dealias(g, U, cfg.dealias_mode)
+            N = nlin_conservative_from_real(g, velocity_real(g, Ud))
+            N[0] = N[0] - FU1
+            return project_rhs(g, N), Ud
+
+        R, Ud = rhs(U0, T0)
+        U = EU(Ud + 0.5 * dt * R, 0.5)
+        tot = (dt / 6) * EU(R, 1.0)
+        R, _ = rhs(U, rbc_slave_temperature(g, U))
+        U = EU(U0, 0.5) + 0.5 * dt * R
+        tot = tot + (dt / 3) * EU(R, 0.5)
+        R, _ = rhs(U, rbc_slave_temperature(g, U))
+        U = EU(EU(U0, 0.5) + dt * R, 0.5)
+        tot = tot + (dt / 3) * EU(R, 0.5)
+        R, _ = rhs(U, rbc_slave_temperature(g, U))
+        U = EU(U0, 1.0) + (tot + (dt / 6) * R)
+        T = rbc_slave_temperature(g, U)
+    elif cfg.pr_option == "PRINFTY":
+        ET = lambda A, a: exp_ksqr(g, A, -co["kappa"] * a * dt)
+
+        def rhs(U, T):
+            FT = co["cT"] * U[0]
+            Td = dealias(g, T, cfg.dealias_mode)
+            ur = velocity_real(g, rbc_slave_velocity(g, Td, co["vs"]))
+            Tr = inverse(g, Td, p("F"))
+            Tn = xderiv(g, forward(g, ur[0] * Tr, p("FVx")), p("FVx"))
+            Tn = Tn + yderiv(g, forward(g, ur[1] * Tr, p("FVy")), p("FVy"))
+            Tn = Tn + zderiv(g, forward(g, ur[2] * Tr, p("FVz")), p("FVz"))
+            return -(Tn - FT), Td
+
+        S, Td = rhs(U0, T0)
+        T = ET(Td + 0.5 * dt * S, 0.5)
+        tot = (dt / 6) * ET(S, 1.0)
+        S, _ = rhs(rbc_slave_velocity(g, T, co["vs"]), T)
+        T = ET(T0, 0.5) + 0.5 * dt * S
+        tot = tot + (dt / 3) * ET(S, 0.5)
+        S, _ = rhs(rbc_slave_velocity(g, T, co["vs"]), T)
+        T = ET(ET(T0, 0.5) + dt * S, 0.5)
+        tot = tot + (dt / 3) * ET(S, 0.5)
+        S, _ = rhs(rbc_slave_velocity(g, T, co["vs"]), T)
+        T = ET(T0, 1.0) + (tot + (dt / 6) * S)
+        U = rbc_slave_velocity(g, T, co["vs"])
+    else:
+        raise ValueError(cfg.pr_option)
     if cfg.reality_fix:
         U = reality_fix_vec(g, U)
         T = reality_fix(g, T)

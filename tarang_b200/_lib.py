@@ -89,6 +89,7 @@ SIGNATURES = {
     "ts_shell_sums": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _D, _D, ctypes.c_int]),
     "ts_force_field": (ctypes.c_int, [_P, _P, _P]),
     "ts_nusselt": (ctypes.c_int, [_P, _P, _P, _D]),
+    "ts_rbc_slave": (ctypes.c_int, [_P, _P, _P]),
     "ts_init_energy_spectrum": (ctypes.c_int, [_P, _D, ctypes.c_int, ctypes.c_uint64, ctypes.c_double, _P]),
     "ts_init_temperature_perturbation": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _P]),
     "ts_ensemble_create": (ctypes.c_int, [ctypes.POINTER(TsConfig), _P, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),

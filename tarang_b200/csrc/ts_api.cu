@@ -70,6 +70,8 @@ struct ts_plan {
   int* err_h = nullptr;     // pinned copy, refreshed after every step call
   double rbc_cu = 1, rbc_cT = 1;    // RBC buoyancy coefficients U.F1 = cu T, T.F = cT U.V1
   double rbc_nu0 = 1, rbc_nuc = 0;  // Nusselt number nu0 + nuc <U.V1, T>
+  int rbc_slave = 0;                // 1: PRZERO (T slaved to U), 2: PRINFTY (U slaved to T)
+  double rbc_vs = 0;                // PRINFTY: factor of the slaved velocity
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
   double* eaxT[3] = {nullptr, nullptr, nullptr}; // per-axis exp(-kappa dt K_i^2 / 2) (SFF scalar)
   void* twq = nullptr;      // SFF, SSF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
@@ -153,11 +155,14 @@ struct ProfScope {
 // (Iscalar_main.cc:52-92), buoyancy U.Force1 += cu T, T.Force += cT U.V1
 // (compute_force_RBC.cc:104-150) and the Nusselt number nu0 + nuc <U.V1, T>
 // (Correlation::Get_Nusselt_no, Correlation.cc:144-176).  PRZERO / PRINFTY slave one
-// field to the other (Single_time_step_RBC, Tadvance_functions.cc:380-395): refused.
+// field to the other (Single_time_step_RBC, Tadvance_functions.cc:380-395): T = U.V1 / K^2
+// (no T force, kappa = 0), or U = vs P(T x) / K^2 (no U force) with the velocity factor
+// vs of FluidVF.cc:259-271.
 static int rbc_coefficients(int pr_option, int uscaling, double Ra, double Pr, double* nu, double* kappa, double* cu,
-                            double* cT, double* nu0, double* nuc) {
+                            double* cT, double* nu0, double* nuc, double* vs = nullptr) {
   if (uscaling != TS_U_LARGE && uscaling != TS_U_SMALL) return TS_ERR_ARG;
   const bool small = uscaling == TS_U_SMALL;
+  if (vs) *vs = 0;
   if (pr_option == TS_PR_LARGE) {
     *nu = small ? Pr : sqrt(Pr / Ra);
     *kappa = small ? 1.0 : 1.0 / sqrt(Pr * Ra);
@@ -176,9 +181,25 @@ static int rbc_coefficients(int pr_option, int uscaling, double Ra, double Pr, d
     *nuc = small ? 2.0 * Pr * Pr : 2.0 * Pr * sqrt(Ra * Pr);
     return TS_OK;
   }
-  if (pr_option == TS_PR_ZERO || pr_option == TS_PR_INFTY) {
-    g_last_error = "Pr_option PRZERO / PRINFTY (a slaved field) is not implemented";
-    return TS_ERR_UNSUPPORTED;
+  if (pr_option == TS_PR_ZERO) {
+    // the buoyancy of the PRSMALL branch; Nu reports 2 <U.V1, T> (Nu = 1 at Pr = 0)
+    *nu = 1.0;
+    *kappa = 0.0;
+    *cu = small ? Ra : Pr;
+    *cT = 0.0;
+    *nu0 = 0.0;
+    *nuc = 2.0;
+    return TS_OK;
+  }
+  if (pr_option == TS_PR_INFTY) {
+    *nu = small ? Pr : 1.0 / sqrt(Ra);
+    *kappa = small ? 1.0 : 1.0 / sqrt(Ra);
+    *cu = 0.0;
+    *cT = 1.0;
+    *nu0 = 1.0;
+    *nuc = small ? 2.0 : 2.0 * sqrt(Ra);
+    if (vs) *vs = small ? Ra : sqrt(Ra);
+    return TS_OK;
   }
   return TS_ERR_ARG;
 }
@@ -361,10 +382,10 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     return TS_ERR_UNSUPPORTED;
   }
   // the RBC coefficients of the plan's scaling (any basis: ts_rk4_step_rbc and ts_nusselt use them)
-  double rbc_nu = 0, rbc_kappa = 0, rbc_cu = 1, rbc_cT = 1, rbc_nu0 = 1, rbc_nuc = 0;
+  double rbc_nu = 0, rbc_kappa = 0, rbc_cu = 1, rbc_cT = 1, rbc_nu0 = 1, rbc_nuc = 0, rbc_vs = 0;
   {
     const int rc0 = rbc_coefficients(cfg->Pr_option, cfg->Uscaling, cfg->Ra, cfg->Pr, &rbc_nu, &rbc_kappa, &rbc_cu,
-                                     &rbc_cT, &rbc_nu0, &rbc_nuc);
+                                     &rbc_cT, &rbc_nu0, &rbc_nuc, &rbc_vs);
     if (rc0 != TS_OK) return rc0;
   }
   ts_plan* p = new ts_plan();
@@ -373,6 +394,8 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   p->rbc_cT = rbc_cT;
   p->rbc_nu0 = rbc_nu0;
   p->rbc_nuc = rbc_nuc;
+  p->rbc_slave = cfg->Pr_option == TS_PR_ZERO ? 1 : (cfg->Pr_option == TS_PR_INFTY ? 2 : 0);
+  p->rbc_vs = rbc_vs;
   p->cfg.energy_supply = nullptr;
   p->cfg.helicity_supply = nullptr;
   Geo& g = p->g;
@@ -759,6 +782,8 @@ static int step_rbc(ts_plan* p, void* U0, void* T0) {
   memset(&a, 0, sizeof(a));
   a.cu = p->rbc_cu;
   a.cT = p->rbc_cT;
+  a.slave = p->rbc_slave;
+  a.vs = p->rbc_vs;
   a.health = p->err_d;
   a.U0 = U0;
   a.T0 = T0;
@@ -1249,6 +1274,10 @@ int ts_rk4_step_rbc(ts_plan* p, void* u_hat, void* T_hat, int nsteps) {
   if (!p || !u_hat || !T_hat || nsteps < 0) return TS_ERR_ARG;
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SSS) {
     const bool sss = p->cfg.basis == TS_BASIS_SSS;
+    if (p->rbc_slave) {
+      g_last_error = "Pr_option PRZERO / PRINFTY step on SFF plans only";
+      return TS_ERR_UNSUPPORTED;
+    }
     CKS(ssf_step_supported(p, true));
     // the health word of earlier calls (copied back without a sync)
     if (*p->err_h) return health_status(p);
@@ -1511,6 +1540,19 @@ int ts_nusselt(ts_plan* p, const void* u_hat, const void* T_hat, double* Nu) {
   CK(cudaStreamSynchronize(p->st));
   *Nu = p->rbc_nu0 + p->rbc_nuc * e;
   return TS_OK;
+}
+
+int ts_rbc_slave(ts_plan* p, void* u_hat, void* T_hat) {
+  if (!p || !u_hat || !T_hat || !p->rbc_slave) return TS_ERR_ARG;
+  if (p->cfg.basis != TS_BASIS_SFF) return TS_ERR_UNSUPPORTED;
+  const size_t bu = 3 * p->g.S * p->cb, bt = p->g.S * p->cb;
+  return with_device(p, &p->stage_u, u_hat, bu, true, [&](void* U) -> int {
+    return with_device(p, &p->stage_t, T_hat, bt, true, [&](void* T) -> int {
+      CK(LAUNCH(p, rbc_slave, p->g, U, T, p->rbc_slave, p->rbc_vs, p->st));
+      CK(cudaStreamSynchronize(p->st));
+      return (int)TS_OK;
+    });
+  });
 }
 
 int ts_init_energy_spectrum(ts_plan* p, const double* E_ic, int n, uint64_t seed, double target_energy,
@@ -1858,6 +1900,10 @@ int ts_ensemble_create(const ts_config* base, const ts_member* members, int coun
     c.Ra = members[m].Ra;
     c.Pr = members[m].Pr;
     if (!(c.Ra > 0) || !(c.Pr > 0)) return fail(TS_ERR_ARG);
+    if (c.Pr_option == TS_PR_ZERO || c.Pr_option == TS_PR_INFTY) {
+      g_last_error = "ensembles step PRLARGE / PRSMALL members (no slaved field)";
+      return fail(TS_ERR_UNSUPPORTED);
+    }
     // nu, kappa of the scaling (Iscalar_main.cc:52-92; ULARGE: sqrt(Pr/Ra), 1/sqrt(Pr Ra))
     double cu, cT, nu0, nuc;
     const int rs = rbc_coefficients(c.Pr_option, c.Uscaling, c.Ra, c.Pr, &c.nu, &c.kappa, &cu, &cT, &nu0, &nuc);

@@ -655,6 +655,12 @@ template <> cudaError_t Launch<T>::reality(const Geo& g, void* A, int ncomp, cud
   return cudaGetLastError();
 }
 
+template <> cudaError_t Launch<T>::rbc_slave(const Geo& g, void* U, void* Tf, int slave, double vs, cudaStream_t st) {
+  k_rbc_slave<T><<<grid1d(g.S, 256), 256, 0, st>>>((V*)U, (V*)Tf, g, slave, vs);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
 template <> cudaError_t Launch<T>::reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st) {
   const long long n = (long long)g.Nx * g.Ny * ncomp;
   k_reality_adj<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((V*)A, ncomp, g);

@@ -76,6 +76,7 @@ template <typename T> struct Launch {
   // FFF MHD: elementwise epilogue of the nine x-transformed Elsasser products in P
   static cudaError_t mhd_epi(const Geo& g, const void* P, const SffArgs& a, cudaStream_t st);
   static cudaError_t reality(const Geo& g, void* A, int ncomp, cudaStream_t st);
+  static cudaError_t rbc_slave(const Geo& g, void* U, void* Tf, int slave, double vs, cudaStream_t st);
   static cudaError_t reality_adj(const Geo& g, void* A, int ncomp, cudaStream_t st);
   static cudaError_t carati(const Geo& g, const void* U, void* fc, int km, double rin, double rout, const double* es,
                             const double* hs, const double* mis, int nsup, cudaStream_t st);

@@ -46,6 +46,10 @@ struct SffArgs {
   // health words, one per member (the member index of the batch): a NaN or Inf written
   // into the state at stage 4 sets HEALTH_NONFINITE (nullptr: no check)
   int* health;
+  // Pr_option PRZERO (slave = 1: T = U.V1 / K^2) or PRINFTY (slave = 2: U = vs P(T x) / K^2,
+  // vs = sqrt(Ra) or Ra); 0: both fields advanced (SFF epilogue only)
+  int slave;
+  double vs;
 };
 
 // blocks per SM the SFF x kernels are compiled for: power-of-two lengths (8
@@ -254,28 +258,93 @@ __device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, lon
   const double ehu = a.eu[0][tb + m] * a.eu[1][tb + ly] * a.eu[2][tb + lz];
   const double eht = a.et[0][tb + m] * a.et[1][tb + ly] * a.et[2][tb + lz];
   const bool dz = dealias_zero(g.dealias, 1, m, ly, lz, g.Nx, g.Ny, g.Nz);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  // the stage update of field i; returns the value stored (the new stage field, or at
+  // stage 4 the new state)
+  auto advance = [&](int i) -> V {
     const double eh = i < 3 ? ehu : eht;
     const double e1 = eh * eh;
     const long long o = i * g.S + off;
     const V R = Rv[i];
     const V u0 = i < 3 ? U0[o] : T0[off];
+    V r;
     if (a.stage == 1) {
-      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
+      Uc[o] = r = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
       tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
     } else if (a.stage == 2) {
-      Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
+      Uc[o] = r = rk_u2_c(u0, R, eh, 0.5 * a.dt);
       tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
     } else if (a.stage == 3) {
-      Uc[o] = rk_u3_c(u0, R, eh, a.dt);
+      Uc[o] = r = rk_u3_c(u0, R, eh, a.dt);
       tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
     } else {
-      V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
-      if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
-      if (i < 3) const_cast<V*>(U0)[o] = un;
-      else const_cast<V*>(T0)[off] = un;
-      health_mark(nonfinite(un), a.health ? a.health + mb : nullptr);
+      r = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+      if (a.reality && lz == g.Nz / 2) r = mk<V>(0, 0);
+      if (i < 3) const_cast<V*>(U0)[o] = r;
+      else const_cast<V*>(T0)[off] = r;
+      health_mark(nonfinite(r), a.health ? a.health + mb : nullptr);
+    }
+    return r;
+  };
+  // a slaved field i: the stage field, or at stage 4 the state
+  auto store = [&](int i, V v) {
+    if (a.stage < 4) Uc[i * g.S + off] = v;
+    else if (i < 3) const_cast<V*>(U0)[i * g.S + off] = v;
+    else const_cast<V*>(T0)[off] = v;
+  };
+  if (a.slave == 1) {
+    // PRZERO (Single_time_step_RBC, Tadvance_functions.cc:383-386): U advanced, then
+    // T = U.V1 / K^2 with T(0) = 0 (Zero_Prandtl_number_compute_temperature, FluidVF.cc:228-232)
+    const V v1 = advance(0);
+    advance(1);
+    advance(2);
+    store(3, K2 > 0 ? mk<V>((T)((double)v1.x / K2), (T)((double)v1.y / K2)) : mk<V>(0, 0));
+    return;
+  }
+  if (a.slave == 2) {
+    // PRINFTY (:388-391): T advanced, then U from it (Infinite_Prandtl_number_compute_velocity,
+    // FluidVF.cc:235-272): X = Kx T / K^2 (T has the Vx parity), V1 = (T - Kx X) / K^2,
+    // V2 = i Ky X / K^2, V3 = i Kz X / K^2 (X has the divergence parity), times vs; 0 at K = 0
+    const V t = advance(3);
+    if (K2 > 0) {
+      const double Xr = (Kxd * t.x) / K2, Xi = (Kxd * t.y) / K2;
+      store(0, mk<V>((T)(a.vs * (((double)t.x - Kxd * Xr) / K2)), (T)(a.vs * (((double)t.y - Kxd * Xi) / K2))));
+      store(1, mk<V>((T)(a.vs * ((-Kyd * Xi) / K2)), (T)(a.vs * ((Kyd * Xr) / K2))));
+      store(2, mk<V>((T)(a.vs * ((-Kzd * Xi) / K2)), (T)(a.vs * ((Kzd * Xr) / K2))));
+    } else {
+      for (int i = 0; i < 3; ++i) store(i, mk<V>(0, 0));
+    }
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) advance(i);
+}
+
+// The slaved field of a PRZERO / PRINFTY state (SFF): slave = 1: T = U.V1 / K^2;
+// slave = 2: U = vs P(T x) / K^2 (the formulas of sff_epilogue, for initial conditions).
+template <typename T>
+__global__ void __launch_bounds__(256) k_rbc_slave(C<T>* __restrict__ U, C<T>* __restrict__ Tf, Geo g, int slave,
+                                                   double vs) {
+  typedef C<T> V;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < g.S; e += stride) {
+    const int lz = (int)(e % g.Hz);
+    const long long r = e / g.Hz;
+    const int ly = (int)(r % g.Ny), m = (int)(r / g.Ny);
+    const double Kxd = m * g.kf[0], Kyd = kfft(ly, g.Ny) * g.kf[1], Kzd = lz * g.kf[2];
+    const double K2 = (Kxd * Kxd + Kyd * Kyd) + Kzd * Kzd;
+    if (slave == 1) {
+      const V v1 = U[e];
+      Tf[e] = K2 > 0 ? mk<V>((T)((double)v1.x / K2), (T)((double)v1.y / K2)) : mk<V>(0, 0);
+    } else {
+      const V t = Tf[e];
+      if (K2 > 0) {
+        const double Xr = (Kxd * t.x) / K2, Xi = (Kxd * t.y) / K2;
+        U[e] = mk<V>((T)(vs * (((double)t.x - Kxd * Xr) / K2)), (T)(vs * (((double)t.y - Kxd * Xi) / K2)));
+        U[g.S + e] = mk<V>((T)(vs * ((-Kyd * Xi) / K2)), (T)(vs * ((Kyd * Xr) / K2)));
+        U[2 * g.S + e] = mk<V>((T)(vs * ((-Kzd * Xi) / K2)), (T)(vs * ((Kzd * Xr) / K2)));
+      } else {
+        U[e] = U[g.S + e] = U[2 * g.S + e] = mk<V>(0, 0);
+      }
     }
   }
 }

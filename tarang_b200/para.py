@@ -158,9 +158,10 @@ def read_para(path: str) -> RunParams:
         ph = p.get("PHYSICS") or {}
         pr_opt = str(ph.get("Pr_option", "PRLARGE")).strip()
         usc = str(ph.get("Uscaling", "USMALL")).strip()
-        if pr_opt not in ("PRLARGE", "PRSMALL") or usc not in ("ULARGE", "USMALL"):
-            raise NotImplementedError(f"PHYSICS Pr_option {pr_opt} / Uscaling {usc}: PRLARGE / PRSMALL with "
-                                      "ULARGE / USMALL (PRZERO and PRINFTY slave one field to the other)")
+        if pr_opt not in ("PRLARGE", "PRSMALL", "PRZERO", "PRINFTY") or usc not in ("ULARGE", "USMALL"):
+            raise NotImplementedError(f"PHYSICS Pr_option {pr_opt} / Uscaling {usc}")
+        if pr_opt in ("PRZERO", "PRINFTY") and basis != "SFF":
+            raise NotImplementedError(f"PHYSICS Pr_option {pr_opt} on {basis}: the slaved scalings step on SFF")
         rp.pr_option, rp.uscaling = pr_opt, usc
         rp.Ra = float(ph.get("Rayleigh", 2000.0))
         rp.Pr = float(ph.get("Prandtl", 1.0))
@@ -342,7 +343,12 @@ def read_init_cond(data_dir: str, plan, rp: RunParams):
     if rp.input_field_procedure != 1:
         raise NotImplementedError(f"io.input_field_procedure {rp.input_field_procedure}: "
                                   "1 (complex fields from in/) only; seeded spectra use Plan.init_energy_spectrum")
-    return load_state(os.path.join(data_dir, "in"), plan, rp.kind)
+    fields, t, step = load_state(os.path.join(data_dir, "in"), plan, rp.kind)
+    if rp.kind == "RBC" and rp.pr_option in ("PRZERO", "PRINFTY"):
+        # Init_cond_RBC_complex_field (init_cond_field.cc:176-190): the slaved field is
+        # computed from the advanced one (T = U.V1 / K^2, or U from T)
+        plan.rbc_slave(fields[0], fields[1])
+    return fields, t, step
 
 
 # ----------------------------------------------------------------------------

@@ -76,13 +76,17 @@ _USCALING = {"ULARGE": 0, "USMALL": 1}
 
 
 def rbc_diss_coefficients(pr_option: str, uscaling: str, Ra: float, Pr: float) -> tuple:
-    """(nu, kappa) of an RBC run (Iscalar_main.cc:52-92) for Pr_option PRLARGE / PRSMALL."""
+    """(nu, kappa) of an RBC run (Iscalar_main.cc:52-92)."""
     small = uscaling == "USMALL"
     if pr_option == "PRLARGE":
         return (Pr, 1.0) if small else (math.sqrt(Pr / Ra), 1.0 / math.sqrt(Pr * Ra))
     if pr_option == "PRSMALL":
         return (1.0, 1.0 / Pr) if small else (math.sqrt(Pr / Ra), 1.0 / math.sqrt(Pr * Ra))
-    raise NotImplementedError(f"Pr_option {pr_option}: PRLARGE / PRSMALL only")
+    if pr_option == "PRZERO":
+        return (1.0, 0.0)
+    if pr_option == "PRINFTY":
+        return (Pr, 1.0) if small else (1.0 / math.sqrt(Ra), 1.0 / math.sqrt(Ra))
+    raise ValueError(f"Pr_option {pr_option}")
 
 
 class Plan:
@@ -317,6 +321,11 @@ class Plan:
         L.check(self.lib.ts_nusselt(self.h, _ptr(u), _ptr(T), ctypes.byref(e)), "ts_nusselt")
         return e.value
 
+    def rbc_slave(self, u, T):
+        """PRZERO: T = U.V1 / K^2; PRINFTY: u = vs P(T x) / K^2 (in place; SFF plans)."""
+        L.check(self.lib.ts_rbc_slave(self.h, _ptr(u), _ptr(T)), "ts_rbc_slave")
+        return u, T
+
     def init_energy_spectrum(self, E_ic, seed: int, target_energy: float, out):
         e = np.ascontiguousarray(E_ic, dtype=np.float64)
         L.check(self.lib.ts_init_energy_spectrum(self.h, e.ctypes.data_as(L._D), len(e), seed, target_energy,
@@ -379,11 +388,13 @@ class Time_advance_incompress:
 
 
 class Ensemble:
-    """Independent RBC runs (SFF, PRLARGE/ULARGE) of uneven sizes advanced together:
-    one CUDA graph launch per ensemble step with one parallel branch per member."""
+    """Independent RBC runs (SFF; Pr_option PRLARGE / PRSMALL, Uscaling ULARGE / USMALL) of
+    uneven sizes advanced together: one CUDA graph launch per group of ensemble steps, with
+    one parallel branch per grid size."""
 
     def __init__(self, members, kfactor=(math.pi, 2 * math.pi, 2 * math.pi), dt: float = 1e-4,
-                 precision: str = "f32", dealias: str = "reference", reality_fix: bool = True):
+                 precision: str = "f32", dealias: str = "reference", reality_fix: bool = True,
+                 Pr_option: str = "PRLARGE", Uscaling: str = "ULARGE"):
         self.lib = L.load()
         c = L.TsConfig()
         self.lib.ts_config_default(ctypes.byref(c))
@@ -395,6 +406,8 @@ class Ensemble:
         c.reality_fix = int(bool(reality_fix))
         c.dt = dt
         c.force_type = L.TS_FORCE_RBC
+        c.Pr_option = _PR_OPTION[Pr_option]
+        c.Uscaling = _USCALING[Uscaling]
         arr = (L.TsMember * len(members))()
         for m, (N, Ra, Pr) in enumerate(members):
             N = (N, N, N) if isinstance(N, int) else N

@@ -181,10 +181,72 @@ def test_rbc_scalings_match_oracle(cuda, basis, pr, us):
         plan.close()
 
 
-def test_rbc_slaved_scalings_are_refused(cuda):
-    """PRZERO and PRINFTY slave one field to the other (Single_time_step_RBC,
-    Tadvance_functions.cc:380-395): refused at plan creation, not run as something else."""
+@pytest.mark.parametrize("pr,us", [("PRZERO", "USMALL"), ("PRZERO", "ULARGE"), ("PRINFTY", "USMALL"),
+                                   ("PRINFTY", "ULARGE")])
+def test_rbc_slaved_scalings_match_oracle(cuda, pr, us):
+    """PRZERO (T = U.V1 / K^2 after every stage) and PRINFTY (U = vs P(T x) / K^2) on SFF
+    against the oracle (rbc_rk4_step_slaved): the slaved initial field of ts_rbc_slave, then
+    3 steps, FP64 <= 1e-12 and FP32 <= 1e-5 in both fields, and the Nusselt number."""
+    import torch
     import tarang_b200 as tb
+    from tarang_b200.solver import rbc_diss_coefficients
+    N = (16, 16, 16)
+    g = R.Grid(N, KF, "SFF")
+    Ra, Pr = 3e4, 0.7
+    cfg = R.RBCConfig(g, Ra=Ra, Pr=Pr, dt=1e-5 if us == "USMALL" else 1e-3, dealias_mode=1, pr_option=pr,
+                      uscaling=us)
+    co = cfg.coeffs
+    U0, T0 = random_state(g, 0.3, 11)
+    if pr == "PRZERO":
+        T0 = R.rbc_slave_temperature(g, U0)
+    else:
+        U0 = R.rbc_slave_velocity(g, T0, co["vs"])
+    Uo, To = U0, T0
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    nu, kappa = rbc_diss_coefficients(pr, us, Ra, Pr)
+    assert (nu, kappa) == (cfg.nu, cfg.kappa)
+    for prec, tol in (("f64", 1e-12), ("f32", 1e-5)):
+        plan = tb.Plan(N, basis="SFF", precision=prec, kfactor=KF, dealias="reference", nu=nu, kappa=kappa,
+                       dt=cfg.dt, Ra=Ra, Pr=Pr, Pr_option=pr, Uscaling=us)
+        u = torch.from_numpy(np.ascontiguousarray(U0)).to(cuda).to(plan.torch_dtype())
+        T = torch.from_numpy(np.ascontiguousarray(T0)[None]).to(cuda).to(plan.torch_dtype())
+        # the slaved field as the reference sets it after an initial condition
+        if pr == "PRZERO":
+            T.zero_()
+        else:
+            u.zero_()
+        plan.rbc_slave(u, T)
+        assert rel(u.cpu().numpy().astype(np.complex128), U0) < tol
+        assert rel(T[0].cpu().numpy().astype(np.complex128), T0) < tol
+        plan.rk4_step_rbc(u, T, 3)
+        plan.status()
+        assert rel(u.cpu().numpy().astype(np.complex128), Uo) < tol
+        assert rel(T[0].cpu().numpy().astype(np.complex128), To) < tol
+        if prec == "f64":
+            ref = R.nusselt(cfg, Uo, To)
+            assert abs(plan.nusselt(u, T) - ref) < 1e-12 * max(1.0, abs(ref))
+        plan.close()
+
+
+def test_rbc_slaved_scalings_refused_off_sff(cuda):
+    """PRZERO / PRINFTY step on SFF only: an SSF plan refuses the step, an ensemble refuses
+    the members, and ts_rbc_slave refuses the non-slaved scalings."""
+    import torch
+    import tarang_b200 as tb
+    plan = tb.Plan((16, 16, 16), basis="SSF", kfactor=KF, Pr_option="PRZERO", Uscaling="USMALL", nu=1.0,
+                   kappa=0.0)
+    u = plan.field(3)
+    T = plan.field(1)
+    with pytest.raises(tb.TsError):
+        plan.rk4_step_rbc(u, T, 1)
+    plan.close()
+    plan = tb.Plan((16, 16, 16), basis="SFF", kfactor=KF)
+    u = plan.field(3)
+    T = plan.field(1)
+    with pytest.raises(tb.TsError):
+        plan.rbc_slave(u, T)
+    plan.close()
     for pr in ("PRZERO", "PRINFTY"):
         with pytest.raises(tb.TsError):
-            tb.Plan((16, 16, 16), basis="SFF", kfactor=KF, Pr_option=pr)
+            tb.Ensemble([((16, 16, 16), 1e4, 1.0)], dt=1e-4, Pr_option=pr, Uscaling="USMALL")

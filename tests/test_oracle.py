@@ -435,8 +435,8 @@ def test_rbc_scalings_are_one_physics(pr, us):
     c = R.rbc_coefficients(pr, us, Ra, Pr)
     assert abs(c["cu"] * c["cT"] / (c["nu"] * c["kappa"]) / Ra - 1) < 1e-14
     assert abs(c["nu"] / c["kappa"] / Pr - 1) < 1e-14
-    with pytest.raises(NotImplementedError):
-        R.rbc_coefficients("PRZERO", us, Ra, Pr)
+    with pytest.raises(ValueError):
+        R.rbc_coefficients("PRHALF", us, Ra, Pr)
 
 
 @pytest.mark.parametrize("pr,us", SCALINGS)
@@ -467,3 +467,73 @@ def test_rbc_roll_follows_the_linear_system_every_scaling(pr, us):
     assert abs(U[0, 1, 0, 1] / eps - 1) > 1e-5   # the state moved
     nu = R.nusselt(cfg, U, T)
     assert nu == co["nu0"] + co["nuc"] * R.cross_energy(g, U[0], T)
+
+
+@pytest.mark.parametrize("pr,us", [("PRZERO", "USMALL"), ("PRZERO", "ULARGE"), ("PRINFTY", "USMALL"),
+                                   ("PRINFTY", "ULARGE")])
+def test_rbc_slaved_roll_follows_its_growth_rate(pr, us):
+    """PRZERO (T = U.V1 / K^2) and PRINFTY (U = vs P(T x) / K^2) reduce one small free-slip
+    roll to one linear equation: da/dt = (cu kz^2 / K^4 - nu K^2) a for PRZERO and
+    db/dt = (cT vs kz^2 / K^4 - kappa K^2) b for PRINFTY.  Over 20 steps the advanced field
+    follows it to 1e-7 of its amplitude, the slaved field equals its formula exactly, and
+    the slaved velocity is divergence-free."""
+    kf = (math.pi, 2 * math.pi, 2 * math.pi)
+    g = R.Grid((16, 8, 8), kf, "SFF")
+    eps = 1e-9
+    kx, kz = kf[0], kf[2]
+    K2 = kx * kx + kz * kz
+    Ra = 2e3 if us == "USMALL" else 2e4
+    cfg = R.RBCConfig(g, Ra=Ra, Pr=0.7, dt=2e-4 if us == "USMALL" else 2e-3, pr_option=pr, uscaling=us)
+    co = cfg.coeffs
+    U0 = np.zeros((3,) + g.shape, complex)
+    T0 = np.zeros(g.shape, complex)
+    if pr == "PRZERO":
+        U0[0, 1, 0, 1] = eps
+        U0[2, 1, 0, 1] = 1j * kx * eps / kz
+        T0 = R.rbc_slave_temperature(g, U0)
+        sigma = co["cu"] * kz * kz / K2 ** 2 - co["nu"] * K2
+    else:
+        T0[1, 0, 1] = eps
+        U0 = R.rbc_slave_velocity(g, T0, co["vs"])
+        sigma = co["cT"] * co["vs"] * kz * kz / K2 ** 2 - co["kappa"] * K2
+        # the slaved roll: U1 = vs kz^2 / K^4 T, U3 = i kx U1 / kz, divergence Kx U1 + i Kz U3 = 0
+        assert abs(U0[0, 1, 0, 1] - co["vs"] * kz * kz / K2 ** 2 * eps) < 1e-15 * abs(U0[0, 1, 0, 1])
+        assert abs(kx * U0[0, 1, 0, 1] + 1j * kz * U0[2, 1, 0, 1]) < 1e-12 * abs(U0[0, 1, 0, 1])
+    U, T = U0.copy(), T0.copy()
+    for _ in range(20):
+        U, T = R.rbc_rk4_step(cfg, U, T)
+    growth = math.exp(sigma * 20 * cfg.dt)
+    assert abs(growth - 1) > 1e-4   # the state moved
+    if pr == "PRZERO":
+        assert abs(U[0, 1, 0, 1] - growth * eps) < 1e-7 * eps
+        assert np.array_equal(T, R.reality_fix(g, R.rbc_slave_temperature(g, U)))
+    else:
+        assert abs(T[1, 0, 1] - growth * eps) < 1e-7 * eps
+        assert np.array_equal(U, R.reality_fix_vec(g, R.rbc_slave_velocity(g, T, co["vs"])))
+    assert R.nusselt(cfg, U, T) == co["nu0"] + co["nuc"] * R.cross_energy(g, U[0], T)
+
+
+def test_rbc_slaved_critical_rayleigh_number():
+    """Free-slip Rayleigh-Benard onset at infinite and zero Prandtl number (USMALL units):
+    growth rate Ra kperp^2 / K^4 - K^2 changes sign at Ra_c = K^6 / kperp^2 = 27 pi^4 / 4 for the
+    roll kx = pi, kperp = pi / sqrt(2).  Below Ra_c the oracle's roll decays, above it grows."""
+    kp = math.pi / math.sqrt(2)
+    kf = (math.pi, kp, kp)
+    g = R.Grid((16, 8, 8), kf, "SFF")
+    Rac = 27 * math.pi ** 4 / 4
+    for pr in ("PRZERO", "PRINFTY"):
+        for Ra, grows in ((0.95 * Rac, False), (1.05 * Rac, True)):
+            cfg = R.RBCConfig(g, Ra=Ra, Pr=1.0, dt=1e-4, pr_option=pr, uscaling="USMALL")
+            T0 = np.zeros(g.shape, complex)
+            T0[1, 0, 1] = 1e-9
+            U0 = R.rbc_slave_velocity(g, T0, cfg.coeffs["vs"]) if pr == "PRINFTY" else None
+            if pr == "PRZERO":
+                U0 = np.zeros((3,) + g.shape, complex)
+                U0[0, 1, 0, 1] = 1e-9
+                U0[2, 1, 0, 1] = 1j * math.pi * 1e-9 / kp
+                T0 = R.rbc_slave_temperature(g, U0)
+            U, T = U0, T0
+            for _ in range(5):
+                U, T = R.rbc_rk4_step(cfg, U, T)
+            a = abs(U[0, 1, 0, 1] / U0[0, 1, 0, 1]) if pr == "PRZERO" else abs(T[1, 0, 1] / T0[1, 0, 1])
+            assert (a > 1) == grows, (pr, Ra, a)

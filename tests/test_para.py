@@ -509,15 +509,22 @@ def test_read_para_input_field_procedure(tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-@pytest.mark.parametrize("name", ["fff", "rbc"])
+@pytest.mark.parametrize("name", ["fff", "rbc", "rbc_przero", "rbc_prinfty"])
 def test_restart_continues_bit_for_bit(cuda, tmp_path, name, precision):
     """Save after 2 steps into out/time_<t>/, restart a second run from it through
     input_field_procedure 1 (the saved folder as the new run's in/), step 2 more: the state equals
-    4 unbroken steps bit for bit."""
+    4 unbroken steps bit for bit (under PRZERO / PRINFTY the slaved field is recomputed from
+    the read one, as Init_cond_RBC_complex_field does)."""
     import shutil
     import torch
     from oracle import tarang_ref as R
     src = FFF_DIR if name == "fff" else RBC_DIR
+    if name in ("rbc_przero", "rbc_prinfty"):
+        pr = "PRZERO" if name == "rbc_przero" else "PRINFTY"
+        os.makedirs(tmp_path / "src" / "in")
+        (tmp_path / "src" / "in" / "para.yaml").write_text(
+            open(os.path.join(RBC_DIR, "in", "para.yaml")).read().replace("Pr_option: PRLARGE", f"Pr_option: {pr}"))
+        src = str(tmp_path / "src")
     plan, rp = para.plan_from_dir(src, precision=precision)
     if name == "fff":
         g = R.Grid(rp.N, rp.kfactor)
@@ -525,7 +532,10 @@ def test_restart_continues_bit_for_bit(cuda, tmp_path, name, precision):
         fields = [torch.from_numpy(V).to(cuda).to(plan.torch_dtype())]
     else:
         u, T = plan.field(3), plan.field(1)
-        plan.init_temperature_perturbation(1e-2, 4.0, 3, T)
+        plan.init_temperature_perturbation(1e-2, 4.0, 3, u[0:1] if name == "rbc_przero" else T)
+        if name != "rbc":
+            plan.rbc_slave(u, T)
+            assert float(torch.linalg.vector_norm(u if name == "rbc_prinfty" else T)) > 0
         fields = [u, T]
     ref = [f.clone() for f in fields]
     para.advance(plan, rp.kind, ref, 4)
@@ -555,10 +565,12 @@ def test_restart_continues_bit_for_bit(cuda, tmp_path, name, precision):
         assert torch.equal(a, b)
 
 
-@pytest.mark.parametrize("pr,us", [("PRSMALL", "USMALL"), ("PRLARGE", "USMALL"), ("PRSMALL", "ULARGE")])
+@pytest.mark.parametrize("pr,us", [("PRSMALL", "USMALL"), ("PRLARGE", "USMALL"), ("PRSMALL", "ULARGE"),
+                                   ("PRZERO", "USMALL"), ("PRINFTY", "ULARGE")])
 def test_read_para_rbc_scalings(tmp_path, pr, us):
-    """Pr_option PRLARGE / PRSMALL with Uscaling ULARGE / USMALL set nu and kappa as
-    Iscalar_main.cc:52-92; PRZERO / PRINFTY are refused by name."""
+    """Every Pr_option with Uscaling ULARGE / USMALL sets nu and kappa as Iscalar_main.cc:52-92
+    (PRZERO: 1 and 0); an unknown option is refused by name, and so are the slaved scalings
+    on SSF."""
     from tarang_b200.solver import rbc_diss_coefficients
     text = open(os.path.join(RBC_DIR, "in", "para.yaml")).read()
     (tmp_path / "in").mkdir()
@@ -569,7 +581,13 @@ def test_read_para_rbc_scalings(tmp_path, pr, us):
     assert (rp.nu, rp.kappa) == rbc_diss_coefficients(pr, us, rp.Ra, rp.Pr)
     if us == "USMALL":
         assert rp.nu == (rp.Pr if pr == "PRLARGE" else 1.0)
-    (tmp_path / "in" / "para.yaml").write_text(text.replace("Pr_option: PRLARGE", "Pr_option: PRZERO"))
+    if pr == "PRZERO":
+        assert (rp.nu, rp.kappa) == (1.0, 0.0)
+    (tmp_path / "in" / "para.yaml").write_text(text.replace("Pr_option: PRLARGE", "Pr_option: PRHALF"))
+    with pytest.raises(NotImplementedError):
+        para.read_para(str(tmp_path / "in" / "para.yaml"))
+    (tmp_path / "in" / "para.yaml").write_text(text.replace("Pr_option: PRLARGE", "Pr_option: PRZERO")
+                                                .replace("basis_type: SFF", "basis_type: SSF"))
     with pytest.raises(NotImplementedError):
         para.read_para(str(tmp_path / "in" / "para.yaml"))
 
