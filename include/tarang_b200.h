@@ -283,11 +283,13 @@ int ts_adjoint_window(ts_plan* plan, const void* u_start, int nsteps, void* lam_
 
 /* Launch tuning (no reference counterpart: the reference leaves the FFT plan
  * to FFTW's planner).  Each right-hand side runs five pass classes; for each
- * the library holds a fixed rule (candidate 0) and up to four other kernel
+ * the library holds a fixed rule (candidate 0) and up to five other kernel
  * candidates that change the radix schedule (elements per thread, so the
  * Stockham passes' radices), the column-tile width, the staging depth (y passes:
- * candidate 4 keeps two items in flight ahead of the one transformed), or the
- * kernel form (z: shared-memory slot kernels; FFF forward x: split x FFF +
+ * candidate 4 keeps two items in flight ahead of the one transformed; candidate 5
+ * at 1024 points in FP32, one tile per block and 32 elements per thread), or the
+ * kernel form (z: shared-memory slot kernels, and at 1024 points the register
+ * kernel with every load issued up front; FFF forward x: split x FFF +
  * elementwise epilogue; SFF forward x: the other fused/split choice), plus a
  * blocks-per-SM count for the persistent launches (y passes, fused FFF
  * forward x; 0 = the rule).  Every candidate computes the same transform;

@@ -416,11 +416,11 @@ template <typename V> __device__ __forceinline__ bool nonfinite(const V& v) { re
 
 // ---------------------------------------------------------------------------
 // IF-RK4 stage arithmetic of one mode (RK.cc:91-170: Single_time_step,
-// Compute_RK4_parts), every product and sum in FP64 and one rounding per stored
-// value.  eh = E(1/2) = exp(-nu dt K^2 / 2), e1 = E(1) (FP64 tables); c = the dt factor.
-// In the FP32 path a factor rounded to FP32 (eh or e1 to 24 bits) would scale a mode by
-// the same wrong amount every step, a bias that grows linearly with the step count; in
-// FP64 these are the plain expressions.
+// Compute_RK4_parts).  eh = E(1/2) = exp(-nu dt K^2 / 2), e1 = E(1) (FP64 tables);
+// c = the dt factor.  The templates compute every product and sum in FP64 with one
+// rounding per stored value (in FP64 the plain expressions).  In the FP32 path a factor
+// rounded to FP32 (eh or e1 to 24 bits) would scale a mode by the same wrong amount
+// every step, a bias that grows linearly with the step count.
 // ---------------------------------------------------------------------------
 template <typename S> __device__ __forceinline__ S rk_u1(S u0, S R, double eh, double c) {
   return (S)(((double)u0 + (double)R * c) * eh);      // (u0 + R dt/2) E(1/2)
@@ -439,6 +439,32 @@ template <typename S> __device__ __forceinline__ S rk_u3(S u0, S R, double eh, d
 }
 template <typename S> __device__ __forceinline__ S rk_u4(S u0, S tt, S R, double e1, double c) {
   return (S)((double)u0 * e1 + ((double)tt + (double)R * c));  // u0 E(1) + (tot + R dt/6)
+}
+// FP32 stages 1-3: the stage fields are rounded to FP32 before the next right-hand side
+// anyway, and their rounding does not carry from step to step (each step restarts from
+// the stored state), so these run in FP32 with every factor applied exactly: x as the
+// pair hi = fl32(x), lo = fl32(x - hi), and a x = fma(a, hi, a lo) rounded once.  Only
+// stage 4, whose rounding enters the state every step, stays in FP64 (rk_u4 above).
+struct Fx { float hi, lo; };
+__device__ __forceinline__ Fx fx(double x) {
+  const float h = (float)x;
+  return {h, (float)(x - (double)h)};
+}
+__device__ __forceinline__ float fmul(float a, Fx f) { return fmaf(a, f.hi, a * f.lo); }
+template <> __device__ __forceinline__ float rk_u1(float u0, float R, double eh, double c) {
+  return fmul(u0 + fmul(R, fx(c)), fx(eh));
+}
+template <> __device__ __forceinline__ float rk_t1(float R, double e1, double c) {
+  return fmul(fmul(R, fx(e1)), fx(c));
+}
+template <> __device__ __forceinline__ float rk_u2(float u0, float R, double eh, double c) {
+  return fmul(u0, fx(eh)) + fmul(R, fx(c));
+}
+template <> __device__ __forceinline__ float rk_tacc(float tt, float R, double eh, double c) {
+  return tt + fmul(fmul(R, fx(eh)), fx(c));
+}
+template <> __device__ __forceinline__ float rk_u3(float u0, float R, double eh, double c) {
+  return fmul(fmul(u0, fx(eh)) + fmul(R, fx(c)), fx(eh));
 }
 #define TS_RK_CPLX(NAME, ...) \
   template <typename V> __device__ __forceinline__ V NAME##_c(__VA_ARGS__)

@@ -18,7 +18,7 @@
 namespace ts {
 
 // pass classes of the launch tuning: inverse x, inverse y, z, forward y, forward x
-enum { TUNE_X_INV = 0, TUNE_Y_INV = 1, TUNE_Z = 2, TUNE_Y_FWD = 3, TUNE_X_FWD = 4, TUNE_NCLASS = 5, TUNE_NCAND = 5 };
+enum { TUNE_X_INV = 0, TUNE_Y_INV = 1, TUNE_Z = 2, TUNE_Y_FWD = 3, TUNE_X_FWD = 4, TUNE_NCLASS = 5, TUNE_NCAND = 6 };
 
 struct Geo {
   int Nx, Ny, Nz, Hz;
@@ -46,7 +46,9 @@ constexpr int SHELL_WARPS = 4;
 // or 2 staging tiles with the consumed one doubling as the exchange tile
 // (NT = 2: wider column tiles fit, e.g. 8 columns at L = 1024 in FP32), or
 // 3 staging tiles with the consumed one as the exchange tile (NT = 4: the tiles of
-// the next two items stream in while one is transformed).
+// the next two items stream in while one is transformed), or one tile that is also
+// the exchange tile (NT = 1: no prefetch inside a block; the blocks sharing an SM
+// overlap one another's loads).
 // ---------------------------------------------------------------------------
 __host__ __device__ constexpr int str_tiles(int nt) { return nt == 4 ? 3 : nt; }
 template <typename T, int L, int E, int CW, int DIR, int NT = 3>
@@ -55,8 +57,8 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
                   long long ostride, int nouter, const C<T>* __restrict__ tw, int per, long long mstride,
                   int zero_hi) {
   typedef C<T> V;
-  static_assert(NT == 2 || NT == 3 || NT == 4, "two or three staging tiles");
-  constexpr int NBUF = NT == 4 ? 3 : 2;  // staging tiles: items in flight = NBUF - 1 ahead
+  static_assert(NT >= 1 && NT <= 4, "one to three staging tiles");
+  constexpr int NBUF = NT == 4 ? 3 : (NT == 1 ? 1 : 2);  // staging tiles: items in flight = NBUF - 1 ahead
   constexpr bool XC = NT != 3;           // exchange in the consumed staging tile
   extern __shared__ __align__(16) unsigned char smraw[];
   V* stage = reinterpret_cast<V*>(smraw);
@@ -826,8 +828,10 @@ template <int NZ, int EZ = 0, int FORM = 0> __host__ __device__ constexpr int zr
 }
 
 // EZ = 0: 8 elements per thread, 12 for a line length with a factor 3 (radices
-// 4, 2|4, 3); EZ = 4: 4 elements per thread (twice the lanes per line)
-template <typename T, int NZ, int FORM, int EZ = 0>
+// 4, 2|4, 3); EZ = 4: 4 elements per thread (twice the lanes per line).
+// BATCH: a line over two warps also issues every component's loads before the first
+// transform (one load latency per line instead of one per component)
+template <typename T, int NZ, int FORM, int EZ = 0, bool BATCH = false>
 __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ, FORM>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
@@ -847,7 +851,7 @@ __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ, 
   V* xch = xch_all + l * LDX;
 
   V in[NIN][E];
-  if constexpr (TPL <= 32) {
+  if constexpr (TPL <= 32 || BATCH) {
     // lines within a warp: every component's loads are issued before the first transform
     V XM[NIN];
 #pragma unroll

@@ -125,13 +125,15 @@ constexpr Tile str_cand(int L, int v) {
        : v == 2 ? (str_cw(L) > 1 ? Tile{str_e(L), str_cw(L) / 2, str_nt(L)} : Tile{0, 0, 0})
        : v == 3 ? Tile{str_e(L), str_cw(L), 5 - str_nt(L)}
        : v == 4 ? Tile{str_e(L), str_cw(L), 4}
+       : v == 5 ? (wide1024(L) ? Tile{32, 8, 1} : Tile{0, 0, 0})
                 : Tile{0, 0, 0};
 }
 constexpr bool str_valid(int L, int v) {
   return v == 0 || (v < NCAND && tile_fits(L, str_cand(L, v), str_tiles(str_cand(L, v).NT)) &&
                     !tile_eq(str_cand(L, v), str_cand(L, 0)) && (v < 2 || !tile_eq(str_cand(L, v), str_cand(L, 1))) &&
                     (v < 3 || !tile_eq(str_cand(L, v), str_cand(L, 2))) &&
-                    (v < 4 || !tile_eq(str_cand(L, v), str_cand(L, 3))));
+                    (v < 4 || !tile_eq(str_cand(L, v), str_cand(L, 3))) &&
+                    (v < 5 || !tile_eq(str_cand(L, v), str_cand(L, 4))));
 }
 
 template <int L, int VV, typename Fn> void with_str_tile(Fn&& fn) {
@@ -180,6 +182,7 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       case 2: with_str_tile<LL, 2>(run); break;
       case 3: with_str_tile<LL, 3>(run); break;
       case 4: with_str_tile<LL, 4>(run); break;
+      case 5: with_str_tile<LL, 5>(run); break;
       default: run(std::integral_constant<int, 0>{});
     }
   });
@@ -194,18 +197,22 @@ constexpr int ix_e_alt(int L) {
   return std::is_same<T, float>::value ? (ix_e(L) == 8 ? (16 <= L ? 16 : 0) : 8) : (ix_e(L) > 4 ? ix_e(L) / 2 : 0);
 }
 // candidate 3 (FP32): the persistent prefetching kernel k_inv_x_pf, 8 elements per thread
-// (the three components of U held in registers), staging + exchange tiles (NT = 4 tiles)
+// (the three components of U held in registers), staging + exchange tiles (NT = 4 tiles);
+// candidate 4 (FP32, 1024-point lines): 32 elements per thread over 8-column tiles
+// (256-thread blocks, two per SM; radix 32 x 32, one exchange per field)
 constexpr Tile ix_cand(int L, int v) {
   return v == 0 ? Tile{ix_e(L), ix_cw(L), 1}
        : v == 1 ? (ix_e_alt(L) > 0 ? Tile{ix_e_alt(L), cw_for(L, ix_e_alt(L)), 1} : Tile{0, 0, 0})
        : v == 2 ? (ix_cw(L) > 1 ? Tile{ix_e(L), ix_cw(L) / 2, 1} : Tile{0, 0, 0})
        : v == 3 ? (std::is_same<T, float>::value ? Tile{8, cw_for(L, 8), 4} : Tile{0, 0, 0})
+       : v == 4 ? (wide1024(L) ? Tile{32, 8, 1} : Tile{0, 0, 0})
                 : Tile{0, 0, 0};
 }
 constexpr bool ix_valid(int L, int v) {
-  return v == 0 || (v < 4 && tile_fits(L, ix_cand(L, v), ix_cand(L, v).NT == 4 ? 4 : 1) &&
+  return v == 0 || (v < NCAND && tile_fits(L, ix_cand(L, v), ix_cand(L, v).NT == 4 ? 4 : 1) &&
                     !tile_eq(ix_cand(L, v), ix_cand(L, 0)) && (v < 2 || !tile_eq(ix_cand(L, v), ix_cand(L, 1))) &&
-                    (v < 3 || !tile_eq(ix_cand(L, v), ix_cand(L, 2))));
+                    (v < 3 || !tile_eq(ix_cand(L, v), ix_cand(L, 2))) &&
+                    (v < 4 || !tile_eq(ix_cand(L, v), ix_cand(L, 3))));
 }
 
 template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
@@ -265,6 +272,8 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
       if constexpr (ix_valid(LL, 1)) tile(std::integral_constant<int, 1>{});
     } else if (v == 2 && ix_valid(LL, 2)) {
       if constexpr (ix_valid(LL, 2)) tile(std::integral_constant<int, 2>{});
+    } else if (v == 4 && ix_valid(LL, 4)) {
+      if constexpr (ix_valid(LL, 4)) tile(std::integral_constant<int, 4>{});
     } else {
       tile(std::integral_constant<int, 0>{});
     }
@@ -295,7 +304,9 @@ static cudaError_t z_slots(const Geo& g, void* P, const void* tw, cudaStream_t s
 
 // z candidates (forms 0, 1, 2): 1 = the slot kernel with 8 elements per thread
 // (12 with a factor 3), 2 = the slot kernel with 4 (power-of-two lines), 3 = the
-// FP32 register kernel with 4 elements per thread (lines of up to 256 points)
+// FP32 register kernel with 4 elements per thread (lines of up to 256 points),
+// 4 = the FP32 register kernel on 1024-point lines (two warps per line) with every
+// component's loads issued up front
 template <int NZ, int FORM> constexpr bool z_rule_slots() {
   constexpr int M = NZ / 2;
   return !(std::is_same<T, float>::value && M <= 512) &&
@@ -305,7 +316,8 @@ template <int NZ, int FORM> constexpr bool z_valid(int v) {
   constexpr int M = NZ / 2;
   return v == 0 || (FORM <= 2 && ((v == 1 && !z_rule_slots<NZ, FORM>()) ||
                                   (v == 2 && M % 3 != 0 && M >= 8 && M / 4 <= 256) ||
-                                  (v == 3 && std::is_same<T, float>::value && M % 3 != 0 && M >= 8 && M / 4 <= 64)));
+                                  (v == 3 && std::is_same<T, float>::value && M % 3 != 0 && M >= 8 && M / 4 <= 64) ||
+                                  (v == 4 && std::is_same<T, float>::value && M == 512)));
 }
 
 template <int NZ, int FORM>
@@ -321,6 +333,15 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
   }
   if constexpr (z_valid<NZ, FORM>(2)) {
     if (v == 2) return z_slots<NZ, FORM, 4>(g, P, tw, st, nmem, msP, zkeep);
+  }
+  if constexpr (z_valid<NZ, FORM>(4)) {
+    if (v == 4) {
+      constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
+      k_z_reg<T, NZ, FORM, 0, true><<<dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), NT, 0, st>>>(
+          (V*)P, g, (const V*)tw, msP, zkeep);
+      ++g_launches;
+      return cudaGetLastError();
+    }
   }
   if constexpr (z_valid<NZ, FORM>(3)) {
     if (v == 3) {

@@ -45,6 +45,8 @@ FFF_CASES = [
     ((32, 256, 256), "f32", "rotational", "two_thirds"),
     ((32, 32, 1024), "f32", "rotational", "two_thirds"),
     ((1024, 16, 32), "f32", "conservative", "reference"),
+    ((1024, 32, 32), "f32", "rotational", "two_thirds"),
+    ((32, 1024, 32), "f32", "rotational", "two_thirds"),
     ((64, 64, 64), "f64", "conservative", "reference"),
     ((32, 128, 64), "f64", "rotational", "two_thirds"),
 ]
