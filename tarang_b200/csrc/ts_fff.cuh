@@ -346,6 +346,81 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
 
 
 // ---------------------------------------------------------------------------
+// inverse x pass with the tile's U staged in shared memory (two-thirds dealiasing,
+// FORM 0 / 1): one column tile per block (the kept-column mapping of k_inv_x_ld); every
+// thread stages the kept rows (3 |kx| <= Nx) of the three components that it will read
+// itself with cp.async, all in one group, so a tile pays one load latency instead of one
+// per output field; the output fields are then built from shared memory (the vorticity
+// from the staged components) and transformed through a separate exchange tile.
+// Shared memory: 3 x LK x CW staged complex (LK = 2 (L/3) + 1 kept rows) + L x CW exchange.
+// ---------------------------------------------------------------------------
+template <int L> __host__ __device__ constexpr int ix_kept_rows() { return 2 * (L / 3) + 1; }
+template <typename T, int L, int E, int CW, int FORM>
+__global__ void __launch_bounds__(CW * (L / E), 1)
+    k_inv_x_st(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw) {
+  typedef C<T> V;
+  static_assert(FORM == 0 || FORM == 1, "the fluid forms");
+  constexpr int LK = ix_kept_rows<L>(), Q = L / 3;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* xch = reinterpret_cast<V*>(smraw);  // exchange tile, L x CW
+  V* stg = xch + L * CW;                  // staged kept rows, 3 x LK x CW
+  const int c = threadIdx.x % CW, t = threadIdx.x / CW;
+  const int inner = g.Ny * g.Hz;
+  const long long rstride = inner;
+  const int qy = g.Ny / 3, nzk = g.Nz / 3 + 1, ntz = (nzk + CW - 1) / CW;
+  const int iy = blockIdx.x / ntz, lzc = (blockIdx.x % ntz) * CW + c;
+  const int ky = iy <= qy ? iy : iy - (2 * qy + 1);
+  const bool ok = lzc < nzk;
+  const int col = ((ky + g.Ny) % g.Ny) * g.Hz + (ok ? lzc : 0);
+  const int lz = ok ? lzc : 0;
+  const T Ky = (T)(ky * g.kf[1]), Kz = (T)(lz * g.kf[2]);
+  // staged row of x row lx (kept rows only: lx <= Q or lx >= L - Q)
+  auto krow = [](int lx) { return lx <= Q ? lx : lx - (L - 2 * Q - 1); };
+  auto kept = [](int lx) { return lx <= Q || lx >= L - Q; };
+  if (ok) {
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int lx = load_row<L, E>(t, s);
+      if (kept(lx))
+#pragma unroll
+        for (int q = 0; q < 3; ++q) cp_async(stg + (q * LK + krow(lx)) * CW + c, U + q * g.S + lx * rstride + col);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait<0>();  // each thread reads back only the rows it staged itself
+  constexpr int nout = FORM == 0 ? 3 : 6;
+#pragma unroll 1
+  for (int f = 0; f < nout; ++f) {
+    V v[E];
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int lx = load_row<L, E>(t, s);
+      V a = mk<V>(0, 0);
+      if (ok && kept(lx)) {
+        const V* st = stg + krow(lx) * CW + c;
+        if (f < 3) {
+          a = st[f * LK * CW];
+        } else {
+          // omega_i = i (K_{i+1} U_{i+2} - K_{i+2} U_{i+1})  (indices mod 3)
+          const T Kx = (T)(kfft(lx, g.Nx) * g.kf[0]);
+          const int i = f - 3, i1 = i == 2 ? 0 : i + 1, i2 = i == 0 ? 2 : i - 1;
+          const T Ka = i1 == 0 ? Kx : (i1 == 1 ? Ky : Kz);
+          const T Kb = i2 == 0 ? Kx : (i2 == 1 ? Ky : Kz);
+          a = mul_i<1>(sub(scale(st[i2 * LK * CW], Ka), scale(st[i1 * LK * CW], Kb)));
+        }
+      }
+      v[s] = a;
+    }
+    fft_regs<L, E, 1, 0, false, false, best_swk(L, E, CW, (int)sizeof(V))>(v, t, xch, CW, c, tw, 1);
+    if (ok) {
+      V* d = W + f * g.S + col;
+#pragma unroll
+      for (int s = 0; s < E; ++s) d[final_row<L, E>(t, s) * rstride] = v[s];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // inverse x pass, persistent with a prefetch (FP32, FORM 0 / 1): each block walks the
 // column tiles tile = blockIdx.x + k G; every thread stages the dealiased U rows it
 // owns (rows load_row(t, s) of its column) with cp.async into its own slots of a

@@ -199,20 +199,24 @@ constexpr int ix_e_alt(int L) {
 // candidate 3 (FP32): the persistent prefetching kernel k_inv_x_pf, 8 elements per thread
 // (the three components of U held in registers), staging + exchange tiles (NT = 4 tiles);
 // candidate 4 (FP32, 1024-point lines): 32 elements per thread over 8-column tiles
-// (256-thread blocks, two per SM; radix 32 x 32, one exchange per field)
+// (256-thread blocks, two per SM; radix 32 x 32, one exchange per field);
+// candidate 5 (FP32, 1024-point lines, two-thirds dealiasing): k_inv_x_st, the tile's
+// kept U rows staged in shared memory in one cp.async group (the rule elsewhere)
 constexpr Tile ix_cand(int L, int v) {
   return v == 0 ? Tile{ix_e(L), ix_cw(L), 1}
        : v == 1 ? (ix_e_alt(L) > 0 ? Tile{ix_e_alt(L), cw_for(L, ix_e_alt(L)), 1} : Tile{0, 0, 0})
        : v == 2 ? (ix_cw(L) > 1 ? Tile{ix_e(L), ix_cw(L) / 2, 1} : Tile{0, 0, 0})
        : v == 3 ? (std::is_same<T, float>::value ? Tile{8, cw_for(L, 8), 4} : Tile{0, 0, 0})
        : v == 4 ? (wide1024(L) ? Tile{32, 8, 1} : Tile{0, 0, 0})
+       : v == 5 ? (wide1024(L) ? Tile{16, 8, 2} : Tile{0, 0, 0})
                 : Tile{0, 0, 0};
 }
 constexpr bool ix_valid(int L, int v) {
   return v == 0 || (v < NCAND && tile_fits(L, ix_cand(L, v), ix_cand(L, v).NT == 4 ? 4 : 1) &&
                     !tile_eq(ix_cand(L, v), ix_cand(L, 0)) && (v < 2 || !tile_eq(ix_cand(L, v), ix_cand(L, 1))) &&
                     (v < 3 || !tile_eq(ix_cand(L, v), ix_cand(L, 2))) &&
-                    (v < 4 || !tile_eq(ix_cand(L, v), ix_cand(L, 3))));
+                    (v < 4 || !tile_eq(ix_cand(L, v), ix_cand(L, 3))) &&
+                    (v < 5 || !tile_eq(ix_cand(L, v), ix_cand(L, 4))));
 }
 
 template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, void* W, const void* tw,
@@ -222,6 +226,24 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
   const int v = form <= 1 ? g.tv[TUNE_X_INV] : 0;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
+    if constexpr (ix_valid(LL, 5)) {
+      if (v == 5 && kept) {
+        // the kept U rows of a tile staged in shared memory (one load latency per tile)
+        constexpr Tile c = ix_cand(LL, 5);
+        constexpr int E = c.E, CW = c.CW;
+        const size_t sm = ((size_t)LL + 3 * ix_kept_rows<LL>()) * CW * sizeof(V);
+        const int nzk = g.Nz / 3 + 1;
+        const unsigned blocks = (unsigned)((2 * (g.Ny / 3) + 1) * ((nzk + CW - 1) / CW));
+        auto run = [&](auto kern) {
+          if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
+          kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw);
+          ++g_launches;
+          err_ = cudaGetLastError();
+        };
+        if (form == 0) { run(k_inv_x_st<T, LL, E, CW, 0>); return; }
+        if (form == 1) { run(k_inv_x_st<T, LL, E, CW, 1>); return; }
+      }
+    }
     if constexpr (ix_valid(LL, 3)) {
       if (v == 3) {
         // persistent, prefetching form: one block per SM
