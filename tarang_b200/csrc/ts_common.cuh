@@ -55,19 +55,18 @@ template <int SIGN, typename V> __device__ __forceinline__ V mul_i(V a) {
 // i * K * a for real K
 template <typename V, typename S> __device__ __forceinline__ V ik(S K, V a) { return mk<V>(-K * a.y, K * a.x); }
 
-// cos / sin of pi*k/8, k = 0..8 (exact mathematical constants)
-__device__ __forceinline__ double c16(int k) {
-  const double t[9] = {1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173, 0.0,
-                       -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613, -1.0};
+// cos / sin of pi*k/16, k = 0..16 (exact mathematical constants)
+__device__ __forceinline__ double c32(int k) {
+  const double t[17] = {1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+                        0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+                        0.19509032201612826785, 0.0, -0.19509032201612826785, -0.38268343236508977173,
+                        -0.55557023301960222474, -0.70710678118654752440, -0.83146961230254523708,
+                        -0.92387953251128675613, -0.98078528040323044913, -1.0};
   return t[k];
 }
-__device__ __forceinline__ double s16(int k) {
-  const double t[9] = {0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613, 1.0,
-                       0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173, 0.0};
-  return t[k];
-}
+__device__ __forceinline__ double s32(int k) { return k <= 8 ? c32(8 - k) : c32(k - 8); }
 
-// In-register DFT of size R (2,4,8,16), natural order in and out.
+// In-register DFT of size R (2, 3, 4, 8, 16, 32), natural order in and out.
 // DIR = -1: forward (e^{-2 pi i jk/R}), +1: inverse (unnormalised).
 template <int R, int DIR, typename V> struct DFT;
 template <int DIR, typename V> struct DFT<1, DIR, V> {
@@ -104,10 +103,11 @@ template <int R, int DIR, typename V> struct DFT {
 #pragma unroll
     for (int k = 0; k < R / 2; ++k) {
       V t;
-      const int q = k * (16 / R);  // angle pi*q/8 = 2 pi k / R
+      static_assert(R <= 32, "the twiddle table covers radices up to 32");
+      const int q = k * (32 / R);  // angle pi*q/16 = 2 pi k / R
       if (k == 0) t = o[k];
       else if (4 * k == R) t = mul_i<DIR>(o[k]);
-      else t = mul(o[k], mk<V>((S)c16(q), (S)(DIR * s16(q))));
+      else t = mul(o[k], mk<V>((S)c32(q), (S)(DIR * s32(q))));
       v[k] = add(e[k], t);
       v[k + R / 2] = sub(e[k], t);
     }
@@ -416,66 +416,72 @@ template <typename V> __device__ __forceinline__ bool nonfinite(const V& v) { re
 
 // ---------------------------------------------------------------------------
 // IF-RK4 stage arithmetic of one mode (RK.cc:91-170: Single_time_step,
-// Compute_RK4_parts).  eh = E(1/2) = exp(-nu dt K^2 / 2), e1 = E(1) (FP64 tables);
-// c = the dt factor.  The templates compute every product and sum in FP64 with one
-// rounding per stored value (in FP64 the plain expressions).  In the FP32 path a factor
-// rounded to FP32 (eh or e1 to 24 bits) would scale a mode by the same wrong amount
-// every step, a bias that grows linearly with the step count.
+// Compute_RK4_parts).  eh = E(1/2) = exp(-nu dt K^2 / 2), e1 = E(1) (from FP64 tables);
+// c = the dt factor.  Each factor reaches the arithmetic as a Fac: in FP64 the value; in
+// FP32 the pair hi = fl32(x), lo = fl32(x - hi), applied as a x = fma(a, hi, a lo), so
+// the factor carries about 48 bits.  A factor rounded to FP32 (eh or e1 to 24 bits) would
+// scale a mode by the same wrong amount every step, a bias that grows linearly with the
+// step count.  The state update u0 E(1) + (tot + R dt/6) folds the small terms into one
+// fma chain, fma(u0, e1.hi, fma(u0, e1.lo, tot + R dt/6)), so the decay u0 (E(1) - 1),
+// often below half an FP32 ulp of u0, reaches the single final rounding instead of being
+// rounded away (which would bias slowly decaying modes towards no decay).  No FP64
+// operation and no FP64 <-> FP32 conversion runs per component.
 // ---------------------------------------------------------------------------
-template <typename S> __device__ __forceinline__ S rk_u1(S u0, S R, double eh, double c) {
-  return (S)(((double)u0 + (double)R * c) * eh);      // (u0 + R dt/2) E(1/2)
-}
-template <typename S> __device__ __forceinline__ S rk_t1(S R, double e1, double c) {
-  return (S)(((double)R * e1) * c);                   // (R E(1)) dt/6
-}
-template <typename S> __device__ __forceinline__ S rk_u2(S u0, S R, double eh, double c) {
-  return (S)((double)u0 * eh + (double)R * c);        // u0 E(1/2) + R dt/2
-}
-template <typename S> __device__ __forceinline__ S rk_tacc(S tt, S R, double eh, double c) {
-  return (S)((double)tt + ((double)R * eh) * c);      // tot + (R E(1/2)) dt/3
-}
-template <typename S> __device__ __forceinline__ S rk_u3(S u0, S R, double eh, double c) {
-  return (S)(((double)u0 * eh + (double)R * c) * eh); // (u0 E(1/2) + R dt) E(1/2)
-}
-template <typename S> __device__ __forceinline__ S rk_u4(S u0, S tt, S R, double e1, double c) {
-  return (S)((double)u0 * e1 + ((double)tt + (double)R * c));  // u0 E(1) + (tot + R dt/6)
-}
-// FP32 stages 1-3: the stage fields are rounded to FP32 before the next right-hand side
-// anyway, and their rounding does not carry from step to step (each step restarts from
-// the stored state), so these run in FP32 with every factor applied exactly: x as the
-// pair hi = fl32(x), lo = fl32(x - hi), and a x = fma(a, hi, a lo) rounded once.  Only
-// stage 4, whose rounding enters the state every step, stays in FP64 (rk_u4 above).
-struct Fx { float hi, lo; };
-__device__ __forceinline__ Fx fx(double x) {
+template <typename S> struct Fac;
+template <> struct Fac<double> { double v; };
+template <> struct Fac<float> { float hi, lo; };
+template <typename S> __device__ __forceinline__ Fac<S> fac(double x);
+template <> __device__ __forceinline__ Fac<double> fac<double>(double x) { return {x}; }
+template <> __device__ __forceinline__ Fac<float> fac<float>(double x) {
   const float h = (float)x;
   return {h, (float)(x - (double)h)};
 }
-__device__ __forceinline__ float fmul(float a, Fx f) { return fmaf(a, f.hi, a * f.lo); }
-template <> __device__ __forceinline__ float rk_u1(float u0, float R, double eh, double c) {
-  return fmul(u0 + fmul(R, fx(c)), fx(eh));
+__device__ __forceinline__ float fmulx(float a, Fac<float> f) { return fmaf(a, f.hi, a * f.lo); }
+// a x + b, the low part of x folded into b before the final fma
+__device__ __forceinline__ float fmaddx(float a, Fac<float> f, float b) { return fmaf(a, f.hi, fmaf(a, f.lo, b)); }
+
+// FP64: the plain expressions
+__device__ __forceinline__ double rk_u1(double u0, double R, Fac<double> eh, Fac<double> c) {
+  return (u0 + R * c.v) * eh.v;               // (u0 + R dt/2) E(1/2)
 }
-template <> __device__ __forceinline__ float rk_t1(float R, double e1, double c) {
-  return fmul(fmul(R, fx(e1)), fx(c));
+__device__ __forceinline__ double rk_t1(double R, Fac<double> e1, Fac<double> c) { return (R * e1.v) * c.v; }
+__device__ __forceinline__ double rk_u2(double u0, double R, Fac<double> eh, Fac<double> c) {
+  return u0 * eh.v + R * c.v;                 // u0 E(1/2) + R dt/2
 }
-template <> __device__ __forceinline__ float rk_u2(float u0, float R, double eh, double c) {
-  return fmul(u0, fx(eh)) + fmul(R, fx(c));
+__device__ __forceinline__ double rk_tacc(double tt, double R, Fac<double> eh, Fac<double> c) {
+  return tt + (R * eh.v) * c.v;               // tot + (R E(1/2)) dt/3
 }
-template <> __device__ __forceinline__ float rk_tacc(float tt, float R, double eh, double c) {
-  return tt + fmul(fmul(R, fx(eh)), fx(c));
+__device__ __forceinline__ double rk_u3(double u0, double R, Fac<double> eh, Fac<double> c) {
+  return (u0 * eh.v + R * c.v) * eh.v;        // (u0 E(1/2) + R dt) E(1/2)
 }
-template <> __device__ __forceinline__ float rk_u3(float u0, float R, double eh, double c) {
-  return fmul(fmul(u0, fx(eh)) + fmul(R, fx(c)), fx(eh));
+__device__ __forceinline__ double rk_u4(double u0, double tt, double R, Fac<double> e1, Fac<double> c) {
+  return u0 * e1.v + (tt + R * c.v);          // u0 E(1) + (tot + R dt/6)
+}
+// FP32: exact factors, small terms folded before the last rounding
+__device__ __forceinline__ float rk_u1(float u0, float R, Fac<float> eh, Fac<float> c) {
+  return fmulx(fmaf(R, c.hi, fmaf(R, c.lo, u0)), eh);
+}
+__device__ __forceinline__ float rk_t1(float R, Fac<float> e1, Fac<float> c) { return fmulx(fmulx(R, e1), c); }
+__device__ __forceinline__ float rk_u2(float u0, float R, Fac<float> eh, Fac<float> c) {
+  return fmaddx(u0, eh, fmulx(R, c));
+}
+__device__ __forceinline__ float rk_tacc(float tt, float R, Fac<float> eh, Fac<float> c) {
+  return tt + fmulx(fmulx(R, eh), c);
+}
+__device__ __forceinline__ float rk_u3(float u0, float R, Fac<float> eh, Fac<float> c) {
+  return fmulx(fmaddx(u0, eh, fmulx(R, c)), eh);
+}
+__device__ __forceinline__ float rk_u4(float u0, float tt, float R, Fac<float> e1, Fac<float> c) {
+  return fmaddx(u0, e1, tt + fmulx(R, c));
 }
 #define TS_RK_CPLX(NAME, ...) \
-  template <typename V> __device__ __forceinline__ V NAME##_c(__VA_ARGS__)
-TS_RK_CPLX(rk_u1, V u0, V R, double eh, double c) { return mk<V>(rk_u1(u0.x, R.x, eh, c), rk_u1(u0.y, R.y, eh, c)); }
-TS_RK_CPLX(rk_t1, V R, double e1, double c) { return mk<V>(rk_t1(R.x, e1, c), rk_t1(R.y, e1, c)); }
-TS_RK_CPLX(rk_u2, V u0, V R, double eh, double c) { return mk<V>(rk_u2(u0.x, R.x, eh, c), rk_u2(u0.y, R.y, eh, c)); }
-TS_RK_CPLX(rk_tacc, V tt, V R, double eh, double c) {
-  return mk<V>(rk_tacc(tt.x, R.x, eh, c), rk_tacc(tt.y, R.y, eh, c));
-}
-TS_RK_CPLX(rk_u3, V u0, V R, double eh, double c) { return mk<V>(rk_u3(u0.x, R.x, eh, c), rk_u3(u0.y, R.y, eh, c)); }
-TS_RK_CPLX(rk_u4, V u0, V tt, V R, double e1, double c) {
+  template <typename V, typename F> __device__ __forceinline__ V NAME##_c(__VA_ARGS__)
+TS_RK_CPLX(rk_u1, V u0, V R, F eh, F c) { return mk<V>(rk_u1(u0.x, R.x, eh, c), rk_u1(u0.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_t1, V R, F e1, F c) { return mk<V>(rk_t1(R.x, e1, c), rk_t1(R.y, e1, c)); }
+TS_RK_CPLX(rk_u2, V u0, V R, F eh, F c) { return mk<V>(rk_u2(u0.x, R.x, eh, c), rk_u2(u0.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_tacc, V tt, V R, F eh, F c) { return mk<V>(rk_tacc(tt.x, R.x, eh, c), rk_tacc(tt.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_u3, V u0, V R, F eh, F c) { return mk<V>(rk_u3(u0.x, R.x, eh, c), rk_u3(u0.y, R.y, eh, c)); }
+TS_RK_CPLX(rk_u4, V u0, V tt, V R, F e1, F c) {
   return mk<V>(rk_u4(u0.x, tt.x, R.x, e1, c), rk_u4(u0.y, tt.y, R.y, e1, c));
 }
 #undef TS_RK_CPLX

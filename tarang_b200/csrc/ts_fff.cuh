@@ -1311,7 +1311,9 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
                    scale(add(N3, ik(Kz, pr)), (T)-1)};
   // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
   const double eh = a.ex[lx] * exy;
-  const double e1 = eh * eh;
+  const Fac<T> Feh = fac<T>(eh), Fe1 = fac<T>(eh * eh);
+  const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+               Fc6 = fac<T>((1.0 / 6) * a.dt);
   V* Uc = reinterpret_cast<V*>(a.Ucur);
   V* tot = reinterpret_cast<V*>(a.tot);
   const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
@@ -1322,18 +1324,18 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
     const V R = Rv[i];
     const V u0 = st0[i * sstr];
     if (a.stage == 1) {
-      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+      Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, Fc2);
+      tot[o] = rk_t1_c(R, Fe1, Fc6);
     } else {
       const V tt = st1[i * sstr];
       if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2_c(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc_c(tt, R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
-        tot[o] = rk_tacc_c(tt, R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3_c(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc_c(tt, R, Feh, Fc3);
       } else {
-        const V un = rk_u4_c(u0, tt, R, e1, (1.0 / 6) * a.dt);
+        const V un = rk_u4_c(u0, tt, R, Fe1, Fc6);
         reinterpret_cast<V*>(a.Uout)[o] = (a.reality && lz == g.Nz / 2) ? mk<V>(0, 0) : un;
         health_mark(nonfinite(un), a.err);
       }

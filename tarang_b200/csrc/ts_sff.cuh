@@ -257,27 +257,29 @@ __device__ __forceinline__ void sff_epilogue(const Geo& g, const SffArgs& a, lon
   const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
   const double ehu = a.eu[0][tb + m] * a.eu[1][tb + ly] * a.eu[2][tb + lz];
   const double eht = a.et[0][tb + m] * a.et[1][tb + ly] * a.et[2][tb + lz];
+  const Fac<T> Fhu = fac<T>(ehu), F1u = fac<T>(ehu * ehu), Fht = fac<T>(eht), F1t = fac<T>(eht * eht);
+  const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+               Fc6 = fac<T>((1.0 / 6) * a.dt);
   const bool dz = dealias_zero(g.dealias, 1, m, ly, lz, g.Nx, g.Ny, g.Nz);
   // the stage update of field i; returns the value stored (the new stage field, or at
   // stage 4 the new state)
   auto advance = [&](int i) -> V {
-    const double eh = i < 3 ? ehu : eht;
-    const double e1 = eh * eh;
+    const Fac<T> Feh = i < 3 ? Fhu : Fht, Fe1 = i < 3 ? F1u : F1t;
     const long long o = i * g.S + off;
     const V R = Rv[i];
     const V u0 = i < 3 ? U0[o] : T0[off];
     V r;
     if (a.stage == 1) {
-      Uc[o] = r = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-      tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+      Uc[o] = r = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, Fc2);
+      tot[o] = rk_t1_c(R, Fe1, Fc6);
     } else if (a.stage == 2) {
-      Uc[o] = r = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-      tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+      Uc[o] = r = rk_u2_c(u0, R, Feh, Fc2);
+      tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
     } else if (a.stage == 3) {
-      Uc[o] = r = rk_u3_c(u0, R, eh, a.dt);
-      tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+      Uc[o] = r = rk_u3_c(u0, R, Feh, Fc1);
+      tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
     } else {
-      r = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+      r = rk_u4_c(u0, tot[o], R, Fe1, Fc6);
       if (a.reality && lz == g.Nz / 2) r = mk<V>(0, 0);
       if (i < 3) const_cast<V*>(U0)[o] = r;
       else const_cast<V*>(T0)[off] = r;
@@ -520,25 +522,27 @@ __global__ void __launch_bounds__(256) k_scalar_epi(const C<T>* __restrict__ P, 
     const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
     const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lz];
     const double eht = a.et[0][lx] * a.et[1][ly] * a.et[2][lz];
+    const Fac<T> Fhu = fac<T>(ehu), F1u = fac<T>(ehu * ehu), Fht = fac<T>(eht), F1t = fac<T>(eht * eht);
+    const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+                 Fc6 = fac<T>((1.0 / 6) * a.dt);
     const bool dz = dealias_zero(g.dealias, 0, lx, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double eh = i < 3 ? ehu : eht;
-      const double e1 = eh * eh;
+      const Fac<T> Feh = i < 3 ? Fhu : Fht, Fe1 = i < 3 ? F1u : F1t;
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, Fc2);
+        tot[o] = rk_t1_c(R, Fe1, Fc6);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2_c(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3_c(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else {
-        V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+        V un = rk_u4_c(u0, tot[o], R, Fe1, Fc6);
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(T0)[e] = un;
@@ -606,25 +610,27 @@ __global__ void __launch_bounds__(256, 3) k_mhd_epi(const C<T>* __restrict__ P, 
     }
     const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lz];
     const double ehb = a.et[0][lx] * a.et[1][ly] * a.et[2][lz];
+    const Fac<T> Fhu = fac<T>(ehu), F1u = fac<T>(ehu * ehu), Fht = fac<T>(ehb), F1t = fac<T>(ehb * ehb);
+    const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+                 Fc6 = fac<T>((1.0 / 6) * a.dt);
     const bool dz = dealias_zero(g.dealias, 0, lx, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-      const double eh = i < 3 ? ehu : ehb;
-      const double e1 = eh * eh;
+      const Fac<T> Feh = i < 3 ? Fhu : Fht, Fe1 = i < 3 ? F1u : F1t;
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : B0[(i - 3) * g.S + e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, Fc2);
+        tot[o] = rk_t1_c(R, Fe1, Fc6);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2_c(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3_c(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else {
-        V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+        V un = rk_u4_c(u0, tot[o], R, Fe1, Fc6);
         if (a.reality && lz == g.Nz / 2) un = mk<V>(0, 0);
         if (i < 3) const_cast<V*>(U0)[o] = un;
         else const_cast<V*>(B0)[(i - 3) * g.S + e] = un;
@@ -675,7 +681,9 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
     N3 = add(N3, ik(Kz, pr));
     const V Rv[3] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1)};
     const double eh = a.ex[lx] * a.ey[ly] * a.ez[lz];
-    const double e1 = eh * eh;
+    const Fac<T> Feh = fac<T>(eh), Fe1 = fac<T>(eh * eh);
+    const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+                 Fc6 = fac<T>((1.0 / 6) * a.dt);
     const bool dz = dealias_zero(g.dealias, 2, lx, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -683,16 +691,16 @@ __global__ void __launch_bounds__(256) k_ssf_epi(const C<T>* __restrict__ P, Geo
       const V R = Rv[i];
       const V u0 = U0[o];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, Fc2);
+        tot[o] = rk_t1_c(R, Fe1, Fc6);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2_c(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3_c(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else {
-        const V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+        const V un = rk_u4_c(u0, tot[o], R, Fe1, Fc6);
         Uo[o] = un;
         health_mark(nonfinite(un), a.err);
       }
@@ -755,23 +763,25 @@ __global__ void __launch_bounds__(256) k_sss_epi(const T* __restrict__ P, Geo g,
     N3 += -Kz * pr;
     const T Rv[3] = {-N1, -N2, -N3};
     const double eh = a.ex[lx] * a.ey[ly] * a.ez[lzr];
-    const double e1 = eh * eh;
+    const Fac<T> Feh = fac<T>(eh), Fe1 = fac<T>(eh * eh);
+    const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+                 Fc6 = fac<T>((1.0 / 6) * a.dt);
     const bool dz = sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const long long o = i * per + e;
       const T R = Rv[i], u0 = U0[o];
       if (a.stage == 1) {
-        Uc[o] = rk_u1(dz ? (T)0 : u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_t1(R, e1, (1.0 / 6) * a.dt);
+        Uc[o] = rk_u1(dz ? (T)0 : u0, R, Feh, Fc2);
+        tot[o] = rk_t1(R, Fe1, Fc6);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc(tot[o], R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3(u0, R, eh, a.dt);
-        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc(tot[o], R, Feh, Fc3);
       } else {
-        const T un = rk_u4(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+        const T un = rk_u4(u0, tot[o], R, Fe1, Fc6);
         Uo[o] = un;
         health_mark(!isfinite(un), a.err);
       }
@@ -828,25 +838,27 @@ __global__ void __launch_bounds__(256) k_ssf_rbc_epi(const C<T>* __restrict__ P,
     const V Rv[4] = {scale(N1, (T)-1), scale(N2, (T)-1), scale(N3, (T)-1), scale(NT, (T)-1)};
     const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lz];
     const double eht = a.et[0][lx] * a.et[1][ly] * a.et[2][lz];
+    const Fac<T> Fhu = fac<T>(ehu), F1u = fac<T>(ehu * ehu), Fht = fac<T>(eht), F1t = fac<T>(eht * eht);
+    const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+                 Fc6 = fac<T>((1.0 / 6) * a.dt);
     const bool dz = dealias_zero(g.dealias, 2, lx, ly, lz, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double eh = i < 3 ? ehu : eht;
-      const double e1 = eh * eh;
+      const Fac<T> Feh = i < 3 ? Fhu : Fht, Fe1 = i < 3 ? F1u : F1t;
       const long long o = i * g.S + e;
       const V R = Rv[i];
       const V u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_t1_c(R, e1, (1.0 / 6) * a.dt);
+        Uc[o] = rk_u1_c(dz ? mk<V>(0, 0) : u0, R, Feh, Fc2);
+        tot[o] = rk_t1_c(R, Fe1, Fc6);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2_c(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2_c(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3_c(u0, R, eh, a.dt);
-        tot[o] = rk_tacc_c(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3_c(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc_c(tot[o], R, Feh, Fc3);
       } else {
-        const V un = rk_u4_c(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+        const V un = rk_u4_c(u0, tot[o], R, Fe1, Fc6);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
         health_mark(nonfinite(un), a.health);
@@ -891,24 +903,26 @@ __global__ void __launch_bounds__(256) k_sss_rbc_epi(const T* __restrict__ P, Ge
     const T Rv[4] = {-N1, -N2, -N3, -NT};
     const double ehu = a.eu[0][lx] * a.eu[1][ly] * a.eu[2][lzr];
     const double eht = a.et[0][lx] * a.et[1][ly] * a.et[2][lzr];
+    const Fac<T> Fhu = fac<T>(ehu), F1u = fac<T>(ehu * ehu), Fht = fac<T>(eht), F1t = fac<T>(eht * eht);
+    const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
+                 Fc6 = fac<T>((1.0 / 6) * a.dt);
     const bool dz = sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double eh = i < 3 ? ehu : eht;
-      const double e1 = eh * eh;
+      const Fac<T> Feh = i < 3 ? Fhu : Fht, Fe1 = i < 3 ? F1u : F1t;
       const long long o = i * per + e;
       const T R = Rv[i], u0 = i < 3 ? U0[o] : T0[e];
       if (a.stage == 1) {
-        Uc[o] = rk_u1(dz ? (T)0 : u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_t1(R, e1, (1.0 / 6) * a.dt);
+        Uc[o] = rk_u1(dz ? (T)0 : u0, R, Feh, Fc2);
+        tot[o] = rk_t1(R, Fe1, Fc6);
       } else if (a.stage == 2) {
-        Uc[o] = rk_u2(u0, R, eh, 0.5 * a.dt);
-        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u2(u0, R, Feh, Fc2);
+        tot[o] = rk_tacc(tot[o], R, Feh, Fc3);
       } else if (a.stage == 3) {
-        Uc[o] = rk_u3(u0, R, eh, a.dt);
-        tot[o] = rk_tacc(tot[o], R, eh, (1.0 / 3) * a.dt);
+        Uc[o] = rk_u3(u0, R, Feh, Fc1);
+        tot[o] = rk_tacc(tot[o], R, Feh, Fc3);
       } else {
-        const T un = rk_u4(u0, tot[o], R, e1, (1.0 / 6) * a.dt);
+        const T un = rk_u4(u0, tot[o], R, Fe1, Fc6);
         if (i < 3) U0[o] = un;
         else T0[e] = un;
         health_mark(!isfinite(un), a.health);
