@@ -286,11 +286,14 @@ int ts_adjoint_window(ts_plan* plan, const void* u_start, int nsteps, void* lam_
  * the library holds a fixed rule (candidate 0) and up to five other kernel
  * candidates that change the radix schedule (elements per thread, so the
  * Stockham passes' radices), the column-tile width, the staging depth (y passes:
- * candidate 4 keeps two items in flight ahead of the one transformed; candidate 5
- * at 1024 points in FP32, one tile per block and 32 elements per thread), or the
- * kernel form (z: shared-memory slot kernels, and at 1024 points the register
- * kernel with every load issued up front; FFF forward x: split x FFF +
- * elementwise epilogue; SFF forward x: the other fused/split choice), plus a
+ * candidate 4 keeps two items in flight ahead of the one transformed; at 1024 points
+ * in FP32 the y forward rule is one tile per block with 32 elements per thread and
+ * candidate 5 swaps it with the y inverse rule's form), or the kernel form (z:
+ * shared-memory slot kernels, and at 1024 points in FP32 candidate 4 loads each
+ * component just before its transform; FFF inverse x at 1024 points in FP32 under
+ * two-thirds dealiasing: candidate 5 swaps the staged rule kernel with the
+ * direct-load one; FFF forward x: split x FFF + elementwise epilogue; SFF forward x:
+ * the other fused/split choice), plus a
  * blocks-per-SM count for the persistent launches (y passes, fused FFF
  * forward x; 0 = the rule).  Every candidate computes the same transform;
  * results differ from the rule's in rounding only.

@@ -73,6 +73,7 @@ struct ts_plan {
   int rbc_slave = 0;                // 1: PRZERO (T slaved to U), 2: PRINFTY (U slaved to T)
   double rbc_vs = 0;                // PRINFTY: factor of the slaved velocity
   double* eax[3] = {nullptr, nullptr, nullptr};  // per-axis exp(-nu dt K_i^2 / 2)
+  float2* eaxf[3] = {nullptr, nullptr, nullptr}; // the same as FP32 (hi, lo) pairs
   double* eaxT[3] = {nullptr, nullptr, nullptr}; // per-axis exp(-kappa dt K_i^2 / 2) (SFF scalar)
   void* twq = nullptr;      // SFF, SSF: exp(-2 pi i j / (4 Nx)), j < 4 Nx
   void* twqy = nullptr;     // SSF, SSS: exp(-2 pi i j / (4 Ny)), j < 4 Ny
@@ -288,7 +289,8 @@ static int ensure_stage(void** buf, size_t bytes) {
 
 // Integrating-factor tables: E(1/2)(K) = exp(-nu dt K^2 / 2) factorises over the
 // axes, exp(-nu dt/2 Kx^2) exp(-nu dt/2 Ky^2) exp(-nu dt/2 Kz^2) (FP64)
-static int upload_if_tables(ts_plan* p, double nu, double dt, double** tab) {
+// tabf (optional): the same factors as FP32 pairs hi = fl32(x), lo = fl32(x - hi)
+static int upload_if_tables(ts_plan* p, double nu, double dt, double** tab, float2** tabf = nullptr) {
   const Geo& g = p->g;
   // SSS: real z coefficients kz = lz < Nz
   const int n[3] = {g.Nx, g.Ny, g.basis == TS_BASIS_SSS ? g.Nz : g.Hz};
@@ -304,6 +306,15 @@ static int upload_if_tables(ts_plan* p, double nu, double dt, double** tab) {
     }
     if (!tab[ax]) CK(cudaMalloc(&tab[ax], n[ax] * sizeof(double)));
     CK(cudaMemcpy(tab[ax], h.data(), n[ax] * sizeof(double), cudaMemcpyHostToDevice));
+    if (tabf) {
+      std::vector<float2> hf(n[ax]);
+      for (int l = 0; l < n[ax]; ++l) {
+        hf[l].x = (float)h[l];
+        hf[l].y = (float)(h[l] - (double)hf[l].x);
+      }
+      if (!tabf[ax]) CK(cudaMalloc(&tabf[ax], n[ax] * sizeof(float2)));
+      CK(cudaMemcpy(tabf[ax], hf.data(), n[ax] * sizeof(float2), cudaMemcpyHostToDevice));
+    }
   }
   return TS_OK;
 }
@@ -346,6 +357,7 @@ int ts_plan_destroy(ts_plan* p) {
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
   for (int i = 0; i < 3; ++i) {
     if (p->eax[i]) cudaFree(p->eax[i]);
+    if (p->eaxf[i]) cudaFree(p->eaxf[i]);
     if (p->eaxT[i]) cudaFree(p->eaxT[i]);
   }
   if (p->twq) cudaFree(p->twq);
@@ -490,7 +502,7 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
     return TS_ERR_CUDA;
   }
   *p->err_h = 0;
-  CKP(upload_if_tables(p, cfg->nu, cfg->dt, p->eax));
+  CKP(upload_if_tables(p, cfg->nu, cfg->dt, p->eax, p->eaxf));
   // the scalar's factors: the SFF Boussinesq step and the FFF passive-scalar step
   CKP(upload_if_tables(p, cfg->kappa, cfg->dt, p->eaxT));
   if (cfg->basis == TS_BASIS_SSS) {
@@ -579,7 +591,7 @@ int ts_plan_set_dt(ts_plan* p, double dt) {
   if (dt == p->cfg.dt) return TS_OK;
   CK(cudaStreamSynchronize(p->st));
   p->cfg.dt = dt;
-  CKS(upload_if_tables(p, p->cfg.nu, dt, p->eax));
+  CKS(upload_if_tables(p, p->cfg.nu, dt, p->eax, p->eaxf));
   CKS(upload_if_tables(p, p->cfg.kappa, dt, p->eaxT));
   return TS_OK;
 }
@@ -642,6 +654,9 @@ static int rhs_fff(ts_plan* p, const void* Uin, int mode, const StageArgs& a_in)
   a.ex = p->eax[0];
   a.ey = p->eax[1];
   a.ez = p->eax[2];
+  a.exf = p->eaxf[0];
+  a.eyf = p->eaxf[1];
+  a.ezf = p->eaxf[2];
   const int rot = p->cfg.nlin_form == TS_NLIN_ROTATIONAL;
   const int nin = rot ? 6 : 3, nout = rot ? 3 : 6;
   // two-thirds dealiasing: after the x inverse only the columns with 3|ky| <= Ny and

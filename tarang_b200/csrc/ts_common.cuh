@@ -437,6 +437,14 @@ template <> __device__ __forceinline__ Fac<float> fac<float>(double x) {
   return {h, (float)(x - (double)h)};
 }
 __device__ __forceinline__ float fmulx(float a, Fac<float> f) { return fmaf(a, f.hi, a * f.lo); }
+// product of two pairs (hi + lo): the rounded product of the high parts plus its exact
+// rounding error (fma) and the cross terms; the sum hi + lo carries about 46 bits
+__device__ __forceinline__ Fac<float> pair_mul(Fac<float> a, Fac<float> b) {
+  const float h = a.hi * b.hi;
+  return {h, fmaf(a.lo, b.hi, fmaf(a.hi, b.lo, fmaf(a.hi, b.hi, -h)))};
+}
+__device__ __forceinline__ Fac<float> pair_mul(float2 a, Fac<float> b) { return pair_mul(Fac<float>{a.x, a.y}, b); }
+__device__ __forceinline__ Fac<float> pair_mul(float2 a, float2 b) { return pair_mul(Fac<float>{a.x, a.y}, Fac<float>{b.x, b.y}); }
 // a x + b, the low part of x folded into b before the final fma
 __device__ __forceinline__ float fmaddx(float a, Fac<float> f, float b) { return fmaf(a, f.hi, fmaf(a, f.lo, b)); }
 

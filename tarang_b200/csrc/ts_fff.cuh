@@ -1192,6 +1192,9 @@ struct StageArgs {
   const double* ex;  // per-axis integrating factors exp(-nu dt K_i^2 / 2), FP64
   const double* ey;
   const double* ez;
+  const float2* exf; // the same as FP32 (hi, lo) pairs (nullptr: split the FP64 product)
+  const float2* eyf;
+  const float2* ezf;
 };
 
 enum { MODE_STEP = 0, MODE_FLUX = 1, MODE_NLIN = 2, MODE_ADJ = 3 };
@@ -1310,8 +1313,23 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
   const V Rv[3] = {scale(add(N1, ik(Kx, pr)), (T)-1), scale(add(N2, ik(Ky, pr)), (T)-1),
                    scale(add(N3, ik(Kz, pr)), (T)-1)};
   // integrating factors (FP64): E(1/2) = ex ey ez = exp(-nu dt K^2 / 2), E(1) = E(1/2)^2
-  const double eh = a.ex[lx] * exy;
-  const Fac<T> Feh = fac<T>(eh), Fe1 = fac<T>(eh * eh);
+  Fac<T> Feh, Fe1;
+  if constexpr (std::is_same<T, float>::value) {
+    if (a.exf) {
+      // E(1/2) = ex ey ez and E(1) = E(1/2)^2 as FP32 pair products (about 46 bits; no
+      // FP64 operation or conversion per mode)
+      Feh = pair_mul(a.exf[lx], pair_mul(a.eyf[ly], a.ezf[lz]));
+      Fe1 = pair_mul(Feh, Feh);
+    } else {
+      const double eh = a.ex[lx] * exy;
+      Feh = fac<T>(eh);
+      Fe1 = fac<T>(eh * eh);
+    }
+  } else {
+    const double eh = a.ex[lx] * exy;
+    Feh = fac<T>(eh);
+    Fe1 = fac<T>(eh * eh);
+  }
   const Fac<T> Fc1 = fac<T>(a.dt), Fc2 = fac<T>(0.5 * a.dt), Fc3 = fac<T>((1.0 / 3) * a.dt),
                Fc6 = fac<T>((1.0 / 6) * a.dt);
   V* Uc = reinterpret_cast<V*>(a.Ucur);

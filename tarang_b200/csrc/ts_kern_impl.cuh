@@ -177,7 +177,12 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       if (dir < 0) launch(k_strided_fft<T, LL, E, CW, -1, NT>);
       else launch(k_strided_fft<T, LL, E, CW, 1, NT>);
     };
-    switch (v) {
+    // the y forward pass of 1024 points in FP32: the one-tile, 32-element form is the rule
+    // (on B200 at 1024^3 7.7 ms against 8.9 for the two-tile, 16-element form; the y
+    // inverse and the x forward pass stayed faster with the latter) and candidate 5 is
+    // then the 16-element form
+    const int vv = (wide1024(LL) && dir < 0 && axis == 1) ? (v == 0 ? 5 : (v == 5 ? 0 : v)) : v;
+    switch (vv) {
       case 1: with_str_tile<LL, 1>(run); break;
       case 2: with_str_tile<LL, 2>(run); break;
       case 3: with_str_tile<LL, 3>(run); break;
@@ -226,8 +231,12 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
   const int v = form <= 1 ? g.tv[TUNE_X_INV] : 0;
   dispatch_L(g.Nx, [&](auto Lc) {
     constexpr int LL = decltype(Lc)::value;
+    // 1024 points in FP32 under two-thirds dealiasing: the staged kernel k_inv_x_st is the
+    // rule (on B200 7.0 against 10.1 ms per launch at 1024^3) and candidate 5 is then the
+    // direct-load kernel
+    const int vv = (ix_valid(LL, 5) && kept && form <= 1) ? (v == 0 ? 5 : (v == 5 ? 0 : v)) : v;
     if constexpr (ix_valid(LL, 5)) {
-      if (v == 5 && kept) {
+      if (vv == 5 && kept) {
         // the kept U rows of a tile staged in shared memory (one load latency per tile)
         constexpr Tile c = ix_cand(LL, 5);
         constexpr int E = c.E, CW = c.CW;
@@ -245,7 +254,7 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
       }
     }
     if constexpr (ix_valid(LL, 3)) {
-      if (v == 3) {
+      if (vv == 3) {
         // persistent, prefetching form: one block per SM
         constexpr Tile c = ix_cand(LL, 3);
         constexpr int E = c.E, CW = c.CW;
@@ -290,11 +299,11 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
         else if (form == 5) run(k_inv_x_ld<T, LL, E, CW, 5>);
       }
     };
-    if (v == 1 && ix_valid(LL, 1)) {
+    if (vv == 1 && ix_valid(LL, 1)) {
       if constexpr (ix_valid(LL, 1)) tile(std::integral_constant<int, 1>{});
-    } else if (v == 2 && ix_valid(LL, 2)) {
+    } else if (vv == 2 && ix_valid(LL, 2)) {
       if constexpr (ix_valid(LL, 2)) tile(std::integral_constant<int, 2>{});
-    } else if (v == 4 && ix_valid(LL, 4)) {
+    } else if (vv == 4 && ix_valid(LL, 4)) {
       if constexpr (ix_valid(LL, 4)) tile(std::integral_constant<int, 4>{});
     } else {
       tile(std::integral_constant<int, 0>{});
@@ -327,8 +336,8 @@ static cudaError_t z_slots(const Geo& g, void* P, const void* tw, cudaStream_t s
 // z candidates (forms 0, 1, 2): 1 = the slot kernel with 8 elements per thread
 // (12 with a factor 3), 2 = the slot kernel with 4 (power-of-two lines), 3 = the
 // FP32 register kernel with 4 elements per thread (lines of up to 256 points),
-// 4 = the FP32 register kernel on 1024-point lines (two warps per line) with every
-// component's loads issued up front
+// 4 = on 1024-point lines in FP32, the register kernel that loads each component just
+// before its transform (the rule there issues every load up front)
 template <int NZ, int FORM> constexpr bool z_rule_slots() {
   constexpr int M = NZ / 2;
   return !(std::is_same<T, float>::value && M <= 512) &&
@@ -357,10 +366,14 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
     if (v == 2) return z_slots<NZ, FORM, 4>(g, P, tw, st, nmem, msP, zkeep);
   }
   if constexpr (z_valid<NZ, FORM>(4)) {
-    if (v == 4) {
-      constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
-      k_z_reg<T, NZ, FORM, 0, true><<<dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), NT, 0, st>>>(
-          (V*)P, g, (const V*)tw, msP, zkeep);
+    // 1024-point z lines in FP32: the register kernel with every component's loads issued
+    // up front is the rule (on B200 13.0 against 15.8 ms per launch at 1024^3); candidate 4
+    // loads each component just before its transform
+    constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
+    const dim3 grid((unsigned)((nlines + LPB - 1) / LPB), nmem);
+    if (v == 4) k_z_reg<T, NZ, FORM, 0, false><<<grid, NT, 0, st>>>((V*)P, g, (const V*)tw, msP, zkeep);
+    else if (v == 0) k_z_reg<T, NZ, FORM, 0, true><<<grid, NT, 0, st>>>((V*)P, g, (const V*)tw, msP, zkeep);
+    if (v == 4 || v == 0) {
       ++g_launches;
       return cudaGetLastError();
     }
@@ -504,6 +517,7 @@ constexpr bool fx_valid(int L, int v) {
   return v == 0 || (v == 1 && fx_rule_fused(L)) || (v == 2 && fx_cw2(L) * sizeof(V) >= 16 && fx_cw2(L) * (L / emin(E_ACC, L)) >= 32) ||
          (v == 3 && fx_rule_fused(L) && emin(E_ACC_ALT, L) != emin(E_ACC, L));
 }
+
 
 template <int FORM, int MODE, int LL>
 static cudaError_t fwd_x_impl(const Geo& g, const void* P, const StageArgs& a, const void* tw, cudaStream_t st) {
