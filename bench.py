@@ -82,6 +82,8 @@ def ensemble_leg(rank: int, world: int, steps: int, warmup: int):
         rep = ens.autotune(reps=3)
         tuned = [{"N": gr["N"], "members": gr["members"], "confirm": gr["tuning"]["confirm"],
                   **gr["tuning"]["final"]} for gr in rep["groups"]]
+        tuned.append({"schedule": rep.get("schedule"), "parallel_ms": rep.get("parallel_ms"),
+                      "serial_ms": rep.get("serial_ms")})
     ens.run(warmup)
     ens.synchronize()
     t0 = time.perf_counter()

@@ -1811,6 +1811,9 @@ struct ts_ensemble {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graphK = nullptr;     // kEnsSteps ensemble steps, each group a chain of its own
   cudaGraphExec_t execK = nullptr;
+  // graph schedule of the size groups: parallel branches between one fork and one join,
+  // or (serial) one chain, group after group, each with the GPU to itself
+  bool serial = false;
 };
 // ensemble steps per launch of the multi-step graph: the size groups advance this many
 // steps between one fork and one join, so a group does not wait for the slowest one
@@ -2011,10 +2014,11 @@ static int ens_capture(ts_ensemble* e, int steps, cudaGraph_t* graph_out, cudaGr
   cudaEventRecord(e->fork, e->origin);
   for (size_t k = 0; k < e->groups.size() && rc == TS_OK; ++k) {
     ens_group& G = e->groups[k];
-    cudaStreamWaitEvent(G.st, e->fork, 0);
+    // parallel: every group starts at the fork; serial: after the previous group
+    cudaStreamWaitEvent(G.st, (e->serial && k > 0) ? e->groups[k - 1].done : e->fork, 0);
     for (int s = 0; s < steps && rc == TS_OK; ++s) rc = step_rbc_group(G);
     cudaEventRecord(G.done, G.st);
-    cudaStreamWaitEvent(e->origin, G.done, 0);
+    if (!e->serial || k + 1 == e->groups.size()) cudaStreamWaitEvent(e->origin, G.done, 0);
   }
   cudaGraph_t graph = nullptr;
   cudaError_t ce = cudaStreamEndCapture(e->origin, &graph);
@@ -2412,7 +2416,23 @@ int ts_ensemble_autotune(ts_ensemble* e, int reps, char* report, size_t report_l
     rc = descend(G.gp, G.gp->g, measure, js);
     js += "}";
   }
-  js += "]}";
+  js += "]";
+  // the graph schedule: time kEnsSteps ensemble steps per launch both ways, keep the faster
+  if (rc == TS_OK) {
+    auto stepK = [&]() -> int { return ts_ensemble_run(e, kEnsSteps); };
+    double ms[2] = {0, 0};
+    for (int sc = 0; sc < 2 && rc == TS_OK; ++sc) {
+      e->serial = sc == 1;
+      ens_invalidate(e);
+      rc = time_calls(e->origin, 2, reps, stepK, &ms[sc]);
+    }
+    e->serial = rc == TS_OK && ms[1] < ms[0];
+    char buf[160];
+    snprintf(buf, sizeof(buf), ", \"schedule\": \"%s\", \"parallel_ms\": %.4f, \"serial_ms\": %.4f",
+             e->serial ? "serial" : "parallel", ms[0] / kEnsSteps, ms[1] / kEnsSteps);
+    js += buf;
+  }
+  js += "}";
   ens_invalidate(e);
   const int rr = restore();
   if (rc == TS_OK) rc = rr;

@@ -169,6 +169,8 @@ def test_ensemble_autotune_keeps_states(cuda):
     e_before = [ens.energy(m) for m in range(3)]
     rep = ens.autotune(reps=1)
     assert len(rep["groups"]) == 2
+    # the graph schedule of the size groups is chosen by timing both
+    assert rep["schedule"] in ("parallel", "serial") and rep["parallel_ms"] > 0 and rep["serial_ms"] > 0
     assert [ens.energy(m) for m in range(3)] == e_before
     # tuned and untuned ensembles agree to FP32 rounding
     ref = tb.Ensemble(members, dt=1e-4, precision="f32")
