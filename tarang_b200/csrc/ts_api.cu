@@ -373,8 +373,10 @@ int ts_plan_create(const ts_config* cfg, ts_plan** out) {
   for (int i = 0; i < 3; ++i) {
     // 48 and 96 (factor 3) are supported for the SFF path
     const bool mixed = (cfg->N[i] == 48 || cfg->N[i] == 96) && cfg->basis != TS_BASIS_FFF;
-    if (!size_supported(cfg->N[i]) && !mixed) {
-      g_last_error = "N must be a power of two in [16, 1024] (48 and 96 also for SFF)";
+    // SFF takes Ny = 1: a two-dimensional run in the x-z plane (program.two_dimension)
+    const bool flat = i == 1 && cfg->N[1] == 1 && cfg->basis == TS_BASIS_SFF;
+    if (!size_supported(cfg->N[i]) && !mixed && !flat) {
+      g_last_error = "N must be a power of two in [16, 1024] (48 and 96 also for SFF; Ny = 1 on SFF)";
       return TS_ERR_ARG;
     }
   }

@@ -147,6 +147,7 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
   if (per <= 0) per = nf;
   cudaError_t err = cudaErrorInvalidValue;
   const int L = axis == 0 ? g.Nx : g.Ny;
+  if (L == 1) return cudaSuccess;  // a one-point transform is the identity (two-dimensional runs)
   // the y passes follow the tuning of their class; x passes keep the rule
   const int cls = axis == 1 ? (dir > 0 ? TUNE_Y_INV : TUNE_Y_FWD) : -1;
   const int v = cls >= 0 ? g.tv[cls] : 0, bps = cls >= 0 ? g.tb[cls] : 0;

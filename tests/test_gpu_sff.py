@@ -250,3 +250,44 @@ def test_rbc_slaved_scalings_refused_off_sff(cuda):
     for pr in ("PRZERO", "PRINFTY"):
         with pytest.raises(tb.TsError):
             tb.Ensemble([((16, 16, 16), 1e4, 1.0)], dt=1e-4, Pr_option=pr, Uscaling="USMALL")
+
+@pytest.mark.parametrize("dealias", ["reference", "two_thirds"])
+def test_rbc_two_dimensional_matches_oracle(cuda, dealias):
+    """A two-dimensional RBC run (Ny = 1, program.two_dimension; the reference's RBC/2d and
+    RBC_scaling/2d inputs are 32 x 1 x 32 on SFF): the y transforms are the identity and
+    u2 stays zero. FP64 <= 1e-12 and FP32 <= 1e-5 against the oracle after 3 steps, and
+    the Nusselt number."""
+    import torch
+    import tarang_b200 as tb
+    mode = {"reference": 1, "two_thirds": 2}[dealias]
+    N = (32, 1, 32)
+    g = R.Grid(N, KF, "SFF")
+    U0, T0 = random_state(g, 0.3, 9)
+    U0[1] = 0
+    cfg = R.RBCConfig(g, Ra=1e5, Pr=1.0, dt=1e-3, dealias_mode=mode)
+    Uo, To = U0, T0
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    assert np.abs(Uo[1]).max() == 0.0
+    for prec, tol in (("f64", 1e-12), ("f32", 1e-5)):
+        plan = tb.Plan(N, basis="SFF", precision=prec, kfactor=KF, dealias=dealias, nu=cfg.nu, kappa=cfg.kappa,
+                       dt=cfg.dt, Ra=cfg.Ra, Pr=cfg.Pr)
+        u = torch.from_numpy(np.ascontiguousarray(U0)).to(cuda).to(plan.torch_dtype())
+        T = torch.from_numpy(np.ascontiguousarray(T0)[None]).to(cuda).to(plan.torch_dtype())
+        plan.rk4_step_rbc(u, T, 3)
+        plan.status()
+        assert rel(u.cpu().numpy().astype(np.complex128), Uo) < tol
+        assert rel(T[0].cpu().numpy().astype(np.complex128), To) < tol
+        assert float(u[1].abs().max()) == 0.0
+        if prec == "f64":
+            ref = R.nusselt(cfg, Uo, To)
+            assert abs(plan.nusselt(u, T) - ref) < 1e-12 * max(1.0, abs(ref))
+        plan.close()
+
+
+def test_two_dimensional_refused_off_sff(cuda):
+    """Ny = 1 is taken on SFF plans only."""
+    import tarang_b200 as tb
+    for basis in ("FFF", "SSF", "SSS"):
+        with pytest.raises(tb.TsError):
+            tb.Plan((32, 1, 32), basis=basis)

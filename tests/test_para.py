@@ -14,7 +14,7 @@ from tarang_b200 import para
 HERE = os.path.dirname(os.path.abspath(__file__))
 FFF_DIR = os.path.join(HERE, "golden", "para_fff")
 RBC_DIR = os.path.join(HERE, "golden", "para_rbc")
-KIND_DIRS = {k: os.path.join(HERE, "golden", f"para_{k}") for k in ("mhd", "scalar", "ssf", "sss", "rbc_sss")}
+KIND_DIRS = {k: os.path.join(HERE, "golden", f"para_{k}") for k in ("mhd", "scalar", "ssf", "sss", "rbc_sss", "rbc_2d")}
 
 
 def test_read_para_fff_forced():
@@ -50,6 +50,8 @@ def test_read_para_other_kinds():
     assert (rp.kind, rp.basis, rp.kfactor, rp.nu, rp.nsteps) == ("FLUID_INCOMPRESS", "SSF", (1.0, 1.0, 1.0), 0.02, 3)
     rp = para.read_para(os.path.join(KIND_DIRS["sss"], "in", "para.yaml"))
     assert (rp.basis, rp.N, rp.kfactor, rp.dealias) == ("SSS", (16, 32, 16), (1.0, 1.0, 1.0), "reference")
+    rp = para.read_para(os.path.join(KIND_DIRS["rbc_2d"], "in", "para.yaml"))
+    assert (rp.kind, rp.basis, rp.N) == ("RBC", "SFF", (32, 1, 32))
     rp = para.read_para(os.path.join(KIND_DIRS["rbc_sss"], "in", "para.yaml"))
     assert (rp.kind, rp.basis, rp.Ra, rp.Pr, rp.nsteps, rp.force_on) == ("RBC", "SSS", 2e4, 0.7, 3, False)
     assert np.allclose(rp.kfactor, (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0)))
@@ -141,6 +143,12 @@ def _kind_state(g, kind, basis):
         if kind == "RBC":
             return U, 0.3 * R.forward(g, rng.standard_normal(g.rshape), par["F"])
         return (U,)
+    if basis == "SFF":
+        # sin/cos parities along x (u1, T sine; u2, u3 cosine); u2 = 0 in a two-dimensional run
+        U = np.stack([R.reality_fix(g, 0.3 * R.forward(g, rng.standard_normal(g.rshape), p)) for p in "SCC"])
+        if g.N[1] == 1:
+            U[1] = 0
+        return U, R.reality_fix(g, 0.3 * R.forward(g, rng.standard_normal(g.rshape), "S"))
     U = R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 4.0), 0, 0.5)
     if kind == "MHD_INCOMPRESS":
         return U, R.init_energy_spectrum(g, R.spectrum_k4_gauss(g.n_shells(), 3.0), 1, 0.3)
@@ -163,9 +171,10 @@ def _kind_oracle(g, rp, state):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["mhd", "scalar", "ssf", "sss", "rbc_sss"])
+@pytest.mark.parametrize("name", ["mhd", "scalar", "ssf", "sss", "rbc_sss", "rbc_2d"])
 def test_plan_from_para_other_kinds_step_like_the_oracle(cuda, name):
-    """MHD, passive-scalar, SSF and SSS fluid and SSS RBC runs set up from a para.yaml,
+    """MHD, passive-scalar, SSF and SSS fluid, SSS RBC and two-dimensional SFF RBC
+    (Ny = 1) runs set up from a para.yaml,
     stepped through para.advance, match the FP64 oracle over the run's 3 steps
     (relative L2 <= 1e-12)."""
     import torch
