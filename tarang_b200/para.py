@@ -392,6 +392,21 @@ def sff_max_radius_inside(N, kfactor) -> int:
     return int(min((Nx - 1) * kfactor[0], (Ny // 2) * kfactor[1], (Nz // 2) * kfactor[2]))
 
 
+def ssf_max_radius_inside(N, kfactor) -> int:
+    """``Max_radius_inside`` for the SSF basis with waveno_switch (SSF_pencil_inline.h:456-474):
+    min((Nx - 1) Kx, (Ny - 1) Ky, (Nz/2) Kz), truncated."""
+    Nx, Ny, Nz = N
+    return int(min((Nx - 1) * kfactor[0], (Ny - 1) * kfactor[1], (Nz // 2) * kfactor[2]))
+
+
+def sss_max_radius_inside(N, kfactor) -> int:
+    """``Max_radius_inside`` for the SSS basis with waveno_switch (SSS_pencil_inline.h:481-499):
+    min((Nx - 1) Kx, (Ny - 1) Ky, (Ny - 1) Kz) as the reference writes it (its third term
+    takes Ny, not Nz), truncated."""
+    Nx, Ny, Nz = N
+    return int(min((Nx - 1) * kfactor[0], (Ny - 1) * kfactor[1], (Ny - 1) * kfactor[2]))
+
+
 def _fff_multiplicity(kx, ky, kz, Nx, Ny):
     """Multiplicity_factor (FFF_pencil_inline.h:583-602): 1 (kz > 0) or 1/2 (kz = 0),
     doubled on the kx = Nx/2 and ky = Ny/2 planes."""
@@ -417,14 +432,12 @@ class Output:
     """
 
     def __init__(self, plan, out_dir: str, radii=None):
-        if plan.basis not in ("FFF", "SFF"):
-            raise NotImplementedError("Output writes the FFF fluid layouts and the SFF RBC glob.d")
         os.makedirs(out_dir, exist_ok=True)
         self.plan = plan
         self.out_dir = out_dir
         self.kf = tuple(plan.cfg.kfactor[i] for i in range(3))
-        self.kmax_inside = (max_radius_inside(plan.N, self.kf) if plan.basis == "FFF"
-                            else sff_max_radius_inside(plan.N, self.kf))
+        self.kmax_inside = {"FFF": max_radius_inside, "SFF": sff_max_radius_inside, "SSF": ssf_max_radius_inside,
+                            "SSS": sss_max_radius_inside}[plan.basis](plan.N, self.kf)
         self.radii = list(radii) if radii is not None else default_flux_radii(8, self.kmax_inside)
         self.forced = plan.cfg.force_type != 0
 
@@ -552,10 +565,14 @@ class Output:
         bits (universal_energy.cc:449-537), kmax eta_1 = kmax (nu^3/eps)^(1/4),
         kmax eta_2 = kmax eta_1 (nu/kappa)^(1/4) / (nu/kappa), nu, kappa,
         R_lambda = 2 E_u sqrt(15/eps), dt, and the three component energies of u.
-        kmax = Max_radius_inside of SFF; mult = SFF Multiplicity_factor
-        (SFF_pencil_inline.h:492-515)."""
-        if self.plan.basis != "SFF":
-            raise NotImplementedError("glob_rbc writes RBC runs on the SFF basis")
+        kmax = Max_radius_inside of the basis; mult = its Multiplicity_factor
+        (SFF_pencil_inline.h:492-515; on SSF and SSS 1/2 at the origin, 1, 2 or 4 with two,
+        one or no zero indices, SSF_pencil_inline.h:512-532, SSS_pencil_inline.h:537-556).
+        The sums run over the complex array shape as the reference's loops do
+        (universal_energy.cc:106-141): on SSS each pair of real z coefficients is one
+        complex slot lz with Kz = lz kfactor_z."""
+        if self.plan.basis == "FFF":
+            raise NotImplementedError("glob_rbc writes RBC runs on the SFF, SSF and SSS bases")
         return self._glob_uT(u, T, t, dt, nusselt=True)
 
     def glob_scalar(self, u, T, t: float, dt: float, helicity: bool = False):
@@ -649,7 +666,13 @@ class Output:
         ly = torch.arange(Ny, device=dev)
         ky = torch.where(ly <= Ny // 2, ly, ly - Ny).double()[None, :, None]
         lz = torch.arange(Nz // 2 + 1, device=dev).double()[None, None, :]
-        if p.basis == "SFF":
+        if p.basis in ("SSF", "SSS"):
+            # grid indices; the SSS z slot lz holds the real pair (2 lz, 2 lz + 1)
+            lx = lxi.double()[:, None, None]
+            ky = ly.double()[None, :, None]
+            zeros = (lx == 0).double() + (ky == 0).double() + (lz == 0).double()
+            mult = torch.where(zeros >= 3, 0.5, torch.where(zeros == 2, 1.0, torch.where(zeros == 1, 2.0, 4.0)))
+        elif p.basis == "SFF":
             lx = lxi.double()[:, None, None]
             mult = torch.where(lz > 0, torch.where(lx > 0, 2.0, 1.0), torch.where(lx > 0, 1.0, 0.5))
             mult = mult * torch.where((ky == Ny // 2) & (Ny > 1), 2.0, 1.0)

@@ -354,6 +354,59 @@ def test_output_glob_rbc_matches_oracle(cuda, tmp_path):
     assert line.endswith("\t\n") and len(line.split("\t")) == 22
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("basis", ["SSF", "SSS"])
+def test_output_glob_rbc_ssf_sss_matches_oracle(cuda, tmp_path, basis):
+    """glob.d for RBC runs on SSF and SSS (the same 21 columns): the k^2 sums and entropies
+    over the complex array shape with the sin/cos multiplicity (on SSS the real pair of a z
+    slot with Kz = lz kfactor_z, as the reference's universal loops take it), Max_radius_inside
+    of the basis, energies and Nusselt from the oracle (relative 1e-10, FP64)."""
+    import torch
+    import tarang_b200 as tb
+    from oracle import tarang_ref as R
+    N, kf, Ra, Pr = (16, 32, 16), (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0)), 3e4, 0.7
+    g = R.Grid(N, kf, basis)
+    par = R.SSF_PARITY if basis == "SSF" else R.SSS_PARITY
+    rng = np.random.default_rng(23)
+    U = np.stack([0.3 * R.forward(g, rng.standard_normal(g.rshape), par[v]) for v in ("Vx", "Vy", "Vz")])
+    T = 0.2 * R.forward(g, rng.standard_normal(g.rshape), par["F"])
+    cfg = R.RBCConfig(g, Ra=Ra, Pr=Pr, dt=1e-3)
+    plan = tb.Plan(N, basis=basis, kfactor=kf, nu=cfg.nu, kappa=cfg.kappa, Ra=Ra, Pr=Pr, dt=1e-3)
+    if basis == "SSS":
+        def dev(a):
+            pad = np.zeros(a.shape[:-1] + (N[2] + 2,))
+            pad[..., :N[2]] = a
+            return torch.from_numpy(pad.view(np.complex128)).to(cuda)
+        Uc = np.stack([R.sss_complex_view(g, U[i])[0] for i in range(3)])
+        Tc, gc = R.sss_complex_view(g, T)
+        mult, K2 = R._sss_mult(gc), gc.Ksqr()
+    else:
+        def dev(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+        Uc, Tc, mult, K2 = U, T, g.multiplicity(), g.Ksqr()
+    out = para.Output(plan, str(tmp_path))
+    row = out.glob_rbc(dev(U), dev(T[None]), 0.5, 1e-3)
+    Eu, ET = R.total_energy(g, U), R.total_energy_scalar(g, T)
+    eps = cfg.nu * 2 * (mult * K2 * (np.abs(Uc) ** 2).sum(0)).sum()
+    epsT = cfg.kappa * 2 * (mult * K2 * np.abs(Tc) ** 2).sum()
+
+    def ent(a2, e):
+        pr = mult * a2 / e
+        pr = pr[pr > 1e-15]
+        return float((-pr * np.log(pr) / np.log(2.0)).sum())
+
+    third = (N[2] // 2) * kf[2] if basis == "SSF" else (N[1] - 1) * kf[2]
+    kmax = int(min((N[0] - 1) * kf[0], (N[1] - 1) * kf[1], third))
+    k1 = kmax * (cfg.nu ** 3 / eps) ** 0.25
+    r = cfg.nu / cfg.kappa
+    want = [0.5, Eu, ET, eps, epsT, R.nusselt(cfg, U, T), 0, 0, 0, 0, ent((np.abs(Uc) ** 2).sum(0), Eu),
+            ent(np.abs(Tc) ** 2, ET), k1, k1 * r ** 0.25 / r, cfg.nu, cfg.kappa, 2 * Eu * math.sqrt(15 / eps), 1e-3,
+            R.total_energy(g, U[:1]), R.total_energy(g, U[1:2]), R.total_energy(g, U[2:])]
+    assert len(row) == 21
+    for i, (a, b) in enumerate(zip(row, want)):
+        assert abs(a - b) <= max(1e-10 * abs(b), 1e-12), (i, a, b)
+
+
 def _helicity_np(V, kx, ky, kz, mult):
     """H1, H2, k2H1, k2H2 on FFF with kfactor 1: h = 2 mult K . (Vr x Vi)"""
     cr = np.cross(V.real, V.imag, axis=0)
