@@ -46,9 +46,10 @@ typedef enum {
 } ts_status;
 
 /* TS_BASIS_SSF (sin/cos along x and y, Fourier along z; basis/SSF/pencil) offers the
- * transforms (ts_fft_forward / ts_fft_inverse with parities "SCF", "CSF", "SSF", "CCF")
- * and ts_rk4_step for the conservative, unforced fluid (sincostr_switch "SCF":
- * Vx = SCF, Vy = CSF, Vz = CCF); every other call on an SSF plan returns
+ * transforms (ts_fft_forward / ts_fft_inverse with parities "SCF", "CSF", "SSF", "CCF"),
+ * ts_rk4_step for the conservative, unforced fluid (sincostr_switch "SCF":
+ * Vx = SCF, Vy = CSF, Vz = CCF), ts_rk4_step_rbc, ts_energy, ts_nusselt, ts_max_div,
+ * ts_shell_spectrum and ts_flux; the other calls on an SSF plan return
  * TS_ERR_UNSUPPORTED. */
 /* TS_BASIS_SSS (sin/cos along every axis; basis/SSS/pencil) stores real coefficients in
  * the padded real layout (Nx, Ny, Nz + 2) of each component (the complex buffer viewed
@@ -194,7 +195,9 @@ int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, i
  * sum_{|K| <= R} 2 mult Re(N . conj(D U)), N = F[(u.grad)u] (there the products
  * alias only onto modes D U does not hold, so the two forms agree).  FP64 sums in a
  * fixed order.  u_hat is not modified (the reference dealiases U in place here:
- * call ts_dealias_field first to reproduce that side effect). */
+ * call ts_dealias_field first to reproduce that side effect).  FFF and SSF plans (on
+ * SSF the per-sphere algorithm in every dealias mode, through the sin/cos passes with
+ * each product's parities); SSS plans return TS_ERR_UNSUPPORTED. */
 int ts_flux(ts_plan* plan, const void* u_hat, const double* radii, int n_radii, double* Pi);
 /* Universal::Dealias on ncomp components in place (FFF_pencil_basic.cc:87-90 corner
  * box, or the plan's two-thirds rule; nothing for dealias NONE). */

@@ -778,6 +778,21 @@ template <> cudaError_t Launch<T>::flux_outside(const Geo& g, const void* P, con
   return cudaGetLastError();
 }
 
+template <> cudaError_t Launch<T>::ssf_giver(const Geo& g, const void* U, void* P, double R, cudaStream_t st) {
+  k_ssf_giver<T><<<grid1d(g.S, 256), 256, 0, st>>>((const V*)U, (V*)P, g, R);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::ssf_flux_outside(const Geo& g, const void* P, const void* U, double R, int qx,
+                                                    int qy, double* out, cudaStream_t st) {
+  const unsigned blocks = grid1d(g.S, 256);
+  k_ssf_flux_outside<T><<<blocks, 256, 0, st>>>((const V*)P, (const V*)U, g, R, qx, qy, out);
+  k_sum_partials<<<1, 256, 0, st>>>(out, (int)blocks);
+  g_launches += 2;
+  return cudaGetLastError();
+}
+
 template <> cudaError_t Launch<T>::force_scatter(const Geo& g, const void* fc, void* F, int km, cudaStream_t st) {
   const long long n = 3LL * (2 * km + 1) * (2 * km + 1) * (km + 1);
   k_force_scatter<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const V*)fc, (V*)F, g, km);

@@ -89,6 +89,9 @@ template <typename T> struct Launch {
                            const void* B = nullptr, unsigned cap = SHELL_MAX_BLOCKS);
   // per-sphere energy flux: out[0] = sum over |K| > R of 2 mult Re(N . conj(D U)), N from the
   // nine x-forward-transformed giver products in P; out must hold 1 + 148 * 16 doubles
+  static cudaError_t ssf_giver(const Geo& g, const void* U, void* P, double R, cudaStream_t st);
+  static cudaError_t ssf_flux_outside(const Geo& g, const void* P, const void* U, double R, int qx, int qy,
+                                      double* out, cudaStream_t st);
   static cudaError_t flux_outside(const Geo& g, const void* P, const void* U, double R, double* out,
                                   cudaStream_t st);
   static cudaError_t force_scatter(const Geo& g, const void* fc, void* F, int km, cudaStream_t st);

@@ -407,6 +407,75 @@ __global__ void k_flux_outside(const C<T>* __restrict__ P, const C<T>* __restric
 }
 
 // ---------------------------------------------------------------------------
+// SSF per-sphere energy flux (EnergyTr::Compute_flux, compute_flux.cc:51-65, on the SSF
+// basis): k_ssf_giver writes the inputs of the giver nonlinear term, D U into P[0, 3)
+// and the giver D(U inside |K| <= R) (Fill_in_sphere, fill_space.cc:56-64) into
+// P[3, 6), with the SSF wavenumbers Kx = lx kx, Ky = ly ky, Kz = lz kz; after the
+// transforms P[3 j + i] holds F[u_j G_i], normalised, with x / y sine letters
+// qx, qy (bit f); k_ssf_flux_outside then forms N_i = sum_j D_j F[u_j G_i] (D_x, D_y:
+// +K on a sine series, -K on a cosine series; D_z = i Kz) and sums
+// 2 mult Re(N . conj(D U)) over |K| > R, per block (k_sum_partials adds the blocks).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_ssf_giver(const C<T>* __restrict__ U, C<T>* __restrict__ P, Geo g, double R) {
+  const long long n = g.S;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
+    const double Kx = lx * g.kf[0], Ky = ly * g.kf[1], Kz = lz * g.kf[2];
+    const bool in = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz) <= R;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const C<T> u = dz ? mk<C<T>>(0, 0) : U[i * n + e];
+      P[i * n + e] = u;
+      P[(3 + i) * n + e] = in ? u : mk<C<T>>(0, 0);
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_ssf_flux_outside(const C<T>* __restrict__ P, const C<T>* __restrict__ U, Geo g, double R,
+                                   int qx, int qy, double* __restrict__ out) {
+  const long long n = g.S;
+  double s = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lz = (int)(e % g.Hz);
+    const int ly = (int)((e / g.Hz) % g.Ny);
+    const int lx = (int)(e / ((long long)g.Ny * g.Hz));
+    if (dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) continue;
+    const double K[3] = {lx * g.kf[0], ly * g.kf[1], lz * g.kf[2]};
+    const double Kmag = sqrt((K[0] * K[0] + K[1] * K[1]) + K[2] * K[2]);
+    if (!(Kmag > R)) continue;
+    double re = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double nr = 0, ni = 0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int f = 3 * j + i;
+        const C<T> q = P[f * n + e];
+        if (j == 2) {  // i Kz X
+          nr -= K[2] * (double)q.y;
+          ni += K[2] * (double)q.x;
+        } else {
+          const int sine = j == 0 ? (qx >> f & 1) : (qy >> f & 1);
+          const double d = sine ? K[j] : -K[j];
+          nr += d * (double)q.x;
+          ni += d * (double)q.y;
+        }
+      }
+      const C<T> u = U[i * n + e];
+      re += nr * (double)u.x + ni * (double)u.y;
+    }
+    s += 2.0 * multiplicity(g.basis, lx, ly, lz, g.Nx, g.Ny) * re;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[1 + blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------
 // random-phase helical initial condition (init_cond_energy.cc:67-120 construction;
 // this project's counter-based splitmix64 phases, identical to the oracle)
 // ---------------------------------------------------------------------------

@@ -179,6 +179,24 @@ def test_flux_one_pass_equals_per_sphere():
     assert np.max(np.abs(a - b)) < 1e-15
 
 
+def test_flux_one_pass_equals_per_sphere_on_ssf():
+    """On the SSF basis too the two flux forms agree under two-thirds dealiasing (the
+    per-sphere restatement goes through the sin/cos parities of every product)."""
+    kf = (math.pi, math.pi / math.sqrt(2.0), math.pi / math.sqrt(2.0))
+    g = R.Grid((16, 32, 16), kf, "SSF")
+    rng = np.random.default_rng(3)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), R.SSF_PARITY[v]) for v in ("Vx", "Vy", "Vz")])
+    U = -0.3 * R.project_rhs(g, U)
+    radii = [1.0, 2.0, 4.0, 6.0]
+    a = R.flux_per_sphere(g, U, radii, R.DEALIAS_TWO_THIRDS)
+    b = R.flux_one_pass(g, U, radii, R.DEALIAS_TWO_THIRDS)
+    assert np.max(np.abs(a - b)) < 1e-12 * np.max(np.abs(a))
+    # and under the corner box they differ, as on FFF
+    a = R.flux_per_sphere(g, U, radii, R.DEALIAS_REFERENCE_CORNER)
+    b = R.flux_one_pass(g, U, radii, R.DEALIAS_REFERENCE_CORNER)
+    assert np.max(np.abs(a - b)) > 0.1 * np.max(np.abs(a))
+
+
 def test_flux_forms_differ_under_the_corner_box():
     """Under the reference's corner-box dealiasing (and none) the products alias onto modes the
     field holds, so the one-pass form is not the reference's per-sphere Pi(R): at 32^3 with
