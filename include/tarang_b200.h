@@ -187,7 +187,8 @@ int ts_energy(ts_plan* plan, const void* a_hat, int ncomp, double* energy);
  * ncomp components: Ek[n_shells]. */
 int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, int n_shells);
 /* EnergyTr::Compute_flux(U) (compute_flux.cc:51-65): the energy flux Pi(R_i) out of
- * each sphere |K| <= R_i, radii ascending, at most 63.  Corner-box or no dealiasing:
+ * each sphere |K| <= R_i, at most 63 radii (in any order: the reference's default
+ * radii do not ascend on small grids; the one-pass form runs for ascending radii).  Corner-box or no dealiasing:
  * the reference's per-sphere algorithm, one giver nonlinear term per sphere
  * (Fill_in_sphere fill_space.cc:56-64, Compute_nlin(U, Giver) compute_nlin_ET_VF.cc:
  * 71-87) and Pi(R) = -sum_{|K| > R} 2 mult Re(N . conj(D U)) (prod_nlinV.cc:61-69).

@@ -1520,8 +1520,13 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
     g_last_error = "ts_flux: at most " + std::to_string(FLUX_MAX_BINS - 1) + " radii";
     return TS_ERR_ARG;
   }
-  for (int i = 1; i < n_radii; ++i)
-    if (!(radii[i] >= radii[i - 1])) return TS_ERR_ARG;
+  // the reference's default radii need not ascend on small grids
+  // (Global_process_advanced_vars.cc:133-154); the one-pass form bins ascending radii
+  bool ascending = true;
+  for (int i = 0; i < n_radii; ++i) {
+    if (radii[i] != radii[i]) return TS_ERR_ARG;
+    if (i > 0 && radii[i] < radii[i - 1]) ascending = false;
+  }
   const Geo& g = p->g;
   if (p->cfg.basis == TS_BASIS_SSF)
     return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false,
@@ -1529,7 +1534,7 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
   const long long nb = 1 + 148 * 16;  // a result plus the per-block partials of one reduction
   return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false, [&](void* U) -> int {
     std::vector<double> h(n_radii + 1);
-    if (g.dealias == TS_DEALIAS_TWO_THIRDS) {
+    if (g.dealias == TS_DEALIAS_TWO_THIRDS && ascending) {
       // one pass: with two-thirds dealiasing the products of kept modes alias only onto
       // modes the dealiased field does not hold, so <u_<, (u.grad)u> = -<u_>, (u.grad)u_<>
       // and Pi(R) = sum_{|K| <= R} 2 mult Re(N . conj(D U)) from one nonlinear term

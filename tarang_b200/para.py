@@ -522,8 +522,8 @@ class Output:
         return row
 
     def flux(self, u, t: float):
-        if self.plan.basis != "FFF":
-            raise NotImplementedError("this output is written for FFF fluid runs")
+        if self.plan.basis not in ("FFF", "SSF"):
+            raise NotImplementedError("flux.d is written for fluid runs on FFF and SSF")
         p = self.plan
         # Compute_flux runs Compute_nlin(U, Giver), which dealiases U in place
         # (compute_nlin_ET_VF.cc:73-76): the run goes on from the dealiased state

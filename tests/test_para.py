@@ -407,6 +407,27 @@ def test_output_glob_rbc_ssf_sss_matches_oracle(cuda, tmp_path, basis):
         assert abs(a - b) <= max(1e-10 * abs(b), 1e-12), (i, a, b)
 
 
+@pytest.mark.gpu
+def test_output_flux_ssf_matches_oracle(cuda, tmp_path):
+    """flux.d of an SSF fluid run (the reference's per-sphere flux on the SSF basis, the
+    default radii from SSF's Max_radius_inside, radii[0] never computed) against the oracle,
+    and U dealiased in place as Compute_nlin(U, Giver) leaves it."""
+    import torch
+    from oracle import tarang_ref as R
+    plan, rp = para.plan_from_dir(KIND_DIRS["ssf"], precision="f64")
+    g = R.Grid(rp.N, rp.kfactor, rp.basis)
+    (U,) = _kind_state(g, rp.kind, rp.basis)
+    u = torch.from_numpy(U.copy()).to(cuda)
+    out = para.Output(plan, str(tmp_path))
+    out.flux(u, 0.0)
+    flux = _read_blocks(tmp_path / "flux.d", "flux: U2U ")[0][0]
+    ref = R.flux_per_sphere(g, U, out.radii, 1)
+    ref[0] = 0.0
+    assert len(out.radii) == len(flux)
+    assert np.allclose(flux, ref, rtol=2e-5, atol=1e-9 * np.abs(ref).max())
+    assert np.array_equal(u.cpu().numpy(), R.dealias(g, U, 1))
+
+
 def _helicity_np(V, kx, ky, kz, mult):
     """H1, H2, k2H1, k2H2 on FFF with kfactor 1: h = 2 mult K . (Vr x Vi)"""
     cr = np.cross(V.real, V.imag, axis=0)
