@@ -1237,16 +1237,27 @@ __device__ __forceinline__ void accum_product(int f, V p, S Kx, S Ky, S Kz, V& a
   }
 }
 
+// ey[ly] ez[lz] from the FP32 pair tables (once per column), for the FP32 step
+template <typename T, int MODE>
+__device__ __forceinline__ Fac<float> col_pair(const StageArgs& a, int ly, int lz) {
+  if constexpr (std::is_same<T, float>::value && MODE == MODE_STEP) {
+    if (a.exf) return pair_mul(a.eyf[ly], a.ezf[lz]);
+  }
+  return Fac<float>{1.0f, 0.0f};
+}
+
 // Per-mode epilogue of a right-hand side at spectral element (lx, ly, lz),
 // linear offset `off` in a component.  N1..N3 = the assembled vector; the
 // state the mode reads comes from st0[i * sstr] (U0 / Lam / the flux field)
 // and st1[i * sstr] (tot / the adjoint accumulator), i = component; the
 // fused x kernel passes its shared-memory state tiles, the elementwise
-// epilogue kernel the global arrays.  exy = ey[ly] ez[lz] (MODE_STEP, MODE_ADJ).
+// epilogue kernel the global arrays.  exy = ey[ly] ez[lz] (MODE_STEP, MODE_ADJ); pexy = the
+// same product from the FP32 pair tables (FP32 MODE_STEP with a.exf; see col_pair).
 template <typename T, int MODE>
 __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, int lx, int ly, int lz,
-                                              long long off, double exy, C<T> N1, C<T> N2, C<T> N3,
-                                              const C<T>* st0, const C<T>* st1, long long sstr, double* sbins) {
+                                              long long off, double exy, Fac<float> pexy, C<T> N1, C<T> N2,
+                                              C<T> N3, const C<T>* st0, const C<T>* st1, long long sstr,
+                                              double* sbins) {
   typedef C<T> V;
   const int kx = kfft(lx, g.Nx), ky = kfft(ly, g.Ny);
   const double Kxd = kx * g.kf[0], Kyd = ky * g.kf[1], Kzd = lz * g.kf[2];
@@ -1322,7 +1333,7 @@ __device__ __forceinline__ void spec_epilogue(const Geo& g, const StageArgs& a, 
     if (a.exf) {
       // E(1/2) = ex ey ez and E(1) = E(1/2)^2 as FP32 pair products (about 46 bits; no
       // FP64 operation or conversion per mode)
-      Feh = pair_mul(a.exf[lx], pair_mul(a.eyf[ly], a.ezf[lz]));
+      Feh = pair_mul(a.exf[lx], pexy);
       Fe1 = pair_mul(Feh, Feh);
     } else {
       const double eh = a.ex[lx] * exy;
@@ -1502,12 +1513,13 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
     }
     if (ok) {
       const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
+      const Fac<float> pexy = col_pair<T, MODE>(a, ly, lz);
 #pragma unroll
       for (int s = 0; s < E; ++s) {
         const int lx = final_row<L, E>(t, s);
         const long long off = lx * rstride + col;
         const int so = lx * CW + c;
-        spec_epilogue<T, MODE>(g, a, lx, ly, lz, off, exy, acc[0][s], acc[1][s], acc[2][s], sst + so,
+        spec_epilogue<T, MODE>(g, a, lx, ly, lz, off, exy, pexy, acc[0][s], acc[1][s], acc[2][s], sst + so,
                                sst + 3 * TILE + so, TILE, tb);
       }
     }
@@ -1573,7 +1585,7 @@ __global__ void __launch_bounds__(256) k_spec_epi(const C<T>* __restrict__ P, Ge
 #pragma unroll
       for (int f = 0; f < NF; ++f) accum_product<FORM>(f, scale(pv[j][f], inv), Kx, Ky, Kz, a0, a1, a2);
       const double exy = (MODE == MODE_STEP || MODE == MODE_ADJ) ? a.ey[ly] * a.ez[lz] : 0.0;
-      spec_epilogue<T, MODE>(g, a, lx, ly, lz, e, exy, a0, a1, a2, s0[j], s1[j], 1, tb);
+      spec_epilogue<T, MODE>(g, a, lx, ly, lz, e, exy, col_pair<T, MODE>(a, ly, lz), a0, a1, a2, s0[j], s1[j], 1, tb);
     }
   }
   if (MODE == MODE_FLUX) {
