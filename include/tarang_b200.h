@@ -196,9 +196,10 @@ int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, i
  * sum_{|K| <= R} 2 mult Re(N . conj(D U)), N = F[(u.grad)u] (there the products
  * alias only onto modes D U does not hold, so the two forms agree).  FP64 sums in a
  * fixed order.  u_hat is not modified (the reference dealiases U in place here:
- * call ts_dealias_field first to reproduce that side effect).  FFF and SSF plans (on
- * SSF the per-sphere algorithm in every dealias mode, through the sin/cos passes with
- * each product's parities); SSS plans return TS_ERR_UNSUPPORTED. */
+ * call ts_dealias_field first to reproduce that side effect).  FFF, SFF and SSF plans
+ * (on SFF and SSF the per-sphere algorithm in every dealias mode, through the sin/cos
+ * passes with each product's parities; on SFF the velocity flux of an RBC plan, in three
+ * dimensions or two); SSS plans return TS_ERR_UNSUPPORTED. */
 int ts_flux(ts_plan* plan, const void* u_hat, const double* radii, int n_radii, double* Pi);
 /* Universal::Dealias on ncomp components in place (FFF_pencil_basic.cc:87-90 corner
  * box, or the plan's two-thirds rule; nothing for dealias NONE). */

@@ -1471,19 +1471,22 @@ int ts_force_field(ts_plan* p, const void* u_hat, void* f_hat) {
   return TS_OK;
 }
 
-// the reference's per-sphere flux on the SSF basis: per radius the giver inputs (D U and
-// D U inside the sphere), the x and y sin/cos inverses, the FFF z pass with the nine
-// products u_j G_i, the y and x forward passes with the products' sine letters, and the
-// sum outside the sphere (the SSF step's passes, with the giver's product set)
+// the reference's per-sphere flux on the SSF and SFF bases: per radius the giver inputs
+// (D U and D U inside the sphere), the x sin/cos inverse, the y inverse (sin/cos on SSF,
+// FFT on SFF), the FFF z pass with the nine products u_j G_i, the y and x forward passes
+// with the products' sine letters, and the sum outside the sphere (the step's passes,
+// with the giver's product set)
 static int flux_ssf(ts_plan* p, const void* U, const double* radii, int n_radii, double* Pi) {
   const Geo& g = p->g;
   const Geo gy = y_as_x(g);
+  const bool sff = g.basis == TS_BASIS_SFF;
   const long long nb = 1 + 148 * 16;
   CKS(ensure_work(p, p->nS, 9));
   CKS(ensure_scratch(p, (size_t)n_radii * nb));
-  // x, y sine letters of u (Vx = SCF, Vy = CSF, Vz = CCF), the giver has the same; the
-  // product u_j G_i (field 3 j + i) is a sine series along an axis when exactly one factor is
-  const int vx[3] = {1, 0, 0}, vy[3] = {0, 1, 0};
+  // x, y sine letters of u (SSF: Vx = SCF, Vy = CSF, Vz = CCF; SFF: Vx = SFF, Vy = Vz = CFF,
+  // no y letters), the giver has the same; the product u_j G_i (field 3 j + i) is a sine
+  // series along an axis when exactly one factor is
+  const int vx[3] = {1, 0, 0}, vy[3] = {0, sff ? 0 : 1, 0};
   int mx_in = 0, my_in = 0, mx_out = 0, my_out = 0;
   for (int c = 0; c < 3; ++c) {
     mx_in |= (vx[c] << c) | (vx[c] << (3 + c));
@@ -1494,13 +1497,17 @@ static int flux_ssf(ts_plan* p, const void* U, const double* radii, int n_radii,
       mx_out |= (vx[j] ^ vx[i]) << (3 * j + i);
       my_out |= (vy[j] ^ vy[i]) << (3 * j + i);
     }
-  const double sy = 1.0 / (2.0 * g.Ny), sx = 1.0 / (2.0 * g.Nx * (double)g.Nz);
+  // forward normalisation: 1 / (2 Ny) on the SSF y sin/cos pass, and the rest
+  // (1 / (2 Nx Nz), on SFF 1 / (2 Nx Ny Nz)) on the x pass
+  const double sy = 1.0 / (2.0 * g.Ny), sx = 1.0 / (2.0 * g.Nx * (double)g.Nz * (sff ? g.Ny : 1));
   for (int r = 0; r < n_radii; ++r) {
     CK(LAUNCH(p, ssf_giver, g, U, p->P, radii[r], p->st));
     CK(LAUNCH(p, sff_x, g, +1, p->P, 1, mx_in, 1.0, p->twq, p->st, 6, g.S));
-    CK(LAUNCH(p, sff_x, gy, +1, p->P, g.Nx, my_in, 1.0, p->twqy, p->st, 6, g.S));
+    if (sff) CK(LAUNCH(p, strided, g, 1, +1, p->P, 6, p->twy, p->st));
+    else CK(LAUNCH(p, sff_x, gy, +1, p->P, g.Nx, my_in, 1.0, p->twqy, p->st, 6, g.S));
     CK(LAUNCH(p, z_fused, g, 6, p->P, p->twz, p->err_d, p->st));
-    CK(LAUNCH(p, sff_x, gy, -1, p->P, g.Nx, my_out, sy, p->twqy, p->st, 9, g.S));
+    if (sff) CK(LAUNCH(p, strided, g, 1, -1, p->P, 9, p->twy, p->st));
+    else CK(LAUNCH(p, sff_x, gy, -1, p->P, g.Nx, my_out, sy, p->twqy, p->st, 9, g.S));
     CK(LAUNCH(p, sff_x, g, -1, p->P, 1, mx_out, sx, p->twq, p->st, 9, g.S));
     CK(LAUNCH(p, ssf_flux_outside, g, p->P, U, radii[r], mx_out, my_out, p->dscr + r * nb, p->st));
   }
@@ -1515,7 +1522,8 @@ static int flux_ssf(ts_plan* p, const void* U, const double* radii, int n_radii,
 int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, double* Pi) {
   if (p && p->cfg.basis == TS_BASIS_SSS) return ssf_transforms_only();
   if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
-  if (p->cfg.basis != TS_BASIS_FFF && p->cfg.basis != TS_BASIS_SSF) return TS_ERR_UNSUPPORTED;
+  if (p->cfg.basis != TS_BASIS_FFF && p->cfg.basis != TS_BASIS_SSF && p->cfg.basis != TS_BASIS_SFF)
+    return TS_ERR_UNSUPPORTED;
   if (n_radii >= FLUX_MAX_BINS) {
     g_last_error = "ts_flux: at most " + std::to_string(FLUX_MAX_BINS - 1) + " radii";
     return TS_ERR_ARG;
@@ -1528,7 +1536,7 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
     if (i > 0 && radii[i] < radii[i - 1]) ascending = false;
   }
   const Geo& g = p->g;
-  if (p->cfg.basis == TS_BASIS_SSF)
+  if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SFF)
     return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false,
                        [&](void* U) -> int { return flux_ssf(p, U, radii, n_radii, Pi); });
   const long long nb = 1 + 148 * 16;  // a result plus the per-block partials of one reduction

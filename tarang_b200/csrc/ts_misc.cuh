@@ -407,15 +407,20 @@ __global__ void k_flux_outside(const C<T>* __restrict__ P, const C<T>* __restric
 }
 
 // ---------------------------------------------------------------------------
-// SSF per-sphere energy flux (EnergyTr::Compute_flux, compute_flux.cc:51-65, on the SSF
-// basis): k_ssf_giver writes the inputs of the giver nonlinear term, D U into P[0, 3)
-// and the giver D(U inside |K| <= R) (Fill_in_sphere, fill_space.cc:56-64) into
-// P[3, 6), with the SSF wavenumbers Kx = lx kx, Ky = ly ky, Kz = lz kz; after the
-// transforms P[3 j + i] holds F[u_j G_i], normalised, with x / y sine letters
-// qx, qy (bit f); k_ssf_flux_outside then forms N_i = sum_j D_j F[u_j G_i] (D_x, D_y:
-// +K on a sine series, -K on a cosine series; D_z = i Kz) and sums
-// 2 mult Re(N . conj(D U)) over |K| > R, per block (k_sum_partials adds the blocks).
+// SSF and SFF per-sphere energy flux (EnergyTr::Compute_flux, compute_flux.cc:51-65):
+// k_ssf_giver writes the inputs of the giver nonlinear term, D U into P[0, 3) and the
+// giver D(U inside |K| <= R) (Fill_in_sphere, fill_space.cc:56-64) into P[3, 6), with
+// Kx = lx kx (sin/cos along x), Ky = ly ky on SSF (sin/cos along y) and the FFT-order
+// ky on SFF (Fourier along y), Kz = lz kz; after the transforms P[3 j + i] holds
+// F[u_j G_i], normalised, with x / y sine letters qx, qy (bit f); k_ssf_flux_outside
+// then forms N_i = sum_j D_j F[u_j G_i] (D on a sin/cos axis: +K on a sine series, -K
+// on a cosine series; on a Fourier axis: i K) and sums 2 mult Re(N . conj(D U)) over
+// |K| > R, per block (k_sum_partials adds the blocks).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double flux_ky(const Geo& g, int ly) {
+  return (g.basis == 1 ? (double)kfft(ly, g.Ny) : (double)ly) * g.kf[1];
+}
+
 template <typename T>
 __global__ void k_ssf_giver(const C<T>* __restrict__ U, C<T>* __restrict__ P, Geo g, double R) {
   const long long n = g.S;
@@ -424,7 +429,7 @@ __global__ void k_ssf_giver(const C<T>* __restrict__ U, C<T>* __restrict__ P, Ge
     const int ly = (int)((e / g.Hz) % g.Ny);
     const int lx = (int)(e / ((long long)g.Ny * g.Hz));
     const bool dz = dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz);
-    const double Kx = lx * g.kf[0], Ky = ly * g.kf[1], Kz = lz * g.kf[2];
+    const double Kx = lx * g.kf[0], Ky = flux_ky(g, ly), Kz = lz * g.kf[2];
     const bool in = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz) <= R;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -445,7 +450,7 @@ __global__ void k_ssf_flux_outside(const C<T>* __restrict__ P, const C<T>* __res
     const int ly = (int)((e / g.Hz) % g.Ny);
     const int lx = (int)(e / ((long long)g.Ny * g.Hz));
     if (dealias_zero(g.dealias, g.basis, lx, ly, lz, g.Nx, g.Ny, g.Nz)) continue;
-    const double K[3] = {lx * g.kf[0], ly * g.kf[1], lz * g.kf[2]};
+    const double K[3] = {lx * g.kf[0], flux_ky(g, ly), lz * g.kf[2]};
     const double Kmag = sqrt((K[0] * K[0] + K[1] * K[1]) + K[2] * K[2]);
     if (!(Kmag > R)) continue;
     double re = 0;
@@ -456,9 +461,9 @@ __global__ void k_ssf_flux_outside(const C<T>* __restrict__ P, const C<T>* __res
       for (int j = 0; j < 3; ++j) {
         const int f = 3 * j + i;
         const C<T> q = P[f * n + e];
-        if (j == 2) {  // i Kz X
-          nr -= K[2] * (double)q.y;
-          ni += K[2] * (double)q.x;
+        if (j == 2 || (j == 1 && g.basis == 1)) {  // i K_j X on a Fourier axis
+          nr -= K[j] * (double)q.y;
+          ni += K[j] * (double)q.x;
         } else {
           const int sine = j == 0 ? (qx >> f & 1) : (qy >> f & 1);
           const double d = sine ? K[j] : -K[j];

@@ -70,6 +70,7 @@ class RunParams:
     input_field_procedure: int = 5   # io.input_field_procedure (1: read complex fields from in/)
     pr_option: str = "PRLARGE"       # PHYSICS.Pr_option (RBC)
     uscaling: str = "ULARGE"         # PHYSICS.Uscaling (RBC)
+    init_cond_modes: list = field(default_factory=list)   # io.init_cond_modes: ((kx, ky, kz), values)
 
     @property
     def nsteps(self) -> int:
@@ -192,6 +193,11 @@ def read_para(path: str) -> RunParams:
     io = p.get("io") or {}
     if io.get("input_field_procedure") is not None:
         rp.input_field_procedure = int(io["input_field_procedure"])
+    if rp.input_field_procedure == 4:
+        # Global_read.cc:506-540: coord [kx, ky, kz] and the mode's values, complex
+        # "(re,im)" entries (real numbers on SSS)
+        for m in io.get("init_cond_modes") or []:
+            rp.init_cond_modes.append((tuple(int(k) for k in m["coord"]), _mode_values(m["mode"])))
     et = p.get("energy_transfer") or {}
     fl = et.get("flux") or {}
     if _flag(et.get("turnon", False)) and _flag(fl.get("turnon", False)):
@@ -335,14 +341,154 @@ def load_state(folder: str, plan, kind: str, device: str = "cuda"):
     return out, float(head["t"]), int(head["step"])
 
 
+def _mode_values(items) -> list:
+    """The values of one ``init_cond_modes`` entry: numbers, or complex numbers written
+    "(re,im)" as yaml-cpp reads them (PyYAML splits a flow list at every comma, so the
+    items are joined back before the pairs are read)."""
+    import re
+    text = ",".join(str(v) for v in (items if isinstance(items, list) else [items]))
+    out = []
+    for pair_re, pair_im, num in re.findall(r"\(\s*([^,()\s]+)\s*,\s*([^,()\s]+)\s*\)|([^,()\s]+)", text):
+        out.append(complex(float(pair_re), float(pair_im)) if pair_re else complex(float(num), 0.0))
+    return out
+
+
+def _last_component(rp: RunParams, kx: int, ky: int, kz: int, Vx: complex, Vy: complex):
+    """Universal::Last_component: the third component from incompressibility, or the input
+    pair reinterpreted on the kz = 0 plane (FFF_pencil_basic.cc:51-73; SFF_pencil_basic.cc:
+    51-83 with Vx a sine series, sincostr_switch "SFF": d_x Vx = +Kx Vx)."""
+    Kx, Ky, Kz = kx * rp.kfactor[0], ky * rp.kfactor[1], kz * rp.kfactor[2]
+    dvx = 1j * Kx * Vx if rp.basis == "FFF" else Kx * Vx
+    if kz != 0:
+        return Vx, Vy, (dvx + 1j * Ky * Vy) / (-1j * Kz)
+    if ky != 0:
+        return Vx, dvx / (-1j * Ky), Vy
+    if rp.basis == "FFF":
+        return 0j, Vx, Vy
+    return 0j, complex(Vx.real, 0.0), complex(Vy.real, 0.0)
+
+
+def init_cond_modes(rp: RunParams) -> list:
+    """FluidIO::Init_cond_modes for ``io.input_field_procedure: 4`` (init_cond_modes.cc:
+    56-100 fluid, 153-221 scalar / RBC, 224-275 RBC PRZERO / PRINFTY) on FFF and SFF:
+    host arrays (complex128, the spectral layout) of the run's fields with every listed
+    mode set.  Per mode (kx, ky, kz): the fluid reads Vx and, for Ny > 1, Vy; the scalar
+    and RBC (PRLARGE, PRSMALL) read Vx, Vy and the scalar G; PRINFTY reads G only and
+    PRZERO the fluid's values (their slaved field comes from ``Plan.rbc_slave``).  The last
+    velocity component is ``_last_component``; Assign_field_and_comp_conj (FluidVF.cc:
+    407-433, FluidSF.cc:265-292) also sets, on the kz = 0 plane, the mirror mode
+    (FFF (-kx, -ky), SFF (kx, -ky)) of the velocity to its conjugate, and, on the kz = 0
+    and kz = Nz/2 planes, the scalar's mirror to the same value G (the reference assigns
+    G there, not its conjugate).  Modes outside the array are skipped (Assign_spectral_field
+    range check).  Then Read_init_cond's preprocessing (init_cond_main.cc:80-88, 138-150):
+    the strong reality condition (always for the fluid, with
+    apply_strong_realitycond_alltime_switch for the scalar kinds) and, on SFF, Zero_modes
+    (SFF_pencil_basic.cc:214-243: the sine components Vx and T at kx = 0).  Other kinds
+    and bases are refused by name."""
+    if rp.basis not in ("FFF", "SFF") or rp.kind not in ("FLUID_INCOMPRESS", "RBC", "SCALAR_INCOMPRESS"):
+        raise NotImplementedError(f"io.input_field_procedure 4 for {rp.kind} on {rp.basis}: "
+                                  "the fluid, scalar and RBC modes on FFF and SFF")
+    Nx, Ny, Nz = rp.N
+    H = Nz // 2 + 1
+    U = np.zeros((3, Nx, Ny, H), np.complex128)
+    scal = rp.kind != "FLUID_INCOMPRESS"
+    T = np.zeros((1, Nx, Ny, H), np.complex128) if scal else None
+
+    def index(kx, ky, kz):
+        lx = kx if rp.basis == "SFF" else (kx + Nx if kx < 0 else kx)
+        ly = ky + Ny if ky < 0 else ky
+        ok = 0 <= lx < Nx and 0 <= ly < Ny and 0 <= kz < H
+        return (lx, ly, kz) if ok else None
+
+    def mirror(kx, ky):
+        return (-kx, -ky) if rp.basis == "FFF" else (kx, -ky)
+
+    def put_vector(kx, ky, kz, V):
+        i = index(kx, ky, kz)
+        if i is not None:
+            U[(slice(None),) + i] = V
+        if kz == 0:
+            j = index(*mirror(kx, ky), kz)
+            if j is not None:
+                U[(slice(None),) + j] = np.conj(V)
+
+    def put_scalar(kx, ky, kz, G):
+        i = index(kx, ky, kz)
+        if i is not None:
+            T[(0,) + i] = G
+        if kz == 0 or kz == Nz // 2:
+            j = index(*mirror(kx, ky), kz)
+            if j is not None:
+                T[(0,) + j] = G
+
+    prinfty = rp.kind == "RBC" and rp.pr_option == "PRINFTY"
+    fluid_only = rp.kind == "FLUID_INCOMPRESS" or (rp.kind == "RBC" and rp.pr_option == "PRZERO")
+    for (kx, ky, kz), vals in rp.init_cond_modes:
+        vals = list(vals) + [0j] * 3
+        if prinfty:
+            put_scalar(kx, ky, kz, vals[0])
+            continue
+        Vy = vals[1] if (Ny > 1 or not fluid_only) else 0j
+        put_vector(kx, ky, kz, np.array(_last_component(rp, kx, ky, kz, vals[0], Vy)))
+        if not fluid_only:
+            put_scalar(kx, ky, kz, vals[2])
+    if not scal or rp.reality_fix:
+        U = np.stack([_strong_reality(rp, U[c]) for c in range(3)])
+        if scal:
+            T = _strong_reality(rp, T[0])[None]
+    if rp.basis == "SFF":
+        U[0, 0] = 0
+        if scal:
+            T[0, 0] = 0
+    return [U] if not scal else [U, T]
+
+
+def _strong_reality(rp: RunParams, A: np.ndarray) -> np.ndarray:
+    """Satisfy_strong_reality_condition_in_Array on one component: FFF (FFF_pencil_basic.cc:
+    139-179) A(kx, ky, 0) = conj A(-kx, -ky, 0) for kx < 0 (ky != Ny/2) and for kx = 0,
+    ky < 0; SFF (SFF_pencil_basic.cc:143-167) A(m, ky, 0) = conj A(m, -ky, 0) for ky < 0;
+    then the kz = Nz/2 plane is zero."""
+    Nx, Ny, Nz = rp.N
+    B = A.copy()
+    ky = np.where(np.arange(Ny) <= Ny // 2, np.arange(Ny), np.arange(Ny) - Ny)
+    neg_y = (-ky) % Ny
+    if rp.basis == "FFF":
+        kx = np.where(np.arange(Nx) <= Nx // 2, np.arange(Nx), np.arange(Nx) - Nx)
+        for lx in range(Nx):
+            if kx[lx] < 0:
+                src = (-kx[lx]) % Nx
+                for ly in range(Ny):
+                    if ky[ly] != Ny // 2 or Ny == 1:
+                        B[lx, ly, 0] = np.conj(B[src, neg_y[ly], 0])
+        for ly in range(Ny):
+            if ky[ly] < 0:
+                B[0, ly, 0] = np.conj(B[0, neg_y[ly], 0])
+    else:
+        for ly in range(Ny):
+            if ky[ly] < 0:
+                B[:, ly, 0] = np.conj(B[:, neg_y[ly], 0])
+    if Nz // 2 < B.shape[2] and Nz > 1:
+        B[:, :, Nz // 2] = 0
+    return B
+
+
 def read_init_cond(data_dir: str, plan, rp: RunParams):
-    """FluidIO::Read_init_cond for ``io.input_field_procedure: 1`` (init_cond_main.cc:48-56,
-    Init_cond_complex_field init_cond_field.cc:49-58): the run's complex fields from
-    ``<data_dir>/in/`` as ``save_state`` writes them.  Returns (fields, t, step); the run
-    continues from time t.  Other procedures are refused by name."""
+    """FluidIO::Read_init_cond (init_cond_main.cc:48-56): ``io.input_field_procedure: 1``
+    (Init_cond_complex_field init_cond_field.cc:49-58) reads the run's complex fields from
+    ``<data_dir>/in/`` as ``save_state`` writes them; ``4`` sets the listed modes
+    (``init_cond_modes``).  Returns (fields, t, step); the run continues from time t.
+    Other procedures are refused by name."""
+    if rp.input_field_procedure == 4:
+        import torch
+        want = torch.complex64 if plan.precision == "f32" else torch.complex128
+        fields = [torch.from_numpy(a).to(want).to("cuda").contiguous() for a in init_cond_modes(rp)]
+        if rp.kind == "RBC" and rp.pr_option in ("PRZERO", "PRINFTY"):
+            plan.rbc_slave(fields[0], fields[1])
+        return fields, rp.t_init, 0
     if rp.input_field_procedure != 1:
         raise NotImplementedError(f"io.input_field_procedure {rp.input_field_procedure}: "
-                                  "1 (complex fields from in/) only; seeded spectra use Plan.init_energy_spectrum")
+                                  "1 (complex fields from in/) and 4 (modes) only; seeded spectra use "
+                                  "Plan.init_energy_spectrum")
     fields, t, step = load_state(os.path.join(data_dir, "in"), plan, rp.kind)
     if rp.kind == "RBC" and rp.pr_option in ("PRZERO", "PRINFTY"):
         # Init_cond_RBC_complex_field (init_cond_field.cc:176-190): the slaved field is

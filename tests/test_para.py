@@ -585,7 +585,7 @@ def test_read_para_input_field_procedure(tmp_path):
     (tmp_path / "in" / "para.yaml").write_text(text.replace("io:\n", "io:\n    input_field_procedure: 1\n"))
     rp = para.read_para(str(tmp_path / "in" / "para.yaml"))
     assert rp.input_field_procedure == 1
-    rp.input_field_procedure = 4
+    rp.input_field_procedure = 6
     with pytest.raises(NotImplementedError):
         para.read_init_cond(str(tmp_path), None, rp)
 
@@ -722,3 +722,116 @@ def test_glob_helicity_of_a_beltrami_mode(cuda, tmp_path, sign):
     E = plan.energy(u)
     assert abs(row[3] - sign * Km * E) < 1e-13 * Km * E
     assert abs(row[4] - sign * E / Km) < 1e-13 * E / Km
+
+
+MODES_RBC_2D = """io:
+    input_field_procedure: 4
+    init_cond_modes:
+            - coord: [1,0,1]
+              mode: [ (0.01,0), (0,0), (0,0) ]
+            - coord: [2,0,0]
+              mode: [ (0,0), (0,0), (-0.16,0) ]
+            - coord: [3,0,40]
+              mode: [ (1,0), (0,0), (1,0) ]
+"""
+
+
+def _modes_para(tmp_path, src_dir, modes_text, edit=None):
+    text = open(os.path.join(src_dir, "in", "para.yaml")).read()
+    text = "\n".join(line for line in text.split("\n") if not line.startswith("io:")) + "\n" + modes_text
+    if edit:
+        text = edit(text)
+    (tmp_path / "in").mkdir(exist_ok=True)
+    (tmp_path / "in" / "para.yaml").write_text(text)
+    return para.read_para(str(tmp_path / "in" / "para.yaml"))
+
+
+def test_init_cond_modes_rbc_two_dimensional(tmp_path):
+    """io.input_field_procedure 4 on the reference's RBC/2d layout (SFF, 32 x 1 x 32): the
+    "(re,im)" values parse, Vz follows from incompressibility (SFF: d_x of the sine series
+    Vx is +Kx Vx), the scalar takes its value, a mode outside the array (kz = 40) is
+    skipped, and nothing else is set."""
+    rp = _modes_para(tmp_path, KIND_DIRS["rbc_2d"], MODES_RBC_2D)
+    assert rp.input_field_procedure == 4 and len(rp.init_cond_modes) == 3
+    assert rp.init_cond_modes[0] == ((1, 0, 1), [0.01 + 0j, 0j, 0j])
+    U, T = para.init_cond_modes(rp)
+    Kx, Kz = 1 * rp.kfactor[0], 1 * rp.kfactor[2]
+    want_U = np.zeros_like(U)
+    want_U[0, 1, 0, 1] = 0.01
+    want_U[2, 1, 0, 1] = Kx * 0.01 / (-1j * Kz)
+    want_T = np.zeros_like(T)
+    want_T[0, 2, 0, 0] = -0.16
+    assert np.array_equal(U, want_U) and np.array_equal(T, want_T)
+    # divergence of the set mode: Kx Vx + i Kz Vz = 0
+    assert abs(Kx * U[0, 1, 0, 1] + 1j * Kz * U[2, 1, 0, 1]) < 1e-18
+
+
+def test_init_cond_modes_fff_fluid_conjugates_and_divergence(tmp_path):
+    """FFF fluid modes: Vz from incompressibility off the kz = 0 plane; on it the pair read
+    is (Vx, Vz) with Vy computed (ky != 0), or (Vy, Vz) with Vx = 0 (ky = 0); the mirror
+    (-kx, -ky, 0) holds the conjugate; every set mode is solenoidal."""
+    modes = """io:
+    input_field_procedure: 4
+    init_cond_modes:
+            - coord: [1,2,3]
+              mode: [ (0.1,0.2), (0.3,-0.1) ]
+            - coord: [2,-1,0]
+              mode: [ (0.5,0.1), (0.2,0.0) ]
+            - coord: [3,0,0]
+              mode: [ (0.4,0.0), (0.0,0.7) ]
+"""
+    rp = _modes_para(tmp_path, FFF_DIR, modes)
+    (U,) = para.init_cond_modes(rp)
+    Nx, Ny, Nz = rp.N
+    kf = rp.kfactor
+    set_modes = np.argwhere(np.abs(U).sum(axis=0) > 0)
+    for lx, ly, lz in set_modes:
+        kx = lx if lx <= Nx // 2 else lx - Nx
+        ky = ly if ly <= Ny // 2 else ly - Ny
+        div = 1j * (kx * kf[0] * U[0, lx, ly, lz] + ky * kf[1] * U[1, lx, ly, lz] + lz * kf[2] * U[2, lx, ly, lz])
+        assert abs(div) < 1e-15
+    assert np.allclose(U[:, 1, 2, 3], [0.1 + 0.2j, 0.3 - 0.1j, U[2, 1, 2, 3]])
+    # kz = 0, ky != 0: the pair is (Vx, Vz), the mirror is the conjugate
+    assert U[0, 2, Ny - 1, 0] == 0.5 + 0.1j and U[2, 2, Ny - 1, 0] == 0.2
+    assert np.array_equal(U[:, Nx - 2, 1, 0], np.conj(U[:, 2, Ny - 1, 0]))
+    # kz = 0, ky = 0: the pair is (Vy, Vz) and Vx = 0
+    assert U[0, 3, 0, 0] == 0 and U[1, 3, 0, 0] == 0.4 and U[2, 3, 0, 0] == 0.7j
+    assert np.array_equal(U[:, Nx - 3, 0, 0], np.conj(U[:, 3, 0, 0]))
+
+
+def test_init_cond_modes_refused_off_fff_sff(tmp_path):
+    rp = _modes_para(tmp_path, KIND_DIRS["sss"], "io:\n    input_field_procedure: 4\n    init_cond_modes:\n"
+                     "            - coord: [1,0,1]\n              mode: [ 1, 0 ]\n")
+    with pytest.raises(NotImplementedError):
+        para.init_cond_modes(rp)
+    rp = _modes_para(tmp_path, KIND_DIRS["mhd"], MODES_RBC_2D)
+    with pytest.raises(NotImplementedError):
+        para.init_cond_modes(rp)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pr", ["PRLARGE", "PRZERO"])
+def test_init_cond_modes_rbc_steps_like_the_oracle(cuda, tmp_path, pr):
+    """A two-dimensional RBC run started from io.input_field_procedure 4 (the reference's
+    RBC/2d modes; PRZERO also slaves T = U1 / K^2 on the device) steps like the oracle
+    from the same modes: FP64 relative L2 <= 1e-12 after 3 steps."""
+    from oracle import tarang_ref as R
+    rp = _modes_para(tmp_path, KIND_DIRS["rbc_2d"], MODES_RBC_2D,
+                     edit=lambda t: t.replace("Pr_option: PRLARGE", f"Pr_option: {pr}"))
+    plan, rp2 = para.plan_from_dir(str(tmp_path), precision="f64")
+    fields, t, step = para.read_init_cond(str(tmp_path), plan, rp2)
+    U0, T0 = para.init_cond_modes(rp2)
+    g = R.Grid(rp2.N, rp2.kfactor, "SFF")
+    cfg = R.RBCConfig(g, Ra=rp2.Ra, Pr=rp2.Pr, dt=rp2.dt, dealias_mode=1, reality_fix=rp2.reality_fix,
+                      pr_option=pr, uscaling=rp2.uscaling)
+    if pr == "PRZERO":
+        T0 = R.rbc_slave_temperature(g, U0)[None]
+    assert np.abs(fields[1][0].cpu().numpy() - T0[0]).max() <= 1e-15 * max(1.0, np.abs(T0).max())
+    Uo, To = U0, T0[0]
+    for _ in range(3):
+        Uo, To = R.rbc_rk4_step(cfg, Uo, To)
+    para.advance(plan, rp2.kind, fields, 3)
+    u, T = fields
+    assert np.linalg.norm(u.cpu().numpy() - Uo) <= 1e-12 * np.linalg.norm(Uo)
+    assert np.linalg.norm(T[0].cpu().numpy() - To) <= 1e-12 * max(np.linalg.norm(To), 1e-300)
+    plan.close()
