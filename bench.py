@@ -119,10 +119,13 @@ def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024), prec:
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clk = Clocks(torch.cuda.current_device())
+    clk.start()
     e0.record()
     plan.rk4_step(u, steps)
     e1.record()
     torch.cuda.synchronize()
+    clocks = clk.stop()
     ms = e0.elapsed_time(e1)
     # per-kernel rates from one further, separately profiled step
     L.check(plan.lib.ts_profile_reset(plan.h), "reset")
@@ -139,7 +142,8 @@ def fff1024_leg(steps: int = 3, warmup: int = 2, shape=(1024, 1024, 1024), prec:
     n3 = float(shape[0]) * shape[1] * shape[2]
     sb = 4 if prec == "f32" else 8
     out = {"steps_per_s": steps / (ms / 1e3), "kernel_GBps": kern, "energy": plan.energy(u),
-           "model_frac": 288.0 * n3 * sb * steps / (ms / 1e3) / 1e9 / measured_peak()[0], "tuning": tuned}
+           "model_frac": 288.0 * n3 * sb * steps / (ms / 1e3) / 1e9 / measured_peak()[0], "tuning": tuned,
+           "clocks": clocks}
     plan.close()
     del u
     torch.cuda.empty_cache()

@@ -57,7 +57,6 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
                   long long ostride, int nouter, const C<T>* __restrict__ tw, int per, long long mstride,
                   int zero_hi) {
   typedef C<T> V;
-  pdl_begin();
   static_assert(NT >= 1 && NT <= 4, "one to three staging tiles");
   constexpr int NBUF = NT == 4 ? 3 : (NT == 1 ? 1 : 2);  // staging tiles: items in flight = NBUF - 1 ahead
   constexpr bool XC = NT != 3;           // exchange in the consumed staging tile
@@ -240,7 +239,6 @@ __global__ void __launch_bounds__(CW * (L / E), (CW * (L / E)) <= 256 ? 2 : 1)
     k_inv_x_ld(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw,
                const C<T>* __restrict__ Lam, T lsc, int kept, double rad) {
   typedef C<T> V;
-  pdl_begin();
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
   const int c = threadIdx.x % CW, t = threadIdx.x / CW;
@@ -361,7 +359,6 @@ template <typename T, int L, int E, int CW, int FORM>
 __global__ void __launch_bounds__(CW * (L / E), 1)
     k_inv_x_st(const C<T>* __restrict__ U, C<T>* __restrict__ W, Geo g, const C<T>* __restrict__ tw) {
   typedef C<T> V;
-  pdl_begin();
   static_assert(FORM == 0 || FORM == 1, "the fluid forms");
   constexpr int LK = ix_kept_rows<L>(), Q = L / 3;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -913,7 +910,6 @@ template <typename T, int NZ, int FORM, int EZ = 0, bool BATCH = false>
 __global__ void __launch_bounds__(zreg_threads<FORM>(), zreg_min_blocks<NZ, EZ, FORM>())
     k_z_reg(C<T>* __restrict__ P, Geo g, const C<T>* __restrict__ tw, long long msP, int zkeep) {
   typedef C<T> V;
-  pdl_begin();
   constexpr int M = NZ / 2, H = M + 1, E = EZ ? EZ : ((M % 3 == 0) ? 12 : 8), TPL = M / E, LDX = zslot<M>();
   static_assert(TPL >= 1 && TPL <= 64, "a line spans at most two warps");
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
@@ -1395,7 +1391,6 @@ __global__ void __launch_bounds__(CW * (L / E), 1)
     k_fwd_x(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mA,
             const __grid_constant__ CUtensorMap mB, Geo g, StageArgs a, const C<T>* __restrict__ tw) {
   typedef C<T> V;
-  pdl_begin();
   constexpr int NF = FORM == 1 ? 3 : 6;
   constexpr int TILE = L * CW, BR = L < 256 ? L : 256, UNITS = (int)sizeof(V) / 8;
   constexpr int NST = MODE == MODE_NLIN ? 0 : 6;

@@ -76,23 +76,6 @@ template <typename K> cudaError_t smem_attr(K kernel, size_t bytes) {
   return cudaSuccess;
 }
 
-// launch with programmatic stream serialisation (the kernel calls pdl_begin before its
-// first global memory access, so it may be scheduled while the previous kernel drains)
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t sm, cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = sm;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
-}
-
 inline unsigned grid1d(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b > 148 * 16) b = 148 * 16;
@@ -187,9 +170,10 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       if (blocks > nwork) blocks = nwork;
       auto launch = [&](auto k) {
         if ((err = smem_attr(k, sm)) != cudaSuccess) return;
-        err = launch_pdl(k, dim3((unsigned)blocks), dim3(CW * (LL / E)), sm, st, (V*)data, nf, g.S, inner, rstride,
-                         ostride, nouter, (const V*)tw, per, mstride, zero_hi);
+        k<<<(unsigned)blocks, CW * (LL / E), sm, st>>>((V*)data, nf, g.S, inner, rstride, ostride, nouter,
+                                                      (const V*)tw, per, mstride, zero_hi);
         ++g_launches;
+        err = cudaGetLastError();
       };
       if (dir < 0) launch(k_strided_fft<T, LL, E, CW, -1, NT>);
       else launch(k_strided_fft<T, LL, E, CW, 1, NT>);
@@ -262,8 +246,9 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
         const unsigned blocks = (unsigned)((2 * (g.Ny / 3) + 1) * ((nzk + CW - 1) / CW));
         auto run = [&](auto kern) {
           if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
-          err_ = launch_pdl(kern, dim3(blocks), dim3(CW * (LL / E)), sm, st, (const V*)U, (V*)W, g, (const V*)tw);
+          kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw);
           ++g_launches;
+          err_ = cudaGetLastError();
         };
         if (form == 0) { run(k_inv_x_st<T, LL, E, CW, 0>); return; }
         if (form == 1) { run(k_inv_x_st<T, LL, E, CW, 1>); return; }
@@ -302,9 +287,10 @@ template <> cudaError_t Launch<T>::inv_x(const Geo& g, int form, const void* U, 
                                    : (unsigned)((inner + CW - 1) / CW);
       auto run = [&](auto kern) {
         if ((err_ = smem_attr(kern, sm)) != cudaSuccess) return;
-        err_ = launch_pdl(kern, dim3(blocks), dim3(CW * (LL / E)), sm, st, (const V*)U, (V*)W, g, (const V*)tw,
-                          (const V*)lam, (T)lsc, kept, rad);
+        kern<<<blocks, CW * (LL / E), sm, st>>>((const V*)U, (V*)W, g, (const V*)tw, (const V*)lam, (T)lsc, kept,
+                                                 rad);
         ++g_launches;
+        err_ = cudaGetLastError();
       };
       if (form == 0) run(k_inv_x_ld<T, LL, E, CW, 0>);
       else if (form == 1) run(k_inv_x_ld<T, LL, E, CW, 1>);
@@ -386,10 +372,11 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
     // loads each component just before its transform
     constexpr int NT = zreg_threads<FORM>(), LPB = NT / (M / 8);
     const dim3 grid((unsigned)((nlines + LPB - 1) / LPB), nmem);
+    if (v == 4) k_z_reg<T, NZ, FORM, 0, false><<<grid, NT, 0, st>>>((V*)P, g, (const V*)tw, msP, zkeep);
+    else if (v == 0) k_z_reg<T, NZ, FORM, 0, true><<<grid, NT, 0, st>>>((V*)P, g, (const V*)tw, msP, zkeep);
     if (v == 4 || v == 0) {
       ++g_launches;
-      return v == 4 ? launch_pdl(k_z_reg<T, NZ, FORM, 0, false>, grid, dim3(NT), 0, st, (V*)P, g, (const V*)tw, msP, zkeep)
-                    : launch_pdl(k_z_reg<T, NZ, FORM, 0, true>, grid, dim3(NT), 0, st, (V*)P, g, (const V*)tw, msP, zkeep);
+      return cudaGetLastError();
     }
   }
   if constexpr (z_valid<NZ, FORM>(3)) {
@@ -429,11 +416,8 @@ static cudaError_t z_fused_impl(const Geo& g, void* P, const void* tw, int* zerr
     if constexpr (FORM == 3)
       k_z_reg_adj<T, NZ><<<(unsigned)((nlines + LPB - 1) / LPB), NT, 0, st>>>((V*)P, g, (const V*)tw, zkeep);
     else
-    {
-      ++g_launches;
-      return launch_pdl(k_z_reg<T, NZ, FORM>, dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), dim3(NT), 0, st,
-                        (V*)P, g, (const V*)tw, msP, zkeep);
-    }
+      k_z_reg<T, NZ, FORM><<<dim3((unsigned)((nlines + LPB - 1) / LPB), nmem), NT, 0, st>>>((V*)P, g, (const V*)tw,
+                                                                                           msP, zkeep);
     ++g_launches;
     return cudaGetLastError();
   }
@@ -583,8 +567,7 @@ static cudaError_t fwd_x_fused(const Geo& g, const void* P, const StageArgs& a, 
   if ((err = make_field_map(&mB, B, inner, 3LL * g.Nx, UNITS, CW, br)) != cudaSuccess) return err;
   auto k = k_fwd_x<T, LL, E, CW, FORM, MODE>;
   if ((err = smem_attr(k, sm)) != cudaSuccess) return err;
-  if ((err = launch_pdl(k, dim3(blocks), dim3(CW * (LL / E)), sm, st, mP, mA, mB, g, a, (const V*)tw)) != cudaSuccess)
-    return err;
+  k<<<blocks, CW * (LL / E), sm, st>>>(mP, mA, mB, g, a, (const V*)tw);
   ++g_launches;
   if (MODE == MODE_FLUX) {
     k_bins_finish<<<1, 64, 0, st>>>(a.bins + (a.nradii + 1), blocks, a.nradii + 1, a.bins);

@@ -19,16 +19,6 @@ namespace ts {
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Programmatic dependent launch: a kernel launched with programmatic stream
-// serialisation may start while the previous kernel on its stream finishes.  pdl_begin
-// waits until that kernel has completed and its memory is visible (a no-op for a plain
-// launch), then lets the next kernel be scheduled once every block of this one has
-// started; call it before the kernel's first global memory access.
-__device__ __forceinline__ void pdl_begin() {
-  asm volatile("griddepcontrol.wait;\n" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
-}
-
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
