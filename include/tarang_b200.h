@@ -55,7 +55,8 @@ typedef enum {
  * the padded real layout (Nx, Ny, Nz + 2) of each component (the complex buffer viewed
  * as reals, as SSS_PENCIL does) and offers the transforms (parities [SC][SC][SC]) and
  * ts_rk4_step for the conservative, unforced fluid (sincostr_switch "SCC": Vx = SCC,
- * Vy = CSC, Vz = CCS). */
+ * Vy = CSC, Vz = CCS), ts_rk4_step_rbc, ts_energy, ts_nusselt, ts_max_div,
+ * ts_shell_spectrum, ts_flux and ts_dealias_field. */
 typedef enum { TS_BASIS_FFF = 0, TS_BASIS_SFF = 1, TS_BASIS_SSF = 2, TS_BASIS_SSS = 3 } ts_basis;
 typedef enum { TS_F64 = 0, TS_F32 = 1 } ts_precision;
 typedef enum { TS_NLIN_CONSERVATIVE = 0, TS_NLIN_ROTATIONAL = 1 } ts_nlin_form;
@@ -199,10 +200,12 @@ int ts_shell_spectrum(ts_plan* plan, const void* a_hat, int ncomp, double* Ek, i
  * call ts_dealias_field first to reproduce that side effect).  FFF, SFF and SSF plans
  * (on SFF and SSF the per-sphere algorithm in every dealias mode, through the sin/cos
  * passes with each product's parities; on SFF the velocity flux of an RBC plan, in three
- * dimensions or two); SSS plans return TS_ERR_UNSUPPORTED. */
+ * dimensions or two), and SSS plans (the per-sphere algorithm on the real coefficients,
+ * sphere fill and outside sum over the real z index, SSS_pencil_ET.cc:50-70, 662-678). */
 int ts_flux(ts_plan* plan, const void* u_hat, const double* radii, int n_radii, double* Pi);
 /* Universal::Dealias on ncomp components in place (FFF_pencil_basic.cc:87-90 corner
- * box, or the plan's two-thirds rule; nothing for dealias NONE). */
+ * box, or the plan's two-thirds rule; nothing for dealias NONE; on SSS plans the real
+ * coefficients by the real z index). */
 int ts_dealias_field(ts_plan* plan, void* a_hat, int ncomp);
 /* Raw shell sums for the reference's text outputs: sums[k] = sum over modes with
  * ceil|K| = k of mult K^2 Re(A . conj(B)) (B = NULL: |A|^2), counts[k] = sum of

@@ -1519,11 +1519,49 @@ static int flux_ssf(ts_plan* p, const void* U, const double* radii, int n_radii,
   return TS_OK;
 }
 
+// the reference's per-sphere flux on the SSS basis (real coefficients; sincostr_switch
+// "SCC": Vx = SCC, Vy = CSC, Vz = CCS, the giver the same): per radius the giver inputs,
+// the x and y sin/cos inverses, the fused SSS z pass with the nine products u_j G_i
+// (sin/cos inverse, products, sin/cos forward), the y and x forward passes with the
+// products' sine letters, and the sum outside the sphere
+static int flux_sss(ts_plan* p, const void* U, const double* radii, int n_radii, double* Pi) {
+  const Geo& g = p->g;
+  const Geo gy = y_as_x(g);
+  const long long nb = 1 + 148 * 16;
+  CKS(ensure_work(p, p->nS, 9));
+  CKS(ensure_scratch(p, (size_t)n_radii * nb));
+  const int vx[3] = {1, 0, 0}, vy[3] = {0, 1, 0}, vz[3] = {0, 0, 1};
+  int mx_in = 0, my_in = 0, mz_in = 0, mx_out = 0, my_out = 0, mz_out = 0;
+  for (int c = 0; c < 3; ++c) {
+    mx_in |= (vx[c] << c) | (vx[c] << (3 + c));
+    my_in |= (vy[c] << c) | (vy[c] << (3 + c));
+    mz_in |= (vz[c] << c) | (vz[c] << (3 + c));
+  }
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) {
+      mx_out |= (vx[j] ^ vx[i]) << (3 * j + i);
+      my_out |= (vy[j] ^ vy[i]) << (3 * j + i);
+      mz_out |= (vz[j] ^ vz[i]) << (3 * j + i);
+    }
+  for (int r = 0; r < n_radii; ++r) {
+    CK(LAUNCH(p, sss_giver, g, U, p->P, radii[r], p->st));
+    CK(LAUNCH(p, sff_x, g, +1, p->P, 1, mx_in, 1.0, p->twq, p->st, 6, g.S));
+    CK(LAUNCH(p, sff_x, gy, +1, p->P, g.Nx, my_in, 1.0, p->twqy, p->st, 6, g.S));
+    CK(LAUNCH(p, sss_z_fused, g, 6, p->P, p->twz, p->twqz, mz_in, mz_out, p->st));
+    CK(LAUNCH(p, sff_x, gy, -1, p->P, g.Nx, my_out, 1.0 / (2.0 * g.Ny), p->twqy, p->st, 9, g.S));
+    CK(LAUNCH(p, sff_x, g, -1, p->P, 1, mx_out, 1.0 / (2.0 * g.Nx), p->twq, p->st, 9, g.S));
+    CK(LAUNCH(p, sss_flux_outside, g, p->P, U, radii[r], mx_out, my_out, mz_out, p->dscr + r * nb, p->st));
+  }
+  std::vector<double> h(n_radii);
+  for (int r = 0; r < n_radii; ++r)
+    CK(cudaMemcpyAsync(&h[r], p->dscr + r * nb, sizeof(double), cudaMemcpyDeviceToHost, p->st));
+  CK(cudaStreamSynchronize(p->st));
+  for (int r = 0; r < n_radii; ++r) Pi[r] = -h[r];
+  return TS_OK;
+}
+
 int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, double* Pi) {
-  if (p && p->cfg.basis == TS_BASIS_SSS) return ssf_transforms_only();
   if (!p || !u_hat || !radii || !Pi || n_radii < 1) return TS_ERR_ARG;
-  if (p->cfg.basis != TS_BASIS_FFF && p->cfg.basis != TS_BASIS_SSF && p->cfg.basis != TS_BASIS_SFF)
-    return TS_ERR_UNSUPPORTED;
   if (n_radii >= FLUX_MAX_BINS) {
     g_last_error = "ts_flux: at most " + std::to_string(FLUX_MAX_BINS - 1) + " radii";
     return TS_ERR_ARG;
@@ -1539,6 +1577,9 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
   if (p->cfg.basis == TS_BASIS_SSF || p->cfg.basis == TS_BASIS_SFF)
     return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false,
                        [&](void* U) -> int { return flux_ssf(p, U, radii, n_radii, Pi); });
+  if (p->cfg.basis == TS_BASIS_SSS)
+    return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false,
+                       [&](void* U) -> int { return flux_sss(p, U, radii, n_radii, Pi); });
   const long long nb = 1 + 148 * 16;  // a result plus the per-block partials of one reduction
   return with_device(p, &p->stage_u, u_hat, 3 * g.S * p->cb, false, [&](void* U) -> int {
     std::vector<double> h(n_radii + 1);
@@ -1591,13 +1632,11 @@ int ts_flux(ts_plan* p, const void* u_hat, const double* radii, int n_radii, dou
 
 int ts_dealias_field(ts_plan* p, void* a_hat, int ncomp) {
   if (!p || !a_hat || ncomp < 1 || ncomp > 3) return TS_ERR_ARG;
-  if (p->cfg.basis == TS_BASIS_SSS) {
-    g_last_error = "ts_dealias_field: SSS plans hold real coefficients (use the step's own dealiasing)";
-    return TS_ERR_UNSUPPORTED;
-  }
   if (!p->g.dealias) return TS_OK;
   return with_device(p, &p->stage_u, a_hat, (size_t)ncomp * p->g.S * p->cb, true, [&](void* A) -> int {
-    CK(LAUNCH(p, dealias_copy, p->g, A, A, ncomp, p->st));
+    // SSS: real coefficients, each element read and written by the same thread
+    if (p->cfg.basis == TS_BASIS_SSS) CK(LAUNCH(p, sss_dealias_copy, p->g, A, A, ncomp, p->st));
+    else CK(LAUNCH(p, dealias_copy, p->g, A, A, ncomp, p->st));
     CK(cudaStreamSynchronize(p->st));
     return (int)TS_OK;
   });

@@ -689,7 +689,8 @@ __global__ void __launch_bounds__(256) k_sss_z_fused(C<T>* __restrict__ P, Geo g
   typedef C<T> V;
   constexpr int N = NZ, M = NZ / 2, H = M + 1, TPL = M / E, LDS = zslot<M>();
   constexpr int NIN = z_nin(FORM), NOUT = z_nout(FORM);
-  static_assert(FORM == 0 || FORM == 2, "SSS z pass: conservative products, with or without T");
+  static_assert(FORM == 0 || FORM == 2 || FORM == 6,
+                "SSS z pass: conservative products, with or without T, or the flux giver's products");
   extern __shared__ __align__(16) unsigned char smraw[];
   V* sm = reinterpret_cast<V*>(smraw);
   const long long nlines = (long long)g.Nx * g.Ny;

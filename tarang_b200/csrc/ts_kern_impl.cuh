@@ -470,10 +470,12 @@ static cudaError_t sss_z_slots(const Geo& g, void* P, const void* tw, const void
 template <> cudaError_t Launch<T>::sss_z_fused(const Geo& g, int form, void* P, const void* tw, const void* tq, int zin,
                                                int zout, cudaStream_t st) {
   cudaError_t err = cudaErrorInvalidValue;
-  if (form != 0 && form != 2) return err;
+  if (form != 0 && form != 2 && form != 6) return err;
   dispatch_L(g.Nz, [&](auto Lc) {
     constexpr int NZ = decltype(Lc)::value;
-    err = form == 0 ? sss_z_slots<NZ, 0>(g, P, tw, tq, zin, zout, st) : sss_z_slots<NZ, 2>(g, P, tw, tq, zin, zout, st);
+    err = form == 0 ? sss_z_slots<NZ, 0>(g, P, tw, tq, zin, zout, st)
+        : form == 2 ? sss_z_slots<NZ, 2>(g, P, tw, tq, zin, zout, st)
+                    : sss_z_slots<NZ, 6>(g, P, tw, tq, zin, zout, st);
   });
   return err;
 }
@@ -788,6 +790,21 @@ template <> cudaError_t Launch<T>::ssf_flux_outside(const Geo& g, const void* P,
                                                     int qy, double* out, cudaStream_t st) {
   const unsigned blocks = grid1d(g.S, 256);
   k_ssf_flux_outside<T><<<blocks, 256, 0, st>>>((const V*)P, (const V*)U, g, R, qx, qy, out);
+  k_sum_partials<<<1, 256, 0, st>>>(out, (int)blocks);
+  g_launches += 2;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::sss_giver(const Geo& g, const void* U, void* P, double R, cudaStream_t st) {
+  k_sss_giver<T><<<grid1d(2 * g.S, 256), 256, 0, st>>>((const T*)U, (T*)P, g, R);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+template <> cudaError_t Launch<T>::sss_flux_outside(const Geo& g, const void* P, const void* U, double R, int qx,
+                                                    int qy, int qz, double* out, cudaStream_t st) {
+  const unsigned blocks = grid1d(2 * g.S, 256);
+  k_sss_flux_outside<T><<<blocks, 256, 0, st>>>((const T*)P, (const T*)U, g, R, qx, qy, qz, out);
   k_sum_partials<<<1, 256, 0, st>>>(out, (int)blocks);
   g_launches += 2;
   return cudaGetLastError();

@@ -94,6 +94,10 @@ template <typename T> struct Launch {
                                       double* out, cudaStream_t st);
   static cudaError_t flux_outside(const Geo& g, const void* P, const void* U, double R, double* out,
                                   cudaStream_t st);
+  // the same on SSS (real coefficients, sine letters along x, y and z)
+  static cudaError_t sss_giver(const Geo& g, const void* U, void* P, double R, cudaStream_t st);
+  static cudaError_t sss_flux_outside(const Geo& g, const void* P, const void* U, double R, int qx, int qy, int qz,
+                                      double* out, cudaStream_t st);
   static cudaError_t force_scatter(const Geo& g, const void* fc, void* F, int km, cudaStream_t st);
   static cudaError_t init_ic(const Geo& g, void* U, const double* Eic, const double* mis, int nsh,
                              unsigned long long key, cudaStream_t st);

@@ -481,6 +481,66 @@ __global__ void k_ssf_flux_outside(const C<T>* __restrict__ P, const C<T>* __res
 }
 
 // ---------------------------------------------------------------------------
+// SSS per-sphere energy flux (compute_flux.cc:51-65 on the SSS basis, whose sphere fill
+// and shell product, SSS_pencil_ET.cc:50-70 and 662-678, loop over the real
+// coefficients with kz the real z index): k_sss_giver writes D U into P[0, 3) and the
+// giver D(U on |K| <= R) into P[3, 6), in the padded real layout (Nx, Ny, Nz + 2) of
+// each component; after the transforms P[3 j + i] holds the coefficients of F[u_j G_i]
+// with sine letters qx, qy, qz (bit f); k_sss_flux_outside forms
+// N_i = sum_j D_j F[u_j G_i] (+K_j on a sine series, -K_j on a cosine series) and sums
+// 2 mult N_i D u_i over |K| > R, per block.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_sss_giver(const T* __restrict__ U, T* __restrict__ P, Geo g, double R) {
+  const long long n = 2 * g.S;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lzr = (int)(e % (g.Nz + 2));
+    const long long r = e / (g.Nz + 2);
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    const bool dz = lzr >= g.Nz || sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz);
+    const double Kx = lx * g.kf[0], Ky = ly * g.kf[1], Kz = lzr * g.kf[2];
+    const bool in = sqrt((Kx * Kx + Ky * Ky) + Kz * Kz) <= R;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T u = dz ? (T)0 : U[i * n + e];
+      P[i * n + e] = u;
+      P[(3 + i) * n + e] = in ? u : (T)0;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_sss_flux_outside(const T* __restrict__ P, const T* __restrict__ U, Geo g, double R, int qx,
+                                   int qy, int qz, double* __restrict__ out) {
+  const long long n = 2 * g.S;
+  double s = 0;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int lzr = (int)(e % (g.Nz + 2));
+    const long long r = e / (g.Nz + 2);
+    const int ly = (int)(r % g.Ny), lx = (int)(r / g.Ny);
+    if (lzr >= g.Nz || sss_dealias_zero(g.dealias, lx, ly, lzr, g.Nx, g.Ny, g.Nz)) continue;
+    const double K[3] = {lx * g.kf[0], ly * g.kf[1], lzr * g.kf[2]};
+    const double Kmag = sqrt((K[0] * K[0] + K[1] * K[1]) + K[2] * K[2]);
+    if (!(Kmag > R)) continue;
+    double re = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double nr = 0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int f = 3 * j + i;
+        const int sine = ((j == 0 ? qx : (j == 1 ? qy : qz)) >> f) & 1;
+        nr += (sine ? K[j] : -K[j]) * (double)P[f * n + e];
+      }
+      re += nr * (double)U[i * n + e];
+    }
+    s += 2.0 * multiplicity(3, lx, ly, lzr, g.Nx, g.Ny) * re;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[1 + blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------
 // random-phase helical initial condition (init_cond_energy.cc:67-120 construction;
 // this project's counter-based splitmix64 phases, identical to the oracle)
 // ---------------------------------------------------------------------------

@@ -8,7 +8,8 @@ Inputs (a reference data directory ``<dir>/in/``):
   ``field.N``, ``field.kfactor`` / ``field.L``, ``field.diss_coefficients``,
   ``time.init / final / dt_fixed``, ``force.U_switch / W_switch / T_switch /
   field_procedure / parameters``, ``PHYSICS.Pr_option / Uscaling / Rayleigh / Prandtl`` and
-  ``energy_transfer.flux.no_spheres / radii``.  Kinds and bases: FLUID_INCOMPRESS on
+  ``energy_transfer.flux.no_spheres / radii``, ``io.input_field_procedure`` (1: complex
+  fields, 4: ``io.init_cond_modes``).  Kinds and bases: FLUID_INCOMPRESS on
   FFF, SSF and SSS; RBC on SFF, SSF and SSS; SCALAR_INCOMPRESS and MHD_INCOMPRESS on
   FFF (``diss_coefficients`` = [nu, kappa] or [nu, eta]).  Any other kind or basis is
   refused by name (NotImplementedError), never silently changed.
@@ -668,8 +669,8 @@ class Output:
         return row
 
     def flux(self, u, t: float):
-        if self.plan.basis not in ("FFF", "SSF"):
-            raise NotImplementedError("flux.d is written for fluid runs on FFF and SSF")
+        if self.plan.basis not in ("FFF", "SSF", "SSS"):
+            raise NotImplementedError("flux.d is written for fluid runs on FFF, SSF and SSS")
         p = self.plan
         # Compute_flux runs Compute_nlin(U, Giver), which dealiases U in place
         # (compute_nlin_ET_VF.cc:73-76): the run goes on from the dealiased state

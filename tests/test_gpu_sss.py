@@ -239,3 +239,48 @@ def test_sss_rbc_scalings_match_oracle(cuda, pr, us):
     plan.status()
     assert rel(from_padded(u, N[2]), Uo) < 1e-12
     assert rel(from_padded(T, N[2])[0], To) < 1e-12
+
+
+def _sss_state(g, seed, width):
+    """a random solenoidal field with the SSS parities, energy at |K| <~ width, unit norm"""
+    rng = np.random.default_rng(seed)
+    U = np.stack([R.forward(g, rng.standard_normal(g.rshape), R.SSS_PARITY[v]) for v in ("Vx", "Vy", "Vz")])
+    U = -np.exp(-(g.Kmag() / width) ** 2) * R.project_rhs(g, U)
+    return U / np.sqrt(np.sum(U ** 2))
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("N,dealias", [((16, 16, 16), "reference"), ((32, 16, 32), "none"),
+                                       ((32, 32, 16), "two_thirds")])
+def test_sss_flux_matches_oracle(cuda, N, dealias, prec):
+    """Pi(R) on SSS, the reference's per-sphere algorithm (EnergyTr::Compute_flux,
+    compute_flux.cc:51-65, with SSS_PENCIL's sphere fill and outside sum over the real
+    coefficients, SSS_pencil_ET.cc:50-70, 662-678) against the oracle's flux_per_sphere:
+    FP64 to 1e-12, FP32 to 2e-6 of max|Pi|; radii in any order."""
+    import tarang_b200 as tb
+    mode = {"none": 0, "reference": 1, "two_thirds": 2}[dealias]
+    g = R.Grid(N, KF, "SSS")
+    U = _sss_state(g, 23, 10.0)
+    radii = [7.0, 1.0, 3.5, 10.0, 14.0, 20.0]
+    want = R.flux_per_sphere(g, U, radii, mode)
+    assert np.max(np.abs(want)) > 0
+    plan = tb.Plan(N, basis="SSS", precision=prec, kfactor=KF, dealias=dealias)
+    got = plan.flux(_dev(U, cuda, prec), radii)
+    tol = 1e-12 if prec == "f64" else 2e-6
+    assert np.max(np.abs(got - want)) <= tol * np.max(np.abs(want)), (got, want)
+    plan.close()
+
+
+@pytest.mark.parametrize("dealias", ["reference", "two_thirds"])
+def test_sss_dealias_field_matches_oracle(cuda, dealias):
+    """ts_dealias_field on SSS real coefficients: the oracle's dealias, bit for bit."""
+    import tarang_b200 as tb
+    mode = {"reference": 1, "two_thirds": 2}[dealias]
+    N = (32, 16, 32)
+    g = R.Grid(N, KF, "SSS")
+    U = _sss_state(g, 5, 40.0)
+    plan = tb.Plan(N, basis="SSS", precision="f64", kfactor=KF, dealias=dealias)
+    u = _dev(U, cuda, "f64")
+    plan.dealias(u)
+    assert np.array_equal(from_padded(u, N[2]), R.dealias(g, U, mode))
+    plan.close()
