@@ -473,12 +473,36 @@ def _strong_reality(rp: RunParams, A: np.ndarray) -> np.ndarray:
     return B
 
 
+def init_cond_energy_spectrum(data_dir: str, plan, rp: RunParams, seed: int = 0):
+    """FluidIO::Init_cond_energy_helicity_spectrum for ``io.input_field_procedure: 5`` on an
+    FFF fluid run (init_cond_energy.cc:67-120): the shell energies E(k) of
+    ``<data_dir>/in/initial.txt`` (its first Blitz array, Global::Read_IC_energy_supply_arrays,
+    Global_read.cc:822-833), a solenoidal random-phase field with exactly that energy per
+    shell, no rescaling, then the strong reality condition (init_cond_main.cc:80-84).  The
+    reference seeds its phases from the clock; here they come from ``seed`` (splitmix64), so
+    a run is repeatable.  A nonzero helicity spectrum (the second array), other kinds and
+    other bases are refused by name."""
+    if rp.kind != "FLUID_INCOMPRESS" or rp.basis != "FFF":
+        raise NotImplementedError(f"io.input_field_procedure 5 for {rp.kind} on {rp.basis}: the FFF fluid only")
+    arrs = read_blitz_arrays(os.path.join(data_dir, "in", "initial.txt"))
+    if not arrs:
+        raise ValueError(f"{data_dir}/in/initial.txt: no E(k) array")
+    if len(arrs) > 1 and np.any(arrs[1] != 0):
+        raise NotImplementedError("io.input_field_procedure 5 with a helicity spectrum: non-helical fields only")
+    u = plan.field(3)
+    plan.init_energy_spectrum(arrs[0], seed, 0.0, u)
+    return u
+
+
 def read_init_cond(data_dir: str, plan, rp: RunParams):
     """FluidIO::Read_init_cond (init_cond_main.cc:48-56): ``io.input_field_procedure: 1``
     (Init_cond_complex_field init_cond_field.cc:49-58) reads the run's complex fields from
     ``<data_dir>/in/`` as ``save_state`` writes them; ``4`` sets the listed modes
-    (``init_cond_modes``).  Returns (fields, t, step); the run continues from time t.
-    Other procedures are refused by name."""
+    (``init_cond_modes``); ``5`` builds an FFF fluid field from E(k)
+    (``init_cond_energy_spectrum``).  Returns (fields, t, step); the run continues from
+    time t.  Other procedures are refused by name."""
+    if rp.input_field_procedure == 5:
+        return [init_cond_energy_spectrum(data_dir, plan, rp)], rp.t_init, 0
     if rp.input_field_procedure == 4:
         import torch
         want = torch.complex64 if plan.precision == "f32" else torch.complex128
@@ -488,8 +512,7 @@ def read_init_cond(data_dir: str, plan, rp: RunParams):
         return fields, rp.t_init, 0
     if rp.input_field_procedure != 1:
         raise NotImplementedError(f"io.input_field_procedure {rp.input_field_procedure}: "
-                                  "1 (complex fields from in/) and 4 (modes) only; seeded spectra use "
-                                  "Plan.init_energy_spectrum")
+                                  "1 (complex fields from in/), 4 (modes) and 5 (E(k) of an FFF fluid) only")
     fields, t, step = load_state(os.path.join(data_dir, "in"), plan, rp.kind)
     if rp.kind == "RBC" and rp.pr_option in ("PRZERO", "PRINFTY"):
         # Init_cond_RBC_complex_field (init_cond_field.cc:176-190): the slaved field is

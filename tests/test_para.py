@@ -835,3 +835,44 @@ def test_init_cond_modes_rbc_steps_like_the_oracle(cuda, tmp_path, pr):
     assert np.linalg.norm(u.cpu().numpy() - Uo) <= 1e-12 * np.linalg.norm(Uo)
     assert np.linalg.norm(T[0].cpu().numpy() - To) <= 1e-12 * max(np.linalg.norm(To), 1e-300)
     plan.close()
+
+
+def _write_initial(tmp_path, E, H=None):
+    def arr(a):
+        return f"({0},{len(a) - 1})\n[ " + " ".join(f"{x:.17g}" for x in a) + " ]\n"
+    (tmp_path / "in").mkdir(exist_ok=True)
+    (tmp_path / "in" / "initial.txt").write_text(arr(E) + arr(np.zeros(len(E)) if H is None else H))
+
+
+def test_init_cond_energy_spectrum_refusals(tmp_path):
+    """io.input_field_procedure 5 is taken for the FFF fluid with a zero helicity spectrum;
+    other kinds and a helical spectrum are refused by name."""
+    rp = _modes_para(tmp_path, KIND_DIRS["rbc_2d"], "io:\n    input_field_procedure: 5\n")
+    assert rp.input_field_procedure == 5
+    with pytest.raises(NotImplementedError):
+        para.read_init_cond(str(tmp_path), None, rp)
+    rp = _modes_para(tmp_path, FFF_DIR, "io:\n    input_field_procedure: 5\n")
+    _write_initial(tmp_path, np.linspace(0, 1, 8), np.full(8, 0.1))
+    with pytest.raises(NotImplementedError):
+        para.read_init_cond(str(tmp_path), None, rp)
+
+
+@pytest.mark.gpu
+def test_init_cond_energy_spectrum_matches_oracle(cuda, tmp_path):
+    """io.input_field_procedure 5 on an FFF fluid run: E(k) from in/initial.txt, the
+    random-phase construction of init_cond_energy.cc:67-120 with the splitmix64 phases of
+    seed 0, no rescaling: the oracle's field to 1e-13, and the run steps."""
+    from oracle import tarang_ref as R
+    rp = _modes_para(tmp_path, FFF_DIR, "io:\n    input_field_procedure: 5\n")
+    g = R.Grid(rp.N, rp.kfactor)
+    E = R.spectrum_k4_gauss(g.n_shells(), 3.0) * 0.7
+    _write_initial(tmp_path, E)
+    (tmp_path / "in" / "forcing.txt").write_text(open(os.path.join(FFF_DIR, "in", "forcing.txt")).read())
+    plan, rp2 = para.plan_from_dir(str(tmp_path), precision="f64")
+    fields, t, step = para.read_init_cond(str(tmp_path), plan, rp2)
+    want = R.init_energy_spectrum(g, E, 0, None)
+    u = fields[0].cpu().numpy()
+    assert np.abs(u - want).max() <= 1e-13 * np.abs(want).max()
+    para.advance(plan, rp2.kind, fields, 2)
+    assert np.isfinite(fields[0].cpu().numpy()).all()
+    plan.close()
