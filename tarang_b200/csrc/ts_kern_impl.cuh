@@ -126,10 +126,11 @@ constexpr Tile str_cand(int L, int v) {
        : v == 3 ? Tile{str_e(L), str_cw(L), 5 - str_nt(L)}
        : v == 4 ? Tile{str_e(L), str_cw(L), 4}
        : v == 5 ? (wide1024(L) ? Tile{32, 8, 1} : Tile{0, 0, 0})
+       : v == 6 ? (wide1024(L) ? Tile{32, 16, 1} : Tile{0, 0, 0})
                 : Tile{0, 0, 0};
 }
 constexpr bool str_valid(int L, int v) {
-  return v == 0 || (v < NCAND && tile_fits(L, str_cand(L, v), str_tiles(str_cand(L, v).NT)) &&
+  return v == 0 || (v == 6 && wide1024(L) && tile_fits(L, str_cand(L, 6), 1)) || (v < NCAND && tile_fits(L, str_cand(L, v), str_tiles(str_cand(L, v).NT)) &&
                     !tile_eq(str_cand(L, v), str_cand(L, 0)) && (v < 2 || !tile_eq(str_cand(L, v), str_cand(L, 1))) &&
                     (v < 3 || !tile_eq(str_cand(L, v), str_cand(L, 2))) &&
                     (v < 4 || !tile_eq(str_cand(L, v), str_cand(L, 3))) &&
@@ -182,8 +183,15 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
     // (on B200 at 1024^3 7.7 ms against 8.9 for the two-tile, 16-element form; the y
     // inverse and the x forward pass stayed faster with the latter) and candidate 5 is
     // then the 16-element form
-    const int vv = (wide1024(LL) && dir < 0 && axis == 1) ? (v == 0 ? 5 : (v == 5 ? 0 : v)) : v;
+    int vv = (wide1024(LL) && dir < 0 && axis == 1) ? (v == 0 ? 5 : (v == 5 ? 0 : v)) : v;
+    // the x forward pass of 1024 points in FP32 (the split form's FFT): 16-column tiles,
+    // 128-byte row segments, 32 elements per thread, one staging tile (tile 6, not a tuning
+    // candidate).  An x row is Ny*Hz complex long (4.2 MB at 1024^3), so every row of a
+    // tile is a separate memory page; twice the bytes per row visit took the forward x
+    // FFT + epilogue from 20.4 to 17.0 ms per right-hand side at 1024^3 on B200
+    if (wide1024(LL) && axis == 0 && dir < 0) vv = 6;
     switch (vv) {
+      case 6: with_str_tile<LL, 6>(run); break;
       case 1: with_str_tile<LL, 1>(run); break;
       case 2: with_str_tile<LL, 2>(run); break;
       case 3: with_str_tile<LL, 3>(run); break;
