@@ -179,11 +179,12 @@ template <> cudaError_t Launch<T>::strided(const Geo& g, int axis, int dir, void
       if (dir < 0) launch(k_strided_fft<T, LL, E, CW, -1, NT>);
       else launch(k_strided_fft<T, LL, E, CW, 1, NT>);
     };
-    // the y forward pass of 1024 points in FP32: the one-tile, 32-element form is the rule
-    // (on B200 at 1024^3 7.7 ms against 8.9 for the two-tile, 16-element form; the y
-    // inverse and the x forward pass stayed faster with the latter) and candidate 5 is
+    // the y passes of 1024 points in FP32: the one-tile, 32-element form on 16-column
+    // tiles (tile 6) is the rule (on B200 at 1024^3: y inverse 9.9 ms against 10.4 for the
+    // two-tile, 16-element form on 8 columns; y forward 7.5 against 7.6 for 32 elements on
+    // 8 columns and 8.9 for the 16-element form); for the y forward pass candidate 5 is
     // then the 16-element form
-    int vv = (wide1024(LL) && dir < 0 && axis == 1) ? (v == 0 ? 5 : (v == 5 ? 0 : v)) : v;
+    int vv = (wide1024(LL) && axis == 1) ? (v == 0 ? 6 : ((dir < 0 && v == 5) ? 0 : v)) : v;
     // the x forward pass of 1024 points in FP32 (the split form's FFT): 16-column tiles,
     // 128-byte row segments, 32 elements per thread, one staging tile (tile 6, not a tuning
     // candidate).  An x row is Ny*Hz complex long (4.2 MB at 1024^3), so every row of a
